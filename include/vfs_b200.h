@@ -1,0 +1,186 @@
+/*
+ * vfs_b200.h — C ABI of the B200 (sm_100a) fractional-step projection path of the
+ * VFS-Geophysics curvilinear immersed-boundary solver.
+ *
+ * One context = one structured block on one GPU, one CUDA stream.  Every field lives
+ * in device memory for the life of the context.  Host arrays cross the boundary only
+ * through vfs_set_field / vfs_get_field, in the reference's own layout: the PETSc DA of
+ * (IM+1) x (JM+1) x (KM+1) points, [k][j][i] with i fastest, vector fields as
+ * interleaved {x,y,z} doubles (struct Cmpnts, variables.h:45-57).
+ *
+ * All entry points return 0 on success or a VFS_ERR_* code; vfs_last_error() gives a
+ * one-line message.  No entry point exits the process, and no kernel waits on a flag.
+ *
+ * Each operator names the reference function it replaces (file:line in the reference
+ * solver's sources).  Operators read and write the context's fields exactly where the
+ * reference reads and writes its UserCtx vectors.
+ */
+#ifndef VFS_B200_H
+#define VFS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VFS_OK 0
+#define VFS_ERR_INVALID 1        /* bad argument / unsupported option */
+#define VFS_ERR_CUDA 2           /* CUDA runtime error (message in vfs_last_error) */
+#define VFS_ERR_NOT_CONVERGED 3  /* Poisson solver hit its iteration cap */
+#define VFS_ERR_NO_DEVICE 4      /* no CUDA device / kernels missing for this GPU */
+#define VFS_ERR_STATE 5          /* operator called before its prerequisites */
+
+typedef struct vfs_ctx vfs_ctx;
+
+/* Run configuration: the subset of the reference's control.dat / bcs.dat options that
+ * the projection path reads (main.c:1593-2250, init.c:52-69, init.c:562-568). */
+typedef struct {
+  int IM, JM, KM;        /* grid nodes per direction (grid.dat header, init.c:374) */
+  int bctype[6];         /* bcs.dat codes: i-, i+, j-, j+, k-, k+ */
+  int i_periodic, j_periodic, k_periodic; /* main.c:191-195 */
+  int immersed;          /* -imm: 0 none, 1 sharp-interface IB (nvert masking + QUICK) */
+  int les;               /* -les: 0 laminar, 2 dynamic Smagorinsky eddy viscosity */
+  int inletprofile;      /* -inlet (bcs.c:399-466) */
+  int reserved_i[8];
+  double ren;            /* Reynolds number (user->ren) */
+  double dt;             /* time step (user->dt) */
+  double st;             /* Strouhal scaling (user->st) */
+  double inlet_flux;     /* -inlet_flux target bulk flux (main.c:198; <0: unset) */
+  double mean_pressure_gradient; /* -mean_pressure_gradient (main.c) */
+  int dpdz_set;          /* non-zero: impose mean_pressure_gradient (momentum.c:379) */
+  int reserved_j[7];
+  double reserved_d[8];
+} vfs_config;
+
+/* Field identifiers for vfs_set_field / vfs_get_field (dof in brackets). */
+enum {
+  VFS_UCONT = 0,    /* [3] contravariant face fluxes Ucont (variables.h:561) */
+  VFS_UCAT = 1,     /* [3] Cartesian centre velocity Ucat (variables.h:562) */
+  VFS_P = 2,        /* [1] pressure P */
+  VFS_PHI = 3,      /* [1] pressure correction Phi */
+  VFS_NVERT = 4,    /* [1] IB flags 0/1/3 as doubles (stored as uint8 on the device) */
+  VFS_NU_T = 5,     /* [1] eddy viscosity lNu_t */
+  VFS_RHS = 6,      /* [3] momentum right-hand side (Formfunction_2 accumulates here) */
+  VFS_DP = 7,       /* [3] pressure gradient dP (Pressure_Gradient output) */
+  VFS_UCONT_O = 8,  /* [3] Ucont of the previous time step */
+  VFS_UCAT_O = 9,   /* [3] lUcat_old (slip-wall ghost source) */
+  VFS_B = 10,       /* [1] Poisson right-hand side on the grid (PoissonRHS2 output) */
+  VFS_CENT = 11,    /* [3] cell centres */
+  VFS_CSI = 12, VFS_ETA = 13, VFS_ZET = 14, VFS_AJ = 15,     /* centre metrics */
+  VFS_ICSI = 16, VFS_IETA = 17, VFS_IZET = 18, VFS_IAJ = 19, /* i-face metrics */
+  VFS_JCSI = 20, VFS_JETA = 21, VFS_JZET = 22, VFS_JAJ = 23, /* j-face metrics */
+  VFS_KCSI = 24, VFS_KETA = 25, VFS_KZET = 26, VFS_KAJ = 27, /* k-face metrics */
+  VFS_CS = 28,      /* [1] dynamic Smagorinsky coefficient lCs */
+  VFS_NFIELDS = 29
+};
+
+/* Scalars for vfs_set_scalar / vfs_get_scalar. */
+enum {
+  VFS_S_MEAN_K_FLUX = 0,  /* user->mean_k_flux (Calc_k_Flux, rhs2.c:1562) */
+  VFS_S_MEAN_K_AREA = 1,  /* user->mean_k_area (Calc_Inlet_Area, bcs.c:216) */
+  VFS_S_INLET_FLUX = 2,   /* inlet_flux global */
+  VFS_S_INLET_AREA = 3,   /* inletArea (bcs.c:212) */
+  VFS_S_DT = 4, VFS_S_REN = 5, VFS_S_ST = 6,
+  VFS_NSCALARS = 7
+};
+
+/* Poisson solver options (replaces PoissonSolver_Hypre, poisson_hypre.c:498). */
+typedef struct {
+  int precision;     /* 0: mixed (FP32 V-cycle inside FP64 FGMRES), 1: all-FP64 */
+  int restart;       /* FGMRES restart length (default 30) */
+  int max_iter;      /* outer iteration cap (default 200) */
+  int levels;        /* multigrid levels including the finest (default 4) */
+  int pre_smooth, post_smooth; /* Chebyshev steps per level (default 2, 2) */
+  int coarse_iters;  /* smoothing steps on the coarsest level (default 16) */
+  int reserved[5];
+  double rtol;       /* relative residual target (default 1e-10) */
+  double atol;       /* absolute residual target (default 0) */
+  double reserved_d[4];
+} vfs_solve_opts;
+
+typedef struct {
+  int iterations;       /* outer FGMRES iterations taken */
+  int converged;        /* 1 if rtol/atol met */
+  double r0, rfinal;    /* initial / final residual 2-norms */
+  double ms;            /* device time of the solve */
+  double reserved[4];
+} vfs_solve_stats;
+
+typedef struct {
+  double max_div;       /* Divergence() maximum (main.c:1083-1090) after the step */
+  double mean_k_flux;   /* Calc_k_Flux result at the start of the step */
+  vfs_solve_stats poisson;
+  double ms;            /* device time of the whole step */
+  double reserved[4];
+} vfs_step_stats;
+
+/* ---- context ---------------------------------------------------------------- */
+int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out);
+int vfs_destroy(vfs_ctx *ctx);
+const char *vfs_last_error(const vfs_ctx *ctx);   /* ctx may be NULL: last global error */
+int vfs_dims(const vfs_ctx *ctx, int *mx, int *my, int *mz);
+int vfs_synchronize(vfs_ctx *ctx);
+/* Kernels launched by this context since creation (a diagnostic counter). */
+long long vfs_launch_count(const vfs_ctx *ctx);
+
+/* Host <-> device copies in the reference layout (mx*my*mz*dof doubles). */
+int vfs_set_field(vfs_ctx *ctx, int field, const double *host);
+int vfs_get_field(vfs_ctx *ctx, int field, double *host);
+int vfs_set_scalar(vfs_ctx *ctx, int which, double value);
+int vfs_get_scalar(vfs_ctx *ctx, int which, double *value);
+/* Device address of a field's component (SoA, mx*my*mz doubles), for zero-copy callers. */
+int vfs_field_device_ptr(vfs_ctx *ctx, int field, int component, void **dptr);
+
+/* ---- hot-path operators (each replaces the cited reference function) --------------- */
+
+/* Contra2Cart / Contra2Cart_2 (rhs.c:27, rhs.c:57): Ucat from Ucont at fluid cells,
+ * then the boundary ghost values of Ucat. */
+int vfs_contra2cart(vfs_ctx *ctx);
+
+/* Formfunction_2(user, Rhs, scale) (momentum.c:456): ADDS scale * RHS into VFS_RHS. */
+int vfs_formfunction2(vfs_ctx *ctx, double scale);
+
+/* Pressure_Gradient(user, dP) (momentum.c:197): writes VFS_DP. */
+int vfs_pressure_gradient(vfs_ctx *ctx);
+
+/* Calc_k_Flux (rhs2.c:1562): mean k-face flux -> VFS_S_MEAN_K_FLUX. */
+int vfs_calc_k_flux(vfs_ctx *ctx, double *mean_k_flux);
+
+/* RungeKutta (rhs.c:1578), explicit momentum predictor, 4 stages. */
+int vfs_runge_kutta(vfs_ctx *ctx);
+
+/* PoissonLHSNew (poisson.c:971): builds the 19-point operator of the fluid cells and
+ * the multigrid hierarchy.  Call again whenever VFS_NVERT or the metrics change. */
+int vfs_poisson_lhs(vfs_ctx *ctx);
+
+/* PoissonRHS2 (poisson.c:1774) with the volume-weighted compatibility shift of
+ * Remove_Nullspace_Scale (poisson_hypre.c:110): writes VFS_B. */
+int vfs_poisson_rhs(vfs_ctx *ctx);
+
+/* Poisson solve for VFS_PHI (replaces PoissonSolver_Hypre, poisson_hypre.c:498,
+ * including Remove_Nullspace poisson_hypre.c:194 and Convert_Phi2_Phi poisson.c:92). */
+int vfs_poisson_solve(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_solve_stats *stats);
+
+/* y = A x with the operator of vfs_poisson_lhs, on the grid layout (mx*my*mz doubles;
+ * entries of non-fluid cells are ignored in x and returned as 0 in y). */
+int vfs_poisson_apply(vfs_ctx *ctx, const double *x_host, double *y_host);
+
+/* UpdatePressure (poisson.c:3144): P += Phi at fluid cells, P = 0 where nvert > 1.1. */
+int vfs_update_pressure(vfs_ctx *ctx);
+
+/* Projection (poisson.c:2707): Ucont -= dt*st*G(Phi) on fluid faces, periodic copies,
+ * then Contra2Cart. */
+int vfs_projection(vfs_ctx *ctx);
+
+/* Divergence (main.c:1047): max |div Ucont * aj| over cells with an all-fluid 7-point
+ * neighbourhood. */
+int vfs_divergence(vfs_ctx *ctx, double *max_div);
+
+/* One projection time step: Calc_k_Flux, Pressure_Gradient, RungeKutta, Poisson
+ * (RHS, solve), UpdatePressure, Projection, Divergence (solvers.c:562-1390 for
+ * implicit=0).  opts may be NULL for the defaults. */
+int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VFS_B200_H */

@@ -1,0 +1,220 @@
+// Driver for the shim-compiled reference (oracle/_ref/libvfsref.so).
+//
+// Test infrastructure only.  It replaces the reference's main()/Flow_Solver() with a
+// handful of extern "C" entry points so the parity tests can run the reference's own
+// hot-path functions (momentum.c, rhs.c, poisson.c, main.c, les.c ...) on synthetic
+// grid.dat/bcs.dat inputs and read every field back.  The reference's scalar globals
+// (i_periodic, les, immersed, ...) are plain C symbols of this library and are set by
+// the caller by name.
+//
+// Set-up follows the reference: MG_Initial (init.c:270) reads grid.dat and bcs.dat,
+// creates the DA and every Vec, and calls FormMetrics (metrics.c:4); main() then adds
+// lUstar (main.c:2245) and Flow_Solver adds Fp/Div*/Visc* (solvers.c:779-785).
+#include "variables.h"
+
+#include <string>
+
+extern PetscInt ti, tistart;
+extern char path[256], gridfile[256];
+extern PetscReal L_dim;
+extern int block_number;
+extern PetscErrorCode VolumeFlux(UserCtx *user, PetscReal *ibm_Flux, PetscReal *ibm_Area, PetscInt flg);
+extern PetscErrorCode VolumeFlux(UserCtx *user, Vec lUcor, PetscReal *ibm_Flux, PetscReal *ibm_Area);
+extern void Convert_Phi2_Phi(UserCtx *user);
+extern PetscInt setup_lidx2(UserCtx *user);
+extern void Pressure_Gradient(UserCtx *user, Vec dP);
+extern void IB_BC(UserCtx *user);
+extern PetscErrorCode PoissonRHS2(UserCtx *user, Vec B);
+extern PetscErrorCode ibm_interpolation_advanced(UserCtx *user);
+extern void PoissonRHS2_hypre(UserCtx *user, HYPRE_IJVector &B, int i_lower);
+extern void Remove_Nullspace(UserCtx *user, HYPRE_IJVector &B, int i_lower);
+
+static UserMG g_usermg;
+static UserCtx *g_user = 0;
+static IBMNodes *g_ibm = 0;
+static FSInfo *g_fsi = 0;
+static Vec g_B = 0;  // compressed Poisson right-hand side (PoissonRHS2 output)
+
+static Vec field_vec(const std::string &n) {
+  UserCtx *u = g_user;
+  if (n == "Ucont") return u->Ucont;
+  if (n == "lUcont") return u->lUcont;
+  if (n == "Ucat") return u->Ucat;
+  if (n == "lUcat") return u->lUcat;
+  if (n == "lUcat_old") return u->lUcat_old;
+  if (n == "Ucont_o") return u->Ucont_o;
+  if (n == "lUcont_o") return u->lUcont_o;
+  if (n == "P") return u->P;
+  if (n == "lP") return u->lP;
+  if (n == "Phi") return u->Phi;
+  if (n == "lPhi") return u->lPhi;
+  if (n == "Nvert") return u->Nvert;
+  if (n == "lNvert") return u->lNvert;
+  if (n == "Nvert_o") return u->Nvert_o;
+  if (n == "lNvert_o") return u->lNvert_o;
+  if (n == "Rhs") return u->Rhs;
+  if (n == "dP") return u->dP;
+  if (n == "lNu_t") return u->lNu_t;
+  if (n == "lCs") return u->lCs;
+  if (n == "lUstar") return u->lUstar;
+  if (n == "Gid") return u->Gid;
+  if (n == "Fp") return u->Fp;
+  if (n == "Div1") return u->Div1;
+  if (n == "Div2") return u->Div2;
+  if (n == "Div3") return u->Div3;
+  if (n == "Visc1") return u->Visc1;
+  if (n == "Visc2") return u->Visc2;
+  if (n == "Visc3") return u->Visc3;
+  if (n == "lCent") return u->lCent;
+  if (n == "lCsi") return u->lCsi;
+  if (n == "lEta") return u->lEta;
+  if (n == "lZet") return u->lZet;
+  if (n == "lAj") return u->lAj;
+  if (n == "lICsi") return u->lICsi;
+  if (n == "lIEta") return u->lIEta;
+  if (n == "lIZet") return u->lIZet;
+  if (n == "lIAj") return u->lIAj;
+  if (n == "lJCsi") return u->lJCsi;
+  if (n == "lJEta") return u->lJEta;
+  if (n == "lJZet") return u->lJZet;
+  if (n == "lJAj") return u->lJAj;
+  if (n == "lKCsi") return u->lKCsi;
+  if (n == "lKEta") return u->lKEta;
+  if (n == "lKZet") return u->lKZet;
+  if (n == "lKAj") return u->lKAj;
+  if (n == "Phi2") return u->Phi2;
+  if (n == "B") return g_B;
+  if (n == "coor") { Vec c; DAGetGhostedCoordinates(u->da, &c); return c; }
+  return 0;
+}
+
+extern "C" {
+
+// Reads <dir>/grid.dat and <dir>/bcs.dat with the reference's MG_Initial.  The caller
+// sets the reference globals that MG_Initial consults (les, immersed, rans ...) first.
+int ref_setup(const char *dir) {
+  strncpy(path, dir, sizeof(path) - 1);
+  strcpy(gridfile, "grid.dat");
+  L_dim = 1.0;
+  memset(&g_usermg, 0, sizeof(g_usermg));
+  g_ibm = (IBMNodes *)calloc(4, sizeof(IBMNodes));
+  g_fsi = (FSInfo *)calloc(4, sizeof(FSInfo));
+  if (MG_Initial(&g_usermg, g_ibm)) return 1;
+  g_user = g_usermg.mgctx[g_usermg.mglevels - 1].user;
+  VecDuplicate(g_user->lP, &g_user->lUstar);
+  VecDuplicate(g_user->lUcont, &g_user->Fp);
+  VecDuplicate(g_user->lUcont, &g_user->Div1);
+  VecDuplicate(g_user->lUcont, &g_user->Div2);
+  VecDuplicate(g_user->lUcont, &g_user->Div3);
+  VecDuplicate(g_user->lUcont, &g_user->Visc1);
+  VecDuplicate(g_user->lUcont, &g_user->Visc2);
+  VecDuplicate(g_user->lUcont, &g_user->Visc3);
+  VecDuplicate(g_user->Ucont, &g_user->Rhs);
+  if (!g_user->lNu_t) VecDuplicate(g_user->lP, &g_user->lNu_t);
+  if (!g_user->lCs) VecDuplicate(g_user->lP, &g_user->lCs);
+  return 0;
+}
+
+void ref_dims(int *mx, int *my, int *mz) {
+  *mx = g_user->info.mx; *my = g_user->info.my; *mz = g_user->info.mz;
+}
+
+UserCtx *ref_user(void) { return g_user; }
+
+void ref_set_params(double ren, double dt, double st) { g_user->ren = ren; g_user->dt = dt; g_user->st = st; }
+void ref_get_params(double *ren, double *dt, double *st) { *ren = g_user->ren; *dt = g_user->dt; *st = g_user->st; }
+void ref_set_bctype(const int *bc) { for (int q = 0; q < 6; q++) g_user->bctype[q] = bc[q]; }
+void ref_get_bctype(int *bc) { for (int q = 0; q < 6; q++) bc[q] = g_user->bctype[q]; }
+void ref_get_kflux(double *flux, double *area) { *flux = g_user->mean_k_flux; *area = g_user->mean_k_area; }
+void ref_set_kflux(double flux, double area) { g_user->mean_k_flux = flux; g_user->mean_k_area = area; }
+
+// Entries of a named Vec (mx*my*mz*dof for DA vectors); -1 if unknown.
+long ref_field_size(const char *name) {
+  Vec v = field_vec(name);
+  return v ? (long)v->n : -1;
+}
+int ref_get_field(const char *name, double *out) {
+  Vec v = field_vec(name);
+  if (!v) return 1;
+  memcpy(out, v->data, sizeof(double) * v->n);
+  return 0;
+}
+int ref_set_field(const char *name, const double *in) {
+  Vec v = field_vec(name);
+  if (!v) return 1;
+  memcpy(v->data, in, sizeof(double) * v->n);
+  return 0;
+}
+
+// ---- hot-path entry points, each a direct call of the reference function
+int ref_contra2cart(void) { Contra2Cart(g_user); return 0; }
+int ref_formfunction2(double scale) { return Formfunction_2(g_user, g_user->Rhs, scale); }
+int ref_pressure_gradient(void) { Pressure_Gradient(g_user, g_user->dP); return 0; }
+int ref_calc_k_flux(void) { Calc_k_Flux(g_user); return 0; }
+int ref_runge_kutta(void) { return RungeKutta(g_user, g_ibm, g_fsi); }
+int ref_form_bcs(void) { return FormBCS(g_user, g_fsi); }
+int ref_inflow_flux(void) { return InflowFlux(g_user); }
+int ref_ib_bc(void) { IB_BC(g_user); return 0; }
+int ref_update_pressure(void) { return UpdatePressure(g_user); }
+int ref_projection(void) { return Projection(g_user); }
+int ref_divergence(void) { return Divergence(g_user); }
+int ref_les(int recompute_cs) {
+  if (recompute_cs) Compute_Smagorinsky_Constant_1(g_user, g_user->lUcont, g_user->lUcat);
+  Compute_eddy_viscosity_LES(g_user);
+  return 0;
+}
+int ref_volume_flux(double *flux, double *area) {
+  return VolumeFlux(g_user, g_user->Ucont, flux, area);
+}
+
+// PoissonLHSNew (poisson.c:971); the matrix stays recorded in user->A.
+int ref_poisson_lhs(void) {
+  g_user->assignedA = PETSC_FALSE;
+  return PoissonLHSNew(g_user, g_ibm, g_user->ibm_intp);
+}
+long ref_poisson_csr(int *row_ptr, int *col, double *val, int *m) {
+  return shim_mat_to_csr(g_user->A, row_ptr, col, val, m);
+}
+// PoissonRHS2 (poisson.c:1774) into a compressed vector sized like Phi2.
+int ref_poisson_rhs2(void) {
+  if (g_B) VecDestroy(g_B);
+  VecDuplicate(g_user->Phi2, &g_B);
+  return PoissonRHS2(g_user, g_B);
+}
+// PoissonRHS2_hypre (poisson_hypre.c:330, with Remove_Nullspace_Scale) into out[0..n);
+// returns the number of unknowns (Phi2 size) or -1.
+static HYPRE_IJVector g_ijb = 0;
+int ref_poisson_rhs2_hypre(double *out) {
+  int n = 0;
+  VecGetLocalSize(g_user->Phi2, &n);
+  if (g_ijb) HYPRE_IJVectorDestroy(g_ijb);
+  HYPRE_IJVectorCreate(PETSC_COMM_WORLD, 0, n - 1, &g_ijb);
+  PoissonRHS2_hypre(g_user, g_ijb, 0);
+  int m = 0;
+  double *d = shim_ij_data(g_ijb, &m);
+  if (out) memcpy(out, d, sizeof(double) * m);
+  return m;
+}
+// Remove_Nullspace (poisson_hypre.c:194) applied to a compressed solution in place.
+int ref_remove_nullspace(double *x, int n) {
+  HYPRE_IJVector v;
+  HYPRE_IJVectorCreate(PETSC_COMM_WORLD, 0, n - 1, &v);
+  int m = 0;
+  double *d = shim_ij_data(v, &m);
+  memcpy(d, x, sizeof(double) * n);
+  Remove_Nullspace(g_user, v, 0);
+  memcpy(x, d, sizeof(double) * n);
+  HYPRE_IJVectorDestroy(v);
+  return 0;
+}
+int ref_phi2_size(void) { int n = 0; VecGetLocalSize(g_user->Phi2, &n); return n; }
+
+// Convert_Phi2_Phi (poisson.c:92): compressed solution -> grid Phi (and lPhi).
+int ref_convert_phi2_phi(void) {
+  Convert_Phi2_Phi(g_user);
+  DAGlobalToLocalBegin(g_user->da, g_user->Phi, INSERT_VALUES, g_user->lPhi);
+  DAGlobalToLocalEnd(g_user->da, g_user->Phi, INSERT_VALUES, g_user->lPhi);
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,423 @@
+// C-ABI layer: context life cycle, host<->device field transfer in the reference's
+// AoS DA layout, scalars, errors and the operator entry points declared in
+// include/vfs_b200.h.
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+
+#include "vfs_internal.cuh"
+
+using namespace vfs;
+
+static std::string g_last_err;
+
+namespace vfs {
+
+int set_err(Ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  g_last_err = msg;
+  return code;
+}
+
+int check_launch(Ctx *c, const char *what) {
+  c->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return VFS_OK;
+}
+
+V3 field3(Ctx *c, int f) { return V3{c->f[f][0], c->f[f][1], c->f[f][2]}; }
+
+Metrics metrics(Ctx *c) {
+  Metrics m;
+  m.csi = cv(field3(c, VFS_CSI)); m.eta = cv(field3(c, VFS_ETA)); m.zet = cv(field3(c, VFS_ZET));
+  m.aj = c->f[VFS_AJ][0];
+  m.icsi = cv(field3(c, VFS_ICSI)); m.ieta = cv(field3(c, VFS_IETA)); m.izet = cv(field3(c, VFS_IZET));
+  m.iaj = c->f[VFS_IAJ][0];
+  m.jcsi = cv(field3(c, VFS_JCSI)); m.jeta = cv(field3(c, VFS_JETA)); m.jzet = cv(field3(c, VFS_JZET));
+  m.jaj = c->f[VFS_JAJ][0];
+  m.kcsi = cv(field3(c, VFS_KCSI)); m.keta = cv(field3(c, VFS_KETA)); m.kzet = cv(field3(c, VFS_KZET));
+  m.kaj = c->f[VFS_KAJ][0];
+  return m;
+}
+
+int ensure_red(Ctx *c, int n) {
+  if (n <= c->red_cap) return VFS_OK;
+  if (c->red) cudaFree(c->red);
+  if (c->red_host) cudaFreeHost(c->red_host);
+  c->red = nullptr; c->red_host = nullptr;
+  if (cudaMalloc(&c->red, sizeof(double) * n) != cudaSuccess ||
+      cudaMallocHost(&c->red_host, sizeof(double) * n) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "reduction buffer allocation failed");
+  c->red_cap = n;
+  return VFS_OK;
+}
+
+// Sum of nparts partial sums in a fixed order (single block, deterministic).
+__global__ void k_sum_parts(const double *parts, int n, double *out) {
+  __shared__ double sh[256];
+  double s = 0;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) s += parts[q];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+int reduce_sum(Ctx *c, const double *parts, int nparts, double *out) {
+  int rc = ensure_red(c, 64);
+  if (rc) return rc;
+  k_sum_parts<<<1, 256, 0, c->stream>>>(parts, nparts, c->red + 63);
+  if ((rc = check_launch(c, "k_sum_parts"))) return rc;
+  cudaMemcpyAsync(c->red_host + 63, c->red + 63, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "reduce_sum: stream sync failed");
+  *out = c->red_host[63];
+  return VFS_OK;
+}
+
+}  // namespace vfs
+
+// ---------------------------------------------------------------- pack kernels
+// AoS (reference Cmpnts layout) <-> SoA component arrays.
+__global__ void k_unpack(const double *__restrict__ aos, int dof, long long n, double *c0,
+                         double *c1, double *c2) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  if (dof == 1) { c0[p] = aos[p]; return; }
+  c0[p] = aos[3 * p]; c1[p] = aos[3 * p + 1]; c2[p] = aos[3 * p + 2];
+}
+__global__ void k_pack(double *__restrict__ aos, int dof, long long n, const double *c0,
+                       const double *c1, const double *c2) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  if (dof == 1) { aos[p] = c0[p]; return; }
+  aos[3 * p] = c0[p]; aos[3 * p + 1] = c1[p]; aos[3 * p + 2] = c2[p];
+}
+// nvert (double 0/1/3) -> uint8, flagging non-integral or out-of-range values.
+__global__ void k_nvert_to_u8(const double *__restrict__ nvd, long long n, uint8_t *nv, int *bad) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  double v = nvd[p];
+  double r = rint(v);
+  if (!(v >= 0.0 && v <= 255.0) || r != v) { atomicExch(bad, 1); nv[p] = 0; return; }
+  nv[p] = (uint8_t)r;
+}
+
+static const int kDof[VFS_NFIELDS] = {
+    3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3,  // UCONT..CENT
+    3, 3, 3, 1,                            // CSI ETA ZET AJ
+    3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1,    // I J K face metrics
+    1};                                     // CS
+
+extern "C" {
+
+const char *vfs_last_error(const vfs_ctx *ctx) {
+  const Ctx *c = (const Ctx *)ctx;
+  return c ? c->err.c_str() : g_last_err.c_str();
+}
+
+int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
+  if (!cfg || !out) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(nullptr, VFS_ERR_NO_DEVICE, "vfs_create: no CUDA device");
+  if (device < 0 || device >= ndev) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: bad device");
+  if (cfg->IM < 4 || cfg->JM < 4 || cfg->KM < 4)
+    return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: grid needs at least 4 nodes per direction");
+  // Boundary codes handled on this path: 0 (unset), 1 no-slip wall, 2 moving lid (j+),
+  // 4 outlet, 5 inlet, 7 periodic face, 10 free-slip, 12 moving wall, 13/14 slip lid.
+  for (int q = 0; q < 6; q++) {
+    int b = cfg->bctype[q];
+    bool ok = (b == 0 || b == 1 || b == 2 || b == 4 || b == 5 || b == 7 || b == 10 || b == 12 ||
+               b == 13 || b == 14 || b == -10);
+    if (!ok) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: unsupported bctype " + std::to_string(b));
+  }
+  if (cfg->immersed < 0 || cfg->immersed > 1)
+    return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: immersed must be 0 or 1");
+  if (cfg->les != 0 && cfg->les != 1 && cfg->les != 2)
+    return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: les must be 0, 1 or 2");
+  if (cudaSetDevice(device) != cudaSuccess) return set_err(nullptr, VFS_ERR_CUDA, "cudaSetDevice failed");
+  // The kernels are built for sm_100a only; refuse other GPUs up front.
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  if (prop.major != 10)
+    return set_err(nullptr, VFS_ERR_NO_DEVICE, "vfs_create: this library is built for sm_100a (B200)");
+
+  Ctx *c = new Ctx();
+  c->cfg = *cfg;
+  c->device = device;
+  Grid &g = c->g;
+  g.mx = cfg->IM + 1; g.my = cfg->JM + 1; g.mz = cfg->KM + 1;
+  g.N = (long long)g.mx * g.my * g.mz;
+  g.iper = cfg->i_periodic; g.jper = cfg->j_periodic; g.kper = cfg->k_periodic;
+  for (int q = 0; q < 6; q++) g.bc[q] = cfg->bctype[q];
+  g.immersed = cfg->immersed; g.les = cfg->les;
+  g.ren = cfg->ren; g.dt = cfg->dt; g.st = cfg->st;
+  c->scal[VFS_S_DT] = cfg->dt; c->scal[VFS_S_REN] = cfg->ren; c->scal[VFS_S_ST] = cfg->st;
+  c->scal[VFS_S_INLET_FLUX] = cfg->inlet_flux;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return set_err(nullptr, VFS_ERR_CUDA, "stream creation failed");
+  }
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+  const size_t bytes = sizeof(double) * (size_t)g.N;
+  bool okm = true;
+  for (int f = 0; f < VFS_NFIELDS; f++) {
+    c->dof[f] = kDof[f];
+    for (int q = 0; q < kDof[f]; q++) {
+      okm &= cudaMalloc(&c->f[f][q], bytes) == cudaSuccess;
+      if (okm) cudaMemsetAsync(c->f[f][q], 0, bytes, c->stream);
+    }
+  }
+  okm &= cudaMalloc(&c->nv, (size_t)g.N) == cudaSuccess;
+  if (okm) cudaMemsetAsync(c->nv, 0, (size_t)g.N, c->stream);
+  for (int d = 0; d < 3; d++)
+    for (int q = 0; q < 3; q++) {
+      okm &= cudaMalloc(&c->div[d][q], bytes) == cudaSuccess;
+      okm &= cudaMalloc(&c->visc[d][q], bytes) == cudaSuccess;
+      if (okm) { cudaMemsetAsync(c->div[d][q], 0, bytes, c->stream); cudaMemsetAsync(c->visc[d][q], 0, bytes, c->stream); }
+    }
+  for (int q = 0; q < 3; q++) {
+    okm &= cudaMalloc(&c->fp[q], bytes) == cudaSuccess;
+    okm &= cudaMalloc(&c->pucont[q], bytes) == cudaSuccess;
+    okm &= cudaMalloc(&c->bcbuf[q], bytes) == cudaSuccess;
+    if (okm) {
+      cudaMemsetAsync(c->fp[q], 0, bytes, c->stream);
+      cudaMemsetAsync(c->pucont[q], 0, bytes, c->stream);
+      cudaMemsetAsync(c->bcbuf[q], 0, bytes, c->stream);
+    }
+  }
+  okm &= cudaMalloc(&c->bcflag, (size_t)g.N) == cudaSuccess;
+  if (okm) cudaMemsetAsync(c->bcflag, 0, (size_t)g.N, c->stream);
+  okm &= ensure_red(c, 4096) == VFS_OK;
+  if (!okm) {
+    vfs_destroy((vfs_ctx *)c);
+    return set_err(nullptr, VFS_ERR_CUDA, "vfs_create: device allocation failed");
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    vfs_destroy((vfs_ctx *)c);
+    return set_err(nullptr, VFS_ERR_CUDA, "vfs_create: initialisation failed");
+  }
+  *out = (vfs_ctx *)c;
+  return VFS_OK;
+}
+
+int vfs_destroy(vfs_ctx *ctx) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c) return VFS_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int f = 0; f < VFS_NFIELDS; f++)
+    for (int q = 0; q < 3; q++) if (c->f[f][q]) cudaFree(c->f[f][q]);
+  if (c->nv) cudaFree(c->nv);
+  if (c->bcflag) cudaFree(c->bcflag);
+  for (int d = 0; d < 3; d++)
+    for (int q = 0; q < 3; q++) { cudaFree(c->div[d][q]); cudaFree(c->visc[d][q]); }
+  for (int q = 0; q < 3; q++) { cudaFree(c->fp[q]); cudaFree(c->pucont[q]); cudaFree(c->bcbuf[q]); }
+  if (c->red) cudaFree(c->red);
+  if (c->red_host) cudaFreeHost(c->red_host);
+  Poisson &P = c->ps;
+  cudaFree(P.coef); cudaFree(P.coef32); cudaFree(P.invdiag); cudaFree(P.invdiag32); cudaFree(P.fluid);
+  cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t);
+  cudaFree(P.f32); cudaFree(P.f64);
+  for (size_t l = 1; l < P.lv.size(); l++) {
+    MGLevel &L = P.lv[l];
+    cudaFree(L.op64); cudaFree(L.op32); cudaFree(L.x64); cudaFree(L.x32);
+  }
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return VFS_OK;
+}
+
+int vfs_dims(const vfs_ctx *ctx, int *mx, int *my, int *mz) {
+  const Ctx *c = (const Ctx *)ctx;
+  if (!c) return VFS_ERR_INVALID;
+  if (mx) *mx = c->g.mx;
+  if (my) *my = c->g.my;
+  if (mz) *mz = c->g.mz;
+  return VFS_OK;
+}
+
+long long vfs_launch_count(const vfs_ctx *ctx) { return ctx ? ((const Ctx *)ctx)->launches : 0; }
+
+int vfs_synchronize(vfs_ctx *ctx) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c) return VFS_ERR_INVALID;
+  cudaSetDevice(c->device);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, std::string("synchronize: ") + cudaGetErrorString(cudaGetLastError()));
+  return VFS_OK;
+}
+
+int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c || !host || field < 0 || field >= VFS_NFIELDS) return set_err(c, VFS_ERR_INVALID, "vfs_set_field: bad argument");
+  cudaSetDevice(c->device);
+  const int dof = c->dof[field];
+  const size_t bytes = sizeof(double) * (size_t)c->g.N * dof;
+  double *stage = nullptr;
+  if (cudaMallocAsync(&stage, bytes, c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "vfs_set_field: staging allocation failed");
+  cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, c->stream);
+  int rc = VFS_OK;
+  if (field == VFS_NVERT) {
+    int *bad = (int *)c->red;  // first word of the reduction buffer as a flag
+    cudaMemsetAsync(bad, 0, sizeof(int), c->stream);
+    k_nvert_to_u8<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, c->g.N, c->nv, bad);
+    rc = check_launch(c, "k_nvert_to_u8");
+    int hbad = 0;
+    cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    cudaMemcpyAsync(c->f[field][0], stage, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaFreeAsync(stage, c->stream);
+    cudaStreamSynchronize(c->stream);
+    if (!rc && hbad) rc = set_err(c, VFS_ERR_INVALID, "vfs_set_field: nvert must hold integers 0..255");
+    c->nvert_set = true;
+    c->ps.built = false;
+    return rc;
+  }
+  k_unpack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
+                                                       c->f[field][1], c->f[field][2]);
+  rc = check_launch(c, "k_unpack");
+  cudaFreeAsync(stage, c->stream);
+  if (field >= VFS_CSI && field <= VFS_KAJ) { c->metrics_set = true; c->ps.built = false; }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "vfs_set_field: copy failed");
+  return rc;
+}
+
+int vfs_get_field(vfs_ctx *ctx, int field, double *host) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c || !host || field < 0 || field >= VFS_NFIELDS) return set_err(c, VFS_ERR_INVALID, "vfs_get_field: bad argument");
+  cudaSetDevice(c->device);
+  const int dof = c->dof[field];
+  const size_t bytes = sizeof(double) * (size_t)c->g.N * dof;
+  double *stage = nullptr;
+  if (cudaMallocAsync(&stage, bytes, c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "vfs_get_field: staging allocation failed");
+  k_pack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
+                                                     c->f[field][1], c->f[field][2]);
+  int rc = check_launch(c, "k_pack");
+  cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(stage, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "vfs_get_field: copy failed");
+  return rc;
+}
+
+int vfs_field_device_ptr(vfs_ctx *ctx, int field, int component, void **dptr) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c || !dptr || field < 0 || field >= VFS_NFIELDS || component < 0 || component >= c->dof[field])
+    return set_err(c, VFS_ERR_INVALID, "vfs_field_device_ptr: bad argument");
+  *dptr = c->f[field][component];
+  return VFS_OK;
+}
+
+int vfs_set_scalar(vfs_ctx *ctx, int which, double value) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c || which < 0 || which >= VFS_NSCALARS) return set_err(c, VFS_ERR_INVALID, "vfs_set_scalar: bad argument");
+  c->scal[which] = value;
+  if (which == VFS_S_DT) c->g.dt = value;
+  if (which == VFS_S_REN) c->g.ren = value;
+  if (which == VFS_S_ST) c->g.st = value;
+  return VFS_OK;
+}
+
+int vfs_get_scalar(vfs_ctx *ctx, int which, double *value) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c || !value || which < 0 || which >= VFS_NSCALARS) return set_err(c, VFS_ERR_INVALID, "vfs_get_scalar: bad argument");
+  *value = c->scal[which];
+  return VFS_OK;
+}
+
+#define VFS_REQUIRE_SETUP(c)                                                                   \
+  do {                                                                                         \
+    if (!(c)) return set_err(nullptr, VFS_ERR_INVALID, "null context");                       \
+    if (!(c)->metrics_set) return set_err((c), VFS_ERR_STATE, "metrics have not been uploaded"); \
+    cudaSetDevice((c)->device);                                                                \
+  } while (0)
+
+int vfs_contra2cart(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return contra2cart(c); }
+int vfs_formfunction2(vfs_ctx *ctx, double scale) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return formfunction2(c, scale, false, 0.0); }
+int vfs_pressure_gradient(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return pressure_gradient(c); }
+int vfs_calc_k_flux(vfs_ctx *ctx, double *flux) {
+  Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  double f = 0;
+  int rc = calc_k_flux(c, &f);
+  if (flux) *flux = f;
+  return rc;
+}
+int vfs_runge_kutta(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return runge_kutta(c); }
+int vfs_poisson_lhs(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return poisson_lhs(c); }
+int vfs_poisson_rhs(vfs_ctx *ctx) {
+  Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  if (!c->ps.built) { int rc = poisson_lhs(c); if (rc) return rc; }
+  return poisson_rhs(c);
+}
+int vfs_poisson_solve(vfs_ctx *ctx, const vfs_solve_opts *o, vfs_solve_stats *st) {
+  Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  if (!c->ps.built) { int rc = poisson_lhs(c); if (rc) return rc; }
+  return poisson_solve(c, o, st);
+}
+int vfs_poisson_apply(vfs_ctx *ctx, const double *xh, double *yh) {
+  Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  if (!xh || !yh) return set_err(c, VFS_ERR_INVALID, "vfs_poisson_apply: null array");
+  if (!c->ps.built) { int rc = poisson_lhs(c); if (rc) return rc; }
+  const size_t bytes = sizeof(double) * (size_t)c->g.N;
+  double *dx = nullptr, *dy = nullptr;
+  if (cudaMallocAsync(&dx, bytes, c->stream) != cudaSuccess || cudaMallocAsync(&dy, bytes, c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "vfs_poisson_apply: allocation failed");
+  cudaMemcpyAsync(dx, xh, bytes, cudaMemcpyHostToDevice, c->stream);
+  int rc = poisson_apply_dev(c, dx, dy);
+  cudaMemcpyAsync(yh, dy, bytes, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(dx, c->stream);
+  cudaFreeAsync(dy, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "vfs_poisson_apply: failed");
+  return rc;
+}
+int vfs_update_pressure(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return update_pressure(c); }
+int vfs_projection(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return projection(c); }
+int vfs_divergence(vfs_ctx *ctx, double *maxdiv) {
+  Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  double m = 0;
+  int rc = divergence(c, &m);
+  if (maxdiv) *maxdiv = m;
+  return rc;
+}
+
+int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
+  Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  int rc;
+  vfs_step_stats s;
+  memset(&s, 0, sizeof(s));
+  cudaEventRecord(c->ev0, c->stream);
+  if (!c->ps.built && (rc = poisson_lhs(c))) return rc;
+  // Flow_Solver order for implicit=0 (solvers.c:644-1385)
+  if ((rc = calc_k_flux(c, &s.mean_k_flux))) return rc;
+  if ((rc = pressure_gradient(c))) return rc;
+  if ((rc = runge_kutta(c))) return rc;
+  if ((rc = poisson_rhs(c))) return rc;
+  rc = poisson_solve(c, opts, &s.poisson);
+  if (rc && rc != VFS_ERR_NOT_CONVERGED) return rc;
+  int solve_rc = rc;
+  if ((rc = update_pressure(c))) return rc;
+  if ((rc = projection(c))) return rc;
+  if ((rc = divergence(c, &s.max_div))) return rc;
+  cudaEventRecord(c->ev1, c->stream);
+  cudaEventSynchronize(c->ev1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  s.ms = ms;
+  if (st) *st = s;
+  return solve_rc;
+}
+
+}  // extern "C"

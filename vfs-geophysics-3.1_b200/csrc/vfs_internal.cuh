@@ -1,0 +1,167 @@
+// Internal definitions shared by the sm_100a kernels and the C-ABI layer.
+//
+// Device data layout (one structured block, one GPU):
+//   * Every field covers the reference's whole DA extent, mx*my*mz points with
+//     mx = IM+1 (init.c:154), in the reference's linear order ((k*my)+j)*mx+i, so a
+//     host array in the reference layout maps 1:1 onto a device index.
+//   * Vector fields are stored as three separate component arrays (SoA) so that a warp
+//     reading consecutive i of one component issues fully coalesced 8-byte loads.
+//   * The IB flag field nvert (0/1/3 in the reference, stored as doubles) is stored as
+//     uint8: every threshold test of the reference (>0.1, <0.1, (int)(x+0.5)==1, >1.1,
+//     (int)(x+0.1)==3 ...) is exact on small integers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/vfs_b200.h"
+
+namespace vfs {
+
+// Scalar run parameters passed by value to every kernel.
+struct Grid {
+  int mx, my, mz;
+  long long N;          // mx*my*mz
+  int iper, jper, kper; // i_periodic, j_periodic, k_periodic
+  int bc[6];            // bctype
+  int immersed, les;
+  double ren, dt, st;
+};
+
+__host__ __device__ inline long long lidx(const Grid &g, int i, int j, int k) {
+  return ((long long)k * g.my + j) * g.mx + i;
+}
+
+// Periodic image of a ghost index (0 -> m-2, m-1 -> 1) in a periodic direction, as the
+// reference's periodic copy loops do (e.g. momentum.c:641-669); identity otherwise.
+__host__ __device__ inline int wrapi(const Grid &g, int i) {
+  if (g.iper) { if (i == 0) return g.mx - 2; if (i == g.mx - 1) return 1; }
+  return i;
+}
+__host__ __device__ inline int wrapj(const Grid &g, int j) {
+  if (g.jper) { if (j == 0) return g.my - 2; if (j == g.my - 1) return 1; }
+  return j;
+}
+__host__ __device__ inline int wrapk(const Grid &g, int k) {
+  if (g.kper) { if (k == 0) return g.mz - 2; if (k == g.mz - 1) return 1; }
+  return k;
+}
+
+// Three-component SoA vector field.
+struct V3 {
+  double *x, *y, *z;
+};
+struct CV3 {
+  const double *x, *y, *z;
+};
+inline CV3 cv(const V3 &v) { return CV3{v.x, v.y, v.z}; }
+
+// Metric arrays (FormMetrics, metrics.c:4).
+struct Metrics {
+  CV3 csi, eta, zet;    // centre
+  const double *aj;
+  CV3 icsi, ieta, izet; // i-faces
+  const double *iaj;
+  CV3 jcsi, jeta, jzet; // j-faces
+  const double *jaj;
+  CV3 kcsi, keta, kzet; // k-faces
+  const double *kaj;
+};
+
+// Poisson operator: 19 coefficients per cell in the slot order of PoissonLHSNew
+// (poisson.c:951-969: CP EP WP NP SP TP BP NE SE NW SW TN BN TS BS TE BE TW BW).
+enum { CP = 0, EP, WP, NP, SP, TP, BP, NE, SE, NW, SW, TN, BN, TS, BS, TE, BE, TW, BW, NSLOT };
+
+struct MGLevel {
+  int nx, ny, nz;          // interior cells (coarse levels use a ghost-free layout)
+  long long n;
+  double *op64 = nullptr;  // 4*n: conductance to +i, +j, +k neighbour, diagonal (FP64)
+  float *op32 = nullptr;   // FP32 copy of op64
+  double *x64 = nullptr, *b64 = nullptr, *d64 = nullptr, *t64 = nullptr;
+  float *x32 = nullptr, *b32 = nullptr, *d32 = nullptr, *t32 = nullptr;
+};
+
+struct Poisson {
+  bool built = false;
+  double *coef = nullptr;   // NSLOT * N doubles (SoA by slot)
+  float *coef32 = nullptr;  // NSLOT * N floats
+  double *invdiag = nullptr;
+  float *invdiag32 = nullptr;
+  uint8_t *fluid = nullptr; // 1 if the cell is a Poisson unknown (gid >= 0)
+  long long nfluid = 0;
+  double sum_aj = 0;        // sum of aj over fluid cells (Remove_Nullspace_Scale)
+  std::vector<MGLevel> lv;  // lv[0] describes the fine level (coefficients above)
+  // FGMRES workspace (grid layout, N doubles each)
+  int restart = 0;
+  double *V = nullptr;      // (restart+1) * N
+  double *Z = nullptr;      // restart * N
+  double *w = nullptr, *r = nullptr, *t = nullptr;
+  float *f32 = nullptr;     // 4*N FP32 fine-level work (b, x, x', d)
+  double *f64 = nullptr;    // 4*N FP64 fine-level work
+  double lmax0 = 0;         // fine-level bound of the spectrum of D^-1 A
+};
+
+struct Ctx {
+  vfs_config cfg;
+  Grid g;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long launches = 0;
+
+  // fields (SoA component pointers; scalar fields use comp[0])
+  double *f[VFS_NFIELDS][3] = {};
+  int dof[VFS_NFIELDS] = {};
+  uint8_t *nv = nullptr;        // nvert as uint8
+  // scratch for Formfunction_2 (face fluxes and Fp) and Contra2Cart
+  double *div[3][3] = {};       // div1..3 x comps
+  double *visc[3][3] = {};
+  double *fp[3] = {};
+  double *pucont[3] = {};
+  double *bcbuf[3] = {};        // Contra2Cart boundary two-phase buffer
+  uint8_t *bcflag = nullptr;    // points written by the boundary phase
+  // reductions
+  double *red = nullptr;        // partial sums (device)
+  double *red_host = nullptr;   // pinned host mirror
+  int red_cap = 0;
+  double scal[VFS_NSCALARS] = {};
+  bool metrics_set = false, nvert_set = false;
+  Poisson ps;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+V3 field3(Ctx *c, int f);
+Metrics metrics(Ctx *c);
+
+// launch bookkeeping / error checking
+int check_launch(Ctx *c, const char *what);
+int set_err(Ctx *c, int code, const std::string &msg);
+
+inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// momentum path
+int periodic_copy3(Ctx *c, V3 v);
+int periodic_copy1(Ctx *c, double *s);
+int contra2cart(Ctx *c);
+int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff);
+int pressure_gradient(Ctx *c);
+int calc_k_flux(Ctx *c, double *flux);
+int runge_kutta(Ctx *c);
+int form_bcs(Ctx *c);
+
+// Poisson / correction path
+int poisson_lhs(Ctx *c);
+int poisson_rhs(Ctx *c);
+int poisson_solve(Ctx *c, const vfs_solve_opts *o, vfs_solve_stats *st);
+int poisson_apply_dev(Ctx *c, const double *x, double *y);
+int update_pressure(Ctx *c);
+int projection(Ctx *c);
+int divergence(Ctx *c, double *maxdiv);
+
+// reductions (deterministic two-pass); result copied to host
+int reduce_sum(Ctx *c, const double *parts, int nparts, double *out);
+int ensure_red(Ctx *c, int n);
+
+}  // namespace vfs

@@ -1,0 +1,279 @@
+"""Host-side binding of the B200 projection-path library (libvfs_b200.so).
+
+The library is the product: hand-written sm_100a kernels behind the C ABI declared in
+include/vfs_b200.h.  This module only loads it with ctypes and wraps the entry points in
+a small class whose method names follow the reference functions they replace
+(Formfunction_2, Contra2Cart, PoissonLHSNew, ...).  There is no CPU fallback: if the
+shared library is missing or no B200 is present, construction raises.
+
+Host arrays use the reference's layout: the DA of (IM+1) x (JM+1) x (KM+1) points,
+[k][j][i] with i fastest, vector fields as interleaved {x,y,z} (numpy shape
+(mz, my, mx, 3)).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "libvfs_b200.so")
+
+# field identifiers (include/vfs_b200.h)
+UCONT, UCAT, P, PHI, NVERT, NU_T, RHS, DP, UCONT_O, UCAT_O, B, CENT = range(12)
+CSI, ETA, ZET, AJ = 12, 13, 14, 15
+ICSI, IETA, IZET, IAJ = 16, 17, 18, 19
+JCSI, JETA, JZET, JAJ = 20, 21, 22, 23
+KCSI, KETA, KZET, KAJ = 24, 25, 26, 27
+CS = 28
+NFIELDS = 29
+FIELD_DOF = [3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 1]
+METRIC_FIELDS = {
+    "csi": CSI, "eta": ETA, "zet": ZET, "aj": AJ,
+    "icsi": ICSI, "ieta": IETA, "izet": IZET, "iaj": IAJ,
+    "jcsi": JCSI, "jeta": JETA, "jzet": JZET, "jaj": JAJ,
+    "kcsi": KCSI, "keta": KETA, "kzet": KZET, "kaj": KAJ,
+    "cent": CENT,
+}
+
+# scalars
+S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST = range(7)
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOT_CONVERGED, ERR_NO_DEVICE, ERR_STATE = range(6)
+
+
+class VfsConfig(ctypes.Structure):
+    _fields_ = [
+        ("IM", ctypes.c_int), ("JM", ctypes.c_int), ("KM", ctypes.c_int),
+        ("bctype", ctypes.c_int * 6),
+        ("i_periodic", ctypes.c_int), ("j_periodic", ctypes.c_int), ("k_periodic", ctypes.c_int),
+        ("immersed", ctypes.c_int), ("les", ctypes.c_int), ("inletprofile", ctypes.c_int),
+        ("reserved_i", ctypes.c_int * 8),
+        ("ren", ctypes.c_double), ("dt", ctypes.c_double), ("st", ctypes.c_double),
+        ("inlet_flux", ctypes.c_double), ("mean_pressure_gradient", ctypes.c_double),
+        ("dpdz_set", ctypes.c_int), ("reserved_j", ctypes.c_int * 7),
+        ("reserved_d", ctypes.c_double * 8),
+    ]
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [
+        ("precision", ctypes.c_int), ("restart", ctypes.c_int), ("max_iter", ctypes.c_int),
+        ("levels", ctypes.c_int), ("pre_smooth", ctypes.c_int), ("post_smooth", ctypes.c_int),
+        ("coarse_iters", ctypes.c_int), ("reserved", ctypes.c_int * 5),
+        ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("reserved_d", ctypes.c_double * 4),
+    ]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+        ("r0", ctypes.c_double), ("rfinal", ctypes.c_double), ("ms", ctypes.c_double),
+        ("reserved", ctypes.c_double * 4),
+    ]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [
+        ("max_div", ctypes.c_double), ("mean_k_flux", ctypes.c_double),
+        ("poisson", SolveStats), ("ms", ctypes.c_double), ("reserved", ctypes.c_double * 4),
+    ]
+
+
+EXPORTS = [
+    "vfs_create", "vfs_destroy", "vfs_last_error", "vfs_dims", "vfs_synchronize",
+    "vfs_launch_count", "vfs_set_field", "vfs_get_field", "vfs_set_scalar", "vfs_get_scalar",
+    "vfs_field_device_ptr", "vfs_contra2cart", "vfs_formfunction2", "vfs_pressure_gradient",
+    "vfs_calc_k_flux", "vfs_runge_kutta", "vfs_poisson_lhs", "vfs_poisson_rhs",
+    "vfs_poisson_solve", "vfs_poisson_apply", "vfs_update_pressure", "vfs_projection",
+    "vfs_divergence", "vfs_step",
+]
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load libvfs_b200.so (built in-tree by build.py).  Raises if it is absent."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError("libvfs_b200.so not built (%s); run __graft_entry__.build()" % p)
+    lib = ctypes.CDLL(p)
+    vp = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.vfs_create.argtypes = [ctypes.POINTER(VfsConfig), ctypes.c_int, ctypes.POINTER(vp)]
+    lib.vfs_destroy.argtypes = [vp]
+    lib.vfs_last_error.argtypes = [vp]
+    lib.vfs_last_error.restype = ctypes.c_char_p
+    lib.vfs_dims.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                             ctypes.POINTER(ctypes.c_int)]
+    lib.vfs_synchronize.argtypes = [vp]
+    lib.vfs_launch_count.argtypes = [vp]
+    lib.vfs_launch_count.restype = ctypes.c_longlong
+    lib.vfs_set_field.argtypes = [vp, ctypes.c_int, vp]
+    lib.vfs_get_field.argtypes = [vp, ctypes.c_int, vp]
+    lib.vfs_set_scalar.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    lib.vfs_get_scalar.argtypes = [vp, ctypes.c_int, dp]
+    lib.vfs_field_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    for n in ("vfs_contra2cart", "vfs_pressure_gradient", "vfs_runge_kutta", "vfs_poisson_lhs",
+              "vfs_poisson_rhs", "vfs_update_pressure", "vfs_projection"):
+        getattr(lib, n).argtypes = [vp]
+    lib.vfs_formfunction2.argtypes = [vp, ctypes.c_double]
+    lib.vfs_calc_k_flux.argtypes = [vp, dp]
+    lib.vfs_divergence.argtypes = [vp, dp]
+    lib.vfs_poisson_solve.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats)]
+    lib.vfs_poisson_apply.argtypes = [vp, vp, vp]
+    lib.vfs_step.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(StepStats)]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class VfsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("vfs error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Context:
+    """One structured block on one GPU (vfs_ctx)."""
+
+    def __init__(self, cfg: VfsConfig, device=0):
+        self.lib = load_library()
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        rc = self.lib.vfs_create(ctypes.byref(cfg), device, ctypes.byref(h))
+        if rc:
+            raise VfsError(rc, self.lib.vfs_last_error(None).decode())
+        self.h = h
+        mx, my, mz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self.lib.vfs_dims(h, ctypes.byref(mx), ctypes.byref(my), ctypes.byref(mz))
+        self.shape = (mz.value, my.value, mx.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.vfs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, allow=()):
+        if rc and rc not in allow:
+            raise VfsError(rc, self.lib.vfs_last_error(self.h).decode())
+        return rc
+
+    # ---- fields
+    def set_field(self, field, arr):
+        dof = FIELD_DOF[field]
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        want = int(np.prod(self.shape)) * dof
+        if a.size != want:
+            raise ValueError("field %d: expected %d values, got %d" % (field, want, a.size))
+        self._check(self.lib.vfs_set_field(self.h, field, a.ctypes.data))
+
+    def get_field(self, field):
+        dof = FIELD_DOF[field]
+        shape = self.shape + ((3,) if dof == 3 else ())
+        out = np.empty(shape, dtype=np.float64)
+        self._check(self.lib.vfs_get_field(self.h, field, out.ctypes.data))
+        return out
+
+    def set_metrics(self, m):
+        """m: dict name -> array (names of METRIC_FIELDS)."""
+        for name, fid in METRIC_FIELDS.items():
+            if name in m:
+                self.set_field(fid, m[name])
+
+    def set_scalar(self, which, v):
+        self._check(self.lib.vfs_set_scalar(self.h, which, float(v)))
+
+    def get_scalar(self, which):
+        v = ctypes.c_double()
+        self._check(self.lib.vfs_get_scalar(self.h, which, ctypes.byref(v)))
+        return v.value
+
+    def launch_count(self):
+        return self.lib.vfs_launch_count(self.h)
+
+    def synchronize(self):
+        self._check(self.lib.vfs_synchronize(self.h))
+
+    # ---- operators (reference names in comments)
+    def contra2cart(self):            # Contra2Cart, rhs.c:27
+        self._check(self.lib.vfs_contra2cart(self.h))
+
+    def formfunction2(self, scale=1.0):  # Formfunction_2, momentum.c:456
+        self._check(self.lib.vfs_formfunction2(self.h, scale))
+
+    def pressure_gradient(self):      # Pressure_Gradient, momentum.c:197
+        self._check(self.lib.vfs_pressure_gradient(self.h))
+
+    def calc_k_flux(self):            # Calc_k_Flux, rhs2.c:1562
+        v = ctypes.c_double()
+        self._check(self.lib.vfs_calc_k_flux(self.h, ctypes.byref(v)))
+        return v.value
+
+    def runge_kutta(self):            # RungeKutta, rhs.c:1578
+        self._check(self.lib.vfs_runge_kutta(self.h))
+
+    def poisson_lhs(self):            # PoissonLHSNew, poisson.c:971
+        self._check(self.lib.vfs_poisson_lhs(self.h))
+
+    def poisson_rhs(self):            # PoissonRHS2 (+ Remove_Nullspace_Scale)
+        self._check(self.lib.vfs_poisson_rhs(self.h))
+
+    def poisson_apply(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.shape)
+        y = np.empty_like(x)
+        self._check(self.lib.vfs_poisson_apply(self.h, x.ctypes.data, y.ctypes.data))
+        return y
+
+    def poisson_solve(self, precision=0, rtol=1e-10, restart=30, max_iter=200, levels=4,
+                      pre_smooth=2, post_smooth=2, coarse_iters=16, allow_unconverged=False):
+        o = SolveOpts(precision=precision, restart=restart, max_iter=max_iter, levels=levels,
+                      pre_smooth=pre_smooth, post_smooth=post_smooth, coarse_iters=coarse_iters,
+                      rtol=rtol)
+        st = SolveStats()
+        allow = (ERR_NOT_CONVERGED,) if allow_unconverged else ()
+        self._check(self.lib.vfs_poisson_solve(self.h, ctypes.byref(o), ctypes.byref(st)), allow)
+        return st
+
+    def update_pressure(self):        # UpdatePressure, poisson.c:3144
+        self._check(self.lib.vfs_update_pressure(self.h))
+
+    def projection(self):             # Projection, poisson.c:2707
+        self._check(self.lib.vfs_projection(self.h))
+
+    def divergence(self):             # Divergence, main.c:1047
+        v = ctypes.c_double()
+        self._check(self.lib.vfs_divergence(self.h, ctypes.byref(v)))
+        return v.value
+
+    def step(self, precision=0, rtol=1e-10, **kw):  # Flow_Solver, solvers.c:562 (implicit=0)
+        o = SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
+                      max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 4),
+                      pre_smooth=kw.get("pre_smooth", 2), post_smooth=kw.get("post_smooth", 2),
+                      coarse_iters=kw.get("coarse_iters", 16))
+        st = StepStats()
+        self._check(self.lib.vfs_step(self.h, ctypes.byref(o), ctypes.byref(st)))
+        return st
+
+
+def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
+                inletprofile=13, ren=3000.0, dt=0.04, st=1.0, inlet_flux=-1.0,
+                mean_pressure_gradient=0.0, dpdz_set=0):
+    c = VfsConfig()
+    c.IM, c.JM, c.KM = IM, JM, KM
+    for q in range(6):
+        c.bctype[q] = bctype[q]
+    c.i_periodic, c.j_periodic, c.k_periodic = i_periodic, j_periodic, k_periodic
+    c.immersed, c.les, c.inletprofile = immersed, les, inletprofile
+    c.ren, c.dt, c.st = ren, dt, st
+    c.inlet_flux, c.mean_pressure_gradient, c.dpdz_set = inlet_flux, mean_pressure_gradient, dpdz_set
+    return c
