@@ -1,0 +1,438 @@
+"""Benchmark of the B200 projection step (one JSON line on stdout, rank 0).
+
+Workload: the 256 x 192 x 256-cell open channel with a staggered 3 x 2 array of vertical
+cylinders (D = 0.2, spacing 4D) encoded in nvert as blocked cells (immersed = 0), no-slip
+bottom, free-slip top, periodic spanwise and streamwise with the bulk flux held by the
+k-periodic forcing; seeded turbulent-like initial field (log-law mean plus random Fourier
+modes with a k^-5/3 spectrum, 5 % intensity).  One step = Flow_Solver for implicit = 0:
+Calc_k_Flux, Pressure_Gradient, 4-stage RungeKutta, VolumeFlux, Poisson RHS, Poisson
+solve to rtol 1e-10, UpdatePressure, Projection, Divergence, IB_BC, Contra2Cart.
+
+`value` is the mixed-precision (FP32 V-cycle in FP64 FGMRES) step time in ms with every
+field resident in HBM; the all-FP64 form is timed on the same state for the comparison.
+`e2e` runs the same step through the C ABI with the flow state (Ucont, Ucat, P) copied
+from pinned host memory before and back after every step.
+
+Multi-GPU: the reference's north star keeps this path on one GPU, so N GPUs run N
+independent replicas (weak scaling); the step time is the maximum over ranks.
+
+`--impl reference` times the reference's own CPU code (oracle/_ref: its momentum.c,
+rhs.c, poisson.c ... under the single-rank shim; the Poisson solve, HYPRE in the
+reference, is scipy GMRES with an incomplete-LU preconditioner on the reference's own
+matrix) on a bounded sample of the workload and scales it to the full grid.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "vfs-geophysics-3.1_b200"))
+
+METRIC = "ms/step @256x192x256: mixed vs FP64 GPU at max|div u|<=1e-8; adjoint/forward ratio"
+NX, NY, NZ = 256, 192, 256
+WORKLOAD = ("open channel 256x192x256 cells, 3x2 staggered cylinders D=0.2 spacing 4D as nvert "
+            "blocked cells (immersed=0), no-slip bottom, free-slip top, periodic i and k with "
+            "k-periodic flux forcing; Poisson rtol 1e-10")
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------------ workload
+def make_case(nx=NX, ny=NY, nz=NZ):
+    from vfs_b200 import cases
+    c = cases.open_channel_cylinders(nx, ny, nz)
+    c.immersed = 0
+    return c
+
+
+def turbulent_like(case, seed=0, intensity=0.05, ub=1.0):
+    """Log-law mean streamwise velocity plus divergence-agnostic random Fourier modes with
+    an E(k) ~ k^-5/3 spectrum in the periodic (x, z) plane, rms `intensity`*ub."""
+    KM, JM, IM = case.X.shape
+    nz, ny, nx = KM - 1, JM - 1, IM - 1
+    Y = case.Y
+    yc = 0.125 * sum(Y[a:KM - 1 + a, b:JM - 1 + b, c:IM - 1 + c] for a in (0, 1) for b in (0, 1) for c in (0, 1))
+    H = getattr(case, "Ly", 1.0)
+    yp = np.clip(yc / H, 1e-3, 1.0)
+    mean = 1.0 + np.log(yp / 0.2) / 0.41 * 0.0566   # log law, u_tau = 0.0566 ub
+    mean /= mean.mean()
+    rng = np.random.Generator(np.random.Philox(seed))
+    kx = np.fft.fftfreq(nx)[None, None, :]
+    kz = np.fft.fftfreq(nz)[:, None, None]
+    kk = np.sqrt(kx ** 2 + kz ** 2)
+    amp = np.zeros_like(kk)
+    amp[kk > 0] = kk[kk > 0] ** (-5.0 / 6.0 - 0.5)   # |u_k| ~ sqrt(E(k)/k) in 2-D
+    u = np.zeros(case.da_shape + (3,))
+    for comp in range(3):
+        ph = rng.standard_normal((nz, ny, nx)) + 1j * rng.standard_normal((nz, ny, nx))
+        f = np.real(np.fft.ifft2(np.fft.fft2(ph, axes=(0, 2)) * amp, axes=(0, 2)))
+        f *= intensity * ub / max(f.std(), 1e-30)
+        u[1:-1, 1:-1, 1:-1, comp] = f
+    u[1:-1, 1:-1, 1:-1, 2] += mean * ub
+    u[case.nvert > 0.1] = 0.0
+    return u
+
+
+def setup_context(case):
+    import vfs_b200 as vfs
+    from vfs_b200 import cases
+    ctx = vfs.Context(case.config())
+    ctx.form_metrics(case.X, case.Y, case.Z)
+    ctx.set_field(vfs.NVERT, case.nvert)
+    m = {"icsi": ctx.get_field(vfs.ICSI), "jeta": ctx.get_field(vfs.JETA), "kzet": ctx.get_field(vfs.KZET)}
+    u = turbulent_like(case)
+    uc = cases.ucont_from_ucat(case, u, m)
+    ctx.set_field(vfs.UCONT, uc)
+    ctx.set_field(vfs.UCAT, u)
+    ctx.set_field(vfs.UCAT_O, u)
+    _, inlet_area = ctx.calc_inlet_area()
+    ctx.set_scalar(vfs.S_INLET_FLUX, 1.0 * inlet_area)   # bulk velocity 1
+    ctx.contra2cart()
+    del m, uc
+    return ctx, u
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = []
+        for q, n in enumerate(names):
+            if any(len(r) > 5 + q and r[5 + q].lower().startswith("active") for r in self.rows):
+                reasons.append(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ timing helpers
+def timed(ctx, fn, reps, torch):
+    """Device time of `reps` calls of fn, with events recorded on the context's stream."""
+    s = torch.cuda.ExternalStream(ctx.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    e0.record(s)
+    out = [fn() for _ in range(reps)]
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+# Algorithmic bytes per interior cell of the profiled kernels (compulsory traffic: each
+# input read once, each output written once, at the stored precision, nvert as 1 byte).
+KERNEL_BYTES = {
+    # Formfunction_2 as three kernels (face fluxes, Fp, RHS) of the fused-op figure: Ucont
+    # 24 + Ucat 24 + nvert 1 + nu_t 8 + face metrics 240 + centre metrics 72 + rhs 24
+    "formfunction2": 393.0,
+    # FP64 matrix-free Poisson apply: g_ab 72 + phi 8 + mask 1 + y 8
+    "poisson_apply_fp64": 89.0,
+    # FP32 smoother sweep: g_ab 36 + x 4 + b 4 + mask 1 + out 4
+    "smoother_fp32": 49.0,
+}
+
+
+def roofline_probe(ctx, torch, reps=20):
+    """Time the profiled operators on the context's stream; returns per-launch ms."""
+    res = {}
+    for name, ids in (("formfunction2", (0, 1, 2)), ("poisson_apply_fp64", (3,)), ("smoother_fp32", (4,)),
+                      ("smoother_fp64", (5,))):
+        for w in range(3):
+            for i in ids:
+                ctx.run_kernel(i, 1)
+        def body():
+            for i in ids:
+                ctx.run_kernel(i, 1)
+        ms, _ = timed(ctx, body, reps, torch)
+        res[name] = ms / reps
+    return res
+
+
+# ------------------------------------------------------------------ reference arm
+def reference_sample(nx=32, ny=24, nz=32, seed=0):
+    """One reference step (oracle/_ref) on a 32x24x32 sample of the workload, one host
+    thread; returns (ms for the sample, cells in the sample)."""
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(limits=1):
+        return _reference_sample(nx, ny, nz, seed)
+
+
+def _reference_sample(nx, ny, nz, seed):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    from oracle import ref
+    from vfs_b200 import cases
+    case = make_case(nx, ny, nz)
+    case.dt = 5e-4
+    R = ref.Reference(case)
+    m = R.metrics()
+    u = turbulent_like(case, seed=seed)
+    uc = cases.ucont_from_ucat(case, u, m)
+    for n in ("Ucont", "lUcont", "Ucont_o", "lUcont_o"):
+        R.set(n, uc)
+    for n in ("Ucat", "lUcat", "lUcat_old"):
+        R.set(n, u)
+    ref.set_global("inlet_flux", R.inlet_area())
+    R.call("ref_poisson_lhs")   # first-step set-up, outside the timed sample
+    t0 = time.perf_counter()
+    R.call("ref_ib_bc")
+    R.set("Ucont", R.get("lUcont"))
+    R.call("ref_calc_k_flux")
+    R.call("ref_pressure_gradient")
+    R.call("ref_runge_kutta")
+    R.volume_flux()
+    b = R.poisson_rhs_hypre()
+    rp, col, val = R.poisson_csr()
+    n = len(rp) - 1
+    A = sp.csr_matrix((val, col, rp), shape=(n, n))
+    ilu = spla.spilu(A.tocsc(), drop_tol=1e-4, fill_factor=10)
+    M = spla.LinearOperator((n, n), ilu.solve)
+    x, info = spla.gmres(A, b, M=M, rtol=1e-10, restart=50, maxiter=200)
+    x = R.remove_nullspace(x)
+    R.set("Phi2", x)
+    R.call("ref_convert_phi2_phi")
+    R.call("ref_update_pressure")
+    R.call("ref_projection")
+    R.call("ref_ib_bc")
+    R.set("Ucont", R.get("lUcont"))
+    R.call("ref_contra2cart")
+    ms = (time.perf_counter() - t0) * 1e3
+    R.close()
+    return ms, nx * ny * nz
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvfsref.so was not built"}))
+        return
+    scale = (NX * NY * NZ)
+    samples = []
+    for s in range(args.warmup + args.steps):
+        ms, cells = reference_sample(seed=s)
+        if s >= args.warmup:
+            samples.append(ms * scale / cells)
+    v = float(np.mean(samples))
+    out = {"metric": METRIC, "value": round(v, 3), "unit": "ms/step", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+           "config": {"workload": WORKLOAD, "precision": "reference FP64 CPU"},
+           "cpu_baseline": {"value": round(v, 3), "unit": "ms/step", "cores": 1, "kind": "reference",
+                            "sample": "one reference step on a 32x24x32-cell sample of the same workload, "
+                                      "scaled by the cell ratio (x512); Poisson solve by scipy GMRES+ILU "
+                                      "(HYPRE is not in the image); one host thread"},
+           "e2e": {"value": round(v, 3), "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", default=None, help="nx,ny,nz override (not for reported numbers)")
+    args = ap.parse_args()
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+    import vfs_b200 as vfs
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    nx, ny, nz = (NX, NY, NZ) if not args.size else tuple(int(v) for v in args.size.split(","))
+    case = make_case(nx, ny, nz)
+    ctx, u0 = setup_context(case)
+    ncell = nx * ny * nz
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also the first-step set-up: inlet area, Poisson operator, IB_BC)
+    for _ in range(max(3, args.warmup)):
+        ctx.step(precision=0, rtol=1e-10)
+
+    sampler = ClockSampler(local)
+    with sampler:
+        barrier()
+        ms_mixed, stats = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10), args.steps, torch)
+        barrier()
+        for _ in range(2):
+            ctx.step(precision=1, rtol=1e-10)
+        ms_fp64, stats64 = timed(ctx, lambda: ctx.step(precision=1, rtol=1e-10), args.steps, torch)
+        barrier()
+    ms_mixed /= args.steps
+    ms_fp64 /= args.steps
+    maxdiv = max(s.max_div for s in stats)
+    maxdiv64 = max(s.max_div for s in stats64)
+    its = float(np.mean([s.poisson.iterations for s in stats]))
+    its64 = float(np.mean([s.poisson.iterations for s in stats64]))
+
+    # e2e: flow state from pinned host memory each step, result back to the host
+    shp3 = ctx.shape + (3,)
+    h_uc = torch.empty(shp3, dtype=torch.float64, pin_memory=True).numpy()
+    h_u = torch.empty(shp3, dtype=torch.float64, pin_memory=True).numpy()
+    h_p = torch.empty(ctx.shape, dtype=torch.float64, pin_memory=True).numpy()
+    h_uc[...] = ctx.get_field(vfs.UCONT)
+    h_u[...] = ctx.get_field(vfs.UCAT)
+    h_p[...] = ctx.get_field(vfs.P)
+
+    def e2e_step():
+        ctx.set_field(vfs.UCONT, h_uc)
+        ctx.set_field(vfs.UCAT, h_u)
+        ctx.set_field(vfs.P, h_p)
+        st = ctx.step(precision=0, rtol=1e-10)
+        h_uc[...] = ctx.get_field(vfs.UCONT)
+        h_u[...] = ctx.get_field(vfs.UCAT)
+        h_p[...] = ctx.get_field(vfs.P)
+        return st
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_ms, _ = timed(ctx, e2e_step, max(2, args.steps // 2), torch)
+    barrier()
+    e2e_ms /= max(2, args.steps // 2)
+    npts = int(np.prod(ctx.shape))
+    io_bytes = npts * 8 * 7
+
+    # roofline of the dominant operator
+    launch = roofline_probe(ctx, torch)
+    peak, peak_kind = hbm_peak()
+    dom = "formfunction2"
+    achieved = KERNEL_BYTES[dom] * ncell / (launch[dom] * 1e-3) / 1e9
+    launches_per_step = None
+
+    if dist is not None:
+        t = torch.tensor([ms_mixed, ms_fp64, e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_mixed, ms_fp64, e2e_ms = [float(v) for v in t.tolist()]
+
+    n0 = ctx.launch_count()
+    ctx.step(precision=0, rtol=1e-10)
+    launches_per_step = ctx.launch_count() - n0
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline and not args.size:
+            try:
+                from oracle import ref
+                if ref.available():
+                    runs = [reference_sample(seed=s) for s in range(5)]
+                    ms_ref = float(np.median([r[0] for r in runs]))
+                    cells = runs[0][1]
+                    cpu = {"value": round(ms_ref * ncell / cells, 1), "unit": "ms/step", "cores": 1,
+                           "kind": "reference",
+                           "sample": "median of 5 reference steps (oracle/_ref) on a 32x24x32-cell sample "
+                                     "of this workload, scaled by the cell ratio (x512); Poisson by scipy "
+                                     "GMRES+ILU; one host thread"}
+            except Exception as e:  # the baseline is reported, never required
+                cpu = {"value": None, "unit": "ms/step", "cores": 1, "kind": "reference",
+                       "sample": "failed: %s" % e}
+        out = {
+            "metric": METRIC, "value": round(ms_mixed * world / world, 3), "unit": "ms/step",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD if not args.size else "size override %s" % args.size,
+                       "cells": ncell, "parallelism": "replicas" if world > 1 else "single-gpu",
+                       "precision": "mixed: FP32 V-cycle (Chebyshev, %d levels) in FP64 FGMRES(30)" % 4,
+                       "l2": "inputs larger than L2 (every field is a %d MB array)" % (npts * 8 // 2 ** 20)},
+            "fp64_ms_per_step": round(ms_fp64, 3),
+            "mixed_speedup_vs_fp64": round(ms_fp64 / ms_mixed, 3),
+            "max_div": {"mixed": maxdiv, "fp64": maxdiv64},
+            "poisson_iterations": {"mixed": its, "fp64": its64},
+            "adjoint_forward_ratio": None,
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms/step", "h2d_bytes_per_step": io_bytes,
+                    "d2h_bytes_per_step": io_bytes},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "kernel": dom,
+                         "peak_source": peak_kind, "bytes_per_cell": KERNEL_BYTES[dom],
+                         "ms_per_launch": round(launch[dom], 4),
+                         "other_ms_per_launch": {k: round(v, 4) for k, v in launch.items()}},
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": sampler.summary(),
+        }
+        if cpu is not None:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out))
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -130,6 +130,13 @@ int vfs_get_scalar(vfs_ctx *ctx, int which, double *value);
 /* Device address of a field's component (SoA, mx*my*mz doubles), for zero-copy callers. */
 int vfs_field_device_ptr(vfs_ctx *ctx, int field, int component, void **dptr);
 
+/* ---- set-up -------------------------------------------------------------------- */
+
+/* FormMetrics (metrics.c:4, NEWMETRIC) on the device from the grid.dat node coordinates:
+ * x, y, z each hold IM*JM*KM doubles in grid.dat order ([k][j][i], i fastest,
+ * init.c:384-437).  Fills VFS_CENT and every centre and face metric field. */
+int vfs_form_metrics(vfs_ctx *ctx, const double *x, const double *y, const double *z);
+
 /* ---- hot-path operators (each replaces the cited reference function) --------------- */
 
 /* Contra2Cart / Contra2Cart_2 (rhs.c:27, rhs.c:57): Ucat from Ucont at fluid cells,
@@ -144,6 +151,22 @@ int vfs_pressure_gradient(vfs_ctx *ctx);
 
 /* Calc_k_Flux (rhs2.c:1562): mean k-face flux -> VFS_S_MEAN_K_FLUX. */
 int vfs_calc_k_flux(vfs_ctx *ctx, double *mean_k_flux);
+
+/* Calc_Inlet_Area (bcs.c:216): mean fluid k-face area -> VFS_S_MEAN_K_AREA and the
+ * fluid inlet-plane area -> VFS_S_INLET_AREA (k inlet or periodic k). */
+int vfs_calc_inlet_area(vfs_ctx *ctx);
+
+/* FormBCS (bcs.c:1841) for the boundary codes accepted by vfs_create: Contra2Cart, zero
+ * normal flux through no-slip/free-slip i/j walls, Contra2Cart, Ucat = 0 on box edges. */
+int vfs_form_bcs(vfs_ctx *ctx);
+
+/* IB_BC (momentum.c:1982) without immersed bodies: zero normal flux on free-slip faces,
+ * periodic normal flux on ghost planes. */
+int vfs_ib_bc(vfs_ctx *ctx);
+
+/* VolumeFlux(user, Ucont, ...) (poisson.c:3306) for immersed = 0: zero flux through
+ * every interior face between a fluid and a non-fluid cell (blocked-cell bodies). */
+int vfs_volume_flux(vfs_ctx *ctx);
 
 /* RungeKutta (rhs.c:1578), explicit momentum predictor, 4 stages. */
 int vfs_runge_kutta(vfs_ctx *ctx);
@@ -179,6 +202,17 @@ int vfs_divergence(vfs_ctx *ctx, double *max_div);
  * (RHS, solve), UpdatePressure, Projection, Divergence (solvers.c:562-1390 for
  * implicit=0).  opts may be NULL for the defaults. */
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
+
+/* ---- diagnostics ----------------------------------------------------------------- */
+
+/* The context's CUDA stream (cudaStream_t), so callers can record events on it. */
+int vfs_get_stream(vfs_ctx *ctx, void **stream);
+
+/* Launch one kernel of the path `reps` times on the context's stream without a host
+ * synchronisation, on the context's current fields: 0 face fluxes of Formfunction_2,
+ * 1 Fp, 2 RHS projection, 3 FP64 Poisson operator apply, 4 FP32 fine-level Chebyshev
+ * step, 5 FP64 fine-level Chebyshev step, 6 Projection.  For timing only. */
+int vfs_run_kernel(vfs_ctx *ctx, int which, int reps);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,7 @@ def lib():
         L.ref_poisson_rhs2_hypre.argtypes = [vp]
         L.ref_remove_nullspace.argtypes = [vp, ctypes.c_int]
         L.ref_les.argtypes = [ctypes.c_int]
+        L.ref_inlet_area.restype = ctypes.c_double
         L.ref_volume_flux.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
         _lib = L
     return _lib
@@ -118,6 +119,8 @@ class Reference:
         L.ref_set_params(case.ren, case.dt, case.st)
         self.set("lNvert", case.nvert)
         self.set("Nvert", case.nvert)
+        # first-step set-up of main.c:3488 (mean k-face area, inlet area)
+        L.ref_calc_inlet_area()
 
     def close(self):
         shutil.rmtree(self.dir, ignore_errors=True)
@@ -156,6 +159,15 @@ class Reference:
         f, a = ctypes.c_double(), ctypes.c_double()
         lib().ref_get_kflux(ctypes.byref(f), ctypes.byref(a))
         return f.value, a.value
+
+    def volume_flux(self):
+        """VolumeFlux(user, Ucont, ...) (poisson.c:3306); returns (ibm_Flux, ibm_Area)."""
+        f, a = ctypes.c_double(), ctypes.c_double()
+        lib().ref_volume_flux(ctypes.byref(f), ctypes.byref(a))
+        return f.value, a.value
+
+    def inlet_area(self):
+        return lib().ref_inlet_area()
 
     def set_kflux(self, flux, area):
         lib().ref_set_kflux(flux, area)

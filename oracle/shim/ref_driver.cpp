@@ -29,6 +29,9 @@ extern PetscErrorCode ibm_interpolation_advanced(UserCtx *user);
 extern void PoissonRHS2_hypre(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 extern void Remove_Nullspace(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 
+extern double inletArea;
+extern int k_area_allocated;  // bcs.c:213, once per process in the reference
+
 static UserMG g_usermg;
 static UserCtx *g_user = 0;
 static IBMNodes *g_ibm = 0;
@@ -151,6 +154,16 @@ int ref_contra2cart(void) { Contra2Cart(g_user); return 0; }
 int ref_formfunction2(double scale) { return Formfunction_2(g_user, g_user->Rhs, scale); }
 int ref_pressure_gradient(void) { Pressure_Gradient(g_user, g_user->dP); return 0; }
 int ref_calc_k_flux(void) { Calc_k_Flux(g_user); return 0; }
+// Calc_Inlet_Area (bcs.c:216), called once at the first time step (main.c:3488); it also
+// allocates user->k_area, which Calc_k_Flux reads.
+int ref_calc_inlet_area(void) {
+  // each oracle set-up builds a fresh UserCtx, so its k_area must be allocated again
+  k_area_allocated = 0;
+  g_user->mean_k_area = 0;
+  Calc_Inlet_Area(g_user);
+  return 0;
+}
+double ref_inlet_area(void) { return inletArea; }
 int ref_runge_kutta(void) { return RungeKutta(g_user, g_ibm, g_fsi); }
 int ref_form_bcs(void) { return FormBCS(g_user, g_fsi); }
 int ref_inflow_flux(void) { return InflowFlux(g_user); }

@@ -96,17 +96,16 @@ def _csr_apply(R, x_grid):
     rp, col, val = R.poisson_csr()
     gid = R.gid()
     n = len(rp) - 1
+    # interior owners only (the periodic ghost copies of Gid name the same unknowns)
+    inner = np.zeros(R.shape, dtype=bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    m = (gid >= 0) & inner
     xc = np.zeros(n)
-    sel = gid >= 0
-    xc[gid[sel]] = x_grid[sel]
+    xc[gid[m]] = x_grid[m]
     y = np.zeros(n)
     for r in range(n):
         y[r] = np.dot(val[rp[r]:rp[r + 1]], xc[col[rp[r]:rp[r + 1]]])
     out = np.zeros(R.shape)
-    # interior owners only (ghost copies of Gid point at the same unknowns)
-    inner = np.zeros(R.shape, dtype=bool)
-    inner[1:-1, 1:-1, 1:-1] = True
-    m = sel & inner
     out[m] = y[gid[m]]
     return out
 
@@ -166,7 +165,10 @@ def test_update_pressure_projection_divergence(name):
     np.testing.assert_array_equal(ctx.get_field(vfs.P), R.get("P"))
     R.call("ref_projection")
     ctx.projection()
-    np.testing.assert_array_equal(ctx.get_field(vfs.UCONT), R.get("Ucont"))
+    # the device keeps one Ucont array, equal to the reference's local lUcont (the copy
+    # every consumer reads after its periodic refresh); the global Ucont differs from it
+    # only on periodic ghost planes in the components tangential to them
+    np.testing.assert_array_equal(ctx.get_field(vfs.UCONT), R.get("lUcont"))
     np.testing.assert_array_equal(ctx.get_field(vfs.UCAT), R.get("Ucat"))
     # Divergence (main.c:1083-1090) recomputed from the reference's fields
     uc, aj, nv = R.get("lUcont"), R.get("lAj"), R.get("lNvert")
@@ -203,4 +205,20 @@ def test_poisson_solve_matches_direct(name, precision):
     assert st.converged == 1
     got = ctx.get_field(vfs.PHI)
     assert_close(got, want, rtol=1e-8, atol_frac=1e-9, what="phi")
+    R.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_form_metrics_bitwise(name):
+    """FormMetrics on the device from the grid.dat nodes equals the reference's metrics,
+    ghost planes and periodic images included."""
+    case = CASES[name]()
+    R = ref.Reference(case)
+    ctx = vfs.Context(case.config())
+    ctx.form_metrics(case.X, case.Y, case.Z)
+    for key, fid in vfs.METRIC_FIELDS.items():
+        want = R.get(ref.METRIC_VECS[key])
+        got = ctx.get_field(fid)
+        np.testing.assert_array_equal(got, want, err_msg=key)
     R.close()

@@ -1,0 +1,99 @@
+"""One whole projection time step (Flow_Solver, solvers.c:562-1390, implicit = 0) on the
+periodic channel, B200 library against the reference's own functions.  The reference's
+HYPRE solve is replaced by a dense least-squares solve of its own matrix and right-hand
+side (both mean-free, Remove_Nullspace), so the comparison is solver independent up to
+the Poisson tolerance; the GPU solve runs to rtol 1e-13."""
+import numpy as np
+import pytest
+
+from oracle import ref
+import vfs_b200 as vfs
+from helpers import assert_close, build_pair, small_channel, small_cylinders
+
+pytestmark = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+
+
+def reference_step(R):
+    R.call("ref_ib_bc")                               # solvers.c:609 (ti == tistart)
+    R.set("Ucont", R.get("lUcont"))                   # DALocalToGlobal, solvers.c:610
+    R.call("ref_calc_k_flux")                         # solvers.c:644
+    R.call("ref_pressure_gradient")                   # solvers.c:786
+    R.call("ref_runge_kutta")                         # solvers.c:1294
+    R.call("ref_poisson_lhs")                         # poisson_hypre.c:527
+    R.volume_flux()                                   # poisson_hypre.c:566
+    b = R.poisson_rhs_hypre()                         # poisson_hypre.c:568
+    rp, col, val = R.poisson_csr()
+    n = len(rp) - 1
+    A = np.zeros((n, n))
+    for r in range(n):
+        A[r, col[rp[r]:rp[r + 1]]] = val[rp[r]:rp[r + 1]]
+    x = np.linalg.lstsq(A, b, rcond=None)[0]
+    x = R.remove_nullspace(x)                         # poisson_hypre.c:602
+    R.set("Phi2", x)
+    R.call("ref_convert_phi2_phi")                    # poisson_hypre.c:610
+    R.call("ref_update_pressure")                     # solvers.c:1341
+    R.call("ref_projection")                          # solvers.c:1342
+    R.call("ref_ib_bc")                               # solvers.c:1381
+    R.set("Ucont", R.get("lUcont"))
+    R.call("ref_contra2cart")                         # solvers.c:1385
+
+
+def _blocked_cylinders():
+    """The open channel with the cylinder array as blocked cells (immersed = 0): bottom
+    no-slip, top free-slip, spanwise and streamwise periodic."""
+    c = small_cylinders()
+    c.immersed = 0
+    return c
+
+
+STEP_CASES = {"channel": lambda: small_channel(), "wavy": lambda: small_channel(wavy=0.15),
+              "cylinders": _blocked_cylinders}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(STEP_CASES))
+@pytest.mark.parametrize("precision", [0, 1])
+def test_one_step_matches_reference(name, precision):
+    case = STEP_CASES[name]()
+    case.inlet_flux = 5.0
+    R, ctx = build_pair(case)
+    ref.set_global("inlet_flux", case.inlet_flux)
+    ctx.set_scalar(vfs.S_INLET_FLUX, case.inlet_flux)
+    reference_step(R)
+    st = ctx.step(precision=precision, rtol=1e-13)
+    assert st.poisson.converged == 1
+    flux, area = R.kflux()
+    assert abs(st.mean_k_flux - flux) <= 1e-13 * abs(flux)
+    assert abs(ctx.get_scalar(vfs.S_MEAN_K_AREA) - area) <= 1e-13 * area
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-8, atol_frac=1e-9, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-9, atol_frac=1e-10, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
+    assert st.max_div < 1e-8
+    R.close()
+
+
+@pytest.mark.gpu
+def test_ten_steps_stay_divergence_free():
+    """Ten steps on the 64^3 channel: every step ends with max|div| below 1e-8 in both
+    precisions (the Divergence() gate of main.c:1083-1090)."""
+    from vfs_b200 import cases
+    case = cases.channel(32, 32, 32)
+    case.inlet_flux = 5.0
+    R = ref.Reference(case)
+    m = R.metrics()
+    u = cases.initial_ucat(case)
+    uc = cases.ucont_from_ucat(case, u, m)
+    for prec in (0, 1):
+        ctx = vfs.Context(case.config())
+        ctx.set_metrics(m)
+        ctx.set_field(vfs.NVERT, case.nvert)
+        ctx.set_field(vfs.UCONT, uc)
+        ctx.set_field(vfs.UCAT, u)
+        ctx.set_field(vfs.UCAT_O, u)
+        ctx.set_scalar(vfs.S_INLET_FLUX, case.inlet_flux)
+        for s in range(10):
+            st = ctx.step(precision=prec, rtol=1e-10)
+            assert st.poisson.converged == 1
+            assert st.max_div < 1e-8, (prec, s, st.max_div)
+        ctx.close()
+    R.close()

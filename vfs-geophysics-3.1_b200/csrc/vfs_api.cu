@@ -196,7 +196,7 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
   }
   okm &= cudaMalloc(&c->bcflag, (size_t)g.N) == cudaSuccess;
   if (okm) cudaMemsetAsync(c->bcflag, 0, (size_t)g.N, c->stream);
-  okm &= ensure_red(c, 4096) == VFS_OK;
+  okm &= ensure_red(c, 16384) == VFS_OK;
   if (!okm) {
     vfs_destroy((vfs_ctx *)c);
     return set_err(nullptr, VFS_ERR_CUDA, "vfs_create: device allocation failed");
@@ -393,24 +393,47 @@ int vfs_divergence(vfs_ctx *ctx, double *maxdiv) {
   return rc;
 }
 
+int vfs_calc_inlet_area(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return calc_inlet_area(c); }
+int vfs_form_bcs(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return form_bcs(c); }
+int vfs_volume_flux(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return volume_flux(c); }
+int vfs_ib_bc(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return ib_bc(c); }
+
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
   Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
   int rc;
   vfs_step_stats s;
   memset(&s, 0, sizeof(s));
   cudaEventRecord(c->ev0, c->stream);
-  if (!c->ps.built && (rc = poisson_lhs(c))) return rc;
-  // Flow_Solver order for implicit=0 (solvers.c:644-1385)
+  if (c->first_step) {
+    // first time step: Calc_Inlet_Area (main.c:3488), PoissonLHSNew (poisson_hypre.c:527),
+    // IB_BC (solvers.c:603-611)
+    if ((rc = calc_inlet_area(c))) return rc;
+    if ((rc = poisson_lhs(c))) return rc;
+    if ((rc = ib_bc(c))) return rc;
+    c->first_step = false;
+  } else if (!c->ps.built && (rc = poisson_lhs(c))) {
+    return rc;
+  }
+  // Flow_Solver for implicit = 0 (solvers.c:644-1385)
   if ((rc = calc_k_flux(c, &s.mean_k_flux))) return rc;
   if ((rc = pressure_gradient(c))) return rc;
   if ((rc = runge_kutta(c))) return rc;
+  if ((rc = volume_flux(c))) return rc;  // poisson_hypre.c:566
   if ((rc = poisson_rhs(c))) return rc;
   rc = poisson_solve(c, opts, &s.poisson);
   if (rc && rc != VFS_ERR_NOT_CONVERGED) return rc;
-  int solve_rc = rc;
+  const int solve_rc = rc;
   if ((rc = update_pressure(c))) return rc;
   if ((rc = projection(c))) return rc;
   if ((rc = divergence(c, &s.max_div))) return rc;
+  if ((rc = ib_bc(c))) return rc;
+  if ((rc = contra2cart(c))) return rc;
+  // end of the time step: keep Ucont and Ucat of this step (main.c:3584-3602)
+  const size_t bytes = sizeof(double) * (size_t)c->g.N;
+  for (int q = 0; q < 3; q++) {
+    cudaMemcpyAsync(c->f[VFS_UCONT_O][q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(c->f[VFS_UCAT_O][q], c->f[VFS_UCAT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  }
   cudaEventRecord(c->ev1, c->stream);
   cudaEventSynchronize(c->ev1);
   float ms = 0;

@@ -128,6 +128,7 @@ struct Ctx {
   int red_cap = 0;
   double scal[VFS_NSCALARS] = {};
   bool metrics_set = false, nvert_set = false;
+  bool first_step = true;        // ti == tistart set-up pending (main.c:3488, solvers.c:603)
   Poisson ps;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -150,10 +151,13 @@ int pressure_gradient(Ctx *c);
 int calc_k_flux(Ctx *c, double *flux);
 int runge_kutta(Ctx *c);
 int form_bcs(Ctx *c);
+int calc_inlet_area(Ctx *c);
+int ib_bc(Ctx *c);
 
 // Poisson / correction path
 int poisson_lhs(Ctx *c);
 int poisson_rhs(Ctx *c);
+int volume_flux(Ctx *c);
 int poisson_solve(Ctx *c, const vfs_solve_opts *o, vfs_solve_stats *st);
 int poisson_apply_dev(Ctx *c, const double *x, double *y);
 int update_pressure(Ctx *c);

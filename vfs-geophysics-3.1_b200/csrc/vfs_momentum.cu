@@ -628,6 +628,23 @@ int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   return check_launch(c, "k_rhs");
 }
 
+// single-kernel launchers for the diagnostics entry point (vfs_run_kernel)
+void launch_face_flux(Ctx *c) {
+  k_face_flux<<<nblocks(c->g.N, 128), 128, 0, c->stream>>>(c->g, metrics(c), cv(field3(c, VFS_UCONT)),
+                                                           cv(field3(c, VFS_UCAT)), c->nv, c->f[VFS_NU_T][0],
+                                                           flux_out(c, 0), flux_out(c, 1), flux_out(c, 2));
+}
+void launch_fp(Ctx *c) {
+  k_fp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2), c->nv,
+                                                   c->fp[0], c->fp[1], c->fp[2]);
+}
+void launch_rhs(Ctx *c) {
+  V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
+  k_rhs<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, c->fp[0], c->fp[1], c->fp[2], 1.0,
+                                                    field3(c, VFS_RHS), 0, 0.0, cv(field3(c, VFS_DP)), cv(pu),
+                                                    field3(c, VFS_UCONT));
+}
+
 // ------------------------------------------------------------------ Pressure_Gradient
 // momentum.c:197-443 (levelset off): dP on the three faces of each interior cell, with
 // one-sided cross differences next to IB nodes (nvert == 1) and non-periodic walls, and
@@ -766,6 +783,98 @@ int calc_k_flux(Ctx *c, double *flux) {
   s /= (c->g.mz - 2);
   c->scal[VFS_S_MEAN_K_FLUX] = s;
   if (flux) *flux = s;
+  return VFS_OK;
+}
+
+// ------------------------------------------------------------------ Calc_Inlet_Area
+// bcs.c:216-322: mean over k = 1..mz-2 of the fluid k-face area |zet| of the interior
+// (i,j), and the fluid area of the k = 0 plane (inletArea) for an inlet or periodic k.
+__global__ void k_area_parts(Grid g, CV3 zet, const uint8_t *__restrict__ nv, double *parts) {
+  __shared__ double s1[256], s2[256];
+  double a = 0, b = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long sz = (long long)g.mx * g.my;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
+    int i = (int)(p % g.mx);
+    long long q = p / g.mx;
+    int j = (int)(q % g.my);
+    int k = (int)(q / g.my);
+    if (j < 1 || j > g.my - 2 || i < 1 || i > g.mx - 2) continue;
+    const double area = sqrt(zet.x[p] * zet.x[p] + zet.y[p] * zet.y[p] + zet.z[p] * zet.z[p]);
+    if (k >= 1 && k <= g.mz - 2 && nv[p - sz] + nv[p] == 0) a += area;
+    if (k == 0 && nv[p + sz] == 0) b += area;
+  }
+  s1[threadIdx.x] = a; s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { s1[threadIdx.x] += s1[threadIdx.x + w]; s2[threadIdx.x] += s2[threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { parts[blockIdx.x] = s1[0]; parts[gridDim.x + blockIdx.x] = s2[0]; }
+}
+
+int calc_inlet_area(Ctx *c) {
+  int rc;
+  const int nb = 148 * 2;
+  if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
+  k_area_parts<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_ZET)), c->nv, c->red);
+  if ((rc = check_launch(c, "k_area_parts"))) return rc;
+  double a = 0, b = 0;
+  if ((rc = reduce_sum(c, c->red, nb, &a))) return rc;
+  if ((rc = reduce_sum(c, c->red + nb, nb, &b))) return rc;
+  c->scal[VFS_S_MEAN_K_AREA] = a / (double)(c->g.mz - 2);
+  if (c->g.bc[4] == 5 || c->g.kper) c->scal[VFS_S_INLET_AREA] = b;
+  return VFS_OK;
+}
+
+// ------------------------------------------------------------------ IB_BC (no IB nodes)
+// momentum.c:1982-2195 without immersed bodies: normal flux through free-slip faces set
+// to zero and the normal flux of periodic ghost planes taken from the image plane.
+__global__ void k_ib_bc_faces(Grid g, V3 uc) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  int i = (int)(p % mx);
+  long long q = p / mx;
+  int j = (int)(q % my);
+  int k = (int)(q / my);
+  const long long sy = mx, sz = (long long)mx * my;
+  const int *bc = g.bc;
+  // the reference loops over all points and writes the plane values named below; each
+  // thread writes exactly the entries the loop would write at its (i,j,k)
+  if (bc[0] == 10 && i == 1) uc.x[p - 1] = 0;
+  if (bc[1] == 10 && i == mx - 2) uc.x[p] = 0;
+  if (bc[2] == 10 && j == 1) uc.y[p - sy] = 0;
+  if (bc[3] == 10 && j == my - 2) uc.y[p] = 0;
+  if (bc[4] == 10 && k == 1) uc.z[p - sz] = 0;
+  if (bc[5] == 10 && k == mz - 2) uc.z[p] = 0;
+}
+__global__ void k_periodic_normal(Grid g, V3 uc) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  int i = (int)(p % mx);
+  long long q = p / mx;
+  int j = (int)(q % my);
+  int k = (int)(q / my);
+  const long long sy = mx, sz = (long long)mx * my;
+  if (g.iper && i == 0) uc.x[p] = uc.x[p + (mx - 2)];
+  if (g.iper && i == mx - 1) uc.x[p] = uc.x[p - (mx - 2)];
+  if (g.jper && j == 0) uc.y[p] = uc.y[p + (long long)(my - 2) * sy];
+  if (g.jper && j == my - 1) uc.y[p] = uc.y[p - (long long)(my - 2) * sy];
+  if (g.kper && k == 0) uc.z[p] = uc.z[p + (long long)(mz - 2) * sz];
+  if (g.kper && k == mz - 1) uc.z[p] = uc.z[p - (long long)(mz - 2) * sz];
+}
+
+int ib_bc(Ctx *c) {
+  int rc;
+  if (c->g.immersed) return set_err(c, VFS_ERR_INVALID, "IB_BC: immersed-boundary reconstruction is not on this path yet");
+  k_ib_bc_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
+  if ((rc = check_launch(c, "k_ib_bc_faces"))) return rc;
+  if (c->g.iper || c->g.jper || c->g.kper) {
+    k_periodic_normal<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
+    if ((rc = check_launch(c, "k_periodic_normal"))) return rc;
+  }
   return VFS_OK;
 }
 

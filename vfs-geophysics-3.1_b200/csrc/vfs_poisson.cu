@@ -927,6 +927,37 @@ static int sum_fluid(Ctx *c, const double *a, double *out) {
   return reduce_sum(c, c->red, kRedBlocks, out);
 }
 
+// VolumeFlux(user, Ucont, ...) (poisson.c:3306-3500) without sharp-interface IB nodes
+// (immersed = 0): the flux through every interior face between a fluid cell and a
+// non-fluid cell is set to zero.  The face index is the lower cell of the pair, as in
+// the reference loops over interior cells (i <= mx-2 always holds there).
+__global__ void k_volume_flux_blocked(Grid g, const uint8_t *__restrict__ nv, V3 uc) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  int i = (int)(p % g.mx);
+  long long q = p / g.mx;
+  int j = (int)(q % g.my);
+  int k = (int)(q / g.my);
+  if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
+  const long long sy = g.mx, sz = (long long)g.mx * g.my;
+  const bool f0 = nv[p] == 0;
+  if (f0) {
+    if (nv[p + 1] > 0) uc.x[p] = 0;
+    if (nv[p + sy] > 0) uc.y[p] = 0;
+    if (nv[p + sz] > 0) uc.z[p] = 0;
+  } else {
+    if (nv[p + 1] == 0) uc.x[p] = 0;
+    if (nv[p + sy] == 0) uc.y[p] = 0;
+    if (nv[p + sz] == 0) uc.z[p] = 0;
+  }
+}
+
+int volume_flux(Ctx *c) {
+  if (c->g.immersed) return set_err(c, VFS_ERR_INVALID, "VolumeFlux: IB-node flux balance is not on this path yet");
+  k_volume_flux_blocked<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->nv, field3(c, VFS_UCONT));
+  return check_launch(c, "k_volume_flux_blocked");
+}
+
 int poisson_rhs(Ctx *c) {
   int rc;
   double *b = c->f[VFS_B][0];
@@ -1256,3 +1287,58 @@ int divergence(Ctx *c, double *maxdiv) {
 }
 
 }  // namespace vfs
+
+// ------------------------------------------------------------------ diagnostics
+namespace vfs {
+// Launches one kernel of the path `reps` times on the context's stream (no host sync),
+// so a caller can bracket it with events recorded on that stream.
+int run_kernel(Ctx *c, int which, int reps) {
+  const Grid &g = c->g;
+  Poisson &P = c->ps;
+  int rc = VFS_OK;
+  if ((which >= 3) && !P.built && (rc = poisson_lhs(c))) return rc;
+  Metrics m = metrics(c);
+  for (int r = 0; r < reps; r++) {
+    switch (which) {
+      case 0: extern void launch_face_flux(Ctx *); launch_face_flux(c); break;
+      case 1: extern void launch_fp(Ctx *); launch_fp(c); break;
+      case 2: extern void launch_rhs(Ctx *); launch_rhs(c); break;
+      case 3:
+        k_apply64<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, P.coef, P.fluid, c->f[VFS_PHI][0], P.t);
+        break;
+      case 4: {
+        float *w = P.f32;
+        k_cheb_fine<float><<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, P.coef32, P.invdiag32, P.fluid, w, w + g.N,
+                                                                     w + 2 * g.N, w + 3 * g.N, 0.5f, 0.5f, 0);
+        break;
+      }
+      case 5: {
+        double *w = P.f64;
+        k_cheb_fine<double><<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, P.coef, P.invdiag, P.fluid, w, w + g.N,
+                                                                      w + 2 * g.N, w + 3 * g.N, 0.5, 0.5, 0);
+        break;
+      }
+      case 6:
+        k_projection<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->f[VFS_PHI][0], field3(c, VFS_UCONT));
+        break;
+      default: return set_err(c, VFS_ERR_INVALID, "run_kernel: unknown kernel id");
+    }
+    if ((rc = check_launch(c, "run_kernel"))) return rc;
+  }
+  return VFS_OK;
+}
+}  // namespace vfs
+
+extern "C" int vfs_run_kernel(vfs_ctx *ctx, int which, int reps) {
+  vfs::Ctx *c = (vfs::Ctx *)ctx;
+  if (!c || reps < 0) return vfs::set_err(c, VFS_ERR_INVALID, "vfs_run_kernel: bad argument");
+  cudaSetDevice(c->device);
+  return vfs::run_kernel(c, which, reps);
+}
+
+extern "C" int vfs_get_stream(vfs_ctx *ctx, void **stream) {
+  vfs::Ctx *c = (vfs::Ctx *)ctx;
+  if (!c || !stream) return vfs::set_err(c, VFS_ERR_INVALID, "vfs_get_stream: bad argument");
+  *stream = (void *)c->stream;
+  return VFS_OK;
+}

@@ -86,7 +86,8 @@ EXPORTS = [
     "vfs_field_device_ptr", "vfs_contra2cart", "vfs_formfunction2", "vfs_pressure_gradient",
     "vfs_calc_k_flux", "vfs_runge_kutta", "vfs_poisson_lhs", "vfs_poisson_rhs",
     "vfs_poisson_solve", "vfs_poisson_apply", "vfs_update_pressure", "vfs_projection",
-    "vfs_divergence", "vfs_step",
+    "vfs_divergence", "vfs_step", "vfs_calc_inlet_area", "vfs_form_bcs", "vfs_ib_bc",
+    "vfs_form_metrics", "vfs_volume_flux", "vfs_get_stream", "vfs_run_kernel",
 ]
 
 _lib = None
@@ -118,7 +119,8 @@ def load_library(path=None):
     lib.vfs_get_scalar.argtypes = [vp, ctypes.c_int, dp]
     lib.vfs_field_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     for n in ("vfs_contra2cart", "vfs_pressure_gradient", "vfs_runge_kutta", "vfs_poisson_lhs",
-              "vfs_poisson_rhs", "vfs_update_pressure", "vfs_projection"):
+              "vfs_poisson_rhs", "vfs_update_pressure", "vfs_projection", "vfs_calc_inlet_area",
+              "vfs_form_bcs", "vfs_ib_bc", "vfs_volume_flux"):
         getattr(lib, n).argtypes = [vp]
     lib.vfs_formfunction2.argtypes = [vp, ctypes.c_double]
     lib.vfs_calc_k_flux.argtypes = [vp, dp]
@@ -126,6 +128,9 @@ def load_library(path=None):
     lib.vfs_poisson_solve.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats)]
     lib.vfs_poisson_apply.argtypes = [vp, vp, vp]
     lib.vfs_step.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(StepStats)]
+    lib.vfs_form_metrics.argtypes = [vp, vp, vp, vp]
+    lib.vfs_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.vfs_run_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     if path is None:
         _lib = lib
     return lib
@@ -190,6 +195,12 @@ class Context:
             if name in m:
                 self.set_field(fid, m[name])
 
+    def form_metrics(self, X, Y, Z):
+        """FormMetrics on the device from grid.dat node arrays of shape (KM, JM, IM)."""
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (X, Y, Z)]
+        self._check(self.lib.vfs_form_metrics(self.h, xs[0].ctypes.data, xs[1].ctypes.data,
+                                              xs[2].ctypes.data))
+
     def set_scalar(self, which, v):
         self._check(self.lib.vfs_set_scalar(self.h, which, float(v)))
 
@@ -197,6 +208,15 @@ class Context:
         v = ctypes.c_double()
         self._check(self.lib.vfs_get_scalar(self.h, which, ctypes.byref(v)))
         return v.value
+
+    def stream(self):
+        """Address of the context's cudaStream_t."""
+        s = ctypes.c_void_p()
+        self._check(self.lib.vfs_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def run_kernel(self, which, reps=1):
+        self._check(self.lib.vfs_run_kernel(self.h, which, reps))
 
     def launch_count(self):
         return self.lib.vfs_launch_count(self.h)
@@ -218,6 +238,19 @@ class Context:
         v = ctypes.c_double()
         self._check(self.lib.vfs_calc_k_flux(self.h, ctypes.byref(v)))
         return v.value
+
+    def calc_inlet_area(self):        # Calc_Inlet_Area, bcs.c:216
+        self._check(self.lib.vfs_calc_inlet_area(self.h))
+        return self.get_scalar(S_MEAN_K_AREA), self.get_scalar(S_INLET_AREA)
+
+    def form_bcs(self):               # FormBCS, bcs.c:1841
+        self._check(self.lib.vfs_form_bcs(self.h))
+
+    def volume_flux(self):            # VolumeFlux, poisson.c:3306 (immersed = 0)
+        self._check(self.lib.vfs_volume_flux(self.h))
+
+    def ib_bc(self):                  # IB_BC, momentum.c:1982
+        self._check(self.lib.vfs_ib_bc(self.h))
 
     def runge_kutta(self):            # RungeKutta, rhs.c:1578
         self._check(self.lib.vfs_runge_kutta(self.h))
