@@ -210,8 +210,8 @@ int vfs_get_stream(vfs_ctx *ctx, void **stream);
 
 /* Launch one kernel of the path `reps` times on the context's stream without a host
  * synchronisation, on the context's current fields: 0 face fluxes of Formfunction_2,
- * 1 Fp, 2 RHS projection, 3 FP64 Poisson operator apply, 4 FP32 fine-level Chebyshev
- * step, 5 FP64 fine-level Chebyshev step, 6 Projection.  For timing only. */
+ * 1 Fp, 2 RHS projection, 3 FP64 Poisson operator apply, 4 FP32 fine-level y-line
+ * smoothing sweep, 5 FP64 fine-level y-line sweep, 6 Projection.  For timing only. */
 int vfs_run_kernel(vfs_ctx *ctx, int which, int reps);
 
 #ifdef __cplusplus

@@ -270,6 +270,57 @@ __global__ void k_cheb_fine(Grid g, const T *__restrict__ coef, const T *__restr
   xo[p] = (x_is_zero ? T(0) : x[p]) + dn;
 }
 
+// y-line Jacobi smoothing on the fine level (the wall-normal direction of the stretched
+// channel grids carries the strongest coupling, which point smoothers cannot damp).
+// One thread per (i,k) column solves the tridiagonal system of its fluid cells along j
+// (Thomas algorithm; the j-1 / j+1 couplings inside the column, everything else taken
+// from the previous iterate), then x <- x + omega (x_line - x).  Consecutive threads
+// own consecutive i, so every j-step of the sweep is a coalesced row access.
+template <typename T>
+__global__ void k_yline_fine(Grid g, const T *__restrict__ coef, const uint8_t *__restrict__ fluid,
+                             const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ xn,
+                             T *__restrict__ cp, T *__restrict__ dp, T omega, int x_is_zero) {
+  const int ni = g.mx - 2, nk = g.mz - 2;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)ni * nk) return;
+  const int i = 1 + (int)(t % ni), k = 1 + (int)(t / ni);
+  const long long sy = g.mx, N = g.N;
+  const int jn = g.my - 2;
+  T pc = 0, pd = 0;
+  for (int j = 1; j <= jn; j++) {
+    const long long p = lidx(g, i, j, k);
+    T a = 0, bb = 1, cc = 0, r = 0;
+    if (fluid[p] && coef[CP * N + p] != T(0)) {  // a fluid cell without fluid neighbours keeps 0
+      bb = coef[CP * N + p];
+      if (j > 1) a = coef[SP * N + p];
+      if (j < jn) cc = coef[NP * N + p];
+      r = b[p];
+      if (!x_is_zero) {
+#pragma unroll
+        for (int s = 1; s < NSLOT; s++) {
+          if ((s == SP && j > 1) || (s == NP && j < jn)) continue;
+          const T cf = coef[s * N + p];
+          if (cf != T(0)) r -= cf * x[nb_index(g, i, j, k, s)];
+        }
+      }
+    }
+    const T den = bb - a * pc;
+    pc = cc / den;
+    pd = (r - a * pd) / den;
+    cp[p] = pc;
+    dp[p] = pd;
+  }
+  T xnext = 0;
+  for (int j = jn; j >= 1; j--) {
+    const long long p = lidx(g, i, j, k);
+    const T xv = dp[p] - cp[p] * xnext;
+    xnext = xv;
+    if (!fluid[p]) { xn[p] = 0; continue; }
+    xn[p] = x_is_zero ? omega * xv : x[p] + omega * (xv - x[p]);
+  }
+  (void)sy;
+}
+
 // Coarse-level layout: interior cells only, (k*ny + j)*nx + i, periodic wrap in the
 // periodic directions, closed (zero conductance) otherwise.
 struct CL {
@@ -299,6 +350,55 @@ __device__ __forceinline__ T capply(const CL &L, const T *cx, const T *cy, const
   if (k > 0) s += cz[p - sz] * x[p - sz];
   else if (L.kp) s += cz[p + (L.nz - 1) * sz] * x[p + (L.nz - 1) * sz];
   return s;
+}
+
+// y-line Jacobi on a coarse level (7-point conductances, ghost-free layout).
+template <typename T>
+__global__ void k_yline_coarse(CL L, const T *cx, const T *cy, const T *cz, const T *diag,
+                               const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ xn,
+                               T *__restrict__ cp, T *__restrict__ dp, T omega, int x_is_zero) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)L.nx * L.nz) return;
+  const int i = (int)(t % L.nx), k = (int)(t / L.nx);
+  const long long sy = L.nx, sz = (long long)L.nx * L.ny;
+  T pc = 0, pd = 0;
+  for (int j = 0; j < L.ny; j++) {
+    const long long p = cidx(L, i, j, k);
+    T a = 0, bb = 1, cc = 0, r = 0;
+    if (diag[p] != T(0)) {
+      bb = diag[p];
+      if (j > 0) a = cy[p - sy];
+      if (j + 1 < L.ny) cc = cy[p];
+      r = b[p];
+      if (!x_is_zero) {
+        if (i + 1 < L.nx) r -= cx[p] * x[p + 1];
+        else if (L.ip) r -= cx[p] * x[p - (L.nx - 1)];
+        if (i > 0) r -= cx[p - 1] * x[p - 1];
+        else if (L.ip) r -= cx[p + (L.nx - 1)] * x[p + (L.nx - 1)];
+        if (k + 1 < L.nz) r -= cz[p] * x[p + sz];
+        else if (L.kp) r -= cz[p] * x[p - (L.nz - 1) * sz];
+        if (k > 0) r -= cz[p - sz] * x[p - sz];
+        else if (L.kp) r -= cz[p + (L.nz - 1) * sz] * x[p + (L.nz - 1) * sz];
+        if (L.jp) {  // the periodic wrap of the column is taken explicitly
+          if (j == 0) r -= cy[p + (L.ny - 1) * sy] * x[p + (L.ny - 1) * sy];
+          if (j == L.ny - 1) r -= cy[p] * x[p - (L.ny - 1) * sy];
+        }
+      }
+    }
+    const T den = bb - a * pc;
+    pc = cc / den;
+    pd = (r - a * pd) / den;
+    cp[p] = pc;
+    dp[p] = pd;
+  }
+  T xnext = 0;
+  for (int j = L.ny - 1; j >= 0; j--) {
+    const long long p = cidx(L, i, j, k);
+    const T xv = dp[p] - cp[p] * xnext;
+    xnext = xv;
+    if (diag[p] == T(0)) { xn[p] = 0; continue; }
+    xn[p] = x_is_zero ? omega * xv : x[p] + omega * (xv - x[p]);
+  }
 }
 
 template <typename T>
@@ -648,14 +748,14 @@ int poisson_lhs(Ctx *c) {
     ok &= cudaMalloc(&P.invdiag, sizeof(double) * N) == cudaSuccess;
     ok &= cudaMalloc(&P.invdiag32, sizeof(float) * N) == cudaSuccess;
     ok &= cudaMalloc(&P.fluid, N) == cudaSuccess;
-    ok &= cudaMalloc(&P.f32, sizeof(float) * N * 4) == cudaSuccess;
-    ok &= cudaMalloc(&P.f64, sizeof(double) * N * 4) == cudaSuccess;
+    ok &= cudaMalloc(&P.f32, sizeof(float) * N * 6) == cudaSuccess;
+    ok &= cudaMalloc(&P.f64, sizeof(double) * N * 6) == cudaSuccess;
     ok &= cudaMalloc(&P.w, sizeof(double) * N) == cudaSuccess;
     ok &= cudaMalloc(&P.r, sizeof(double) * N) == cudaSuccess;
     ok &= cudaMalloc(&P.t, sizeof(double) * N) == cudaSuccess;
     if (!ok) return set_err(c, VFS_ERR_CUDA, "poisson_lhs: allocation failed");
-    cudaMemsetAsync(P.f32, 0, sizeof(float) * N * 4, c->stream);
-    cudaMemsetAsync(P.f64, 0, sizeof(double) * N * 4, c->stream);
+    cudaMemsetAsync(P.f32, 0, sizeof(float) * N * 6, c->stream);
+    cudaMemsetAsync(P.f64, 0, sizeof(double) * N * 6, c->stream);
     cudaMemsetAsync(P.w, 0, sizeof(double) * N, c->stream);
     cudaMemsetAsync(P.r, 0, sizeof(double) * N, c->stream);
     cudaMemsetAsync(P.t, 0, sizeof(double) * N, c->stream);
@@ -692,13 +792,13 @@ int poisson_lhs(Ctx *c) {
     L.n = (long long)L.nx * L.ny * L.nz;
     bool ok = cudaMalloc(&L.op64, sizeof(double) * L.n * 4) == cudaSuccess;
     ok &= cudaMalloc(&L.op32, sizeof(float) * L.n * 4) == cudaSuccess;
-    ok &= cudaMalloc(&L.x64, sizeof(double) * L.n * 4) == cudaSuccess;
-    ok &= cudaMalloc(&L.x32, sizeof(float) * L.n * 4) == cudaSuccess;
+    ok &= cudaMalloc(&L.x64, sizeof(double) * L.n * 6) == cudaSuccess;
+    ok &= cudaMalloc(&L.x32, sizeof(float) * L.n * 6) == cudaSuccess;
     if (!ok) return set_err(c, VFS_ERR_CUDA, "poisson_lhs: level allocation failed");
     L.b64 = L.x64 + L.n; L.d64 = L.b64 + L.n; L.t64 = L.d64 + L.n;
     L.b32 = L.x32 + L.n; L.d32 = L.b32 + L.n; L.t32 = L.d32 + L.n;
-    cudaMemsetAsync(L.x64, 0, sizeof(double) * L.n * 4, c->stream);
-    cudaMemsetAsync(L.x32, 0, sizeof(float) * L.n * 4, c->stream);
+    cudaMemsetAsync(L.x64, 0, sizeof(double) * L.n * 6, c->stream);
+    cudaMemsetAsync(L.x32, 0, sizeof(float) * L.n * 6, c->stream);
     double *cx = L.op64, *cy = cx + L.n, *cz = cy + L.n, *dg = cz + L.n;
     CL Lc = clevel(c, L);
     if (P.lv.size() == 1) {
@@ -765,41 +865,40 @@ template <> struct FineOps<double> {
   static double *work(Poisson &P) { return P.f64; }
 };
 
-// Chebyshev smoothing of level l; x is updated in place (ping-pong through t).
+// Smoothing of level l: damped y-line Jacobi sweeps (omega = 0.8); x is updated in place
+// (ping-pong through t, the Thomas coefficients in the two scratch slots after it).
+static const double kLineOmega = 0.8;
 template <typename T>
 static int smooth(Ctx *c, int l, int steps, bool x_zero) {
   Poisson &P = c->ps;
-  std::vector<double> c1, c2;
-  const double lmax = (l == 0) ? P.lmax0 : 2.0;
-  cheb_coeffs(lmax, steps, c1, c2);
   int rc;
   if (l == 0) {
     const long long N = c->g.N;
     T *w = FineOps<T>::work(P);
-    T *b = w, *x = w + N, *xt = w + 2 * N, *d = w + 3 * N;
+    T *b = w, *x = w + N, *xt = w + 2 * N, *cp = w + 4 * N, *dp = w + 5 * N;
+    const long long cols = (long long)(c->g.mx - 2) * (c->g.mz - 2);
     for (int s = 0; s < steps; s++) {
       const bool z = x_zero && s == 0;
-      k_cheb_fine<T><<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, FineOps<T>::coef(P), FineOps<T>::invd(P), P.fluid,
-                                                            b, x, xt, d, (T)c1[s], (T)c2[s], z ? 1 : 0);
-      if ((rc = check_launch(c, "k_cheb_fine"))) return rc;
+      k_yline_fine<T><<<nblocks(cols, 128), 128, 0, c->stream>>>(c->g, FineOps<T>::coef(P), P.fluid, b, x, xt, cp, dp,
+                                                                (T)kLineOmega, z ? 1 : 0);
+      if ((rc = check_launch(c, "k_yline_fine"))) return rc;
       std::swap(x, xt);
     }
-    // keep the result in the canonical slot (w + N)
-    if (x != w + N) {
-      cudaMemcpyAsync(w + N, x, sizeof(T) * N, cudaMemcpyDeviceToDevice, c->stream);
-    }
+    if (x != w + N) cudaMemcpyAsync(w + N, x, sizeof(T) * N, cudaMemcpyDeviceToDevice, c->stream);
     return VFS_OK;
   }
   MGLevel &L = P.lv[l];
   CL cl = clevel(c, L);
   const T *op = LvPtr<T>::op(L);
   T *x = LvPtr<T>::x(L), *xt = LvPtr<T>::t(L);
+  T *cp = LvPtr<T>::x(L) + 4 * L.n, *dp = LvPtr<T>::x(L) + 5 * L.n;
+  const long long cols = (long long)L.nx * L.nz;
   for (int s = 0; s < steps; s++) {
     const bool z = x_zero && s == 0;
-    k_cheb_coarse<T><<<nblocks(L.n, 256), 256, 0, c->stream>>>(cl, op, op + L.n, op + 2 * L.n, op + 3 * L.n,
-                                                              LvPtr<T>::b(L), x, xt, LvPtr<T>::d(L), (T)c1[s],
-                                                              (T)c2[s], z ? 1 : 0);
-    if ((rc = check_launch(c, "k_cheb_coarse"))) return rc;
+    k_yline_coarse<T><<<nblocks(cols, 128), 128, 0, c->stream>>>(cl, op, op + L.n, op + 2 * L.n, op + 3 * L.n,
+                                                                LvPtr<T>::b(L), x, xt, cp, dp, (T)kLineOmega,
+                                                                z ? 1 : 0);
+    if ((rc = check_launch(c, "k_yline_coarse"))) return rc;
     std::swap(x, xt);
   }
   if (x != LvPtr<T>::x(L)) cudaMemcpyAsync(LvPtr<T>::x(L), x, sizeof(T) * L.n, cudaMemcpyDeviceToDevice, c->stream);
@@ -1308,14 +1407,16 @@ int run_kernel(Ctx *c, int which, int reps) {
         break;
       case 4: {
         float *w = P.f32;
-        k_cheb_fine<float><<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, P.coef32, P.invdiag32, P.fluid, w, w + g.N,
-                                                                     w + 2 * g.N, w + 3 * g.N, 0.5f, 0.5f, 0);
+        const long long cols = (long long)(g.mx - 2) * (g.mz - 2);
+        k_yline_fine<float><<<nblocks(cols, 128), 128, 0, c->stream>>>(g, P.coef32, P.fluid, w, w + g.N, w + 2 * g.N,
+                                                                      w + 4 * g.N, w + 5 * g.N, 0.8f, 0);
         break;
       }
       case 5: {
         double *w = P.f64;
-        k_cheb_fine<double><<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, P.coef, P.invdiag, P.fluid, w, w + g.N,
-                                                                      w + 2 * g.N, w + 3 * g.N, 0.5, 0.5, 0);
+        const long long cols = (long long)(g.mx - 2) * (g.mz - 2);
+        k_yline_fine<double><<<nblocks(cols, 128), 128, 0, c->stream>>>(g, P.coef, P.fluid, w, w + g.N, w + 2 * g.N,
+                                                                       w + 4 * g.N, w + 5 * g.N, 0.8, 0);
         break;
       }
       case 6:
