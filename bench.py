@@ -294,6 +294,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", default=None, help="nx,ny,nz override (not for reported numbers)")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="after the warm-up, run one mixed step inside cudaProfilerStart/Stop and exit "
+                         "(for ncu --profile-from-start off); prints no JSON")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -323,6 +326,14 @@ def main():
     # warm-up (also the first-step set-up: inlet area, Poisson operator, IB_BC)
     for _ in range(max(3, args.warmup)):
         ctx.step(precision=0, rtol=1e-10)
+    if args.profile_step:
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        ctx.step(precision=0, rtol=1e-10)
+        ctx.synchronize()
+        torch.cuda.profiler.stop()
+        ctx.close()
+        return
 
     sampler = ClockSampler(local)
     with sampler:
