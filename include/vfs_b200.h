@@ -203,6 +203,36 @@ int vfs_divergence(vfs_ctx *ctx, double *max_div);
  * implicit=0).  opts may be NULL for the defaults. */
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
 
+/* ---- allocation-free variant ---------------------------------------------------- */
+
+/* Largest grid (DA points (IM+1)*(JM+1)*(KM+1)) vfs_contra2cart_noalloc accepts, and the
+ * size of the static device scratch it keeps for that limit (26 bytes per point). */
+#define VFS_NOALLOC_MAX_POINTS (1 << 21)
+#define VFS_NOALLOC_SCRATCH_BYTES (26ull * (1ull << 21) + 256ull)
+
+/* Contra2Cart for callers that cannot allocate device memory, for instance a solver
+ * embedded in a framework that owns every device allocation through its own pool, or a
+ * process whose device memory is fixed before the solver starts.  No counterpart in the
+ * reference: it is the same computation as vfs_contra2cart (rhs.c:57), on caller-owned
+ * device buffers, without a context and without any allocation.
+ *
+ * All arrays are device pointers on the current device, in the reference's DA layout
+ * with vector fields as three consecutive component blocks (x block, y block, z block,
+ * each (IM+1)*(JM+1)*(KM+1) doubles):  ucont [3N, its periodic ghost values are
+ * refreshed in place, as the reference does on lUcont], csi/eta/zet [3N each], nvert
+ * [N, integer values], ucat_old [3N, slip-wall ghost source], ucat [3N, in/out: cells
+ * with nvert >= 0.1 keep their value].  stream is a cudaStream_t (NULL: default).
+ *
+ * Scratch lives in one static device array of VFS_NOALLOC_SCRATCH_BYTES (about 52 MB)
+ * that every GPU loading the library holds until the process exits.  Grids above
+ * VFS_NOALLOC_MAX_POINTS are rejected with VFS_ERR_INVALID.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Every call shares the array: calls that overlap on the GPU race.  The
+ * call synchronises its stream before returning.  Nothing is allocated or freed. */
+int vfs_contra2cart_noalloc(const vfs_config *cfg, double *ucont, const double *csi, const double *eta,
+                            const double *zet, const double *nvert, const double *ucat_old, double *ucat,
+                            void *stream);
+
 /* ---- diagnostics ----------------------------------------------------------------- */
 
 /* The context's CUDA stream (cudaStream_t), so callers can record events on it. */
