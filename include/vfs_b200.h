@@ -88,9 +88,10 @@ typedef struct {
   int precision;     /* 0: mixed (FP32 V-cycle inside FP64 FGMRES), 1: all-FP64 */
   int restart;       /* FGMRES restart length (default 30) */
   int max_iter;      /* outer iteration cap (default 200) */
-  int levels;        /* multigrid levels including the finest (default 4) */
-  int pre_smooth, post_smooth; /* Chebyshev steps per level (default 2, 2) */
-  int coarse_iters;  /* smoothing steps on the coarsest level (default 16) */
+  int levels;        /* multigrid levels including the finest (default 0: every level
+                        the grid coarsens to) */
+  int pre_smooth, post_smooth; /* zebra line Gauss-Seidel sweeps per level (default 2, 2) */
+  int coarse_iters;  /* sweeps on the coarsest level (default 16) */
   int reserved[5];
   double rtol;       /* relative residual target (default 1e-10) */
   double atol;       /* absolute residual target (default 0) */

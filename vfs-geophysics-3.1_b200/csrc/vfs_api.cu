@@ -224,13 +224,9 @@ int vfs_destroy(vfs_ctx *ctx) {
   if (c->red) cudaFree(c->red);
   if (c->red_host) cudaFreeHost(c->red_host);
   Poisson &P = c->ps;
-  cudaFree(P.coef); cudaFree(P.coef32); cudaFree(P.invdiag); cudaFree(P.invdiag32); cudaFree(P.fluid);
-  cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t);
-  cudaFree(P.f32); cudaFree(P.f64);
-  for (size_t l = 1; l < P.lv.size(); l++) {
-    MGLevel &L = P.lv[l];
-    cudaFree(L.op64); cudaFree(L.op32); cudaFree(L.x64); cudaFree(L.x32);
-  }
+  cudaFree(P.coef); cudaFree(P.fluid);
+  cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t); cudaFree(P.hdev);
+  mg_free(P);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -74,33 +74,36 @@ struct Metrics {
 // (poisson.c:951-969: CP EP WP NP SP TP BP NE SE NW SW TN BN TS BS TE BE TW BW).
 enum { CP = 0, EP, WP, NP, SP, TP, BP, NE, SE, NW, SW, TN, BN, TS, BS, TE, BE, TW, BW, NSLOT };
 
-struct MGLevel {
-  int nx, ny, nz;          // interior cells (coarse levels use a ghost-free layout)
+// One multigrid level in zebra order (see vfs_mg.cu): cells ((k*ny + j)*2 + colour)*hx
+// + i/2 with colour = (i xor k) & 1, hx = ceil(nx/2), n slots in all.
+struct ZL {
+  int nx, ny, nz, hx, ip, jp, kp;
   long long n;
-  double *op64 = nullptr;  // 4*n: conductance to +i, +j, +k neighbour, diagonal (FP64)
-  float *op32 = nullptr;   // FP32 copy of op64
-  double *x64 = nullptr, *b64 = nullptr, *d64 = nullptr, *t64 = nullptr;
-  float *x32 = nullptr, *b32 = nullptr, *d32 = nullptr, *t32 = nullptr;
+};
+
+struct MGLevel {
+  ZL z;
+  bool zebra = true;        // two-colour line Gauss-Seidel is race-free on this level
+  double *op64 = nullptr;   // 6n: couplings +i, +j, +k, diagonal, Thomas factors cpr, 1/pivot
+  float *op32 = nullptr;    // FP32 copy
+  double *v64 = nullptr;    // 4n: x, b, previous x (line Jacobi), forward-elimination scratch
+  float *v32 = nullptr;
 };
 
 struct Poisson {
   bool built = false;
   double *coef = nullptr;   // NSLOT * N doubles (SoA by slot)
-  float *coef32 = nullptr;  // NSLOT * N floats
-  double *invdiag = nullptr;
-  float *invdiag32 = nullptr;
+  int nslot = NSLOT;        // 7 when every cross slot is zero (the apply reads slots 0..6)
   uint8_t *fluid = nullptr; // 1 if the cell is a Poisson unknown (gid >= 0)
   long long nfluid = 0;
   double sum_aj = 0;        // sum of aj over fluid cells (Remove_Nullspace_Scale)
-  std::vector<MGLevel> lv;  // lv[0] describes the fine level (coefficients above)
+  std::vector<MGLevel> lv;  // multigrid levels, finest first
   // FGMRES workspace (grid layout, N doubles each)
   int restart = 0;
   double *V = nullptr;      // (restart+1) * N
   double *Z = nullptr;      // restart * N
   double *w = nullptr, *r = nullptr, *t = nullptr;
-  float *f32 = nullptr;     // 4*N FP32 fine-level work (b, x, x', d)
-  double *f64 = nullptr;    // 4*N FP64 fine-level work
-  double lmax0 = 0;         // fine-level bound of the spectrum of D^-1 A
+  double *hdev = nullptr;   // Gram-Schmidt coefficients on the device (64 doubles)
 };
 
 struct Ctx {
@@ -163,6 +166,12 @@ int poisson_apply_dev(Ctx *c, const double *x, double *y);
 int update_pressure(Ctx *c);
 int projection(Ctx *c);
 int divergence(Ctx *c, double *maxdiv);
+
+// multigrid preconditioner (vfs_mg.cu)
+int mg_setup(Ctx *c);
+void mg_free(Poisson &P);
+int mg_precondition(Ctx *c, const double *v, double *z, const vfs_solve_opts &o);
+int mg_sweep_fine(Ctx *c, int precision);
 
 // reductions (deterministic two-pass); result copied to host
 int reduce_sum(Ctx *c, const double *parts, int nparts, double *out);

@@ -118,7 +118,7 @@ __device__ __forceinline__ void main_term(StencilCtx &S, const int d[3], double 
 // MatSetValues filter (|v| > 1e-10 and a valid column, or the diagonal; INSERT keeps the
 // last slot that names a column) of poisson.c:1608-1612.
 __global__ void k_poisson_coef(Grid g, Metrics m, const uint8_t *__restrict__ nv, double *coef,
-                               uint8_t *fluid, double *invdiag) {
+                               uint8_t *fluid) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
@@ -131,7 +131,6 @@ __global__ void k_poisson_coef(Grid g, Metrics m, const uint8_t *__restrict__ nv
   if (!interior || nv[p] != 0) {
     for (int s = 0; s < NSLOT; s++) coef[s * N + p] = 0;
     fluid[p] = 0;
-    invdiag[p] = 0;
     return;
   }
   StencilCtx S;
@@ -193,15 +192,9 @@ __global__ void k_poisson_coef(Grid g, Metrics m, const uint8_t *__restrict__ nv
       if (set[t] && col[t] == col[s]) { set[s] = false; break; }
   }
   // A slot overwritten by a later one contributes nothing; the later slot carries the
-  // inserted value.  The diagonal is the entry whose column is the cell itself.
-  double diag = 0;
-  for (int s = 0; s < NSLOT; s++) {
-    double v = set[s] ? S.vol[s] : 0.0;
-    coef[s * N + p] = v;
-    if (set[s] && col[s] == p) diag = v;
-  }
+  // inserted value.
+  for (int s = 0; s < NSLOT; s++) coef[s * N + p] = set[s] ? S.vol[s] : 0.0;
   fluid[p] = 1;
-  invdiag[p] = diag != 0 ? 1.0 / diag : 0.0;
 }
 
 // Neighbour index of slot s for an unknown (valid only where the coefficient is non-zero;
@@ -210,423 +203,149 @@ __device__ __forceinline__ long long nb_index(const Grid &g, int i, int j, int k
   return lidx(g, wrapi(g, i + c_off[s][0]), wrapj(g, j + c_off[s][1]), wrapk(g, k + c_off[s][2]));
 }
 
-// y = A x on the grid layout (FP64).
-__global__ void k_apply64(Grid g, const double *__restrict__ coef, const uint8_t *__restrict__ fluid,
-                          const double *__restrict__ x, double *__restrict__ y) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
-  if (!fluid[p]) { y[p] = 0; return; }
-  const int mx = g.mx, my = g.my;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+// (A x)[p] on the grid layout from the first NS stencil slots: NS = 7 when every cross
+// slot of the operator is zero (orthogonal grids), else 19.  A skipped slot is zero, so
+// both forms give the same sums.  Rows of non-unknowns are all zero.
+template <int NS>
+__device__ __forceinline__ double apply_row64(const Grid &g, const double *__restrict__ coef,
+                                              const double *__restrict__ x, long long p) {
+  const int i = (int)(p % g.mx);
+  const long long q = p / g.mx;
+  const int j = (int)(q % g.my), k = (int)(q / g.my);
   double s = 0;
 #pragma unroll
-  for (int t = 0; t < NSLOT; t++) {
+  for (int t = 0; t < NS; t++) {
     const double c = coef[t * g.N + p];
     if (c != 0.0) s += c * x[nb_index(g, i, j, k, t)];
   }
-  y[p] = s;
+  return s;
+}
+
+// y = A x on the grid layout (FP64).
+template <int NS>
+__global__ void k_apply(Grid g, const double *__restrict__ coef, const double *__restrict__ x,
+                        double *__restrict__ y) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  y[p] = apply_row64<NS>(g, coef, x, p);
 }
 
 int poisson_apply_dev(Ctx *c, const double *x, double *y) {
-  k_apply64<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, c->ps.fluid, x, y);
-  return check_launch(c, "k_apply64");
+  if (c->ps.nslot == 7) k_apply<7><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
+  else k_apply<NSLOT><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
+  return check_launch(c, "k_apply");
 }
 
-// ------------------------------------------------------------------ multigrid
-// Fine-level smoother / residual in type T on the 19-point operator.
-template <typename T>
-__device__ __forceinline__ T apply_row(const Grid &g, const T *__restrict__ coef, const T *__restrict__ x,
-                                       long long p, int i, int j, int k) {
-  T s = 0;
-#pragma unroll
-  for (int t = 0; t < NSLOT; t++) {
-    const T cf = coef[t * g.N + p];
-    if (cf != T(0)) s += cf * x[nb_index(g, i, j, k, t)];
-  }
-  return s;
-}
+// ------------------------------------------------------------------ Krylov kernels
+// The FGMRES vectors are exactly zero off the unknowns, so every dot product runs over
+// the whole grid layout.  Reductions are deterministic: per-thread sums in a fixed order,
+// warp shuffles, a fixed-order sum over warps, then k_sum_rows over the block partials.
+static const int kKryBlocks = 148 * 4;
+static const int kKryThreads = 256;
 
-// One Chebyshev step on the fine level: r = D^-1 (b - A x), d = c1*d + c2*r, xo = x + d.
-template <typename T>
-__global__ void k_cheb_fine(Grid g, const T *__restrict__ coef, const T *__restrict__ invd,
-                            const uint8_t *__restrict__ fluid, const T *__restrict__ b,
-                            const T *__restrict__ x, T *__restrict__ xo, T *__restrict__ d, T c1,
-                            T c2, int x_is_zero) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
-  if (!fluid[p]) { xo[p] = 0; d[p] = 0; return; }
-  const int mx = g.mx, my = g.my;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
-  T ax = x_is_zero ? T(0) : apply_row<T>(g, coef, x, p, i, j, k);
-  T r = invd[p] * (b[p] - ax);
-  T dn = (x_is_zero ? T(0) : c1 * d[p]) + c2 * r;
-  d[p] = dn;
-  xo[p] = (x_is_zero ? T(0) : x[p]) + dn;
-}
-
-// y-line Jacobi smoothing on the fine level (the wall-normal direction of the stretched
-// channel grids carries the strongest coupling, which point smoothers cannot damp).
-// One thread per (i,k) column solves the tridiagonal system of its fluid cells along j
-// (Thomas algorithm; the j-1 / j+1 couplings inside the column, everything else taken
-// from the previous iterate), then x <- x + omega (x_line - x).  Consecutive threads
-// own consecutive i, so every j-step of the sweep is a coalesced row access.
-template <typename T>
-__global__ void k_yline_fine(Grid g, const T *__restrict__ coef, const uint8_t *__restrict__ fluid,
-                             const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ xn,
-                             T *__restrict__ cp, T *__restrict__ dp, T omega, int x_is_zero) {
-  const int ni = g.mx - 2, nk = g.mz - 2;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)ni * nk) return;
-  const int i = 1 + (int)(t % ni), k = 1 + (int)(t / ni);
-  const long long sy = g.mx, N = g.N;
-  const int jn = g.my - 2;
-  T pc = 0, pd = 0;
-  for (int j = 1; j <= jn; j++) {
-    const long long p = lidx(g, i, j, k);
-    T a = 0, bb = 1, cc = 0, r = 0;
-    if (fluid[p] && coef[CP * N + p] != T(0)) {  // a fluid cell without fluid neighbours keeps 0
-      bb = coef[CP * N + p];
-      if (j > 1) a = coef[SP * N + p];
-      if (j < jn) cc = coef[NP * N + p];
-      r = b[p];
-      if (!x_is_zero) {
-#pragma unroll
-        for (int s = 1; s < NSLOT; s++) {
-          if ((s == SP && j > 1) || (s == NP && j < jn)) continue;
-          const T cf = coef[s * N + p];
-          if (cf != T(0)) r -= cf * x[nb_index(g, i, j, k, s)];
-        }
-      }
-    }
-    const T den = bb - a * pc;
-    pc = cc / den;
-    pd = (r - a * pd) / den;
-    cp[p] = pc;
-    dp[p] = pd;
-  }
-  T xnext = 0;
-  for (int j = jn; j >= 1; j--) {
-    const long long p = lidx(g, i, j, k);
-    const T xv = dp[p] - cp[p] * xnext;
-    xnext = xv;
-    if (!fluid[p]) { xn[p] = 0; continue; }
-    xn[p] = x_is_zero ? omega * xv : x[p] + omega * (xv - x[p]);
-  }
-  (void)sy;
-}
-
-// Coarse-level layout: interior cells only, (k*ny + j)*nx + i, periodic wrap in the
-// periodic directions, closed (zero conductance) otherwise.
-struct CL {
-  int nx, ny, nz, ip, jp, kp;
-  long long n;
-};
-__device__ __forceinline__ long long cidx(const CL &L, int i, int j, int k) {
-  return ((long long)k * L.ny + j) * L.nx + i;
-}
-
-template <typename T>
-__device__ __forceinline__ T capply(const CL &L, const T *cx, const T *cy, const T *cz, const T *diag,
-                                    const T *x, long long p, int i, int j, int k) {
-  T s = diag[p] * x[p];
-  // +i / -i
-  if (i + 1 < L.nx) s += cx[p] * x[p + 1];
-  else if (L.ip) s += cx[p] * x[p - (L.nx - 1)];
-  if (i > 0) s += cx[p - 1] * x[p - 1];
-  else if (L.ip) s += cx[p + (L.nx - 1)] * x[p + (L.nx - 1)];
-  const long long sy = L.nx, sz = (long long)L.nx * L.ny;
-  if (j + 1 < L.ny) s += cy[p] * x[p + sy];
-  else if (L.jp) s += cy[p] * x[p - (L.ny - 1) * sy];
-  if (j > 0) s += cy[p - sy] * x[p - sy];
-  else if (L.jp) s += cy[p + (L.ny - 1) * sy] * x[p + (L.ny - 1) * sy];
-  if (k + 1 < L.nz) s += cz[p] * x[p + sz];
-  else if (L.kp) s += cz[p] * x[p - (L.nz - 1) * sz];
-  if (k > 0) s += cz[p - sz] * x[p - sz];
-  else if (L.kp) s += cz[p + (L.nz - 1) * sz] * x[p + (L.nz - 1) * sz];
-  return s;
-}
-
-// y-line Jacobi on a coarse level (7-point conductances, ghost-free layout).
-template <typename T>
-__global__ void k_yline_coarse(CL L, const T *cx, const T *cy, const T *cz, const T *diag,
-                               const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ xn,
-                               T *__restrict__ cp, T *__restrict__ dp, T omega, int x_is_zero) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)L.nx * L.nz) return;
-  const int i = (int)(t % L.nx), k = (int)(t / L.nx);
-  const long long sy = L.nx, sz = (long long)L.nx * L.ny;
-  T pc = 0, pd = 0;
-  for (int j = 0; j < L.ny; j++) {
-    const long long p = cidx(L, i, j, k);
-    T a = 0, bb = 1, cc = 0, r = 0;
-    if (diag[p] != T(0)) {
-      bb = diag[p];
-      if (j > 0) a = cy[p - sy];
-      if (j + 1 < L.ny) cc = cy[p];
-      r = b[p];
-      if (!x_is_zero) {
-        if (i + 1 < L.nx) r -= cx[p] * x[p + 1];
-        else if (L.ip) r -= cx[p] * x[p - (L.nx - 1)];
-        if (i > 0) r -= cx[p - 1] * x[p - 1];
-        else if (L.ip) r -= cx[p + (L.nx - 1)] * x[p + (L.nx - 1)];
-        if (k + 1 < L.nz) r -= cz[p] * x[p + sz];
-        else if (L.kp) r -= cz[p] * x[p - (L.nz - 1) * sz];
-        if (k > 0) r -= cz[p - sz] * x[p - sz];
-        else if (L.kp) r -= cz[p + (L.nz - 1) * sz] * x[p + (L.nz - 1) * sz];
-        if (L.jp) {  // the periodic wrap of the column is taken explicitly
-          if (j == 0) r -= cy[p + (L.ny - 1) * sy] * x[p + (L.ny - 1) * sy];
-          if (j == L.ny - 1) r -= cy[p] * x[p - (L.ny - 1) * sy];
-        }
-      }
-    }
-    const T den = bb - a * pc;
-    pc = cc / den;
-    pd = (r - a * pd) / den;
-    cp[p] = pc;
-    dp[p] = pd;
-  }
-  T xnext = 0;
-  for (int j = L.ny - 1; j >= 0; j--) {
-    const long long p = cidx(L, i, j, k);
-    const T xv = dp[p] - cp[p] * xnext;
-    xnext = xv;
-    if (diag[p] == T(0)) { xn[p] = 0; continue; }
-    xn[p] = x_is_zero ? omega * xv : x[p] + omega * (xv - x[p]);
-  }
-}
-
-template <typename T>
-__global__ void k_cheb_coarse(CL L, const T *cx, const T *cy, const T *cz, const T *diag,
-                              const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ xo,
-                              T *__restrict__ d, T c1, T c2, int x_is_zero) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= L.n) return;
-  if (diag[p] == T(0)) { xo[p] = 0; d[p] = 0; return; }
-  int i = (int)(p % L.nx);
-  long long q = p / L.nx;
-  int j = (int)(q % L.ny);
-  int k = (int)(q / L.ny);
-  T ax = x_is_zero ? T(0) : capply<T>(L, cx, cy, cz, diag, x, p, i, j, k);
-  T r = (b[p] - ax) / diag[p];
-  T dn = (x_is_zero ? T(0) : c1 * d[p]) + c2 * r;
-  d[p] = dn;
-  xo[p] = (x_is_zero ? T(0) : x[p]) + dn;
-}
-
-// Residual of the fine level summed over the 8 children of each level-1 cell.
-template <typename T>
-__global__ void k_restrict_fine(Grid g, CL L1, const T *__restrict__ coef, const uint8_t *__restrict__ fluid,
-                                const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ bc) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= L1.n) return;
-  int I = (int)(p % L1.nx);
-  long long q = p / L1.nx;
-  int J = (int)(q % L1.ny);
-  int K = (int)(q / L1.ny);
-  T s = 0;
-  for (int c = 0; c < 2; c++)
-    for (int b2 = 0; b2 < 2; b2++)
-      for (int a = 0; a < 2; a++) {
-        const int i = 2 * I + 1 + a, j = 2 * J + 1 + b2, k = 2 * K + 1 + c;
-        const long long f = lidx(g, i, j, k);
-        if (!fluid[f]) continue;
-        s += b[f] - apply_row<T>(g, coef, x, f, i, j, k);
-      }
-  bc[p] = s;
-}
-
-template <typename T>
-__global__ void k_restrict_coarse(CL L, CL Lc, const T *cx, const T *cy, const T *cz, const T *diag,
-                                  const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ bc) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= Lc.n) return;
-  int I = (int)(p % Lc.nx);
-  long long q = p / Lc.nx;
-  int J = (int)(q % Lc.ny);
-  int K = (int)(q / Lc.ny);
-  T s = 0;
-  for (int c = 0; c < 2; c++)
-    for (int b2 = 0; b2 < 2; b2++)
-      for (int a = 0; a < 2; a++) {
-        const int i = 2 * I + a, j = 2 * J + b2, k = 2 * K + c;
-        const long long f = cidx(L, i, j, k);
-        if (diag[f] == T(0)) continue;
-        s += b[f] - capply<T>(L, cx, cy, cz, diag, x, f, i, j, k);
-      }
-  bc[p] = s;
-}
-
-// x_fine += x_coarse (piecewise-constant prolongation, transpose of the restriction).
-template <typename T>
-__global__ void k_prolong_fine(Grid g, CL L1, const uint8_t *__restrict__ fluid, T *x, const T *__restrict__ xc) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
-  if (!fluid[p]) return;
-  const int mx = g.mx, my = g.my;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
-  x[p] += xc[cidx(L1, (i - 1) >> 1, (j - 1) >> 1, (k - 1) >> 1)];
-}
-template <typename T>
-__global__ void k_prolong_coarse(CL L, CL Lc, const T *diag, T *x, const T *__restrict__ xc) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= L.n) return;
-  if (diag[p] == T(0)) return;
-  int i = (int)(p % L.nx);
-  long long q = p / L.nx;
-  int j = (int)(q % L.ny);
-  int k = (int)(q / L.ny);
-  x[p] += xc[cidx(Lc, i >> 1, j >> 1, k >> 1)];
-}
-
-// Level-1 conductances from the fine operator's 7-point couplings (symmetrised, clipped
-// at zero): C = 0.5 * sum of the four fine face couplings on the coarse face.
-__global__ void k_build_l1(Grid g, CL L1, const double *__restrict__ coef, const uint8_t *__restrict__ fluid,
-                           double *cx, double *cy, double *cz) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= L1.n) return;
-  int I = (int)(p % L1.nx);
-  long long q = p / L1.nx;
-  int J = (int)(q % L1.ny);
-  int K = (int)(q / L1.ny);
-  const long long N = g.N;
-  double sx = 0, sy = 0, sz = 0;
-  for (int u = 0; u < 2; u++)
-    for (int v = 0; v < 2; v++) {
-      {  // x face: fine cells (2I+2, 2J+1+u, 2K+1+v) -> +i
-        const int i = 2 * I + 2, j = 2 * J + 1 + u, k = 2 * K + 1 + v;
-        const long long f = lidx(g, i, j, k);
-        const long long e = lidx(g, wrapi(g, i + 1), j, k);
-        if (i + 1 <= g.mx - 2 || g.iper)
-          if (fluid[f] && fluid[e]) sx += fmax(0.0, 0.5 * (coef[EP * N + f] + coef[WP * N + e]));
-      }
-      {
-        const int i = 2 * I + 1 + u, j = 2 * J + 2, k = 2 * K + 1 + v;
-        const long long f = lidx(g, i, j, k);
-        const long long e = lidx(g, i, wrapj(g, j + 1), k);
-        if (j + 1 <= g.my - 2 || g.jper)
-          if (fluid[f] && fluid[e]) sy += fmax(0.0, 0.5 * (coef[NP * N + f] + coef[SP * N + e]));
-      }
-      {
-        const int i = 2 * I + 1 + u, j = 2 * J + 1 + v, k = 2 * K + 2;
-        const long long f = lidx(g, i, j, k);
-        const long long e = lidx(g, i, j, wrapk(g, k + 1));
-        if (k + 1 <= g.mz - 2 || g.kper)
-          if (fluid[f] && fluid[e]) sz += fmax(0.0, 0.5 * (coef[TP * N + f] + coef[BP * N + e]));
-      }
-    }
-  cx[p] = 0.5 * sx;
-  cy[p] = 0.5 * sy;
-  cz[p] = 0.5 * sz;
-}
-
-// Coarser conductances from the level below (same rule), and the diagonal.
-__global__ void k_build_coarse(CL L, CL Lc, const double *cx, const double *cy, const double *cz,
-                               double *ccx, double *ccy, double *ccz) {
-  // cx/cy/cz: the finer level's conductances (op64 rows 0..2)
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= Lc.n) return;
-  int I = (int)(p % Lc.nx);
-  long long q = p / Lc.nx;
-  int J = (int)(q % Lc.ny);
-  int K = (int)(q / Lc.ny);
-  double sx = 0, sy = 0, sz = 0;
-  for (int u = 0; u < 2; u++)
-    for (int v = 0; v < 2; v++) {
-      sx += cx[cidx(L, 2 * I + 1, 2 * J + u, 2 * K + v)];
-      sy += cy[cidx(L, 2 * I + u, 2 * J + 1, 2 * K + v)];
-      sz += cz[cidx(L, 2 * I + u, 2 * J + v, 2 * K + 1)];
-    }
-  ccx[p] = 0.5 * sx;
-  ccy[p] = 0.5 * sy;
-  ccz[p] = 0.5 * sz;
-}
-
-__global__ void k_coarse_diag(CL L, double *cx, double *cy, double *cz, double *diag) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= L.n) return;
-  int i = (int)(p % L.nx);
-  long long q = p / L.nx;
-  int j = (int)(q % L.ny);
-  int k = (int)(q / L.ny);
-  const long long sy = L.nx, sz = (long long)L.nx * L.ny;
-  // close faces leaving a non-periodic domain
-  if (i == L.nx - 1 && !L.ip) cx[p] = 0;
-  if (j == L.ny - 1 && !L.jp) cy[p] = 0;
-  if (k == L.nz - 1 && !L.kp) cz[p] = 0;
-  double s = cx[p] + cy[p] + cz[p];
-  s += (i > 0) ? cx[p - 1] : (L.ip ? cx[p + L.nx - 1] : 0.0);
-  s += (j > 0) ? cy[p - sy] : (L.jp ? cy[p + (L.ny - 1) * sy] : 0.0);
-  s += (k > 0) ? cz[p - sz] : (L.kp ? cz[p + (L.nz - 1) * sz] : 0.0);
-  diag[p] = -s;
-}
-
-__global__ void k_cast_d2f(long long n, const double *a, float *b) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p < n) b[p] = (float)a[p];
-}
-__global__ void k_cast_f2d(long long n, const float *a, double *b) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p < n) b[p] = (double)a[p];
-}
-
-// Gershgorin bound of D^-1 A (max over rows of sum |a_ij| / |a_ii|) for the fine level.
-__global__ void k_gersh_fine(Grid g, const double *coef, const double *invd, const uint8_t *fluid, double *parts) {
-  __shared__ double sh[256];
-  double mval = 0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
-    if (!fluid[p]) continue;
-    double s = 0;
-    for (int t = 0; t < NSLOT; t++) s += fabs(coef[t * g.N + p]);
-    mval = fmax(mval, s * fabs(invd[p]));
-  }
-  sh[threadIdx.x] = mval;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
-}
-
-// ------------------------------------------------------------------ reductions
-// Partial sums of up to NV dot products <v_i, w> plus <w,w>, one pass over w.
+// Block sums of rows 0..nv-1 and of row NV (stored as row nv) of acc into
+// parts[row * gridDim.x + blockIdx.x].
 template <int NV>
-__global__ void k_multidot(long long n, const double *__restrict__ V, int nv, const double *__restrict__ w,
-                           double *parts) {
-  // parts layout: [nv+1][gridDim.x]
-  __shared__ double sh[NV + 1][128];
+__device__ __forceinline__ void block_sums(const double (&acc)[NV + 1], int nv, double *__restrict__ parts) {
+  __shared__ double sh[NV + 1][kKryThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t <= NV; t++) {
+    double v = acc[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[t][warp] = v;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t <= NV; t += blockDim.x) {
+    if (t < nv || t == NV) {
+      double s = 0;
+      for (int w = 0; w < kKryThreads / 32; w++) s += sh[t][w];
+      parts[(long long)(t == NV ? nv : t) * gridDim.x + blockIdx.x] = s;
+    }
+  }
+}
+
+// w = A z, with <V_t, w> (t < nv) and <w, w>.
+template <int NS, int NV>
+__global__ void __launch_bounds__(kKryThreads) k_apply_dots(Grid g, const double *__restrict__ coef,
+                                                            const double *__restrict__ z, double *__restrict__ w,
+                                                            const double *__restrict__ V, int nv,
+                                                            double *__restrict__ parts) {
   double acc[NV + 1];
 #pragma unroll
   for (int t = 0; t <= NV; t++) acc[t] = 0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += stride) {
-    const double wp = w[p];
+  const long long N = g.N, stride = (long long)gridDim.x * blockDim.x;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
+    const double wp = apply_row64<NS>(g, coef, z, p);
+    w[p] = wp;
 #pragma unroll
-    for (int t = 0; t < NV; t++)
-      if (t < nv) acc[t] += V[(long long)t * n + p] * wp;
+    for (int t = 0; t < NV; t++) {
+      const double v = t < nv ? V[t * N + p] : 0.0;
+      acc[t] += v * wp;
+    }
     acc[NV] += wp * wp;
   }
-  for (int t = 0; t <= NV; t++) sh[t][threadIdx.x] = acc[t];
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-      for (int t = 0; t <= NV; t++) sh[t][threadIdx.x] += sh[t][threadIdx.x + s];
-    __syncthreads();
+  block_sums<NV>(acc, nv, parts);
+}
+
+// w -= sum_t h_t V_t, with <V_t, w> (t < nv) and <w, w> of the result.
+template <int NV>
+__global__ void __launch_bounds__(kKryThreads) k_update_dots(long long N, const double *__restrict__ V, int nv,
+                                                             const double *__restrict__ h, double *__restrict__ w,
+                                                             double *__restrict__ parts) {
+  double hr[NV], acc[NV + 1];
+#pragma unroll
+  for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
+#pragma unroll
+  for (int t = 0; t <= NV; t++) acc[t] = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
+    double v[NV];
+#pragma unroll
+    for (int t = 0; t < NV; t++) v[t] = t < nv ? V[t * N + p] : 0.0;
+    double s = w[p];
+#pragma unroll
+    for (int t = 0; t < NV; t++) s -= hr[t] * v[t];
+    w[p] = s;
+#pragma unroll
+    for (int t = 0; t < NV; t++) acc[t] += v[t] * s;
+    acc[NV] += s * s;
   }
-  if (threadIdx.x == 0) {
-    for (int t = 0; t < nv; t++) parts[(long long)t * gridDim.x + blockIdx.x] = sh[t][0];
-    parts[(long long)nv * gridDim.x + blockIdx.x] = sh[NV][0];
+  block_sums<NV>(acc, nv, parts);
+}
+
+// out = (w - sum_t h_t V_t) * scale.
+template <int NV>
+__global__ void __launch_bounds__(kKryThreads) k_update_scale(long long N, const double *__restrict__ V, int nv,
+                                                              const double *__restrict__ h,
+                                                              const double *__restrict__ w, double scale,
+                                                              double *__restrict__ out) {
+  double hr[NV];
+#pragma unroll
+  for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
+    double s = w[p];
+#pragma unroll
+    for (int t = 0; t < NV; t++) s -= hr[t] * (t < nv ? V[t * N + p] : 0.0);
+    out[p] = s * scale;
   }
+}
+
+// r = b - A x, with <r, r>.
+template <int NS>
+__global__ void __launch_bounds__(kKryThreads) k_residual(Grid g, const double *__restrict__ coef,
+                                                          const double *__restrict__ b, const double *__restrict__ x,
+                                                          double *__restrict__ r, double *__restrict__ parts) {
+  double acc[1] = {0};
+  const long long N = g.N, stride = (long long)gridDim.x * blockDim.x;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
+    const double v = b[p] - apply_row64<NS>(g, coef, x, p);
+    r[p] = v;
+    acc[0] += v * v;
+  }
+  block_sums<0>(acc, 0, parts);
 }
 
 __global__ void k_sum_rows(const double *parts, int nrows, int ncols, double *out) {
@@ -644,15 +363,6 @@ __global__ void k_sum_rows(const double *parts, int nrows, int ncols, double *ou
   if (threadIdx.x == 0) out[r] = sh[0];
 }
 
-// w -= sum_i h_i v_i
-__global__ void k_orth_update(long long n, const double *__restrict__ V, int nv, const double *__restrict__ h,
-                              double *__restrict__ w) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  double s = w[p];
-  for (int t = 0; t < nv; t++) s -= h[t] * V[(long long)t * n + p];
-  w[p] = s;
-}
 __global__ void k_scale_copy(long long n, const double *a, double s, double *b) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p < n) b[p] = a[p] * s;
@@ -666,34 +376,99 @@ __global__ void k_lincomb_add(long long n, const double *__restrict__ Z, int m, 
   for (int t = 0; t < m; t++) s += y[t] * Z[(long long)t * n + p];
   x[p] = s;
 }
-// r = b - y
-__global__ void k_sub(long long n, const double *b, const double *y, double *r) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p < n) r[p] = b[p] - y[p];
-}
 
 static const int kRedBlocks = 148 * 2;
 
-// Dots <V_t, w> for t < nv and <w, w>; results in c->red_host[0..nv].
-static int multidot(Ctx *c, const double *V, int nv, const double *w, double *out) {
+// Sums the block partials of rows 0..nrows-1 (left by one of the kernels above in
+// c->red) and copies them to out on the host.
+static int finish_rows(Ctx *c, int nrows, double *out) {
+  double *res = c->red + (long long)nrows * kKryBlocks;
+  k_sum_rows<<<nrows, 256, 0, c->stream>>>(c->red, nrows, kKryBlocks, res);
   int rc;
-  const long long n = c->g.N;
-  if ((rc = ensure_red(c, (nv + 1) * kRedBlocks + 64 + nv + 1))) return rc;
-  double *parts = c->red;
-  double *res = c->red + (nv + 1) * kRedBlocks;
-  if (nv <= 8) k_multidot<8><<<kRedBlocks, 128, 0, c->stream>>>(n, V, nv, w, parts);
-  else if (nv <= 16) k_multidot<16><<<kRedBlocks, 128, 0, c->stream>>>(n, V, nv, w, parts);
-  else if (nv <= 32) k_multidot<32><<<kRedBlocks, 128, 0, c->stream>>>(n, V, nv, w, parts);
-  else return set_err(c, VFS_ERR_INVALID, "FGMRES restart above 32 is not supported");
-  if ((rc = check_launch(c, "k_multidot"))) return rc;
-  k_sum_rows<<<nv + 1, 256, 0, c->stream>>>(parts, nv + 1, kRedBlocks, res);
   if ((rc = check_launch(c, "k_sum_rows"))) return rc;
-  cudaMemcpyAsync(c->red_host, res, sizeof(double) * (nv + 1), cudaMemcpyDeviceToHost, c->stream);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "multidot sync failed");
-  for (int t = 0; t <= nv; t++) out[t] = c->red_host[t];
+  cudaMemcpyAsync(c->red_host, res, sizeof(double) * nrows, cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "FGMRES reduction failed");
+  for (int t = 0; t < nrows; t++) out[t] = c->red_host[t];
   return VFS_OK;
 }
 
+template <int NS>
+static void launch_apply_dots(Ctx *c, const double *z, double *w, const double *V, int nv) {
+  const Grid &g = c->g;
+  const double *cf = c->ps.coef;
+  if (nv <= 4) k_apply_dots<NS, 4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
+  else if (nv <= 8) k_apply_dots<NS, 8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
+  else if (nv <= 16) k_apply_dots<NS, 16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
+  else k_apply_dots<NS, 32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
+}
+
+// w = A z; h[0..nv-1] = <V_t, w>; h[nv] = <w, w>.
+static int apply_dots(Ctx *c, const double *z, double *w, const double *V, int nv, double *h) {
+  if (c->ps.nslot == 7) launch_apply_dots<7>(c, z, w, V, nv);
+  else launch_apply_dots<NSLOT>(c, z, w, V, nv);
+  int rc;
+  if ((rc = check_launch(c, "k_apply_dots"))) return rc;
+  return finish_rows(c, nv + 1, h);
+}
+
+// w -= V h (h on the device); out[0..nv-1] = <V_t, w>; out[nv] = <w, w>.
+static int update_dots(Ctx *c, const double *V, int nv, const double *hdev, double *w, double *out) {
+  const long long N = c->g.N;
+  if (nv <= 4) k_update_dots<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
+  else if (nv <= 8) k_update_dots<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
+  else if (nv <= 16) k_update_dots<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
+  else k_update_dots<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
+  int rc;
+  if ((rc = check_launch(c, "k_update_dots"))) return rc;
+  return finish_rows(c, nv + 1, out);
+}
+
+// out = (w - V h) * scale (h on the device).
+static int update_scale(Ctx *c, const double *V, int nv, const double *hdev, const double *w, double scale,
+                        double *out) {
+  const long long N = c->g.N;
+  if (nv <= 4) k_update_scale<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
+  else if (nv <= 8) k_update_scale<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
+  else if (nv <= 16) k_update_scale<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
+  else k_update_scale<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
+  return check_launch(c, "k_update_scale");
+}
+
+// r = b - A x; returns ||r||.
+static int residual(Ctx *c, const double *b, const double *x, double *r, double *rnorm) {
+  if (c->ps.nslot == 7)
+    k_residual<7><<<kKryBlocks, kKryThreads, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
+  else
+    k_residual<NSLOT><<<kKryBlocks, kKryThreads, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
+  int rc;
+  if ((rc = check_launch(c, "k_residual"))) return rc;
+  double rr;
+  if ((rc = finish_rows(c, 1, &rr))) return rc;
+  *rnorm = sqrt(rr);
+  return VFS_OK;
+}
+
+// Copies h[0..n-1] to the device vector hdev (through the pinned staging buffer).
+static void upload_h(Ctx *c, const double *h, int n, double *hdev) {
+  for (int t = 0; t < n; t++) c->red_host[t] = h[t];
+  cudaMemcpyAsync(hdev, c->red_host, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+}
+
+// Number of non-zero cross-derivative slots (7..18) of the operator.
+__global__ void k_count_cross(long long N, const double *__restrict__ coef, double *parts) {
+  __shared__ double sh[256];
+  double s = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride)
+    for (int t = NE; t < NSLOT; t++) s += coef[t * N + p] != 0.0 ? 1.0 : 0.0;
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
+}
 
 // ------------------------------------------------------------------ LHS set-up
 __global__ void k_count_fluid(long long n, const uint8_t *fluid, const double *aj, double *parts) {
@@ -711,32 +486,6 @@ __global__ void k_count_fluid(long long n, const uint8_t *fluid, const double *a
   if (threadIdx.x == 0) { parts[blockIdx.x] = s1[0]; parts[gridDim.x + blockIdx.x] = s2[0]; }
 }
 
-static CL clevel(const Ctx *c, const MGLevel &L) {
-  CL r;
-  r.nx = L.nx; r.ny = L.ny; r.nz = L.nz; r.n = L.n;
-  r.ip = c->g.iper; r.jp = c->g.jper; r.kp = c->g.kper;
-  return r;
-}
-
-static void free_levels(Poisson &P) {
-  for (size_t l = 1; l < P.lv.size(); l++) {
-    MGLevel &L = P.lv[l];
-    cudaFree(L.op64); cudaFree(L.op32); cudaFree(L.x64); cudaFree(L.x32);
-  }
-  P.lv.clear();
-}
-
-static double gersh_max(Ctx *c) {
-  k_gersh_fine<<<kRedBlocks, 256, 0, c->stream>>>(c->g, c->ps.coef, c->ps.invdiag, c->ps.fluid, c->red);
-  check_launch(c, "k_gersh_fine");
-  std::vector<double> h(kRedBlocks);
-  cudaMemcpyAsync(h.data(), c->red, sizeof(double) * kRedBlocks, cudaMemcpyDeviceToHost, c->stream);
-  cudaStreamSynchronize(c->stream);
-  double m = 0;
-  for (double v : h) m = std::max(m, v);
-  return m;
-}
-
 int poisson_lhs(Ctx *c) {
   Poisson &P = c->ps;
   const Grid &g = c->g;
@@ -744,28 +493,17 @@ int poisson_lhs(Ctx *c) {
   int rc;
   if (!P.coef) {
     bool ok = cudaMalloc(&P.coef, sizeof(double) * NSLOT * N) == cudaSuccess;
-    ok &= cudaMalloc(&P.coef32, sizeof(float) * NSLOT * N) == cudaSuccess;
-    ok &= cudaMalloc(&P.invdiag, sizeof(double) * N) == cudaSuccess;
-    ok &= cudaMalloc(&P.invdiag32, sizeof(float) * N) == cudaSuccess;
     ok &= cudaMalloc(&P.fluid, N) == cudaSuccess;
-    ok &= cudaMalloc(&P.f32, sizeof(float) * N * 6) == cudaSuccess;
-    ok &= cudaMalloc(&P.f64, sizeof(double) * N * 6) == cudaSuccess;
     ok &= cudaMalloc(&P.w, sizeof(double) * N) == cudaSuccess;
     ok &= cudaMalloc(&P.r, sizeof(double) * N) == cudaSuccess;
     ok &= cudaMalloc(&P.t, sizeof(double) * N) == cudaSuccess;
     if (!ok) return set_err(c, VFS_ERR_CUDA, "poisson_lhs: allocation failed");
-    cudaMemsetAsync(P.f32, 0, sizeof(float) * N * 6, c->stream);
-    cudaMemsetAsync(P.f64, 0, sizeof(double) * N * 6, c->stream);
     cudaMemsetAsync(P.w, 0, sizeof(double) * N, c->stream);
     cudaMemsetAsync(P.r, 0, sizeof(double) * N, c->stream);
     cudaMemsetAsync(P.t, 0, sizeof(double) * N, c->stream);
   }
-  k_poisson_coef<<<nblocks(N, 128), 128, 0, c->stream>>>(g, metrics(c), c->nv, P.coef, P.fluid, P.invdiag);
+  k_poisson_coef<<<nblocks(N, 128), 128, 0, c->stream>>>(g, metrics(c), c->nv, P.coef, P.fluid);
   if ((rc = check_launch(c, "k_poisson_coef"))) return rc;
-  k_cast_d2f<<<nblocks(NSLOT * N, 256), 256, 0, c->stream>>>(NSLOT * N, P.coef, P.coef32);
-  if ((rc = check_launch(c, "k_cast_d2f"))) return rc;
-  k_cast_d2f<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.invdiag, P.invdiag32);
-  if ((rc = check_launch(c, "k_cast_d2f"))) return rc;
   // fluid-cell count and sum of aj (Remove_Nullspace / Remove_Nullspace_Scale)
   if ((rc = ensure_red(c, 2 * kRedBlocks + 64))) return rc;
   k_count_fluid<<<kRedBlocks, 256, 0, c->stream>>>(N, P.fluid, c->f[VFS_AJ][0], c->red);
@@ -775,188 +513,15 @@ int poisson_lhs(Ctx *c) {
   if ((rc = reduce_sum(c, c->red + kRedBlocks, kRedBlocks, &saj))) return rc;
   P.nfluid = (long long)llround(cnt);
   P.sum_aj = saj;
-  P.lmax0 = gersh_max(c);
-
-  // Multigrid hierarchy: coarsen by 2 while every interior dimension stays even.
-  free_levels(P);
-  MGLevel L0;
-  L0.nx = g.mx - 2; L0.ny = g.my - 2; L0.nz = g.mz - 2;
-  L0.n = N;
-  P.lv.push_back(L0);
-  const int maxlev = 8;
-  while ((int)P.lv.size() < maxlev) {
-    const MGLevel F = P.lv.back();
-    if (F.nx % 2 || F.ny % 2 || F.nz % 2 || F.nx < 4 || F.ny < 4 || F.nz < 4) break;
-    MGLevel L;
-    L.nx = F.nx / 2; L.ny = F.ny / 2; L.nz = F.nz / 2;
-    L.n = (long long)L.nx * L.ny * L.nz;
-    bool ok = cudaMalloc(&L.op64, sizeof(double) * L.n * 4) == cudaSuccess;
-    ok &= cudaMalloc(&L.op32, sizeof(float) * L.n * 4) == cudaSuccess;
-    ok &= cudaMalloc(&L.x64, sizeof(double) * L.n * 6) == cudaSuccess;
-    ok &= cudaMalloc(&L.x32, sizeof(float) * L.n * 6) == cudaSuccess;
-    if (!ok) return set_err(c, VFS_ERR_CUDA, "poisson_lhs: level allocation failed");
-    L.b64 = L.x64 + L.n; L.d64 = L.b64 + L.n; L.t64 = L.d64 + L.n;
-    L.b32 = L.x32 + L.n; L.d32 = L.b32 + L.n; L.t32 = L.d32 + L.n;
-    cudaMemsetAsync(L.x64, 0, sizeof(double) * L.n * 6, c->stream);
-    cudaMemsetAsync(L.x32, 0, sizeof(float) * L.n * 6, c->stream);
-    double *cx = L.op64, *cy = cx + L.n, *cz = cy + L.n, *dg = cz + L.n;
-    CL Lc = clevel(c, L);
-    if (P.lv.size() == 1) {
-      k_build_l1<<<nblocks(L.n, 128), 128, 0, c->stream>>>(g, Lc, P.coef, P.fluid, cx, cy, cz);
-    } else {
-      const double *f = F.op64;
-      k_build_coarse<<<nblocks(L.n, 128), 128, 0, c->stream>>>(clevel(c, F), Lc, f, f + F.n, f + 2 * F.n, cx, cy, cz);
-    }
-    if ((rc = check_launch(c, "k_build_level"))) return rc;
-    k_coarse_diag<<<nblocks(L.n, 128), 128, 0, c->stream>>>(Lc, cx, cy, cz, dg);
-    if ((rc = check_launch(c, "k_coarse_diag"))) return rc;
-    k_cast_d2f<<<nblocks(4 * L.n, 256), 256, 0, c->stream>>>(4 * L.n, L.op64, L.op32);
-    if ((rc = check_launch(c, "k_cast_d2f"))) return rc;
-    P.lv.push_back(L);
-  }
+  // the apply reads only slots CP..BP when no row has a cross-derivative entry
+  k_count_cross<<<kRedBlocks, 256, 0, c->stream>>>(N, P.coef, c->red);
+  if ((rc = check_launch(c, "k_count_cross"))) return rc;
+  double ncross = 0;
+  if ((rc = reduce_sum(c, c->red, kRedBlocks, &ncross))) return rc;
+  P.nslot = ncross == 0 ? 7 : NSLOT;
+  if ((rc = mg_setup(c))) return rc;
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "poisson_lhs failed");
   P.built = true;
-  return VFS_OK;
-}
-
-// ------------------------------------------------------------------ V-cycle
-// Chebyshev polynomial smoothing of D^-1 A on [lmin, lmax] (the classical three-term
-// recurrence): step coefficients c1 (momentum) and c2 (residual weight) per step.
-static void cheb_coeffs(double lmax, int steps, std::vector<double> &c1, std::vector<double> &c2) {
-  const double hi = 1.1 * lmax, lo = hi / 8.0;
-  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
-  const double sigma = theta / delta;
-  double rho = 1.0 / sigma;
-  c1.assign(steps, 0.0); c2.assign(steps, 0.0);
-  c1[0] = 0.0; c2[0] = 1.0 / theta;
-  for (int s = 1; s < steps; s++) {
-    const double rn = 1.0 / (2.0 * sigma - rho);
-    c1[s] = rn * rho;
-    c2[s] = 2.0 * rn / delta;
-    rho = rn;
-  }
-}
-
-template <typename T> struct LvPtr;
-template <> struct LvPtr<float> {
-  static float *x(MGLevel &L) { return L.x32; }
-  static float *b(MGLevel &L) { return L.b32; }
-  static float *d(MGLevel &L) { return L.d32; }
-  static float *t(MGLevel &L) { return L.t32; }
-  static const float *op(MGLevel &L) { return L.op32; }
-};
-template <> struct LvPtr<double> {
-  static double *x(MGLevel &L) { return L.x64; }
-  static double *b(MGLevel &L) { return L.b64; }
-  static double *d(MGLevel &L) { return L.d64; }
-  static double *t(MGLevel &L) { return L.t64; }
-  static const double *op(MGLevel &L) { return L.op64; }
-};
-
-template <typename T> struct FineOps;
-template <> struct FineOps<float> {
-  static const float *coef(Poisson &P) { return P.coef32; }
-  static const float *invd(Poisson &P) { return P.invdiag32; }
-  static float *work(Poisson &P) { return P.f32; }
-};
-template <> struct FineOps<double> {
-  static const double *coef(Poisson &P) { return P.coef; }
-  static const double *invd(Poisson &P) { return P.invdiag; }
-  static double *work(Poisson &P) { return P.f64; }
-};
-
-// Smoothing of level l: damped y-line Jacobi sweeps (omega = 0.8); x is updated in place
-// (ping-pong through t, the Thomas coefficients in the two scratch slots after it).
-static const double kLineOmega = 0.8;
-template <typename T>
-static int smooth(Ctx *c, int l, int steps, bool x_zero) {
-  Poisson &P = c->ps;
-  int rc;
-  if (l == 0) {
-    const long long N = c->g.N;
-    T *w = FineOps<T>::work(P);
-    T *b = w, *x = w + N, *xt = w + 2 * N, *cp = w + 4 * N, *dp = w + 5 * N;
-    const long long cols = (long long)(c->g.mx - 2) * (c->g.mz - 2);
-    for (int s = 0; s < steps; s++) {
-      const bool z = x_zero && s == 0;
-      k_yline_fine<T><<<nblocks(cols, 128), 128, 0, c->stream>>>(c->g, FineOps<T>::coef(P), P.fluid, b, x, xt, cp, dp,
-                                                                (T)kLineOmega, z ? 1 : 0);
-      if ((rc = check_launch(c, "k_yline_fine"))) return rc;
-      std::swap(x, xt);
-    }
-    if (x != w + N) cudaMemcpyAsync(w + N, x, sizeof(T) * N, cudaMemcpyDeviceToDevice, c->stream);
-    return VFS_OK;
-  }
-  MGLevel &L = P.lv[l];
-  CL cl = clevel(c, L);
-  const T *op = LvPtr<T>::op(L);
-  T *x = LvPtr<T>::x(L), *xt = LvPtr<T>::t(L);
-  T *cp = LvPtr<T>::x(L) + 4 * L.n, *dp = LvPtr<T>::x(L) + 5 * L.n;
-  const long long cols = (long long)L.nx * L.nz;
-  for (int s = 0; s < steps; s++) {
-    const bool z = x_zero && s == 0;
-    k_yline_coarse<T><<<nblocks(cols, 128), 128, 0, c->stream>>>(cl, op, op + L.n, op + 2 * L.n, op + 3 * L.n,
-                                                                LvPtr<T>::b(L), x, xt, cp, dp, (T)kLineOmega,
-                                                                z ? 1 : 0);
-    if ((rc = check_launch(c, "k_yline_coarse"))) return rc;
-    std::swap(x, xt);
-  }
-  if (x != LvPtr<T>::x(L)) cudaMemcpyAsync(LvPtr<T>::x(L), x, sizeof(T) * L.n, cudaMemcpyDeviceToDevice, c->stream);
-  return VFS_OK;
-}
-
-// V-cycle on level l for the right-hand side already in the level's b slot.
-template <typename T>
-static int vcycle(Ctx *c, int l, const vfs_solve_opts &o) {
-  Poisson &P = c->ps;
-  const int nl = std::min((int)P.lv.size(), o.levels);
-  int rc;
-  if (l == nl - 1) return smooth<T>(c, l, o.coarse_iters, true);
-  if ((rc = smooth<T>(c, l, o.pre_smooth, true))) return rc;
-  MGLevel &C = P.lv[l + 1];
-  CL cc = clevel(c, C);
-  if (l == 0) {
-    const long long N = c->g.N;
-    T *w = FineOps<T>::work(P);
-    k_restrict_fine<T><<<nblocks(C.n, 128), 128, 0, c->stream>>>(c->g, cc, FineOps<T>::coef(P), P.fluid, w, w + N,
-                                                                LvPtr<T>::b(C));
-  } else {
-    MGLevel &F = P.lv[l];
-    const T *op = LvPtr<T>::op(F);
-    k_restrict_coarse<T><<<nblocks(C.n, 128), 128, 0, c->stream>>>(clevel(c, F), cc, op, op + F.n, op + 2 * F.n,
-                                                                  op + 3 * F.n, LvPtr<T>::b(F), LvPtr<T>::x(F),
-                                                                  LvPtr<T>::b(C));
-  }
-  if ((rc = check_launch(c, "k_restrict"))) return rc;
-  if ((rc = vcycle<T>(c, l + 1, o))) return rc;
-  if (l == 0) {
-    T *w = FineOps<T>::work(P);
-    k_prolong_fine<T><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, cc, P.fluid, w + c->g.N, LvPtr<T>::x(C));
-  } else {
-    MGLevel &F = P.lv[l];
-    const T *op = LvPtr<T>::op(F);
-    k_prolong_coarse<T><<<nblocks(F.n, 256), 256, 0, c->stream>>>(clevel(c, F), cc, op + 3 * F.n, LvPtr<T>::x(F),
-                                                                  LvPtr<T>::x(C));
-  }
-  if ((rc = check_launch(c, "k_prolong"))) return rc;
-  return smooth<T>(c, l, o.post_smooth, false);
-}
-
-// z = M^-1 v (one V-cycle, FP32 or FP64), v and z on the grid layout in FP64.
-static int precondition(Ctx *c, const double *v, double *z, const vfs_solve_opts &o) {
-  Poisson &P = c->ps;
-  const long long N = c->g.N;
-  int rc;
-  if (o.precision == 0) {
-    k_cast_d2f<<<nblocks(N, 256), 256, 0, c->stream>>>(N, v, P.f32);
-    if ((rc = check_launch(c, "k_cast_d2f"))) return rc;
-    if ((rc = vcycle<float>(c, 0, o))) return rc;
-    k_cast_f2d<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.f32 + N, z);
-    return check_launch(c, "k_cast_f2d");
-  }
-  cudaMemcpyAsync(P.f64, v, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream);
-  if ((rc = vcycle<double>(c, 0, o))) return rc;
-  cudaMemcpyAsync(z, P.f64 + N, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream);
   return VFS_OK;
 }
 
@@ -1080,7 +645,7 @@ int poisson_rhs(Ctx *c) {
 int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   vfs_solve_opts o;
   memset(&o, 0, sizeof(o));
-  o.precision = 0; o.restart = 30; o.max_iter = 200; o.levels = 4; o.pre_smooth = 2; o.post_smooth = 2;
+  o.precision = 0; o.restart = 30; o.max_iter = 200; o.levels = 0; o.pre_smooth = 2; o.post_smooth = 2;
   o.coarse_iters = 16; o.rtol = 1e-10; o.atol = 0.0;
   if (oin) {
     o.precision = oin->precision;
@@ -1093,7 +658,9 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
     if (oin->rtol > 0) o.rtol = oin->rtol;
     if (oin->atol > 0) o.atol = oin->atol;
   }
-  if (o.restart > 32) o.restart = 32;
+  if (o.restart > 31) o.restart = 31;
+  if (o.pre_smooth < 1) o.pre_smooth = 1;
+  if (o.coarse_iters < 1) o.coarse_iters = 1;
   Poisson &P = c->ps;
   const long long N = c->g.N;
   int rc;
@@ -1105,34 +672,29 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       return set_err(c, VFS_ERR_CUDA, "poisson_solve: Krylov basis allocation failed");
     P.restart = o.restart;
   }
+  if (!P.hdev && cudaMalloc(&P.hdev, sizeof(double) * 64) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "poisson_solve: allocation failed");
+  if ((rc = ensure_red(c, 34 * kKryBlocks + 64))) return rc;
   cudaEventRecord(c->ev0, c->stream);
   double *x = c->f[VFS_PHI][0];
   const double *b = c->f[VFS_B][0];
   cudaMemsetAsync(x, 0, sizeof(double) * N, c->stream);
   const int m = o.restart;
   std::vector<double> H((m + 1) * m), cs(m), sn(m), gv(m + 1), y(m), h(m + 2), h2(m + 2);
-  double bnorm = 0;
-  {
-    double dd[1];
-    if ((rc = multidot(c, nullptr, 0, b, dd))) return rc;
-    bnorm = sqrt(dd[0]);
-  }
   vfs_solve_stats s;
   memset(&s, 0, sizeof(s));
+  double rnorm = 0;
+  if ((rc = residual(c, b, x, P.r, &rnorm))) return rc;  // x = 0: r = b
+  const double bnorm = rnorm;
   s.r0 = bnorm;
   const double tol = std::max(o.rtol * bnorm, o.atol);
   int it = 0;
   bool conv = bnorm <= tol;
-  double rnorm = bnorm;
+  bool fresh = true;  // P.r holds b - A x for the current x
   while (!conv && it < o.max_iter) {
-    // r = b - A x
-    if ((rc = poisson_apply_dev(c, x, P.t))) return rc;
-    k_sub<<<nblocks(N, 256), 256, 0, c->stream>>>(N, b, P.t, P.r);
-    if ((rc = check_launch(c, "k_sub"))) return rc;
-    double rr[1];
-    if ((rc = multidot(c, nullptr, 0, P.r, rr))) return rc;
-    double beta = sqrt(rr[0]);
-    rnorm = beta;
+    if (!fresh && (rc = residual(c, b, x, P.r, &rnorm))) return rc;
+    fresh = false;
+    const double beta = rnorm;
     if (beta <= tol) { conv = true; break; }
     k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.r, 1.0 / beta, P.V);
     if ((rc = check_launch(c, "k_scale_copy"))) return rc;
@@ -1140,27 +702,35 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
     gv[0] = beta;
     int jdone = 0;
     for (int j = 0; j < m && it < o.max_iter; j++) {
+      const int nv = j + 1;
       double *Vj = P.V + (long long)j * N, *Zj = P.Z + (long long)j * N;
-      if ((rc = precondition(c, Vj, Zj, o))) return rc;
-      if ((rc = poisson_apply_dev(c, Zj, P.w))) return rc;
-      // CGS with one re-orthogonalisation pass
-      if ((rc = multidot(c, P.V, j + 1, P.w, h.data()))) return rc;
-      cudaMemcpyAsync(c->red + 8, h.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, c->stream);
-      k_orth_update<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.V, j + 1, c->red + 8, P.w);
-      if ((rc = check_launch(c, "k_orth_update"))) return rc;
-      if ((rc = multidot(c, P.V, j + 1, P.w, h2.data()))) return rc;
-      cudaMemcpyAsync(c->red + 8, h2.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, c->stream);
-      k_orth_update<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.V, j + 1, c->red + 8, P.w);
-      if ((rc = check_launch(c, "k_orth_update"))) return rc;
-      double nn[1];
-      if ((rc = multidot(c, nullptr, 0, P.w, nn))) return rc;
-      for (int t = 0; t <= j; t++) H[t * m + j] = h[t] + h2[t];
-      const double hn = sqrt(nn[0]);
-      H[(j + 1) * m + j] = hn;
-      if (hn > 0) {
-        k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, 1.0 / hn, P.V + (long long)(j + 1) * N);
-        if ((rc = check_launch(c, "k_scale_copy"))) return rc;
+      if ((rc = mg_precondition(c, Vj, Zj, o))) return rc;
+      // classical Gram-Schmidt with one re-orthogonalisation, three passes over V:
+      // (1) w = A z_j and h = V^T w; (2) w -= V h and h2 = V^T w; (3) v_{j+1} = (w - V h2)/|.|
+      if ((rc = apply_dots(c, Zj, P.w, P.V, nv, h.data()))) return rc;
+      upload_h(c, h.data(), nv, P.hdev);
+      if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h2.data()))) return rc;
+      double ww = h2[nv], proj = 0;
+      for (int t = 0; t < nv; t++) proj += h2[t] * h2[t];
+      double hn2 = ww - proj;  // |w - V h2|^2 for orthonormal V
+      upload_h(c, h2.data(), nv, P.hdev);
+      for (int t = 0; t < nv; t++) H[t * m + j] = h[t] + h2[t];
+      double hn;
+      double *Vn = P.V + (long long)(j + 1) * N;
+      if (hn2 > 1e-4 * ww) {
+        hn = sqrt(hn2);
+        if ((rc = update_scale(c, P.V, nv, P.hdev, P.w, 1.0 / hn, Vn))) return rc;
+      } else {
+        // w is nearly in span(V): form w - V h2 explicitly and take its norm
+        std::vector<double> h3(nv + 1);
+        if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h3.data()))) return rc;
+        hn = sqrt(std::max(h3[nv], 0.0));
+        if (hn > 0) {
+          k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, 1.0 / hn, Vn);
+          if ((rc = check_launch(c, "k_scale_copy"))) return rc;
+        }
       }
+      H[(j + 1) * m + j] = hn;
       // Givens rotations
       for (int t = 0; t < j; t++) {
         const double a = H[t * m + j], bb = H[(t + 1) * m + j];
@@ -1186,17 +756,13 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       for (int u = t + 1; u < jdone; u++) sum -= H[t * m + u] * y[u];
       y[t] = sum / H[t * m + t];
     }
-    cudaMemcpyAsync(c->red + 8, y.data(), sizeof(double) * jdone, cudaMemcpyHostToDevice, c->stream);
-    k_lincomb_add<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.Z, jdone, c->red + 8, x);
+    upload_h(c, y.data(), jdone, P.hdev);
+    k_lincomb_add<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.Z, jdone, P.hdev, x);
     if ((rc = check_launch(c, "k_lincomb_add"))) return rc;
     if (rnorm <= tol) {
       // confirm with the true residual
-      if ((rc = poisson_apply_dev(c, x, P.t))) return rc;
-      k_sub<<<nblocks(N, 256), 256, 0, c->stream>>>(N, b, P.t, P.r);
-      if ((rc = check_launch(c, "k_sub"))) return rc;
-      double r2[1];
-      if ((rc = multidot(c, nullptr, 0, P.r, r2))) return rc;
-      rnorm = sqrt(r2[0]);
+      if ((rc = residual(c, b, x, P.r, &rnorm))) return rc;
+      fresh = true;
       conv = rnorm <= tol * 1.0000001 || rnorm <= 2 * tol;
     }
   }
@@ -1403,22 +969,11 @@ int run_kernel(Ctx *c, int which, int reps) {
       case 1: extern void launch_fp(Ctx *); launch_fp(c); break;
       case 2: extern void launch_rhs(Ctx *); launch_rhs(c); break;
       case 3:
-        k_apply64<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, P.coef, P.fluid, c->f[VFS_PHI][0], P.t);
+        rc = poisson_apply_dev(c, c->f[VFS_PHI][0], P.t);
+        if (rc) return rc;
         break;
-      case 4: {
-        float *w = P.f32;
-        const long long cols = (long long)(g.mx - 2) * (g.mz - 2);
-        k_yline_fine<float><<<nblocks(cols, 128), 128, 0, c->stream>>>(g, P.coef32, P.fluid, w, w + g.N, w + 2 * g.N,
-                                                                      w + 4 * g.N, w + 5 * g.N, 0.8f, 0);
-        break;
-      }
-      case 5: {
-        double *w = P.f64;
-        const long long cols = (long long)(g.mx - 2) * (g.mz - 2);
-        k_yline_fine<double><<<nblocks(cols, 128), 128, 0, c->stream>>>(g, P.coef, P.fluid, w, w + g.N, w + 2 * g.N,
-                                                                       w + 4 * g.N, w + 5 * g.N, 0.8, 0);
-        break;
-      }
+      case 4: rc = mg_sweep_fine(c, 0); if (rc) return rc; break;
+      case 5: rc = mg_sweep_fine(c, 1); if (rc) return rc; break;
       case 6:
         k_projection<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->f[VFS_PHI][0], field3(c, VFS_UCONT));
         break;

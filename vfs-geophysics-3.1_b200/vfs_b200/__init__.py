@@ -182,10 +182,15 @@ class Context:
             raise ValueError("field %d: expected %d values, got %d" % (field, want, a.size))
         self._check(self.lib.vfs_set_field(self.h, field, a.ctypes.data))
 
-    def get_field(self, field):
+    def get_field(self, field, out=None):
+        """Field in the reference layout; written into `out` (C-contiguous float64 of the
+        field's shape, e.g. pinned memory) when given."""
         dof = FIELD_DOF[field]
         shape = self.shape + ((3,) if dof == 3 else ())
-        out = np.empty(shape, dtype=np.float64)
+        if out is None:
+            out = np.empty(shape, dtype=np.float64)
+        elif out.shape != shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("get_field: out must be C-contiguous float64 of shape %s" % (shape,))
         self._check(self.lib.vfs_get_field(self.h, field, out.ctypes.data))
         return out
 
@@ -267,7 +272,7 @@ class Context:
         self._check(self.lib.vfs_poisson_apply(self.h, x.ctypes.data, y.ctypes.data))
         return y
 
-    def poisson_solve(self, precision=0, rtol=1e-10, restart=30, max_iter=200, levels=4,
+    def poisson_solve(self, precision=0, rtol=1e-10, restart=30, max_iter=200, levels=0,
                       pre_smooth=2, post_smooth=2, coarse_iters=16, allow_unconverged=False):
         o = SolveOpts(precision=precision, restart=restart, max_iter=max_iter, levels=levels,
                       pre_smooth=pre_smooth, post_smooth=post_smooth, coarse_iters=coarse_iters,
@@ -290,7 +295,7 @@ class Context:
 
     def step(self, precision=0, rtol=1e-10, **kw):  # Flow_Solver, solvers.c:562 (implicit=0)
         o = SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
-                      max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 4),
+                      max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 0),
                       pre_smooth=kw.get("pre_smooth", 2), post_smooth=kw.get("post_smooth", 2),
                       coarse_iters=kw.get("coarse_iters", 16))
         st = StepStats()
