@@ -85,8 +85,9 @@ struct MGLevel {
   ZL z;
   bool zebra = true;        // two-colour line Gauss-Seidel is race-free on this level
   double *op64 = nullptr;   // 6n: couplings +i, +j, +k, diagonal, Thomas factors cpr, 1/pivot
-  float *op32 = nullptr;    // FP32 copy
-  double *v64 = nullptr;    // 4n: x, b, previous x (line Jacobi), forward-elimination scratch
+  double *pk64 = nullptr;   // 8n: packed operator (two 4-vectors per cell), FP64
+  float *pk32 = nullptr;    // the same in FP32
+  double *v64 = nullptr;    // 5n: x, b, previous x (line Jacobi), forward-elimination pairs (2n)
   float *v32 = nullptr;
 };
 

@@ -157,9 +157,42 @@ __global__ void k_mg_thomas(ZL L, double *__restrict__ op) {
   }
 }
 
-__global__ void k_mg_cast(long long n, const double *__restrict__ a, float *__restrict__ b) {
-  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p < n) b[p] = (float)a[p];
+// ------------------------------------------------------------------ packed operator
+// The smoother and the transfers read the operator as two 4-vectors per cell, so a
+// row costs two vector loads: cpl = {ce, cw, ct, cb} (couplings to i+1, i-1, k+1, k-1)
+// and tri = {cs, iden, cpr, dg} (coupling to j-1, Thomas pivot inverse and factor,
+// diagonal).  A missing neighbour has a zero coupling; cs at j = 0 is the periodic
+// wrap coupling when j is periodic, else 0.
+template <typename T>
+struct __align__(4 * sizeof(T)) Q4 {
+  T a, b, c, d;
+};
+template <typename T>
+struct __align__(2 * sizeof(T)) Q2 {
+  T a, b;
+};
+
+template <typename T>
+__global__ void k_mg_pack(ZL L, const double *__restrict__ op, Q4<T> *__restrict__ cpl, Q4<T> *__restrict__ tri) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long ncell = (long long)L.nx * L.ny * L.nz;
+  if (t >= ncell) return;
+  const int i = (int)(t % L.nx);
+  const long long r = t / L.nx;
+  const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+  const long long q = zidx(L, i, j, k), n = L.n;
+  const ZNb nb = znb(L, i, j, k);
+  Q4<T> a, b;
+  a.a = (T)op[OP_CE * n + q];
+  a.b = nb.iw >= 0 ? (T)op[OP_CE * n + zidx(L, nb.iw, j, k)] : T(0);
+  a.c = (T)op[OP_CT * n + q];
+  a.d = nb.kb >= 0 ? (T)op[OP_CT * n + zidx(L, i, j, nb.kb)] : T(0);
+  b.a = nb.js >= 0 ? (T)op[OP_CN * n + zidx(L, i, nb.js, k)] : T(0);
+  b.b = (T)op[OP_IDEN * n + q];
+  b.c = (T)op[OP_CPR * n + q];
+  b.d = (T)op[OP_DG * n + q];
+  cpl[q] = a;
+  tri[q] = b;
 }
 
 // ------------------------------------------------------------------ smoother
@@ -167,13 +200,15 @@ __global__ void k_mg_cast(long long n, const double *__restrict__ a, float *__re
 // written for this one), or, with colour < 0, one damped line-Jacobi sweep over all
 // columns (neighbours read from xr = the previous iterate, a separate array).
 // x_zero: the neighbours read are known to be zero (first pass from a zero guess).
-// The forward elimination stores d'_j in ds; the back substitution writes x.
-template <typename T>
-__global__ void __launch_bounds__(64) k_zline(ZL L, const T *__restrict__ op, const T *__restrict__ b,
-                                              const T *__restrict__ xr, T *__restrict__ ds, T *__restrict__ xw,
-                                              int colour, T omega, int x_zero) {
+// The forward elimination stores (d'_j, cpr_j) in ds; the back substitution writes x.
+// Rows are processed in chunks of CH: every load of a chunk is issued before the
+// recurrence consumes the first one, so a column keeps CH rows of loads in flight.
+template <typename T, int CH>
+__device__ __forceinline__ void zline_column(const ZL &L, const Q4<T> *__restrict__ cpl, const Q4<T> *__restrict__ tri,
+                                             const T *__restrict__ b, const T *__restrict__ xr,
+                                             Q2<T> *__restrict__ ds, T *__restrict__ xw, int colour, T omega,
+                                             int x_zero, long long t) {
   const int hx = L.hx;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   int c, h, k;
   if (colour >= 0) {
     if (t >= (long long)L.nz * hx) return;
@@ -184,96 +219,256 @@ __global__ void __launch_bounds__(64) k_zline(ZL L, const T *__restrict__ op, co
   }
   const int i = 2 * h + (c ^ (k & 1));
   if (i >= L.nx) return;
-  const long long n = L.n;
   const ZNb nb = znb(L, i, 0, k);
   const long long p0 = zidx(L, i, 0, k);
   // offsets of the neighbour columns (constant along j).  A missing neighbour (domain
-  // edge) borrows the offset of the opposite one with a zero weight, so every x read
-  // is of the other colour (every level has at least 2 cells along i and k).
-  const T me = nb.ie >= 0 ? T(1) : T(0), mw = nb.iw >= 0 ? T(1) : T(0);
-  const T mt = nb.kt >= 0 ? T(1) : T(0), mb = nb.kb >= 0 ? T(1) : T(0);
+  // edge, zero coupling) borrows the offset of the opposite one, so every x read is of
+  // the other colour (every level has at least 2 cells along i and k).
   const long long oe = zidx(L, nb.ie >= 0 ? nb.ie : nb.iw, 0, k) - p0;
   const long long ow = zidx(L, nb.iw >= 0 ? nb.iw : nb.ie, 0, k) - p0;
   const long long ot = zidx(L, i, 0, nb.kt >= 0 ? nb.kt : nb.kb) - p0;
   const long long ob = zidx(L, i, 0, nb.kb >= 0 ? nb.kb : nb.kt) - p0;
   const long long sj = 2LL * hx;
-  const T *__restrict__ ce = op + OP_CE * n;
-  const T *__restrict__ cn = op + OP_CN * n;
-  const T *__restrict__ ct = op + OP_CT * n;
-  const T *__restrict__ cpr = op + OP_CPR * n;
-  const T *__restrict__ idn = op + OP_IDEN * n;
   const int ny = L.ny;
-  T dprev = 0, lower = 0;
-  if (x_zero) {
-#pragma unroll 8
-    for (int j = 0; j < ny; j++) {
-      const long long q = p0 + j * sj;
-      const T d = (b[q] - lower * dprev) * idn[q];
-      lower = cn[q];
-      ds[q] = d;
-      dprev = d;
-    }
-  } else {
-    const T *__restrict__ xs = colour >= 0 ? xw : xr;  // own column (periodic j only)
-#pragma unroll 8
-    for (int j = 0; j < ny; j++) {
-      const long long q = p0 + j * sj;
-      T r = b[q];
-      r -= me * ce[q] * xr[q + oe];
-      r -= mw * ce[q + ow] * xr[q + ow];
-      r -= mt * ct[q] * xr[q + ot];
-      r -= mb * ct[q + ob] * xr[q + ob];
-      if (L.jp) {
-        if (j == 0) r -= cn[p0 + (ny - 1) * sj] * xs[p0 + (ny - 1) * sj];
-        if (j == ny - 1) r -= cn[q] * xs[p0];
+  // periodic j: the wrap coupling and the far end of the own column (old values)
+  T wrap_c = 0, x_first = 0, x_last = 0;
+  if (L.jp && !x_zero) {
+    const T *__restrict__ xs = colour >= 0 ? xw : xr;
+    wrap_c = tri[p0].a;
+    x_first = xs[p0];
+    x_last = xs[p0 + (ny - 1) * sj];
+  }
+  T dprev = 0;
+  for (int j0 = 0; j0 < ny; j0 += CH) {
+    T bb[CH], xe[CH], xwv[CH], xt[CH], xb[CH];
+    Q4<T> cp[CH], tr[CH];
+#pragma unroll
+    for (int u = 0; u < CH; u++) {
+      const int j = j0 + u;
+      if (j < ny) {
+        const long long q = p0 + j * sj;
+        bb[u] = b[q];
+        tr[u] = tri[q];
+        if (!x_zero) {
+          cp[u] = cpl[q];
+          xe[u] = xr[q + oe];
+          xwv[u] = xr[q + ow];
+          xt[u] = xr[q + ot];
+          xb[u] = xr[q + ob];
+        }
       }
-      const T d = (r - lower * dprev) * idn[q];
-      lower = cn[q];
-      ds[q] = d;
-      dprev = d;
+    }
+#pragma unroll
+    for (int u = 0; u < CH; u++) {
+      const int j = j0 + u;
+      if (j < ny) {
+        T r = bb[u];
+        if (!x_zero) {
+          r -= cp[u].a * xe[u];
+          r -= cp[u].b * xwv[u];
+          r -= cp[u].c * xt[u];
+          r -= cp[u].d * xb[u];
+          if (L.jp) {
+            if (j == 0) r -= wrap_c * x_last;
+            if (j == ny - 1) r -= wrap_c * x_first;
+          }
+        }
+        const T lower = j > 0 ? tr[u].a : T(0);
+        const T d = (r - lower * dprev) * tr[u].b;
+        Q2<T> o;
+        o.a = d; o.b = tr[u].c;
+        ds[p0 + j * sj] = o;
+        dprev = d;
+      }
     }
   }
   T xnext = 0;
-  if (colour >= 0) {
-#pragma unroll 8
-    for (int j = ny - 1; j >= 0; j--) {
-      const long long q = p0 + j * sj;
-      const T v = ds[q] - cpr[q] * xnext;
-      xnext = v;
-      xw[q] = v;
+  for (int j1 = ny - 1; j1 >= 0; j1 -= CH) {
+    Q2<T> dd[CH];
+    T xo[CH];
+#pragma unroll
+    for (int u = 0; u < CH; u++) {
+      const int j = j1 - u;
+      if (j >= 0) {
+        dd[u] = ds[p0 + j * sj];
+        if (colour < 0 && !x_zero) xo[u] = xr[p0 + j * sj];
+      }
     }
-  } else {
-#pragma unroll 8
-    for (int j = ny - 1; j >= 0; j--) {
-      const long long q = p0 + j * sj;
-      const T v = ds[q] - cpr[q] * xnext;
-      xnext = v;
-      xw[q] = x_zero ? omega * v : xr[q] + omega * (v - xr[q]);
+#pragma unroll
+    for (int u = 0; u < CH; u++) {
+      const int j = j1 - u;
+      if (j >= 0) {
+        const T v = dd[u].a - dd[u].b * xnext;
+        xnext = v;
+        T out = v;
+        if (colour < 0) out = x_zero ? omega * v : xo[u] + omega * (v - xo[u]);
+        xw[p0 + j * sj] = out;
+      }
     }
   }
 }
 
+template <typename T> struct ZChunk;
+template <> struct ZChunk<float> { static constexpr int v = 8; };
+template <> struct ZChunk<double> { static constexpr int v = 4; };
+
+template <typename T>
+__global__ void __launch_bounds__(64) k_zline(ZL L, const Q4<T> *__restrict__ cpl, const Q4<T> *__restrict__ tri,
+                                              const T *__restrict__ b, const T *__restrict__ xr,
+                                              Q2<T> *__restrict__ ds, T *__restrict__ xw, int colour, T omega,
+                                              int x_zero) {
+  zline_column<T, ZChunk<T>::v>(L, cpl, tri, b, xr, ds, xw, colour, omega, x_zero,
+                                blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+
+// Tiled zebra colour pass for the large levels.  One thread block owns W columns of
+// one colour that are consecutive in memory (same k, half-row positions h0..h0+W-1):
+//   A. all threads load the tile's rows (coalesced across the W columns, many loads in
+//      flight) and form each row's scaled right-hand side r' = r / pivot, the scaled
+//      lower coupling m = lower / pivot and the Thomas factor cpr, in shared memory;
+//   B. each warp solves whole columns: the forward elimination d_j = r'_j - m_j d_{j-1}
+//      and the back substitution x_j = d_j - cpr_j x_{j+1} are first-order linear
+//      recurrences, evaluated as warp scans (each lane composes its run of rows, a
+//      5-step shuffle scan combines the lanes, each lane then replays its rows);
+//   C. all threads write the tile's x back, coalesced.
+// Shared memory: 3 * W * P values of T, P = ny rounded up to odd (conflict-free rows).
+constexpr int kTileThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ void scan_compose_up(T &A, T &B, int lane) {
+  // inclusive scan over lanes 0..lane of x -> A x + B maps (later lanes applied last)
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T pa = __shfl_up_sync(0xffffffffu, A, off), pb = __shfl_up_sync(0xffffffffu, B, off);
+    if (lane >= off) { B = A * pb + B; A = A * pa; }
+  }
+}
+template <typename T>
+__device__ __forceinline__ void scan_compose_down(T &A, T &B, int lane) {
+  // inclusive scan over lanes lane..31 (higher lanes applied first)
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const T pa = __shfl_down_sync(0xffffffffu, A, off), pb = __shfl_down_sync(0xffffffffu, B, off);
+    if (lane + off < 32) { B = A * pb + B; A = A * pa; }
+  }
+}
+
+template <typename T, int W>
+__global__ void __launch_bounds__(kTileThreads) k_zline_tile(ZL L, const Q4<T> *__restrict__ cpl,
+                                                             const Q4<T> *__restrict__ tri, const T *__restrict__ b,
+                                                             const T *__restrict__ xr, T *__restrict__ xw, int colour,
+                                                             int x_zero) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int hx = L.hx, ny = L.ny;
+  const int P = ny | 1;
+  T *sr = reinterpret_cast<T *>(smem_raw);  // [W][P]: r', then d, then x
+  T *sm = sr + W * P;                        // [W][P]: m
+  T *sc = sm + W * P;                        // [W][P]: cpr
+  const int tiles_per_row = (hx + W - 1) / W;
+  const int k = blockIdx.x / tiles_per_row;
+  const int h0 = (blockIdx.x % tiles_per_row) * W;
+  if (k >= L.nz) return;
+  const long long sj = 2LL * hx;
+  // A
+  for (int e = threadIdx.x; e < ny * W; e += blockDim.x) {
+    const int j = e / W, w = e - (e / W) * W;
+    const int h = h0 + w;
+    const int i = 2 * h + (colour ^ (k & 1));
+    T rr = 0, mm = 0, cc = 0;
+    if (h < hx && i < L.nx) {
+      const long long q = zidx(L, i, j, k);
+      const Q4<T> tr = tri[q];
+      T r = b[q];
+      if (!x_zero) {
+        const ZNb nb = znb(L, i, j, k);
+        const Q4<T> cp = cpl[q];
+        // a missing neighbour has a zero coupling; read the opposite one instead
+        const int ie = nb.ie >= 0 ? nb.ie : nb.iw, iw = nb.iw >= 0 ? nb.iw : nb.ie;
+        const int kt = nb.kt >= 0 ? nb.kt : nb.kb, kb = nb.kb >= 0 ? nb.kb : nb.kt;
+        r -= cp.a * xr[zidx(L, ie, j, k)];
+        r -= cp.b * xr[zidx(L, iw, j, k)];
+        r -= cp.c * xr[zidx(L, i, j, kt)];
+        r -= cp.d * xr[zidx(L, i, j, kb)];
+        if (L.jp) {
+          const long long p0 = q - j * sj;
+          if (j == 0) r -= tr.a * xw[p0 + (ny - 1) * sj];
+          if (j == ny - 1) r -= tri[p0].a * xw[p0];
+        }
+      }
+      rr = r * tr.b;
+      mm = j > 0 ? tr.a * tr.b : T(0);
+      cc = tr.c;
+    }
+    sr[w * P + j] = rr;
+    sm[w * P + j] = mm;
+    sc[w * P + j] = cc;
+  }
+  __syncthreads();
+  // B
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int seg = (ny + 31) >> 5;
+  const int j0 = lane * seg, j1 = min(ny, j0 + seg);
+  for (int w = warp; w < W; w += nwarp) {
+    T *cr = sr + w * P;
+    const T *cm = sm + w * P, *cx = sc + w * P;
+    // forward: d_j = -m_j d_{j-1} + r'_j
+    T A = 1, B = 0;
+    for (int j = j0; j < j1; j++) { const T mj = cm[j]; B = -mj * B + cr[j]; A = -mj * A; }
+    scan_compose_up<T>(A, B, lane);
+    T d = __shfl_up_sync(0xffffffffu, B, 1);
+    if (lane == 0) d = 0;
+    for (int j = j0; j < j1; j++) { d = -cm[j] * d + cr[j]; cr[j] = d; }
+    __syncwarp();
+    // backward: x_j = -cpr_j x_{j+1} + d_j
+    A = 1; B = 0;
+    for (int j = j1 - 1; j >= j0; j--) { const T cj = cx[j]; B = -cj * B + cr[j]; A = -cj * A; }
+    scan_compose_down<T>(A, B, lane);
+    T x = __shfl_down_sync(0xffffffffu, B, 1);
+    if (lane == 31) x = 0;
+    for (int j = j1 - 1; j >= j0; j--) { x = -cx[j] * x + cr[j]; cr[j] = x; }
+    __syncwarp();
+  }
+  __syncthreads();
+  // C
+  for (int e = threadIdx.x; e < ny * W; e += blockDim.x) {
+    const int j = e / W, w = e - (e / W) * W;
+    const int h = h0 + w;
+    const int i = 2 * h + (colour ^ (k & 1));
+    if (h < hx && i < L.nx) xw[zidx(L, i, j, k)] = sr[w * P + j];
+  }
+}
+
+template <typename T, int W>
+static size_t tile_smem(int ny) {
+  return (size_t)3 * W * (ny | 1) * sizeof(T);
+}
+template <typename T, int W>
+static bool tile_fits(int ny) {
+  return tile_smem<T, W>(ny) <= 200 * 1024;
+}
+
 // Residual b - A x at one cell of a level.
 template <typename T>
-__device__ __forceinline__ T zresid(const ZL &L, const T *__restrict__ op, const T *__restrict__ x,
-                                    const T *__restrict__ b, int i, int j, int k, long long q) {
-  const long long n = L.n;
+__device__ __forceinline__ T zresid(const ZL &L, const Q4<T> *__restrict__ cpl, const Q4<T> *__restrict__ tri,
+                                    const T *__restrict__ x, const T *__restrict__ b, int i, int j, int k,
+                                    long long q) {
   const ZNb nb = znb(L, i, j, k);
-  T ax = op[OP_DG * n + q] * x[q];
-  if (nb.ie >= 0) ax += op[OP_CE * n + q] * x[zidx(L, nb.ie, j, k)];
-  if (nb.iw >= 0) { const long long w = zidx(L, nb.iw, j, k); ax += op[OP_CE * n + w] * x[w]; }
-  if (nb.jn >= 0) ax += op[OP_CN * n + q] * x[zidx(L, i, nb.jn, k)];
-  if (nb.js >= 0) { const long long s = zidx(L, i, nb.js, k); ax += op[OP_CN * n + s] * x[s]; }
-  if (nb.kt >= 0) ax += op[OP_CT * n + q] * x[zidx(L, i, j, nb.kt)];
-  if (nb.kb >= 0) { const long long s = zidx(L, i, j, nb.kb); ax += op[OP_CT * n + s] * x[s]; }
+  const Q4<T> cp = cpl[q], tr = tri[q];
+  T ax = tr.d * x[q];
+  if (nb.ie >= 0) ax += cp.a * x[zidx(L, nb.ie, j, k)];
+  if (nb.iw >= 0) ax += cp.b * x[zidx(L, nb.iw, j, k)];
+  if (nb.js >= 0) ax += tr.a * x[zidx(L, i, nb.js, k)];
+  if (nb.jn >= 0) { const long long s = zidx(L, i, nb.jn, k); ax += tri[s].a * x[s]; }
+  if (nb.kt >= 0) ax += cp.c * x[zidx(L, i, j, nb.kt)];
+  if (nb.kb >= 0) ax += cp.d * x[zidx(L, i, j, nb.kb)];
   return b[q] - ax;
 }
 
 // Coarse right-hand side: the sum of the residuals of the (active) children.
 template <typename T>
-__global__ void k_zrestrict(ZL F, ZL C, const T *__restrict__ opF, const T *__restrict__ x, const T *__restrict__ b,
-                            T *__restrict__ bc) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void zrestrict_cell(const ZL &F, const ZL &C, const Q4<T> *__restrict__ cpl,
+                                              const Q4<T> *__restrict__ tri, const T *__restrict__ x,
+                                              const T *__restrict__ b, T *__restrict__ bc, long long t) {
   const long long ncell = (long long)C.nx * C.ny * C.nz;
   if (t >= ncell) return;
   const int I = (int)(t % C.nx);
@@ -285,24 +480,30 @@ __global__ void k_zrestrict(ZL F, ZL C, const T *__restrict__ opF, const T *__re
       for (int a = 0; a < 2; a++) {
         const int i = 2 * I + a, j = 2 * J + bb, k = 2 * K + c;
         const long long q = zidx(F, i, j, k);
-        if (opF[OP_DG * F.n + q] == T(0)) continue;
-        s += zresid<T>(F, opF, x, b, i, j, k, q);
+        if (tri[q].d == T(0)) continue;
+        s += zresid<T>(F, cpl, tri, x, b, i, j, k, q);
       }
   bc[zidx(C, I, J, K)] = s;
 }
 
+template <typename T>
+__global__ void k_zrestrict(ZL F, ZL C, const Q4<T> *__restrict__ cpl, const Q4<T> *__restrict__ tri,
+                            const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ bc) {
+  zrestrict_cell<T>(F, C, cpl, tri, x, b, bc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+
 // x_fine += P x_coarse (cell-centred trilinear).
 template <typename T>
-__global__ void k_zprolong(ZL F, ZL C, const T *__restrict__ opF, const T *__restrict__ opC, T *__restrict__ x,
-                           const T *__restrict__ xc) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void zprolong_cell(const ZL &F, const ZL &C, const Q4<T> *__restrict__ triF,
+                                             const Q4<T> *__restrict__ triC, T *__restrict__ x,
+                                             const T *__restrict__ xc, long long t) {
   const long long ncell = (long long)F.nx * F.ny * F.nz;
   if (t >= ncell) return;
   const int i = (int)(t % F.nx);
   const long long r = t / F.nx;
   const int j = (int)(r % F.ny), k = (int)(r / F.ny);
   const long long q = zidx(F, i, j, k);
-  if (opF[OP_DG * F.n + q] == T(0)) return;
+  if (triF[q].d == T(0)) return;
   const int I = i >> 1, J = j >> 1, K = k >> 1;
   // the other coarse cell nearest along each direction, or -1
   int In = I + ((i & 1) ? 1 : -1), Jn = J + ((j & 1) ? 1 : -1), Kn = K + ((k & 1) ? 1 : -1);
@@ -310,7 +511,6 @@ __global__ void k_zprolong(ZL F, ZL C, const T *__restrict__ opF, const T *__res
   if (Jn < 0 || Jn >= C.ny) Jn = C.jp ? (Jn + C.ny) % C.ny : -1;
   if (Kn < 0 || Kn >= C.nz) Kn = C.kp ? (Kn + C.nz) % C.nz : -1;
   const long long own = zidx(C, I, J, K);
-  const T *__restrict__ dgC = opC + OP_DG * C.n;
   T wown = T(27) / T(64);
   T s = 0;
   for (int c = 0; c < 2; c++)
@@ -321,10 +521,84 @@ __global__ void k_zprolong(ZL F, ZL C, const T *__restrict__ opF, const T *__res
         const int ii = a ? In : I, jj = bb ? Jn : J, kk = c ? Kn : K;
         if (ii < 0 || jj < 0 || kk < 0) { wown += w; continue; }
         const long long qc = zidx(C, ii, jj, kk);
-        if (dgC[qc] == T(0)) { wown += w; continue; }
+        if (triC[qc].d == T(0)) { wown += w; continue; }
         s += w * xc[qc];
       }
   x[q] += s + wown * xc[own];
+}
+
+template <typename T>
+__global__ void k_zprolong(ZL F, ZL C, const Q4<T> *__restrict__ triF, const Q4<T> *__restrict__ triC,
+                           T *__restrict__ x, const T *__restrict__ xc) {
+  zprolong_cell<T>(F, C, triF, triC, x, xc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+
+// ------------------------------------------------------------------ bottom of the V-cycle
+// The coarse levels are too small to fill the GPU, and a launch per colour pass costs
+// more than the work.  From the first level of at most kBottomCells cells down, one
+// thread block runs the rest of the V-cycle (smoothing, restriction, coarsest sweeps,
+// prolongation) with block barriers between the phases; the level data stay in L2.
+constexpr int kBottomMaxLevels = 12;
+constexpr int kBottomThreads = 512;
+constexpr long long kBottomCells = 32768;
+
+template <typename T>
+struct BLevel {
+  ZL z;
+  const Q4<T> *cpl, *tri;
+  T *x, *b, *xo;
+  Q2<T> *ds;
+  int zebra;
+};
+template <typename T>
+struct Bottom {
+  int nl;
+  int pre, post, coarse;
+  T omega;
+  BLevel<T> lv[kBottomMaxLevels];
+};
+
+template <typename T>
+__device__ void blk_smooth(const BLevel<T> &L, int sweeps, bool x_zero, T omega) {
+  const long long half = (long long)L.z.nz * L.z.hx;
+  for (int s = 0; s < sweeps; s++) {
+    const bool z = x_zero && s == 0;
+    if (L.zebra) {
+      for (int col = 0; col < 2; col++) {
+        for (long long t = threadIdx.x; t < half; t += blockDim.x)
+          zline_column<T, 2>(L.z, L.cpl, L.tri, L.b, L.x, L.ds, L.x, col, T(1), (z && col == 0) ? 1 : 0, t);
+        __syncthreads();
+      }
+    } else {
+      if (!z) {
+        for (long long t = threadIdx.x; t < L.z.n; t += blockDim.x) L.xo[t] = L.x[t];
+        __syncthreads();
+      }
+      for (long long t = threadIdx.x; t < 2 * half; t += blockDim.x)
+        zline_column<T, 2>(L.z, L.cpl, L.tri, L.b, L.xo, L.ds, L.x, -1, omega, z ? 1 : 0, t);
+      __syncthreads();
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBottomThreads) k_mg_bottom(Bottom<T> B) {
+  for (int l = 0; l < B.nl - 1; l++) {
+    const BLevel<T> &F = B.lv[l], &C = B.lv[l + 1];
+    blk_smooth<T>(F, B.pre, true, B.omega);
+    const long long nc = (long long)C.z.nx * C.z.ny * C.z.nz;
+    for (long long t = threadIdx.x; t < nc; t += blockDim.x)
+      zrestrict_cell<T>(F.z, C.z, F.cpl, F.tri, F.x, F.b, C.b, t);
+    __syncthreads();
+  }
+  blk_smooth<T>(B.lv[B.nl - 1], B.coarse, true, B.omega);
+  for (int l = B.nl - 2; l >= 0; l--) {
+    const BLevel<T> &F = B.lv[l], &C = B.lv[l + 1];
+    const long long nf = (long long)F.z.nx * F.z.ny * F.z.nz;
+    for (long long t = threadIdx.x; t < nf; t += blockDim.x) zprolong_cell<T>(F.z, C.z, F.tri, C.tri, F.x, C.x, t);
+    __syncthreads();
+    blk_smooth<T>(F, B.post, false, B.omega);
+  }
 }
 
 // DA-layout FP64 vector -> finest-level right-hand side.
@@ -366,11 +640,13 @@ static ZL make_zl(int nx, int ny, int nz, const Grid &g) {
 
 void mg_free(Poisson &P) {
   for (MGLevel &L : P.lv) {
-    cudaFree(L.op64); cudaFree(L.op32); cudaFree(L.v64); cudaFree(L.v32);
+    cudaFree(L.op64); cudaFree(L.pk64); cudaFree(L.pk32); cudaFree(L.v64); cudaFree(L.v32);
   }
   P.lv.clear();
 }
 
+// Per level: raw FP64 couplings and Thomas factors (op64, used to build the next level),
+// the packed FP64 and FP32 operators, and the work vectors x | b | xo | ds (2n).
 int mg_setup(Ctx *c) {
   Poisson &P = c->ps;
   const Grid &g = c->g;
@@ -384,16 +660,19 @@ int mg_setup(Ctx *c) {
     L.zebra = !((L.z.ip && (nx & 1)) || (L.z.kp && (nz & 1)));
     const long long n = L.z.n;
     bool ok = cudaMalloc(&L.op64, sizeof(double) * NOP * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.op32, sizeof(float) * NOP * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.v64, sizeof(double) * 4 * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.v32, sizeof(float) * 4 * n) == cudaSuccess;
+    ok &= cudaMalloc(&L.pk64, sizeof(double) * 8 * n) == cudaSuccess;
+    ok &= cudaMalloc(&L.pk32, sizeof(float) * 8 * n) == cudaSuccess;
+    ok &= cudaMalloc(&L.v64, sizeof(double) * 5 * n) == cudaSuccess;
+    ok &= cudaMalloc(&L.v32, sizeof(float) * 5 * n) == cudaSuccess;
     if (!ok) {
       P.lv.push_back(L);
       return set_err(c, VFS_ERR_CUDA, "poisson_lhs: multigrid allocation failed");
     }
     cudaMemsetAsync(L.op64, 0, sizeof(double) * NOP * n, c->stream);
-    cudaMemsetAsync(L.v64, 0, sizeof(double) * 4 * n, c->stream);
-    cudaMemsetAsync(L.v32, 0, sizeof(float) * 4 * n, c->stream);
+    cudaMemsetAsync(L.pk64, 0, sizeof(double) * 8 * n, c->stream);
+    cudaMemsetAsync(L.pk32, 0, sizeof(float) * 8 * n, c->stream);
+    cudaMemsetAsync(L.v64, 0, sizeof(double) * 5 * n, c->stream);
+    cudaMemsetAsync(L.v32, 0, sizeof(float) * 5 * n, c->stream);
     const long long ncell = (long long)nx * ny * nz;
     if (P.lv.empty()) {
       k_mg_fine_couplings<<<nblocks(ncell, 128), 128, 0, c->stream>>>(g, L.z, P.coef, P.fluid, L.op64);
@@ -404,7 +683,10 @@ int mg_setup(Ctx *c) {
     if ((rc = check_launch(c, "k_mg_couplings"))) { P.lv.push_back(L); return rc; }
     k_mg_diag<<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64);
     k_mg_thomas<<<nblocks((long long)nx * nz, 64), 64, 0, c->stream>>>(L.z, L.op64);
-    k_mg_cast<<<nblocks(NOP * n, 256), 256, 0, c->stream>>>(NOP * n, L.op64, L.op32);
+    k_mg_pack<double><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<double> *)L.pk64,
+                                                                 (Q4<double> *)L.pk64 + n);
+    k_mg_pack<float><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<float> *)L.pk32,
+                                                                (Q4<float> *)L.pk32 + n);
     P.lv.push_back(L);
     if ((rc = check_launch(c, "k_mg_setup"))) return rc;
     if ((nx & 1) || (ny & 1) || (nz & 1) || nx < 4 || ny < 4 || nz < 4) break;
@@ -413,51 +695,114 @@ int mg_setup(Ctx *c) {
   return VFS_OK;
 }
 
-template <typename T> struct MGp;
-template <> struct MGp<float> {
-  static const float *op(const MGLevel &L) { return L.op32; }
-  static float *v(const MGLevel &L) { return L.v32; }
+// Typed views of a level's packed operator and work vectors.
+template <typename T>
+struct LvT {
+  const Q4<T> *cpl, *tri;
+  T *x, *b, *xo;
+  Q2<T> *ds;
 };
-template <> struct MGp<double> {
-  static const double *op(const MGLevel &L) { return L.op64; }
-  static double *v(const MGLevel &L) { return L.v64; }
-};
+template <typename T>
+static LvT<T> lvt(const MGLevel &L);
+template <>
+LvT<float> lvt<float>(const MGLevel &L) {
+  const long long n = L.z.n;
+  LvT<float> r;
+  r.cpl = (const Q4<float> *)L.pk32; r.tri = (const Q4<float> *)L.pk32 + n;
+  r.x = L.v32; r.b = L.v32 + n; r.xo = L.v32 + 2 * n; r.ds = (Q2<float> *)(L.v32 + 3 * n);
+  return r;
+}
+template <>
+LvT<double> lvt<double>(const MGLevel &L) {
+  const long long n = L.z.n;
+  LvT<double> r;
+  r.cpl = (const Q4<double> *)L.pk64; r.tri = (const Q4<double> *)L.pk64 + n;
+  r.x = L.v64; r.b = L.v64 + n; r.xo = L.v64 + 2 * n; r.ds = (Q2<double> *)(L.v64 + 3 * n);
+  return r;
+}
 
 static const double kJacobiOmega = 0.8;
+
+// Launches one tiled colour pass; false when the level's columns do not fit the tile.
+template <typename T, int W>
+static bool launch_tile_w(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour, int x_zero) {
+  if (!tile_fits<T, W>(L.z.ny)) return false;
+  const size_t smem = tile_smem<T, W>(L.z.ny);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_zline_tile<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  const int tiles = (L.z.hx + W - 1) / W;
+  k_zline_tile<T, W><<<tiles * L.z.nz, kTileThreads, smem, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.x, v.x, colour,
+                                                                        x_zero);
+  return true;
+}
+template <typename T>
+static bool launch_zline_tile(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour, int x_zero) {
+  if (sizeof(T) == 4) return launch_tile_w<T, 32>(c, L, v, colour, x_zero) || launch_tile_w<T, 8>(c, L, v, colour, x_zero);
+  return launch_tile_w<T, 16>(c, L, v, colour, x_zero) || launch_tile_w<T, 8>(c, L, v, colour, x_zero);
+}
 
 // `sweeps` smoothing sweeps on level l; x_zero: x is taken as zero on entry.
 template <typename T>
 static int mg_smooth(Ctx *c, int l, int sweeps, bool x_zero) {
   const MGLevel &L = c->ps.lv[l];
-  const long long n = L.z.n;
-  const T *op = MGp<T>::op(L);
-  T *x = MGp<T>::v(L), *b = x + n, *xo = x + 2 * n, *ds = x + 3 * n;
+  const LvT<T> v = lvt<T>(L);
   const long long half = (long long)L.z.nz * L.z.hx;
   for (int s = 0; s < sweeps; s++) {
     const bool z = x_zero && s == 0;
     if (L.zebra) {
-      for (int col = 0; col < 2; col++)
-        k_zline<T><<<nblocks(half, 64), 64, 0, c->stream>>>(L.z, op, b, x, ds, x, col, T(1), (z && col == 0) ? 1 : 0);
+      for (int col = 0; col < 2; col++) {
+        const int xz = (z && col == 0) ? 1 : 0;
+        if (!launch_zline_tile<T>(c, L, v, col, xz))
+          k_zline<T><<<nblocks(half, 64), 64, 0, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.x, v.ds, v.x, col, T(1), xz);
+      }
     } else {
-      if (!z) cudaMemcpyAsync(xo, x, sizeof(T) * n, cudaMemcpyDeviceToDevice, c->stream);
-      k_zline<T><<<nblocks(2 * half, 64), 64, 0, c->stream>>>(L.z, op, b, xo, ds, x, -1, T(kJacobiOmega), z ? 1 : 0);
+      if (!z) cudaMemcpyAsync(v.xo, v.x, sizeof(T) * L.z.n, cudaMemcpyDeviceToDevice, c->stream);
+      k_zline<T><<<nblocks(2 * half, 64), 64, 0, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.xo, v.ds, v.x, -1,
+                                                               T(kJacobiOmega), z ? 1 : 0);
     }
   }
   return check_launch(c, "k_zline");
 }
 
 template <typename T>
+static int mg_bottom(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
+  Bottom<T> B;
+  B.nl = nl - l;
+  if (B.nl > kBottomMaxLevels) return set_err(c, VFS_ERR_INVALID, "multigrid: too many levels");
+  B.pre = o.pre_smooth; B.post = o.post_smooth; B.coarse = o.coarse_iters;
+  B.omega = T(kJacobiOmega);
+  for (int q = 0; q < B.nl; q++) {
+    const MGLevel &L = c->ps.lv[l + q];
+    const LvT<T> v = lvt<T>(L);
+    BLevel<T> &d = B.lv[q];
+    d.z = L.z;
+    d.cpl = v.cpl; d.tri = v.tri;
+    d.x = v.x; d.b = v.b; d.xo = v.xo; d.ds = v.ds;
+    d.zebra = L.zebra ? 1 : 0;
+  }
+  k_mg_bottom<T><<<1, kBottomThreads, 0, c->stream>>>(B);
+  return check_launch(c, "k_mg_bottom");
+}
+
+// V-cycle from level l (its right-hand side already in place); levels at or below
+// kBottomCells run inside one thread block.
+template <typename T>
 static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   int rc;
+  const MGLevel &Lv = c->ps.lv[l];
+  if ((long long)Lv.z.nx * Lv.z.ny * Lv.z.nz <= kBottomCells) return mg_bottom<T>(c, l, nl, o);
   if (l == nl - 1) return mg_smooth<T>(c, l, o.coarse_iters, true);
   if ((rc = mg_smooth<T>(c, l, o.pre_smooth, true))) return rc;
   const MGLevel &F = c->ps.lv[l], &C = c->ps.lv[l + 1];
   const long long nc = (long long)C.z.nx * C.z.ny * C.z.nz, nf = (long long)F.z.nx * F.z.ny * F.z.nz;
-  T *xf = MGp<T>::v(F), *xc = MGp<T>::v(C);
-  k_zrestrict<T><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, MGp<T>::op(F), xf, xf + F.z.n, xc + C.z.n);
+  const LvT<T> f = lvt<T>(F), cc = lvt<T>(C);
+  k_zrestrict<T><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
   if ((rc = check_launch(c, "k_zrestrict"))) return rc;
   if ((rc = mg_vcycle<T>(c, l + 1, nl, o))) return rc;
-  k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, MGp<T>::op(F), MGp<T>::op(C), xf, xc);
+  k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, f.tri, cc.tri, f.x, cc.x);
   if ((rc = check_launch(c, "k_zprolong"))) return rc;
   return mg_smooth<T>(c, l, o.post_smooth, false);
 }
@@ -467,13 +812,13 @@ static int mg_apply(Ctx *c, const double *v, double *z, const vfs_solve_opts &o)
   Poisson &P = c->ps;
   const MGLevel &L0 = P.lv[0];
   const long long ncell = (long long)L0.z.nx * L0.z.ny * L0.z.nz;
-  T *x0 = MGp<T>::v(L0);
+  const LvT<T> l0 = lvt<T>(L0);
   int rc;
-  k_to_zebra<T><<<nblocks(ncell, 256), 256, 0, c->stream>>>(c->g, L0.z, v, x0 + L0.z.n);
+  k_to_zebra<T><<<nblocks(ncell, 256), 256, 0, c->stream>>>(c->g, L0.z, v, l0.b);
   if ((rc = check_launch(c, "k_to_zebra"))) return rc;
   const int nl = o.levels > 0 ? std::min((int)P.lv.size(), o.levels) : (int)P.lv.size();
   if ((rc = mg_vcycle<T>(c, 0, nl, o))) return rc;
-  k_from_zebra<T><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, L0.z, P.fluid, x0, z);
+  k_from_zebra<T><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, L0.z, P.fluid, l0.x, z);
   return check_launch(c, "k_from_zebra");
 }
 

@@ -20,29 +20,46 @@ __device__ __forceinline__ double dot3(double ax, double ay, double az, double b
 // periodic image (all flagged directions at once), as the reference's copy loops do
 // (e.g. momentum.c:641-669, rhs.c:161-181).  Sources are never flagged points, so the
 // copy is order independent.
+// One thread per point of the ghost planes of the periodic directions (points on two such
+// planes appear twice and write the same value); each takes the value of its periodic
+// image, whose indices are all interior or non-periodic ghosts, so no thread reads a
+// point another one writes.
 __global__ void k_periodic_copy(Grid g, double *a, double *b, double *c) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
-  int ii = wrapi(g, i), jj = wrapj(g, j), kk = wrapk(g, k);
-  if (ii == i && jj == j && kk == k) return;
-  long long s = lidx(g, ii, jj, kk);
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long ni = g.iper ? 2LL * g.my * g.mz : 0, nj = g.jper ? 2LL * g.mx * g.mz : 0;
+  const long long nk = g.kper ? 2LL * g.mx * g.my : 0;
+  int i, j, k;
+  if (t < ni) {
+    const long long r = t >> 1;
+    i = (t & 1) ? g.mx - 1 : 0; j = (int)(r % g.my); k = (int)(r / g.my);
+  } else if ((t -= ni) < nj) {
+    const long long r = t >> 1;
+    j = (t & 1) ? g.my - 1 : 0; i = (int)(r % g.mx); k = (int)(r / g.mx);
+  } else if ((t -= nj) < nk) {
+    const long long r = t >> 1;
+    k = (t & 1) ? g.mz - 1 : 0; i = (int)(r % g.mx); j = (int)(r / g.mx);
+  } else {
+    return;
+  }
+  const long long p = lidx(g, i, j, k);
+  const long long s = lidx(g, wrapi(g, i), wrapj(g, j), wrapk(g, k));
   a[p] = a[s];
   if (b) b[p] = b[s];
   if (c) c[p] = c[s];
 }
 
+static long long ghost_points(const Grid &g) {
+  return (g.iper ? 2LL * g.my * g.mz : 0) + (g.jper ? 2LL * g.mx * g.mz : 0) + (g.kper ? 2LL * g.mx * g.my : 0);
+}
+
 int periodic_copy3(Ctx *c, V3 v) {
   if (!(c->g.iper || c->g.jper || c->g.kper)) return VFS_OK;
-  k_periodic_copy<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
+  k_periodic_copy<<<nblocks(ghost_points(c->g), 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
   return check_launch(c, "k_periodic_copy");
 }
 int periodic_copy1(Ctx *c, double *s) {
   if (!(c->g.iper || c->g.jper || c->g.kper)) return VFS_OK;
-  k_periodic_copy<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, s, nullptr, nullptr);
+  k_periodic_copy<<<nblocks(ghost_points(c->g), 256), 256, 0, c->stream>>>(c->g, s, nullptr, nullptr);
   return check_launch(c, "k_periodic_copy");
 }
 
@@ -123,12 +140,16 @@ __global__ void k_contra2cart_bc(Grid g, Metrics m, const uint8_t *__restrict__ 
   const long long sx = 1, sy = mx, sz = (long long)mx * my;
   const int *bc = g.bc;
   bool w = false;
-  double v[3] = {lu.x[p], lu.y[p], lu.z[p]};
   if (nv[p] == 3) {  // (int)(nvert+0.1)==3 and fixed bodies (rhs.c:296-299)
     out.x[p] = 0; out.y[p] = 0; out.z[p] = 0;
     flag[p] = 1;
     return;
   }
+  // every rule below acts on a ghost point or on a cell (1 or mx-2, 1, k)
+  if (!(i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == mz - 1 ||
+        (j == 1 && (i == 1 || i == mx - 2))))
+    return;
+  double v[3] = {lu.x[p], lu.y[p], lu.z[p]};
   int solid_flag = 0;
   if (bc[3] == 13 && j == my - 1) {
     v[0] = lu.x[p - sy]; v[2] = lu.z[p - sy]; v[1] = -lu.y[p - sy]; w = true;

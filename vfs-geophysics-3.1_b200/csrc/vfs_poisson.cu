@@ -209,9 +209,12 @@ __device__ __forceinline__ long long nb_index(const Grid &g, int i, int j, int k
 template <int NS>
 __device__ __forceinline__ double apply_row64(const Grid &g, const double *__restrict__ coef,
                                               const double *__restrict__ x, long long p) {
-  const int i = (int)(p % g.mx);
-  const long long q = p / g.mx;
-  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  // 32-bit index arithmetic (grids below 2^31 points)
+  const unsigned up = (unsigned)p, umx = (unsigned)g.mx, umy = (unsigned)g.my;
+  const unsigned q = up / umx;
+  const int i = (int)(up - q * umx);
+  const unsigned kk = q / umy;
+  const int j = (int)(q - kk * umy), k = (int)kk;
   double s = 0;
 #pragma unroll
   for (int t = 0; t < NS; t++) {
@@ -277,13 +280,13 @@ __global__ void __launch_bounds__(kKryThreads) k_apply_dots(Grid g, const double
   for (int t = 0; t <= NV; t++) acc[t] = 0;
   const long long N = g.N, stride = (long long)gridDim.x * blockDim.x;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
+    double v[NV];
+#pragma unroll
+    for (int t = 0; t < NV; t++) v[t] = t < nv ? V[t * N + p] : 0.0;
     const double wp = apply_row64<NS>(g, coef, z, p);
     w[p] = wp;
 #pragma unroll
-    for (int t = 0; t < NV; t++) {
-      const double v = t < nv ? V[t * N + p] : 0.0;
-      acc[t] += v * wp;
-    }
+    for (int t = 0; t < NV; t++) acc[t] += v[t] * wp;
     acc[NV] += wp * wp;
   }
   block_sums<NV>(acc, nv, parts);
@@ -326,9 +329,12 @@ __global__ void __launch_bounds__(kKryThreads) k_update_scale(long long N, const
   for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
+    double v[NV];
+#pragma unroll
+    for (int t = 0; t < NV; t++) v[t] = t < nv ? V[t * N + p] : 0.0;
     double s = w[p];
 #pragma unroll
-    for (int t = 0; t < NV; t++) s -= hr[t] * (t < nv ? V[t * N + p] : 0.0);
+    for (int t = 0; t < NV; t++) s -= hr[t] * v[t];
     out[p] = s * scale;
   }
 }
