@@ -91,7 +91,7 @@ typedef struct {
   int levels;        /* multigrid levels including the finest (default 0: every level
                         the grid coarsens to) */
   int pre_smooth, post_smooth; /* zebra line Gauss-Seidel sweeps per level (default 2, 2) */
-  int coarse_iters;  /* sweeps on the coarsest level (default 16) */
+  int coarse_iters;  /* sweeps on the coarsest level (default 4) */
   int reserved[5];
   double rtol;       /* relative residual target (default 1e-10) */
   double atol;       /* absolute residual target (default 0) */
@@ -240,9 +240,11 @@ int vfs_contra2cart_noalloc(const vfs_config *cfg, double *ucont, const double *
 int vfs_get_stream(vfs_ctx *ctx, void **stream);
 
 /* Launch one kernel of the path `reps` times on the context's stream without a host
- * synchronisation, on the context's current fields: 0 face fluxes of Formfunction_2,
- * 1 Fp, 2 RHS projection, 3 FP64 Poisson operator apply, 4 FP32 fine-level y-line
- * smoothing sweep, 5 FP64 fine-level y-line sweep, 6 Projection.  For timing only. */
+ * synchronisation, on the context's current fields: 0 face fluxes of Formfunction_2
+ * (three-kernel form), 1 its Fp, 2 its RHS projection, 3 FP64 Poisson operator apply,
+ * 4 FP32 fine-level zebra line sweep (both colours), 5 the same in FP64, 6 Projection,
+ * 7 Formfunction_2 as one fused kernel, 8 Formfunction_2 as a step runs it (kernels
+ * 0-2).  Kernels 7 and 8 add into RHS as vfs_formfunction2 does.  For timing only. */
 int vfs_run_kernel(vfs_ctx *ctx, int which, int reps);
 
 #ifdef __cplusplus

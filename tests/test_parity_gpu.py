@@ -222,3 +222,20 @@ def test_form_metrics_bitwise(name):
         got = ctx.get_field(fid)
         np.testing.assert_array_equal(got, want, err_msg=key)
     R.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_fused_formfunction2_matches_three_kernel_form(name):
+    """The single-kernel Formfunction_2 (diagnostic id 7) against the form a step runs
+    (id 8): same inputs, identical right-hand sides."""
+    case, (R, ctx) = _pair(name)
+    ctx.contra2cart()
+    rhs0 = np.random.Generator(np.random.Philox(9)).standard_normal(R.shape + (3,))
+    ctx.set_field(vfs.RHS, rhs0)
+    ctx.run_kernel(8, 1)
+    want = ctx.get_field(vfs.RHS)
+    ctx.set_field(vfs.RHS, rhs0)
+    ctx.run_kernel(7, 1)
+    np.testing.assert_array_equal(ctx.get_field(vfs.RHS), want)
+    R.close()

@@ -218,6 +218,7 @@ int vfs_destroy(vfs_ctx *ctx) {
     for (int q = 0; q < 3; q++) if (c->f[f][q]) cudaFree(c->f[f][q]);
   if (c->nv) cudaFree(c->nv);
   if (c->bcflag) cudaFree(c->bcflag);
+  if (c->solid) cudaFree(c->solid);
   for (int d = 0; d < 3; d++)
     for (int q = 0; q < 3; q++) { cudaFree(c->div[d][q]); cudaFree(c->visc[d][q]); }
   for (int q = 0; q < 3; q++) { cudaFree(c->fp[q]); cudaFree(c->pucont[q]); cudaFree(c->bcbuf[q]); }
@@ -277,6 +278,7 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
     cudaStreamSynchronize(c->stream);
     if (!rc && hbad) rc = set_err(c, VFS_ERR_INVALID, "vfs_set_field: nvert must hold integers 0..255");
     c->nvert_set = true;
+    c->nsolid = -1;
     c->ps.built = false;
     return rc;
   }

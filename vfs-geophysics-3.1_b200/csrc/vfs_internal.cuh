@@ -87,6 +87,7 @@ struct MGLevel {
   double *op64 = nullptr;   // 6n: couplings +i, +j, +k, diagonal, Thomas factors cpr, 1/pivot
   double *pk64 = nullptr;   // 8n: packed operator (two 4-vectors per cell), FP64
   float *pk32 = nullptr;    // the same in FP32
+  uint8_t *act = nullptr;   // n: 1 for an active unknown (non-zero diagonal)
   double *v64 = nullptr;    // 5n: x, b, previous x (line Jacobi), forward-elimination pairs (2n)
   float *v32 = nullptr;
 };
@@ -101,8 +102,9 @@ struct Poisson {
   std::vector<MGLevel> lv;  // multigrid levels, finest first
   // FGMRES workspace (grid layout, N doubles each)
   int restart = 0;
-  double *V = nullptr;      // (restart+1) * N
-  double *Z = nullptr;      // restart * N
+  long long ldv = 0;        // distance between basis vectors (N rounded up to 32)
+  double *V = nullptr;      // (restart+1) * ldv
+  double *Z = nullptr;      // restart * ldv
   double *w = nullptr, *r = nullptr, *t = nullptr;
   double *hdev = nullptr;   // Gram-Schmidt coefficients on the device (64 doubles)
 };
@@ -126,6 +128,8 @@ struct Ctx {
   double *pucont[3] = {};
   double *bcbuf[3] = {};        // Contra2Cart boundary two-phase buffer
   uint8_t *bcflag = nullptr;    // points written by the boundary phase
+  long long *solid = nullptr;   // indices of the solid (nvert 3) points
+  long long nsolid = -1;        // their number; -1 until built for the current nvert
   // reductions
   double *red = nullptr;        // partial sums (device)
   double *red_host = nullptr;   // pinned host mirror
@@ -150,7 +154,9 @@ inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / 
 int periodic_copy3(Ctx *c, V3 v);
 int periodic_copy1(Ctx *c, double *s);
 int contra2cart(Ctx *c);
+int solid_list(Ctx *c);
 int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff);
+int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff);
 int pressure_gradient(Ctx *c);
 int calc_k_flux(Ctx *c, double *flux);
 int runge_kutta(Ctx *c);

@@ -39,8 +39,20 @@ namespace vfs {
 
 enum { OP_CE = 0, OP_CN, OP_CT, OP_DG, OP_CPR, OP_IDEN, NOP };
 
+// 32-bit index arithmetic: mg_setup refuses levels of 2^31 slots or more.
 __host__ __device__ inline long long zidx(const ZL &L, int i, int j, int k) {
-  return (((long long)k * L.ny + j) * 2 + ((i ^ k) & 1)) * L.hx + (i >> 1);
+  return (long long)((((unsigned)k * (unsigned)L.ny + (unsigned)j) * 2u + (unsigned)((i ^ k) & 1)) * (unsigned)L.hx +
+                     (unsigned)(i >> 1));
+}
+
+// Cell (i, j, k) of a level from its natural index t = (k*ny + j)*nx + i.
+__device__ __forceinline__ void zcell(const ZL &L, long long t, int &i, int &j, int &k) {
+  const unsigned ut = (unsigned)t, nx = (unsigned)L.nx, ny = (unsigned)L.ny;
+  const unsigned r = ut / nx;
+  i = (int)(ut - r * nx);
+  const unsigned kk = r / ny;
+  j = (int)(r - kk * ny);
+  k = (int)kk;
 }
 
 // ------------------------------------------------------------------ set-up (FP64)
@@ -369,39 +381,67 @@ __global__ void __launch_bounds__(kTileThreads) k_zline_tile(ZL L, const Q4<T> *
   const int h0 = (blockIdx.x % tiles_per_row) * W;
   if (k >= L.nz) return;
   const long long sj = 2LL * hx;
-  // A
-  for (int e = threadIdx.x; e < ny * W; e += blockDim.x) {
-    const int j = e / W, w = e - (e / W) * W;
+  // A: the block size is a multiple of W, so each thread keeps one column and takes
+  // every (blockDim/W)-th row; U rows are loaded before any of them is used.
+  {
+    constexpr int U = sizeof(T) == 4 ? 6 : 3;
+    const int w = threadIdx.x % W, jstep = blockDim.x / W;
     const int h = h0 + w;
     const int i = 2 * h + (colour ^ (k & 1));
-    T rr = 0, mm = 0, cc = 0;
-    if (h < hx && i < L.nx) {
-      const long long q = zidx(L, i, j, k);
-      const Q4<T> tr = tri[q];
-      T r = b[q];
-      if (!x_zero) {
-        const ZNb nb = znb(L, i, j, k);
-        const Q4<T> cp = cpl[q];
-        // a missing neighbour has a zero coupling; read the opposite one instead
-        const int ie = nb.ie >= 0 ? nb.ie : nb.iw, iw = nb.iw >= 0 ? nb.iw : nb.ie;
-        const int kt = nb.kt >= 0 ? nb.kt : nb.kb, kb = nb.kb >= 0 ? nb.kb : nb.kt;
-        r -= cp.a * xr[zidx(L, ie, j, k)];
-        r -= cp.b * xr[zidx(L, iw, j, k)];
-        r -= cp.c * xr[zidx(L, i, j, kt)];
-        r -= cp.d * xr[zidx(L, i, j, kb)];
-        if (L.jp) {
-          const long long p0 = q - j * sj;
-          if (j == 0) r -= tr.a * xw[p0 + (ny - 1) * sj];
-          if (j == ny - 1) r -= tri[p0].a * xw[p0];
+    const bool valid = h < hx && i < L.nx;
+    const int ic = valid ? i : (colour ^ (k & 1));  // a real column for the address arithmetic
+    const ZNb nb = znb(L, ic, 0, k);
+    const long long p0 = zidx(L, ic, 0, k);
+    const long long oe = zidx(L, nb.ie >= 0 ? nb.ie : nb.iw, 0, k) - p0;
+    const long long ow = zidx(L, nb.iw >= 0 ? nb.iw : nb.ie, 0, k) - p0;
+    const long long ot = zidx(L, ic, 0, nb.kt >= 0 ? nb.kt : nb.kb) - p0;
+    const long long ob = zidx(L, ic, 0, nb.kb >= 0 ? nb.kb : nb.kt) - p0;
+    for (int jb = threadIdx.x / W; jb < ny; jb += U * jstep) {
+      T bb[U], xe[U], xwv[U], xt[U], xb[U];
+      Q4<T> tr[U], cp[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int j = jb + u * jstep;
+        if (valid && j < ny) {
+          const long long q = p0 + j * sj;
+          bb[u] = b[q];
+          tr[u] = tri[q];
+          if (!x_zero) {
+            cp[u] = cpl[q];
+            xe[u] = xr[q + oe];
+            xwv[u] = xr[q + ow];
+            xt[u] = xr[q + ot];
+            xb[u] = xr[q + ob];
+          }
         }
       }
-      rr = r * tr.b;
-      mm = j > 0 ? tr.a * tr.b : T(0);
-      cc = tr.c;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int j = jb + u * jstep;
+        if (j >= ny) continue;
+        T rr = 0, mm = 0, cc = 0;
+        if (valid) {
+          T r = bb[u];
+          if (!x_zero) {
+            // a missing neighbour has a zero coupling (its offset is the opposite one's)
+            r -= cp[u].a * xe[u];
+            r -= cp[u].b * xwv[u];
+            r -= cp[u].c * xt[u];
+            r -= cp[u].d * xb[u];
+            if (L.jp) {
+              if (j == 0) r -= tr[u].a * xw[p0 + (ny - 1) * sj];
+              if (j == ny - 1) r -= tri[p0].a * xw[p0];
+            }
+          }
+          rr = r * tr[u].b;
+          mm = j > 0 ? tr[u].a * tr[u].b : T(0);
+          cc = tr[u].c;
+        }
+        sr[w * P + j] = rr;
+        sm[w * P + j] = mm;
+        sc[w * P + j] = cc;
+      }
     }
-    sr[w * P + j] = rr;
-    sm[w * P + j] = mm;
-    sc[w * P + j] = cc;
   }
   __syncthreads();
   // B
@@ -471,9 +511,8 @@ __device__ __forceinline__ void zrestrict_cell(const ZL &F, const ZL &C, const Q
                                               const T *__restrict__ b, T *__restrict__ bc, long long t) {
   const long long ncell = (long long)C.nx * C.ny * C.nz;
   if (t >= ncell) return;
-  const int I = (int)(t % C.nx);
-  const long long r = t / C.nx;
-  const int J = (int)(r % C.ny), K = (int)(r / C.ny);
+  int I, J, K;
+  zcell(C, t, I, J, K);
   T s = 0;
   for (int c = 0; c < 2; c++)
     for (int bb = 0; bb < 2; bb++)
@@ -494,16 +533,15 @@ __global__ void k_zrestrict(ZL F, ZL C, const Q4<T> *__restrict__ cpl, const Q4<
 
 // x_fine += P x_coarse (cell-centred trilinear).
 template <typename T>
-__device__ __forceinline__ void zprolong_cell(const ZL &F, const ZL &C, const Q4<T> *__restrict__ triF,
-                                             const Q4<T> *__restrict__ triC, T *__restrict__ x,
+__device__ __forceinline__ void zprolong_cell(const ZL &F, const ZL &C, const uint8_t *__restrict__ actF,
+                                             const uint8_t *__restrict__ actC, T *__restrict__ x,
                                              const T *__restrict__ xc, long long t) {
   const long long ncell = (long long)F.nx * F.ny * F.nz;
   if (t >= ncell) return;
-  const int i = (int)(t % F.nx);
-  const long long r = t / F.nx;
-  const int j = (int)(r % F.ny), k = (int)(r / F.ny);
+  int i, j, k;
+  zcell(F, t, i, j, k);
   const long long q = zidx(F, i, j, k);
-  if (triF[q].d == T(0)) return;
+  if (!actF[q]) return;
   const int I = i >> 1, J = j >> 1, K = k >> 1;
   // the other coarse cell nearest along each direction, or -1
   int In = I + ((i & 1) ? 1 : -1), Jn = J + ((j & 1) ? 1 : -1), Kn = K + ((k & 1) ? 1 : -1);
@@ -521,16 +559,22 @@ __device__ __forceinline__ void zprolong_cell(const ZL &F, const ZL &C, const Q4
         const int ii = a ? In : I, jj = bb ? Jn : J, kk = c ? Kn : K;
         if (ii < 0 || jj < 0 || kk < 0) { wown += w; continue; }
         const long long qc = zidx(C, ii, jj, kk);
-        if (triC[qc].d == T(0)) { wown += w; continue; }
+        if (!actC[qc]) { wown += w; continue; }
         s += w * xc[qc];
       }
   x[q] += s + wown * xc[own];
 }
 
 template <typename T>
-__global__ void k_zprolong(ZL F, ZL C, const Q4<T> *__restrict__ triF, const Q4<T> *__restrict__ triC,
+__global__ void k_zprolong(ZL F, ZL C, const uint8_t *__restrict__ actF, const uint8_t *__restrict__ actC,
                            T *__restrict__ x, const T *__restrict__ xc) {
-  zprolong_cell<T>(F, C, triF, triC, x, xc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  zprolong_cell<T>(F, C, actF, actC, x, xc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+
+// act[q] = 1 where the level's diagonal is non-zero (an active unknown).
+__global__ void k_mg_active(long long n, const double *__restrict__ op, uint8_t *__restrict__ act) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q < n) act[q] = op[OP_DG * n + q] != 0.0 ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ bottom of the V-cycle
@@ -545,6 +589,7 @@ constexpr long long kBottomCells = 32768;
 template <typename T>
 struct BLevel {
   ZL z;
+  const uint8_t *act;
   const Q4<T> *cpl, *tri;
   T *x, *b, *xo;
   Q2<T> *ds;
@@ -595,7 +640,7 @@ __global__ void __launch_bounds__(kBottomThreads) k_mg_bottom(Bottom<T> B) {
   for (int l = B.nl - 2; l >= 0; l--) {
     const BLevel<T> &F = B.lv[l], &C = B.lv[l + 1];
     const long long nf = (long long)F.z.nx * F.z.ny * F.z.nz;
-    for (long long t = threadIdx.x; t < nf; t += blockDim.x) zprolong_cell<T>(F.z, C.z, F.tri, C.tri, F.x, C.x, t);
+    for (long long t = threadIdx.x; t < nf; t += blockDim.x) zprolong_cell<T>(F.z, C.z, F.act, C.act, F.x, C.x, t);
     __syncthreads();
     blk_smooth<T>(F, B.post, false, B.omega);
   }
@@ -607,9 +652,8 @@ __global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, T *__rest
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long ncell = (long long)L.nx * L.ny * L.nz;
   if (t >= ncell) return;
-  const int i = (int)(t % L.nx);
-  const long long r = t / L.nx;
-  const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+  int i, j, k;
+  zcell(L, t, i, j, k);
   b[zidx(L, i, j, k)] = (T)v[lidx(g, i + 1, j + 1, k + 1)];
 }
 
@@ -619,9 +663,9 @@ __global__ void k_from_zebra(Grid g, ZL L, const uint8_t *__restrict__ fluid, co
                              double *__restrict__ z) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  const unsigned up = (unsigned)p, umx = (unsigned)g.mx, umy = (unsigned)g.my;
+  const unsigned r = up / umx, kk = r / umy;
+  const int i = (int)(up - r * umx), j = (int)(r - kk * umy), k = (int)kk;
   double v = 0;
   if (fluid[p] && i >= 1 && i <= g.mx - 2 && j >= 1 && j <= g.my - 2 && k >= 1 && k <= g.mz - 2)
     v = (double)x[zidx(L, i - 1, j - 1, k - 1)];
@@ -640,7 +684,7 @@ static ZL make_zl(int nx, int ny, int nz, const Grid &g) {
 
 void mg_free(Poisson &P) {
   for (MGLevel &L : P.lv) {
-    cudaFree(L.op64); cudaFree(L.pk64); cudaFree(L.pk32); cudaFree(L.v64); cudaFree(L.v32);
+    cudaFree(L.op64); cudaFree(L.pk64); cudaFree(L.pk32); cudaFree(L.v64); cudaFree(L.v32); cudaFree(L.act);
   }
   P.lv.clear();
 }
@@ -659,11 +703,13 @@ int mg_setup(Ctx *c) {
     L.z = make_zl(nx, ny, nz, g);
     L.zebra = !((L.z.ip && (nx & 1)) || (L.z.kp && (nz & 1)));
     const long long n = L.z.n;
+    if (n >= (1LL << 31)) return set_err(c, VFS_ERR_INVALID, "poisson_lhs: grid too large for the multigrid indexing");
     bool ok = cudaMalloc(&L.op64, sizeof(double) * NOP * n) == cudaSuccess;
     ok &= cudaMalloc(&L.pk64, sizeof(double) * 8 * n) == cudaSuccess;
     ok &= cudaMalloc(&L.pk32, sizeof(float) * 8 * n) == cudaSuccess;
     ok &= cudaMalloc(&L.v64, sizeof(double) * 5 * n) == cudaSuccess;
     ok &= cudaMalloc(&L.v32, sizeof(float) * 5 * n) == cudaSuccess;
+    ok &= cudaMalloc(&L.act, n) == cudaSuccess;
     if (!ok) {
       P.lv.push_back(L);
       return set_err(c, VFS_ERR_CUDA, "poisson_lhs: multigrid allocation failed");
@@ -683,6 +729,7 @@ int mg_setup(Ctx *c) {
     if ((rc = check_launch(c, "k_mg_couplings"))) { P.lv.push_back(L); return rc; }
     k_mg_diag<<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64);
     k_mg_thomas<<<nblocks((long long)nx * nz, 64), 64, 0, c->stream>>>(L.z, L.op64);
+    k_mg_active<<<nblocks(n, 256), 256, 0, c->stream>>>(n, L.op64, L.act);
     k_mg_pack<double><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<double> *)L.pk64,
                                                                  (Q4<double> *)L.pk64 + n);
     k_mg_pack<float><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<float> *)L.pk32,
@@ -779,6 +826,7 @@ static int mg_bottom(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
     const LvT<T> v = lvt<T>(L);
     BLevel<T> &d = B.lv[q];
     d.z = L.z;
+    d.act = L.act;
     d.cpl = v.cpl; d.tri = v.tri;
     d.x = v.x; d.b = v.b; d.xo = v.xo; d.ds = v.ds;
     d.zebra = L.zebra ? 1 : 0;
@@ -802,7 +850,7 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   k_zrestrict<T><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
   if ((rc = check_launch(c, "k_zrestrict"))) return rc;
   if ((rc = mg_vcycle<T>(c, l + 1, nl, o))) return rc;
-  k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, f.tri, cc.tri, f.x, cc.x);
+  k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, F.act, C.act, f.x, cc.x);
   if ((rc = check_launch(c, "k_zprolong"))) return rc;
   return mg_smooth<T>(c, l, o.post_smooth, false);
 }

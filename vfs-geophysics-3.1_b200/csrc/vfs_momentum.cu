@@ -128,15 +128,10 @@ __device__ void slip_ghost(long long nb, int col, double sgn, Metrics m, CV3 uo,
 // boundary loop assigns gets its new value in `out` (reads the pre-loop snapshot `ucat`),
 // `flag` marks it.  Phase 2 (k_bc_commit) copies the marked values, which reproduces the
 // reference's read-from-lUcat / write-to-Ucat semantics exactly.
-__global__ void k_contra2cart_bc(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV3 lu,
-                                 CV3 uo, V3 out, uint8_t *flag) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
+__device__ __forceinline__ void contra2cart_bc_point(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv,
+                                                     CV3 lu, CV3 uo, V3 out, uint8_t *flag, long long p, int i,
+                                                     int j, int k) {
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
   const long long sx = 1, sy = mx, sz = (long long)mx * my;
   const int *bc = g.bc;
   bool w = false;
@@ -228,12 +223,124 @@ __global__ void k_contra2cart_bc(Grid g, Metrics m, const uint8_t *__restrict__ 
   }
 }
 
+__global__ void k_contra2cart_bc(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV3 lu,
+                                 CV3 uo, V3 out, uint8_t *flag) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  int i = (int)(p % g.mx);
+  long long q = p / g.mx;
+  int j = (int)(q % g.my);
+  int k = (int)(q / g.my);
+  contra2cart_bc_point(g, m, nv, lu, uo, out, flag, p, i, j, k);
+}
+
+// The points the boundary phase can assign apart from solid (nvert 3) cells: the six
+// ghost planes and the cells (1, 1, k), (mx-2, 1, k).  Points on two planes appear twice;
+// both threads compute and write the same values.
+__host__ __device__ inline long long edge_points(const Grid &g) {
+  return 2LL * g.my * g.mz + 2LL * g.mx * g.mz + 2LL * g.mx * g.my + 2LL * g.mz;
+}
+__device__ __forceinline__ long long edge_point(const Grid &g, long long t, int &i, int &j, int &k) {
+  const long long ni = 2LL * g.my * g.mz, nj = 2LL * g.mx * g.mz, nk = 2LL * g.mx * g.my;
+  if (t < ni) {
+    const long long r = t >> 1;
+    i = (t & 1) ? g.mx - 1 : 0; j = (int)(r % g.my); k = (int)(r / g.my);
+  } else if ((t -= ni) < nj) {
+    const long long r = t >> 1;
+    j = (t & 1) ? g.my - 1 : 0; i = (int)(r % g.mx); k = (int)(r / g.mx);
+  } else if ((t -= nj) < nk) {
+    const long long r = t >> 1;
+    k = (t & 1) ? g.mz - 1 : 0; i = (int)(r % g.mx); j = (int)(r / g.mx);
+  } else {
+    t -= nk;
+    i = (t & 1) ? g.mx - 2 : 1; j = 1; k = (int)(t >> 1);
+  }
+  return lidx(g, i, j, k);
+}
+
+__global__ void k_contra2cart_bc_edges(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV3 lu, CV3 uo, V3 out,
+                                       uint8_t *flag) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= edge_points(g)) return;
+  int i, j, k;
+  const long long p = edge_point(g, t, i, j, k);
+  contra2cart_bc_point(g, m, nv, lu, uo, out, flag, p, i, j, k);
+}
+
+// Solid cells (nvert 3) get zero (rhs.c:296-299), through the same two-phase buffer.
+__global__ void k_solid_zero(long long n, const long long *__restrict__ idx, V3 out, uint8_t *flag) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const long long p = idx[t];
+  out.x[p] = 0; out.y[p] = 0; out.z[p] = 0;
+  flag[p] = 1;
+}
+
+__global__ void k_bc_commit_edges(Grid g, CV3 in, uint8_t *flag, V3 dst) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= edge_points(g)) return;
+  int i, j, k;
+  const long long p = edge_point(g, t, i, j, k);
+  if (!flag[p]) return;
+  dst.x[p] = in.x[p]; dst.y[p] = in.y[p]; dst.z[p] = in.z[p];
+}
+__global__ void k_bc_commit_list(long long n, const long long *__restrict__ idx, CV3 in, V3 dst) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const long long p = idx[t];
+  dst.x[p] = in.x[p]; dst.y[p] = in.y[p]; dst.z[p] = in.z[p];
+}
+// Flags are cleared after every commit so the next call starts from zero.
+__global__ void k_bc_clear_edges(Grid g, uint8_t *flag) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= edge_points(g)) return;
+  int i, j, k;
+  flag[edge_point(g, t, i, j, k)] = 0;
+}
+__global__ void k_bc_clear_list(long long n, const long long *__restrict__ idx, uint8_t *flag) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < n) flag[idx[t]] = 0;
+}
+
+// Indices of the solid (nvert 3) points, in any order.
+__global__ void k_collect_solid(long long n, const uint8_t *__restrict__ nv, long long *idx,
+                                unsigned long long *count) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= n || nv[p] != 3) return;
+  const unsigned long long s = atomicAdd(count, 1ull);
+  if (idx) idx[s] = p;
+}
+
 __global__ void k_bc_commit(long long n, CV3 in, uint8_t *flag, V3 dst) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= n) return;
   if (!flag[p]) return;
   dst.x[p] = in.x[p]; dst.y[p] = in.y[p]; dst.z[p] = in.z[p];
   flag[p] = 0;
+}
+
+// The solid-point list is built once per nvert field (the count, then the indices).
+int solid_list(Ctx *c) {
+  if (c->nsolid >= 0) return VFS_OK;
+  int rc;
+  if ((rc = ensure_red(c, 64))) return rc;
+  unsigned long long *cnt = (unsigned long long *)(c->red + 62);
+  cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), c->stream);
+  k_collect_solid<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->nv, nullptr, cnt);
+  unsigned long long n = 0;
+  cudaMemcpyAsync(&n, cnt, sizeof(n), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "solid_list: count failed");
+  cudaFree(c->solid);
+  c->solid = nullptr;
+  if (n > 0) {
+    if (cudaMalloc(&c->solid, sizeof(long long) * n) != cudaSuccess)
+      return set_err(c, VFS_ERR_CUDA, "solid_list: allocation failed");
+    cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), c->stream);
+    k_collect_solid<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->nv, c->solid, cnt);
+    if ((rc = check_launch(c, "k_collect_solid"))) return rc;
+  }
+  c->nsolid = (long long)n;
+  return VFS_OK;
 }
 
 int contra2cart(Ctx *c) {
@@ -247,9 +354,16 @@ int contra2cart(Ctx *c) {
   if ((rc = periodic_copy3(c, ucat))) return rc;
   V3 out{c->bcbuf[0], c->bcbuf[1], c->bcbuf[2]};
   uint8_t *fl = c->bcflag;
-  k_contra2cart_bc<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, cv(ucat), cv(field3(c, VFS_UCAT_O)), out, fl);
+  if ((rc = solid_list(c))) return rc;
+  const long long ne = edge_points(g), ns = c->nsolid;
+  k_contra2cart_bc_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, m, c->nv, cv(ucat), cv(field3(c, VFS_UCAT_O)),
+                                                                  out, fl);
+  if (ns > 0) k_solid_zero<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, out, fl);
   if ((rc = check_launch(c, "k_contra2cart_bc"))) return rc;
-  k_bc_commit<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, cv(out), fl, ucat);
+  k_bc_commit_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, cv(out), fl, ucat);
+  if (ns > 0) k_bc_commit_list<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, cv(out), ucat);
+  k_bc_clear_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, fl);
+  if (ns > 0) k_bc_clear_list<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, fl);
   if ((rc = check_launch(c, "k_bc_commit"))) return rc;
   return periodic_copy3(c, ucat);
 }
@@ -296,6 +410,220 @@ __device__ __forceinline__ double visc_term(double g11, double g21, double g31, 
 
 struct FluxOut { double *div[3]; double *visc[3]; };
 
+// Convective (d) and viscous (v) flux of one face of Formfunction_2, following the three
+// face loops (momentum.c:671-1415): the i-face between (i,j,k) and (i+1,j,k), and the j
+// and k analogues.
+__device__ __forceinline__ void flux_i(const Grid &g, const Metrics &m, CV3 uc, CV3 u,
+                                      const uint8_t *__restrict__ nv, const double *__restrict__ nut, long long p,
+                                      int i, int j, int k, double d[3], double v[3]) {
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  const long long sx = 1, sy = mx, sz = (long long)mx * my;
+  const double nu = 1. / g.ren;
+  const bool les = g.les != 0;
+  (void)sx; (void)sy; (void)sz; (void)mx; (void)my; (void)mz;
+  const double ajc = m.iaj[p];
+  const double csi0 = m.icsi.x[p], csi1 = m.icsi.y[p], csi2 = m.icsi.z[p];
+  const double eta0 = m.ieta.x[p], eta1 = m.ieta.y[p], eta2 = m.ieta.z[p];
+  const double zet0 = m.izet.x[p], zet1 = m.izet.y[p], zet2 = m.izet.z[p];
+  double dc[3], de[3], dz[3];
+  dc[0] = u.x[p + sx] - u.x[p]; dc[1] = u.y[p + sx] - u.y[p]; dc[2] = u.z[p + sx] - u.z[p];
+  cross_diff(u, p, p + sx, p + sy, p + sy + sx, p - sy, p - sy + sx,
+             nv[p + sy] > 0 || nv[p + sy + sx] > 0, nv[p - sy] > 0 || nv[p - sy + sx] > 0, de);
+  cross_diff(u, p, p + sx, p + sz, p + sz + sx, p - sz, p - sz + sx,
+             nv[p + sz] > 0 || nv[p + sz + sx] > 0, nv[p - sz] > 0 || nv[p - sz + sx] > 0, dz);
+  const double g11 = csi0 * csi0 + csi1 * csi1 + csi2 * csi2;
+  const double g21 = eta0 * csi0 + eta1 * csi1 + eta2 * csi2;
+  const double g31 = zet0 * csi0 + zet1 * csi1 + zet2 * csi2;
+  const double r11 = dc[0] * csi0 + de[0] * eta0 + dz[0] * zet0;
+  const double r21 = dc[1] * csi0 + de[1] * eta0 + dz[1] * zet0;
+  const double r31 = dc[2] * csi0 + de[2] * eta0 + dz[2] * zet0;
+  const double r12 = dc[0] * csi1 + de[0] * eta1 + dz[0] * zet1;
+  const double r22 = dc[1] * csi1 + de[1] * eta1 + dz[1] * zet1;
+  const double r32 = dc[2] * csi1 + de[2] * eta1 + dz[2] * zet1;
+  const double r13 = dc[0] * csi2 + de[0] * eta2 + dz[0] * zet2;
+  const double r23 = dc[1] * csi2 + de[1] * eta2 + dz[1] * zet2;
+  const double r33 = dc[2] * csi2 + de[2] * eta2 + dz[2] * zet2;
+  int iL = i - 1, iR = i + 2;
+  if (i == 0 || i == mx - 2) {
+    if (g.iper) iL = mx - 3, iR = 2;
+    else iL = i, iR = i + 1;
+  } else if (nv[p - 1] + nv[p + 2] > 0) iL = i, iR = i + 1;
+  double ucon = uc.x[p];
+  if (g.iper && (i == 0 || i == mx - 2)) ucon = uc.x[p - i + (mx - 2)];
+  const double up = -0.5 * (ucon + fabs(ucon));
+  const double um = -0.5 * (ucon - fabs(ucon));
+  const long long pL = p - i + iL, pR = p - i + iR;
+  if (g.immersed && i != mx - 2 && nv[p] > 0) {
+    d[0] = quick_a(um, up, u.x[p], u.x[p + 1], u.x[p + 2]);
+    d[1] = quick_a(um, up, u.y[p], u.y[p + 1], u.y[p + 2]);
+    d[2] = quick_a(um, up, u.z[p], u.z[p + 1], u.z[p + 2]);
+  } else if (g.immersed && i != 0 && nv[p + 1] > 0) {
+    d[0] = quick_b(um, up, u.x[p - 1], u.x[p], u.x[p + 1]);
+    d[1] = quick_b(um, up, u.y[p - 1], u.y[p], u.y[p + 1]);
+    d[2] = quick_b(um, up, u.z[p - 1], u.z[p], u.z[p + 1]);
+  } else {
+    const double cu = uc.x[p];
+    d[0] = -cu * 0.0625 * (-u.x[pL] + 9. * u.x[p] + 9. * u.x[p + 1] - u.x[pR]);
+    d[1] = -cu * 0.0625 * (-u.y[pL] + 9. * u.y[p] + 9. * u.y[p + 1] - u.y[pR]);
+    d[2] = -cu * 0.0625 * (-u.z[pL] + 9. * u.z[p] + 9. * u.z[p + 1] - u.z[pR]);
+  }
+  if (nv[p] + nv[p + 1] > 0 && !g.immersed) d[0] = d[1] = d[2] = 0;
+  v[0] = 0; v[1] = 0; v[2] = 0;
+  if (les) {
+    double nut_f;
+    if ((i == 0 && !g.iper) || nv[p] > 0) nut_f = nut[p + 1];
+    else if ((i == mx - 2 && !g.iper) || nv[p + 1] > 0) nut_f = nut[p];
+    else nut_f = 0.5 * (nut[p] + nut[p + 1]);
+    v[0] = visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, csi0, csi1, csi2, ajc, nut_f);
+    v[1] = visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, csi0, csi1, csi2, ajc, nut_f);
+    v[2] = visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, csi0, csi1, csi2, ajc, nut_f);
+  }
+  v[0] += visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, csi0, csi1, csi2, ajc, nu);
+  v[1] += visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, csi0, csi1, csi2, ajc, nu);
+  v[2] += visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, csi0, csi1, csi2, ajc, nu);
+}
+
+__device__ __forceinline__ void flux_j(const Grid &g, const Metrics &m, CV3 uc, CV3 u,
+                                      const uint8_t *__restrict__ nv, const double *__restrict__ nut, long long p,
+                                      int i, int j, int k, double d[3], double v[3]) {
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  const long long sx = 1, sy = mx, sz = (long long)mx * my;
+  const double nu = 1. / g.ren;
+  const bool les = g.les != 0;
+  (void)sx; (void)sy; (void)sz; (void)mx; (void)my; (void)mz;
+  const double ajc = m.jaj[p];
+  const double csi0 = m.jcsi.x[p], csi1 = m.jcsi.y[p], csi2 = m.jcsi.z[p];
+  const double eta0 = m.jeta.x[p], eta1 = m.jeta.y[p], eta2 = m.jeta.z[p];
+  const double zet0 = m.jzet.x[p], zet1 = m.jzet.y[p], zet2 = m.jzet.z[p];
+  double dc[3], de[3], dz[3];
+  cross_diff(u, p, p + sy, p + sx, p + sy + sx, p - sx, p + sy - sx,
+             nv[p + sx] > 0 || nv[p + sy + sx] > 0, nv[p - sx] > 0 || nv[p + sy - sx] > 0, dc);
+  de[0] = u.x[p + sy] - u.x[p]; de[1] = u.y[p + sy] - u.y[p]; de[2] = u.z[p + sy] - u.z[p];
+  cross_diff(u, p, p + sy, p + sz, p + sz + sy, p - sz, p - sz + sy,
+             nv[p + sz] > 0 || nv[p + sz + sy] > 0, nv[p - sz] > 0 || nv[p - sz + sy] > 0, dz);
+  const double g11 = csi0 * eta0 + csi1 * eta1 + csi2 * eta2;
+  const double g21 = eta0 * eta0 + eta1 * eta1 + eta2 * eta2;
+  const double g31 = zet0 * eta0 + zet1 * eta1 + zet2 * eta2;
+  const double r11 = dc[0] * csi0 + de[0] * eta0 + dz[0] * zet0;
+  const double r21 = dc[1] * csi0 + de[1] * eta0 + dz[1] * zet0;
+  const double r31 = dc[2] * csi0 + de[2] * eta0 + dz[2] * zet0;
+  const double r12 = dc[0] * csi1 + de[0] * eta1 + dz[0] * zet1;
+  const double r22 = dc[1] * csi1 + de[1] * eta1 + dz[1] * zet1;
+  const double r32 = dc[2] * csi1 + de[2] * eta1 + dz[2] * zet1;
+  const double r13 = dc[0] * csi2 + de[0] * eta2 + dz[0] * zet2;
+  const double r23 = dc[1] * csi2 + de[1] * eta2 + dz[1] * zet2;
+  const double r33 = dc[2] * csi2 + de[2] * eta2 + dz[2] * zet2;
+  int jL = j - 1, jR = j + 2;
+  if (j == 0 || j == my - 2) {
+    if (g.jper) jL = my - 3, jR = 2;
+    else jL = j, jR = j + 1;
+  } else if (nv[p - sy] + nv[p + 2 * sy] > 0) jL = j, jR = j + 1;
+  double ucon = uc.y[p];
+  if (g.jper && (j == 0 || j == my - 2)) ucon = uc.y[p + (long long)(my - 2 - j) * sy];
+  const double up = -0.5 * (ucon + fabs(ucon));
+  const double um = -0.5 * (ucon - fabs(ucon));
+  const long long pL = p + (long long)(jL - j) * sy, pR = p + (long long)(jR - j) * sy;
+  if (g.immersed && j != my - 2 && nv[p] > 0) {
+    d[0] = quick_a(um, up, u.x[p], u.x[p + sy], u.x[p + 2 * sy]);
+    d[1] = quick_a(um, up, u.y[p], u.y[p + sy], u.y[p + 2 * sy]);
+    d[2] = quick_a(um, up, u.z[p], u.z[p + sy], u.z[p + 2 * sy]);
+  } else if (g.immersed && j != 0 && nv[p + sy] > 0) {
+    d[0] = quick_b(um, up, u.x[p - sy], u.x[p], u.x[p + sy]);
+    d[1] = quick_b(um, up, u.y[p - sy], u.y[p], u.y[p + sy]);
+    d[2] = quick_b(um, up, u.z[p - sy], u.z[p], u.z[p + sy]);
+  } else {
+    const double cu = uc.y[p];
+    d[0] = -cu * 0.0625 * (-u.x[pL] + 9. * u.x[p] + 9. * u.x[p + sy] - u.x[pR]);
+    d[1] = -cu * 0.0625 * (-u.y[pL] + 9. * u.y[p] + 9. * u.y[p + sy] - u.y[pR]);
+    d[2] = -cu * 0.0625 * (-u.z[pL] + 9. * u.z[p] + 9. * u.z[p + sy] - u.z[pR]);
+  }
+  if (nv[p] + nv[p + sy] > 0 && !g.immersed) d[0] = d[1] = d[2] = 0;
+  v[0] = 0; v[1] = 0; v[2] = 0;
+  if (les) {
+    double nut_f;
+    if ((j == 0 && !g.jper) || nv[p] > 0) nut_f = nut[p + sy];
+    else if ((j == my - 2 && !g.jper) || nv[p + sy] > 0) nut_f = nut[p];
+    else nut_f = 0.5 * (nut[p] + nut[p + sy]);
+    v[0] = visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, eta0, eta1, eta2, ajc, nut_f);
+    v[1] = visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, eta0, eta1, eta2, ajc, nut_f);
+    v[2] = visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, eta0, eta1, eta2, ajc, nut_f);
+  }
+  v[0] += visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, eta0, eta1, eta2, ajc, nu);
+  v[1] += visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, eta0, eta1, eta2, ajc, nu);
+  v[2] += visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, eta0, eta1, eta2, ajc, nu);
+}
+
+__device__ __forceinline__ void flux_k(const Grid &g, const Metrics &m, CV3 uc, CV3 u,
+                                      const uint8_t *__restrict__ nv, const double *__restrict__ nut, long long p,
+                                      int i, int j, int k, double d[3], double v[3]) {
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  const long long sx = 1, sy = mx, sz = (long long)mx * my;
+  const double nu = 1. / g.ren;
+  const bool les = g.les != 0;
+  (void)sx; (void)sy; (void)sz; (void)mx; (void)my; (void)mz;
+  const double ajc = m.kaj[p];
+  const double csi0 = m.kcsi.x[p], csi1 = m.kcsi.y[p], csi2 = m.kcsi.z[p];
+  const double eta0 = m.keta.x[p], eta1 = m.keta.y[p], eta2 = m.keta.z[p];
+  const double zet0 = m.kzet.x[p], zet1 = m.kzet.y[p], zet2 = m.kzet.z[p];
+  double dc[3], de[3], dz[3];
+  cross_diff(u, p, p + sz, p + sx, p + sz + sx, p - sx, p + sz - sx,
+             nv[p + sx] > 0 || nv[p + sz + sx] > 0, nv[p - sx] > 0 || nv[p + sz - sx] > 0, dc);
+  cross_diff(u, p, p + sz, p + sy, p + sz + sy, p - sy, p + sz - sy,
+             nv[p + sy] > 0 || nv[p + sz + sy] > 0, nv[p - sy] > 0 || nv[p + sz - sy] > 0, de);
+  dz[0] = u.x[p + sz] - u.x[p]; dz[1] = u.y[p + sz] - u.y[p]; dz[2] = u.z[p + sz] - u.z[p];
+  const double g11 = csi0 * zet0 + csi1 * zet1 + csi2 * zet2;
+  const double g21 = eta0 * zet0 + eta1 * zet1 + eta2 * zet2;
+  const double g31 = zet0 * zet0 + zet1 * zet1 + zet2 * zet2;
+  const double r11 = dc[0] * csi0 + de[0] * eta0 + dz[0] * zet0;
+  const double r21 = dc[1] * csi0 + de[1] * eta0 + dz[1] * zet0;
+  const double r31 = dc[2] * csi0 + de[2] * eta0 + dz[2] * zet0;
+  const double r12 = dc[0] * csi1 + de[0] * eta1 + dz[0] * zet1;
+  const double r22 = dc[1] * csi1 + de[1] * eta1 + dz[1] * zet1;
+  const double r32 = dc[2] * csi1 + de[2] * eta1 + dz[2] * zet1;
+  const double r13 = dc[0] * csi2 + de[0] * eta2 + dz[0] * zet2;
+  const double r23 = dc[1] * csi2 + de[1] * eta2 + dz[1] * zet2;
+  const double r33 = dc[2] * csi2 + de[2] * eta2 + dz[2] * zet2;
+  int kL = k - 1, kR = k + 2;
+  if (k == 0 || k == mz - 2) {
+    if (g.kper) kL = mz - 3, kR = 2;
+    else kL = k, kR = k + 1;
+  } else if (nv[p - sz] + nv[p + 2 * sz] > 0) kL = k, kR = k + 1;
+  double ucon = uc.z[p];
+  if (g.kper && (k == 0 || k == mz - 2)) ucon = uc.z[p + (long long)(mz - 2 - k) * sz];
+  if (k == mz - 2 && g.bc[5] == 4 && nv[p] == 0) ucon = uc.z[p - sz];
+  const double up = -0.5 * (ucon + fabs(ucon));
+  const double um = -0.5 * (ucon - fabs(ucon));
+  const long long pL = p + (long long)(kL - k) * sz, pR = p + (long long)(kR - k) * sz;
+  if (g.immersed && k != mz - 2 && nv[p] > 0) {
+    d[0] = quick_a(um, up, u.x[p], u.x[p + sz], u.x[p + 2 * sz]);
+    d[1] = quick_a(um, up, u.y[p], u.y[p + sz], u.y[p + 2 * sz]);
+    d[2] = quick_a(um, up, u.z[p], u.z[p + sz], u.z[p + 2 * sz]);
+  } else if (g.immersed && k != 0 && nv[p + sz] > 0) {
+    d[0] = quick_b(um, up, u.x[p - sz], u.x[p], u.x[p + sz]);
+    d[1] = quick_b(um, up, u.y[p - sz], u.y[p], u.y[p + sz]);
+    d[2] = quick_b(um, up, u.z[p - sz], u.z[p], u.z[p + sz]);
+  } else {
+    const double cu = uc.z[p];
+    d[0] = -cu * 0.0625 * (-u.x[pL] + 9. * u.x[p] + 9. * u.x[p + sz] - u.x[pR]);
+    d[1] = -cu * 0.0625 * (-u.y[pL] + 9. * u.y[p] + 9. * u.y[p + sz] - u.y[pR]);
+    d[2] = -cu * 0.0625 * (-u.z[pL] + 9. * u.z[p] + 9. * u.z[p + sz] - u.z[pR]);
+  }
+  if (nv[p] + nv[p + sz] > 0 && !g.immersed) d[0] = d[1] = d[2] = 0;
+  v[0] = 0; v[1] = 0; v[2] = 0;
+  if (les) {
+    double nut_f;
+    if ((k == 0 && !g.kper) || nv[p] > 0) nut_f = nut[p + sz];
+    else if ((k == mz - 2 && !g.kper) || nv[p + sz] > 0) nut_f = nut[p];
+    else nut_f = 0.5 * (nut[p] + nut[p + sz]);
+    v[0] = visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, zet0, zet1, zet2, ajc, nut_f);
+    v[1] = visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, zet0, zet1, zet2, ajc, nut_f);
+    v[2] = visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, zet0, zet1, zet2, ajc, nut_f);
+  }
+  v[0] += visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, zet0, zet1, zet2, ajc, nu);
+  v[1] += visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, zet0, zet1, zet2, ajc, nu);
+  v[2] += visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, zet0, zet1, zet2, ajc, nu);
+}
+
 // One thread per DA point (i,j,k) with i<mx-1, j<my-1, k<mz-1: computes the fluxes of
 // its i-face (if j,k >= 1), j-face (if i,k >= 1) and k-face (if i,j >= 1), following
 // the three face loops of Formfunction_2 (momentum.c:671-1415).
@@ -309,208 +637,19 @@ __global__ void k_face_flux(Grid g, Metrics m, CV3 uc, CV3 u, const uint8_t *__r
   int j = (int)(q % my);
   int k = (int)(q / my);
   if (i == mx - 1 || j == my - 1 || k == mz - 1) return;
-  const long long sx = 1, sy = mx, sz = (long long)mx * my;
-  const double nu = 1. / g.ren;
-  const bool les = g.les != 0;
-
-  // ---------------- i direction
+  double d[3], v[3];
   if (j != 0 && k != 0) {
-    const double ajc = m.iaj[p];
-    const double csi0 = m.icsi.x[p], csi1 = m.icsi.y[p], csi2 = m.icsi.z[p];
-    const double eta0 = m.ieta.x[p], eta1 = m.ieta.y[p], eta2 = m.ieta.z[p];
-    const double zet0 = m.izet.x[p], zet1 = m.izet.y[p], zet2 = m.izet.z[p];
-    double dc[3], de[3], dz[3];
-    dc[0] = u.x[p + sx] - u.x[p]; dc[1] = u.y[p + sx] - u.y[p]; dc[2] = u.z[p + sx] - u.z[p];
-    cross_diff(u, p, p + sx, p + sy, p + sy + sx, p - sy, p - sy + sx,
-               nv[p + sy] > 0 || nv[p + sy + sx] > 0, nv[p - sy] > 0 || nv[p - sy + sx] > 0, de);
-    cross_diff(u, p, p + sx, p + sz, p + sz + sx, p - sz, p - sz + sx,
-               nv[p + sz] > 0 || nv[p + sz + sx] > 0, nv[p - sz] > 0 || nv[p - sz + sx] > 0, dz);
-    const double g11 = csi0 * csi0 + csi1 * csi1 + csi2 * csi2;
-    const double g21 = eta0 * csi0 + eta1 * csi1 + eta2 * csi2;
-    const double g31 = zet0 * csi0 + zet1 * csi1 + zet2 * csi2;
-    const double r11 = dc[0] * csi0 + de[0] * eta0 + dz[0] * zet0;
-    const double r21 = dc[1] * csi0 + de[1] * eta0 + dz[1] * zet0;
-    const double r31 = dc[2] * csi0 + de[2] * eta0 + dz[2] * zet0;
-    const double r12 = dc[0] * csi1 + de[0] * eta1 + dz[0] * zet1;
-    const double r22 = dc[1] * csi1 + de[1] * eta1 + dz[1] * zet1;
-    const double r32 = dc[2] * csi1 + de[2] * eta1 + dz[2] * zet1;
-    const double r13 = dc[0] * csi2 + de[0] * eta2 + dz[0] * zet2;
-    const double r23 = dc[1] * csi2 + de[1] * eta2 + dz[1] * zet2;
-    const double r33 = dc[2] * csi2 + de[2] * eta2 + dz[2] * zet2;
-    int iL = i - 1, iR = i + 2;
-    if (i == 0 || i == mx - 2) {
-      if (g.iper) iL = mx - 3, iR = 2;
-      else iL = i, iR = i + 1;
-    } else if (nv[p - 1] + nv[p + 2] > 0) iL = i, iR = i + 1;
-    double ucon = uc.x[p];
-    if (g.iper && (i == 0 || i == mx - 2)) ucon = uc.x[p - i + (mx - 2)];
-    const double up = -0.5 * (ucon + fabs(ucon));
-    const double um = -0.5 * (ucon - fabs(ucon));
-    const long long pL = p - i + iL, pR = p - i + iR;
-    double d[3];
-    if (g.immersed && i != mx - 2 && nv[p] > 0) {
-      d[0] = quick_a(um, up, u.x[p], u.x[p + 1], u.x[p + 2]);
-      d[1] = quick_a(um, up, u.y[p], u.y[p + 1], u.y[p + 2]);
-      d[2] = quick_a(um, up, u.z[p], u.z[p + 1], u.z[p + 2]);
-    } else if (g.immersed && i != 0 && nv[p + 1] > 0) {
-      d[0] = quick_b(um, up, u.x[p - 1], u.x[p], u.x[p + 1]);
-      d[1] = quick_b(um, up, u.y[p - 1], u.y[p], u.y[p + 1]);
-      d[2] = quick_b(um, up, u.z[p - 1], u.z[p], u.z[p + 1]);
-    } else {
-      const double cu = uc.x[p];
-      d[0] = -cu * 0.0625 * (-u.x[pL] + 9. * u.x[p] + 9. * u.x[p + 1] - u.x[pR]);
-      d[1] = -cu * 0.0625 * (-u.y[pL] + 9. * u.y[p] + 9. * u.y[p + 1] - u.y[pR]);
-      d[2] = -cu * 0.0625 * (-u.z[pL] + 9. * u.z[p] + 9. * u.z[p + 1] - u.z[pR]);
-    }
-    if (nv[p] + nv[p + 1] > 0 && !g.immersed) d[0] = d[1] = d[2] = 0;
-    double v[3] = {0, 0, 0};
-    if (les) {
-      double nut_f;
-      if ((i == 0 && !g.iper) || nv[p] > 0) nut_f = nut[p + 1];
-      else if ((i == mx - 2 && !g.iper) || nv[p + 1] > 0) nut_f = nut[p];
-      else nut_f = 0.5 * (nut[p] + nut[p + 1]);
-      v[0] = visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, csi0, csi1, csi2, ajc, nut_f);
-      v[1] = visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, csi0, csi1, csi2, ajc, nut_f);
-      v[2] = visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, csi0, csi1, csi2, ajc, nut_f);
-    }
-    v[0] += visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, csi0, csi1, csi2, ajc, nu);
-    v[1] += visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, csi0, csi1, csi2, ajc, nu);
-    v[2] += visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, csi0, csi1, csi2, ajc, nu);
+    flux_i(g, m, uc, u, nv, nut, p, i, j, k, d, v);
     f1.div[0][p] = d[0]; f1.div[1][p] = d[1]; f1.div[2][p] = d[2];
     f1.visc[0][p] = v[0]; f1.visc[1][p] = v[1]; f1.visc[2][p] = v[2];
   }
-
-  // ---------------- j direction
   if (i != 0 && k != 0) {
-    const double ajc = m.jaj[p];
-    const double csi0 = m.jcsi.x[p], csi1 = m.jcsi.y[p], csi2 = m.jcsi.z[p];
-    const double eta0 = m.jeta.x[p], eta1 = m.jeta.y[p], eta2 = m.jeta.z[p];
-    const double zet0 = m.jzet.x[p], zet1 = m.jzet.y[p], zet2 = m.jzet.z[p];
-    double dc[3], de[3], dz[3];
-    cross_diff(u, p, p + sy, p + sx, p + sy + sx, p - sx, p + sy - sx,
-               nv[p + sx] > 0 || nv[p + sy + sx] > 0, nv[p - sx] > 0 || nv[p + sy - sx] > 0, dc);
-    de[0] = u.x[p + sy] - u.x[p]; de[1] = u.y[p + sy] - u.y[p]; de[2] = u.z[p + sy] - u.z[p];
-    cross_diff(u, p, p + sy, p + sz, p + sz + sy, p - sz, p - sz + sy,
-               nv[p + sz] > 0 || nv[p + sz + sy] > 0, nv[p - sz] > 0 || nv[p - sz + sy] > 0, dz);
-    const double g11 = csi0 * eta0 + csi1 * eta1 + csi2 * eta2;
-    const double g21 = eta0 * eta0 + eta1 * eta1 + eta2 * eta2;
-    const double g31 = zet0 * eta0 + zet1 * eta1 + zet2 * eta2;
-    const double r11 = dc[0] * csi0 + de[0] * eta0 + dz[0] * zet0;
-    const double r21 = dc[1] * csi0 + de[1] * eta0 + dz[1] * zet0;
-    const double r31 = dc[2] * csi0 + de[2] * eta0 + dz[2] * zet0;
-    const double r12 = dc[0] * csi1 + de[0] * eta1 + dz[0] * zet1;
-    const double r22 = dc[1] * csi1 + de[1] * eta1 + dz[1] * zet1;
-    const double r32 = dc[2] * csi1 + de[2] * eta1 + dz[2] * zet1;
-    const double r13 = dc[0] * csi2 + de[0] * eta2 + dz[0] * zet2;
-    const double r23 = dc[1] * csi2 + de[1] * eta2 + dz[1] * zet2;
-    const double r33 = dc[2] * csi2 + de[2] * eta2 + dz[2] * zet2;
-    int jL = j - 1, jR = j + 2;
-    if (j == 0 || j == my - 2) {
-      if (g.jper) jL = my - 3, jR = 2;
-      else jL = j, jR = j + 1;
-    } else if (nv[p - sy] + nv[p + 2 * sy] > 0) jL = j, jR = j + 1;
-    double ucon = uc.y[p];
-    if (g.jper && (j == 0 || j == my - 2)) ucon = uc.y[p + (long long)(my - 2 - j) * sy];
-    const double up = -0.5 * (ucon + fabs(ucon));
-    const double um = -0.5 * (ucon - fabs(ucon));
-    const long long pL = p + (long long)(jL - j) * sy, pR = p + (long long)(jR - j) * sy;
-    double d[3];
-    if (g.immersed && j != my - 2 && nv[p] > 0) {
-      d[0] = quick_a(um, up, u.x[p], u.x[p + sy], u.x[p + 2 * sy]);
-      d[1] = quick_a(um, up, u.y[p], u.y[p + sy], u.y[p + 2 * sy]);
-      d[2] = quick_a(um, up, u.z[p], u.z[p + sy], u.z[p + 2 * sy]);
-    } else if (g.immersed && j != 0 && nv[p + sy] > 0) {
-      d[0] = quick_b(um, up, u.x[p - sy], u.x[p], u.x[p + sy]);
-      d[1] = quick_b(um, up, u.y[p - sy], u.y[p], u.y[p + sy]);
-      d[2] = quick_b(um, up, u.z[p - sy], u.z[p], u.z[p + sy]);
-    } else {
-      const double cu = uc.y[p];
-      d[0] = -cu * 0.0625 * (-u.x[pL] + 9. * u.x[p] + 9. * u.x[p + sy] - u.x[pR]);
-      d[1] = -cu * 0.0625 * (-u.y[pL] + 9. * u.y[p] + 9. * u.y[p + sy] - u.y[pR]);
-      d[2] = -cu * 0.0625 * (-u.z[pL] + 9. * u.z[p] + 9. * u.z[p + sy] - u.z[pR]);
-    }
-    if (nv[p] + nv[p + sy] > 0 && !g.immersed) d[0] = d[1] = d[2] = 0;
-    double v[3] = {0, 0, 0};
-    if (les) {
-      double nut_f;
-      if ((j == 0 && !g.jper) || nv[p] > 0) nut_f = nut[p + sy];
-      else if ((j == my - 2 && !g.jper) || nv[p + sy] > 0) nut_f = nut[p];
-      else nut_f = 0.5 * (nut[p] + nut[p + sy]);
-      v[0] = visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, eta0, eta1, eta2, ajc, nut_f);
-      v[1] = visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, eta0, eta1, eta2, ajc, nut_f);
-      v[2] = visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, eta0, eta1, eta2, ajc, nut_f);
-    }
-    v[0] += visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, eta0, eta1, eta2, ajc, nu);
-    v[1] += visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, eta0, eta1, eta2, ajc, nu);
-    v[2] += visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, eta0, eta1, eta2, ajc, nu);
+    flux_j(g, m, uc, u, nv, nut, p, i, j, k, d, v);
     f2.div[0][p] = d[0]; f2.div[1][p] = d[1]; f2.div[2][p] = d[2];
     f2.visc[0][p] = v[0]; f2.visc[1][p] = v[1]; f2.visc[2][p] = v[2];
   }
-
-  // ---------------- k direction
   if (i != 0 && j != 0) {
-    const double ajc = m.kaj[p];
-    const double csi0 = m.kcsi.x[p], csi1 = m.kcsi.y[p], csi2 = m.kcsi.z[p];
-    const double eta0 = m.keta.x[p], eta1 = m.keta.y[p], eta2 = m.keta.z[p];
-    const double zet0 = m.kzet.x[p], zet1 = m.kzet.y[p], zet2 = m.kzet.z[p];
-    double dc[3], de[3], dz[3];
-    cross_diff(u, p, p + sz, p + sx, p + sz + sx, p - sx, p + sz - sx,
-               nv[p + sx] > 0 || nv[p + sz + sx] > 0, nv[p - sx] > 0 || nv[p + sz - sx] > 0, dc);
-    cross_diff(u, p, p + sz, p + sy, p + sz + sy, p - sy, p + sz - sy,
-               nv[p + sy] > 0 || nv[p + sz + sy] > 0, nv[p - sy] > 0 || nv[p + sz - sy] > 0, de);
-    dz[0] = u.x[p + sz] - u.x[p]; dz[1] = u.y[p + sz] - u.y[p]; dz[2] = u.z[p + sz] - u.z[p];
-    const double g11 = csi0 * zet0 + csi1 * zet1 + csi2 * zet2;
-    const double g21 = eta0 * zet0 + eta1 * zet1 + eta2 * zet2;
-    const double g31 = zet0 * zet0 + zet1 * zet1 + zet2 * zet2;
-    const double r11 = dc[0] * csi0 + de[0] * eta0 + dz[0] * zet0;
-    const double r21 = dc[1] * csi0 + de[1] * eta0 + dz[1] * zet0;
-    const double r31 = dc[2] * csi0 + de[2] * eta0 + dz[2] * zet0;
-    const double r12 = dc[0] * csi1 + de[0] * eta1 + dz[0] * zet1;
-    const double r22 = dc[1] * csi1 + de[1] * eta1 + dz[1] * zet1;
-    const double r32 = dc[2] * csi1 + de[2] * eta1 + dz[2] * zet1;
-    const double r13 = dc[0] * csi2 + de[0] * eta2 + dz[0] * zet2;
-    const double r23 = dc[1] * csi2 + de[1] * eta2 + dz[1] * zet2;
-    const double r33 = dc[2] * csi2 + de[2] * eta2 + dz[2] * zet2;
-    int kL = k - 1, kR = k + 2;
-    if (k == 0 || k == mz - 2) {
-      if (g.kper) kL = mz - 3, kR = 2;
-      else kL = k, kR = k + 1;
-    } else if (nv[p - sz] + nv[p + 2 * sz] > 0) kL = k, kR = k + 1;
-    double ucon = uc.z[p];
-    if (g.kper && (k == 0 || k == mz - 2)) ucon = uc.z[p + (long long)(mz - 2 - k) * sz];
-    if (k == mz - 2 && g.bc[5] == 4 && nv[p] == 0) ucon = uc.z[p - sz];
-    const double up = -0.5 * (ucon + fabs(ucon));
-    const double um = -0.5 * (ucon - fabs(ucon));
-    const long long pL = p + (long long)(kL - k) * sz, pR = p + (long long)(kR - k) * sz;
-    double d[3];
-    if (g.immersed && k != mz - 2 && nv[p] > 0) {
-      d[0] = quick_a(um, up, u.x[p], u.x[p + sz], u.x[p + 2 * sz]);
-      d[1] = quick_a(um, up, u.y[p], u.y[p + sz], u.y[p + 2 * sz]);
-      d[2] = quick_a(um, up, u.z[p], u.z[p + sz], u.z[p + 2 * sz]);
-    } else if (g.immersed && k != 0 && nv[p + sz] > 0) {
-      d[0] = quick_b(um, up, u.x[p - sz], u.x[p], u.x[p + sz]);
-      d[1] = quick_b(um, up, u.y[p - sz], u.y[p], u.y[p + sz]);
-      d[2] = quick_b(um, up, u.z[p - sz], u.z[p], u.z[p + sz]);
-    } else {
-      const double cu = uc.z[p];
-      d[0] = -cu * 0.0625 * (-u.x[pL] + 9. * u.x[p] + 9. * u.x[p + sz] - u.x[pR]);
-      d[1] = -cu * 0.0625 * (-u.y[pL] + 9. * u.y[p] + 9. * u.y[p + sz] - u.y[pR]);
-      d[2] = -cu * 0.0625 * (-u.z[pL] + 9. * u.z[p] + 9. * u.z[p + sz] - u.z[pR]);
-    }
-    if (nv[p] + nv[p + sz] > 0 && !g.immersed) d[0] = d[1] = d[2] = 0;
-    double v[3] = {0, 0, 0};
-    if (les) {
-      double nut_f;
-      if ((k == 0 && !g.kper) || nv[p] > 0) nut_f = nut[p + sz];
-      else if ((k == mz - 2 && !g.kper) || nv[p + sz] > 0) nut_f = nut[p];
-      else nut_f = 0.5 * (nut[p] + nut[p + sz]);
-      v[0] = visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, zet0, zet1, zet2, ajc, nut_f);
-      v[1] = visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, zet0, zet1, zet2, ajc, nut_f);
-      v[2] = visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, zet0, zet1, zet2, ajc, nut_f);
-    }
-    v[0] += visc_term(g11, g21, g31, dc[0], de[0], dz[0], r11, r21, r31, zet0, zet1, zet2, ajc, nu);
-    v[1] += visc_term(g11, g21, g31, dc[1], de[1], dz[1], r12, r22, r32, zet0, zet1, zet2, ajc, nu);
-    v[2] += visc_term(g11, g21, g31, dc[2], de[2], dz[2], r13, r23, r33, zet0, zet1, zet2, ajc, nu);
+    flux_k(g, m, uc, u, nv, nut, p, i, j, k, d, v);
     f3.div[0][p] = d[0]; f3.div[1][p] = d[1]; f3.div[2][p] = d[2];
     f3.visc[0][p] = v[0]; f3.visc[1][p] = v[1]; f3.visc[2][p] = v[2];
   }
@@ -520,6 +659,72 @@ __global__ void k_face_flux(Grid g, Metrics m, CV3 uc, CV3 u, const uint8_t *__r
 // viscous divergence (momentum.c:1508-1640).  Face fluxes on a periodic ghost plane are
 // read from their periodic image (momentum.c:1456-1500 copy loop).
 struct FluxIn { const double *div[3]; const double *visc[3]; };
+
+// Unwrapped face index u (u = cell + offset) -> the face whose flux the reference reads:
+// on a periodic direction the faces 0 and m-1 and beyond are images of interior faces
+// (the copy loop of momentum.c:1456-1500); m = number of points in the direction.
+__device__ __forceinline__ int face_image(int u, int m, int per) {
+  if (per) {
+    if (u <= 0) return u + (m - 2);
+    if (u >= m - 1) return u - (m - 2);
+  }
+  return u;
+}
+
+// Stencil offsets of the wide (4th-order) difference of Fp along one direction at cell
+// index c (1..m-2): faces c+oR and c+oL, divided by den (momentum.c:1508-1640).
+__device__ __forceinline__ void fp_offsets(int c, int m, int per, int nvsum, int &oR, int &oL, double &den) {
+  oR = 1; oL = -2; den = 3.;
+  if (!per && (c == 1 || c == 2 || c == m - 3 || c == m - 2)) { oR = 0; oL = -1; den = 1.; }
+  if (nvsum > 0) { oR = 0; oL = -1; den = 1.; }
+}
+
+// Fp at interior cell (i,j,k): 9/8 div - 1/8 wide / den plus the viscous divergence.
+// F supplies face fluxes by direction, component and offset from the cell:
+// F.d(dir, comp, off) (off in -2..1) and F.v(dir, comp, off) (off in -1..0).
+template <class F>
+__device__ __forceinline__ void fp_cell(const Grid &g, const uint8_t *__restrict__ nv, long long p, int i, int j,
+                                        int k, const F &f, double fpv[3]) {
+  const long long sy = g.mx, sz = (long long)g.mx * g.my;
+  int oiR, oiL, ojR, ojL, okR, okL;
+  double di, dj, dk;
+  fp_offsets(i, g.mx, g.iper, nv[p - 1] + nv[p] + nv[p + 1], oiR, oiL, di);
+  fp_offsets(j, g.my, g.jper, nv[p - sy] + nv[p] + nv[p + sy], ojR, ojL, dj);
+  fp_offsets(k, g.mz, g.kper, nv[p - sz] + nv[p] + nv[p + sz], okR, okL, dk);
+  const double ai = 1. / di, aj_ = 1. / dj, ak = 1. / dk;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const double div = (f.d(0, c, 0) - f.d(0, c, -1) + f.d(1, c, 0) - f.d(1, c, -1) + f.d(2, c, 0) - f.d(2, c, -1));
+    double acc = 0;
+    acc += (f.d(0, c, oiR) - f.d(0, c, oiL)) * ai;
+    acc += (f.d(1, c, ojR) - f.d(1, c, ojL)) * aj_;
+    acc += (f.d(2, c, okR) - f.d(2, c, okL)) * ak;
+    double v = 9. / 8. * div + -1. / 8. * acc;
+    v += (f.v(0, c, 0) - f.v(0, c, -1) + f.v(1, c, 0) - f.v(1, c, -1) + f.v(2, c, 0) - f.v(2, c, -1)) / 1.0;
+    fpv[c] = v;
+  }
+}
+
+// Face fluxes from the global face-flux arrays.
+struct GlobalFaces {
+  const Grid *g;
+  FluxIn f1, f2, f3;
+  long long rowi, rowj, rowk;
+  int i, j, k;
+  __device__ __forceinline__ long long at(int dir, int off) const {
+    if (dir == 0) return rowi + face_image(i + off, g->mx, g->iper);
+    if (dir == 1) return rowj + (long long)face_image(j + off, g->my, g->jper) * g->mx;
+    return rowk + (long long)face_image(k + off, g->mz, g->kper) * ((long long)g->mx * g->my);
+  }
+  __device__ __forceinline__ double d(int dir, int c, int off) const {
+    const FluxIn &f = dir == 0 ? f1 : (dir == 1 ? f2 : f3);
+    return f.div[c][at(dir, off)];
+  }
+  __device__ __forceinline__ double v(int dir, int c, int off) const {
+    const FluxIn &f = dir == 0 ? f1 : (dir == 1 ? f2 : f3);
+    return f.visc[c][at(dir, off)];
+  }
+};
 
 __global__ void k_fp(Grid g, FluxIn f1, FluxIn f2, FluxIn f3, const uint8_t *__restrict__ nv,
                      double *fpx, double *fpy, double *fpz) {
@@ -531,41 +736,76 @@ __global__ void k_fp(Grid g, FluxIn f1, FluxIn f2, FluxIn f3, const uint8_t *__r
   int j = (int)(q % my);
   int k = (int)(q / my);
   if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
-  const long long sy = mx, sz = (long long)mx * my;
-  const long long rowi = p - i, rowj = p - (long long)j * sy, rowk = p - (long long)k * sz;
-  // periodic images of face indices
-  auto fi = [&](int ii) { return rowi + wrapi(g, ii); };
-  auto fj = [&](int jj) { return rowj + (long long)wrapj(g, jj) * sy; };
-  auto fk = [&](int kk) { return rowk + (long long)wrapk(g, kk) * sz; };
-  double div[3], acc[3] = {0, 0, 0}, fpv[3];
-  for (int c = 0; c < 3; c++)
-    div[c] = (f1.div[c][p] - f1.div[c][fi(i - 1)] + f2.div[c][p] - f2.div[c][fj(j - 1)] +
-              f3.div[c][p] - f3.div[c][fk(k - 1)]);
-  int iR = i + 1, iL = i - 2, jR = j + 1, jL = j - 2, kR = k + 1, kL = k - 2;
-  double di = 3., dj = 3., dk = 3.;
-  if (i == 1) { if (g.iper) iL = mx - 3; else iR = i, iL = i - 1, di = 1.; }
-  else if (i == 2 || i == mx - 3) { if (!g.iper) iR = i, iL = i - 1, di = 1.; }
-  else if (i == mx - 2) { if (g.iper) iR = 1; else iR = i, iL = i - 1, di = 1.; }
-  if (j == 1) { if (g.jper) jL = my - 3; else jR = j, jL = j - 1, dj = 1.; }
-  else if (j == 2 || j == my - 3) { if (!g.jper) jR = j, jL = j - 1, dj = 1.; }
-  else if (j == my - 2) { if (g.jper) jR = 1; else jR = j, jL = j - 1, dj = 1.; }
-  if (k == 1) { if (g.kper) kL = mz - 3; else kR = k, kL = k - 1, dk = 1.; }
-  else if (k == 2 || k == mz - 3) { if (!g.kper) kR = k, kL = k - 1, dk = 1.; }
-  else if (k == mz - 2) { if (g.kper) kR = 1; else kR = k, kL = k - 1, dk = 1.; }
-  if (nv[p - 1] + nv[p] + nv[p + 1] > 0) iR = i, iL = i - 1, di = 1.;
-  if (nv[p - sy] + nv[p] + nv[p + sy] > 0) jR = j, jL = j - 1, dj = 1.;
-  if (nv[p - sz] + nv[p] + nv[p + sz] > 0) kR = k, kL = k - 1, dk = 1.;
-  const double ai = 1. / di, aj_ = 1. / dj, ak = 1. / dk;
-  for (int c = 0; c < 3; c++) {
-    acc[c] += (f1.div[c][fi(iR)] - f1.div[c][fi(iL)]) * ai;
-    acc[c] += (f2.div[c][fj(jR)] - f2.div[c][fj(jL)]) * aj_;
-    acc[c] += (f3.div[c][fk(kR)] - f3.div[c][fk(kL)]) * ak;
-    fpv[c] = 9. / 8. * div[c] + -1. / 8. * acc[c];
-    fpv[c] += (f1.visc[c][p] - f1.visc[c][fi(i - 1)] + f2.visc[c][p] - f2.visc[c][fj(j - 1)] +
-               f3.visc[c][p] - f3.visc[c][fk(k - 1)]) / 1.0;
-  }
+  GlobalFaces F;
+  F.g = &g; F.f1 = f1; F.f2 = f2; F.f3 = f3;
+  F.rowi = p - i; F.rowj = p - (long long)j * mx; F.rowk = p - (long long)k * mx * my;
+  F.i = i; F.j = j; F.k = k;
+  double fpv[3];
+  fp_cell(g, nv, p, i, j, k, F, fpv);
   fpx[p] = fpv[0]; fpy[p] = fpv[1]; fpz[p] = fpv[2];
 }
+
+// Contravariant projection of Fp onto the faces, scale, masks and the boundary zeroing
+// of the right-hand side (momentum.c:1686-1900).  In RK mode the stage update
+// Ucont = pUcont + a*(RHS - dP) (rhs.c:1644-1650) is fused into the epilogue and the
+// accumulation starts from a zeroed RHS (VecSet(Rhs,0) at rhs.c:1643).
+// Right-hand side at one point from Fp, accessed as F.fp(w, c) with w = 0 the cell and
+// w = 1, 2, 3 its +i, +j, +k neighbour (the periodic image on the last interior plane);
+// ghost points get zero.  With rk set, the stage update is applied as well.
+template <class FPA>
+__device__ __forceinline__ void rhs_point(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv,
+                                          long long p, int i, int j, int k, bool ghost, const FPA &f, double scale,
+                                          V3 rhs, int rk, double a, CV3 dP, CV3 pu, V3 ucont) {
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  double r[3];
+  if (ghost) {
+    r[0] = r[1] = r[2] = 0;
+  } else {
+    const long long sy = mx, sz = (long long)mx * my;
+    if (rk) { r[0] = 0; r[1] = 0; r[2] = 0; }
+    else { r[0] = rhs.x[p]; r[1] = rhs.y[p]; r[2] = rhs.z[p]; }
+    r[0] += scale * (0.5 * (m.csi.x[p] * f.fp(0, 0) + m.csi.y[p] * f.fp(0, 1) + m.csi.z[p] * f.fp(0, 2)) +
+                     0.5 * (m.csi.x[p + 1] * f.fp(1, 0) + m.csi.y[p + 1] * f.fp(1, 1) + m.csi.z[p + 1] * f.fp(1, 2))) *
+            m.iaj[p];
+    r[1] += scale * (0.5 * (m.eta.x[p] * f.fp(0, 0) + m.eta.y[p] * f.fp(0, 1) + m.eta.z[p] * f.fp(0, 2)) +
+                     0.5 * (m.eta.x[p + sy] * f.fp(2, 0) + m.eta.y[p + sy] * f.fp(2, 1) + m.eta.z[p + sy] * f.fp(2, 2))) *
+            m.jaj[p];
+    r[2] += scale * (0.5 * (m.zet.x[p] * f.fp(0, 0) + m.zet.y[p] * f.fp(0, 1) + m.zet.z[p] * f.fp(0, 2)) +
+                     0.5 * (m.zet.x[p + sz] * f.fp(3, 0) + m.zet.y[p + sz] * f.fp(3, 1) + m.zet.z[p + sz] * f.fp(3, 2))) *
+            m.kaj[p];
+    if (nv[p] + nv[p + 1] > 0 || (!g.iper && i == mx - 2)) r[0] = 0;
+    if (nv[p] + nv[p + sy] > 0 || (!g.jper && j == my - 2)) r[1] = 0;
+    if (nv[p] + nv[p + sz] > 0 || (!g.kper && k == mz - 2)) r[2] = 0;
+  }
+  if (!rk) {
+    rhs.x[p] = r[0]; rhs.y[p] = r[1]; rhs.z[p] = r[2];
+  } else {
+    r[0] = r[0] + -1 * dP.x[p];
+    r[1] = r[1] + -1 * dP.y[p];
+    r[2] = r[2] + -1 * dP.z[p];
+    rhs.x[p] = r[0]; rhs.y[p] = r[1]; rhs.z[p] = r[2];
+    if (ucont.x) {
+      ucont.x[p] = a * r[0] + pu.x[p];
+      ucont.y[p] = a * r[1] + pu.y[p];
+      ucont.z[p] = a * r[2] + pu.z[p];
+    }
+  }
+}
+
+// The stage update Ucont = pUcont + a * RHS (RHS already holding -dP) over every point.
+__global__ void k_rk_update(long long n, double a, CV3 rhs, CV3 pu, V3 ucont) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  ucont.x[p] = a * rhs.x[p] + pu.x[p];
+  ucont.y[p] = a * rhs.y[p] + pu.y[p];
+  ucont.z[p] = a * rhs.z[p] + pu.z[p];
+}
+
+struct GlobalFp {
+  const double *f[3];
+  long long q[4];
+  __device__ __forceinline__ double fp(int w, int c) const { return f[c][q[w]]; }
+};
 
 // Contravariant projection of Fp onto the faces, scale, masks and the boundary zeroing
 // of the right-hand side (momentum.c:1686-1900).  In RK mode the stage update
@@ -581,41 +821,165 @@ __global__ void k_rhs(Grid g, Metrics m, const uint8_t *__restrict__ nv, const d
   long long q = p / mx;
   int j = (int)(q % my);
   int k = (int)(q / my);
-  double r[3];
-  if (i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == mz - 1) {
-    r[0] = r[1] = r[2] = 0;
-  } else {
-    const long long sy = mx, sz = (long long)mx * my;
-    // Fp on the periodic ghost plane is the image of the first interior plane
-    const long long pi1 = (g.iper && i == mx - 2) ? p - i + 1 : p + 1;
-    const long long pj1 = (g.jper && j == my - 2) ? p - (long long)j * sy + sy : p + sy;
-    const long long pk1 = (g.kper && k == mz - 2) ? p - (long long)k * sz + sz : p + sz;
-    if (rk) { r[0] = 0; r[1] = 0; r[2] = 0; }
-    else { r[0] = rhs.x[p]; r[1] = rhs.y[p]; r[2] = rhs.z[p]; }
-    r[0] += scale * (0.5 * (m.csi.x[p] * fpx[p] + m.csi.y[p] * fpy[p] + m.csi.z[p] * fpz[p]) +
-                     0.5 * (m.csi.x[p + 1] * fpx[pi1] + m.csi.y[p + 1] * fpy[pi1] + m.csi.z[p + 1] * fpz[pi1])) *
-            m.iaj[p];
-    r[1] += scale * (0.5 * (m.eta.x[p] * fpx[p] + m.eta.y[p] * fpy[p] + m.eta.z[p] * fpz[p]) +
-                     0.5 * (m.eta.x[p + sy] * fpx[pj1] + m.eta.y[p + sy] * fpy[pj1] + m.eta.z[p + sy] * fpz[pj1])) *
-            m.jaj[p];
-    r[2] += scale * (0.5 * (m.zet.x[p] * fpx[p] + m.zet.y[p] * fpy[p] + m.zet.z[p] * fpz[p]) +
-                     0.5 * (m.zet.x[p + sz] * fpx[pk1] + m.zet.y[p + sz] * fpy[pk1] + m.zet.z[p + sz] * fpz[pk1])) *
-            m.kaj[p];
-    if (nv[p] + nv[p + 1] > 0 || (!g.iper && i == mx - 2)) r[0] = 0;
-    if (nv[p] + nv[p + sy] > 0 || (!g.jper && j == my - 2)) r[1] = 0;
-    if (nv[p] + nv[p + sz] > 0 || (!g.kper && k == mz - 2)) r[2] = 0;
+  const bool ghost = i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == mz - 1;
+  const long long sy = mx, sz = (long long)mx * my;
+  GlobalFp F;
+  F.f[0] = fpx; F.f[1] = fpy; F.f[2] = fpz;
+  // Fp on the periodic ghost plane is the image of the first interior plane
+  F.q[0] = p;
+  F.q[1] = (g.iper && i == mx - 2) ? p - i + 1 : p + 1;
+  F.q[2] = (g.jper && j == my - 2) ? p - (long long)j * sy + sy : p + sy;
+  F.q[3] = (g.kper && k == mz - 2) ? p - (long long)k * sz + sz : p + sz;
+  rhs_point(g, m, nv, p, i, j, k, ghost, F, scale, rhs, rk, a, dP, pu, ucont);
+}
+
+// ------------------------------------------------------------------ fused Formfunction_2
+// One kernel for the face fluxes, Fp and the right-hand side (with the RK stage update):
+// a thread block owns an FTI x FTJ tile of cells in (i, j) and marches through FKC planes
+// of k.  For the current plane kc it computes, into shared memory, the i-face fluxes
+// (faces i0-2 .. i0+FTI+1) and j-face fluxes of the tile extended by one cell on the high
+// side, plus the k-face fluxes of plane kc+1 (a ring of four k-face planes kc-2 .. kc+1);
+// then Fp of the extended tile at plane kc (a ring of two Fp planes); then the right-hand
+// side of plane kc-1.  Only the inputs (velocities, metrics, nvert, nu_t) and the outputs
+// travel through HBM.  Neighbouring tiles read Ucont in their halos, so in RK mode the
+// kernel writes only the right-hand side and k_rk_update applies the stage update after.  Face indices are handled unwrapped within the tile: on a periodic
+// direction a face or cell outside 1..m-2 is computed at its periodic image, which is the
+// value the reference reads there.  Every expression is the one of the three-kernel path,
+// so the results are identical.
+constexpr int FTI = 32, FTJ = 8, FKC = 16;
+constexpr int FEI = FTI + 1, FEJ = FTJ + 1, FE = FEI * FEJ;
+constexpr int FAI = FTI + 4, FBJ = FTJ + 4;
+constexpr int FNI = FAI * FEJ, FNJ = FEI * FBJ;
+constexpr int kFF2Threads = 256;
+struct FF2Smem {
+  double ifl[6][FNI];      // i-faces of plane kc: div x,y,z then visc x,y,z
+  double jfl[6][FNJ];      // j-faces of plane kc
+  double kfl[4][6][FE];    // k-faces, ring over planes kc-2 .. kc+1
+  double fp[2][3][FE];     // Fp, ring over planes kc-1, kc
+};
+
+// Image of a cell index (1..m-2 unchanged; m-1 -> 1 on a periodic direction), -1 if none.
+__device__ __forceinline__ int cell_image(int u, int m, int per) {
+  if (u >= 1 && u <= m - 2) return u;
+  if (per && u == m - 1) return 1;
+  return -1;
+}
+// Image of a face index, -1 if the face does not exist.
+__device__ __forceinline__ int face_image_or_none(int u, int m, int per) {
+  const int f = face_image(u, m, per);
+  return (f >= 0 && f <= m - 2) ? f : -1;
+}
+
+struct SmemFaces {
+  const FF2Smem *S;
+  int ei, ej, kc;
+  __device__ __forceinline__ double get(int dir, int q, int off) const {
+    if (dir == 0) return S->ifl[q][ej * FAI + ei + off + 2];
+    if (dir == 1) return S->jfl[q][(ej + off + 2) * FEI + ei];
+    return S->kfl[(kc + off + 4) & 3][q][ej * FEI + ei];
   }
-  if (!rk) {
-    rhs.x[p] = r[0]; rhs.y[p] = r[1]; rhs.z[p] = r[2];
-  } else {
-    r[0] = r[0] + -1 * dP.x[p];
-    r[1] = r[1] + -1 * dP.y[p];
-    r[2] = r[2] + -1 * dP.z[p];
-    rhs.x[p] = r[0]; rhs.y[p] = r[1]; rhs.z[p] = r[2];
-    ucont.x[p] = a * r[0] + pu.x[p];
-    ucont.y[p] = a * r[1] + pu.y[p];
-    ucont.z[p] = a * r[2] + pu.z[p];
+  __device__ __forceinline__ double d(int dir, int c, int off) const { return get(dir, c, off); }
+  __device__ __forceinline__ double v(int dir, int c, int off) const { return get(dir, 3 + c, off); }
+};
+struct SmemFp {
+  const FF2Smem *S;
+  int t, s0, s1;
+  __device__ __forceinline__ double fp(int w, int c) const {
+    if (w == 0) return S->fp[s0][c][t];
+    if (w == 1) return S->fp[s0][c][t + 1];
+    if (w == 2) return S->fp[s0][c][t + FEI];
+    return S->fp[s1][c][t];
   }
+};
+
+__device__ __forceinline__ void ff2_kfaces(const Grid &g, const Metrics &m, CV3 uc, CV3 u,
+                                           const uint8_t *__restrict__ nv, const double *__restrict__ nut,
+                                           FF2Smem &S, int i0, int j0, int kf) {
+  const int kimg = face_image_or_none(kf, g.mz, g.kper);
+  double (*dst)[FE] = S.kfl[(kf + 4) & 3];
+  for (int t = threadIdx.x; t < FE; t += blockDim.x) {
+    const int ei = t % FEI, ej = t / FEI;
+    const int ii = cell_image(i0 + ei, g.mx, g.iper), jj = cell_image(j0 + ej, g.my, g.jper);
+    double d[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+    if (ii >= 0 && jj >= 0 && kimg >= 0) flux_k(g, m, uc, u, nv, nut, lidx(g, ii, jj, kimg), ii, jj, kimg, d, v);
+    dst[0][t] = d[0]; dst[1][t] = d[1]; dst[2][t] = d[2];
+    dst[3][t] = v[0]; dst[4][t] = v[1]; dst[5][t] = v[2];
+  }
+}
+
+__global__ void __launch_bounds__(kFF2Threads) k_ff2_fused(Grid g, Metrics m, CV3 uc, CV3 u,
+                                                           const uint8_t *__restrict__ nv,
+                                                           const double *__restrict__ nut, double scale, V3 rhs,
+                                                           int rk, double a, CV3 dP, CV3 pu) {
+  extern __shared__ __align__(16) unsigned char ff2_raw[];
+  FF2Smem &S = *reinterpret_cast<FF2Smem *>(ff2_raw);
+  const int i0 = 1 + blockIdx.x * FTI, j0 = 1 + blockIdx.y * FTJ, kb = 1 + blockIdx.z * FKC;
+  const int ke = min(kb + FKC, g.mz - 1);  // output planes kb .. ke-1
+  for (int kf = kb - 2; kf <= kb; kf++) ff2_kfaces(g, m, uc, u, nv, nut, S, i0, j0, kf);
+  for (int kc = kb; kc <= ke; kc++) {
+    const int kimg = cell_image(kc, g.mz, g.kper);
+    // i-faces and j-faces of plane kc, k-faces of plane kc+1
+    for (int t = threadIdx.x; t < FNI; t += blockDim.x) {
+      const int a_ = t % FAI, ej = t / FAI;
+      const int fi = face_image_or_none(i0 - 2 + a_, g.mx, g.iper), jj = cell_image(j0 + ej, g.my, g.jper);
+      double d[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+      if (fi >= 0 && jj >= 0 && kimg >= 0) flux_i(g, m, uc, u, nv, nut, lidx(g, fi, jj, kimg), fi, jj, kimg, d, v);
+      S.ifl[0][t] = d[0]; S.ifl[1][t] = d[1]; S.ifl[2][t] = d[2];
+      S.ifl[3][t] = v[0]; S.ifl[4][t] = v[1]; S.ifl[5][t] = v[2];
+    }
+    for (int t = threadIdx.x; t < FNJ; t += blockDim.x) {
+      const int ei = t % FEI, b_ = t / FEI;
+      const int ii = cell_image(i0 + ei, g.mx, g.iper), fj = face_image_or_none(j0 - 2 + b_, g.my, g.jper);
+      double d[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+      if (ii >= 0 && fj >= 0 && kimg >= 0) flux_j(g, m, uc, u, nv, nut, lidx(g, ii, fj, kimg), ii, fj, kimg, d, v);
+      S.jfl[0][t] = d[0]; S.jfl[1][t] = d[1]; S.jfl[2][t] = d[2];
+      S.jfl[3][t] = v[0]; S.jfl[4][t] = v[1]; S.jfl[5][t] = v[2];
+    }
+    ff2_kfaces(g, m, uc, u, nv, nut, S, i0, j0, kc + 1);
+    __syncthreads();
+    // Fp of the extended tile at plane kc
+    for (int t = threadIdx.x; t < FE; t += blockDim.x) {
+      const int ei = t % FEI, ej = t / FEI;
+      const int ii = cell_image(i0 + ei, g.mx, g.iper), jj = cell_image(j0 + ej, g.my, g.jper);
+      double fpv[3] = {0, 0, 0};
+      if (ii >= 0 && jj >= 0 && kimg >= 0) {
+        SmemFaces F;
+        F.S = &S; F.ei = ei; F.ej = ej; F.kc = kc;
+        fp_cell(g, nv, lidx(g, ii, jj, kimg), ii, jj, kimg, F, fpv);
+      }
+      S.fp[kc & 1][0][t] = fpv[0]; S.fp[kc & 1][1][t] = fpv[1]; S.fp[kc & 1][2][t] = fpv[2];
+    }
+    __syncthreads();
+    // right-hand side of plane kc-1
+    if (kc > kb) {
+      const int k = kc - 1;
+      for (int t = threadIdx.x; t < FTI * FTJ; t += blockDim.x) {
+        const int oi = t % FTI, oj = t / FTI;
+        const int i = i0 + oi, j = j0 + oj;
+        if (i > g.mx - 2 || j > g.my - 2) continue;
+        SmemFp F;
+        F.S = &S; F.t = oj * FEI + oi; F.s0 = k & 1; F.s1 = kc & 1;
+        rhs_point(g, m, nv, lidx(g, i, j, k), i, j, k, false, F, scale, rhs, rk, a, dP, pu, V3{nullptr, nullptr, nullptr});
+      }
+    }
+  }
+}
+
+// Ghost points of the right-hand side (zero, and the stage update in RK mode).
+__global__ void k_rhs_ghosts(Grid g, Metrics m, const uint8_t *__restrict__ nv, double scale, V3 rhs, int rk,
+                             double a, CV3 dP, CV3 pu) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long ni = 2LL * g.my * g.mz, nj = 2LL * g.mx * g.mz, nk = 2LL * g.mx * g.my;
+  if (t >= ni + nj + nk) return;
+  long long r = t;
+  int i, j, k;
+  if (r < ni) { i = (r & 1) ? g.mx - 1 : 0; r >>= 1; j = (int)(r % g.my); k = (int)(r / g.my); }
+  else if ((r -= ni) < nj) { j = (r & 1) ? g.my - 1 : 0; r >>= 1; i = (int)(r % g.mx); k = (int)(r / g.mx); }
+  else { r -= nj; k = (r & 1) ? g.mz - 1 : 0; r >>= 1; i = (int)(r % g.mx); j = (int)(r / g.mx); }
+  GlobalFp F;  // unused for ghost points
+  F.f[0] = F.f[1] = F.f[2] = nullptr;
+  F.q[0] = F.q[1] = F.q[2] = F.q[3] = 0;
+  rhs_point(g, m, nv, lidx(g, i, j, k), i, j, k, true, F, scale, rhs, rk, a, dP, pu, V3{nullptr, nullptr, nullptr});
 }
 
 static FluxOut flux_out(Ctx *c, int d) {
@@ -629,6 +993,10 @@ static FluxIn flux_in(Ctx *c, int d) {
   return f;
 }
 
+// Formfunction_2 as three kernels: face fluxes, Fp, right-hand side (with the RK stage
+// update).  The single-kernel form (formfunction2_fused) gives the same results; on the
+// B200 it is slower at this tile size (its block barriers leave it latency-bound), so
+// the step uses this one.
 int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   const Grid &g = c->g;
   int rc;
@@ -647,6 +1015,35 @@ int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
                                                  field3(c, VFS_RHS), rk_stage ? 1 : 0, rk_coeff,
                                                  cv(field3(c, VFS_DP)), cv(pu), uc);
   return check_launch(c, "k_rhs");
+}
+
+int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
+  const Grid &g = c->g;
+  int rc;
+  V3 uc = field3(c, VFS_UCONT);
+  if ((rc = periodic_copy3(c, uc))) return rc;
+  Metrics m = metrics(c);
+  V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_ff2_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FF2Smem));
+    attr = true;
+  }
+  dim3 grid((g.mx - 2 + FTI - 1) / FTI, (g.my - 2 + FTJ - 1) / FTJ, (g.mz - 2 + FKC - 1) / FKC);
+  k_ff2_fused<<<grid, kFF2Threads, sizeof(FF2Smem), c->stream>>>(g, m, cv(uc), cv(field3(c, VFS_UCAT)), c->nv,
+                                                               c->f[VFS_NU_T][0], scale, field3(c, VFS_RHS),
+                                                               rk_stage ? 1 : 0, rk_coeff, cv(field3(c, VFS_DP)),
+                                                               cv(pu));
+  if ((rc = check_launch(c, "k_ff2_fused"))) return rc;
+  const long long ng = 2LL * g.my * g.mz + 2LL * g.mx * g.mz + 2LL * g.mx * g.my;
+  k_rhs_ghosts<<<nblocks(ng, 256), 256, 0, c->stream>>>(g, m, c->nv, scale, field3(c, VFS_RHS), rk_stage ? 1 : 0,
+                                                       rk_coeff, cv(field3(c, VFS_DP)), cv(pu));
+  if ((rc = check_launch(c, "k_rhs_ghosts"))) return rc;
+  if (rk_stage) {
+    k_rk_update<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, rk_coeff, cv(field3(c, VFS_RHS)), cv(pu), uc);
+    if ((rc = check_launch(c, "k_rk_update"))) return rc;
+  }
+  return VFS_OK;
 }
 
 // single-kernel launchers for the diagnostics entry point (vfs_run_kernel)
@@ -959,7 +1356,10 @@ int runge_kutta(Ctx *c) {
   for (int q = 0; q < 3; q++)
     cudaMemcpyAsync(c->pucont[q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
   for (int s = 0; s < 4; s++) {
-    if ((rc = contra2cart(c))) return rc;
+    // the reference converts at the start and at the end of every stage; the start of
+    // stage s > 0 sees exactly the Ucont the end of stage s-1 converted, and Contra2Cart
+    // of the same Ucont reproduces the same Ucat, so only stage 0 converts first
+    if (s == 0 && (rc = contra2cart(c))) return rc;
     const double a = alfa[s] * c->g.dt * c->g.st;
     if ((rc = formfunction2(c, 1.0, true, a))) return rc;
     if ((rc = contra2cart(c))) return rc;

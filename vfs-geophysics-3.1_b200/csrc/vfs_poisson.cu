@@ -269,24 +269,38 @@ __device__ __forceinline__ void block_sums(const double (&acc)[NV + 1], int nv, 
   }
 }
 
-// w = A z, with <V_t, w> (t < nv) and <w, w>.
-template <int NS, int NV>
-__global__ void __launch_bounds__(kKryThreads) k_apply_dots(Grid g, const double *__restrict__ coef,
-                                                            const double *__restrict__ z, double *__restrict__ w,
-                                                            const double *__restrict__ V, int nv,
-                                                            double *__restrict__ parts) {
+// The Krylov kernels below stream the basis two points at a time (16-byte loads): the
+// basis vectors are stored ldv apart, ldv a multiple of 32, and every other vector is a
+// separate allocation, so pair loads are aligned; an odd last point is done alone.
+
+// <V_t, w> (t < nv) and <w, w>.
+template <int NV>
+__global__ void __launch_bounds__(kKryThreads) k_multidot(long long N, long long ldv, const double *__restrict__ V,
+                                                          int nv, const double *__restrict__ w,
+                                                          double *__restrict__ parts) {
   double acc[NV + 1];
 #pragma unroll
   for (int t = 0; t <= NV; t++) acc[t] = 0;
-  const long long N = g.N, stride = (long long)gridDim.x * blockDim.x;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
-    double v[NV];
+  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
+  for (long long p2 = tid; p2 < N2; p2 += stride) {
+    const double2 wp = w2[p2];
 #pragma unroll
-    for (int t = 0; t < NV; t++) v[t] = t < nv ? V[t * N + p] : 0.0;
-    const double wp = apply_row64<NS>(g, coef, z, p);
-    w[p] = wp;
+    for (int t = 0; t < NV; t++) {
+      if (t < nv) {
+        const double2 v = reinterpret_cast<const double2 *>(V + t * ldv)[p2];
+        acc[t] += v.x * wp.x + v.y * wp.y;
+      }
+    }
+    acc[NV] += wp.x * wp.x + wp.y * wp.y;
+  }
+  if ((N & 1) && tid == 0) {
+    const long long p = N - 1;
+    const double wp = w[p];
 #pragma unroll
-    for (int t = 0; t < NV; t++) acc[t] += v[t] * wp;
+    for (int t = 0; t < NV; t++)
+      if (t < nv) acc[t] += V[t * ldv + p] * wp;
     acc[NV] += wp * wp;
   }
   block_sums<NV>(acc, nv, parts);
@@ -294,25 +308,40 @@ __global__ void __launch_bounds__(kKryThreads) k_apply_dots(Grid g, const double
 
 // w -= sum_t h_t V_t, with <V_t, w> (t < nv) and <w, w> of the result.
 template <int NV>
-__global__ void __launch_bounds__(kKryThreads) k_update_dots(long long N, const double *__restrict__ V, int nv,
-                                                             const double *__restrict__ h, double *__restrict__ w,
-                                                             double *__restrict__ parts) {
+__global__ void __launch_bounds__(kKryThreads) k_update_dots(long long N, long long ldv, const double *__restrict__ V,
+                                                             int nv, const double *__restrict__ h,
+                                                             double *__restrict__ w, double *__restrict__ parts) {
   double hr[NV], acc[NV + 1];
 #pragma unroll
   for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
 #pragma unroll
   for (int t = 0; t <= NV; t++) acc[t] = 0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
-    double v[NV];
+  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double2 *__restrict__ w2 = reinterpret_cast<double2 *>(w);
+  for (long long p2 = tid; p2 < N2; p2 += stride) {
+    double2 v[NV];
 #pragma unroll
-    for (int t = 0; t < NV; t++) v[t] = t < nv ? V[t * N + p] : 0.0;
+    for (int t = 0; t < NV; t++)
+      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
+    double2 s = w2[p2];
+#pragma unroll
+    for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
+    w2[p2] = s;
+#pragma unroll
+    for (int t = 0; t < NV; t++) acc[t] += v[t].x * s.x + v[t].y * s.y;
+    acc[NV] += s.x * s.x + s.y * s.y;
+  }
+  if ((N & 1) && tid == 0) {
+    const long long p = N - 1;
     double s = w[p];
 #pragma unroll
-    for (int t = 0; t < NV; t++) s -= hr[t] * v[t];
+    for (int t = 0; t < NV; t++)
+      if (t < nv) s -= hr[t] * V[t * ldv + p];
     w[p] = s;
 #pragma unroll
-    for (int t = 0; t < NV; t++) acc[t] += v[t] * s;
+    for (int t = 0; t < NV; t++)
+      if (t < nv) acc[t] += V[t * ldv + p] * s;
     acc[NV] += s * s;
   }
   block_sums<NV>(acc, nv, parts);
@@ -320,21 +349,34 @@ __global__ void __launch_bounds__(kKryThreads) k_update_dots(long long N, const 
 
 // out = (w - sum_t h_t V_t) * scale.
 template <int NV>
-__global__ void __launch_bounds__(kKryThreads) k_update_scale(long long N, const double *__restrict__ V, int nv,
-                                                              const double *__restrict__ h,
+__global__ void __launch_bounds__(kKryThreads) k_update_scale(long long N, long long ldv, const double *__restrict__ V,
+                                                              int nv, const double *__restrict__ h,
                                                               const double *__restrict__ w, double scale,
                                                               double *__restrict__ out) {
   double hr[NV];
 #pragma unroll
   for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
-    double v[NV];
+  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
+  double2 *__restrict__ o2 = reinterpret_cast<double2 *>(out);
+  for (long long p2 = tid; p2 < N2; p2 += stride) {
+    double2 v[NV];
 #pragma unroll
-    for (int t = 0; t < NV; t++) v[t] = t < nv ? V[t * N + p] : 0.0;
+    for (int t = 0; t < NV; t++)
+      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
+    double2 s = w2[p2];
+#pragma unroll
+    for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
+    s.x *= scale; s.y *= scale;
+    o2[p2] = s;
+  }
+  if ((N & 1) && tid == 0) {
+    const long long p = N - 1;
     double s = w[p];
 #pragma unroll
-    for (int t = 0; t < NV; t++) s -= hr[t] * v[t];
+    for (int t = 0; t < NV; t++)
+      if (t < nv) s -= hr[t] * V[t * ldv + p];
     out[p] = s * scale;
   }
 }
@@ -374,12 +416,12 @@ __global__ void k_scale_copy(long long n, const double *a, double s, double *b) 
   if (p < n) b[p] = a[p] * s;
 }
 // x += sum_i y_i Z_i
-__global__ void k_lincomb_add(long long n, const double *__restrict__ Z, int m, const double *__restrict__ y,
-                              double *__restrict__ x) {
+__global__ void k_lincomb_add(long long n, long long ldv, const double *__restrict__ Z, int m,
+                              const double *__restrict__ y, double *__restrict__ x) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= n) return;
   double s = x[p];
-  for (int t = 0; t < m; t++) s += y[t] * Z[(long long)t * n + p];
+  for (int t = 0; t < m; t++) s += y[t] * Z[(long long)t * ldv + p];
   x[p] = s;
 }
 
@@ -398,32 +440,26 @@ static int finish_rows(Ctx *c, int nrows, double *out) {
   return VFS_OK;
 }
 
-template <int NS>
-static void launch_apply_dots(Ctx *c, const double *z, double *w, const double *V, int nv) {
-  const Grid &g = c->g;
-  const double *cf = c->ps.coef;
-  if (nv <= 4) k_apply_dots<NS, 4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
-  else if (nv <= 8) k_apply_dots<NS, 8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
-  else if (nv <= 16) k_apply_dots<NS, 16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
-  else k_apply_dots<NS, 32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(g, cf, z, w, V, nv, c->red);
-}
-
 // w = A z; h[0..nv-1] = <V_t, w>; h[nv] = <w, w>.
 static int apply_dots(Ctx *c, const double *z, double *w, const double *V, int nv, double *h) {
-  if (c->ps.nslot == 7) launch_apply_dots<7>(c, z, w, V, nv);
-  else launch_apply_dots<NSLOT>(c, z, w, V, nv);
   int rc;
-  if ((rc = check_launch(c, "k_apply_dots"))) return rc;
+  if ((rc = poisson_apply_dev(c, z, w))) return rc;
+  const long long N = c->g.N, ldv = c->ps.ldv;
+  if (nv <= 4) k_multidot<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else if (nv <= 8) k_multidot<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else if (nv <= 16) k_multidot<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else k_multidot<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  if ((rc = check_launch(c, "k_multidot"))) return rc;
   return finish_rows(c, nv + 1, h);
 }
 
 // w -= V h (h on the device); out[0..nv-1] = <V_t, w>; out[nv] = <w, w>.
 static int update_dots(Ctx *c, const double *V, int nv, const double *hdev, double *w, double *out) {
-  const long long N = c->g.N;
-  if (nv <= 4) k_update_dots<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
-  else if (nv <= 8) k_update_dots<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
-  else if (nv <= 16) k_update_dots<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
-  else k_update_dots<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, c->red);
+  const long long N = c->g.N, ldv = c->ps.ldv;
+  if (nv <= 4) k_update_dots<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else if (nv <= 8) k_update_dots<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else if (nv <= 16) k_update_dots<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else k_update_dots<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
   int rc;
   if ((rc = check_launch(c, "k_update_dots"))) return rc;
   return finish_rows(c, nv + 1, out);
@@ -432,11 +468,12 @@ static int update_dots(Ctx *c, const double *V, int nv, const double *hdev, doub
 // out = (w - V h) * scale (h on the device).
 static int update_scale(Ctx *c, const double *V, int nv, const double *hdev, const double *w, double scale,
                         double *out) {
-  const long long N = c->g.N;
-  if (nv <= 4) k_update_scale<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
-  else if (nv <= 8) k_update_scale<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
-  else if (nv <= 16) k_update_scale<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
-  else k_update_scale<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, V, nv, hdev, w, scale, out);
+  const long long N = c->g.N, ldv = c->ps.ldv;
+  if (nv <= 4) k_update_scale<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  else if (nv <= 8) k_update_scale<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  else if (nv <= 16)
+    k_update_scale<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  else k_update_scale<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
   return check_launch(c, "k_update_scale");
 }
 
@@ -652,7 +689,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   vfs_solve_opts o;
   memset(&o, 0, sizeof(o));
   o.precision = 0; o.restart = 30; o.max_iter = 200; o.levels = 0; o.pre_smooth = 2; o.post_smooth = 2;
-  o.coarse_iters = 16; o.rtol = 1e-10; o.atol = 0.0;
+  o.coarse_iters = 4; o.rtol = 1e-10; o.atol = 0.0;
   if (oin) {
     o.precision = oin->precision;
     if (oin->restart > 0) o.restart = oin->restart;
@@ -673,8 +710,9 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   if (P.restart < o.restart) {
     cudaFree(P.V); cudaFree(P.Z);
     P.V = P.Z = nullptr;
-    if (cudaMalloc(&P.V, sizeof(double) * N * (o.restart + 1)) != cudaSuccess ||
-        cudaMalloc(&P.Z, sizeof(double) * N * o.restart) != cudaSuccess)
+    P.ldv = (N + 31) / 32 * 32;
+    if (cudaMalloc(&P.V, sizeof(double) * P.ldv * (o.restart + 1)) != cudaSuccess ||
+        cudaMalloc(&P.Z, sizeof(double) * P.ldv * o.restart) != cudaSuccess)
       return set_err(c, VFS_ERR_CUDA, "poisson_solve: Krylov basis allocation failed");
     P.restart = o.restart;
   }
@@ -709,7 +747,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
     int jdone = 0;
     for (int j = 0; j < m && it < o.max_iter; j++) {
       const int nv = j + 1;
-      double *Vj = P.V + (long long)j * N, *Zj = P.Z + (long long)j * N;
+      double *Vj = P.V + (long long)j * P.ldv, *Zj = P.Z + (long long)j * P.ldv;
       if ((rc = mg_precondition(c, Vj, Zj, o))) return rc;
       // classical Gram-Schmidt with one re-orthogonalisation, three passes over V:
       // (1) w = A z_j and h = V^T w; (2) w -= V h and h2 = V^T w; (3) v_{j+1} = (w - V h2)/|.|
@@ -722,7 +760,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       upload_h(c, h2.data(), nv, P.hdev);
       for (int t = 0; t < nv; t++) H[t * m + j] = h[t] + h2[t];
       double hn;
-      double *Vn = P.V + (long long)(j + 1) * N;
+      double *Vn = P.V + (long long)(j + 1) * P.ldv;
       if (hn2 > 1e-4 * ww) {
         hn = sqrt(hn2);
         if ((rc = update_scale(c, P.V, nv, P.hdev, P.w, 1.0 / hn, Vn))) return rc;
@@ -763,7 +801,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       y[t] = sum / H[t * m + t];
     }
     upload_h(c, y.data(), jdone, P.hdev);
-    k_lincomb_add<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.Z, jdone, P.hdev, x);
+    k_lincomb_add<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z, jdone, P.hdev, x);
     if ((rc = check_launch(c, "k_lincomb_add"))) return rc;
     if (rnorm <= tol) {
       // confirm with the true residual
@@ -980,6 +1018,8 @@ int run_kernel(Ctx *c, int which, int reps) {
         break;
       case 4: rc = mg_sweep_fine(c, 0); if (rc) return rc; break;
       case 5: rc = mg_sweep_fine(c, 1); if (rc) return rc; break;
+      case 7: rc = formfunction2_fused(c, 1.0, false, 0.0); if (rc) return rc; break;
+      case 8: rc = formfunction2(c, 1.0, false, 0.0); if (rc) return rc; break;
       case 6:
         k_projection<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->f[VFS_PHI][0], field3(c, VFS_UCONT));
         break;
