@@ -22,6 +22,7 @@ reference, is scipy GMRES with an incomplete-LU preconditioner on the reference'
 matrix) on a bounded sample of the workload and scales it to the full grid.
 """
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -58,6 +59,26 @@ def hbm_peak():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null while the reference's C code runs (it prints
+    progress lines with printf, e.g. poisson.c:262), so stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.libc = ctypes.CDLL(None)
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        dn = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(dn, 1)
+        os.close(dn)
+        return self
+
+    def __exit__(self, *a):
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
 
 
 # ------------------------------------------------------------------ workload
@@ -179,6 +200,12 @@ def timed(ctx, fn, reps, torch):
 
 # Algorithmic bytes per interior cell of the profiled kernels (compulsory traffic: each
 # input read once, each output written once, at the stored precision, nvert as 1 byte).
+# DRAM bytes (read + write) per launch of the profiled kernels from one ncu capture at
+# 128x96x128 cells, scaled by the cell ratio (x8) to 256x192x256 (profiles/
+# formfunction2_128x96x128.md): Formfunction_2 as the step runs it (k_face_flux, k_fp,
+# k_rhs) moved 1271.3 MB per launch there.
+KERNEL_TRAFFIC = {"formfunction2": 1271.3e6 * 8}
+
 KERNEL_BYTES = {
     # Formfunction_2 accumulating into Rhs (Formfunction_2(user, Rhs, scale) adds):
     # Ucont 24 + Ucat 24 + nvert 1 + nu_t 8 + face metrics 240 + centre metrics 72 +
@@ -223,7 +250,7 @@ def reference_sample(nx=32, ny=24, nz=32, seed=0):
     """One reference step (oracle/_ref) on a 32x24x32 sample of the workload, one host
     thread; returns (ms for the sample, cells in the sample)."""
     from threadpoolctl import threadpool_limits
-    with threadpool_limits(limits=1):
+    with threadpool_limits(limits=1), quiet_stdout():
         return _reference_sample(nx, ny, nz, seed)
 
 
@@ -442,7 +469,8 @@ def main():
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms/step", "h2d_bytes_per_step": io_bytes,
                     "d2h_bytes_per_step": io_bytes},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None, "kernel": dom,
+                         "frac": round(achieved / peak, 4),
+                         "traffic": KERNEL_TRAFFIC.get(dom), "traffic_unit": "bytes per launch", "kernel": dom,
                          "peak_source": peak_kind, "bytes_per_cell": KERNEL_BYTES[dom],
                          "ms_per_launch": round(launch[dom], 4),
                          "other_ms_per_launch": {k: round(v, 4) for k, v in launch.items()}},

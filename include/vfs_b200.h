@@ -38,9 +38,13 @@ typedef struct {
   int bctype[6];         /* bcs.dat codes: i-, i+, j-, j+, k-, k+ */
   int i_periodic, j_periodic, k_periodic; /* main.c:191-195 */
   int immersed;          /* -imm: 0 none, 1 sharp-interface IB (nvert masking + QUICK) */
-  int les;               /* -les: 0 laminar, 2 dynamic Smagorinsky eddy viscosity */
+  int les;               /* -les: 0 laminar, 1 constant Cs = 0.01, 2 dynamic Smagorinsky */
   int inletprofile;      /* -inlet (bcs.c:399-466) */
-  int reserved_i[8];
+  int dynamic_freq;      /* -dynamic_freq: Cs recomputed when ti % dynamic_freq == 0 or ti ==
+                            tistart (main.c:1747, solvers.c:652); values < 1 mean 1 */
+  int tistart;           /* index of the first time step (main.c:5, -rstart) */
+  int rstart;            /* non-zero for a restarted run (rstart_flg, main.c:1608) */
+  int reserved_i[5];
   double ren;            /* Reynolds number (user->ren) */
   double dt;             /* time step (user->dt) */
   double st;             /* Strouhal scaling (user->st) */
@@ -48,7 +52,9 @@ typedef struct {
   double mean_pressure_gradient; /* -mean_pressure_gradient (main.c) */
   int dpdz_set;          /* non-zero: impose mean_pressure_gradient (momentum.c:379) */
   int reserved_j[7];
-  double reserved_d[8];
+  double max_cs;         /* -max_cs upper clip of Cs (main.c:216, default 0.5; values <= 0
+                            select the default) */
+  double reserved_d[7];
 } vfs_config;
 
 /* Field identifiers for vfs_set_field / vfs_get_field (dof in brackets). */
@@ -80,7 +86,8 @@ enum {
   VFS_S_INLET_FLUX = 2,   /* inlet_flux global */
   VFS_S_INLET_AREA = 3,   /* inletArea (bcs.c:212) */
   VFS_S_DT = 4, VFS_S_REN = 5, VFS_S_ST = 6,
-  VFS_NSCALARS = 7
+  VFS_S_TI = 7,           /* time step index ti (main.c:3534); vfs_step advances it */
+  VFS_NSCALARS = 8
 };
 
 /* Poisson solver options (replaces PoissonSolver_Hypre, poisson_hypre.c:498). */
@@ -150,6 +157,15 @@ int vfs_formfunction2(vfs_ctx *ctx, double scale);
 /* Pressure_Gradient(user, dP) (momentum.c:197): writes VFS_DP. */
 int vfs_pressure_gradient(vfs_ctx *ctx);
 
+/* Compute_Smagorinsky_Constant_1(user, lUcont, lUcat) (les.c:67): dynamic Smagorinsky
+ * coefficient from VFS_UCAT -> VFS_CS.  Zero while ti < 2 on a fresh run, 0.01 for les = 1,
+ * else the Germano-identity least-squares value with the 3-D box test filter, clipped to
+ * [0, max_cs] with the wall floor 0.001 at IB nodes and filtered once more. */
+int vfs_smagorinsky_constant(vfs_ctx *ctx);
+
+/* Compute_eddy_viscosity_LES (les.c:1135): VFS_NU_T = Cs * (1/aj)^(2/3) * |S|. */
+int vfs_eddy_viscosity(vfs_ctx *ctx);
+
 /* Calc_k_Flux (rhs2.c:1562): mean k-face flux -> VFS_S_MEAN_K_FLUX. */
 int vfs_calc_k_flux(vfs_ctx *ctx, double *mean_k_flux);
 
@@ -199,9 +215,11 @@ int vfs_projection(vfs_ctx *ctx);
  * neighbourhood. */
 int vfs_divergence(vfs_ctx *ctx, double *max_div);
 
-/* One projection time step: Calc_k_Flux, Pressure_Gradient, RungeKutta, Poisson
- * (RHS, solve), UpdatePressure, Projection, Divergence (solvers.c:562-1390 for
- * implicit=0).  opts may be NULL for the defaults. */
+/* One projection time step: Calc_k_Flux, the eddy viscosity when les != 0
+ * (Contra2Cart, Compute_Smagorinsky_Constant_1 every dynamic_freq steps,
+ * Compute_eddy_viscosity_LES), Pressure_Gradient, RungeKutta, Poisson (RHS, solve),
+ * UpdatePressure, Projection, Divergence (solvers.c:562-1390 for implicit=0); then ti
+ * advances by one.  opts may be NULL for the defaults. */
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
 
 /* ---- allocation-free variant ---------------------------------------------------- */

@@ -137,3 +137,13 @@ def projection(st, phi):
 
 def divergence(st):
     return lib().og_divergence(ctypes.byref(st.g), _p(st.ucont), _p(st.m["aj"]), _p(st.nvert))
+
+
+def les(st, ti=5, tistart=0, rstart=0, max_cs=0.5, cs=None):
+    """Compute_Smagorinsky_Constant_1 + Compute_eddy_viscosity_LES (les.c:67-1252) on the
+    state's Ucat; returns Cs and updates st.nut in place."""
+    cs = np.zeros(st.case.da_shape) if cs is None else np.array(cs, dtype=np.float64)
+    lib().og_les(ctypes.byref(st.g), _p(st.ucat), _p(st.m["csi"]), _p(st.m["eta"]), _p(st.m["zet"]),
+                 _p(st.m["aj"]), _p(st.nvert), ctypes.c_int(ti), ctypes.c_int(tistart), ctypes.c_int(rstart),
+                 ctypes.c_double(max_cs), _p(cs), _p(st.nut))
+    return cs

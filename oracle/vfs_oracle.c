@@ -766,3 +766,262 @@ double og_divergence(const og_grid *g, const double *ucont, const double *aj, co
       }
   return mx_;
 }
+
+/* ------------------------------------------------------------------ dynamic Smagorinsky
+ * Compute_Smagorinsky_Constant_1 (les.c:67-1133) with testfilter_ik = 0, clark = 0 and no
+ * homogeneous-direction averaging, then Compute_eddy_viscosity_LES (les.c:1135-1252).
+ * ucat: the Contra2Cart output with its ghost values; cs and nut are updated in place
+ * (nut keeps its values on non-periodic ghost points, as lNu_t does). */
+static void les_du_center(const og_grid *g, const double *u, const double *nv, int i, int j, int k, double d[9]) {
+  /* Compute_du_center, k-omega.c:305-420 (note k == 0 in the lower k test, k-omega.c:395) */
+  int a0[3], b0[3];
+  double f;
+  for (int c = 0; c < 3; c++) {
+    int ia = i, ib = i, ja = j, jb = j, ka = k, kb = k;
+    if (c == 0) {
+      if (S(nv, g, i + 1, j, k) > 0.1 || (!g->iper && i == g->mx - 2)) { ib = i - 1; f = 1; }
+      else if (S(nv, g, i - 1, j, k) > 0.1 || (!g->iper && i == 1)) { ia = i + 1; f = 1; }
+      else { ia = i + 1; ib = i - 1; f = 0.5; }
+    } else if (c == 1) {
+      if (S(nv, g, i, j + 1, k) > 0.1 || (!g->jper && j == g->my - 2)) { jb = j - 1; f = 1; }
+      else if (S(nv, g, i, j - 1, k) > 0.1 || (!g->jper && j == 1)) { ja = j + 1; f = 1; }
+      else { ja = j + 1; jb = j - 1; f = 0.5; }
+    } else {
+      if (S(nv, g, i, j, k + 1) > 0.1 || (!g->kper && k == g->mz - 2)) { kb = k - 1; f = 1; }
+      else if (S(nv, g, i, j, k - 1) > 0.1 || (!g->kper && k == 0)) { ka = k + 1; f = 1; }
+      else { ka = k + 1; kb = k - 1; f = 0.5; }
+    }
+    for (int v = 0; v < 3; v++) {
+      double diff = V(u, g, ia, ja, ka, v) - V(u, g, ib, jb, kb, v);
+      d[3 * c + v] = (f == 1) ? diff : diff * 0.5;
+    }
+    (void)a0; (void)b0;
+  }
+}
+
+static void les_grad(const double *c, const double *e, const double *z, double ajc, const double d[9], double o[9]) {
+  /* Compute_du_dxyz, k-omega.c:597-610; o = du/dx du/dy du/dz dv/dx ... dw/dz */
+  for (int v = 0; v < 3; v++)
+    for (int x = 0; x < 3; x++) o[3 * v + x] = (d[v] * c[x] + d[3 + v] * e[x] + d[6 + v] * z[x]) * ajc;
+}
+
+static double les_strain(const double o[9], double s[3][3]) {
+  s[0][0] = 0.5 * (o[0] + o[0]); s[0][1] = 0.5 * (o[1] + o[3]); s[0][2] = 0.5 * (o[2] + o[6]);
+  s[1][0] = s[0][1]; s[1][1] = 0.5 * (o[4] + o[4]); s[1][2] = 0.5 * (o[5] + o[7]);
+  s[2][0] = s[0][2]; s[2][1] = s[1][2]; s[2][2] = 0.5 * (o[8] + o[8]);
+  return sqrt(2.0 * (s[0][0] * s[0][0] + s[0][1] * s[0][1] + s[0][2] * s[0][2] + s[1][0] * s[1][0] +
+                     s[1][1] * s[1][1] + s[1][2] * s[1][2] + s[2][0] * s[2][0] + s[2][1] * s[2][1] +
+                     s[2][2] * s[2][2]));
+}
+
+/* integrate_testfilter (rhs2.c:412-455), val/w indexed [R][Q][P] = [k][j][i] offsets + 1 */
+static double les_filter(double val[3][3][3], double w[3][3][3]) {
+  double vt = 0, wt = 0;
+  for (int s = 0; s < 8; s++) {
+    const int R0 = s & 1, P0 = (s >> 1) & 1, Q0 = (s >> 2) & 1;
+    double vs = 0, ws = 0;
+    for (int m = 0; m < 8; m++) {
+      const int R = R0 + (m & 1), P = P0 + ((m >> 1) & 1), Q = Q0 + ((m >> 2) & 1);
+      vs = m ? vs + val[R][Q][P] * w[R][Q][P] : val[R][Q][P] * w[R][Q][P];
+      ws = m ? ws + w[R][Q][P] : w[R][Q][P];
+    }
+    vt = s ? vt + vs : vs;
+    wt = s ? wt + ws : ws;
+  }
+  return vt / wt;
+}
+
+static void les_inverse(const double a[3][3], double G[3][3]) {
+  /* Calculate_Covariant_metrics, rhs2.c:538-554 */
+  const double a11 = a[0][0], a12 = a[0][1], a13 = a[0][2], a21 = a[1][0], a22 = a[1][1], a23 = a[1][2];
+  const double a31 = a[2][0], a32 = a[2][1], a33 = a[2][2];
+  const double det = a11 * (a33 * a22 - a32 * a23) - a21 * (a33 * a12 - a32 * a13) + a31 * (a23 * a12 - a22 * a13);
+  G[0][0] = (a33 * a22 - a32 * a23) / det; G[0][1] = -(a33 * a12 - a32 * a13) / det; G[0][2] = (a23 * a12 - a22 * a13) / det;
+  G[1][0] = -(a33 * a21 - a31 * a23) / det; G[1][1] = (a33 * a11 - a31 * a13) / det; G[1][2] = -(a23 * a11 - a21 * a13) / det;
+  G[2][0] = (a32 * a21 - a31 * a22) / det; G[2][1] = -(a32 * a11 - a31 * a12) / det; G[2][2] = (a22 * a11 - a21 * a12) / det;
+}
+
+/* weights of the LM/MM averaging and of the Cs re-filter (les.c:720-762, 1069-1110) */
+static void les_wrap_weights(const og_grid *g, const double *aj, const double *nv, int i, int j, int k,
+                             double w[3][3][3], int src[3][3][3]) {
+  for (int a = -1; a <= 1; a++)
+    for (int b = -1; b <= 1; b++)
+      for (int c = -1; c <= 1; c++) {
+        int I = i + a, J = j + b, K = k + c;
+        double wt = 1. / S(aj, g, I, J, K);
+        if (S(nv, g, I, J, K) > 1.1) wt = 0;
+        if (g->iper) { if (I == 0) I = g->mx - 2; else if (I == g->mx - 1) I = 1; }
+        else if (I == 0 || I == g->mx - 1) wt = 0;
+        if (g->jper) { if (J == 0) J = g->my - 2; else if (J == g->my - 1) J = 1; }
+        else if (J == 0 || j == g->my - 1) wt = 0;
+        if (g->kper) { if (K == 0) K = g->mz - 2; else if (K == g->mz - 1) K = 1; }
+        else if (K == 0 || K == g->mz - 1) wt = 0;
+        w[c + 1][b + 1][a + 1] = wt;
+        src[c + 1][b + 1][a + 1] = (int)IX(g, I, J, K);
+      }
+}
+
+void og_les(const og_grid *g, const double *ucat, const double *csi, const double *eta, const double *zet,
+            const double *aj, const double *nv, int ti, int tistart, int rstart, double max_cs, double *cs,
+            double *nut) {
+  const size_t N = (size_t)g->mx * g->my * g->mz;
+  const int mx = g->mx, my = g->my, mz = g->mz;
+  if (ti < 2 && tistart == 0 && !rstart) {
+    memset(cs, 0, 8 * N);
+  } else if (g->les == 1) {
+    for (size_t p = 0; p < N; p++) cs[p] = 0.01;
+  } else {
+    double *A = calloc(9 * N, 8), *Sa = calloc(N, 8), *uf = calloc(3 * N, 8), *LM = calloc(N, 8), *MM = calloc(N, 8);
+    double *tmp = calloc(N, 8);
+    /* les.c:191-238 */
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++)
+        for (int i = 1; i < mx - 1; i++) {
+          if (S(nv, g, i, j, k) > 1.1) continue;
+          const size_t p = IX(g, i, j, k);
+          double d[9], o[9], s[3][3];
+          les_du_center(g, ucat, nv, i, j, k, d);
+          les_grad(csi + 3 * p, eta + 3 * p, zet + 3 * p, aj[p], d, o);
+          Sa[p] = les_strain(o, s);
+          for (int q = 0; q < 9; q++) A[9 * p + q] = o[q];
+          double w[3][3][3], u[3][3][3][3];
+          for (int a = -1; a <= 1; a++)
+            for (int b = -1; b <= 1; b++)
+              for (int c = -1; c <= 1; c++) {
+                const size_t q = IX(g, i + a, j + b, k + c);
+                w[c + 1][b + 1][a + 1] = nv[q] > 1.1 ? 0 : 1. / aj[q];
+                for (int v = 0; v < 3; v++) u[v][c + 1][b + 1][a + 1] = ucat[3 * q + v];
+              }
+          for (int v = 0; v < 3; v++) uf[3 * p + v] = les_filter(u[v], w);
+        }
+    og_periodic_copy(g, A, 9); og_periodic_copy(g, Sa, 1); og_periodic_copy(g, uf, 3);
+    /* les.c:300-661 */
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++)
+        for (int i = 1; i < mx - 1; i++) {
+          const size_t p = IX(g, i, j, k);
+          if (nv[p] > 1.1) { LM[p] = MM[p] = 0; continue; }
+          double w[3][3][3], L[9][3][3][3], SS[3][3][3][3][3];
+          for (int a = -1; a <= 1; a++)
+            for (int b = -1; b <= 1; b++)
+              for (int c = -1; c <= 1; c++) {
+                const size_t q = IX(g, i + a, j + b, k + c);
+                const int R = c + 1, Q = b + 1, P = a + 1;
+                w[R][Q][P] = nv[q] > 1.1 ? 0 : 1. / aj[q];
+                const double *u3 = ucat + 3 * q;
+                double UVW[3];
+                const double *mt[3] = {csi + 3 * q, eta + 3 * q, zet + 3 * q};
+                for (int x = 0; x < 3; x++) UVW[x] = u3[0] * mt[x][0] + u3[1] * mt[x][1] + u3[2] * mt[x][2];
+                for (int x = 0; x < 3; x++)
+                  for (int y = 0; y < 3; y++) L[3 * x + y][R][Q][P] = UVW[x] * u3[y];
+                double s[3][3];
+                les_strain(A + 9 * q, s);
+                for (int x = 0; x < 3; x++)
+                  for (int y = 0; y < 3; y++) SS[x][y][R][Q][P] = s[x][y] * Sa[q];
+              }
+          double sum_weight = 0;
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+              for (int c = 0; c < 3; c++)
+                sum_weight += w[c][b][a] * ((c == 1 ? 1.0 : 0.5) * (b == 1 ? 1.0 : 0.5) * (a == 1 ? 1.0 : 0.5));
+          const double filter = pow(1. / aj[p], 1. / 3.), test_filter = pow(sum_weight, 1. / 3.);
+          const double *c0 = csi + 3 * p, *e0 = eta + 3 * p, *z0 = zet + 3 * p;
+          const double *f = uf + 3 * p;
+          const double fU[3] = {f[0] * c0[0] + f[1] * c0[1] + f[2] * c0[2], f[0] * e0[0] + f[1] * e0[1] + f[2] * e0[2],
+                                f[0] * z0[0] + f[1] * z0[1] + f[2] * z0[2]};
+          double d[9], o[9], Sh[3][3];
+          les_du_center(g, uf, nv, i, j, k, d);
+          les_grad(c0, e0, z0, aj[p], d, o);
+          const double S_hat = les_strain(o, Sh);
+          double Lij[3][3], SSh[3][3], Mc[3][3], M[3][3], gg[3][3], ggc[3][3], G[3][3];
+          for (int x = 0; x < 3; x++)
+            for (int y = 0; y < 3; y++) {
+              Lij[x][y] = les_filter(L[3 * x + y], w) - fU[x] * f[y];
+              SSh[x][y] = les_filter(SS[x][y], w);
+            }
+          for (int x = 0; x < 3; x++) { gg[0][x] = c0[x]; gg[1][x] = e0[x]; gg[2][x] = z0[x]; }
+          les_inverse(gg, ggc);
+          for (int x = 0; x < 3; x++)
+            for (int y = 0; y < 3; y++)
+              G[x][y] = ggc[0][x] * ggc[0][y] + ggc[1][x] * ggc[1][y] + ggc[2][x] * ggc[2][y];
+          /* les.c:612-614 form the off-diagonal entries with the second index first */
+          G[0][1] = G[1][0] = ggc[0][1] * ggc[0][0] + ggc[1][1] * ggc[1][0] + ggc[2][1] * ggc[2][0];
+          G[0][2] = G[2][0] = ggc[0][2] * ggc[0][0] + ggc[1][2] * ggc[1][0] + ggc[2][2] * ggc[2][0];
+          G[1][2] = G[2][1] = ggc[0][1] * ggc[0][2] + ggc[1][1] * ggc[1][2] + ggc[2][1] * ggc[2][2];
+          for (int x = 0; x < 3; x++)
+            for (int y = 0; y < 3; y++)
+              Mc[x][y] = -pow(test_filter, 2.) * S_hat * Sh[x][y] + pow(filter, 2.) * SSh[x][y];
+          for (int x = 0; x < 3; x++) {
+            M[x][0] = Mc[x][0] * c0[0] + Mc[x][1] * c0[1] + Mc[x][2] * c0[2];
+            M[x][1] = Mc[x][0] * e0[0] + Mc[x][1] * e0[1] + Mc[x][2] * e0[2];
+            M[x][2] = Mc[x][0] * z0[0] + Mc[x][1] * z0[1] + Mc[x][2] * z0[2];
+          }
+          double num = 0, den = 0;
+          for (int q = 0; q < 3; q++)
+            for (int a = 0; a < 3; a++)
+              for (int b = 0; b < 3; b++) num += Lij[b][a] * M[a][q] * G[b][q];
+          for (int m = 0; m < 3; m++)
+            for (int n = 0; n < 3; n++)
+              for (int l = 0; l < 3; l++) den += M[n][m] * M[n][l] * G[m][l];
+          LM[p] = num;
+          MM[p] = den;
+        }
+    og_periodic_copy(g, LM, 1); og_periodic_copy(g, MM, 1);
+    /* les.c:708-788 */
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++)
+        for (int i = 1; i < mx - 1; i++) {
+          const size_t p = IX(g, i, j, k);
+          if (nv[p] > 1.1) { cs[p] = 0; continue; }
+          double w[3][3][3], l0[3][3][3], m0[3][3][3];
+          int src[3][3][3];
+          les_wrap_weights(g, aj, nv, i, j, k, w, src);
+          for (int R = 0; R < 3; R++)
+            for (int Q = 0; Q < 3; Q++)
+              for (int P = 0; P < 3; P++) { l0[R][Q][P] = LM[src[R][Q][P]]; m0[R][Q][P] = MM[src[R][Q][P]]; }
+          const double C = 0.5 * les_filter(l0, w) / (les_filter(m0, w) + 1.e-4);
+          cs[p] = C < 0 ? 0 : C;
+        }
+    /* les.c:959-972, then the periodic copy of les.c:1022-1048 */
+    for (int k = 0; k < mz; k++)
+      for (int j = 0; j < my; j++)
+        for (int i = 0; i < mx; i++) {
+          const size_t p = IX(g, i, j, k);
+          if (nv[p] > 1.1 || k == 0 || k == mz - 1 || j == 0 || j == my - 1 || i == 0 || i == mx - 1) { cs[p] = 0; continue; }
+          if (nv[p] > 0.1 && nv[p] < 1.1) cs[p] = 0.001 < cs[p] ? cs[p] : 0.001;
+          double v = cs[p] < 0 ? 0 : cs[p];
+          cs[p] = v < max_cs ? v : max_cs;
+        }
+    og_periodic_copy(g, cs, 1);
+    /* les.c:1051-1120 */
+    memcpy(tmp, cs, 8 * N);
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++)
+        for (int i = 1; i < mx - 1; i++) {
+          const size_t p = IX(g, i, j, k);
+          if (!(nv[p] < 0.1)) continue;
+          double w[3][3][3], c0[3][3][3];
+          int src[3][3][3];
+          les_wrap_weights(g, aj, nv, i, j, k, w, src);
+          for (int R = 0; R < 3; R++)
+            for (int Q = 0; Q < 3; Q++)
+              for (int P = 0; P < 3; P++) c0[R][Q][P] = tmp[src[R][Q][P]];
+          cs[p] = les_filter(c0, w);
+        }
+    free(A); free(Sa); free(uf); free(LM); free(MM); free(tmp);
+  }
+  /* Compute_eddy_viscosity_LES, les.c:1174-1243 */
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        const size_t p = IX(g, i, j, k);
+        if (nv[p] > 1.1) { nut[p] = 0; continue; }
+        double d[9], o[9], s[3][3];
+        les_du_center(g, ucat, nv, i, j, k, d);
+        les_grad(csi + 3 * p, eta + 3 * p, zet + 3 * p, aj[p], d, o);
+        const double Sabs = les_strain(o, s);
+        const double filter = pow(1. / aj[p], 1. / 3.);
+        nut[p] = cs[p] * pow(filter, 2.0) * Sabs;
+      }
+  og_periodic_copy(g, nut, 1);
+}

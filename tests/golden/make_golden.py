@@ -13,6 +13,8 @@ Each holds the grid nodes (X, Y, Z), nvert, the seeded inputs (ucat, ucont, p, r
 phi) and the reference outputs:
   ucat_c2c     Contra2Cart (rhs.c:27)
   rhs_ff2      Formfunction_2(user, Rhs, 0.75) (momentum.c:456) added to rhs0
+  cs_les, nut_les  Compute_Smagorinsky_Constant_1 + Compute_eddy_viscosity_LES (les.c:67,
+               les.c:1135) with les = 2 at ti = 5 on ucat_c2c, lNu_t starting from nut0
   dp, p_pg     Pressure_Gradient (momentum.c:197) with mean k flux 0.37, area 1.9
   b            PoissonRHS2_hypre + Remove_Nullspace_Scale on the grid layout
   ax           the PoissonLHSNew operator applied to a seeded x (x also stored)
@@ -83,6 +85,18 @@ def make(name):
     R.set("Rhs", rhs0)
     R.call("ref_formfunction2", 0.75)
     d["rhs_ff2"] = R.get("Rhs")
+    # dynamic Smagorinsky model on the Contra2Cart velocity (les = 2, ti = 5)
+    nut0 = np.random.Generator(np.random.Philox(23)).random(R.shape) * 1e-3
+    R.set("lNu_t", nut0)
+    ref.set_global("les", 2)
+    ref.set_global("ti", 5)
+    ref.set_global("tistart", 0)
+    R.call("ref_les", 1)
+    d["nut0"] = nut0
+    d["cs_les"] = R.get("lCs")
+    d["nut_les"] = R.get("lNu_t")
+    ref.set_global("les", case.les)
+    ref.set_global("ti", 0)
     # Pressure_Gradient
     R.set_kflux(0.37, 1.9)
     ref.set_global("inlet_flux", 0.25)

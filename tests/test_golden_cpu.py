@@ -68,3 +68,18 @@ def test_update_pressure_projection(name):
     restatement.projection(st, phi)
     # interior and non-periodic ghosts: the local Ucont of the reference
     np.testing.assert_array_equal(st.ucont[1:-1, 1:-1, 1:-1], d["ucont_proj"][1:-1, 1:-1, 1:-1])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_restatement_les_matches_fixture(name):
+    """The C restatement of the dynamic Smagorinsky model reproduces the fixture's Cs and
+    nu_t bit for bit (les = 2, ti = 5, on the Contra2Cart velocity)."""
+    from oracle import restatement
+    case, d = load(name)
+    case.les = 2
+    m = restatement.form_metrics(case)
+    st = restatement.State(case, m, d["ucont"], d["ucat"], nut=d["nut0"])
+    restatement.contra2cart(st)
+    cs = restatement.les(st, ti=5)
+    np.testing.assert_array_equal(cs, d["cs_les"])
+    np.testing.assert_array_equal(st.nut, d["nut_les"])

@@ -83,3 +83,30 @@ def test_update_pressure_projection_bitwise(name):
     np.testing.assert_array_equal(ctx.get_field(vfs.UCONT), d["ucont_proj"])
     np.testing.assert_array_equal(ctx.get_field(vfs.UCAT), d["ucat_proj"])
     ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_dynamic_smagorinsky(name):
+    """Cs and nu_t of the dynamic model at ti = 5 (les.c:67, les.c:1135).  pow() is CUDA's
+    on the device and the host libm's in the fixture, so the comparison allows 1e-12 of
+    the largest value; zeros (solid cells, boundaries, clipping) must coincide."""
+    case, d = load(name)
+    case.les = 2
+    ctx = vfs.Context(case.config())
+    ctx.form_metrics(case.X, case.Y, case.Z)
+    ctx.set_field(vfs.NVERT, case.nvert)
+    ctx.set_field(vfs.UCONT, d["ucont"])
+    ctx.set_field(vfs.UCAT, d["ucat"])
+    ctx.set_field(vfs.UCAT_O, d["ucat"])
+    ctx.set_field(vfs.NU_T, d["nut0"])
+    ctx.set_scalar(vfs.S_TI, 5)
+    ctx.contra2cart()
+    ctx.smagorinsky_constant()
+    ctx.eddy_viscosity()
+    cs = ctx.get_field(vfs.CS)
+    assert np.abs(cs - d["cs_les"]).max() <= 1e-12 * np.abs(d["cs_les"]).max()
+    np.testing.assert_array_equal(cs == 0.0, d["cs_les"] == 0.0)
+    nut = ctx.get_field(vfs.NU_T)
+    assert np.abs(nut - d["nut_les"]).max() <= 1e-12 * np.abs(d["nut_les"]).max()
+    ctx.close()

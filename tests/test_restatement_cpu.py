@@ -131,3 +131,23 @@ def test_poisson_operator_rhs_projection(name):
     restatement.projection(st, phi)
     np.testing.assert_array_equal(st.ucont, R.get("Ucont"))
     R.close()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("les,ti", [(2, 5), (2, 1), (1, 5)])
+def test_dynamic_smagorinsky(name, les, ti):
+    """Cs and nu_t of the dynamic model (and its fixed-value branches) bit for bit."""
+    case, R, st = _state(name, les=True)
+    st.g.les = les
+    ref.set_global("les", les)
+    ref.set_global("ti", ti)
+    ref.set_global("tistart", 0)
+    R.call("ref_contra2cart")
+    restatement.contra2cart(st)
+    R.call("ref_les", 1)
+    cs = restatement.les(st, ti=ti)
+    if les == 2 and ti >= 2:
+        assert cs.max() > 0.0
+    np.testing.assert_array_equal(cs, R.get("lCs"))
+    np.testing.assert_array_equal(st.nut, R.get("lNu_t"))
+    R.close()

@@ -97,3 +97,57 @@ def test_ten_steps_stay_divergence_free():
             assert st.max_div < 1e-8, (prec, s, st.max_div)
         ctx.close()
     R.close()
+
+
+def reference_les_step(R):
+    """The same step with the eddy viscosity of solvers.c:648-654 before the momentum."""
+    R.call("ref_ib_bc")
+    R.set("Ucont", R.get("lUcont"))
+    R.call("ref_calc_k_flux")
+    R.call("ref_contra2cart")
+    R.call("ref_les", 1)
+    R.call("ref_pressure_gradient")
+    R.call("ref_runge_kutta")
+    R.call("ref_poisson_lhs")
+    R.volume_flux()
+    b = R.poisson_rhs_hypre()
+    rp, col, val = R.poisson_csr()
+    n = len(rp) - 1
+    A = np.zeros((n, n))
+    for r in range(n):
+        A[r, col[rp[r]:rp[r + 1]]] = val[rp[r]:rp[r + 1]]
+    x = np.linalg.lstsq(A, b, rcond=None)[0]
+    x = R.remove_nullspace(x)
+    R.set("Phi2", x)
+    R.call("ref_convert_phi2_phi")
+    R.call("ref_update_pressure")
+    R.call("ref_projection")
+    R.call("ref_ib_bc")
+    R.set("Ucont", R.get("lUcont"))
+    R.call("ref_contra2cart")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["wavy", "cylinders"])
+def test_one_les_step_matches_reference(name):
+    """A step with the dynamic Smagorinsky model (les = 2) at ti = 2, when Cs is first
+    computed on a fresh run."""
+    case = STEP_CASES[name]()
+    case.les = 2
+    case.inlet_flux = 5.0
+    R, ctx = build_pair(case, les_nut=True, extra_globals={"ti": 2, "tistart": 0})
+    ref.set_global("inlet_flux", case.inlet_flux)
+    ctx.set_scalar(vfs.S_INLET_FLUX, case.inlet_flux)
+    ctx.set_scalar(vfs.S_TI, 2)
+    reference_les_step(R)
+    st = ctx.step(precision=0, rtol=1e-13)
+    assert st.poisson.converged == 1
+    assert R.get("lCs").max() > 0.0
+    assert_close(ctx.get_field(vfs.CS), R.get("lCs"), rtol=1e-12, atol_frac=1e-14, what="Cs")
+    assert_close(ctx.get_field(vfs.NU_T), R.get("lNu_t"), rtol=1e-12, atol_frac=1e-14, what="nu_t")
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-8, atol_frac=1e-9, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-9, atol_frac=1e-10, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
+    assert st.max_div < 1e-8
+    assert ctx.get_scalar(vfs.S_TI) == 3
+    R.close()

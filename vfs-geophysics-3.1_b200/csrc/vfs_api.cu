@@ -68,6 +68,19 @@ __global__ void k_sum_parts(const double *parts, int n, double *out) {
   if (threadIdx.x == 0) out[0] = sh[0];
 }
 
+// Staging buffer for vfs_set_field / vfs_get_field: allocated on first use, kept for
+// the life of the context so that repeated transfers allocate nothing.
+static int ensure_stage(Ctx *c, size_t bytes) {
+  if (bytes <= c->stage_bytes) return VFS_OK;
+  if (c->stage) cudaFree(c->stage);
+  c->stage = nullptr;
+  c->stage_bytes = 0;
+  if (cudaMalloc(&c->stage, bytes) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "staging buffer allocation failed");
+  c->stage_bytes = bytes;
+  return VFS_OK;
+}
+
 int reduce_sum(Ctx *c, const double *parts, int nparts, double *out) {
   int rc = ensure_red(c, 64);
   if (rc) return rc;
@@ -161,6 +174,12 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
   g.ren = cfg->ren; g.dt = cfg->dt; g.st = cfg->st;
   c->scal[VFS_S_DT] = cfg->dt; c->scal[VFS_S_REN] = cfg->ren; c->scal[VFS_S_ST] = cfg->st;
   c->scal[VFS_S_INLET_FLUX] = cfg->inlet_flux;
+  c->tistart = cfg->tistart;
+  c->ti = cfg->tistart;
+  c->rstart = cfg->rstart;
+  c->dynamic_freq = cfg->dynamic_freq < 1 ? 1 : cfg->dynamic_freq;
+  c->max_cs = cfg->max_cs > 0 ? cfg->max_cs : 0.5;
+  c->scal[VFS_S_TI] = c->ti;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return set_err(nullptr, VFS_ERR_CUDA, "stream creation failed");
@@ -224,6 +243,7 @@ int vfs_destroy(vfs_ctx *ctx) {
   for (int q = 0; q < 3; q++) { cudaFree(c->fp[q]); cudaFree(c->pucont[q]); cudaFree(c->bcbuf[q]); }
   if (c->red) cudaFree(c->red);
   if (c->red_host) cudaFreeHost(c->red_host);
+  if (c->stage) cudaFree(c->stage);
   Poisson &P = c->ps;
   cudaFree(P.coef); cudaFree(P.fluid);
   cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t); cudaFree(P.hdev);
@@ -261,11 +281,10 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
   cudaSetDevice(c->device);
   const int dof = c->dof[field];
   const size_t bytes = sizeof(double) * (size_t)c->g.N * dof;
-  double *stage = nullptr;
-  if (cudaMallocAsync(&stage, bytes, c->stream) != cudaSuccess)
-    return set_err(c, VFS_ERR_CUDA, "vfs_set_field: staging allocation failed");
+  int rc = ensure_stage(c, sizeof(double) * (size_t)c->g.N * 3);
+  if (rc) return rc;
+  double *stage = c->stage;
   cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, c->stream);
-  int rc = VFS_OK;
   if (field == VFS_NVERT) {
     int *bad = (int *)c->red;  // first word of the reduction buffer as a flag
     cudaMemsetAsync(bad, 0, sizeof(int), c->stream);
@@ -274,7 +293,6 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
     int hbad = 0;
     cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(c->f[field][0], stage, bytes, cudaMemcpyDeviceToDevice, c->stream);
-    cudaFreeAsync(stage, c->stream);
     cudaStreamSynchronize(c->stream);
     if (!rc && hbad) rc = set_err(c, VFS_ERR_INVALID, "vfs_set_field: nvert must hold integers 0..255");
     c->nvert_set = true;
@@ -285,7 +303,6 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
   k_unpack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
                                                        c->f[field][1], c->f[field][2]);
   rc = check_launch(c, "k_unpack");
-  cudaFreeAsync(stage, c->stream);
   if (field >= VFS_CSI && field <= VFS_KAJ) { c->metrics_set = true; c->ps.built = false; }
   if (cudaStreamSynchronize(c->stream) != cudaSuccess)
     return set_err(c, VFS_ERR_CUDA, "vfs_set_field: copy failed");
@@ -298,14 +315,13 @@ int vfs_get_field(vfs_ctx *ctx, int field, double *host) {
   cudaSetDevice(c->device);
   const int dof = c->dof[field];
   const size_t bytes = sizeof(double) * (size_t)c->g.N * dof;
-  double *stage = nullptr;
-  if (cudaMallocAsync(&stage, bytes, c->stream) != cudaSuccess)
-    return set_err(c, VFS_ERR_CUDA, "vfs_get_field: staging allocation failed");
+  int rc = ensure_stage(c, sizeof(double) * (size_t)c->g.N * 3);
+  if (rc) return rc;
+  double *stage = c->stage;
   k_pack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
                                                      c->f[field][1], c->f[field][2]);
-  int rc = check_launch(c, "k_pack");
+  rc = check_launch(c, "k_pack");
   cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, c->stream);
-  cudaFreeAsync(stage, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess)
     return set_err(c, VFS_ERR_CUDA, "vfs_get_field: copy failed");
   return rc;
@@ -326,12 +342,14 @@ int vfs_set_scalar(vfs_ctx *ctx, int which, double value) {
   if (which == VFS_S_DT) c->g.dt = value;
   if (which == VFS_S_REN) c->g.ren = value;
   if (which == VFS_S_ST) c->g.st = value;
+  if (which == VFS_S_TI) c->ti = (int)value;
   return VFS_OK;
 }
 
 int vfs_get_scalar(vfs_ctx *ctx, int which, double *value) {
   Ctx *c = (Ctx *)ctx;
   if (!c || !value || which < 0 || which >= VFS_NSCALARS) return set_err(c, VFS_ERR_INVALID, "vfs_get_scalar: bad argument");
+  if (which == VFS_S_TI) c->scal[VFS_S_TI] = c->ti;
   *value = c->scal[which];
   return VFS_OK;
 }
@@ -353,6 +371,8 @@ int vfs_calc_k_flux(vfs_ctx *ctx, double *flux) {
   if (flux) *flux = f;
   return rc;
 }
+int vfs_smagorinsky_constant(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return smagorinsky_constant(c); }
+int vfs_eddy_viscosity(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return eddy_viscosity(c); }
 int vfs_runge_kutta(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return runge_kutta(c); }
 int vfs_poisson_lhs(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return poisson_lhs(c); }
 int vfs_poisson_rhs(vfs_ctx *ctx) {
@@ -414,6 +434,11 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
   }
   // Flow_Solver for implicit = 0 (solvers.c:644-1385)
   if ((rc = calc_k_flux(c, &s.mean_k_flux))) return rc;
+  if (c->g.les) {  // solvers.c:648-654
+    if ((rc = contra2cart(c))) return rc;
+    if ((c->ti % c->dynamic_freq == 0 || c->ti == c->tistart) && (rc = smagorinsky_constant(c))) return rc;
+    if ((rc = eddy_viscosity(c))) return rc;
+  }
   if ((rc = pressure_gradient(c))) return rc;
   if ((rc = runge_kutta(c))) return rc;
   if ((rc = volume_flux(c))) return rc;  // poisson_hypre.c:566
@@ -432,6 +457,7 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
     cudaMemcpyAsync(c->f[VFS_UCONT_O][q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
     cudaMemcpyAsync(c->f[VFS_UCAT_O][q], c->f[VFS_UCAT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
   }
+  c->ti++;
   cudaEventRecord(c->ev1, c->stream);
   cudaEventSynchronize(c->ev1);
   float ms = 0;

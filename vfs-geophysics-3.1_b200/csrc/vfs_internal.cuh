@@ -134,9 +134,13 @@ struct Ctx {
   double *red = nullptr;        // partial sums (device)
   double *red_host = nullptr;   // pinned host mirror
   int red_cap = 0;
+  double *stage = nullptr;      // host-transfer staging buffer (interleaved layout)
+  size_t stage_bytes = 0;
   double scal[VFS_NSCALARS] = {};
   bool metrics_set = false, nvert_set = false;
   bool first_step = true;        // ti == tistart set-up pending (main.c:3488, solvers.c:603)
+  int ti = 0, tistart = 0, rstart = 0, dynamic_freq = 1;  // time step index and LES schedule
+  double max_cs = 0.5;           // upper clip of the Smagorinsky coefficient
   Poisson ps;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -163,6 +167,10 @@ int runge_kutta(Ctx *c);
 int form_bcs(Ctx *c);
 int calc_inlet_area(Ctx *c);
 int ib_bc(Ctx *c);
+
+// dynamic Smagorinsky model (vfs_les.cu)
+int smagorinsky_constant(Ctx *c);
+int eddy_viscosity(Ctx *c);
 
 // Poisson / correction path
 int poisson_lhs(Ctx *c);

@@ -37,7 +37,7 @@ METRIC_FIELDS = {
 }
 
 # scalars
-S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST = range(7)
+S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST, S_TI = range(8)
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOT_CONVERGED, ERR_NO_DEVICE, ERR_STATE = range(6)
 
@@ -48,11 +48,12 @@ class VfsConfig(ctypes.Structure):
         ("bctype", ctypes.c_int * 6),
         ("i_periodic", ctypes.c_int), ("j_periodic", ctypes.c_int), ("k_periodic", ctypes.c_int),
         ("immersed", ctypes.c_int), ("les", ctypes.c_int), ("inletprofile", ctypes.c_int),
-        ("reserved_i", ctypes.c_int * 8),
+        ("dynamic_freq", ctypes.c_int), ("tistart", ctypes.c_int), ("rstart", ctypes.c_int),
+        ("reserved_i", ctypes.c_int * 5),
         ("ren", ctypes.c_double), ("dt", ctypes.c_double), ("st", ctypes.c_double),
         ("inlet_flux", ctypes.c_double), ("mean_pressure_gradient", ctypes.c_double),
         ("dpdz_set", ctypes.c_int), ("reserved_j", ctypes.c_int * 7),
-        ("reserved_d", ctypes.c_double * 8),
+        ("max_cs", ctypes.c_double), ("reserved_d", ctypes.c_double * 7),
     ]
 
 
@@ -88,6 +89,7 @@ EXPORTS = [
     "vfs_poisson_solve", "vfs_poisson_apply", "vfs_update_pressure", "vfs_projection",
     "vfs_divergence", "vfs_step", "vfs_calc_inlet_area", "vfs_form_bcs", "vfs_ib_bc",
     "vfs_form_metrics", "vfs_volume_flux", "vfs_get_stream", "vfs_run_kernel",
+    "vfs_smagorinsky_constant", "vfs_eddy_viscosity",
 ]
 
 _lib = None
@@ -120,7 +122,8 @@ def load_library(path=None):
     lib.vfs_field_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     for n in ("vfs_contra2cart", "vfs_pressure_gradient", "vfs_runge_kutta", "vfs_poisson_lhs",
               "vfs_poisson_rhs", "vfs_update_pressure", "vfs_projection", "vfs_calc_inlet_area",
-              "vfs_form_bcs", "vfs_ib_bc", "vfs_volume_flux"):
+              "vfs_form_bcs", "vfs_ib_bc", "vfs_volume_flux", "vfs_smagorinsky_constant",
+              "vfs_eddy_viscosity"):
         getattr(lib, n).argtypes = [vp]
     lib.vfs_formfunction2.argtypes = [vp, ctypes.c_double]
     lib.vfs_calc_k_flux.argtypes = [vp, dp]
@@ -257,6 +260,12 @@ class Context:
     def ib_bc(self):                  # IB_BC, momentum.c:1982
         self._check(self.lib.vfs_ib_bc(self.h))
 
+    def smagorinsky_constant(self):   # Compute_Smagorinsky_Constant_1, les.c:67
+        self._check(self.lib.vfs_smagorinsky_constant(self.h))
+
+    def eddy_viscosity(self):         # Compute_eddy_viscosity_LES, les.c:1135
+        self._check(self.lib.vfs_eddy_viscosity(self.h))
+
     def runge_kutta(self):            # RungeKutta, rhs.c:1578
         self._check(self.lib.vfs_runge_kutta(self.h))
 
@@ -305,7 +314,8 @@ class Context:
 
 def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
                 inletprofile=13, ren=3000.0, dt=0.04, st=1.0, inlet_flux=-1.0,
-                mean_pressure_gradient=0.0, dpdz_set=0):
+                mean_pressure_gradient=0.0, dpdz_set=0, dynamic_freq=1, tistart=0, rstart=0,
+                max_cs=0.5):
     c = VfsConfig()
     c.IM, c.JM, c.KM = IM, JM, KM
     for q in range(6):
@@ -314,4 +324,5 @@ def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, im
     c.immersed, c.les, c.inletprofile = immersed, les, inletprofile
     c.ren, c.dt, c.st = ren, dt, st
     c.inlet_flux, c.mean_pressure_gradient, c.dpdz_set = inlet_flux, mean_pressure_gradient, dpdz_set
+    c.dynamic_freq, c.tistart, c.rstart, c.max_cs = dynamic_freq, tistart, rstart, max_cs
     return c
