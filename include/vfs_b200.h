@@ -87,7 +87,9 @@ enum {
   VFS_S_INLET_AREA = 3,   /* inletArea (bcs.c:212) */
   VFS_S_DT = 4, VFS_S_REN = 5, VFS_S_ST = 6,
   VFS_S_TI = 7,           /* time step index ti (main.c:3534); vfs_step advances it */
-  VFS_NSCALARS = 8
+  VFS_S_FLUX_IN = 8,      /* FluxInSum: inlet flux of the last InflowFlux (bcs.c:785) */
+  VFS_S_FLUX_OUT = 9,     /* FluxOutSum: outlet flux before the last rescaling (bcs.c:2369) */
+  VFS_NSCALARS = 10
 };
 
 /* Poisson solver options (replaces PoissonSolver_Hypre, poisson_hypre.c:498). */
@@ -173,9 +175,25 @@ int vfs_calc_k_flux(vfs_ctx *ctx, double *mean_k_flux);
  * fluid inlet-plane area -> VFS_S_INLET_AREA (k inlet or periodic k). */
 int vfs_calc_inlet_area(vfs_ctx *ctx);
 
-/* FormBCS (bcs.c:1841) for the boundary codes accepted by vfs_create: Contra2Cart, zero
- * normal flux through no-slip/free-slip i/j walls, Contra2Cart, Ucat = 0 on box edges. */
-int vfs_form_bcs(vfs_ctx *ctx);
+/* InflowFlux (bcs.c:329) for an inlet on the k = 0 face (bctype[4] = 5): inlet-plane face
+ * fluxes and ghost velocities for inletprofile 2 (uniform inlet_flux/inletArea), 21
+ * (Poiseuille) or 100 (the plane of vfs_set_inflow_plane, rescaled to inlet_flux);
+ * inletprofile 1 gives zero inflow, as in the reference (its second profile selection,
+ * bcs.c:408-466, has no branch for 1 and sets uin = 0).  FluxInSum -> VFS_S_FLUX_IN.
+ * No-op without a k = 0 inlet. */
+int vfs_inflow_flux(vfs_ctx *ctx);
+
+/* The inflow velocity plane of inletprofile 100 (user->ucont_plane filled by
+ * read_inflow_section, rhs2.c:701): my*mx Cartesian {u,v,w} triples, [j][i] with i fastest,
+ * the layout of one record of the reference's inflow files. */
+int vfs_set_inflow_plane(vfs_ctx *ctx, const double *plane);
+
+/* FormBCS (bcs.c:1841) for the boundary codes accepted by vfs_create: Contra2Cart; with
+ * outflow_scale and an outlet on the k+ face (bctype[5] = 4), the last interior k-face
+ * fluxes shifted so the outflow equals VFS_S_FLUX_IN (bcs.c:2285-2417); zero normal flux
+ * through no-slip/free-slip i/j walls; Contra2Cart; Ucat = 0 on box edges.  RungeKutta
+ * calls it with outflow_scale 0 before the stages and 1 after them (rhs.c:1598, 1670). */
+int vfs_form_bcs(vfs_ctx *ctx, int outflow_scale);
 
 /* IB_BC (momentum.c:1982) without immersed bodies: zero normal flux on free-slip faces,
  * periodic normal flux on ghost planes. */
@@ -185,7 +203,8 @@ int vfs_ib_bc(vfs_ctx *ctx);
  * every interior face between a fluid and a non-fluid cell (blocked-cell bodies). */
 int vfs_volume_flux(vfs_ctx *ctx);
 
-/* RungeKutta (rhs.c:1578), explicit momentum predictor, 4 stages. */
+/* RungeKutta (rhs.c:1578), explicit momentum predictor, 4 stages: InflowFlux, FormBCS,
+ * the stages, FormBCS with the outlet rescaling. */
 int vfs_runge_kutta(vfs_ctx *ctx);
 
 /* PoissonLHSNew (poisson.c:971): builds the 19-point operator of the fluid cells and

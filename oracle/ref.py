@@ -51,6 +51,9 @@ def lib():
         L.ref_les.argtypes = [ctypes.c_int]
         L.ref_inlet_area.restype = ctypes.c_double
         L.ref_volume_flux.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
+        L.ref_form_bcs_scaled.argtypes = [ctypes.c_int]
+        L.ref_flux_in.restype = ctypes.c_double
+        L.ref_set_inflow_plane.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -168,6 +171,14 @@ class Reference:
 
     def inlet_area(self):
         return lib().ref_inlet_area()
+
+    def flux_in(self):
+        """FluxInSum after the last InflowFlux (bcs.c:778)."""
+        return lib().ref_flux_in()
+
+    def set_inflow_plane(self, plane):
+        a = np.ascontiguousarray(plane, dtype=np.float64)
+        lib().ref_set_inflow_plane(a.ctypes.data)
 
     def set_kflux(self, flux, area):
         lib().ref_set_kflux(flux, area)

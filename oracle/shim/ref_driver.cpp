@@ -30,6 +30,8 @@ extern void PoissonRHS2_hypre(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 extern void Remove_Nullspace(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 
 extern double inletArea;
+extern int ucont_plane_allocated;  // main.c:238
+extern int outflow_scale;          // bcs.c:1839
 extern int k_area_allocated;  // bcs.c:213, once per process in the reference
 
 static UserMG g_usermg;
@@ -167,6 +169,32 @@ double ref_inlet_area(void) { return inletArea; }
 int ref_runge_kutta(void) { return RungeKutta(g_user, g_ibm, g_fsi); }
 int ref_form_bcs(void) { return FormBCS(g_user, g_fsi); }
 int ref_inflow_flux(void) { return InflowFlux(g_user); }
+// FormBCS with the outlet rescaling switched as RungeKutta switches it (rhs.c:1598, 1670).
+int ref_form_bcs_scaled(int scale) {
+  outflow_scale = scale;
+  int rc = FormBCS(g_user, g_fsi);
+  outflow_scale = 1;
+  return rc;
+}
+double ref_flux_in(void) { return FluxInSum; }
+// The inflow plane of inletprofile 100 (user->ucont_plane, [j][i] of Cmpnts, as
+// read_inflow_section fills it, rhs2.c:712-722).
+int ref_set_inflow_plane(const double *plane) {
+  const int mx = g_user->info.mx, my = g_user->info.my;
+  if (!ucont_plane_allocated) {
+    ucont_plane_allocated = 1;
+    g_user->ucont_plane = (Cmpnts **)malloc(sizeof(Cmpnts *) * my);
+    for (int j = 0; j < my; j++) g_user->ucont_plane[j] = (Cmpnts *)malloc(sizeof(Cmpnts) * mx);
+  }
+  for (int j = 0; j < my; j++)
+    for (int i = 0; i < mx; i++) {
+      const double *p = plane + 3 * ((long)j * mx + i);
+      g_user->ucont_plane[j][i].x = p[0];
+      g_user->ucont_plane[j][i].y = p[1];
+      g_user->ucont_plane[j][i].z = p[2];
+    }
+  return 0;
+}
 int ref_ib_bc(void) { IB_BC(g_user); return 0; }
 int ref_update_pressure(void) { return UpdatePressure(g_user); }
 int ref_projection(void) { return Projection(g_user); }

@@ -144,12 +144,21 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
   if (cfg->IM < 4 || cfg->JM < 4 || cfg->KM < 4)
     return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: grid needs at least 4 nodes per direction");
   // Boundary codes handled on this path: 0 (unset), 1 no-slip wall, 2 moving lid (j+),
-  // 4 outlet, 5 inlet, 7 periodic face, 10 free-slip, 12 moving wall, 13/14 slip lid.
+  // 4 outlet (k+ or j+), 5 inlet (k-), 7 periodic face, 10 free-slip, 12 moving wall,
+  // 13/14 slip lid.
   for (int q = 0; q < 6; q++) {
     int b = cfg->bctype[q];
     bool ok = (b == 0 || b == 1 || b == 2 || b == 4 || b == 5 || b == 7 || b == 10 || b == 12 ||
                b == 13 || b == 14 || b == -10);
     if (!ok) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: unsupported bctype " + std::to_string(b));
+    if (b == 5 && q != 4) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: an inlet (5) is supported on the k = 0 face only");
+    if (b == 4 && q != 5 && q != 3) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: an outlet (4) is supported on the k+ and j+ faces only");
+  }
+  if (cfg->bctype[4] == 5) {
+    const int ip = cfg->inletprofile;
+    if (!(ip == 1 || ip == 2 || ip == 21 || ip == 100))
+      return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: inlet profiles 1, 2, 21 and 100 are supported");
+    if (cfg->k_periodic) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: an inlet face cannot be k-periodic");
   }
   if (cfg->immersed < 0 || cfg->immersed > 1)
     return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: immersed must be 0 or 1");
@@ -244,6 +253,8 @@ int vfs_destroy(vfs_ctx *ctx) {
   if (c->red) cudaFree(c->red);
   if (c->red_host) cudaFreeHost(c->red_host);
   if (c->stage) cudaFree(c->stage);
+  if (c->inflow_plane) cudaFree(c->inflow_plane);
+  if (c->inlet_nodes) cudaFree(c->inlet_nodes);
   Poisson &P = c->ps;
   cudaFree(P.coef); cudaFree(P.fluid);
   cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t); cudaFree(P.hdev);
@@ -412,7 +423,21 @@ int vfs_divergence(vfs_ctx *ctx, double *maxdiv) {
 }
 
 int vfs_calc_inlet_area(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return calc_inlet_area(c); }
-int vfs_form_bcs(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return form_bcs(c); }
+int vfs_form_bcs(vfs_ctx *ctx, int outflow_scale) {
+  Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return form_bcs(c, outflow_scale != 0);
+}
+int vfs_inflow_flux(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return inflow_flux(c); }
+int vfs_set_inflow_plane(vfs_ctx *ctx, const double *plane) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c || !plane) return set_err(c, VFS_ERR_INVALID, "vfs_set_inflow_plane: null argument");
+  cudaSetDevice(c->device);
+  const size_t bytes = sizeof(double) * 3 * (size_t)c->g.mx * c->g.my;
+  if (!c->inflow_plane && cudaMalloc(&c->inflow_plane, bytes) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "vfs_set_inflow_plane: allocation failed");
+  cudaMemcpyAsync(c->inflow_plane, plane, bytes, cudaMemcpyHostToDevice, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "vfs_set_inflow_plane: copy failed");
+  return VFS_OK;
+}
 int vfs_volume_flux(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return volume_flux(c); }
 int vfs_ib_bc(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return ib_bc(c); }
 

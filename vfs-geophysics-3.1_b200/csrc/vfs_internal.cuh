@@ -134,6 +134,8 @@ struct Ctx {
   double *red = nullptr;        // partial sums (device)
   double *red_host = nullptr;   // pinned host mirror
   int red_cap = 0;
+  double *inflow_plane = nullptr;  // inlet velocity plane, my*mx Cartesian triples (inletprofile 100)
+  double *inlet_nodes = nullptr;   // grid nodes of the k = 1 node plane: x, y, z blocks of JM*IM
   double *stage = nullptr;      // host-transfer staging buffer (interleaved layout)
   size_t stage_bytes = 0;
   double scal[VFS_NSCALARS] = {};
@@ -164,7 +166,8 @@ int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff);
 int pressure_gradient(Ctx *c);
 int calc_k_flux(Ctx *c, double *flux);
 int runge_kutta(Ctx *c);
-int form_bcs(Ctx *c);
+int form_bcs(Ctx *c, bool outflow_scale);
+int inflow_flux(Ctx *c);
 int calc_inlet_area(Ctx *c);
 int ib_bc(Ctx *c);
 

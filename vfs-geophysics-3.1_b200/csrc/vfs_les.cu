@@ -384,15 +384,12 @@ __global__ void __launch_bounds__(kLesLmThreads, 2)
 // boundary neighbours, and the neighbour's value read at its periodic image.  In the j
 // direction the reference tests the cell's own j against my-1 (les.c:748, les.c:1097),
 // so only J == 0 is zeroed; that test is kept.
-__device__ __forceinline__ void wrap_weights(const Grid &g, const double *__restrict__ aj,
-                                             const uint8_t *__restrict__ nv, int i, int j, int k, double w[27],
-                                             long long src[27]) {
+__device__ __forceinline__ void wrap_weights(const Grid &g, const double *__restrict__ wgt, int i, int j, int k,
+                                             double w[27], long long src[27]) {
 #pragma unroll
   for (int n = 0; n < 27; n++) {
     int K = k + n / 9 - 1, J = j + (n / 3) % 3 - 1, I = i + n % 3 - 1;
-    const long long q = lidx(g, I, J, K);
-    double wt = 1. / aj[q];
-    if (nv[q] > 1) wt = 0;
+    double wt = wgt[lidx(g, I, J, K)];  // 1/aj, 0 where nvert > 1.1
     if (g.iper) { if (I == 0) I = g.mx - 2; else if (I == g.mx - 1) I = 1; }
     else if (I == 0 || I == g.mx - 1) wt = 0;
     if (g.jper) { if (J == 0) J = g.my - 2; else if (J == g.my - 1) J = 1; }
@@ -405,14 +402,14 @@ __device__ __forceinline__ void wrap_weights(const Grid &g, const double *__rest
 }
 
 // Clipped Cs of one interior cell (les.c:708-788 with les = 2, then les.c:959-972).
-__device__ __forceinline__ double cs_cell(const Grid &g, const double *__restrict__ aj,
+__device__ __forceinline__ double cs_cell(const Grid &g, const double *__restrict__ wgt,
                                           const uint8_t *__restrict__ nv, const double *__restrict__ LM,
                                           const double *__restrict__ MM, int i, int j, int k, double max_cs) {
   const long long p = lidx(g, i, j, k);
   if (nv[p] > 1) return 0.0;
   double w[27], lm[27], mm[27];
   long long src[27];
-  wrap_weights(g, aj, nv, i, j, k, w, src);
+  wrap_weights(g, wgt, i, j, k, w, src);
 #pragma unroll
   for (int n = 0; n < 27; n++) { lm[n] = LM[src[n]]; mm[n] = MM[src[n]]; }
   const double ws = tf_wsum(w);
@@ -428,7 +425,7 @@ __device__ __forceinline__ double cs_cell(const Grid &g, const double *__restric
 
 // Every DA point: interior cells their clipped Cs, periodic ghosts the value of their image
 // (zero when the image is itself a boundary point), other ghosts zero.
-__global__ void k_les_cs(Grid g, const double *__restrict__ aj, const uint8_t *__restrict__ nv,
+__global__ void k_les_cs(Grid g, const double *__restrict__ wgt, const uint8_t *__restrict__ nv,
                          const double *__restrict__ LM, const double *__restrict__ MM, double max_cs, double *cs) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
@@ -436,11 +433,11 @@ __global__ void k_les_cs(Grid g, const double *__restrict__ aj, const uint8_t *_
   const long long r = p / g.mx;
   const int j = (int)(r % g.my), k = (int)(r / g.my);
   const int a = wrapi(g, i), b = wrapj(g, j), c = wrapk(g, k);
-  cs[p] = les_interior(g, a, b, c) ? cs_cell(g, aj, nv, LM, MM, a, b, c, max_cs) : 0.0;
+  cs[p] = les_interior(g, a, b, c) ? cs_cell(g, wgt, nv, LM, MM, a, b, c, max_cs) : 0.0;
 }
 
 // Second filtering of Cs over fluid cells (nvert < 0.1); every other point keeps its value.
-__global__ void k_les_refilter(Grid g, const double *__restrict__ aj, const uint8_t *__restrict__ nv,
+__global__ void k_les_refilter(Grid g, const double *__restrict__ wgt, const uint8_t *__restrict__ nv,
                                const double *__restrict__ cs_tmp, double *cs) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
@@ -450,7 +447,7 @@ __global__ void k_les_refilter(Grid g, const double *__restrict__ aj, const uint
   if (!les_interior(g, i, j, k) || nv[p] != 0) { cs[p] = cs_tmp[p]; return; }
   double w[27], v[27];
   long long src[27];
-  wrap_weights(g, aj, nv, i, j, k, w, src);
+  wrap_weights(g, wgt, i, j, k, w, src);
 #pragma unroll
   for (int n = 0; n < 27; n++) v[n] = cs_tmp[src[n]];
   cs[p] = tf_apply(v, w, tf_wsum(w));
@@ -542,9 +539,9 @@ int smagorinsky_constant(Ctx *c) {
   k_les_lm<<<grid, kLesLmThreads, sizeof(LesLmSmem), c->stream>>>(g, in, m.csi, m.eta, m.zet, m.aj, c->nv, LM, MM);
   if ((rc = check_launch(c, "k_les_lm"))) return rc;
   if ((rc = periodic_copy3(c, V3{LM, MM, nullptr}))) return rc;
-  k_les_cs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m.aj, c->nv, LM, MM, c->max_cs, cs_tmp);
+  k_les_cs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, o.wgt, c->nv, LM, MM, c->max_cs, cs_tmp);
   if ((rc = check_launch(c, "k_les_cs"))) return rc;
-  k_les_refilter<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m.aj, c->nv, cs_tmp, cs);
+  k_les_refilter<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, o.wgt, c->nv, cs_tmp, cs);
   return check_launch(c, "k_les_refilter");
 }
 

@@ -186,6 +186,13 @@ int form_metrics(Ctx *c, const double *x, const double *y, const double *z) {
     else rc = periodic_copy1(c, c->f[f][0]);
     if (rc) return rc;
   }
+  // the node plane k = 1 (x, y, z blocks), for inlet profiles given in node coordinates
+  const size_t plane = (size_t)IM * JM;
+  if (!c->inlet_nodes && cudaMalloc(&c->inlet_nodes, sizeof(double) * plane * 3) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "form_metrics: node-plane allocation failed");
+  for (int q = 0; q < 3; q++)
+    cudaMemcpyAsync(c->inlet_nodes + q * plane, d + q * nn + plane, sizeof(double) * plane, cudaMemcpyDeviceToDevice,
+                    c->stream);
   cudaFreeAsync(d, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "form_metrics failed");
   c->metrics_set = true;

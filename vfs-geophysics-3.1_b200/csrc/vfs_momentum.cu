@@ -627,7 +627,15 @@ __device__ __forceinline__ void flux_k(const Grid &g, const Metrics &m, CV3 uc, 
 // One thread per DA point (i,j,k) with i<mx-1, j<my-1, k<mz-1: computes the fluxes of
 // its i-face (if j,k >= 1), j-face (if i,k >= 1) and k-face (if i,j >= 1), following
 // the three face loops of Formfunction_2 (momentum.c:671-1415).
-__global__ void k_face_flux(Grid g, Metrics m, CV3 uc, CV3 u, const uint8_t *__restrict__ nv,
+// Launch shape: VFS_FF_THREADS threads per block, at least VFS_FF_MINB blocks per SM (the
+// register cap that follows from it sets the occupancy of this latency-bound kernel).
+#ifndef VFS_FF_THREADS
+#define VFS_FF_THREADS 128
+#endif
+#ifndef VFS_FF_MINB
+#define VFS_FF_MINB 1
+#endif
+__global__ void __launch_bounds__(VFS_FF_THREADS, VFS_FF_MINB) k_face_flux(Grid g, Metrics m, CV3 uc, CV3 u, const uint8_t *__restrict__ nv,
                             const double *__restrict__ nut, FluxOut f1, FluxOut f2, FluxOut f3) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
@@ -1003,7 +1011,7 @@ int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   V3 uc = field3(c, VFS_UCONT);
   if ((rc = periodic_copy3(c, uc))) return rc;
   Metrics m = metrics(c);
-  k_face_flux<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, cv(uc), cv(field3(c, VFS_UCAT)), c->nv,
+  k_face_flux<<<nblocks(g.N, VFS_FF_THREADS), VFS_FF_THREADS, 0, c->stream>>>(g, m, cv(uc), cv(field3(c, VFS_UCAT)), c->nv,
                                                         c->f[VFS_NU_T][0], flux_out(c, 0), flux_out(c, 1),
                                                         flux_out(c, 2));
   if ((rc = check_launch(c, "k_face_flux"))) return rc;
@@ -1048,7 +1056,7 @@ int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
 
 // single-kernel launchers for the diagnostics entry point (vfs_run_kernel)
 void launch_face_flux(Ctx *c) {
-  k_face_flux<<<nblocks(c->g.N, 128), 128, 0, c->stream>>>(c->g, metrics(c), cv(field3(c, VFS_UCONT)),
+  k_face_flux<<<nblocks(c->g.N, VFS_FF_THREADS), VFS_FF_THREADS, 0, c->stream>>>(c->g, metrics(c), cv(field3(c, VFS_UCONT)),
                                                            cv(field3(c, VFS_UCAT)), c->nv, c->f[VFS_NU_T][0],
                                                            flux_out(c, 0), flux_out(c, 1), flux_out(c, 2));
 }
@@ -1296,10 +1304,171 @@ int ib_bc(Ctx *c) {
   return VFS_OK;
 }
 
+// ------------------------------------------------------------------ InflowFlux
+// bcs.c:329-706 for an inlet on the k = 0 face (bctype[4] = 5), interior (i, j):
+//   inletprofile 2     uniform uin = inlet_flux/inletArea (1 when inlet_flux < 0);
+//   inletprofile 1     uin = 0: the reference sets the uniform value first, then its
+//                      second profile chain (bcs.c:408-466) has no branch for 1 and ends
+//                      in uin = 0, which is what the reference runs with;
+//   inletprofile 21    laminar Poiseuille 1.5*yc*(2 - yc) at the k = 1 face centre;
+//   inletprofile 100   Cartesian velocity plane supplied by the caller (ucont_plane,
+//                      read_inflow_section, rhs2.c:701), then the flux rescaled to
+//                      inlet_flux over the fluid inlet area.
+// A face whose downstream cell is blocked (nvert[1] >= 0.1) gets zero flux.  The ghost
+// velocity at k = 0 is -Ucat(k=1) + 2*u(face), u from the face flux by Cramer's rule
+// (Contra2Cart_single, rhs.c:34).
+__global__ void k_inflow(Grid g, Metrics m, V3 uc, V3 ucat, const uint8_t *__restrict__ nv, int profile,
+                         double uin_const, const double *__restrict__ plane, const double *__restrict__ ynode,
+                         double *parts) {
+  __shared__ double sh[256];
+  const int nx = g.mx - 2, ny = g.my - 2;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double s = 0;
+  if (t < (long long)nx * ny) {
+    const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
+    const long long p = lidx(g, i, j, 0), p1 = p + (long long)g.mx * g.my;
+    const double zx = m.zet.x[p], zy = m.zet.y[p], zz = m.zet.z[p];
+    const double area = sqrt(zx * zx + zy * zy + zz * zz);
+    if (nv[p1] == 0) {
+      if (profile == 100) {
+        const double *pl = plane + 3 * ((long long)j * g.mx + i);
+        const double u = pl[0], v = pl[1], w = pl[2];
+        ucat.x[p] = u; ucat.y[p] = v; ucat.z[p] = w;
+        uc.z[p] = 0.5 * (u + ucat.x[p1]) * zx + 0.5 * (v + ucat.y[p1]) * zy + 0.5 * (w + ucat.z[p1]) * zz;
+      } else {
+        double uin = uin_const;
+        if (profile == 21) {
+          const int IM = g.mx - 1;
+          const double yc = (ynode[(long long)j * IM + i] + ynode[(long long)(j - 1) * IM + i] +
+                             ynode[(long long)j * IM + i - 1] + ynode[(long long)(j - 1) * IM + i - 1]) * 0.25;
+          const double w_bulk = 1.0;
+          uin = 1.5 * w_bulk * yc * (2 - yc);
+        }
+        const double ux = 0, uy = 0, uz = uin * area;
+        uc.z[p] = uz; uc.x[p] = ux; uc.y[p] = uy;
+        const double cx = m.csi.x[p], cy = m.csi.y[p], cz = m.csi.z[p];
+        const double ex = m.eta.x[p], ey = m.eta.y[p], ez = m.eta.z[p];
+        const double det = cx * (ey * zz - ez * zy) - cy * (ex * zz - ez * zx) + cz * (ex * zy - ey * zx);
+        const double det0 = ux * (ey * zz - ez * zy) - uy * (cy * zz - cz * zy) + uz * (cy * ez - cz * ey);
+        const double det1 = -ux * (ex * zz - ez * zx) + uy * (cx * zz - cz * zx) - uz * (cx * ez - cz * ex);
+        const double det2 = ux * (ex * zy - ey * zx) - uy * (cx * zy - cy * zx) + uz * (cx * ey - cy * ex);
+        const double vx = det0 / det, vy = det1 / det, vz = det2 / det;
+        ucat.x[p] = -ucat.x[p1] + 2 * vx;
+        ucat.y[p] = -ucat.y[p1] + 2 * vy;
+        ucat.z[p] = -ucat.z[p1] + 2 * vz;
+      }
+    } else {
+      ucat.z[p] = 0;
+      uc.z[p] = 0;
+    }
+    s = uc.z[p];
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
+}
+
+// Flux rescaling of the inlet plane (bcs.c:579-587): Ucont.z += dflux*|zet|/inletArea on
+// faces with a fluid downstream cell, and the partial sums of the new inlet flux.
+__global__ void k_inflow_rescale(Grid g, CV3 zet, V3 uc, const uint8_t *__restrict__ nv, double dflux,
+                                 double inlet_area, double *parts) {
+  __shared__ double sh[256];
+  const int nx = g.mx - 2, ny = g.my - 2;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double s = 0;
+  if (t < (long long)nx * ny) {
+    const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
+    const long long p = lidx(g, i, j, 0), p1 = p + (long long)g.mx * g.my;
+    if (nv[p1] == 0) {
+      const double A = sqrt(zet.x[p] * zet.x[p] + zet.y[p] * zet.y[p] + zet.z[p] * zet.z[p]);
+      uc.z[p] += dflux * A / inlet_area;
+      s = uc.z[p];
+    }
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
+}
+
+int inflow_flux(Ctx *c) {
+  const Grid &g = c->g;
+  if (g.bc[4] != 5) return VFS_OK;  // no k = 0 inlet: FluxInSum keeps its value
+  const int prof = c->cfg.inletprofile;
+  int rc;
+  if (prof == 100 && !c->inflow_plane)
+    return set_err(c, VFS_ERR_STATE, "InflowFlux: inletprofile 100 needs vfs_set_inflow_plane first");
+  if (prof == 21 && !c->inlet_nodes)
+    return set_err(c, VFS_ERR_STATE, "InflowFlux: inletprofile 21 needs the grid nodes (vfs_form_metrics)");
+  const double inlet_flux = c->scal[VFS_S_INLET_FLUX], area = c->scal[VFS_S_INLET_AREA];
+  const double uin = (prof == 2) ? ((inlet_flux < 0) ? 1. : inlet_flux / area) : 0.0;
+  const long long npl = (long long)(g.mx - 2) * (g.my - 2);
+  const int nb = (int)nblocks(npl, 256);
+  if ((rc = ensure_red(c, nb + 64))) return rc;
+  k_inflow<<<nb, 256, 0, c->stream>>>(g, metrics(c), field3(c, VFS_UCONT), field3(c, VFS_UCAT), c->nv, prof, uin,
+                                     c->inflow_plane, c->inlet_nodes ? c->inlet_nodes + 1 * (size_t)(g.mx - 1) * (g.my - 1) : nullptr,
+                                     c->red);
+  if ((rc = check_launch(c, "k_inflow"))) return rc;
+  double flux1 = 0;
+  if ((rc = reduce_sum(c, c->red, nb, &flux1))) return rc;
+  double flux_in = flux1;
+  if (prof == 100 && inlet_flux > 0) {  // bcs.c:572-588 (sumFluxIn0 = inlet_flux)
+    k_inflow_rescale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), field3(c, VFS_UCONT), c->nv,
+                                               inlet_flux - flux1, area, c->red);
+    if ((rc = check_launch(c, "k_inflow_rescale"))) return rc;
+    if ((rc = reduce_sum(c, c->red, nb, &flux_in))) return rc;
+  }
+  c->scal[VFS_S_FLUX_IN] = flux_in;
+  return VFS_OK;
+}
+
 // ------------------------------------------------------------------ FormBCS subset
-// bcs.c:1841-2936 for the codes handled here: Contra2Cart, zero normal flux on no-slip
-// and free-slip walls of the i and j faces (interior range), Contra2Cart again, then the
-// twelve edges of the box get Ucat = 0.
+// bcs.c:1841-2936 for the codes handled here: Contra2Cart; at an outlet on the k = mz-1
+// face (bctype[5] = 4) and with outflow_scale set, the last interior k-face fluxes are
+// shifted by (FluxInSum - FluxOut)*|zet|/Area over faces with a fluid upstream cell
+// (bcs.c:2285-2417); zero normal flux on no-slip and free-slip walls of the i and j faces
+// (interior range); Contra2Cart again; the twelve edges of the box get Ucat = 0.
+__global__ void k_outlet_parts(Grid g, CV3 zet, const double *__restrict__ uz, const uint8_t *__restrict__ nv,
+                               double *parts) {
+  __shared__ double s1[256], s2[256];
+  const int nx = g.mx - 2, ny = g.my - 2;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double f = 0, a = 0;
+  if (t < (long long)nx * ny) {
+    const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
+    const long long p = lidx(g, i, j, g.mz - 2);
+    if (nv[p] == 0) {
+      f = uz[p];
+      a = sqrt(zet.x[p] * zet.x[p] + zet.y[p] * zet.y[p] + zet.z[p] * zet.z[p]);
+    }
+  }
+  s1[threadIdx.x] = f; s2[threadIdx.x] = a;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { s1[threadIdx.x] += s1[threadIdx.x + w]; s2[threadIdx.x] += s2[threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { parts[blockIdx.x] = s1[0]; parts[gridDim.x + blockIdx.x] = s2[0]; }
+}
+
+__global__ void k_outlet_scale(Grid g, CV3 zet, double *uz, const uint8_t *__restrict__ nv, double dflux,
+                               double area_sum) {
+  const int nx = g.mx - 2, ny = g.my - 2;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * ny) return;
+  const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
+  const long long p = lidx(g, i, j, g.mz - 2);
+  const double Area = sqrt(zet.x[p] * zet.x[p] + zet.y[p] * zet.y[p] + zet.z[p] * zet.z[p]);
+  if (nv[p] == 0) uz[p] += dflux * Area / area_sum;
+}
+
 __global__ void k_wall_flux(Grid g, V3 uc) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
@@ -1331,12 +1500,24 @@ __global__ void k_zero_edges(Grid g, V3 u) {
   if (bi + bj + bk >= 2) { u.x[p] = 0; u.y[p] = 0; u.z[p] = 0; }
 }
 
-int form_bcs(Ctx *c) {
+int form_bcs(Ctx *c, bool outflow_scale) {
   int rc;
-  for (int q = 0; q < 6; q++)
-    if (c->g.bc[q] == 4 || c->g.bc[q] == 5)
-      return set_err(c, VFS_ERR_INVALID, "FormBCS: inlet/outlet faces are not handled by this step driver");
   if ((rc = contra2cart(c))) return rc;
+  if (c->g.bc[5] == 4 && outflow_scale) {
+    const Grid &g = c->g;
+    const long long npl = (long long)(g.mx - 2) * (g.my - 2);
+    const int nb = (int)nblocks(npl, 256);
+    if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
+    k_outlet_parts<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv, c->red);
+    if ((rc = check_launch(c, "k_outlet_parts"))) return rc;
+    double flux_out = 0, area_sum = 0;
+    if ((rc = reduce_sum(c, c->red, nb, &flux_out))) return rc;
+    if ((rc = reduce_sum(c, c->red + nb, nb, &area_sum))) return rc;
+    c->scal[VFS_S_FLUX_OUT] = flux_out;
+    k_outlet_scale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv,
+                                             c->scal[VFS_S_FLUX_IN] - flux_out, area_sum);
+    if ((rc = check_launch(c, "k_outlet_scale"))) return rc;
+  }
   k_wall_flux<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
   if ((rc = check_launch(c, "k_wall_flux"))) return rc;
   if ((rc = contra2cart(c))) return rc;
@@ -1345,13 +1526,14 @@ int form_bcs(Ctx *c) {
 }
 
 // ------------------------------------------------------------------ RungeKutta
-// rhs.c:1578-1700 (implicit=0): InflowFlux, FormBCS, then four stages
-//   Contra2Cart; Rhs = Formfunction_2 - dP; Ucont = pUcont + alfa*dt*st*Rhs; Contra2Cart
-// and finally FormBCS again.
+// rhs.c:1578-1700 (implicit=0): InflowFlux, FormBCS without outlet rescaling, then four
+// stages  Contra2Cart; Rhs = Formfunction_2 - dP; Ucont = pUcont + alfa*dt*st*Rhs;
+// Contra2Cart  and finally FormBCS with the outlet rescaling (outflow_scale = 1).
 int runge_kutta(Ctx *c) {
   int rc;
   const double alfa[4] = {0.25, 1 / 3., 0.5, 1.};
-  if ((rc = form_bcs(c))) return rc;
+  if ((rc = inflow_flux(c))) return rc;
+  if ((rc = form_bcs(c, false))) return rc;
   const size_t bytes = sizeof(double) * (size_t)c->g.N;
   for (int q = 0; q < 3; q++)
     cudaMemcpyAsync(c->pucont[q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
@@ -1364,7 +1546,7 @@ int runge_kutta(Ctx *c) {
     if ((rc = formfunction2(c, 1.0, true, a))) return rc;
     if ((rc = contra2cart(c))) return rc;
   }
-  return form_bcs(c);
+  return form_bcs(c, true);
 }
 
 }  // namespace vfs

@@ -37,7 +37,7 @@ METRIC_FIELDS = {
 }
 
 # scalars
-S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST, S_TI = range(8)
+S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST, S_TI, S_FLUX_IN, S_FLUX_OUT = range(10)
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOT_CONVERGED, ERR_NO_DEVICE, ERR_STATE = range(6)
 
@@ -89,7 +89,7 @@ EXPORTS = [
     "vfs_poisson_solve", "vfs_poisson_apply", "vfs_update_pressure", "vfs_projection",
     "vfs_divergence", "vfs_step", "vfs_calc_inlet_area", "vfs_form_bcs", "vfs_ib_bc",
     "vfs_form_metrics", "vfs_volume_flux", "vfs_get_stream", "vfs_run_kernel",
-    "vfs_smagorinsky_constant", "vfs_eddy_viscosity",
+    "vfs_smagorinsky_constant", "vfs_eddy_viscosity", "vfs_inflow_flux", "vfs_set_inflow_plane",
 ]
 
 _lib = None
@@ -122,10 +122,12 @@ def load_library(path=None):
     lib.vfs_field_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     for n in ("vfs_contra2cart", "vfs_pressure_gradient", "vfs_runge_kutta", "vfs_poisson_lhs",
               "vfs_poisson_rhs", "vfs_update_pressure", "vfs_projection", "vfs_calc_inlet_area",
-              "vfs_form_bcs", "vfs_ib_bc", "vfs_volume_flux", "vfs_smagorinsky_constant",
-              "vfs_eddy_viscosity"):
+              "vfs_ib_bc", "vfs_volume_flux", "vfs_smagorinsky_constant",
+              "vfs_eddy_viscosity", "vfs_inflow_flux"):
         getattr(lib, n).argtypes = [vp]
     lib.vfs_formfunction2.argtypes = [vp, ctypes.c_double]
+    lib.vfs_form_bcs.argtypes = [vp, ctypes.c_int]
+    lib.vfs_set_inflow_plane.argtypes = [vp, vp]
     lib.vfs_calc_k_flux.argtypes = [vp, dp]
     lib.vfs_divergence.argtypes = [vp, dp]
     lib.vfs_poisson_solve.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats)]
@@ -251,8 +253,18 @@ class Context:
         self._check(self.lib.vfs_calc_inlet_area(self.h))
         return self.get_scalar(S_MEAN_K_AREA), self.get_scalar(S_INLET_AREA)
 
-    def form_bcs(self):               # FormBCS, bcs.c:1841
-        self._check(self.lib.vfs_form_bcs(self.h))
+    def form_bcs(self, outflow_scale=1):  # FormBCS, bcs.c:1841
+        self._check(self.lib.vfs_form_bcs(self.h, int(outflow_scale)))
+
+    def inflow_flux(self):            # InflowFlux, bcs.c:329
+        self._check(self.lib.vfs_inflow_flux(self.h))
+        return self.get_scalar(S_FLUX_IN)
+
+    def set_inflow_plane(self, plane):  # ucont_plane (read_inflow_section, rhs2.c:701)
+        a = np.ascontiguousarray(plane, dtype=np.float64)
+        if a.size != self.shape[1] * self.shape[2] * 3:
+            raise ValueError("inflow plane: expected my*mx*3 values")
+        self._check(self.lib.vfs_set_inflow_plane(self.h, a.ctypes.data))
 
     def volume_flux(self):            # VolumeFlux, poisson.c:3306 (immersed = 0)
         self._check(self.lib.vfs_volume_flux(self.h))

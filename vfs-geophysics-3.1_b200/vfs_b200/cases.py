@@ -129,6 +129,24 @@ def open_channel_cylinders(nx=256, ny=192, nz=256, Lx=3.2, Ly=1.0, Lz=8.0, D=0.2
     return c
 
 
+def inflow_outflow(case, inletprofile=100):
+    """The same grid and bodies with an inlet on the k = 0 face (bctype 5) and an outlet on
+    the k+ face (bctype 4) instead of streamwise periodicity (bcs.c:329, bcs.c:2285)."""
+    case.bctype[4], case.bctype[5] = 5, 4
+    case.k_periodic = 0
+    case.inletprofile = inletprofile
+    case.name += "_inout%d" % inletprofile
+    return case
+
+
+def inflow_plane(case, seed=0, intensity=0.05, ub=1.0):
+    """A Cartesian inflow velocity plane (my, mx, 3) for inletprofile 100: the mean profile
+    of initial_ucat's first interior k plane plus uniform noise of the given intensity."""
+    u0 = initial_ucat(case, seed=seed, noise=0.0, ub=ub)[1]
+    rng = np.random.Generator(np.random.Philox(seed + 101))
+    return u0 + intensity * ub * (2.0 * rng.random(u0.shape) - 1.0)
+
+
 def initial_ucat(case, seed=0, noise=0.1, ub=1.0):
     """Cartesian velocity on the DA cell centres: laminar parabola w = 1.5*Ub*y(2-y)/... in
     the streamwise (z) direction plus uniform noise in +-noise*Ub on all components from a
