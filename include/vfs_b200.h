@@ -147,6 +147,18 @@ int vfs_field_device_ptr(vfs_ctx *ctx, int field, int component, void **dptr);
  * init.c:384-437).  Fills VFS_CENT and every centre and face metric field. */
 int vfs_form_metrics(vfs_ctx *ctx, const double *x, const double *y, const double *z);
 
+/* ibm_search_advanced (ibm.c:85-587), the nvert flags of body ibi: cells whose centre lies
+ * inside the closed triangulated surface become 3, the cells around them 1 (2 on ghost
+ * points, as the reference leaves them), bit for bit with the reference's ray casting
+ * (point_cell_advanced ibm.c:1068, randomdirection ibm.c:52, intsect_triangle
+ * compgeom.c:17).  The surface is given as the reference's reader leaves it in IBMNodes
+ * (ibm_io.c:582-905): n_v vertices x/y/z and n_elmt triangles of 0-based vertex indices
+ * nv1/nv2/nv3.  Body 0 starts from zero flags; later bodies add to them.  Needs the cell
+ * centres (vfs_form_metrics or VFS_CENT); updates VFS_NVERT.  The IB-node interpolation
+ * list that the reference builds next is not formed. */
+int vfs_ibm_search(vfs_ctx *ctx, int ibi, int n_v, const double *x, const double *y, const double *z,
+                   int n_elmt, const int *nv1, const int *nv2, const int *nv3);
+
 /* ---- hot-path operators (each replaces the cited reference function) --------------- */
 
 /* Contra2Cart / Contra2Cart_2 (rhs.c:27, rhs.c:57): Ucat from Ucont at fluid cells,

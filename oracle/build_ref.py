@@ -27,7 +27,7 @@ LIB = os.path.join(OUT, "libvfsref.so")
 REF_SOURCES = [
     "main.c", "init.c", "metrics.c", "momentum.c", "rhs.c", "rhs2.c", "k-omega.c",
     "poisson.c", "poisson_hypre.c", "les.c", "bcs.c", "wallfunction.c", "ibm.c",
-    "compgeom.c", "level.c",
+    "compgeom.c", "level.c", "variables.c",
 ]
 CXXFLAGS = ["-std=c++11", "-O2", "-fPIC", "-w", "-fpermissive", "-ffp-contract=off",
             "-DNDEBUG", "-I" + SHIM]

@@ -54,6 +54,7 @@ def lib():
         L.ref_form_bcs_scaled.argtypes = [ctypes.c_int]
         L.ref_flux_in.restype = ctypes.c_double
         L.ref_set_inflow_plane.argtypes = [vp]
+        L.ref_ibm_classify.argtypes = [ctypes.c_int] * 2 + [vp] * 3 + [ctypes.c_int] + [vp] * 3
         _lib = L
     return _lib
 
@@ -171,6 +172,16 @@ class Reference:
 
     def inlet_area(self):
         return lib().ref_inlet_area()
+
+    def ibm_classify(self, x, y, z, tri, ibi=0):
+        """The nvert flags of ibm_search_advanced (ibm.c:85) for body ibi, classified by the
+        reference's own point_cell_advanced (see ref_driver.cpp); returns lNvert."""
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+        t = np.ascontiguousarray(tri, dtype=np.int32)
+        cols = [np.ascontiguousarray(t[:, q]) for q in range(3)]
+        self.call("ref_ibm_classify", ibi, len(xs[0]), xs[0].ctypes.data, xs[1].ctypes.data, xs[2].ctypes.data,
+                  len(t), cols[0].ctypes.data, cols[1].ctypes.data, cols[2].ctypes.data)
+        return self.get("lNvert")
 
     def flux_in(self):
         """FluxInSum after the last InflowFlux (bcs.c:778)."""

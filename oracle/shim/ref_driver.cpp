@@ -13,6 +13,7 @@
 #include "variables.h"
 
 #include <string>
+#include <vector>
 
 extern PetscInt ti, tistart;
 extern char path[256], gridfile[256];
@@ -30,6 +31,12 @@ extern void PoissonRHS2_hypre(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 extern void Remove_Nullspace(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 
 extern double inletArea;
+extern PetscInt point_cell_advanced(Cmpnts p, PetscInt ip, PetscInt jp, PetscInt kp, IBMNodes *ibm, PetscInt ncx,
+                                    PetscInt ncy, PetscInt ncz, PetscReal dcx, PetscReal dcy, PetscReal xbp_min,
+                                    PetscReal ybp_min, PetscReal zbp_max, LIST *cell_trg, PetscInt flg);
+extern void initlist(LIST *ilist);
+extern void insertnode(LIST *ilist, PetscInt Node);
+extern void destroy(LIST *ilist);
 extern int ucont_plane_allocated;  // main.c:238
 extern int outflow_scale;          // bcs.c:1839
 extern int k_area_allocated;  // bcs.c:213, once per process in the reference
@@ -206,6 +213,103 @@ int ref_les(int recompute_cs) {
 }
 int ref_volume_flux(double *flux, double *area) {
   return VolumeFlux(g_user, g_user->Ucont, flux, area);
+}
+
+// The nvert classification of ibm_search_advanced (ibm.c:85-345, 507-514) for body ibi,
+// with the reference's own ray test: the bins are built with its list functions
+// (initlist/insertnode, variables.c:3-27) over the same bin ranges (ibm.c:132-198), every
+// cell centre inside the widened box is classified by its point_cell_advanced (ibm.c:1068,
+// with randomdirection and intsect_triangle), then the near-boundary marking and the
+// 2 -> 1, 4 -> 3 remap follow ibm.c:322-345 and 507-514.  ibm_search_advanced itself goes
+// on to build the IB-node interpolation list; under this shim that call does not return,
+// so the driver runs the classification steps around the reference's ray test instead.
+// Surface as the reader leaves it (ibm_io.c:582-905), normals formed as it forms them.
+int ref_ibm_classify(int ibi, int n_v, const double *x, const double *y, const double *z, int n_elmt,
+                     const int *n1, const int *n2, const int *n3) {
+  IBMNodes &ibm = *(IBMNodes *)calloc(1, sizeof(IBMNodes));  // too large for the stack
+  ibm.n_v = n_v;
+  ibm.n_elmt = n_elmt;
+  ibm.x_bp = (PetscReal *)x; ibm.y_bp = (PetscReal *)y; ibm.z_bp = (PetscReal *)z;
+  std::vector<PetscInt> v1(n1, n1 + n_elmt), v2(n2, n2 + n_elmt), v3(n3, n3 + n_elmt);
+  std::vector<PetscReal> fx(n_elmt), fy(n_elmt), fz(n_elmt);
+  ibm.nv1 = v1.data(); ibm.nv2 = v2.data(); ibm.nv3 = v3.data();
+  for (int e = 0; e < n_elmt; e++) {
+    const double dx12 = x[n2[e]] - x[n1[e]], dy12 = y[n2[e]] - y[n1[e]], dz12 = z[n2[e]] - z[n1[e]];
+    const double dx13 = x[n3[e]] - x[n1[e]], dy13 = y[n3[e]] - y[n1[e]], dz13 = z[n3[e]] - z[n1[e]];
+    double nx = dy12 * dz13 - dz12 * dy13, ny = -dx12 * dz13 + dz12 * dx13, nz = dx12 * dy13 - dy12 * dx13;
+    const double dr = sqrt(nx * nx + ny * ny + nz * nz);
+    fx[e] = nx / dr; fy[e] = ny / dr; fz[e] = nz / dr;
+  }
+  ibm.nf_x = fx.data(); ibm.nf_y = fy.data(); ibm.nf_z = fz.data();
+  const int ncx = 40, ncy = 40, ncz = 40;
+  double xmin = 1.e23, xmax = -1.e23, ymin = 1.e23, ymax = -1.e23, zmin = 1.e23, zmax = -1.e23;
+  for (int q = 0; q < n_v; q++) {
+    xmin = PetscMin(xmin, x[q]); xmax = PetscMax(xmax, x[q]);
+    ymin = PetscMin(ymin, y[q]); ymax = PetscMax(ymax, y[q]);
+    zmin = PetscMin(zmin, z[q]); zmax = PetscMax(zmax, z[q]);
+  }
+  xmin -= 0.05; xmax += 0.05; ymin -= 0.05; ymax += 0.05; zmin -= 0.05; zmax += 0.05;
+  const double dcx = (xmax - xmin) / (ncx - 1.), dcy = (ymax - ymin) / (ncy - 1.), dcz = (zmax - zmin) / (ncz - 1.);
+  std::vector<LIST> bins(ncx * ncy * ncz);
+  for (auto &l : bins) initlist(&l);
+  for (int e = 0; e < n_elmt; e++) {
+    const int a = n1[e], b = n2[e], c = n3[e];
+    PetscInt i0 = floor((PetscMin(PetscMin(x[a], x[b]), x[c]) - xmin) / dcx);
+    PetscInt i1 = floor((PetscMax(PetscMax(x[a], x[b]), x[c]) - xmin) / dcx) + 1;
+    PetscInt j0 = floor((PetscMin(PetscMin(y[a], y[b]), y[c]) - ymin) / dcy);
+    PetscInt j1 = floor((PetscMax(PetscMax(y[a], y[b]), y[c]) - ymin) / dcy) + 1;
+    PetscInt k0 = floor((PetscMin(PetscMin(z[a], z[b]), z[c]) - zmin) / dcz);
+    PetscInt k1 = floor((PetscMax(PetscMax(z[a], z[b]), z[c]) - zmin) / dcz) + 1;
+    i0 = i0 < 0 ? 0 : i0; i1 = i1 > ncx ? ncx : i1;
+    j0 = j0 < 0 ? 0 : j0; j1 = j1 > ncx ? ncy : j1;
+    k0 = k0 < 0 ? 0 : k0; k1 = k1 > ncz ? ncz : k1;
+    for (int k = k0; k < k1; k++)
+      for (int j = j0; j < j1; j++)
+        for (int i = i0; i < i1; i++) insertnode(&bins[k * ncx * ncy + j * ncx + i], e);
+  }
+  const int mx = g_user->info.mx, my = g_user->info.my, mz = g_user->info.mz;
+  Vec lcent = g_user->lCent, lnv = g_user->lNvert;
+  auto at = [&](int i, int j, int k) { return ((long)k * my + j) * mx + i; };
+  double *nv = lnv->data;
+  const Cmpnts *cent = (const Cmpnts *)lcent->data;
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        const long p = at(i, j, k);
+        if (ibi == 0 && nv[p] < 5.) nv[p] = 0;
+        const Cmpnts c = cent[p];
+        if (c.x > xmin && c.x < xmax && c.y > ymin && c.y < ymax && c.z > zmin && c.z < zmax) {
+          const PetscInt ic = floor((c.x - xmin) / dcx), jc = floor((c.y - ymin) / dcy), kc = floor((c.z - zmin) / dcz);
+          const double val = point_cell_advanced(c, ic, jc, kc, &ibm, ncx, ncy, ncz, dcx, dcy, xmin, ymin, zmax,
+                                                 bins.data(), 0);
+          nv[p] = PetscMax(nv[p], val);
+          if (nv[p] < 0) nv[p] = 0;
+        }
+      }
+  for (int k = 0; k < mz; k++)
+    for (int j = 0; j < my; j++)
+      for (int i = 0; i < mx; i++) {
+        const long p = at(i, j, k);
+        if ((int)(nv[p] + 0.5) == 4) continue;
+        const int ip = i < mx - 1 ? i + 1 : i, im = i > 0 ? i - 1 : i;
+        const int jp = j < my - 1 ? j + 1 : j, jm = j > 0 ? j - 1 : j;
+        const int kp = k < mz - 1 ? k + 1 : k, km = k > 0 ? k - 1 : k;
+        for (int kk = km; kk <= kp; kk++)
+          for (int jj = jm; jj <= jp; jj++)
+            for (int ii = im; ii <= ip; ii++)
+              if ((int)(nv[at(ii, jj, kk)] + 0.5) == 4) nv[p] = PetscMax(2, nv[p]);
+      }
+  for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+      for (int i = 1; i < mx - 1; i++) {
+        const long p = at(i, j, k);
+        if ((int)(nv[p] + 0.5) == 2) nv[p] = 1;
+        if ((int)(nv[p] + 0.5) == 4) nv[p] = 3;
+      }
+  VecCopy(lnv, g_user->Nvert);
+  for (auto &l : bins) destroy(&l);
+  free(&ibm);
+  return 0;
 }
 
 // PoissonLHSNew (poisson.c:971); the matrix stays recorded in user->A.

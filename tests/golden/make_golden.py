@@ -20,6 +20,9 @@ phi) and the reference outputs:
   ax           the PoissonLHSNew operator applied to a seeded x (x also stored)
   p_up, ucont_proj, ucat_proj   UpdatePressure and Projection for the stored phi
 and, for the wavy channel, the metrics of FormMetrics (metrics.c:4).
+
+ibm_sphere_wavy_24x20x28.npz holds a triangulated sphere and the nvert flags that the
+reference's ray test (point_cell_advanced, ibm.c:1068) gives it in the wavy channel.
 """
 import os
 import sys
@@ -133,8 +136,22 @@ def make(name):
     return fixture_path(name)
 
 
+def make_ibm(name="ibm_sphere_wavy_24x20x28"):
+    """nvert of an icosphere (1280 triangles, centre (pi/2, 1, pi), radius 0.4) in the wavy
+    channel, classified by the reference's own ray test (ref_ibm_classify)."""
+    case = cases.channel(24, 20, 28, wavy=0.1)
+    case.immersed = 1
+    R = ref.Reference(case)
+    x, y, z, tri = cases.icosphere((np.pi / 2, 1.0, np.pi), 0.4, level=3)
+    nv = R.ibm_classify(x, y, z, tri)
+    R.close()
+    np.savez_compressed(fixture_path(name), X=case.X, Y=case.Y, Z=case.Z, sx=x, sy=y, sz=z, tri=tri, nvert=nv)
+    return fixture_path(name)
+
+
 if __name__ == "__main__":
     if not ref.available():
         sys.exit("oracle/_ref is not built (python oracle/build_ref.py)")
     for n in FIXTURES:
         print(make(n), os.path.getsize(fixture_path(n)))
+    print(make_ibm(), os.path.getsize(fixture_path("ibm_sphere_wavy_24x20x28")))

@@ -83,3 +83,20 @@ def test_restatement_les_matches_fixture(name):
     cs = restatement.les(st, ti=5)
     np.testing.assert_array_equal(cs, d["cs_les"])
     np.testing.assert_array_equal(st.nut, d["nut_les"])
+
+
+def test_ibm_fixture_is_the_reference_classification():
+    """The committed nvert fixture is what the reference's ray test gives (when oracle/_ref
+    is built here), and holds solid and IB-node cells."""
+    d = np.load(os.path.join(ROOT, "tests", "golden", "ibm_sphere_wavy_24x20x28.npz"))
+    assert (d["nvert"] == 3).sum() > 0 and (d["nvert"] == 1).sum() > 0
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    from vfs_b200 import cases
+    case = cases.channel(24, 20, 28, wavy=0.1)
+    case.immersed = 1
+    R = ref.Reference(case)
+    got = R.ibm_classify(d["sx"], d["sy"], d["sz"], d["tri"])
+    R.close()
+    np.testing.assert_array_equal(got, d["nvert"])

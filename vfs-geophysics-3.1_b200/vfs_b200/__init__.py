@@ -90,6 +90,7 @@ EXPORTS = [
     "vfs_divergence", "vfs_step", "vfs_calc_inlet_area", "vfs_form_bcs", "vfs_ib_bc",
     "vfs_form_metrics", "vfs_volume_flux", "vfs_get_stream", "vfs_run_kernel",
     "vfs_smagorinsky_constant", "vfs_eddy_viscosity", "vfs_inflow_flux", "vfs_set_inflow_plane",
+    "vfs_ibm_search",
 ]
 
 _lib = None
@@ -128,6 +129,7 @@ def load_library(path=None):
     lib.vfs_formfunction2.argtypes = [vp, ctypes.c_double]
     lib.vfs_form_bcs.argtypes = [vp, ctypes.c_int]
     lib.vfs_set_inflow_plane.argtypes = [vp, vp]
+    lib.vfs_ibm_search.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
     lib.vfs_calc_k_flux.argtypes = [vp, dp]
     lib.vfs_divergence.argtypes = [vp, dp]
     lib.vfs_poisson_solve.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats)]
@@ -233,6 +235,17 @@ class Context:
 
     def synchronize(self):
         self._check(self.lib.vfs_synchronize(self.h))
+
+    def ibm_search(self, x, y, z, tri, ibi=0):  # ibm_search_advanced, ibm.c:85
+        """nvert flags of a closed triangulated surface (vertices x, y, z; (n, 3) 0-based
+        triangles); returns the new nvert field."""
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+        t = np.ascontiguousarray(tri, dtype=np.int32)
+        cols = [np.ascontiguousarray(t[:, q]) for q in range(3)]
+        self._check(self.lib.vfs_ibm_search(self.h, ibi, len(xs[0]), xs[0].ctypes.data, xs[1].ctypes.data,
+                                            xs[2].ctypes.data, len(t), cols[0].ctypes.data, cols[1].ctypes.data,
+                                            cols[2].ctypes.data))
+        return self.get_field(NVERT)
 
     # ---- operators (reference names in comments)
     def contra2cart(self):            # Contra2Cart, rhs.c:27

@@ -129,6 +129,48 @@ def open_channel_cylinders(nx=256, ny=192, nz=256, Lx=3.2, Ly=1.0, Lz=8.0, D=0.2
     return c
 
 
+def icosphere(center=(0.0, 0.0, 0.0), radius=0.5, level=3):
+    """Closed triangulated sphere: an icosahedron subdivided `level` times (20*4**level
+    triangles, outward-oriented), its vertices pushed onto the sphere.  Returns the vertex
+    coordinates x, y, z and the (n_elmt, 3) array of 0-based vertex indices, the form the
+    reference's surface reader leaves in IBMNodes (ibm_io.c:582-905)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(v, dtype=np.float64) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(level):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    v = np.array(verts) * radius + np.asarray(center, dtype=np.float64)
+    return v[:, 0].copy(), v[:, 1].copy(), v[:, 2].copy(), np.array(faces, dtype=np.int32)
+
+
+def write_ucd(path, x, y, z, tri):
+    """The surface in the reference's ibmdata UCD form (ibm_io.c:609-905): three header
+    lines, 'n_v n_elmt 0 0 0', the vertices, then 1-based triangles."""
+    with open(path, "w") as f:
+        f.write("# UCD surface\n#\n#\n%d %d 0 0 0\n" % (len(x), len(tri)))
+        for q in range(len(x)):
+            f.write("%d %.17e %.17e %.17e\n" % (q + 1, x[q], y[q], z[q]))
+        for e, (a, b, c) in enumerate(tri):
+            f.write("%d 0 tri %d %d %d\n" % (e + 1, a + 1, b + 1, c + 1))
+
+
 def inflow_outflow(case, inletprofile=100):
     """The same grid and bodies with an inlet on the k = 0 face (bctype 5) and an outlet on
     the k+ face (bctype 4) instead of streamwise periodicity (bcs.c:329, bcs.c:2285)."""
