@@ -188,10 +188,14 @@ double ref_flux_in(void) { return FluxInSum; }
 // read_inflow_section fills it, rhs2.c:712-722).
 int ref_set_inflow_plane(const double *plane) {
   const int mx = g_user->info.mx, my = g_user->info.my;
-  if (!ucont_plane_allocated) {
+  // read_inflow_section allocates the plane once per process (ucont_plane_allocated); each
+  // oracle set-up builds a new UserCtx, which gets its own plane here
+  static UserCtx *owner = 0;
+  if (owner != g_user) {
     ucont_plane_allocated = 1;
     g_user->ucont_plane = (Cmpnts **)malloc(sizeof(Cmpnts *) * my);
     for (int j = 0; j < my; j++) g_user->ucont_plane[j] = (Cmpnts *)malloc(sizeof(Cmpnts) * mx);
+    owner = g_user;
   }
   for (int j = 0; j < my; j++)
     for (int i = 0; i < mx; i++) {
