@@ -2,11 +2,14 @@
 
 Workload: the 256 x 192 x 256-cell open channel with a staggered 3 x 2 array of vertical
 cylinders (D = 0.2, spacing 4D) encoded in nvert as blocked cells (immersed = 0), no-slip
-bottom, free-slip top, periodic spanwise and streamwise with the bulk flux held by the
-k-periodic forcing; seeded turbulent-like initial field (log-law mean plus random Fourier
-modes with a k^-5/3 spectrum, 5 % intensity).  One step = Flow_Solver for implicit = 0:
-Calc_k_Flux, Pressure_Gradient, 4-stage RungeKutta, VolumeFlux, Poisson RHS, Poisson
-solve to rtol 1e-10, UpdatePressure, Projection, Divergence, IB_BC, Contra2Cart.
+bottom, free-slip top, spanwise periodic, an inlet on the k = 0 face (bctype 5, inflow
+plane of inletprofile 100 rescaled to bulk velocity 1) and an outlet on the k+ face
+(bctype 4, outflow rescaled to the inflow); seeded turbulent-like field (log-law mean plus
+random Fourier modes with a k^-5/3 spectrum, 5 % intensity), whose first plane is the
+inflow plane.  One step = Flow_Solver for implicit = 0: Calc_k_Flux, Pressure_Gradient,
+4-stage RungeKutta (InflowFlux, FormBCS, stages, FormBCS with outlet rescaling),
+VolumeFlux, Poisson RHS, Poisson solve to rtol 1e-10, UpdatePressure, Projection,
+Divergence, IB_BC, Contra2Cart.
 
 `value` is the mixed-precision (FP32 V-cycle in FP64 FGMRES) step time in ms with every
 field resident in HBM; the all-FP64 form is timed on the same state for the comparison.
@@ -39,8 +42,9 @@ sys.path.insert(0, os.path.join(ROOT, "vfs-geophysics-3.1_b200"))
 METRIC = "ms/step @256x192x256: mixed vs FP64 GPU at max|div u|<=1e-8; adjoint/forward ratio"
 NX, NY, NZ = 256, 192, 256
 WORKLOAD = ("open channel 256x192x256 cells, 3x2 staggered cylinders D=0.2 spacing 4D as nvert "
-            "blocked cells (immersed=0), no-slip bottom, free-slip top, periodic i and k with "
-            "k-periodic flux forcing; Poisson rtol 1e-10")
+            "blocked cells (immersed=0), no-slip bottom, free-slip top, periodic i, inlet k=0 "
+            "(inletprofile 100: log-law + k^-5/3 Fourier-mode plane, bulk velocity 1), outlet k+ "
+            "with flux rescaling; Poisson rtol 1e-10")
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -84,7 +88,7 @@ class quiet_stdout:
 # ------------------------------------------------------------------ workload
 def make_case(nx=NX, ny=NY, nz=NZ):
     from vfs_b200 import cases
-    c = cases.open_channel_cylinders(nx, ny, nz)
+    c = cases.inflow_outflow(cases.open_channel_cylinders(nx, ny, nz), 100)
     c.immersed = 0
     return c
 
@@ -129,6 +133,7 @@ def setup_context(case):
     ctx.set_field(vfs.UCONT, uc)
     ctx.set_field(vfs.UCAT, u)
     ctx.set_field(vfs.UCAT_O, u)
+    ctx.set_inflow_plane(u[1])
     _, inlet_area = ctx.calc_inlet_area()
     ctx.set_scalar(vfs.S_INLET_FLUX, 1.0 * inlet_area)   # bulk velocity 1
     ctx.contra2cart()
@@ -269,6 +274,7 @@ def _reference_sample(nx, ny, nz, seed):
         R.set(n, uc)
     for n in ("Ucat", "lUcat", "lUcat_old"):
         R.set(n, u)
+    R.set_inflow_plane(u[1])
     ref.set_global("inlet_flux", R.inlet_area())
     R.call("ref_poisson_lhs")   # first-step set-up, outside the timed sample
     t0 = time.perf_counter()
