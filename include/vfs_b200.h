@@ -89,7 +89,8 @@ enum {
   VFS_S_TI = 7,           /* time step index ti (main.c:3534); vfs_step advances it */
   VFS_S_FLUX_IN = 8,      /* FluxInSum: inlet flux of the last InflowFlux (bcs.c:785) */
   VFS_S_FLUX_OUT = 9,     /* FluxOutSum: outlet flux before the last rescaling (bcs.c:2369) */
-  VFS_NSCALARS = 10
+  VFS_S_IB_UNRESOLVED = 10, /* IB nodes whose interception search failed ("IBM Searching Fail!") */
+  VFS_NSCALARS = 11
 };
 
 /* Poisson solver options (replaces PoissonSolver_Hypre, poisson_hypre.c:498). */
@@ -154,10 +155,26 @@ int vfs_form_metrics(vfs_ctx *ctx, const double *x, const double *y, const doubl
  * compgeom.c:17).  The surface is given as the reference's reader leaves it in IBMNodes
  * (ibm_io.c:582-905): n_v vertices x/y/z and n_elmt triangles of 0-based vertex indices
  * nv1/nv2/nv3.  Body 0 starts from zero flags; later bodies add to them.  Needs the cell
- * centres (vfs_form_metrics or VFS_CENT); updates VFS_NVERT.  The IB-node interpolation
- * list that the reference builds next is not formed. */
+ * centres (vfs_form_metrics or VFS_CENT); updates VFS_NVERT.  It also builds the body's
+ * IB-node list (ibm.c:347-505): for each cell marked near the surface, the nearest surface
+ * point (nearestcell1 ibm.c:1366), the interception of the surface normal with the
+ * neighbouring cell-centre triangles (InterceptionPoint ibm.c:1759) and the three fluid
+ * cells interpolated across it; body 0 starts a new list, later bodies append. */
 int vfs_ibm_search(vfs_ctx *ctx, int ibi, int n_v, const double *x, const double *y, const double *z,
                    int n_elmt, const int *nv1, const int *nv2, const int *nv3);
+
+/* The IB-node list: returns its length; with ints/dbls, copies up to cap nodes, 14 ints
+ * each (i j k, nearest triangle, interception mode, stencil i1 j1 k1 i2 j2 k2 i3 j3 k3)
+ * and 8 doubles each (stencil weights cr1..cr3, surface weights cs1..cs3, d_s, d_i).
+ * A negative return is -VFS_ERR_*. */
+int vfs_ibm_list(vfs_ctx *ctx, int *ints, double *dbls, int cap);
+
+/* ibm_interpolation_advanced (ibm.c:3294) for fixed bodies with the no-slip
+ * reconstruction (noslip, wallfunction.c:134): IB-node Ucat = (d_s/(d_s+d_i)) x the velocity
+ * interpolated at its stencil (zero next to non-fluid stencil cells), IB-node P from its
+ * stencil, the face fluxes around IB nodes from the averaged Ucat, then Contra2Cart.
+ * vfs_step calls it where Flow_Solver and RungeKutta do when immersed = 1. */
+int vfs_ibm_interpolation(vfs_ctx *ctx);
 
 /* ---- hot-path operators (each replaces the cited reference function) --------------- */
 
@@ -207,12 +224,15 @@ int vfs_set_inflow_plane(vfs_ctx *ctx, const double *plane);
  * calls it with outflow_scale 0 before the stages and 1 after them (rhs.c:1598, 1670). */
 int vfs_form_bcs(vfs_ctx *ctx, int outflow_scale);
 
-/* IB_BC (momentum.c:1982) without immersed bodies: zero normal flux on free-slip faces,
- * periodic normal flux on ghost planes. */
+/* IB_BC (momentum.c:1982): with immersed = 1 the face fluxes around IB nodes from the
+ * averaged Ucat; zero normal flux on free-slip faces, periodic normal flux on ghost
+ * planes. */
 int vfs_ib_bc(vfs_ctx *ctx);
 
-/* VolumeFlux(user, Ucont, ...) (poisson.c:3306) for immersed = 0: zero flux through
- * every interior face between a fluid and a non-fluid cell (blocked-cell bodies). */
+/* VolumeFlux: for immersed = 0 VolumeFlux(user, Ucont, ...) (poisson.c:3306), zero flux
+ * through every interior face between a fluid and a non-fluid cell (blocked-cell bodies);
+ * for immersed = 1 VolumeFlux(user, &flux, &area, 0) (poisson.c:3570), the net flux through
+ * the fluid/IB-node faces spread back over them in proportion to their area. */
 int vfs_volume_flux(vfs_ctx *ctx);
 
 /* RungeKutta (rhs.c:1578), explicit momentum predictor, 4 stages: InflowFlux, FormBCS,

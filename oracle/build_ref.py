@@ -37,12 +37,21 @@ def _run(cmd, **kw):
     return subprocess.run(cmd, check=False, capture_output=True, text=True, **kw)
 
 
+# ibm.c has non-void functions that end without a return (nearestcell1, ibm.c:1366-1512);
+# g++ 13 at -O2 treats the missing return as unreachable and the generated code runs on
+# past the function's end.  At -O0 the end becomes a single trap instruction, which the
+# oracle driver catches (ref_driver.cpp, call_nearestcell1).  SSE2 double arithmetic is the
+# same at either level.
+O0_SOURCES = ("ibm.c",)
+
+
 def _compile(src, obj, extra_inc):
-    newest = max(os.path.getmtime(src),
+    newest = max(os.path.getmtime(src), os.path.getmtime(os.path.abspath(__file__)),
                  max(os.path.getmtime(os.path.join(SHIM, h)) for h in os.listdir(SHIM)))
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return
-    r = _run(["g++"] + CXXFLAGS + ["-I" + extra_inc, "-c", src, "-o", obj])
+    flags = [("-O0" if f == "-O2" and os.path.basename(src) in O0_SOURCES else f) for f in CXXFLAGS]
+    r = _run(["g++"] + flags + ["-I" + extra_inc, "-c", src, "-o", obj])
     if r.returncode != 0:
         raise RuntimeError("oracle/_ref: compile failed for %s\n%s" % (src, r.stderr[-4000:]))
 

@@ -51,10 +51,13 @@ def lib():
         L.ref_les.argtypes = [ctypes.c_int]
         L.ref_inlet_area.restype = ctypes.c_double
         L.ref_volume_flux.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
+        L.ref_volume_flux_ibm.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
         L.ref_form_bcs_scaled.argtypes = [ctypes.c_int]
         L.ref_flux_in.restype = ctypes.c_double
         L.ref_set_inflow_plane.argtypes = [vp]
-        L.ref_ibm_classify.argtypes = [ctypes.c_int] * 2 + [vp] * 3 + [ctypes.c_int] + [vp] * 3
+        L.ref_ibm_classify.argtypes = [ctypes.c_int] * 2 + [vp] * 3 + [ctypes.c_int] + [vp] * 3 + [ctypes.c_int]
+        L.ref_ibm_list.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int]
+        L.ref_ibm_interpolation.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
 
@@ -170,18 +173,36 @@ class Reference:
         lib().ref_volume_flux(ctypes.byref(f), ctypes.byref(a))
         return f.value, a.value
 
+    def volume_flux_ibm(self):
+        """VolumeFlux(user, &ibm_Flux, &ibm_Area, 0) (poisson.c:3570), the immersed = 1 form;
+        returns (ibm_Flux, ibm_Area)."""
+        f, a = ctypes.c_double(), ctypes.c_double()
+        lib().ref_volume_flux_ibm(ctypes.byref(f), ctypes.byref(a))
+        return f.value, a.value
+
     def inlet_area(self):
         return lib().ref_inlet_area()
 
-    def ibm_classify(self, x, y, z, tri, ibi=0):
+    def ibm_classify(self, x, y, z, tri, ibi=0, build_list=False):
         """The nvert flags of ibm_search_advanced (ibm.c:85) for body ibi, classified by the
-        reference's own point_cell_advanced (see ref_driver.cpp); returns lNvert."""
+        reference's own point_cell_advanced (see ref_driver.cpp), and with build_list its
+        IB-node list from the reference's nearestcell1/InterceptionPoint; returns lNvert."""
         xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
         t = np.ascontiguousarray(tri, dtype=np.int32)
         cols = [np.ascontiguousarray(t[:, q]) for q in range(3)]
         self.call("ref_ibm_classify", ibi, len(xs[0]), xs[0].ctypes.data, xs[1].ctypes.data, xs[2].ctypes.data,
-                  len(t), cols[0].ctypes.data, cols[1].ctypes.data, cols[2].ctypes.data)
+                  len(t), cols[0].ctypes.data, cols[1].ctypes.data, cols[2].ctypes.data, int(build_list))
         return self.get("lNvert")
+
+    def ibm_list(self, ibi=0):
+        """The IB-node list (ints (n, 14): i j k cell imode i1 j1 k1 i2 j2 k2 i3 j3 k3; doubles
+        (n, 8): cr1..3 cs1..3 d_s d_i), in list order."""
+        L = lib()
+        n = L.ref_ibm_list(ibi, None, None, 0)
+        ints = np.zeros((n, 14), dtype=np.int32)
+        dbls = np.zeros((n, 8))
+        L.ref_ibm_list(ibi, ints.ctypes.data, dbls.ctypes.data, n)
+        return ints, dbls
 
     def flux_in(self):
         """FluxInSum after the last InflowFlux (bcs.c:778)."""

@@ -12,6 +12,8 @@
 // lUstar (main.c:2245) and Flow_Solver adds Fp/Div*/Visc* (solvers.c:779-785).
 #include "variables.h"
 
+#include <csetjmp>
+#include <csignal>
 #include <string>
 #include <vector>
 
@@ -35,6 +37,10 @@ extern PetscInt point_cell_advanced(Cmpnts p, PetscInt ip, PetscInt jp, PetscInt
                                     PetscInt ncy, PetscInt ncz, PetscReal dcx, PetscReal dcy, PetscReal xbp_min,
                                     PetscReal ybp_min, PetscReal zbp_max, LIST *cell_trg, PetscInt flg);
 extern void initlist(LIST *ilist);
+extern PetscErrorCode BoundingSphere(IBMNodes *ibm);
+extern PetscErrorCode nearestcell1(Cmpnts p, IBMNodes *ibm, IBMInfo *ibminfo);
+extern PetscErrorCode InterceptionPoint(Cmpnts p, PetscInt i, PetscInt j, PetscInt k, IBMInfo *ibminfo, UserCtx *user);
+extern IBMNodes *ibm_ptr;  // main.c:296
 extern void insertnode(LIST *ilist, PetscInt Node);
 extern void destroy(LIST *ilist);
 extern int ucont_plane_allocated;  // main.c:238
@@ -218,6 +224,27 @@ int ref_les(int recompute_cs) {
 int ref_volume_flux(double *flux, double *area) {
   return VolumeFlux(g_user, g_user->Ucont, flux, area);
 }
+// VolumeFlux(user, &ibm_Flux, &ibm_Area, 0) (poisson.c:3570), the immersed = 1 overload.
+int ref_volume_flux_ibm(double *flux, double *area) {
+  return VolumeFlux(g_user, flux, area, 0);
+}
+
+// nearestcell1 (ibm.c:1366-1512) ends without a return statement; g++ 13 compiles the end
+// of the function to a trap instruction (ud2) at every optimisation level.  Everything the
+// function computes is stored before that point, so the driver calls it under a SIGILL
+// handler that jumps back to the call site: the reference's own arithmetic, run to its
+// last statement.
+static sigjmp_buf g_trap_jmp;
+static void on_trap(int) { siglongjmp(g_trap_jmp, 1); }
+static void call_nearestcell1(Cmpnts p, IBMNodes *ibm, IBMInfo *info) {
+  struct sigaction sa, old;
+  memset(&sa, 0, sizeof(sa));
+  sa.sa_handler = on_trap;
+  sigemptyset(&sa.sa_mask);
+  sigaction(SIGILL, &sa, &old);
+  if (sigsetjmp(g_trap_jmp, 1) == 0) nearestcell1(p, ibm, info);
+  sigaction(SIGILL, &old, 0);
+}
 
 // The nvert classification of ibm_search_advanced (ibm.c:85-345, 507-514) for body ibi,
 // with the reference's own ray test: the bins are built with its list functions
@@ -229,14 +256,24 @@ int ref_volume_flux(double *flux, double *area) {
 // so the driver runs the classification steps around the reference's ray test instead.
 // Surface as the reader leaves it (ibm_io.c:582-905), normals formed as it forms them.
 int ref_ibm_classify(int ibi, int n_v, const double *x, const double *y, const double *z, int n_elmt,
-                     const int *n1, const int *n2, const int *n3) {
-  IBMNodes &ibm = *(IBMNodes *)calloc(1, sizeof(IBMNodes));  // too large for the stack
+                     const int *n1, const int *n2, const int *n3, int build_list) {
+  IBMNodes &ibm = g_ibm[ibi];  // heap storage of ref_setup (the struct is too large for the stack)
+  memset(&ibm, 0, sizeof(IBMNodes));
   ibm.n_v = n_v;
   ibm.n_elmt = n_elmt;
   ibm.x_bp = (PetscReal *)x; ibm.y_bp = (PetscReal *)y; ibm.z_bp = (PetscReal *)z;
-  std::vector<PetscInt> v1(n1, n1 + n_elmt), v2(n2, n2 + n_elmt), v3(n3, n3 + n_elmt);
+  // owned copies: the IB-node interpolation reads the surface at every step
+  ibm.x_bp = (PetscReal *)malloc(sizeof(PetscReal) * n_v);
+  ibm.y_bp = (PetscReal *)malloc(sizeof(PetscReal) * n_v);
+  ibm.z_bp = (PetscReal *)malloc(sizeof(PetscReal) * n_v);
+  memcpy(ibm.x_bp, x, sizeof(double) * n_v);
+  memcpy(ibm.y_bp, y, sizeof(double) * n_v);
+  memcpy(ibm.z_bp, z, sizeof(double) * n_v);
+  ibm.nv1 = (PetscInt *)malloc(sizeof(PetscInt) * n_elmt);
+  ibm.nv2 = (PetscInt *)malloc(sizeof(PetscInt) * n_elmt);
+  ibm.nv3 = (PetscInt *)malloc(sizeof(PetscInt) * n_elmt);
+  for (int e = 0; e < n_elmt; e++) { ibm.nv1[e] = n1[e]; ibm.nv2[e] = n2[e]; ibm.nv3[e] = n3[e]; }
   std::vector<PetscReal> fx(n_elmt), fy(n_elmt), fz(n_elmt);
-  ibm.nv1 = v1.data(); ibm.nv2 = v2.data(); ibm.nv3 = v3.data();
   for (int e = 0; e < n_elmt; e++) {
     const double dx12 = x[n2[e]] - x[n1[e]], dy12 = y[n2[e]] - y[n1[e]], dz12 = z[n2[e]] - z[n1[e]];
     const double dx13 = x[n3[e]] - x[n1[e]], dy13 = y[n3[e]] - y[n1[e]], dz13 = z[n3[e]] - z[n1[e]];
@@ -244,7 +281,23 @@ int ref_ibm_classify(int ibi, int n_v, const double *x, const double *y, const d
     const double dr = sqrt(nx * nx + ny * ny + nz * nz);
     fx[e] = nx / dr; fy[e] = ny / dr; fz[e] = nz / dr;
   }
-  ibm.nf_x = fx.data(); ibm.nf_y = fy.data(); ibm.nf_z = fz.data();
+  ibm.nf_x = (PetscReal *)malloc(sizeof(PetscReal) * n_elmt);
+  ibm.nf_y = (PetscReal *)malloc(sizeof(PetscReal) * n_elmt);
+  ibm.nf_z = (PetscReal *)malloc(sizeof(PetscReal) * n_elmt);
+  memcpy(ibm.nf_x, fx.data(), sizeof(double) * n_elmt);
+  memcpy(ibm.nf_y, fy.data(), sizeof(double) * n_elmt);
+  memcpy(ibm.nf_z, fz.data(), sizeof(double) * n_elmt);
+  // fixed bodies: zero surface velocity; per-triangle statistics the interpolation fills
+  ibm.u = (Cmpnts *)calloc(n_v, sizeof(Cmpnts));
+  ibm.uold = (Cmpnts *)calloc(n_v, sizeof(Cmpnts));
+  ibm.count = (PetscInt *)calloc(n_elmt, sizeof(PetscInt));
+  ibm.shear = (PetscReal *)calloc(n_elmt, sizeof(PetscReal));
+  ibm.mean_shear = (PetscReal *)calloc(n_elmt, sizeof(PetscReal));
+  ibm.reynolds_stress1 = (PetscReal *)calloc(n_elmt, sizeof(PetscReal));
+  ibm.reynolds_stress2 = (PetscReal *)calloc(n_elmt, sizeof(PetscReal));
+  ibm.reynolds_stress3 = (PetscReal *)calloc(n_elmt, sizeof(PetscReal));
+  ibm.pressure = (PetscReal *)calloc(n_elmt, sizeof(PetscReal));
+  ibm_ptr = g_ibm;
   const int ncx = 40, ncy = 40, ncz = 40;
   double xmin = 1.e23, xmax = -1.e23, ymin = 1.e23, ymax = -1.e23, zmin = 1.e23, zmax = -1.e23;
   for (int q = 0; q < n_v; q++) {
@@ -303,6 +356,47 @@ int ref_ibm_classify(int ibi, int n_v, const double *x, const double *y, const d
             for (int ii = im; ii <= ip; ii++)
               if ((int)(nv[at(ii, jj, kk)] + 0.5) == 4) nv[p] = PetscMax(2, nv[p]);
       }
+  if (build_list) {
+    // the IB-node list of ibm.c:347-505 with the reference's own geometry (BoundingSphere,
+    // nearestcell1, InterceptionPoint); the two fallbacks for a failed interception are
+    // those of ibm.c:400-500
+    static UserCtx *listed = 0;
+    if (listed != g_user) {
+      PetscMalloc(4 * sizeof(IBMList), &g_user->ibmlist);
+      for (int b = 0; b < 4; b++) InitIBMList(&g_user->ibmlist[b]);
+      listed = g_user;
+    }
+    if (g_user->ibmlist[ibi].head) DestroyIBMList(&g_user->ibmlist[ibi]);
+    InitIBMList(&g_user->ibmlist[ibi]);
+    BoundingSphere(&ibm);
+    for (int k = 1; k < mz - 1; k++)
+      for (int j = 1; j < my - 1; j++)
+        for (int i = 1; i < mx - 1; i++) {
+          if ((int)(nv[at(i, j, k)] + 0.5) != 2) continue;
+          IBMInfo info;
+          memset(&info, 0, sizeof(info));
+          info.ni = i; info.nj = j; info.nk = k;
+          const Cmpnts c = cent[at(i, j, k)];
+          call_nearestcell1(c, &ibm, &info);
+          InterceptionPoint(c, i, j, k, &info, g_user);
+          if (info.imode < 0) {
+            int dk = 0, dj = 0;
+            if (i == 1 || i == mx - 2 || j == 1 || j == my - 2) dk = ibm.nf_z[info.cell] > 0 ? 1 : -1;
+            else if (k == 1 || k == mz - 2) dj = 1;
+            if (dk || dj) {
+              const Cmpnts q = cent[at(i, j + dj, k + dk)];
+              info.d_i = sqrt((c.x - q.x) * (c.x - q.x) + (c.y - q.y) * (c.y - q.y) + (c.z - q.z) * (c.z - q.z));
+              info.cr1 = 1.; info.cr2 = 0.; info.cr3 = 0.;
+              info.i1 = info.i2 = info.i3 = i;
+              info.j1 = info.j2 = info.j3 = j + dj;
+              info.k1 = info.k2 = info.k3 = k + dk;
+            }
+          }
+          AddIBMNode(&g_user->ibmlist[ibi], info);
+        }
+    free(ibm.qvec);
+    free(ibm.radvec);
+  }
   for (int k = 1; k < mz - 1; k++)
     for (int j = 1; j < my - 1; j++)
       for (int i = 1; i < mx - 1; i++) {
@@ -312,8 +406,31 @@ int ref_ibm_classify(int ibi, int n_v, const double *x, const double *y, const d
       }
   VecCopy(lnv, g_user->Nvert);
   for (auto &l : bins) destroy(&l);
-  free(&ibm);
   return 0;
+}
+
+// The IB-node list of body ibi as arrays (node i j k, cell, imode, stencil i1 j1 k1 i2 ...
+// k3, weights cr1..3, cs1..3, d_s, d_i); returns the number of nodes (list order).
+int ref_ibm_list(int ibi, int *ints, double *dbls, int cap) {
+  int n = 0;
+  for (IBMListNode *c = g_user->ibmlist[ibi].head; c; c = c->next, n++) {
+    if (n >= cap) continue;
+    const IBMInfo &f = c->ibm_intp;
+    int *q = ints + 14 * n;
+    q[0] = f.ni; q[1] = f.nj; q[2] = f.nk; q[3] = f.cell; q[4] = f.imode;
+    q[5] = f.i1; q[6] = f.j1; q[7] = f.k1; q[8] = f.i2; q[9] = f.j2; q[10] = f.k2;
+    q[11] = f.i3; q[12] = f.j3; q[13] = f.k3;
+    double *d = dbls + 8 * n;
+    d[0] = f.cr1; d[1] = f.cr2; d[2] = f.cr3; d[3] = f.cs1; d[4] = f.cs2; d[5] = f.cs3; d[6] = f.d_s; d[7] = f.d_i;
+  }
+  return n;
+}
+
+// ibm_interpolation_advanced (ibm.c:3294) on the current fields.
+int ref_ibm_interpolation(int nbodies) {
+  extern PetscInt NumberOfBodies;
+  NumberOfBodies = nbodies;
+  return ibm_interpolation_advanced(g_user);
 }
 
 // PoissonLHSNew (poisson.c:971); the matrix stays recorded in user->A.

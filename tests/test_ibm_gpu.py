@@ -70,3 +70,76 @@ def test_ibm_search_two_bodies():
     np.testing.assert_array_equal(got, want)
     assert (got == 3).sum() > 0
     ctx.close()
+
+
+def _immersed_pair(size=(24, 20, 28), level=3, radius=0.4, seed=0):
+    """The wavy channel with an icosphere body on both sides: the reference classified and
+    listed it with its own nearestcell1/InterceptionPoint, the B200 library with its own."""
+    from helpers import build_pair
+    nx, ny, nz = size
+    case = cases.channel(nx, ny, nz, wavy=0.1)
+    case.immersed = 1
+    body = cases.icosphere((np.pi / 2, 1.0, np.pi), radius, level=level)
+    R, ctx = build_pair(case, seed=seed)
+    R.ibm_classify(*body, build_list=True)
+    ctx.ibm_search(*body)
+    return case, R, ctx
+
+
+def _by_cell(ints, dbls):
+    order = np.lexsort((ints[:, 0], ints[:, 1], ints[:, 2]))
+    return ints[order], dbls[order]
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("size,level,radius", [((24, 20, 28), 3, 0.4), ((48, 40, 56), 4, 0.35)])
+def test_ibm_list_matches_reference(size, level, radius):
+    """The IB-node list node by node: nearest triangle, interception mode and stencil cells
+    bit for bit; the weights and distances to 1e-12 relative."""
+    case, R, ctx = _immersed_pair(size, level, radius)
+    wi, wd = _by_cell(*R.ibm_list())
+    gi, gd = _by_cell(*ctx.ibm_list())
+    R.close()
+    assert len(wi) > 50 and len(gi) == len(wi)
+    np.testing.assert_array_equal(gi[:, :3], wi[:, :3])
+    np.testing.assert_array_equal(gi, wi)
+    np.testing.assert_allclose(gd, wd, rtol=1e-12, atol=1e-14)
+    assert (gi[:, 4] >= 0).all() and ctx.get_scalar(vfs.S_IB_UNRESOLVED) == 0
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_ibm_interpolation_matches_reference():
+    """ibm_interpolation_advanced (ibm.c:3294) on the seeded state: IB-node Ucat and P,
+    the face fluxes around the nodes and the Cartesian velocity after Contra2Cart."""
+    from helpers import assert_close
+    case, R, ctx = _immersed_pair()
+    u0 = ctx.get_field(vfs.UCAT)
+    R.call("ref_ibm_interpolation", 1)
+    ctx.ibm_interpolation()
+    nv = ctx.get_field(vfs.NVERT)
+    assert ((nv == 1) & (np.abs(ctx.get_field(vfs.UCAT) - u0).max(axis=-1) > 0)).sum() > 0
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-13, atol_frac=1e-15, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("Ucont"), rtol=1e-13, atol_frac=1e-15, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-13, atol_frac=1e-15, what="Ucat")
+    R.close()
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_volume_flux_ibm_matches_reference():
+    """VolumeFlux(user, &flux, &area, 0) (poisson.c:3570) after the interpolation: the
+    net flux into the IB nodes spread over the fluid/IB faces."""
+    from helpers import assert_close
+    case, R, ctx = _immersed_pair()
+    R.call("ref_ibm_interpolation", 1)
+    ctx.ibm_interpolation()
+    flux, area = R.volume_flux_ibm()
+    ctx.volume_flux()
+    assert area > 0 and abs(flux) > 1e-10
+    assert_close(ctx.get_field(vfs.UCONT), R.get("Ucont"), rtol=1e-13, atol_frac=1e-15, what="Ucont")
+    R.close()
+    ctx.close()

@@ -87,3 +87,29 @@ def test_les_and_ibm_sequences():
         nv = R.ibm_classify(*cases.icosphere((np.pi / 2, 1.0, np.pi), 0.4, level=level))
         assert (nv == 3).sum() > 0
         R.close()
+
+
+def test_immersed_sequences():
+    """The IB-node list, interpolation, immersed VolumeFlux and a whole immersed step, as
+    test_ibm_gpu.py and test_step_gpu.py run them."""
+    import test_step_gpu as S
+    for size, level, radius in (((24, 20, 28), 3, 0.4), ((48, 40, 56), 4, 0.35)):
+        case = cases.channel(*size, wavy=0.1)
+        case.immersed = 1
+        R = _ref_state(case)
+        R.ibm_classify(*cases.icosphere((np.pi / 2, 1.0, np.pi), radius, level=level), build_list=True)
+        ints, dbls = R.ibm_list()
+        assert len(ints) > 50 and (ints[:, 4] >= 0).all()
+        R.call("ref_ibm_interpolation", 1)
+        flux, area = R.volume_flux_ibm()
+        assert area > 0 and np.isfinite(flux)
+        R.close()
+    case = helpers.small_channel(16, 14, 20, wavy=0.1)
+    case.immersed = 1
+    case.inlet_flux = 5.0
+    R = _ref_state(case)
+    R.ibm_classify(*cases.icosphere((np.pi / 2, 1.0, np.pi), 0.45, level=3), build_list=True)
+    ref.set_global("inlet_flux", 5.0)
+    S.reference_immersed_step(R)
+    assert np.isfinite(R.get("P")).all()
+    R.close()

@@ -13,14 +13,14 @@ from helpers import assert_close, build_pair, small_channel, small_cylinders
 pytestmark = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
 
 
-def reference_step(R):
-    R.call("ref_ib_bc")                               # solvers.c:609 (ti == tistart)
-    R.set("Ucont", R.get("lUcont"))                   # DALocalToGlobal, solvers.c:610
-    R.call("ref_calc_k_flux")                         # solvers.c:644
-    R.call("ref_pressure_gradient")                   # solvers.c:786
-    R.call("ref_runge_kutta")                         # solvers.c:1294
+def reference_projection(R, immersed=False):
+    """Poisson set-up, a dense solve of the reference's own system, pressure update and
+    projection (poisson_hypre.c:527-610, solvers.c:1341-1342)."""
     R.call("ref_poisson_lhs")                         # poisson_hypre.c:527
-    R.volume_flux()                                   # poisson_hypre.c:566
+    if immersed:
+        R.volume_flux_ibm()                           # poisson_hypre.c:564
+    else:
+        R.volume_flux()                               # poisson_hypre.c:566
     b = R.poisson_rhs_hypre()                         # poisson_hypre.c:568
     rp, col, val = R.poisson_csr()
     n = len(rp) - 1
@@ -33,6 +33,15 @@ def reference_step(R):
     R.call("ref_convert_phi2_phi")                    # poisson_hypre.c:610
     R.call("ref_update_pressure")                     # solvers.c:1341
     R.call("ref_projection")                          # solvers.c:1342
+
+
+def reference_step(R):
+    R.call("ref_ib_bc")                               # solvers.c:609 (ti == tistart)
+    R.set("Ucont", R.get("lUcont"))                   # DALocalToGlobal, solvers.c:610
+    R.call("ref_calc_k_flux")                         # solvers.c:644
+    R.call("ref_pressure_gradient")                   # solvers.c:786
+    R.call("ref_runge_kutta")                         # solvers.c:1294
+    reference_projection(R)
     R.call("ref_ib_bc")                               # solvers.c:1381
     R.set("Ucont", R.get("lUcont"))
     R.call("ref_contra2cart")                         # solvers.c:1385
@@ -113,20 +122,7 @@ def reference_les_step(R, ti):
     ref.set_global("ti", 0)
     R.call("ref_pressure_gradient")
     R.call("ref_runge_kutta")
-    R.call("ref_poisson_lhs")
-    R.volume_flux()
-    b = R.poisson_rhs_hypre()
-    rp, col, val = R.poisson_csr()
-    n = len(rp) - 1
-    A = np.zeros((n, n))
-    for r in range(n):
-        A[r, col[rp[r]:rp[r + 1]]] = val[rp[r]:rp[r + 1]]
-    x = np.linalg.lstsq(A, b, rcond=None)[0]
-    x = R.remove_nullspace(x)
-    R.set("Phi2", x)
-    R.call("ref_convert_phi2_phi")
-    R.call("ref_update_pressure")
-    R.call("ref_projection")
+    reference_projection(R)
     R.call("ref_ib_bc")
     R.set("Ucont", R.get("lUcont"))
     R.call("ref_contra2cart")
@@ -155,4 +151,47 @@ def test_one_les_step_matches_reference(name):
     assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
     assert st.max_div < 1e-8
     assert ctx.get_scalar(vfs.S_TI) == 3
+    R.close()
+
+
+def reference_immersed_step(R):
+    """The first step with an immersed body (immersed = 1): the IB-node interpolation
+    before IB_BC (solvers.c:603-610), inside RungeKutta (rhs.c:1610-1614) and after the
+    projection (solvers.c:1366-1370), the immersed VolumeFlux in the Poisson set-up."""
+    R.call("ref_ibm_interpolation", 1)                # solvers.c:607
+    R.call("ref_ib_bc")
+    R.set("Ucont", R.get("lUcont"))
+    R.call("ref_calc_k_flux")
+    R.call("ref_pressure_gradient")
+    R.call("ref_runge_kutta")
+    reference_projection(R, immersed=True)
+    R.call("ref_ibm_interpolation", 1)                # solvers.c:1368
+    R.call("ref_ib_bc")                               # solvers.c:1382
+    R.set("Ucont", R.get("lUcont"))
+    R.call("ref_contra2cart")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_one_immersed_step_matches_reference(precision):
+    """A step of the wavy channel with an icosphere body, classified and listed on each
+    side by its own search (the lists agree node for node, test_ibm_gpu.py)."""
+    from vfs_b200 import cases
+    case = small_channel(16, 14, 20, wavy=0.1)
+    case.immersed = 1
+    case.inlet_flux = 5.0
+    body = cases.icosphere((np.pi / 2, 1.0, np.pi), 0.45, level=3)
+    R, ctx = build_pair(case)
+    R.ibm_classify(*body, build_list=True)
+    ctx.ibm_search(*body)
+    assert ctx.ibm_list()[0].shape[0] == R.ibm_list()[0].shape[0] > 0
+    ref.set_global("inlet_flux", case.inlet_flux)
+    ctx.set_scalar(vfs.S_INLET_FLUX, case.inlet_flux)
+    reference_immersed_step(R)
+    st = ctx.step(precision=precision, rtol=1e-13)
+    assert st.poisson.converged == 1
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-8, atol_frac=1e-9, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-9, atol_frac=1e-10, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
+    assert st.max_div < 1e-8
     R.close()

@@ -255,6 +255,8 @@ int vfs_destroy(vfs_ctx *ctx) {
   if (c->stage) cudaFree(c->stage);
   if (c->inflow_plane) cudaFree(c->inflow_plane);
   if (c->inlet_nodes) cudaFree(c->inlet_nodes);
+  if (c->ibn) cudaFree(c->ibn);
+  if (c->ibbuf) cudaFree(c->ibbuf);
   Poisson &P = c->ps;
   cudaFree(P.coef); cudaFree(P.fluid);
   cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t); cudaFree(P.hdev);
@@ -361,6 +363,7 @@ int vfs_get_scalar(vfs_ctx *ctx, int which, double *value) {
   Ctx *c = (Ctx *)ctx;
   if (!c || !value || which < 0 || which >= VFS_NSCALARS) return set_err(c, VFS_ERR_INVALID, "vfs_get_scalar: bad argument");
   if (which == VFS_S_TI) c->scal[VFS_S_TI] = c->ti;
+  if (which == VFS_S_IB_UNRESOLVED) c->scal[which] = c->nib_unresolved;
   *value = c->scal[which];
   return VFS_OK;
 }
@@ -440,6 +443,27 @@ int vfs_set_inflow_plane(vfs_ctx *ctx, const double *plane) {
 }
 int vfs_volume_flux(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return volume_flux(c); }
 int vfs_ib_bc(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return ib_bc(c); }
+int vfs_ibm_interpolation(vfs_ctx *ctx) { Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c); return ibm_interpolation(c); }
+int vfs_ibm_list(vfs_ctx *ctx, int *ints, double *dbls, int cap) {
+  Ctx *c = (Ctx *)ctx;
+  if (!c) return -VFS_ERR_INVALID;
+  cudaSetDevice(c->device);
+  if (ints && dbls && c->nib > 0) {
+    std::vector<IbNode> h(c->nib);
+    if (cudaMemcpy(h.data(), c->ibn, sizeof(IbNode) * c->nib, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return -set_err(c, VFS_ERR_CUDA, "vfs_ibm_list: copy failed");
+    for (int q = 0; q < c->nib && q < cap; q++) {
+      const IbNode &n = h[q];
+      int *o = ints + 14 * (size_t)q;
+      o[0] = n.i; o[1] = n.j; o[2] = n.k; o[3] = n.cell; o[4] = n.imode;
+      for (int v = 0; v < 9; v++) o[5 + v] = n.st[v];
+      double *d = dbls + 8 * (size_t)q;
+      d[0] = n.cr[0]; d[1] = n.cr[1]; d[2] = n.cr[2]; d[3] = n.cs[0]; d[4] = n.cs[1]; d[5] = n.cs[2];
+      d[6] = n.ds; d[7] = n.di;
+    }
+  }
+  return c->nib;
+}
 
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
   Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
@@ -452,6 +476,7 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
     // IB_BC (solvers.c:603-611)
     if ((rc = calc_inlet_area(c))) return rc;
     if ((rc = poisson_lhs(c))) return rc;
+    if (c->g.immersed && (rc = ibm_interpolation(c))) return rc;
     if ((rc = ib_bc(c))) return rc;
     c->first_step = false;
   } else if (!c->ps.built && (rc = poisson_lhs(c))) {
@@ -473,6 +498,7 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
   const int solve_rc = rc;
   if ((rc = update_pressure(c))) return rc;
   if ((rc = projection(c))) return rc;
+  if (c->g.immersed && (rc = ibm_interpolation(c))) return rc;  // solvers.c:1366-1370
   if ((rc = divergence(c, &s.max_div))) return rc;
   if ((rc = ib_bc(c))) return rc;
   if ((rc = contra2cart(c))) return rc;

@@ -17,6 +17,7 @@
 // The bin column of a cell holds every triangle whose bin range covers it; a triangle is
 // tested once per ray, which is what the reference's Element_Searched bookkeeping does,
 // and the hit count and the coincidence test do not depend on the order of the tests.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -31,6 +32,7 @@ constexpr int kIbmAttempts = 256;  // ray directions tried before a cell is repo
 constexpr int kIbmMaxHits = 64;    // crossings recorded per ray
 
 struct IbmSurface {
+  int nelmt;
   const double *x, *y, *z;         // vertices
   const int *n1, *n2, *n3;         // triangle vertex indices
   const double *nx, *ny, *nz;      // unit normals
@@ -160,6 +162,278 @@ __global__ void k_ibm_remap(Grid g, const uint8_t *__restrict__ in, uint8_t *nv,
   nvd[p] = (double)v;
 }
 
+// ------------------------------------------------------------------ IB-node list
+// The list ibm_search_advanced builds for the cells it marks 2 (ibm.c:347-505): the nearest
+// surface point (nearestcell1, ibm.c:1366; BoundingSphere ibm.c:1276 prunes the search),
+// the interception of the surface normal through the node with the cell-centre triangles
+// of the six neighbouring faces (InterceptionPoint ibm.c:1759 with ICP ibm.c:1659), and the
+// two boundary fallbacks.  Geometry helpers of compgeom.c in their operation order.
+struct P2 { double x, y; };
+struct P3 { double x, y, z; };
+
+__device__ __forceinline__ double dist3(const P3 &a, const P3 &b) {
+  return sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z));
+}
+
+// ISSameSide2D (compgeom.c:55-106); its first pair of t1/t2 is recomputed unconditionally
+// in the reference, so only the second form is evaluated here.
+__device__ int same_side2d(P2 p, P2 p1, P2 p2, P2 p3) {
+  const double t1 = (p.x - p1.x) * (p2.y - p1.y) - (p.y - p1.y) * (p2.x - p1.x);
+  const double t2 = (p3.x - p1.x) * (p2.y - p1.y) - (p3.y - p1.y) * (p2.x - p1.x);
+  const double lt = sqrt((p1.x - p2.x) * (p1.x - p2.x) + (p1.y - p2.y) * (p1.y - p2.y));
+  if (fabs(t1 / lt) < 1.e-10) return 1;
+  if (t1 > 0) return t2 > 0 ? 1 : -1;
+  return t2 < 0 ? 1 : -1;
+}
+
+// ISInsideTriangle2D (compgeom.c:108-129)
+__device__ int inside_triangle2d(P2 p, P2 a, P2 b, P2 c) {
+  int ls = same_side2d(p, a, b, c);
+  if (ls < 0) return ls;
+  ls = same_side2d(p, b, c, a);
+  if (ls < 0) return ls;
+  return same_side2d(p, c, a, b);
+}
+
+// ISPointInTriangle (compgeom.c:131-158): the test in the plane the normal dominates.
+__device__ int point_in_triangle(P3 p, P3 p1, P3 p2, P3 p3, double nfx, double nfy, double nfz) {
+  P2 q, q1, q2, q3;
+  if (fabs(nfz) >= fabs(nfx) && fabs(nfz) >= fabs(nfy)) {
+    q = {p.x, p.y}; q1 = {p1.x, p1.y}; q2 = {p2.x, p2.y}; q3 = {p3.x, p3.y};
+  } else if (fabs(nfx) >= fabs(nfy) && fabs(nfx) >= fabs(nfz)) {
+    q = {p.z, p.y}; q1 = {p1.z, p1.y}; q2 = {p2.z, p2.y}; q3 = {p3.z, p3.y};
+  } else {
+    q = {p.x, p.z}; q1 = {p1.x, p1.z}; q2 = {p2.x, p2.z}; q3 = {p3.x, p3.z};
+  }
+  return inside_triangle2d(q, q1, q2, q3);
+}
+
+// Dis_P_Line (compgeom.c:160-186): nearest point of segment p1p2 to p, and its distance.
+__device__ void dist_point_segment(P3 p, P3 p1, P3 p2, P3 *po, double *d) {
+  const double dx21 = p2.x - p1.x, dy21 = p2.y - p1.y, dz21 = p2.z - p1.z;
+  const double dx31 = p.x - p1.x, dy31 = p.y - p1.y, dz31 = p.z - p1.z;
+  const double t = (dx31 * dx21 + dy31 * dy21 + dz31 * dz21) / (dx21 * dx21 + dy21 * dy21 + dz21 * dz21);
+  if (t < 0) {
+    *po = p1;
+    *d = sqrt(dx31 * dx31 + dy31 * dy31 + dz31 * dz31);
+  } else if (t > 1) {
+    *po = p2;
+    *d = sqrt((p.x - po->x) * (p.x - po->x) + (p.y - po->y) * (p.y - po->y) + (p.z - po->z) * (p.z - po->z));
+  } else {
+    po->x = p1.x + t * dx21; po->y = p1.y + t * dy21; po->z = p1.z + t * dz21;
+    *d = sqrt((p.x - po->x) * (p.x - po->x) + (p.y - po->y) * (p.y - po->y) + (p.z - po->z) * (p.z - po->z));
+  }
+}
+
+// triangle_intp / triangle_intp2 (compgeom.c:188-226): barycentric weights in 2-D.
+__device__ void bary2d(P2 p, P2 p1, P2 p2, P2 p3, double w[3]) {
+  const double x13 = p1.x - p3.x, y13 = p1.y - p3.y;
+  const double x23 = p2.x - p3.x, y23 = p2.y - p3.y;
+  const double xp3 = p.x - p3.x, yp3 = p.y - p3.y;
+  const double a = x13 * y23 - x23 * y13;
+  w[0] = (y23 * xp3 - x23 * yp3) / a;
+  w[1] = (-y13 * xp3 + x13 * yp3) / a;
+  w[2] = 1. - w[0] - w[1];
+}
+
+// Weights of point q in triangle (t1, t2, t3) projected on the plane the normal n
+// dominates, with the reference's coordinate choice (ibm.c:1481-1505, ibm.c:1717-1737).
+__device__ bool bary_by_normal(P3 q, P3 t1, P3 t2, P3 t3, double nx, double ny, double nz, double w[3]) {
+  if (fabs(nx) >= fabs(ny) && fabs(nx) >= fabs(nz)) {
+    bary2d({q.y, q.z}, {t1.y, t1.z}, {t2.y, t2.z}, {t3.y, t3.z}, w);
+  } else if (fabs(ny) >= fabs(nx) && fabs(ny) >= fabs(nz)) {
+    bary2d({q.x, q.z}, {t1.x, t1.z}, {t2.x, t2.z}, {t3.x, t3.z}, w);
+  } else if (fabs(nz) >= fabs(ny) && fabs(nz) >= fabs(nx)) {
+    bary2d({q.y, q.x}, {t1.y, t1.x}, {t2.y, t2.x}, {t3.y, t3.x}, w);
+  } else {
+    return false;
+  }
+  return true;
+}
+
+struct IbmGeom {
+  IbmSurface S;
+  const double *qx, *qy, *qz, *rad;  // bounding spheres (BoundingSphere)
+  CV3 cent;
+  const long long *cells;            // node cells (linear DA index), ascending
+  int n;
+};
+
+__device__ __forceinline__ P3 vtx(const IbmSurface &S, int v) { return {S.x[v], S.y[v], S.z[v]}; }
+
+// ICP (ibm.c:1659-1757): interception of the ray p + d n (d > 0) with the eight triangles
+// of the nine face cell centres pc; returns the triangle (0..7) or -100.
+__device__ int icp(P3 p, const P3 pc[9], double nfx, double nfy, double nfz, double cr[3], double *d_i) {
+  const int tri[3][8] = {{0, 1, 2, 4, 4, 4, 3, 3}, {1, 2, 4, 5, 7, 6, 4, 4}, {4, 4, 5, 8, 8, 7, 6, 0}};
+  for (int t = 0; t < 8; t++) {
+    const P3 p1 = pc[tri[0][t]], p2 = pc[tri[1][t]], p3 = pc[tri[2][t]];
+    const double dx1 = p.x - p1.x, dy1 = p.y - p1.y, dz1 = p.z - p1.z;
+    const double dx2 = p2.x - p1.x, dy2 = p2.y - p1.y, dz2 = p2.z - p1.z;
+    const double dx3 = p3.x - p1.x, dy3 = p3.y - p1.y, dz3 = p3.z - p1.z;
+    double d = (nfx * (dy2 * dz3 - dz2 * dy3) - nfy * (dx2 * dz3 - dz2 * dx3) + nfz * (dx2 * dy3 - dy2 * dx3));
+    if (!(fabs(d) > 1.e-10)) continue;
+    d = -(dx1 * (dy2 * dz3 - dz2 * dy3) - dy1 * (dx2 * dz3 - dz2 * dx3) + dz1 * (dx2 * dy3 - dy2 * dx3)) / d;
+    if (!(d > 0)) continue;
+    const P3 pint = {p.x + d * nfx, p.y + d * nfy, p.z + d * nfz};
+    const double rx1 = p2.x - p1.x, ry1 = p2.y - p1.y, rz1 = p2.z - p1.z;
+    const double rx2 = p3.x - p1.x, ry2 = p3.y - p1.y, rz2 = p3.z - p1.z;
+    const double nxt = ry1 * rz2 - rz1 * ry2, nyt = -rx1 * rz2 + rz1 * rx2, nzt = rx1 * ry2 - ry1 * rx2;
+    if (point_in_triangle(pint, p1, p2, p3, nxt, nyt, nzt) < 0) continue;
+    bary_by_normal(pint, p1, p2, p3, nxt, nyt, nzt, cr);
+    *d_i = sqrt((pint.x - p.x) * (pint.x - p.x) + (pint.y - p.y) * (pint.y - p.y) + (pint.z - p.z) * (pint.z - p.z));
+    return t;
+  }
+  return -100;
+}
+
+__global__ void k_ibm_nodes(Grid g, IbmGeom G, IbNode *out, int *err) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G.n) return;
+  const IbmSurface &S = G.S;
+  const long long pos = G.cells[q];
+  const int i = (int)(pos % g.mx);
+  const long long r = pos / g.mx;
+  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  IbNode N;
+  N.i = i; N.j = j; N.k = k;
+  const P3 p = {G.cent.x[pos], G.cent.y[pos], G.cent.z[pos]};
+  // nearestcell1 (ibm.c:1366-1512)
+  double dmin = 1.e20;
+  int cmin = -100;
+  P3 pmin = {0, 0, 0};
+  for (int e = 0; e < S.nelmt; e++) {
+    const P3 qc = {G.qx[e], G.qy[e], G.qz[e]};
+    if (!(dist3(p, qc) - G.rad[e] < dmin)) continue;
+    const int a = S.n1[e], b = S.n2[e], c = S.n3[e];
+    const double nfx = S.nx[e], nfy = S.ny[e], nfz = S.nz[e];
+    const P3 p1 = vtx(S, a), p2 = vtx(S, b), p3 = vtx(S, c);
+    double tf = ((p.x - S.x[a]) * nfx + (p.y - S.y[a]) * nfy + (p.z - S.z[a]) * nfz);
+    if (fabs(tf) < 1.e-10) tf = 1.e-10;
+    if (!(tf >= 0)) continue;
+    const P3 pj = {p.x - tf * nfx, p.y - tf * nfy, p.z - tf * nfz};
+    if (point_in_triangle(pj, p1, p2, p3, nfx, nfy, nfz) == 1) {
+      if (tf < dmin) { dmin = tf; pmin = pj; cmin = e; }
+    } else {
+      P3 po;
+      double d;
+      dist_point_segment(p, p1, p2, &po, &d);
+      if (d < dmin) { dmin = d; pmin = po; cmin = e; }
+      dist_point_segment(p, p2, p3, &po, &d);
+      if (d < dmin) { dmin = d; pmin = po; cmin = e; }
+      dist_point_segment(p, p3, p1, &po, &d);
+      if (d < dmin) { dmin = d; pmin = po; cmin = e; }
+    }
+  }
+  if (cmin < 0) {  // "Nearest Cell Searching Error!": flagged; the node stays a harmless self-stencil
+    atomicExch(err, 1);
+    N.cell = 0; N.imode = -2; N.ds = N.di = 0;
+    for (int v = 0; v < 3; v++) { N.st[3 * v] = i; N.st[3 * v + 1] = j; N.st[3 * v + 2] = k; N.cr[v] = N.cs[v] = 0; }
+    out[q] = N;
+    return;
+  }
+  N.cell = cmin;
+  N.ds = dmin;
+  N.cs[0] = N.cs[1] = N.cs[2] = 0;
+  bary_by_normal(pmin, vtx(S, S.n1[cmin]), vtx(S, S.n2[cmin]), vtx(S, S.n3[cmin]), S.nx[cmin], S.ny[cmin],
+                 S.nz[cmin], N.cs);
+  // InterceptionPoint (ibm.c:1759-2250): the faces i-1, i+1, j-1, j+1, k-1, k+1 in turn
+  double nfx = p.x - pmin.x, nfy = p.y - pmin.y, nfz = p.z - pmin.z;
+  const double dr = sqrt(nfx * nfx + nfy * nfy + nfz * nfz);
+  nfx /= dr; nfy /= dr; nfz /= dr;
+  const int pick[8][3] = {{0, 1, 4}, {1, 2, 4}, {2, 4, 5}, {4, 5, 8}, {4, 7, 8}, {4, 6, 7}, {3, 4, 6}, {3, 4, 0}};
+  N.imode = -100;
+  for (int f = 0; f < 6 && N.imode < 0; f++) {
+    int ip[9], jp[9], kp[9];
+    for (int n = 0; n < 9; n++) {
+      const int a = n % 3 - 1, b = n / 3 - 1;
+      if (f < 2) { ip[n] = i + (f == 0 ? -1 : 1); jp[n] = j + a; kp[n] = k + b; }
+      else if (f < 4) { ip[n] = i + a; jp[n] = j + (f == 2 ? -1 : 1); kp[n] = k + b; }
+      else { ip[n] = i + a; jp[n] = j + b; kp[n] = k + (f == 4 ? -1 : 1); }
+    }
+    P3 pc[9];
+    for (int n = 0; n < 9; n++) {
+      const long long c = lidx(g, ip[n], jp[n], kp[n]);
+      pc[n] = {G.cent.x[c], G.cent.y[c], G.cent.z[c]};
+    }
+    const int t = icp(p, pc, nfx, nfy, nfz, N.cr, &N.di);
+    if (t >= 0) {
+      N.imode = t;
+      for (int v = 0; v < 3; v++) {
+        N.st[3 * v] = ip[pick[t][v]]; N.st[3 * v + 1] = jp[pick[t][v]]; N.st[3 * v + 2] = kp[pick[t][v]];
+      }
+    }
+  }
+  if (N.imode < 0) {  // ibm.c:400-498
+    int dj = 0, dk = 0;
+    if (i == 1 || i == g.mx - 2 || j == 1 || j == g.my - 2) dk = S.nz[cmin] > 0 ? 1 : -1;
+    else if (k == 1 || k == g.mz - 2) dj = 1;
+    if (dj || dk) {
+      const long long c = lidx(g, i, j + dj, k + dk);
+      const P3 pt = {G.cent.x[c], G.cent.y[c], G.cent.z[c]};
+      N.di = sqrt((p.x - pt.x) * (p.x - pt.x) + (p.y - pt.y) * (p.y - pt.y) + (p.z - pt.z) * (p.z - pt.z));
+      N.cr[0] = 1.; N.cr[1] = 0.; N.cr[2] = 0.;
+      for (int v = 0; v < 3; v++) { N.st[3 * v] = i; N.st[3 * v + 1] = j + dj; N.st[3 * v + 2] = k + dk; }
+      N.imode = -1;
+    } else {
+      // "IBM Searching Fail!": the reference keeps undefined stencil data; this node
+      // interpolates nothing (its velocity becomes the surface velocity)
+      for (int v = 0; v < 3; v++) { N.st[3 * v] = i; N.st[3 * v + 1] = j; N.st[3 * v + 2] = k; }
+      N.cr[0] = N.cr[1] = N.cr[2] = 0;
+      N.di = 0;
+      N.imode = -2;
+    }
+  }
+  out[q] = N;
+}
+
+__global__ void k_ibm_collect(Grid g, const uint8_t *__restrict__ fl, long long *cells, int *count, int cap) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int i = (int)(p % g.mx);
+  const long long r = p / g.mx;
+  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2 || fl[p] != 2) return;
+  const int slot = atomicAdd(count, 1);
+  if (slot < cap) cells[slot] = p;
+}
+
+// BoundingSphere (ibm.c:1276-1364): a sphere around each triangle that bounds the
+// nearest-point search.
+static void bounding_spheres(int n_elmt, const double *x, const double *y, const double *z, const int *n1,
+                             const int *n2, const int *n3, std::vector<double> &qx, std::vector<double> &qy,
+                             std::vector<double> &qz, std::vector<double> &rad) {
+  struct H { double x, y, z; };
+  auto dist = [](const H &a, const H &b) {
+    return sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z));
+  };
+  qx.resize(n_elmt); qy.resize(n_elmt); qz.resize(n_elmt); rad.resize(n_elmt);
+  const H p0 = {0, 0, 0};
+  for (int e = 0; e < n_elmt; e++) {
+    const H p1 = {x[n1[e]], y[n1[e]], z[n1[e]]}, p2 = {x[n2[e]], y[n2[e]], z[n2[e]]}, p3 = {x[n3[e]], y[n3[e]], z[n3[e]]};
+    const double l12 = dist(p1, p2), l23 = dist(p2, p3), l31 = dist(p3, p1);
+    H pa, pb, pc;
+    if (l12 > l23) {
+      if (l12 > l31) { pa = p1; pb = p2; pc = p3; }
+      else { pa = p3; pb = p1; pc = p2; }
+    } else {
+      if (l31 < l23) { pa = p2; pb = p3; pc = p1; }
+      else { pa = p3; pb = p1; pc = p2; }
+    }
+    const H pf = {0.5 * (pa.x + pb.x), 0.5 * (pa.y + pb.y), 0.5 * (pa.z + pb.z)};
+    const H pu = {pa.x - pf.x, pa.y - pf.y, pa.z - pf.z}, pv = {pc.x - pf.x, pc.y - pf.y, pc.z - pf.z};
+    const H pt = {pu.y * pv.z - pu.z * pv.y, pu.z * pv.x - pu.x * pv.z, pu.x * pv.y - pu.y * pv.x};
+    const H pd = {pt.y * pu.z - pt.z * pu.y, pt.z * pu.x - pt.x * pu.z, pt.x * pu.y - pt.y * pu.x};
+    double gama = -(dist(pu, p0) * dist(pu, p0) - dist(pv, p0) * dist(pv, p0));
+    const H pw = {pv.x - pu.x, pv.y - pu.y, pv.z - pu.z};
+    double lamda = 2 * (pd.x * pw.x + pd.y * pw.y + pd.z * pw.z);
+    gama /= lamda;
+    lamda = (gama < 0) ? 0 : gama;
+    const H q = {pf.x + lamda * pd.x, pf.y + lamda * pd.y, pf.z + lamda * pd.z};
+    qx[e] = q.x; qy[e] = q.y; qz[e] = q.z;
+    rad[e] = dist(q, pa);
+  }
+}
+
 int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const double *z, int n_elmt,
                const int *n1, const int *n2, const int *n3) {
   const Grid &g = c->g;
@@ -227,7 +501,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
   for (int e = 0; e < n_elmt; e++) { nx[e] = nf[3 * (size_t)e]; ny[e] = nf[3 * (size_t)e + 1]; nz[e] = nf[3 * (size_t)e + 2]; }
   const size_t nt = col_tri.size() > 0 ? col_tri.size() : 1;
   const size_t bytes = sizeof(double) * (3 * (size_t)n_v + 3 * (size_t)n_elmt + kIbmAttempts + 1) +
-                       sizeof(int) * (3 * (size_t)n_elmt + col_start.size() + 2 * nt) + sizeof(int) + 256;
+                       sizeof(int) * (3 * (size_t)n_elmt + col_start.size() + 2 * nt) + 2 * sizeof(int) + 256;
   char *buf = nullptr;
   if (cudaMalloc(&buf, bytes) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: allocation failed");
   size_t off = 0;
@@ -238,6 +512,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
     return dst;
   };
   IbmSurface S;
+  S.nelmt = n_elmt;
   S.x = (const double *)put(x, sizeof(double) * n_v);
   S.y = (const double *)put(y, sizeof(double) * n_v);
   S.z = (const double *)put(z, sizeof(double) * n_v);
@@ -251,8 +526,8 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
   S.col_start = (const int *)put(col_start.data(), sizeof(int) * col_start.size());
   S.col_tri = (const int *)put(col_tri.data(), sizeof(int) * col_tri.size());
   S.col_kmax = (const int *)put(col_kmax.data(), sizeof(int) * col_kmax.size());
-  int *err = (int *)(buf + off);
-  cudaMemsetAsync(err, 0, sizeof(int), c->stream);
+  int *err = (int *)(buf + off);  // err[0]: search status, err[1]: node count
+  cudaMemsetAsync(err, 0, 2 * sizeof(int), c->stream);
   S.xmin = xmin; S.xmax = xmax; S.ymin = ymin; S.ymax = ymax; S.zmin = zmin; S.zmax = zmax;
   S.dcx = dcx; S.dcy = dcy; S.dcz = dcz;
   int rc;
@@ -260,6 +535,63 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
   if ((rc = check_launch(c, "k_ibm_cast"))) { cudaFree(buf); return rc; }
   k_ibm_near<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, c->bcflag);
   if ((rc = check_launch(c, "k_ibm_near"))) { cudaFree(buf); return rc; }
+  // the IB-node list of this body (ibm.c:347-505): cells marked 2, ascending
+  {
+    int *cnt = err + 1;
+    cudaMemsetAsync(cnt, 0, sizeof(int), c->stream);
+    const int cap = 1 << 22;
+    long long *cells = nullptr;
+    if (cudaMallocAsync((void **)&cells, sizeof(long long) * cap, c->stream) != cudaSuccess) {
+      cudaFree(buf);
+      return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: allocation failed");
+    }
+    k_ibm_collect<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->bcflag, cells, cnt, cap);
+    int hn = 0;
+    cudaMemcpyAsync(&hn, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    cudaStreamSynchronize(c->stream);
+    if (hn > cap) { cudaFreeAsync(cells, c->stream); cudaFree(buf); return set_err(c, VFS_ERR_INVALID, "vfs_ibm_search: too many IB nodes"); }
+    std::vector<long long> hc(hn);
+    if (hn) cudaMemcpy(hc.data(), cells, sizeof(long long) * hn, cudaMemcpyDeviceToHost);
+    std::sort(hc.begin(), hc.end());
+    if (hn) cudaMemcpy(cells, hc.data(), sizeof(long long) * hn, cudaMemcpyHostToDevice);
+    std::vector<double> qx, qy, qz, rad;
+    bounding_spheres(n_elmt, x, y, z, n1, n2, n3, qx, qy, qz, rad);
+    double *qd = nullptr;
+    IbNode *nodes = nullptr;
+    const int base = (ibi == 0) ? 0 : c->nib;
+    bool ok = cudaMalloc(&qd, sizeof(double) * 4 * (size_t)n_elmt) == cudaSuccess;
+    ok = ok && cudaMalloc(&nodes, sizeof(IbNode) * (size_t)(base + hn + 1)) == cudaSuccess;
+    if (!ok) { cudaFree(qd); cudaFree(nodes); cudaFreeAsync(cells, c->stream); cudaFree(buf); return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: allocation failed"); }
+    cudaMemcpyAsync(qd, qx.data(), sizeof(double) * n_elmt, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(qd + n_elmt, qy.data(), sizeof(double) * n_elmt, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(qd + 2 * (size_t)n_elmt, qz.data(), sizeof(double) * n_elmt, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(qd + 3 * (size_t)n_elmt, rad.data(), sizeof(double) * n_elmt, cudaMemcpyHostToDevice, c->stream);
+    if (base) cudaMemcpyAsync(nodes, c->ibn, sizeof(IbNode) * base, cudaMemcpyDeviceToDevice, c->stream);
+    IbmGeom G;
+    G.S = S;
+    G.qx = qd; G.qy = qd + n_elmt; G.qz = qd + 2 * (size_t)n_elmt; G.rad = qd + 3 * (size_t)n_elmt;
+    G.cent = cv(field3(c, VFS_CENT));
+    G.cells = cells;
+    G.n = hn;
+    if (hn) k_ibm_nodes<<<nblocks(hn, 64), 64, 0, c->stream>>>(g, G, nodes + base, err);
+    if ((rc = check_launch(c, "k_ibm_nodes"))) { cudaFree(qd); cudaFree(nodes); cudaFree(buf); return rc; }
+    cudaFreeAsync(cells, c->stream);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(qd);
+    if (c->ibn) cudaFree(c->ibn);
+    if (c->ibbuf) cudaFree(c->ibbuf);
+    c->ibn = nodes;
+    c->nib = base + hn;
+    c->ibbuf = nullptr;
+    if (c->nib && cudaMalloc(&c->ibbuf, sizeof(double) * 4 * (size_t)c->nib) != cudaSuccess) {
+      cudaFree(buf);
+      return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: allocation failed");
+    }
+    std::vector<IbNode> hnodes(hn);
+    if (hn) cudaMemcpy(hnodes.data(), nodes + base, sizeof(IbNode) * hn, cudaMemcpyDeviceToHost);
+    if (ibi == 0) c->nib_unresolved = 0;
+    for (const IbNode &nd : hnodes) c->nib_unresolved += nd.imode == -2;
+  }
   k_ibm_remap<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->bcflag, c->nv, c->f[VFS_NVERT][0]);
   if ((rc = check_launch(c, "k_ibm_remap"))) { cudaFree(buf); return rc; }
   cudaMemsetAsync(c->bcflag, 0, (size_t)g.N, c->stream);  // Contra2Cart's flag buffer, clear again
@@ -270,11 +602,176 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
     return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: kernel failed");
   }
   cudaFree(buf);
+  if (herr == 1) return set_err(c, VFS_ERR_INVALID, "vfs_ibm_search: no nearest surface point for an IB node");
   if (herr == -1) return set_err(c, VFS_ERR_INVALID, "vfs_ibm_search: a cell's rays kept hitting coincident crossings");
   if (herr == -2) return set_err(c, VFS_ERR_INVALID, "vfs_ibm_search: a ray crossed too many triangles");
   c->nvert_set = true;
   c->nsolid = -1;
   c->ps.built = false;
+  return VFS_OK;
+}
+
+// ------------------------------------------------------------------ per-step IB work
+// ibm_interpolation_advanced (ibm.c:3294-3700) for fixed bodies with the no-slip
+// reconstruction (noslip, wallfunction.c:134-150): each IB node takes
+// Ub = (sb/sc)(Uc - Ua) + Ua from the velocity Uc interpolated at its three stencil cells
+// (sc = sb + d_i), zero when a stencil cell is not fluid or the node is solid, and the
+// pressure interpolated the same way.  All nodes read the fields as they were before the
+// pass (the reference reads the local copies lUcat and lP), then write.
+__global__ void k_ibm_gather(Grid g, const IbNode *__restrict__ nodes, int n, CV3 ucat, const double *__restrict__ p,
+                             const uint8_t *__restrict__ nv, double *out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const IbNode N = nodes[q];
+  const long long s1 = lidx(g, N.st[0], N.st[1], N.st[2]), s2 = lidx(g, N.st[3], N.st[4], N.st[5]);
+  const long long s3 = lidx(g, N.st[6], N.st[7], N.st[8]);
+  const double sb = N.ds, sc = sb + N.di;
+  const double sk1 = N.cr[0], sk2 = N.cr[1], sk3 = N.cr[2];
+  const double cs1 = N.cs[0], cs2 = N.cs[1], cs3 = N.cs[2];
+  // surface velocity of a fixed body (ibm->u = 0) through the surface weights
+  const double z = 0.0;
+  const double uax = z * cs1 + z * cs2 + z * cs3, uay = uax, uaz = uax;
+  const double ucx = (ucat.x[s1] * sk1 + ucat.x[s2] * sk2 + ucat.x[s3] * sk3);
+  const double ucy = (ucat.y[s1] * sk1 + ucat.y[s2] * sk2 + ucat.y[s3] * sk3);
+  const double ucz = (ucat.z[s1] * sk1 + ucat.z[s2] * sk2 + ucat.z[s3] * sk3);
+  const long long pos = lidx(g, N.i, N.j, N.k);
+  double ub[3];
+  if ((double)nv[s1] + (double)nv[s2] + (double)nv[s3] > 0.1 || nv[pos] > 2) {
+    ub[0] = ub[1] = ub[2] = 0;
+  } else {
+    const double u_c = ucx - uax, v_c = ucy - uay, w_c = ucz - uaz;
+    ub[0] = sb / sc * u_c; ub[1] = sb / sc * v_c; ub[2] = sb / sc * w_c;
+    ub[0] += uax; ub[1] += uay; ub[2] += uaz;
+  }
+  const double pn = (p[s1] * sk1 + p[s2] * sk2 + p[s3] * sk3);
+  out[4 * q] = ub[0]; out[4 * q + 1] = ub[1]; out[4 * q + 2] = ub[2]; out[4 * q + 3] = pn;
+}
+
+__global__ void k_ibm_scatter(Grid g, const IbNode *__restrict__ nodes, int n, const double *__restrict__ in, V3 ucat,
+                              double *p) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const IbNode N = nodes[q];
+  const long long pos = lidx(g, N.i, N.j, N.k);
+  ucat.x[pos] = in[4 * q]; ucat.y[pos] = in[4 * q + 1]; ucat.z[pos] = in[4 * q + 2];
+  p[pos] = in[4 * q + 3];
+}
+
+// Face fluxes next to IB nodes from the averaged Cartesian velocity (ibm.c:3605-3650 and
+// the immersed branch of IB_BC, momentum.c:2077-2108): every face of an IB-node cell, and
+// the lower faces of cells whose upper neighbour is an IB node.
+__global__ void k_ib_faces(Grid g, Metrics m, CV3 u, const uint8_t *__restrict__ nv, V3 uc) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int i = (int)(p % g.mx);
+  const long long r = p / g.mx;
+  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
+  const long long sy = g.mx, sz = (long long)g.mx * g.my;
+  const bool self = nv[p] == 1;
+  if (self || nv[p + 1] == 1) {
+    const double ucx = (u.x[p] + u.x[p + 1]) * 0.5, ucy = (u.y[p] + u.y[p + 1]) * 0.5, ucz = (u.z[p] + u.z[p + 1]) * 0.5;
+    uc.x[p] = (ucx * m.icsi.x[p] + ucy * m.icsi.y[p] + ucz * m.icsi.z[p]) * 1.0;
+  }
+  if (self || nv[p + sy] == 1) {
+    const double ucx = (u.x[p + sy] + u.x[p]) * 0.5, ucy = (u.y[p + sy] + u.y[p]) * 0.5, ucz = (u.z[p + sy] + u.z[p]) * 0.5;
+    uc.y[p] = (ucx * m.jeta.x[p] + ucy * m.jeta.y[p] + ucz * m.jeta.z[p]) * 1.0;
+  }
+  if (self || nv[p + sz] == 1) {
+    const double ucx = (u.x[p + sz] + u.x[p]) * 0.5, ucy = (u.y[p + sz] + u.y[p]) * 0.5, ucz = (u.z[p + sz] + u.z[p]) * 0.5;
+    uc.z[p] = (ucx * m.kzet.x[p] + ucy * m.kzet.y[p] + ucz * m.kzet.z[p]) * 1.0;
+  }
+}
+
+int ib_faces(Ctx *c) {
+  k_ib_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), cv(field3(c, VFS_UCAT)), c->nv,
+                                                         field3(c, VFS_UCONT));
+  return check_launch(c, "k_ib_faces");
+}
+
+int ibm_interpolation(Ctx *c) {
+  int rc;
+  if (c->nib > 0) {
+    const Grid &g = c->g;
+    k_ibm_gather<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, cv(field3(c, VFS_UCAT)),
+                                                             c->f[VFS_P][0], c->nv, c->ibbuf);
+    if ((rc = check_launch(c, "k_ibm_gather"))) return rc;
+    k_ibm_scatter<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, c->ibbuf, field3(c, VFS_UCAT),
+                                                              c->f[VFS_P][0]);
+    if ((rc = check_launch(c, "k_ibm_scatter"))) return rc;
+  }
+  if ((rc = ib_faces(c))) return rc;
+  return contra2cart(c);
+}
+
+// VolumeFlux(user, &ibm_Flux, &ibm_Area, 0) (poisson.c:3570-3730): the net flux through the
+// faces between fluid cells and IB nodes, faces carrying |Ucont| <= 1e-8 zeroed, is spread
+// over those faces in proportion to their area (the centre-metric norm the reference uses).
+__device__ __forceinline__ double face_area(CV3 m, long long p) {
+  return sqrt(m.x[p] * m.x[p] + m.y[p] * m.y[p] + m.z[p] * m.z[p]);
+}
+
+template <int PASS>
+__global__ void k_vflux_ibm(Grid g, Metrics m, const uint8_t *__restrict__ nv, V3 uc, double correction,
+                            double *parts) {
+  __shared__ double s1[256], s2[256];
+  double fsum = 0, asum = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long sy = g.mx, sz = (long long)g.mx * g.my;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
+    const int i = (int)(p % g.mx);
+    const long long r = p / g.mx;
+    const int j = (int)(r % g.my), k = (int)(r / g.my);
+    if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) continue;
+    const int v0 = nv[p];
+    double *comp[3] = {uc.x, uc.y, uc.z};
+    const CV3 *met[3] = {&m.csi, &m.eta, &m.zet};  // centre metrics (lCsi, lEta, lZet)
+    const long long off[3] = {1, sy, sz};
+    const bool inner[3] = {i < g.mx - 2, j < g.my - 2, k < g.mz - 2};
+    for (int d = 0; d < 3; d++) {
+      const int vn = nv[p + off[d]];
+      double sign = 0;
+      if (v0 == 0 && vn == 1 && inner[d]) sign = 1;       // fluid cell, IB node above
+      if (v0 == 1 && vn == 0 && inner[d]) sign = -1;      // IB node, fluid cell above
+      if (sign == 0) continue;
+      double &f = comp[d][p];
+      if (PASS == 0) {
+        if (fabs(f) > 1.e-8) {
+          fsum = sign > 0 ? fsum + f : fsum - f;
+          asum += face_area(*met[d], p);
+        } else {
+          f = 0.;
+        }
+      } else if (fabs(f) > 1.e-8) {
+        f = sign > 0 ? f - face_area(*met[d], p) * correction : f + face_area(*met[d], p) * correction;
+      }
+    }
+  }
+  if (PASS == 1) return;
+  s1[threadIdx.x] = fsum; s2[threadIdx.x] = asum;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { s1[threadIdx.x] += s1[threadIdx.x + w]; s2[threadIdx.x] += s2[threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { parts[blockIdx.x] = s1[0]; parts[gridDim.x + blockIdx.x] = s2[0]; }
+}
+
+int volume_flux_ibm(Ctx *c, double *flux, double *area) {
+  int rc;
+  const int nb = 148 * 2;
+  if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
+  Metrics m = metrics(c);
+  k_vflux_ibm<0><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), 0.0, c->red);
+  if ((rc = check_launch(c, "k_vflux_ibm"))) return rc;
+  double f = 0, a = 0;
+  if ((rc = reduce_sum(c, c->red, nb, &f))) return rc;
+  if ((rc = reduce_sum(c, c->red + nb, nb, &a))) return rc;
+  const double correction = (a > 1.e-15) ? f / a : 0;
+  k_vflux_ibm<1><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), correction, c->red);
+  if ((rc = check_launch(c, "k_vflux_ibm"))) return rc;
+  if (flux) *flux = f;
+  if (area) *area = a;
   return VFS_OK;
 }
 

@@ -109,6 +109,20 @@ struct Poisson {
   double *hdev = nullptr;   // Gram-Schmidt coefficients on the device (64 doubles)
 };
 
+// One immersed-boundary node of the IB-node list (IBMInfo, variables.h:95-172, as
+// ibm_search_advanced fills it, ibm.c:347-505): the node cell, the nearest surface
+// triangle and the barycentric weights of its projection, and the three fluid cells
+// whose velocities are interpolated across the surface normal.
+struct IbNode {
+  int i, j, k;        // node cell
+  int cell;           // nearest surface triangle (nearestcell1)
+  int imode;          // interception mode (0..7), -1 a boundary fallback, -2 unresolved
+  int st[9];          // stencil cells i1 j1 k1 i2 j2 k2 i3 j3 k3
+  double cr[3];       // stencil weights cr1..cr3
+  double cs[3];       // surface weights cs1..cs3
+  double ds, di;      // distance to the surface (d_s) and to the interception (d_i)
+};
+
 struct Ctx {
   vfs_config cfg;
   Grid g;
@@ -134,6 +148,10 @@ struct Ctx {
   double *red = nullptr;        // partial sums (device)
   double *red_host = nullptr;   // pinned host mirror
   int red_cap = 0;
+  IbNode *ibn = nullptr;        // IB-node list of every searched body (device)
+  int nib = 0;                  // its length
+  int nib_unresolved = 0;       // nodes whose interception search failed (reference: garbage)
+  double *ibbuf = nullptr;      // per-node gather buffer (4 doubles per node)
   double *inflow_plane = nullptr;  // inlet velocity plane, my*mx Cartesian triples (inletprofile 100)
   double *inlet_nodes = nullptr;   // grid nodes of the k = 1 node plane: x, y, z blocks of JM*IM
   double *stage = nullptr;      // host-transfer staging buffer (interleaved layout)
@@ -170,6 +188,11 @@ int form_bcs(Ctx *c, bool outflow_scale);
 int inflow_flux(Ctx *c);
 int calc_inlet_area(Ctx *c);
 int ib_bc(Ctx *c);
+
+// immersed boundary (vfs_ibm.cu)
+int ibm_interpolation(Ctx *c);
+int ib_faces(Ctx *c);
+int volume_flux_ibm(Ctx *c, double *flux, double *area);
 
 // dynamic Smagorinsky model (vfs_les.cu)
 int smagorinsky_constant(Ctx *c);

@@ -579,12 +579,16 @@ __global__ void k_mg_active(long long n, const double *__restrict__ op, uint8_t 
 
 // ------------------------------------------------------------------ bottom of the V-cycle
 // The coarse levels are too small to fill the GPU, and a launch per colour pass costs
-// more than the work.  From the first level of at most kBottomCells cells down, one
-// thread block runs the rest of the V-cycle (smoothing, restriction, coarsest sweeps,
+// more than the work.  From the first level of at most kBottomCells cells down (8192: on
+// the B200 a 32 x 24 x 32 level is faster as ordinary launches, a 16 x 12 x 16 one in a
+// single block), one thread block runs the rest of the V-cycle (smoothing, restriction, coarsest sweeps,
 // prolongation) with block barriers between the phases; the level data stay in L2.
 constexpr int kBottomMaxLevels = 12;
 constexpr int kBottomThreads = 512;
-constexpr long long kBottomCells = 32768;
+#ifndef VFS_BOTTOM_CELLS
+#define VFS_BOTTOM_CELLS 8192
+#endif
+constexpr long long kBottomCells = VFS_BOTTOM_CELLS;
 
 template <typename T>
 struct BLevel {

@@ -1294,7 +1294,10 @@ __global__ void k_periodic_normal(Grid g, V3 uc) {
 
 int ib_bc(Ctx *c) {
   int rc;
-  if (c->g.immersed) return set_err(c, VFS_ERR_INVALID, "IB_BC: immersed-boundary reconstruction is not on this path yet");
+  if (c->g.immersed) {  // momentum.c:2049-2108: periodic Ucat ghosts, then the IB-node faces
+    if ((rc = periodic_copy3(c, field3(c, VFS_UCAT)))) return rc;
+    if ((rc = ib_faces(c))) return rc;
+  }
   k_ib_bc_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
   if ((rc = check_launch(c, "k_ib_bc_faces"))) return rc;
   if (c->g.iper || c->g.jper || c->g.kper) {
@@ -1526,14 +1529,15 @@ int form_bcs(Ctx *c, bool outflow_scale) {
 }
 
 // ------------------------------------------------------------------ RungeKutta
-// rhs.c:1578-1700 (implicit=0): InflowFlux, FormBCS without outlet rescaling, then four
-// stages  Contra2Cart; Rhs = Formfunction_2 - dP; Ucont = pUcont + alfa*dt*st*Rhs;
+// rhs.c:1578-1700 (implicit=0): InflowFlux, FormBCS without outlet rescaling, the IB-node
+// interpolation when immersed, then four stages  Contra2Cart; Rhs = Formfunction_2 - dP; Ucont = pUcont + alfa*dt*st*Rhs;
 // Contra2Cart  and finally FormBCS with the outlet rescaling (outflow_scale = 1).
 int runge_kutta(Ctx *c) {
   int rc;
   const double alfa[4] = {0.25, 1 / 3., 0.5, 1.};
   if ((rc = inflow_flux(c))) return rc;
   if ((rc = form_bcs(c, false))) return rc;
+  if (c->g.immersed && (rc = ibm_interpolation(c))) return rc;  // rhs.c:1610-1614
   const size_t bytes = sizeof(double) * (size_t)c->g.N;
   for (int q = 0; q < 3; q++)
     cudaMemcpyAsync(c->pucont[q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);

@@ -660,7 +660,7 @@ __global__ void k_volume_flux_blocked(Grid g, const uint8_t *__restrict__ nv, V3
 }
 
 int volume_flux(Ctx *c) {
-  if (c->g.immersed) return set_err(c, VFS_ERR_INVALID, "VolumeFlux: IB-node flux balance is not on this path yet");
+  if (c->g.immersed) return volume_flux_ibm(c, nullptr, nullptr);  // poisson_hypre.c:564
   k_volume_flux_blocked<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->nv, field3(c, VFS_UCONT));
   return check_launch(c, "k_volume_flux_blocked");
 }

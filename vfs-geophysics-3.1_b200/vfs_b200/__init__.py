@@ -37,7 +37,8 @@ METRIC_FIELDS = {
 }
 
 # scalars
-S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST, S_TI, S_FLUX_IN, S_FLUX_OUT = range(10)
+(S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST, S_TI, S_FLUX_IN, S_FLUX_OUT,
+ S_IB_UNRESOLVED) = range(11)
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOT_CONVERGED, ERR_NO_DEVICE, ERR_STATE = range(6)
 
@@ -90,7 +91,7 @@ EXPORTS = [
     "vfs_divergence", "vfs_step", "vfs_calc_inlet_area", "vfs_form_bcs", "vfs_ib_bc",
     "vfs_form_metrics", "vfs_volume_flux", "vfs_get_stream", "vfs_run_kernel",
     "vfs_smagorinsky_constant", "vfs_eddy_viscosity", "vfs_inflow_flux", "vfs_set_inflow_plane",
-    "vfs_ibm_search",
+    "vfs_ibm_search", "vfs_ibm_list", "vfs_ibm_interpolation",
 ]
 
 _lib = None
@@ -124,12 +125,13 @@ def load_library(path=None):
     for n in ("vfs_contra2cart", "vfs_pressure_gradient", "vfs_runge_kutta", "vfs_poisson_lhs",
               "vfs_poisson_rhs", "vfs_update_pressure", "vfs_projection", "vfs_calc_inlet_area",
               "vfs_ib_bc", "vfs_volume_flux", "vfs_smagorinsky_constant",
-              "vfs_eddy_viscosity", "vfs_inflow_flux"):
+              "vfs_eddy_viscosity", "vfs_inflow_flux", "vfs_ibm_interpolation"):
         getattr(lib, n).argtypes = [vp]
     lib.vfs_formfunction2.argtypes = [vp, ctypes.c_double]
     lib.vfs_form_bcs.argtypes = [vp, ctypes.c_int]
     lib.vfs_set_inflow_plane.argtypes = [vp, vp]
     lib.vfs_ibm_search.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
+    lib.vfs_ibm_list.argtypes = [vp, vp, vp, ctypes.c_int]
     lib.vfs_calc_k_flux.argtypes = [vp, dp]
     lib.vfs_divergence.argtypes = [vp, dp]
     lib.vfs_poisson_solve.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats)]
@@ -247,6 +249,20 @@ class Context:
                                             cols[2].ctypes.data))
         return self.get_field(NVERT)
 
+    def ibm_list(self):
+        """The IB-node list: ints (n, 14) i j k cell imode i1 j1 k1 i2 j2 k2 i3 j3 k3 and
+        doubles (n, 8) cr1..3 cs1..3 d_s d_i."""
+        n = self.lib.vfs_ibm_list(self.h, None, None, 0)
+        if n < 0:
+            self._check(-n)
+        ints = np.zeros((n, 14), dtype=np.int32)
+        dbls = np.zeros((n, 8))
+        self.lib.vfs_ibm_list(self.h, ints.ctypes.data, dbls.ctypes.data, n)
+        return ints, dbls
+
+    def ibm_interpolation(self):      # ibm_interpolation_advanced, ibm.c:3294
+        self._check(self.lib.vfs_ibm_interpolation(self.h))
+
     # ---- operators (reference names in comments)
     def contra2cart(self):            # Contra2Cart, rhs.c:27
         self._check(self.lib.vfs_contra2cart(self.h))
@@ -279,7 +295,7 @@ class Context:
             raise ValueError("inflow plane: expected my*mx*3 values")
         self._check(self.lib.vfs_set_inflow_plane(self.h, a.ctypes.data))
 
-    def volume_flux(self):            # VolumeFlux, poisson.c:3306 (immersed = 0)
+    def volume_flux(self):            # VolumeFlux, poisson.c:3306 (immersed = 0) / 3570 (immersed = 1)
         self._check(self.lib.vfs_volume_flux(self.h))
 
     def ib_bc(self):                  # IB_BC, momentum.c:1982
