@@ -158,6 +158,7 @@ def reference_immersed_step(R):
     """The first step with an immersed body (immersed = 1): the IB-node interpolation
     before IB_BC (solvers.c:603-610), inside RungeKutta (rhs.c:1610-1614) and after the
     projection (solvers.c:1366-1370), the immersed VolumeFlux in the Poisson set-up."""
+    R.call("ref_calc_inlet_area")                     # main.c:3488, after the IB search
     R.call("ref_ibm_interpolation", 1)                # solvers.c:607
     R.call("ref_ib_bc")
     R.set("Ucont", R.get("lUcont"))
