@@ -257,6 +257,7 @@ int vfs_destroy(vfs_ctx *ctx) {
   if (c->inlet_nodes) cudaFree(c->inlet_nodes);
   if (c->ibn) cudaFree(c->ibn);
   if (c->ibbuf) cudaFree(c->ibbuf);
+  adjoint_free(c);
   Poisson &P = c->ps;
   cudaFree(P.coef); cudaFree(P.fluid);
   cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t); cudaFree(P.hdev);
@@ -467,10 +468,20 @@ int vfs_ibm_list(vfs_ctx *ctx, int *ints, double *dbls, int cap) {
 
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
   Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  return step_core(c, opts, st);
+}
+
+}  // extern "C"
+
+namespace vfs {
+// One time step (vfs_step); with c->tape set it also records the stage states the
+// tangent and adjoint steps need.
+int step_core(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
   int rc;
   vfs_step_stats s;
   memset(&s, 0, sizeof(s));
   cudaEventRecord(c->ev0, c->stream);
+  if (c->tape) c->tape->first_step = c->first_step;
   if (c->first_step) {
     // first time step: Calc_Inlet_Area (main.c:3488), PoissonLHSNew (poisson_hypre.c:527),
     // IB_BC (solvers.c:603-611)
@@ -517,5 +528,4 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
   if (st) *st = s;
   return solve_rc;
 }
-
-}  // extern "C"
+}  // namespace vfs

@@ -107,6 +107,7 @@ struct Poisson {
   double *Z = nullptr;      // restart * ldv
   double *w = nullptr, *r = nullptr, *t = nullptr;
   double *hdev = nullptr;   // Gram-Schmidt coefficients on the device (64 doubles)
+  bool transpose = false;   // apply A^T (the adjoint solve)
 };
 
 // One immersed-boundary node of the IB-node list (IBMInfo, variables.h:95-172, as
@@ -122,6 +123,16 @@ struct IbNode {
   double cs[3];       // surface weights cs1..cs3
   double ds, di;      // distance to the surface (d_s) and to the interception (d_i)
 };
+
+// Forward quantities of one time step that its tangent and adjoint are linearised about:
+// the Ucont and Ucat entering Formfunction_2 at each Runge-Kutta stage and the Ucont
+// entering the immersed VolumeFlux (whose |flux| > 1e-8 test selects the corrected faces).
+struct StepTape {
+  double *uc[4][3] = {}, *uk[4][3] = {};
+  double *vfi[3] = {};
+  bool first_step = false;
+};
+struct Adjoint;
 
 struct Ctx {
   vfs_config cfg;
@@ -163,6 +174,8 @@ struct Ctx {
   double max_cs = 0.5;           // upper clip of the Smagorinsky coefficient
   Poisson ps;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  StepTape *tape = nullptr;      // set while a step records its linearisation state
+  Adjoint *adj = nullptr;        // tangent/adjoint workspace (vfs_adjoint.cu)
 };
 
 V3 field3(Ctx *c, int f);
@@ -188,6 +201,23 @@ int form_bcs(Ctx *c, bool outflow_scale);
 int inflow_flux(Ctx *c);
 int calc_inlet_area(Ctx *c);
 int ib_bc(Ctx *c);
+int pressure_forcing_mode(const Ctx *c);
+int pressure_gradient_mode(Ctx *c, int mode, double kdiff);
+int step_core(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st);
+int form_bcs_tail(Ctx *c);
+int outlet_rescale(Ctx *c);
+
+// tangent / adjoint of one RK stage and of the periodic ghost copy (vfs_momentum.cu)
+int ff2_stage_tangent(Ctx *c, const double *const uc[3], const double *const uk[3], double a, V3 dU, V3 du, V3 ddp,
+                      V3 dpu, double *const tf[3][6]);
+int ff2_stage_adjoint(Ctx *c, const double *const uc[3], const double *const uk[3], double a, V3 lU, V3 lu, V3 ldp,
+                      V3 lpu, double *const lf[3][6], double *const lfp[3]);
+int periodic_copy_adj3(Ctx *c, V3 v);
+
+// tangent / adjoint support (vfs_adjoint.cu)
+int tape_stage(Ctx *c, int stage);
+int tape_vflux(Ctx *c);
+void adjoint_free(Ctx *c);
 
 // immersed boundary (vfs_ibm.cu)
 int ibm_interpolation(Ctx *c);
@@ -201,6 +231,8 @@ int eddy_viscosity(Ctx *c);
 // Poisson / correction path
 int poisson_lhs(Ctx *c);
 int poisson_rhs(Ctx *c);
+int poisson_rhs_local(Ctx *c);
+int poisson_set_transpose(Ctx *c, bool on);
 int volume_flux(Ctx *c);
 int poisson_solve(Ctx *c, const vfs_solve_opts *o, vfs_solve_stats *st);
 int poisson_apply_dev(Ctx *c, const double *x, double *y);

@@ -1156,20 +1156,29 @@ __global__ void k_pressure_gradient(Grid g, Metrics m, const uint8_t *__restrict
   dp.x[p] = ox; dp.y[p] = oy; dp.z[p] = oz;
 }
 
-int pressure_gradient(Ctx *c) {
+// k-periodic forcing (momentum.c:379-399): dpdz_set -> mean_pressure_gradient (mode 1),
+// else (inletprofile != 17) the flux-deficit term (mean_k_flux - inlet_flux)/dt/mean_k_area
+// (mode 2); only a k-periodic grid applies it.
+int pressure_forcing_mode(const Ctx *c) {
+  if (c->cfg.dpdz_set) return 1;
+  if (c->cfg.inletprofile != 17) return 2;
+  return 0;
+}
+
+// Pressure_Gradient with an explicit forcing mode and flux deficit kdiff.
+int pressure_gradient_mode(Ctx *c, int mode, double kdiff) {
   int rc;
   // P's periodic ghosts are refreshed first (momentum.c:241-273)
   if ((rc = periodic_copy1(c, c->f[VFS_P][0]))) return rc;
-  // k-periodic forcing (momentum.c:379-399): dpdz_set -> mean_pressure_gradient, else
-  // (inletprofile != 17) the flux-deficit term (mean_k_flux - inlet_flux)/dt/mean_k_area.
-  int mode = 0;
-  if (c->cfg.dpdz_set) mode = 1;
-  else if (c->cfg.inletprofile != 17) mode = 2;
-  const double kdiff = c->scal[VFS_S_MEAN_K_FLUX] - c->scal[VFS_S_INLET_FLUX];
   k_pressure_gradient<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(
       c->g, metrics(c), c->nv, c->f[VFS_P][0], kdiff, c->g.dt, c->scal[VFS_S_MEAN_K_AREA], mode,
       c->cfg.mean_pressure_gradient, field3(c, VFS_DP));
   return check_launch(c, "k_pressure_gradient");
+}
+
+int pressure_gradient(Ctx *c) {
+  return pressure_gradient_mode(c, pressure_forcing_mode(c),
+                                c->scal[VFS_S_MEAN_K_FLUX] - c->scal[VFS_S_INLET_FLUX]);
 }
 
 // ------------------------------------------------------------------ Calc_k_Flux
@@ -1503,10 +1512,10 @@ __global__ void k_zero_edges(Grid g, V3 u) {
   if (bi + bj + bk >= 2) { u.x[p] = 0; u.y[p] = 0; u.z[p] = 0; }
 }
 
-int form_bcs(Ctx *c, bool outflow_scale) {
+// The outlet flux rescaling of FormBCS (outflow_scale set, bctype[5] = 4).
+int outlet_rescale(Ctx *c) {
   int rc;
-  if ((rc = contra2cart(c))) return rc;
-  if (c->g.bc[5] == 4 && outflow_scale) {
+  {
     const Grid &g = c->g;
     const long long npl = (long long)(g.mx - 2) * (g.my - 2);
     const int nb = (int)nblocks(npl, 256);
@@ -1521,11 +1530,24 @@ int form_bcs(Ctx *c, bool outflow_scale) {
                                              c->scal[VFS_S_FLUX_IN] - flux_out, area_sum);
     if ((rc = check_launch(c, "k_outlet_scale"))) return rc;
   }
+  return VFS_OK;
+}
+
+// FormBCS after the outlet rescaling: wall fluxes, Contra2Cart, box edges.
+int form_bcs_tail(Ctx *c) {
+  int rc;
   k_wall_flux<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
   if ((rc = check_launch(c, "k_wall_flux"))) return rc;
   if ((rc = contra2cart(c))) return rc;
   k_zero_edges<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCAT));
   return check_launch(c, "k_zero_edges");
+}
+
+int form_bcs(Ctx *c, bool outflow_scale) {
+  int rc;
+  if ((rc = contra2cart(c))) return rc;
+  if (c->g.bc[5] == 4 && outflow_scale && (rc = outlet_rescale(c))) return rc;
+  return form_bcs_tail(c);
 }
 
 // ------------------------------------------------------------------ RungeKutta
@@ -1546,6 +1568,7 @@ int runge_kutta(Ctx *c) {
     // stage s > 0 sees exactly the Ucont the end of stage s-1 converted, and Contra2Cart
     // of the same Ucont reproduces the same Ucat, so only stage 0 converts first
     if (s == 0 && (rc = contra2cart(c))) return rc;
+    if (c->tape && (rc = tape_stage(c, s))) return rc;
     const double a = alfa[s] * c->g.dt * c->g.st;
     if ((rc = formfunction2(c, 1.0, true, a))) return rc;
     if ((rc = contra2cart(c))) return rc;

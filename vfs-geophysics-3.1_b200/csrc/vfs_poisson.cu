@@ -233,7 +233,32 @@ __global__ void k_apply(Grid g, const double *__restrict__ coef, const double *_
   y[p] = apply_row64<NS>(g, coef, x, p);
 }
 
+// y = A^T x: every stencil entry of row p scattered onto its neighbour (atomics).
+__global__ void k_apply_t(Grid g, int ns, const double *__restrict__ coef, const double *__restrict__ x, double *y) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const double xp = x[p];
+  if (xp == 0.0) return;
+  const int i = (int)(p % g.mx);
+  const long long q = p / g.mx;
+  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  for (int t = 0; t < ns; t++) {
+    const double c = coef[t * g.N + p];
+    if (c != 0.0) atomicAdd(y + nb_index(g, i, j, k, t), c * xp);
+  }
+}
+
+int poisson_set_transpose(Ctx *c, bool on) {
+  c->ps.transpose = on;
+  return VFS_OK;
+}
+
 int poisson_apply_dev(Ctx *c, const double *x, double *y) {
+  if (c->ps.transpose) {
+    cudaMemsetAsync(y, 0, sizeof(double) * c->g.N, c->stream);
+    k_apply_t<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.nslot, c->ps.coef, x, y);
+    return check_launch(c, "k_apply_t");
+  }
   if (c->ps.nslot == 7) k_apply<7><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
   else k_apply<NSLOT><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
   return check_launch(c, "k_apply");
@@ -477,8 +502,36 @@ static int update_scale(Ctx *c, const double *V, int nv, const double *hdev, con
   return check_launch(c, "k_update_scale");
 }
 
+// r = b - r and the partial sums of r.r.
+__global__ void k_sub_norm(long long n, const double *__restrict__ b, double *r, double *parts) {
+  __shared__ double sh[256];
+  double s = 0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const double v = b[p] - r[p];
+    r[p] = v;
+    s += v * v;
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
+}
+
 // r = b - A x; returns ||r||.
 static int residual(Ctx *c, const double *b, const double *x, double *r, double *rnorm) {
+  if (c->ps.transpose) {
+    int rc;
+    if ((rc = poisson_apply_dev(c, x, r))) return rc;
+    k_sub_norm<<<kKryBlocks, 256, 0, c->stream>>>(c->g.N, b, r, c->red);
+    if ((rc = check_launch(c, "k_sub_norm"))) return rc;
+    double rr;
+    if ((rc = finish_rows(c, 1, &rr))) return rc;
+    *rnorm = sqrt(rr);
+    return VFS_OK;
+  }
   if (c->ps.nslot == 7)
     k_residual<7><<<kKryBlocks, kKryThreads, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
   else
@@ -660,17 +713,28 @@ __global__ void k_volume_flux_blocked(Grid g, const uint8_t *__restrict__ nv, V3
 }
 
 int volume_flux(Ctx *c) {
-  if (c->g.immersed) return volume_flux_ibm(c, nullptr, nullptr);  // poisson_hypre.c:564
+  if (c->g.immersed) {  // poisson_hypre.c:564
+    int rc;
+    if (c->tape && (rc = tape_vflux(c))) return rc;
+    return volume_flux_ibm(c, nullptr, nullptr);
+  }
   k_volume_flux_blocked<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->nv, field3(c, VFS_UCONT));
   return check_launch(c, "k_volume_flux_blocked");
+}
+
+// The local part of the right-hand side: periodic Ucont ghosts, then b = div(Ucont)/dt*st.
+int poisson_rhs_local(Ctx *c) {
+  int rc;
+  if ((rc = periodic_copy3(c, field3(c, VFS_UCONT)))) return rc;
+  k_poisson_rhs<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->ps.fluid,
+                                                             c->f[VFS_B][0]);
+  return check_launch(c, "k_poisson_rhs");
 }
 
 int poisson_rhs(Ctx *c) {
   int rc;
   double *b = c->f[VFS_B][0];
-  if ((rc = periodic_copy3(c, field3(c, VFS_UCONT)))) return rc;
-  k_poisson_rhs<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->ps.fluid, b);
-  if ((rc = check_launch(c, "k_poisson_rhs"))) return rc;
+  if ((rc = poisson_rhs_local(c))) return rc;
   double sum = 0;
   if ((rc = sum_fluid(c, b, &sum))) return rc;
   k_shift_scaled<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->ps.fluid, c->f[VFS_AJ][0], sum,
