@@ -316,6 +316,60 @@ int vfs_get_stream(vfs_ctx *ctx, void **stream);
  * 0-2).  Kernels 7 and 8 add into RHS as vfs_formfunction2 does.  For timing only. */
 int vfs_run_kernel(vfs_ctx *ctx, int which, int reps);
 
+/* ------------------------------------------------------------------ adjoint
+ * Tangent-linear and discrete adjoint of a window of vfs_step calls (implicit = 0,
+ * les = 0; the boundary codes of vfs_create; an inlet only with inletprofile 100).  The
+ * reference has no adjoint: these entry points differentiate this library's own step,
+ * which reproduces the reference's Flow_Solver step.  Each call leaves the context in
+ * the state it had on entry. */
+enum {
+  VFS_OBJ_KINETIC_ENERGY = 0, /* 0.5 * sum over interior fluid cells of |Ucat|^2 / aj */
+  VFS_OBJ_PRESSURE_DRAG = 1   /* sum over k-faces between a fluid cell and a body cell
+                                 (nvert > 0) of +-P(fluid)*|zet|: streamwise pressure force */
+};
+enum {
+  VFS_CTRL_INITIAL_UCONT = 0, /* the Ucont the window starts from (DA layout, 3 per point) */
+  VFS_CTRL_INFLOW_PLANE = 1   /* the inletprofile 100 plane (vfs_set_inflow_plane layout) */
+};
+typedef struct {
+  int nsteps;            /* time steps in the window */
+  int checkpoint_every;  /* steps between stored states; <= 0: ceil(sqrt(nsteps)) */
+  int objective;         /* VFS_OBJ_* of the final state */
+  int control;           /* VFS_CTRL_* */
+  int reserved[4];
+  vfs_solve_opts solve;  /* forward, tangent and adjoint Poisson solves */
+} vfs_adjoint_opts;
+
+typedef struct {
+  double J;              /* objective */
+  double ms_forward;     /* forward sweep that stores the checkpoints */
+  double ms_adjoint;     /* reverse sweep: segment recomputation and adjoint steps */
+  int recomputed_steps;
+  int checkpoints;
+  long long tape_bytes;  /* per-segment linearisation state held on the device */
+  double reserved[4];
+} vfs_adjoint_stats;
+
+/* Measures the step's fixed linear operators (Contra2Cart, FormBCS tail, Pressure_Gradient,
+ * VolumeFlux, Poisson right-hand side, UpdatePressure, Projection, IB_BC, IB-node
+ * interpolation) as sparse matrices from the forward kernels.  Needs metrics and nvert (and
+ * the IB-node list when immersed); a later change of nvert or of the grid needs a new
+ * context.  The other adjoint entry points call it when needed. */
+int vfs_adjoint_setup(vfs_ctx *ctx);
+/* J after opts->nsteps steps from the current state. */
+int vfs_objective(vfs_ctx *ctx, const vfs_adjoint_opts *opts, double *J);
+/* J and its directional derivative along dir (the control's layout) by the tangent-linear
+ * steps. */
+int vfs_tangent(vfs_ctx *ctx, const vfs_adjoint_opts *opts, const double *dir, double *J, double *dJ);
+/* dJ/dcontrol by the adjoint steps, recomputing each checkpoint segment forward. */
+int vfs_adjoint_gradient(vfs_ctx *ctx, const vfs_adjoint_opts *opts, double *grad, vfs_adjoint_stats *stats);
+/* Test hooks: the slots (field, component pairs) and entry count of measured operator op
+ * (0 Contra2Cart, 1 FormBCS tail, 2 Pressure_Gradient, 3 VolumeFlux, 4 Poisson RHS, 5
+ * UpdatePressure, 6 Projection, 7 IB_BC, 8 IB-node interpolation), and the operator
+ * applied to in (slot-major, N per slot) by its kernels and by its matrix. */
+int vfs_adjoint_op_info(vfs_ctx *ctx, int op, int *nslot, int *fields, long long *nnz);
+int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *in, double *out_forward, double *out_matrix);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1576,4 +1576,428 @@ int runge_kutta(Ctx *c) {
   return form_bcs(c, true);
 }
 
+
+// ------------------------------------------------------------------ tangent / adjoint of a stage
+// Linearisation of one RK stage  Ucont' = pUcont + a*(Formfunction_2(Ucont, Ucat) - dP)
+// (les = 0) about the recorded stage input (uc, u): the face fluxes are linear in Ucat for
+// a fixed Ucont and, through the convecting flux, linear in Ucont (piecewise through the
+// upwind weights of the QUICK faces).  The tangent computes the face-flux tangents and
+// runs the forward Fp and right-hand-side kernels on them; the adjoint mirrors k_rhs,
+// k_fp and the face loops in reverse, scattering with atomics.
+
+// Up to four (index, weight) pairs: one computational-space difference of a face.
+struct DiffW { long long idx[4]; double w[4]; int n; };
+
+__device__ __forceinline__ void cross_desc(long long a0, long long a1, long long bp0, long long bp1, long long bm0,
+                                           long long bm1, bool ps, bool ms, DiffW &d) {
+  d.n = 4;
+  if (ps) {
+    d.idx[0] = a1; d.idx[1] = a0; d.idx[2] = bm1; d.idx[3] = bm0;
+    d.w[0] = 0.5; d.w[1] = 0.5; d.w[2] = -0.5; d.w[3] = -0.5;
+  } else if (ms) {
+    d.idx[0] = bp1; d.idx[1] = bp0; d.idx[2] = a1; d.idx[3] = a0;
+    d.w[0] = 0.5; d.w[1] = 0.5; d.w[2] = -0.5; d.w[3] = -0.5;
+  } else {
+    d.idx[0] = bp1; d.idx[1] = bp0; d.idx[2] = bm1; d.idx[3] = bm0;
+    d.w[0] = 0.25; d.w[1] = 0.25; d.w[2] = -0.25; d.w[3] = -0.25;
+  }
+}
+
+// Everything the face of direction D at point p (index qd along D) reads, as the face
+// loops of flux_i / flux_j / flux_k read it.
+struct FaceLin {
+  DiffW dw[3];                 // d/dcsi, d/deta, d/dzeta of each velocity component
+  double cs[3], et[3], ze[3];  // face metrics
+  double nrm[3];               // the face's own metric (csi, eta or zet)
+  double g[3];                 // g11, g21, g31 of the face
+  double K;                    // ajc * nu
+  int mode;                    // 0 central, 1 QUICK A, 2 QUICK B, 3 no convective flux
+  long long cidx[4];           // central: pL, p, p+s, pR; QUICK: the three cells
+  long long pcu, pucon;        // convecting flux (central) and upwinding flux (QUICK)
+};
+
+__device__ __forceinline__ void face_lin(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv, int D,
+                                         long long p, int i, int j, int k, FaceLin &F) {
+  const long long st[3] = {1, (long long)g.mx, (long long)g.mx * g.my};
+  const long long s = st[D];
+  const int qd = D == 0 ? i : (D == 1 ? j : k);
+  const int mm = D == 0 ? g.mx : (D == 1 ? g.my : g.mz);
+  const int per = D == 0 ? g.iper : (D == 1 ? g.jper : g.kper);
+  CV3 mc = D == 0 ? m.icsi : (D == 1 ? m.jcsi : m.kcsi);
+  CV3 me = D == 0 ? m.ieta : (D == 1 ? m.jeta : m.keta);
+  CV3 mz = D == 0 ? m.izet : (D == 1 ? m.jzet : m.kzet);
+  const double *aj = D == 0 ? m.iaj : (D == 1 ? m.jaj : m.kaj);
+  F.cs[0] = mc.x[p]; F.cs[1] = mc.y[p]; F.cs[2] = mc.z[p];
+  F.et[0] = me.x[p]; F.et[1] = me.y[p]; F.et[2] = me.z[p];
+  F.ze[0] = mz.x[p]; F.ze[1] = mz.y[p]; F.ze[2] = mz.z[p];
+  const double *n = D == 0 ? F.cs : (D == 1 ? F.et : F.ze);
+  for (int a = 0; a < 3; a++) F.nrm[a] = n[a];
+  F.g[0] = F.cs[0] * n[0] + F.cs[1] * n[1] + F.cs[2] * n[2];
+  F.g[1] = F.et[0] * n[0] + F.et[1] * n[1] + F.et[2] * n[2];
+  F.g[2] = F.ze[0] * n[0] + F.ze[1] * n[1] + F.ze[2] * n[2];
+  F.K = aj[p] * (1. / g.ren);
+  for (int E = 0; E < 3; E++) {
+    if (E == D) {
+      F.dw[E].n = 2;
+      F.dw[E].idx[0] = p + s; F.dw[E].w[0] = 1.0;
+      F.dw[E].idx[1] = p; F.dw[E].w[1] = -1.0;
+    } else {
+      const long long t = st[E];
+      cross_desc(p, p + s, p + t, p + t + s, p - t, p - t + s, nv[p + t] > 0 || nv[p + t + s] > 0,
+                 nv[p - t] > 0 || nv[p - t + s] > 0, F.dw[E]);
+    }
+  }
+  int qL = qd - 1, qR = qd + 2;
+  if (qd == 0 || qd == mm - 2) {
+    if (per) qL = mm - 3, qR = 2;
+    else qL = qd, qR = qd + 1;
+  } else if (nv[p - s] + nv[p + 2 * s] > 0) qL = qd, qR = qd + 1;
+  F.pucon = p;
+  if (per && (qd == 0 || qd == mm - 2)) F.pucon = p + (long long)(mm - 2 - qd) * s;
+  if (D == 2 && qd == mm - 2 && g.bc[5] == 4 && nv[p] == 0) F.pucon = p - s;
+  F.pcu = p;
+  if (g.immersed && qd != mm - 2 && nv[p] > 0) {
+    F.mode = 1; F.cidx[0] = p; F.cidx[1] = p + s; F.cidx[2] = p + 2 * s;
+  } else if (g.immersed && qd != 0 && nv[p + s] > 0) {
+    F.mode = 2; F.cidx[0] = p - s; F.cidx[1] = p; F.cidx[2] = p + s;
+  } else {
+    F.mode = 0;
+    F.cidx[0] = p + (long long)(qL - qd) * s; F.cidx[1] = p; F.cidx[2] = p + s;
+    F.cidx[3] = p + (long long)(qR - qd) * s;
+  }
+  if (nv[p] + nv[p + s] > 0 && !g.immersed) F.mode = 3;
+}
+
+__device__ __forceinline__ double comp(CV3 v, int c, long long p) { return c == 0 ? v.x[p] : (c == 1 ? v.y[p] : v.z[p]); }
+__device__ __forceinline__ double *compp(V3 v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+// QUICK coefficients: d = um*A + up*B with A, B linear in the three cells (variant A
+// cells u0 u1 u2 = p, p+s, p+2s; variant B cells um1 u0 u1 = p-s, p, p+s).
+__device__ __forceinline__ void quick_ab(int mode, double x0, double x1, double x2, double &A, double &B,
+                                         double dA[3], double dB[3]) {
+  if (mode == 1) {
+    A = 0.125 * (-x2 - 2. * x1 + 3. * x0) + x1; B = 0.125 * (-x0 - 2. * x0 + 3. * x1) + x0;
+    dA[0] = 0.375; dA[1] = 0.75; dA[2] = -0.125;
+    dB[0] = 0.625; dB[1] = 0.375; dB[2] = 0.0;
+  } else {
+    A = 0.125 * (-x2 - 2. * x2 + 3. * x1) + x2; B = 0.125 * (-x0 - 2. * x1 + 3. * x2) + x1;
+    dA[0] = 0.0; dA[1] = 0.375; dA[2] = 0.625;
+    dB[0] = -0.125; dB[1] = 0.75; dB[2] = 0.375;
+  }
+}
+
+// Tangent face fluxes of direction D at p: delta d (3) and delta v (3).
+__device__ __forceinline__ void face_tangent(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv, int D,
+                                             long long p, int i, int j, int k, CV3 uc, CV3 u, CV3 duc, CV3 du,
+                                             double dd[3], double dv[3]) {
+  FaceLin F;
+  face_lin(g, m, nv, D, p, i, j, k, F);
+  double dg[3][3];  // [E][component]
+  for (int E = 0; E < 3; E++)
+    for (int c = 0; c < 3; c++) {
+      double s = 0;
+      for (int t = 0; t < F.dw[E].n; t++) s += F.dw[E].w[t] * comp(du, c, F.dw[E].idx[t]);
+      dg[E][c] = s;
+    }
+  const double *mt[3] = {F.cs, F.et, F.ze};
+  for (int c = 0; c < 3; c++) {
+    double v = F.g[0] * dg[0][c] + F.g[1] * dg[1][c] + F.g[2] * dg[2][c];
+    for (int a = 0; a < 3; a++) {
+      const double r = dg[0][a] * mt[0][c] + dg[1][a] * mt[1][c] + dg[2][a] * mt[2][c];
+      v += r * F.nrm[a];
+    }
+    dv[c] = v * F.K;
+  }
+  const double *ucD = D == 0 ? uc.x : (D == 1 ? uc.y : uc.z);
+  const double *ducD = D == 0 ? duc.x : (D == 1 ? duc.y : duc.z);
+  for (int c = 0; c < 3; c++) dd[c] = 0;
+  if (F.mode == 0) {
+    const double cu = ucD[F.pcu], dcu = ducD[F.pcu];
+    for (int c = 0; c < 3; c++) {
+      const double S = -comp(u, c, F.cidx[0]) + 9. * comp(u, c, F.cidx[1]) + 9. * comp(u, c, F.cidx[2]) -
+                       comp(u, c, F.cidx[3]);
+      const double dS = -comp(du, c, F.cidx[0]) + 9. * comp(du, c, F.cidx[1]) + 9. * comp(du, c, F.cidx[2]) -
+                        comp(du, c, F.cidx[3]);
+      dd[c] = -dcu * 0.0625 * S - cu * 0.0625 * dS;
+    }
+  } else if (F.mode != 3) {
+    const double ucon = ucD[F.pucon], ducon = ducD[F.pucon];
+    const double up = -0.5 * (ucon + fabs(ucon)), um = -0.5 * (ucon - fabs(ucon));
+    const double sg = ucon > 0 ? 1. : (ucon < 0 ? -1. : 0.);
+    const double dum = -0.5 * (1. - sg) * ducon, dup = -0.5 * (1. + sg) * ducon;
+    for (int c = 0; c < 3; c++) {
+      double A, B, dA[3], dB[3];
+      quick_ab(F.mode, comp(u, c, F.cidx[0]), comp(u, c, F.cidx[1]), comp(u, c, F.cidx[2]), A, B, dA, dB);
+      double dAv = 0, dBv = 0;
+      for (int t = 0; t < 3; t++) {
+        const double x = comp(du, c, F.cidx[t]);
+        dAv += dA[t] * x; dBv += dB[t] * x;
+      }
+      dd[c] = dum * A + dup * B + um * dAv + up * dBv;
+    }
+  }
+}
+
+// Adjoint of the face of direction D at p: scatters lambda_d (3) and lambda_v (3) onto
+// the Ucont (luc) and Ucat (lu) adjoints.
+__device__ __forceinline__ void face_adjoint(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv, int D,
+                                             long long p, int i, int j, int k, CV3 uc, CV3 u, const double ld[3],
+                                             const double lv[3], V3 luc, V3 lu) {
+  FaceLin F;
+  face_lin(g, m, nv, D, p, i, j, k, F);
+  double lg[3][3] = {};  // adjoint of the differences [E][component]
+  const double *mt[3] = {F.cs, F.et, F.ze};
+  for (int c = 0; c < 3; c++) {
+    const double t = lv[c] * F.K;
+    if (t == 0) continue;
+    lg[0][c] += F.g[0] * t; lg[1][c] += F.g[1] * t; lg[2][c] += F.g[2] * t;
+    for (int a = 0; a < 3; a++) {
+      const double ta = t * F.nrm[a];
+      lg[0][a] += mt[0][c] * ta; lg[1][a] += mt[1][c] * ta; lg[2][a] += mt[2][c] * ta;
+    }
+  }
+  for (int E = 0; E < 3; E++)
+    for (int c = 0; c < 3; c++) {
+      if (lg[E][c] == 0) continue;
+      double *dst = compp(lu, c);
+      for (int t = 0; t < F.dw[E].n; t++) atomicAdd(dst + F.dw[E].idx[t], F.dw[E].w[t] * lg[E][c]);
+    }
+  const double *ucD = D == 0 ? uc.x : (D == 1 ? uc.y : uc.z);
+  double *lucD = D == 0 ? luc.x : (D == 1 ? luc.y : luc.z);
+  if (F.mode == 0) {
+    const double cu = ucD[F.pcu];
+    double lcu = 0;
+    for (int c = 0; c < 3; c++) {
+      if (ld[c] == 0) continue;
+      const double S = -comp(u, c, F.cidx[0]) + 9. * comp(u, c, F.cidx[1]) + 9. * comp(u, c, F.cidx[2]) -
+                       comp(u, c, F.cidx[3]);
+      lcu += -0.0625 * S * ld[c];
+      const double w = -cu * 0.0625 * ld[c];
+      double *dst = compp(lu, c);
+      atomicAdd(dst + F.cidx[0], -w);
+      atomicAdd(dst + F.cidx[1], 9. * w);
+      atomicAdd(dst + F.cidx[2], 9. * w);
+      atomicAdd(dst + F.cidx[3], -w);
+    }
+    if (lcu != 0) atomicAdd(lucD + F.pcu, lcu);
+  } else if (F.mode != 3) {
+    const double ucon = ucD[F.pucon];
+    const double up = -0.5 * (ucon + fabs(ucon)), um = -0.5 * (ucon - fabs(ucon));
+    const double sg = ucon > 0 ? 1. : (ucon < 0 ? -1. : 0.);
+    double lum = 0, lup = 0;
+    for (int c = 0; c < 3; c++) {
+      if (ld[c] == 0) continue;
+      double A, B, dA[3], dB[3];
+      quick_ab(F.mode, comp(u, c, F.cidx[0]), comp(u, c, F.cidx[1]), comp(u, c, F.cidx[2]), A, B, dA, dB);
+      lum += A * ld[c]; lup += B * ld[c];
+      double *dst = compp(lu, c);
+      for (int t = 0; t < 3; t++) {
+        const double w = (um * dA[t] + up * dB[t]) * ld[c];
+        if (w != 0) atomicAdd(dst + F.cidx[t], w);
+      }
+    }
+    const double lucon = lum * (-0.5 * (1. - sg)) + lup * (-0.5 * (1. + sg));
+    if (lucon != 0) atomicAdd(lucD + F.pucon, lucon);
+  }
+}
+
+struct FaceBank { double *f[3][6]; };
+
+__global__ void k_tan_face(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV3 uc, CV3 u, CV3 duc, CV3 du,
+                           FaceBank out) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int i = (int)(p % g.mx);
+  const long long q = p / g.mx;
+  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  if (i == g.mx - 1 || j == g.my - 1 || k == g.mz - 1) return;
+  const bool on[3] = {j != 0 && k != 0, i != 0 && k != 0, i != 0 && j != 0};
+  for (int D = 0; D < 3; D++) {
+    if (!on[D]) continue;
+    double dd[3], dv[3];
+    face_tangent(g, m, nv, D, p, i, j, k, uc, u, duc, du, dd, dv);
+    for (int c = 0; c < 3; c++) { out.f[D][c][p] = dd[c]; out.f[D][3 + c][p] = dv[c]; }
+  }
+}
+
+__global__ void k_adj_face(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV3 uc, CV3 u, FaceBank lf, V3 luc,
+                           V3 lu) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int i = (int)(p % g.mx);
+  const long long q = p / g.mx;
+  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  if (i == g.mx - 1 || j == g.my - 1 || k == g.mz - 1) return;
+  const bool on[3] = {j != 0 && k != 0, i != 0 && k != 0, i != 0 && j != 0};
+  for (int D = 0; D < 3; D++) {
+    if (!on[D]) continue;
+    double ld[3], lv[3];
+    bool any = false;
+    for (int c = 0; c < 3; c++) {
+      ld[c] = lf.f[D][c][p]; lv[c] = lf.f[D][3 + c][p];
+      any |= ld[c] != 0 || lv[c] != 0;
+    }
+    if (any) face_adjoint(g, m, nv, D, p, i, j, k, uc, u, ld, lv, luc, lu);
+  }
+}
+
+// Adjoint of fp_cell: lambda_Fp of each interior cell onto the face-flux adjoints it read.
+__global__ void k_adj_fp(Grid g, const uint8_t *__restrict__ nv, const double *__restrict__ lfx,
+                         const double *__restrict__ lfy, const double *__restrict__ lfz, FaceBank lf) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  const int i = (int)(p % mx);
+  const long long q = p / mx;
+  const int j = (int)(q % my), k = (int)(q / my);
+  if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
+  const double l[3] = {lfx[p], lfy[p], lfz[p]};
+  if (l[0] == 0 && l[1] == 0 && l[2] == 0) return;
+  const long long sy = mx, sz = (long long)mx * my;
+  int oR[3], oL[3];
+  double den[3];
+  fp_offsets(i, mx, g.iper, nv[p - 1] + nv[p] + nv[p + 1], oR[0], oL[0], den[0]);
+  fp_offsets(j, my, g.jper, nv[p - sy] + nv[p] + nv[p + sy], oR[1], oL[1], den[1]);
+  fp_offsets(k, mz, g.kper, nv[p - sz] + nv[p] + nv[p + sz], oR[2], oL[2], den[2]);
+  const long long row[3] = {p - i, p - (long long)j * mx, p - (long long)k * mx * my};
+  const int idx[3] = {i, j, k};
+  const int ext[3] = {mx, my, mz};
+  const int per[3] = {g.iper, g.jper, g.kper};
+  const long long str[3] = {1, sy, sz};
+  for (int D = 0; D < 3; D++) {
+    auto at = [&](int off) { return row[D] + (long long)face_image(idx[D] + off, ext[D], per[D]) * str[D]; };
+    const long long f0 = at(0), fm = at(-1), fR = at(oR[D]), fL = at(oL[D]);
+    const double wide = -1. / 8. * (1. / den[D]);
+    for (int c = 0; c < 3; c++) {
+      if (l[c] == 0) continue;
+      atomicAdd(lf.f[D][c] + f0, 9. / 8. * l[c]);
+      atomicAdd(lf.f[D][c] + fm, -9. / 8. * l[c]);
+      atomicAdd(lf.f[D][c] + fR, wide * l[c]);
+      atomicAdd(lf.f[D][c] + fL, -wide * l[c]);
+      atomicAdd(lf.f[D][3 + c] + f0, l[c]);
+      atomicAdd(lf.f[D][3 + c] + fm, -l[c]);
+    }
+  }
+}
+
+// Adjoint of rhs_point in RK mode (scale 1): lambda of the stage output Ucont' onto
+// pUcont, dP and Fp.
+__global__ void k_adj_rhs(Grid g, Metrics m, const uint8_t *__restrict__ nv, double a, CV3 lU, V3 lpu, V3 ldp,
+                          double *lfx, double *lfy, double *lfz) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  const int i = (int)(p % mx);
+  const long long q = p / mx;
+  const int j = (int)(q % my), k = (int)(q / my);
+  const double l0 = lU.x[p], l1 = lU.y[p], l2 = lU.z[p];
+  lpu.x[p] += l0; lpu.y[p] += l1; lpu.z[p] += l2;
+  ldp.x[p] -= a * l0; ldp.y[p] -= a * l1; ldp.z[p] -= a * l2;
+  const bool ghost = i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == mz - 1;
+  if (ghost) return;
+  const long long sy = mx, sz = (long long)mx * my;
+  double r0 = a * l0, r1 = a * l1, r2 = a * l2;
+  if (nv[p] + nv[p + 1] > 0 || (!g.iper && i == mx - 2)) r0 = 0;
+  if (nv[p] + nv[p + sy] > 0 || (!g.jper && j == my - 2)) r1 = 0;
+  if (nv[p] + nv[p + sz] > 0 || (!g.kper && k == mz - 2)) r2 = 0;
+  const long long q1 = (g.iper && i == mx - 2) ? p - i + 1 : p + 1;
+  const long long q2 = (g.jper && j == my - 2) ? p - (long long)j * sy + sy : p + sy;
+  const long long q3 = (g.kper && k == mz - 2) ? p - (long long)k * sz + sz : p + sz;
+  double *lf[3] = {lfx, lfy, lfz};
+  if (r0 != 0) {
+    const double w = 0.5 * m.iaj[p] * r0;
+    const double a0[3] = {m.csi.x[p], m.csi.y[p], m.csi.z[p]}, a1[3] = {m.csi.x[p + 1], m.csi.y[p + 1], m.csi.z[p + 1]};
+    for (int c = 0; c < 3; c++) { atomicAdd(lf[c] + p, w * a0[c]); atomicAdd(lf[c] + q1, w * a1[c]); }
+  }
+  if (r1 != 0) {
+    const double w = 0.5 * m.jaj[p] * r1;
+    const double a0[3] = {m.eta.x[p], m.eta.y[p], m.eta.z[p]};
+    const double a1[3] = {m.eta.x[p + sy], m.eta.y[p + sy], m.eta.z[p + sy]};
+    for (int c = 0; c < 3; c++) { atomicAdd(lf[c] + p, w * a0[c]); atomicAdd(lf[c] + q2, w * a1[c]); }
+  }
+  if (r2 != 0) {
+    const double w = 0.5 * m.kaj[p] * r2;
+    const double a0[3] = {m.zet.x[p], m.zet.y[p], m.zet.z[p]};
+    const double a1[3] = {m.zet.x[p + sz], m.zet.y[p + sz], m.zet.z[p + sz]};
+    for (int c = 0; c < 3; c++) { atomicAdd(lf[c] + p, w * a0[c]); atomicAdd(lf[c] + q3, w * a1[c]); }
+  }
+}
+
+// Transpose of the periodic ghost copy: each ghost point hands its adjoint to its image.
+__global__ void k_periodic_copy_adj(Grid g, double *a, double *b, double *c) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int i = (int)(p % g.mx);
+  const long long q = p / g.mx;
+  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  const bool gi = g.iper && (i == 0 || i == g.mx - 1), gj = g.jper && (j == 0 || j == g.my - 1);
+  const bool gk = g.kper && (k == 0 || k == g.mz - 1);
+  if (!(gi || gj || gk)) return;
+  const long long s = lidx(g, wrapi(g, i), wrapj(g, j), wrapk(g, k));
+  double *arr[3] = {a, b, c};
+  for (int t = 0; t < 3; t++) {
+    if (!arr[t]) continue;
+    const double v = arr[t][p];
+    arr[t][p] = 0;
+    if (v != 0) atomicAdd(arr[t] + s, v);
+  }
+}
+
+int periodic_copy_adj3(Ctx *c, V3 v) {
+  if (!(c->g.iper || c->g.jper || c->g.kper)) return VFS_OK;
+  k_periodic_copy_adj<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
+  return check_launch(c, "k_periodic_copy_adj");
+}
+
+// Tangent of one stage: dU (in: tangent of the stage input; out: of the stage output).
+int ff2_stage_tangent(Ctx *c, const double *const uc[3], const double *const uk[3], double a, V3 dU, V3 du, V3 ddp,
+                      V3 dpu, double *const tf[3][6]) {
+  const Grid &g = c->g;
+  int rc;
+  if ((rc = periodic_copy3(c, dU))) return rc;
+  FaceBank fb;
+  for (int d = 0; d < 3; d++)
+    for (int q = 0; q < 6; q++) fb.f[d][q] = tf[d][q];
+  Metrics m = metrics(c);
+  CV3 ucb{uc[0], uc[1], uc[2]}, ukb{uk[0], uk[1], uk[2]};
+  k_tan_face<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, c->nv, ucb, ukb, cv(dU), cv(du), fb);
+  if ((rc = check_launch(c, "k_tan_face"))) return rc;
+  FluxIn f[3];
+  for (int d = 0; d < 3; d++)
+    for (int q = 0; q < 3; q++) { f[d].div[q] = tf[d][q]; f[d].visc[q] = tf[d][3 + q]; }
+  k_fp<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, f[0], f[1], f[2], c->nv, c->fp[0], c->fp[1], c->fp[2]);
+  if ((rc = check_launch(c, "k_fp"))) return rc;
+  k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], 1.0, field3(c, VFS_RHS),
+                                                 1, a, cv(ddp), cv(dpu), dU);
+  return check_launch(c, "k_rhs");
+}
+
+// Adjoint of one stage: lU (in: adjoint of the stage output; out: of the stage input),
+// lu (Ucat adjoint), ldp and lpu accumulate.
+int ff2_stage_adjoint(Ctx *c, const double *const uc[3], const double *const uk[3], double a, V3 lU, V3 lu, V3 ldp,
+                      V3 lpu, double *const lf[3][6], double *const lfp[3]) {
+  const Grid &g = c->g;
+  const size_t bytes = sizeof(double) * g.N;
+  int rc;
+  for (int d = 0; d < 3; d++) {
+    cudaMemsetAsync(lfp[d], 0, bytes, c->stream);
+    for (int q = 0; q < 6; q++) cudaMemsetAsync(lf[d][q], 0, bytes, c->stream);
+  }
+  Metrics m = metrics(c);
+  k_adj_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, a, cv(lU), lpu, ldp, lfp[0], lfp[1], lfp[2]);
+  if ((rc = check_launch(c, "k_adj_rhs"))) return rc;
+  cudaMemsetAsync(lU.x, 0, bytes, c->stream);
+  cudaMemsetAsync(lU.y, 0, bytes, c->stream);
+  cudaMemsetAsync(lU.z, 0, bytes, c->stream);
+  FaceBank fb;
+  for (int d = 0; d < 3; d++)
+    for (int q = 0; q < 6; q++) fb.f[d][q] = lf[d][q];
+  k_adj_fp<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, lfp[0], lfp[1], lfp[2], fb);
+  if ((rc = check_launch(c, "k_adj_fp"))) return rc;
+  CV3 ucb{uc[0], uc[1], uc[2]}, ukb{uk[0], uk[1], uk[2]};
+  k_adj_face<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, c->nv, ucb, ukb, fb, lU, lu);
+  if ((rc = check_launch(c, "k_adj_face"))) return rc;
+  return periodic_copy_adj3(c, lU);
+}
+
 }  // namespace vfs

@@ -82,6 +82,26 @@ class StepStats(ctypes.Structure):
     ]
 
 
+class AdjointOpts(ctypes.Structure):
+    _fields_ = [
+        ("nsteps", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("objective", ctypes.c_int),
+        ("control", ctypes.c_int), ("reserved", ctypes.c_int * 4), ("solve", SolveOpts),
+    ]
+
+
+class AdjointStats(ctypes.Structure):
+    _fields_ = [
+        ("J", ctypes.c_double), ("ms_forward", ctypes.c_double), ("ms_adjoint", ctypes.c_double),
+        ("recomputed_steps", ctypes.c_int), ("checkpoints", ctypes.c_int), ("tape_bytes", ctypes.c_longlong),
+        ("reserved", ctypes.c_double * 4),
+    ]
+
+
+OBJ_KINETIC_ENERGY, OBJ_PRESSURE_DRAG = 0, 1
+CTRL_INITIAL_UCONT, CTRL_INFLOW_PLANE = 0, 1
+OP_NAMES = ["contra2cart", "form_bcs_tail", "pressure_gradient", "volume_flux", "poisson_rhs",
+            "update_pressure", "projection", "ib_bc", "ibm_interpolation"]
+
 EXPORTS = [
     "vfs_create", "vfs_destroy", "vfs_last_error", "vfs_dims", "vfs_synchronize",
     "vfs_launch_count", "vfs_set_field", "vfs_get_field", "vfs_set_scalar", "vfs_get_scalar",
@@ -92,6 +112,8 @@ EXPORTS = [
     "vfs_form_metrics", "vfs_volume_flux", "vfs_get_stream", "vfs_run_kernel",
     "vfs_smagorinsky_constant", "vfs_eddy_viscosity", "vfs_inflow_flux", "vfs_set_inflow_plane",
     "vfs_ibm_search", "vfs_ibm_list", "vfs_ibm_interpolation",
+    "vfs_adjoint_setup", "vfs_objective", "vfs_tangent", "vfs_adjoint_gradient",
+    "vfs_adjoint_op_info", "vfs_adjoint_op_check",
 ]
 
 _lib = None
@@ -140,6 +162,13 @@ def load_library(path=None):
     lib.vfs_form_metrics.argtypes = [vp, vp, vp, vp]
     lib.vfs_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.vfs_run_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.vfs_adjoint_setup.argtypes = [vp]
+    lib.vfs_objective.argtypes = [vp, ctypes.POINTER(AdjointOpts), dp]
+    lib.vfs_tangent.argtypes = [vp, ctypes.POINTER(AdjointOpts), vp, dp, dp]
+    lib.vfs_adjoint_gradient.argtypes = [vp, ctypes.POINTER(AdjointOpts), vp, ctypes.POINTER(AdjointStats)]
+    lib.vfs_adjoint_op_info.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp,
+                                        ctypes.POINTER(ctypes.c_longlong)]
+    lib.vfs_adjoint_op_check.argtypes = [vp, ctypes.c_int, vp, vp, vp]
     if path is None:
         _lib = lib
     return lib
@@ -351,6 +380,71 @@ class Context:
         st = StepStats()
         self._check(self.lib.vfs_step(self.h, ctypes.byref(o), ctypes.byref(st)))
         return st
+
+    # ---- tangent-linear and adjoint of a window of steps (no reference counterpart)
+    def _adj_opts(self, nsteps, objective, control, checkpoint_every, precision, rtol, kw):
+        return AdjointOpts(nsteps=nsteps, checkpoint_every=checkpoint_every, objective=objective,
+                           control=control, solve=_solve_opts(precision, rtol, **kw))
+
+    def control_shape(self, control):
+        if control == CTRL_INFLOW_PLANE:
+            return (self.shape[1], self.shape[2], 3)
+        return self.shape + (3,)
+
+    def adjoint_setup(self):
+        self._check(self.lib.vfs_adjoint_setup(self.h))
+
+    def objective(self, nsteps, objective=OBJ_KINETIC_ENERGY, control=CTRL_INITIAL_UCONT, checkpoint_every=0,
+                  precision=1, rtol=1e-12, **kw):
+        """J after nsteps steps from the current state (the state is kept)."""
+        o = self._adj_opts(nsteps, objective, control, checkpoint_every, precision, rtol, kw)
+        J = ctypes.c_double()
+        self._check(self.lib.vfs_objective(self.h, ctypes.byref(o), ctypes.byref(J)))
+        return J.value
+
+    def tangent(self, direction, nsteps, objective=OBJ_KINETIC_ENERGY, control=CTRL_INITIAL_UCONT,
+                precision=1, rtol=1e-12, **kw):
+        """(J, dJ) with dJ the derivative of J along direction (the control's shape)."""
+        o = self._adj_opts(nsteps, objective, control, 0, precision, rtol, kw)
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        if d.shape != self.control_shape(control):
+            raise ValueError("direction must have shape %s" % (self.control_shape(control),))
+        J, dJ = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.vfs_tangent(self.h, ctypes.byref(o), d.ctypes.data, ctypes.byref(J), ctypes.byref(dJ)))
+        return J.value, dJ.value
+
+    def adjoint_gradient(self, nsteps, objective=OBJ_KINETIC_ENERGY, control=CTRL_INITIAL_UCONT,
+                         checkpoint_every=0, precision=1, rtol=1e-12, **kw):
+        """(gradient of J with respect to the control, AdjointStats)."""
+        o = self._adj_opts(nsteps, objective, control, checkpoint_every, precision, rtol, kw)
+        g = np.zeros(self.control_shape(control))
+        st = AdjointStats()
+        self._check(self.lib.vfs_adjoint_gradient(self.h, ctypes.byref(o), g.ctypes.data, ctypes.byref(st)))
+        return g, st
+
+    def adjoint_op_info(self, op):
+        n = ctypes.c_int()
+        fields = (ctypes.c_int * 20)()
+        nnz = ctypes.c_longlong()
+        self._check(self.lib.vfs_adjoint_op_info(self.h, op, ctypes.byref(n), fields, ctypes.byref(nnz)))
+        return [(fields[2 * s], fields[2 * s + 1]) for s in range(n.value)], nnz.value
+
+    def adjoint_op_check(self, op, x):
+        """The measured operator op applied to x (slots x N) by its kernels and by its matrix."""
+        slots, _ = self.adjoint_op_info(op)
+        N = int(np.prod(self.shape))
+        a = np.ascontiguousarray(x, dtype=np.float64).reshape(len(slots), N)
+        out_f = np.zeros_like(a)
+        out_m = np.zeros_like(a)
+        self._check(self.lib.vfs_adjoint_op_check(self.h, op, a.ctypes.data, out_f.ctypes.data, out_m.ctypes.data))
+        return out_f, out_m
+
+
+def _solve_opts(precision=0, rtol=1e-10, **kw):
+    return SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
+                     max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 0),
+                     pre_smooth=kw.get("pre_smooth", 2), post_smooth=kw.get("post_smooth", 2),
+                     coarse_iters=kw.get("coarse_iters", 4))
 
 
 def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
