@@ -331,6 +331,54 @@ def reference_arm(args, rank, world):
 
 
 # ------------------------------------------------------------------ our arm
+ADJ_WORKLOAD = ("wavy-wall channel %dx%dx%d cells (bottom y_w = 0.1 sin(2 pi x/Lx) cos(2 pi z/Lz)), "
+                "immersed sphere D=0.4 at the centre (icosphere, 20480 triangles, IB nodes), inlet k=0 "
+                "(inletprofile 100) and outlet k+, FP64 Poisson rtol 1e-10; objective: streamwise "
+                "pressure force on the body after %d steps; control: the inflow plane; checkpoint "
+                "every %d steps")
+
+
+def adjoint_window(nx, ny, nz, steps, every, torch):
+    """The discrete adjoint of a window of FP64 steps on the curvilinear grid with the
+    sphere: gradient of the body's pressure force after `steps` steps with respect to the
+    inflow plane.  Returns the reverse sweep (segment recomputation + adjoint steps) and the
+    forward sweep timed on the device, and the one-off operator set-up time."""
+    import vfs_b200 as vfs
+    from vfs_b200 import cases
+    case = cases.channel(nx, ny, nz, wavy=0.1)
+    case.immersed = 1
+    cases.inflow_outflow(case, 100)
+    ctx = vfs.Context(case.config())
+    ctx.form_metrics(case.X, case.Y, case.Z)
+    ctx.set_field(vfs.NVERT, case.nvert)
+    ctx.ibm_search(*cases.icosphere((np.pi / 2, 1.0, np.pi), 0.2, level=5))
+    m = {n: ctx.get_field(f) for n, f in vfs.METRIC_FIELDS.items()}
+    case.nvert = ctx.get_field(vfs.NVERT)
+    u = cases.initial_ucat(case, seed=0)
+    ctx.set_field(vfs.UCONT, cases.ucont_from_ucat(case, u, m))
+    ctx.set_field(vfs.UCAT, u)
+    ctx.set_field(vfs.UCAT_O, u)
+    ctx.set_scalar(vfs.S_INLET_FLUX, 0.0)
+    _, area = ctx.calc_inlet_area()
+    ctx.set_scalar(vfs.S_INLET_FLUX, area)
+    ctx.set_inflow_plane(cases.inflow_plane(case))
+    t0 = time.perf_counter()
+    ctx.adjoint_setup()
+    setup_s = time.perf_counter() - t0
+    kw = dict(objective=vfs.OBJ_PRESSURE_DRAG, control=vfs.CTRL_INFLOW_PLANE, precision=1, rtol=1e-10)
+    ctx.adjoint_gradient(2, checkpoint_every=1, **kw)  # warm-up: tapes, Krylov space
+    torch.cuda.synchronize()
+    g, st = ctx.adjoint_gradient(steps, checkpoint_every=every, **kw)
+    ctx.close()
+    return {"workload": ADJ_WORKLOAD % (nx, ny, nz, steps, every), "steps": steps, "checkpoint_every": every,
+            "forward_ms": round(st.ms_forward, 2), "adjoint_ms": round(st.ms_adjoint, 2),
+            "ratio": round(st.ms_adjoint / st.ms_forward, 3), "recomputed_steps": st.recomputed_steps,
+            "tape_bytes": st.tape_bytes, "operator_setup_s": round(setup_s, 1),
+            "J": st.J, "gradient_norm": float(np.sqrt((g * g).sum())),
+            "note": "ratio = reverse sweep (recomputation of every checkpoint segment plus the adjoint "
+                    "steps) / forward sweep of the same window"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -339,6 +387,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", default=None, help="nx,ny,nz override (not for reported numbers)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
+    ap.add_argument("--adjoint-size", default="128,128,128")
+    ap.add_argument("--adjoint-steps", type=int, default=20)
     ap.add_argument("--profile-step", action="store_true",
                     help="after the warm-up, run one mixed step inside cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no JSON")
@@ -438,6 +489,15 @@ def main():
     n0 = ctx.launch_count()
     ctx.step(precision=0, rtol=1e-10)
     launches_per_step = ctx.launch_count() - n0
+    ctx.close()
+
+    adj = None
+    if not args.no_adjoint and not args.size:
+        ax, ay, az = (int(v) for v in args.adjoint_size.split(","))
+        try:
+            adj = adjoint_window(ax, ay, az, args.adjoint_steps, 5, torch)
+        except Exception as e:  # reported, never fatal for the forward numbers
+            adj = {"failed": str(e)}
 
     out = None
     if rank == 0:
@@ -471,7 +531,7 @@ def main():
             "mixed_speedup_vs_fp64": round(ms_fp64 / ms_mixed, 3),
             "max_div": {"mixed": maxdiv, "fp64": maxdiv64},
             "poisson_iterations": {"mixed": its, "fp64": its64},
-            "adjoint_forward_ratio": None,
+            "adjoint_forward_ratio": adj.get("ratio") if adj else None,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms/step", "h2d_bytes_per_step": io_bytes,
                     "d2h_bytes_per_step": io_bytes},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -483,10 +543,11 @@ def main():
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": sampler.summary(),
         }
+        if adj is not None:
+            out["adjoint"] = adj
         if cpu is not None:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))
-    ctx.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -146,22 +146,31 @@ def test_adjoint_matches_tangent(name):
 
 @pytest.mark.gpu
 def test_gradient_matches_finite_differences_at_32_inlet_nodes():
-    """dJ/d(inflow plane) at 32 seeded fluid inlet entries against central differences."""
+    """dJ/d(inflow plane) at 32 seeded inlet entries against central differences.  Along a
+    random combination of the 32 entries the difference with a step of 1e-6 agrees to 1e-6
+    relative.  Entry by entry a change of 1e-6 moves J by about 1e-11, near the rounding of
+    J itself (about 1e-12), so each entry is differenced with a step of 1e-5 and must agree
+    to 1e-6 of the largest gradient entry."""
     ctx, case, obj, ctrl = _context("inlet")
-    g, st = ctx.adjoint_gradient(NSTEPS, obj, ctrl, rtol=1e-14, max_iter=400)
+    g, st = ctx.adjoint_gradient(NSTEPS, obj, ctrl)
     x0 = _control(ctx, case, ctrl)
     rng = np.random.Generator(np.random.Philox(32))
     my, mx = ctx.shape[1], ctx.shape[2]
     picks = set()
     while len(picks) < 32:
         picks.add((int(rng.integers(1, my - 1)), int(rng.integers(1, mx - 1)), int(rng.integers(0, 3))))
+    picks = sorted(picks)
+    d = np.zeros_like(x0)
+    for (j, i, c) in picks:
+        d[j, i, c] = rng.standard_normal()
+    fd = _fd(ctx, case, obj, ctrl, d, x0, rel=1e-6)
+    gd = float((g * d).sum())
+    assert abs(gd - fd) <= 1e-6 * abs(fd), (gd, fd)
     gmax = np.abs(g).max()
-    for (j, i, c) in sorted(picks):
-        d = np.zeros_like(x0)
-        d[j, i, c] = 1.0
-        fd = _fd(ctx, case, obj, ctrl, d, x0, rtol=1e-14)
-        # 1e-6 relative to the gradient's largest entry: the central difference with a step
-        # of 1e-6 resolves about that much above the Poisson solves' residual
+    for (j, i, c) in picks:
+        e = np.zeros_like(x0)
+        e[j, i, c] = 1.0
+        fd = _fd(ctx, case, obj, ctrl, e, x0, rel=1e-5)
         assert abs(g[j, i, c] - fd) <= 1e-6 * gmax, ((j, i, c), g[j, i, c], fd, gmax)
     ctx.close()
 

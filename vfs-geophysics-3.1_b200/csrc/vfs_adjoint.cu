@@ -173,17 +173,20 @@ int tape_vflux(Ctx *c) {
 
 // ---------------------------------------------------------------- probing
 // Colouring of the DA points.  Along a periodic direction of L = m-2 interior points the
-// colour follows the position on the periodic circle (ghost 0 is the image of m-2, ghost
-// m-1 of 1): positions 0..L-r-1 take (position mod q), the last r = L mod q positions
-// their own colours, so two points within q-1 of each other around the circle never share
-// a colour.  Other directions take (index mod q).  Any two inputs of an operator whose
-// stencil spans at most q-1 points per direction therefore differ in colour.
+// colour follows the position on the periodic circle: positions 0..L-r-1 take (position
+// mod q), the last r = L mod q positions their own colours, so two interior points within
+// q-1 of each other around the circle never share a colour; the two ghost planes (which
+// operators read beside their periodic images) take two more colours of their own.  Other
+// directions take (index mod q).  Any two inputs of an operator whose stencil spans at
+// most q-1 points per direction therefore differ in colour.
 struct ColourMap {
   int q, m[3], per[3], nc[3];
   __host__ __device__ int dim(int d, int i) const {
     if (!per[d]) return i % q;
     const int L = m[d] - 2, rem = L % q, main = L - rem;
-    const int pos = i == 0 ? L - 1 : (i == m[d] - 1 ? 0 : i - 1);
+    if (i == 0) return q + rem;
+    if (i == m[d] - 1) return q + rem + 1;
+    const int pos = i - 1;
     return pos < main ? pos % q : q + (pos - main);
   }
   __host__ __device__ int of(long long p) const {
@@ -200,7 +203,7 @@ static ColourMap colour_map(const Grid &g, int q) {
   cm.q = q;
   cm.m[0] = g.mx; cm.m[1] = g.my; cm.m[2] = g.mz;
   cm.per[0] = g.iper; cm.per[1] = g.jper; cm.per[2] = g.kper;
-  for (int d = 0; d < 3; d++) cm.nc[d] = cm.per[d] ? q + (cm.m[d] - 2) % q : q;
+  for (int d = 0; d < 3; d++) cm.nc[d] = cm.per[d] ? q + (cm.m[d] - 2) % q + 2 : q;
   return cm;
 }
 
@@ -507,7 +510,7 @@ static int adjoint_setup(Ctx *c) {
   if ((rc = probe(c, "IB_BC", A.op[OP_IBBC], 5, [](Ctx *x) { return ib_bc(x); }))) return rc;
   if (imm) {
     set_slots(A.op[OP_IBM], {VFS_UCAT, VFS_P, VFS_UCONT, VFS_UCAT_O});
-    if ((rc = probe(c, "the IB-node interpolation", A.op[OP_IBM], 9, [](Ctx *x) { return ibm_interpolation(x); }))) return rc;
+    if ((rc = probe(c, "the IB-node interpolation", A.op[OP_IBM], 7, [](Ctx *x) { return ibm_interpolation(x); }))) return rc;
   }
   // dP.z per unit flux deficit of the k-periodic forcing: Pressure_Gradient with P = 0
   if (c->g.kper && pressure_forcing_mode(c) == 2) {
