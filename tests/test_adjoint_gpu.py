@@ -146,11 +146,12 @@ def test_adjoint_matches_tangent(name):
 
 @pytest.mark.gpu
 def test_gradient_matches_finite_differences_at_32_inlet_nodes():
-    """dJ/d(inflow plane) at 32 seeded inlet entries against central differences.  Along a
-    random combination of the 32 entries the difference with a step of 1e-6 agrees to 1e-6
-    relative.  Entry by entry a change of 1e-6 moves J by about 1e-11, near the rounding of
-    J itself (about 1e-12), so each entry is differenced with a step of 1e-5 and must agree
-    to 1e-6 of the largest gradient entry."""
+    """dJ/d(inflow plane) at 32 seeded inlet entries against central differences, along a
+    random combination of the 32 entries and entry by entry.  The differences use a step of
+    1e-4 of the plane's largest value: with the step of 1e-6 the change of J from a single
+    entry (about 1e-11) is of the order of the rounding noise of the forward window itself,
+    while the truncation error of the 1e-4 step stays near 1e-8 relative.  Agreement: 1e-6
+    relative along the combination, 1e-6 of the largest gradient entry entry by entry."""
     ctx, case, obj, ctrl = _context("inlet")
     g, st = ctx.adjoint_gradient(NSTEPS, obj, ctrl)
     x0 = _control(ctx, case, ctrl)
@@ -163,14 +164,14 @@ def test_gradient_matches_finite_differences_at_32_inlet_nodes():
     d = np.zeros_like(x0)
     for (j, i, c) in picks:
         d[j, i, c] = rng.standard_normal()
-    fd = _fd(ctx, case, obj, ctrl, d, x0, rel=1e-6)
+    fd = _fd(ctx, case, obj, ctrl, d, x0, rel=1e-4)
     gd = float((g * d).sum())
     assert abs(gd - fd) <= 1e-6 * abs(fd), (gd, fd)
     gmax = np.abs(g).max()
     for (j, i, c) in picks:
         e = np.zeros_like(x0)
         e[j, i, c] = 1.0
-        fd = _fd(ctx, case, obj, ctrl, e, x0, rel=1e-5)
+        fd = _fd(ctx, case, obj, ctrl, e, x0, rel=1e-4)
         assert abs(g[j, i, c] - fd) <= 1e-6 * gmax, ((j, i, c), g[j, i, c], fd, gmax)
     ctx.close()
 

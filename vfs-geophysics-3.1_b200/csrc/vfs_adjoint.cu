@@ -62,6 +62,7 @@ struct Adjoint {
   std::vector<StepTape> tapes;      // one per step of the recompute segment
   double *ckpt = nullptr;           // checkpoints of the state
   int nckpt = 0;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;  // sweep timing (the step and the solver use the context's)
 };
 
 static int grow(Ctx *c, double **p, size_t n) {
@@ -133,6 +134,8 @@ void adjoint_free(Ctx *c) {
   }
   cudaFree(A.cz);
   cudaFree(A.ckpt);
+  if (A.t0) cudaEventDestroy(A.t0);
+  if (A.t1) cudaEventDestroy(A.t1);
   free_tapes(A);
   delete c->adj;
   c->adj = nullptr;
@@ -1225,7 +1228,9 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
   const int nseg = (n + every - 1) / every;
   if ((rc = ensure_tapes(c, std::min(every, n)))) return rc;
   std::vector<HostState> hs(nseg);
-  cudaEventRecord(c->ev0, c->stream);
+  if (!A.t0) cudaEventCreate(&A.t0);
+  if (!A.t1) cudaEventCreate(&A.t1);
+  cudaEventRecord(A.t0, c->stream);
   for (int sg = 0; sg < nseg && !rc; sg++) {
     save_state(c, ckpt(c, sg), hs[sg]);
     for (int s = 0; s < std::min(every, n - sg * every) && !rc; s++) rc = step_forward(c, o, nullptr);
@@ -1235,11 +1240,11 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
     zero_bank(c, ADJ);
     rc = objective(c, o->objective, true, &J);
   }
-  cudaEventRecord(c->ev1, c->stream);
-  cudaEventSynchronize(c->ev1);
+  cudaEventRecord(A.t1, c->stream);
+  cudaEventSynchronize(A.t1);
   float msf = 0;
-  cudaEventElapsedTime(&msf, c->ev0, c->ev1);
-  cudaEventRecord(c->ev0, c->stream);
+  cudaEventElapsedTime(&msf, A.t0, A.t1);
+  cudaEventRecord(A.t0, c->stream);
   int recomputed = 0;
   for (int sg = nseg - 1; sg >= 0 && !rc; sg--) {
     const int len = std::min(every, n - sg * every);
@@ -1247,10 +1252,10 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
     for (int s = 0; s < len && !rc; s++, recomputed++) rc = step_forward(c, o, &A.tapes[s]);
     for (int s = len - 1; s >= 0 && !rc; s--) rc = adjoint_step(c, A.tapes[s], &o->solve);
   }
-  cudaEventRecord(c->ev1, c->stream);
-  cudaEventSynchronize(c->ev1);
+  cudaEventRecord(A.t1, c->stream);
+  cudaEventSynchronize(A.t1);
   float msa = 0;
-  cudaEventElapsedTime(&msa, c->ev0, c->ev1);
+  cudaEventElapsedTime(&msa, A.t0, A.t1);
   const size_t nc = control_size(c, o->control);
   double *dev = nullptr;
   if (!rc && cudaMalloc(&dev, sizeof(double) * nc) != cudaSuccess) rc = set_err(c, VFS_ERR_CUDA, "adjoint: allocation failed");
