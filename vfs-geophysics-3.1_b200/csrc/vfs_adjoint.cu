@@ -550,9 +550,8 @@ __global__ void k_dot_mask(long long N, int mode, Grid g, const uint8_t *__restr
   double s = 0;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
     if (mode == 1) {
-      const int i = (int)(p % g.mx);
-      const long long r = p / g.mx;
-      const int j = (int)(r % g.my), k = (int)(r / g.my);
+      int i, j, k;
+      dijk(g, p, i, j, k);
       if (k < 1 || k > g.mz - 2 || j < 1 || j > g.my - 2 || i < 1 || i > g.mx - 2) continue;
       if (nv[p - (long long)g.mx * g.my] + nv[p] != 0) continue;
     }
@@ -583,9 +582,8 @@ __global__ void k_axpy(long long n, double s, const double *x, double *y) {
 __global__ void k_add_kflux(Grid g, const uint8_t *__restrict__ nv, double s, double *y) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (k < 1 || k > g.mz - 2 || j < 1 || j > g.my - 2 || i < 1 || i > g.mx - 2) return;
   if (nv[p - (long long)g.mx * g.my] + nv[p] != 0) return;
   y[p] += s;
@@ -731,9 +729,8 @@ __global__ void k_vfi_lin(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV3
   double a1 = 0, a2 = 0;
   const long long sy = g.mx, sz = (long long)g.mx * g.my;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(p % g.mx);
-    const long long r = p / g.mx;
-    const int j = (int)(r % g.my), k = (int)(r / g.my);
+    int i, j, k;
+    dijk(g, p, i, j, k);
     if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) continue;
     const int v0 = nv[p];
     const double *bc[3] = {base.x, base.y, base.z};
@@ -1044,9 +1041,8 @@ __global__ void k_objective(Grid g, Metrics m, const uint8_t *__restrict__ nv, i
   double s = 0;
   const long long sz = (long long)g.mx * g.my;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(p % g.mx);
-    const long long r = p / g.mx;
-    const int j = (int)(r % g.my), k = (int)(r / g.my);
+    int i, j, k;
+    dijk(g, p, i, j, k);
     const bool interior = i >= 1 && i <= g.mx - 2 && j >= 1 && j <= g.my - 2 && k >= 1 && k <= g.mz - 2;
     if (!interior || nv[p] != 0) continue;
     if (obj == VFS_OBJ_KINETIC_ENERGY) {

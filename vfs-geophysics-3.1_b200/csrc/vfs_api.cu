@@ -143,6 +143,8 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
   if (device < 0 || device >= ndev) return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: bad device");
   if (cfg->IM < 4 || cfg->JM < 4 || cfg->KM < 4)
     return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: grid needs at least 4 nodes per direction");
+  if ((long long)(cfg->IM + 1) * (cfg->JM + 1) * (cfg->KM + 1) >= (1LL << 31))
+    return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: grids of 2^31 DA points or more are not supported");
   // Boundary codes handled on this path: 0 (unset), 1 no-slip wall, 2 moving lid (j+),
   // 4 outlet (k+ or j+), 5 inlet (k-), 7 periodic face, 10 free-slip, 12 moving wall,
   // 13/14 slip lid.

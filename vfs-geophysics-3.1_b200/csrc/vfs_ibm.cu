@@ -106,9 +106,8 @@ __device__ int cast_cell(const IbmSurface &S, const double p[3], int ic, int jc,
 __global__ void k_ibm_cast(Grid g, IbmSurface S, CV3 cent, uint8_t *nv, int reset, int *err) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
   int v = nv[p];
   if (reset && v < 5) v = 0;  // a new search starts from zero (ibm.c:233)
@@ -129,9 +128,8 @@ __global__ void k_ibm_cast(Grid g, IbmSurface S, CV3 cent, uint8_t *nv, int rese
 __global__ void k_ibm_near(Grid g, const uint8_t *__restrict__ nv, uint8_t *out) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   int v = nv[p];
   if (v != 4) {
     const int ip = i < g.mx - 1 ? i + 1 : i, im = i > 0 ? i - 1 : i;
@@ -150,9 +148,8 @@ __global__ void k_ibm_near(Grid g, const uint8_t *__restrict__ nv, uint8_t *out)
 __global__ void k_ibm_remap(Grid g, const uint8_t *__restrict__ in, uint8_t *nv, double *nvd) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   int v = in[p];
   if (i >= 1 && i <= g.mx - 2 && j >= 1 && j <= g.my - 2 && k >= 1 && k <= g.mz - 2) {
     if (v == 2) v = 1;
@@ -389,9 +386,8 @@ __global__ void k_ibm_nodes(Grid g, IbmGeom G, IbNode *out, int *err) {
 __global__ void k_ibm_collect(Grid g, const uint8_t *__restrict__ fl, long long *cells, int *count, int cap) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2 || fl[p] != 2) return;
   const int slot = atomicAdd(count, 1);
   if (slot < cap) cells[slot] = p;
@@ -663,9 +659,8 @@ __global__ void k_ibm_scatter(Grid g, const IbNode *__restrict__ nodes, int n, c
 __global__ void k_ib_faces(Grid g, Metrics m, CV3 u, const uint8_t *__restrict__ nv, V3 uc) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
   const long long sy = g.mx, sz = (long long)g.mx * g.my;
   const bool self = nv[p] == 1;
@@ -719,9 +714,8 @@ __global__ void k_vflux_ibm(Grid g, Metrics m, const uint8_t *__restrict__ nv, V
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long sy = g.mx, sz = (long long)g.mx * g.my;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
-    const int i = (int)(p % g.mx);
-    const long long r = p / g.mx;
-    const int j = (int)(r % g.my), k = (int)(r / g.my);
+    int i, j, k;
+    dijk(g, p, i, j, k);
     if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) continue;
     const int v0 = nv[p];
     double *comp[3] = {uc.x, uc.y, uc.z};

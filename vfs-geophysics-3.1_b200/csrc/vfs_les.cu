@@ -135,9 +135,8 @@ __global__ void k_les_image(Grid g, CV3 u, CV3 csi, CV3 eta, CV3 zet, const doub
                             const uint8_t *__restrict__ nv, LesPrep o) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const int a = wrapi(g, i), b = wrapj(g, j), c = wrapk(g, k);
   const long long q = lidx(g, a, b, c);
   double ss[6] = {0, 0, 0, 0, 0, 0}, uf[3] = {0, 0, 0};
@@ -429,9 +428,8 @@ __global__ void k_les_cs(Grid g, const double *__restrict__ wgt, const uint8_t *
                          const double *__restrict__ LM, const double *__restrict__ MM, double max_cs, double *cs) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const int a = wrapi(g, i), b = wrapj(g, j), c = wrapk(g, k);
   cs[p] = les_interior(g, a, b, c) ? cs_cell(g, wgt, nv, LM, MM, a, b, c, max_cs) : 0.0;
 }
@@ -441,9 +439,8 @@ __global__ void k_les_refilter(Grid g, const double *__restrict__ wgt, const uin
                                const double *__restrict__ cs_tmp, double *cs) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (!les_interior(g, i, j, k) || nv[p] != 0) { cs[p] = cs_tmp[p]; return; }
   double w[27], v[27];
   long long src[27];
@@ -476,9 +473,8 @@ __global__ void k_les_nut(Grid g, CV3 u, CV3 csi, CV3 eta, CV3 zet, const double
                           const uint8_t *__restrict__ nv, const double *__restrict__ cs, double *nut) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long r = p / g.mx;
-  const int j = (int)(r % g.my), k = (int)(r / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const int a = wrapi(g, i), b = wrapj(g, j), c = wrapk(g, k);
   if (les_interior(g, a, b, c)) nut[p] = nut_cell(g, u, csi, eta, zet, aj, nv, cs, a, b, c);
   else if (a != i || b != j || c != k) nut[p] = nut[lidx(g, a, b, c)];

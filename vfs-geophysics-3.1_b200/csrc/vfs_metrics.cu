@@ -26,10 +26,8 @@ __device__ __forceinline__ long long nidx(const Nodes &n, int i, int j, int k) {
 __global__ void k_centre_metrics(Grid g, Nodes n, V3 cent, V3 csi, V3 eta, V3 zet, double *aj) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
   const long long a000 = nidx(n, i, j, k), a010 = nidx(n, i, j - 1, k), a100 = nidx(n, i, j, k - 1),
                   a110 = nidx(n, i, j - 1, k - 1), b000 = nidx(n, i - 1, j, k),
@@ -71,10 +69,8 @@ __global__ void k_centre_metrics(Grid g, Nodes n, V3 cent, V3 csi, V3 eta, V3 ze
 __global__ void k_ghost_plane(Grid g, int d, V3 csi, V3 eta, V3 zet, double *aj) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   long long s;
   if (d == 0) {
     if (i == 0) s = p + 1; else if (i == g.mx - 1) s = p - 1; else return;
@@ -96,10 +92,8 @@ __global__ void k_face_metrics(Grid g, CV3 csi, CV3 eta, CV3 zet, const double *
                                V3 keta, V3 kzet, double *kaj) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const int mx = g.mx, my = g.my, mz = g.mz;
   const bool ii = i >= 1 && i <= mx - 2, jj = j >= 1 && j <= my - 2, kk = k >= 1 && k <= mz - 2;
   // i faces: i = 0..mx-2, interior j and k (metrics.c:488-585)

@@ -70,10 +70,8 @@ __global__ void k_contra2cart_interior(Grid g, CV3 uc, CV3 csi, CV3 eta, CV3 zet
                                        const uint8_t *__restrict__ nv, V3 ucat) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
   if (nv[p] != 0) return;
   const double m00 = csi.x[p], m01 = csi.y[p], m02 = csi.z[p];
@@ -227,10 +225,8 @@ __global__ void k_contra2cart_bc(Grid g, Metrics m, const uint8_t *__restrict__ 
                                  CV3 uo, V3 out, uint8_t *flag) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   contra2cart_bc_point(g, m, nv, lu, uo, out, flag, p, i, j, k);
 }
 
@@ -640,10 +636,8 @@ __global__ void __launch_bounds__(VFS_FF_THREADS, VFS_FF_MINB) k_face_flux(Grid 
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i == mx - 1 || j == my - 1 || k == mz - 1) return;
   double d[3], v[3];
   if (j != 0 && k != 0) {
@@ -739,10 +733,8 @@ __global__ void k_fp(Grid g, FluxIn f1, FluxIn f2, FluxIn f3, const uint8_t *__r
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
   GlobalFaces F;
   F.g = &g; F.f1 = f1; F.f2 = f2; F.f3 = f3;
@@ -825,10 +817,8 @@ __global__ void k_rhs(Grid g, Metrics m, const uint8_t *__restrict__ nv, const d
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const bool ghost = i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == mz - 1;
   const long long sy = mx, sz = (long long)mx * my;
   GlobalFp F;
@@ -1081,10 +1071,8 @@ __global__ void k_pressure_gradient(Grid g, Metrics m, const uint8_t *__restrict
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) {
     dp.x[p] = 0; dp.y[p] = 0; dp.z[p] = 0;  // VecSet(dP, 0) outside the loop
     return;
@@ -1190,10 +1178,8 @@ __global__ void k_kflux_parts(Grid g, const double *__restrict__ uz, const uint8
   double s = 0;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
-    int i = (int)(p % g.mx);
-    long long q = p / g.mx;
-    int j = (int)(q % g.my);
-    int k = (int)(q / g.my);
+    int i, j, k;
+    dijk(g, p, i, j, k);
     if (k < 1 || k > g.mz - 2 || j < 1 || j > g.my - 2 || i < 1 || i > g.mx - 2) continue;
     const long long sz = (long long)g.mx * g.my;
     if (nv[p - sz] + nv[p] == 0) s += uz[p];
@@ -1230,10 +1216,8 @@ __global__ void k_area_parts(Grid g, CV3 zet, const uint8_t *__restrict__ nv, do
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long sz = (long long)g.mx * g.my;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
-    int i = (int)(p % g.mx);
-    long long q = p / g.mx;
-    int j = (int)(q % g.my);
-    int k = (int)(q / g.my);
+    int i, j, k;
+    dijk(g, p, i, j, k);
     if (j < 1 || j > g.my - 2 || i < 1 || i > g.mx - 2) continue;
     const double area = sqrt(zet.x[p] * zet.x[p] + zet.y[p] * zet.y[p] + zet.z[p] * zet.z[p]);
     if (k >= 1 && k <= g.mz - 2 && nv[p - sz] + nv[p] == 0) a += area;
@@ -1269,10 +1253,8 @@ __global__ void k_ib_bc_faces(Grid g, V3 uc) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const long long sy = mx, sz = (long long)mx * my;
   const int *bc = g.bc;
   // the reference loops over all points and writes the plane values named below; each
@@ -1288,10 +1270,8 @@ __global__ void k_periodic_normal(Grid g, V3 uc) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const long long sy = mx, sz = (long long)mx * my;
   if (g.iper && i == 0) uc.x[p] = uc.x[p + (mx - 2)];
   if (g.iper && i == mx - 1) uc.x[p] = uc.x[p - (mx - 2)];
@@ -1485,10 +1465,8 @@ __global__ void k_wall_flux(Grid g, V3 uc) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const int *bc = g.bc;
   bool ik = (k >= 1 && k <= mz - 2);
   if (ik && j >= 1 && j <= my - 2) {
@@ -1504,10 +1482,8 @@ __global__ void k_zero_edges(Grid g, V3 u) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   int bi = (i == 0 || i == mx - 1), bj = (j == 0 || j == my - 1), bk = (k == 0 || k == mz - 1);
   if (bi + bj + bk >= 2) { u.x[p] = 0; u.y[p] = 0; u.z[p] = 0; }
 }
@@ -1807,9 +1783,8 @@ __global__ void k_tan_face(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV
                            FaceBank out) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long q = p / g.mx;
-  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i == g.mx - 1 || j == g.my - 1 || k == g.mz - 1) return;
   const bool on[3] = {j != 0 && k != 0, i != 0 && k != 0, i != 0 && j != 0};
   for (int D = 0; D < 3; D++) {
@@ -1824,9 +1799,8 @@ __global__ void k_adj_face(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV
                            V3 lu) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long q = p / g.mx;
-  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i == g.mx - 1 || j == g.my - 1 || k == g.mz - 1) return;
   const bool on[3] = {j != 0 && k != 0, i != 0 && k != 0, i != 0 && j != 0};
   for (int D = 0; D < 3; D++) {
@@ -1847,9 +1821,8 @@ __global__ void k_adj_fp(Grid g, const uint8_t *__restrict__ nv, const double *_
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  const int i = (int)(p % mx);
-  const long long q = p / mx;
-  const int j = (int)(q % my), k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
   const double l[3] = {lfx[p], lfy[p], lfz[p]};
   if (l[0] == 0 && l[1] == 0 && l[2] == 0) return;
@@ -1887,9 +1860,8 @@ __global__ void k_adj_rhs(Grid g, Metrics m, const uint8_t *__restrict__ nv, dou
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  const int i = (int)(p % mx);
-  const long long q = p / mx;
-  const int j = (int)(q % my), k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const double l0 = lU.x[p], l1 = lU.y[p], l2 = lU.z[p];
   lpu.x[p] += l0; lpu.y[p] += l1; lpu.z[p] += l2;
   ldp.x[p] -= a * l0; ldp.y[p] -= a * l1; ldp.z[p] -= a * l2;
@@ -1927,9 +1899,8 @@ __global__ void k_adj_rhs(Grid g, Metrics m, const uint8_t *__restrict__ nv, dou
 __global__ void k_periodic_copy_adj(Grid g, double *a, double *b, double *c) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  const int i = (int)(p % g.mx);
-  const long long q = p / g.mx;
-  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const bool gi = g.iper && (i == 0 || i == g.mx - 1), gj = g.jper && (j == 0 || j == g.my - 1);
   const bool gk = g.kper && (k == 0 || k == g.mz - 1);
   if (!(gi || gj || gk)) return;

@@ -122,10 +122,8 @@ __global__ void k_poisson_coef(Grid g, Metrics m, const uint8_t *__restrict__ nv
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const long long N = g.N;
   const bool interior = !(i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == mz - 1);
   if (!interior || nv[p] != 0) {
@@ -239,9 +237,8 @@ __global__ void k_apply_t(Grid g, int ns, const double *__restrict__ coef, const
   if (p >= g.N) return;
   const double xp = x[p];
   if (xp == 0.0) return;
-  const int i = (int)(p % g.mx);
-  const long long q = p / g.mx;
-  const int j = (int)(q % g.my), k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   for (int t = 0; t < ns; t++) {
     const double c = coef[t * g.N + p];
     if (c != 0.0) atomicAdd(y + nb_index(g, i, j, k, t), c * xp);
@@ -629,10 +626,8 @@ __global__ void k_poisson_rhs(Grid g, CV3 uc, const uint8_t *__restrict__ fluid,
   if (p >= g.N) return;
   if (!fluid[p]) { b[p] = 0; return; }
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   const long long sy = mx, sz = (long long)mx * my;
   const double coeff = 1.0;  // time_coeff() (poisson.c:17) without levelset/RANS
   double val = 0;
@@ -694,10 +689,8 @@ static int sum_fluid(Ctx *c, const double *a, double *out) {
 __global__ void k_volume_flux_blocked(Grid g, const uint8_t *__restrict__ nv, V3 uc) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
   const long long sy = g.mx, sz = (long long)g.mx * g.my;
   const bool f0 = nv[p] == 0;
@@ -743,8 +736,8 @@ int poisson_rhs(Ctx *c) {
 }
 
 // ------------------------------------------------------------------ FGMRES
-// Right-preconditioned flexible GMRES (Saad 1993) in FP64 with classical Gram-Schmidt
-// and one re-orthogonalisation pass.  Solves A phi = b for the fluid unknowns, starting
+// Right-preconditioned flexible GMRES (Saad 1993) in FP64 with classical Gram-Schmidt,
+// re-orthogonalised where the first pass loses more than half the norm.  Solves A phi = b for the fluid unknowns, starting
 // from phi = 0 as HYPRE does with a zero initial vector (Petsc_to_Hypre_Vector of a fresh
 // Phi2), then removes the mean (Remove_Nullspace) and fills the grid Phi like
 // Convert_Phi2_Phi (poisson.c:92): non-fluid interior cells 0, periodic ghosts from
@@ -813,29 +806,43 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       const int nv = j + 1;
       double *Vj = P.V + (long long)j * P.ldv, *Zj = P.Z + (long long)j * P.ldv;
       if ((rc = mg_precondition(c, Vj, Zj, o))) return rc;
-      // classical Gram-Schmidt with one re-orthogonalisation, three passes over V:
-      // (1) w = A z_j and h = V^T w; (2) w -= V h and h2 = V^T w; (3) v_{j+1} = (w - V h2)/|.|
+      // classical Gram-Schmidt, re-orthogonalised when the first pass cancels more than half
+      // of w: (1) w = A z_j and h = V^T w; then either (2) v_{j+1} = (w - V h)/|.| or
+      // (2') w -= V h and h2 = V^T w, (3') v_{j+1} = (w - V h2)/|.|
       if ((rc = apply_dots(c, Zj, P.w, P.V, nv, h.data()))) return rc;
       upload_h(c, h.data(), nv, P.hdev);
-      if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h2.data()))) return rc;
-      double ww = h2[nv], proj = 0;
-      for (int t = 0; t < nv; t++) proj += h2[t] * h2[t];
-      double hn2 = ww - proj;  // |w - V h2|^2 for orthonormal V
-      upload_h(c, h2.data(), nv, P.hdev);
-      for (int t = 0; t < nv; t++) H[t * m + j] = h[t] + h2[t];
-      double hn;
+      double proj0 = 0;
+      for (int t = 0; t < nv; t++) proj0 += h[t] * h[t];
+      const double hn2_0 = h[nv] - proj0;  // |w - V h|^2 for orthonormal V
       double *Vn = P.V + (long long)(j + 1) * P.ldv;
-      if (hn2 > 1e-4 * ww) {
-        hn = sqrt(hn2);
+      double hn;
+      if (hn2_0 > 0.5 * h[nv]) {
+        // w kept more than half its norm: one Gram-Schmidt pass is enough (the
+        // Daniel-Gragg-Kaufman-Stewart criterion), v_{j+1} = (w - V h)/|.|
+        for (int t = 0; t < nv; t++) H[t * m + j] = h[t];
+        hn = sqrt(hn2_0);
         if ((rc = update_scale(c, P.V, nv, P.hdev, P.w, 1.0 / hn, Vn))) return rc;
       } else {
-        // w is nearly in span(V): form w - V h2 explicitly and take its norm
-        std::vector<double> h3(nv + 1);
-        if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h3.data()))) return rc;
-        hn = sqrt(std::max(h3[nv], 0.0));
-        if (hn > 0) {
-          k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, 1.0 / hn, Vn);
-          if ((rc = check_launch(c, "k_scale_copy"))) return rc;
+        // re-orthogonalise: w -= V h and h2 = V^T w, then v_{j+1} = (w - V h2)/|.|
+        if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h2.data()))) return rc;
+        const double ww = h2[nv];
+        double proj = 0;
+        for (int t = 0; t < nv; t++) proj += h2[t] * h2[t];
+        const double hn2 = ww - proj;  // |w - V h2|^2 for orthonormal V
+        upload_h(c, h2.data(), nv, P.hdev);
+        for (int t = 0; t < nv; t++) H[t * m + j] = h[t] + h2[t];
+        if (hn2 > 1e-4 * ww) {
+          hn = sqrt(hn2);
+          if ((rc = update_scale(c, P.V, nv, P.hdev, P.w, 1.0 / hn, Vn))) return rc;
+        } else {
+          // w is nearly in span(V): form w - V h2 explicitly and take its norm
+          std::vector<double> h3(nv + 1);
+          if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h3.data()))) return rc;
+          hn = sqrt(std::max(h3[nv], 0.0));
+          if (hn > 0) {
+            k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, 1.0 / hn, Vn);
+            if ((rc = check_launch(c, "k_scale_copy"))) return rc;
+          }
         }
       }
       H[(j + 1) * m + j] = hn;
@@ -900,10 +907,8 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
 __global__ void k_update_pressure(Grid g, const uint8_t *__restrict__ nv, const double *__restrict__ phi, double *P) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) return;
   if (nv[p] == 0) P[p] += phi[p];
   if (nv[p] >= 2) P[p] = 0;
@@ -937,10 +942,8 @@ __global__ void k_projection(Grid g, Metrics m, const uint8_t *__restrict__ nv, 
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  int i = (int)(p % mx);
-  long long q = p / mx;
-  int j = (int)(q % my);
-  int k = (int)(q / my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
   const long long sx = 1, sy = mx, sz = (long long)mx * my;
   const double coeff = 1.0, r1 = 1.0, r2 = 1.0, r3 = 1.0;
@@ -994,10 +997,8 @@ __global__ void k_projection(Grid g, Metrics m, const uint8_t *__restrict__ nv, 
 __global__ void k_periodic_copy_comp(Grid g, V3 u) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
-  int i = (int)(p % g.mx);
-  long long q = p / g.mx;
-  int j = (int)(q % g.my);
-  int k = (int)(q / g.my);
+  int i, j, k;
+  dijk(g, p, i, j, k);
   int ii = wrapi(g, i), jj = wrapj(g, j), kk = wrapk(g, k);
   if (ii == i && jj == j && kk == k) return;
   long long s = lidx(g, ii, jj, kk);
@@ -1028,10 +1029,8 @@ __global__ void k_divergence(Grid g, CV3 uc, const double *__restrict__ aj, cons
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long sy = g.mx, sz = (long long)g.mx * g.my;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
-    int i = (int)(p % g.mx);
-    long long q = p / g.mx;
-    int j = (int)(q % g.my);
-    int k = (int)(q / g.my);
+    int i, j, k;
+    dijk(g, p, i, j, k);
     if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) continue;
     double d = fabs((uc.x[p] - uc.x[p - 1] + uc.y[p] - uc.y[p - sy] + uc.z[p] - uc.z[p - sz]) * aj[p]);
     if (nv[p] + nv[p + sz] + nv[p - sz] + nv[p + sy] + nv[p - sy] + nv[p + 1] + nv[p - 1] > 0) d = 0.;
