@@ -524,7 +524,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD if not args.size else "size override %s" % args.size,
                        "cells": ncell, "parallelism": "replicas" if world > 1 else "single-gpu",
-                       "precision": "mixed: FP32 multigrid V-cycle (%d levels, zebra y-line Gauss-Seidel 2+2 "
+                       "precision": "mixed: FP32 multigrid V-cycle (%d levels, zebra y-line Gauss-Seidel 3+3 "
                                     "sweeps, trilinear prolongation) in FP64 FGMRES(30)" % mg_levels(nx, ny, nz),
                        "l2": "inputs larger than L2 (every field is a %d MB array)" % (npts * 8 // 2 ** 20)},
             "fp64_ms_per_step": round(ms_fp64, 3),

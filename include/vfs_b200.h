@@ -100,7 +100,7 @@ typedef struct {
   int max_iter;      /* outer iteration cap (default 200) */
   int levels;        /* multigrid levels including the finest (default 0: every level
                         the grid coarsens to) */
-  int pre_smooth, post_smooth; /* zebra line Gauss-Seidel sweeps per level (default 2, 2) */
+  int pre_smooth, post_smooth; /* zebra line Gauss-Seidel sweeps per level (default 3, 3) */
   int coarse_iters;  /* sweeps on the coarsest level (default 4) */
   int reserved[5];
   double rtol;       /* relative residual target (default 1e-10) */

@@ -745,7 +745,7 @@ int poisson_rhs(Ctx *c) {
 int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   vfs_solve_opts o;
   memset(&o, 0, sizeof(o));
-  o.precision = 0; o.restart = 30; o.max_iter = 200; o.levels = 0; o.pre_smooth = 2; o.post_smooth = 2;
+  o.precision = 0; o.restart = 30; o.max_iter = 200; o.levels = 0; o.pre_smooth = 3; o.post_smooth = 3;
   o.coarse_iters = 4; o.rtol = 1e-10; o.atol = 0.0;
   if (oin) {
     o.precision = oin->precision;

@@ -352,7 +352,7 @@ class Context:
         return y
 
     def poisson_solve(self, precision=0, rtol=1e-10, restart=30, max_iter=200, levels=0,
-                      pre_smooth=2, post_smooth=2, coarse_iters=4, allow_unconverged=False):
+                      pre_smooth=3, post_smooth=3, coarse_iters=4, allow_unconverged=False):
         o = SolveOpts(precision=precision, restart=restart, max_iter=max_iter, levels=levels,
                       pre_smooth=pre_smooth, post_smooth=post_smooth, coarse_iters=coarse_iters,
                       rtol=rtol)
@@ -375,7 +375,7 @@ class Context:
     def step(self, precision=0, rtol=1e-10, **kw):  # Flow_Solver, solvers.c:562 (implicit=0)
         o = SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
                       max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 0),
-                      pre_smooth=kw.get("pre_smooth", 2), post_smooth=kw.get("post_smooth", 2),
+                      pre_smooth=kw.get("pre_smooth", 3), post_smooth=kw.get("post_smooth", 3),
                       coarse_iters=kw.get("coarse_iters", 4))
         st = StepStats()
         self._check(self.lib.vfs_step(self.h, ctypes.byref(o), ctypes.byref(st)))
@@ -443,7 +443,7 @@ class Context:
 def _solve_opts(precision=0, rtol=1e-10, **kw):
     return SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
                      max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 0),
-                     pre_smooth=kw.get("pre_smooth", 2), post_smooth=kw.get("post_smooth", 2),
+                     pre_smooth=kw.get("pre_smooth", 3), post_smooth=kw.get("post_smooth", 3),
                      coarse_iters=kw.get("coarse_iters", 4))
 
 
