@@ -765,8 +765,16 @@ __global__ void __launch_bounds__(kFpTi * kFpTj) k_fp_march(Grid g, FluxIn f1, F
   F.gf.g = &g; F.gf.f1 = f1; F.gf.f2 = f2; F.gf.f3 = f3;
   F.gf.i = i; F.gf.j = j;
   const long long col = (long long)j * mx + i;  // (i, j) at k = 0
+  // k-face kk of this column; on a non-periodic k the faces below 0 do not exist (cells 1
+  // and 2 read faces 0 and above only, fp_offsets), so they are left at zero
   auto kface = [&](int kk, int slot) {
-    const long long q = col + (long long)face_image(kk, mz, g.kper) * sz;
+    const int f = face_image(kk, mz, g.kper);
+    if (f < 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) { F.wd[slot][c] = 0.0; F.wv[slot][c] = 0.0; }
+      return;
+    }
+    const long long q = col + (long long)f * sz;
 #pragma unroll
     for (int c = 0; c < 3; c++) { F.wd[slot][c] = f3.div[c][q]; F.wv[slot][c] = f3.visc[c][q]; }
   };
