@@ -580,67 +580,6 @@ __global__ void k_zprolong(ZL F, ZL C, const uint8_t *__restrict__ actF, const u
   zprolong_cell<T>(F, C, actF, actC, x, xc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
-// The same prolongation with one thread per coarse cell: its 3x3x3 coarse neighbourhood is
-// read once into registers and its eight fine children are updated from it (each child's
-// arithmetic is zprolong_cell's, in its order).  The fine level is the coarse one doubled
-// in every direction.
-template <typename T>
-__global__ void k_zprolong_coarse(ZL F, ZL C, const uint8_t *__restrict__ actF, const uint8_t *__restrict__ actC,
-                                  T *__restrict__ x, const T *__restrict__ xc) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)C.nx * C.ny * C.nz) return;
-  int I, J, K;
-  zcell(C, t, I, J, K);
-  // coarse neighbour index along each direction for offset -1, 0, +1 (-1 when missing)
-  int ni[3], nj[3], nk[3];
-  const int base[3] = {I, J, K}, ext[3] = {C.nx, C.ny, C.nz}, per[3] = {C.ip, C.jp, C.kp};
-  int *nn[3] = {ni, nj, nk};
-  for (int d = 0; d < 3; d++)
-    for (int o = 0; o < 3; o++) {
-      int v = base[d] + o - 1;
-      if (v < 0 || v >= ext[d]) v = per[d] ? (v + ext[d]) % ext[d] : -1;
-      nn[d][o] = v;
-    }
-  T val[3][3][3];
-  bool ok[3][3][3];
-#pragma unroll
-  for (int c = 0; c < 3; c++)
-#pragma unroll
-    for (int b = 0; b < 3; b++)
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        const bool in = ni[a] >= 0 && nj[b] >= 0 && nk[c] >= 0;
-        long long q = in ? zidx(C, ni[a], nj[b], nk[c]) : 0;
-        ok[c][b][a] = in && actC[q];
-        val[c][b][a] = ok[c][b][a] ? xc[q] : T(0);
-      }
-  const T own = xc[zidx(C, I, J, K)];  // read whatever its flag, as zprolong_cell does
-#pragma unroll
-  for (int fc = 0; fc < 2; fc++)
-#pragma unroll
-    for (int fb = 0; fb < 2; fb++)
-#pragma unroll
-      for (int fa = 0; fa < 2; fa++) {
-        const int i = 2 * I + fa, j = 2 * J + fb, k = 2 * K + fc;
-        const long long q = zidx(F, i, j, k);
-        if (!actF[q]) continue;
-        // the other coarse cell nearest along each direction: offset +1 for an odd child
-        const int oa = fa ? 2 : 0, ob = fb ? 2 : 0, oc = fc ? 2 : 0;
-        T wown = T(27) / T(64);
-        T sum = 0;
-        for (int c = 0; c < 2; c++)
-          for (int bb = 0; bb < 2; bb++)
-            for (int a = 0; a < 2; a++) {
-              if (a + bb + c == 0) continue;
-              const T w = (a ? T(1) : T(3)) * (bb ? T(1) : T(3)) * (c ? T(1) : T(3)) / T(64);
-              const int xa = a ? oa : 1, xb = bb ? ob : 1, xcc = c ? oc : 1;
-              if (!ok[xcc][xb][xa]) { wown += w; continue; }
-              sum += w * val[xcc][xb][xa];
-            }
-        x[q] += sum + wown * own;
-      }
-}
-
 // act[q] = 1 where the level's diagonal is non-zero (an active unknown).
 __global__ void k_mg_active(long long n, const double *__restrict__ op, uint8_t *__restrict__ act) {
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -925,12 +864,7 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   k_zrestrict<T><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
   if ((rc = check_launch(c, "k_zrestrict"))) return rc;
   if ((rc = mg_vcycle<T>(c, l + 1, nl, o))) return rc;
-  if (F.z.nx == 2 * C.z.nx && F.z.ny == 2 * C.z.ny && F.z.nz == 2 * C.z.nz) {
-    const long long ncc = (long long)C.z.nx * C.z.ny * C.z.nz;
-    k_zprolong_coarse<T><<<nblocks(ncc, 128), 128, 0, c->stream>>>(F.z, C.z, F.act, C.act, f.x, cc.x);
-  } else {
-    k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, F.act, C.act, f.x, cc.x);
-  }
+  k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, F.act, C.act, f.x, cc.x);
   if ((rc = check_launch(c, "k_zprolong"))) return rc;
   return mg_smooth<T>(c, l, o.post_smooth, false);
 }

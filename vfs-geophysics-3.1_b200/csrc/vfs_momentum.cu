@@ -728,77 +728,21 @@ struct GlobalFaces {
   }
 };
 
-// k_fp marching along k: a 32 x 8 thread tile in (i, j) (the j-face rows a tile reads are
-// shared in L1 by its warps), each thread walking KFP cells up its column with the k-face
-// fluxes of planes k-2 .. k+1 in registers, so every k-face flux is loaded once per column
-// instead of four times.  Each cell's Fp is fp_cell's, term for term.
-constexpr int kFpTi = 32, kFpTj = 8, kFpK = 8;
-
-struct MarchFaces {
-  GlobalFaces gf;
-  double wd[4][3], wv[4][3];  // k-faces k-2 .. k+1: div and visc of the three components
-  __device__ __forceinline__ static double sel(const double (&w)[4][3], int c, int off) {
-    switch (off) {
-      case -2: return w[0][c];
-      case -1: return w[1][c];
-      case 0: return w[2][c];
-      default: return w[3][c];
-    }
-  }
-  __device__ __forceinline__ double d(int dir, int c, int off) const {
-    return dir == 2 ? sel(wd, c, off) : gf.d(dir, c, off);
-  }
-  __device__ __forceinline__ double v(int dir, int c, int off) const {
-    return dir == 2 ? sel(wv, c, off) : gf.v(dir, c, off);
-  }
-};
-
-__global__ void __launch_bounds__(kFpTi * kFpTj) k_fp_march(Grid g, FluxIn f1, FluxIn f2, FluxIn f3,
-                                                             const uint8_t *__restrict__ nv, double *fpx,
-                                                             double *fpy, double *fpz) {
+__global__ void k_fp(Grid g, FluxIn f1, FluxIn f2, FluxIn f3, const uint8_t *__restrict__ nv,
+                     double *fpx, double *fpy, double *fpz) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
-  const int i = 1 + blockIdx.x * kFpTi + threadIdx.x, j = 1 + blockIdx.y * kFpTj + threadIdx.y;
-  const int k0 = 1 + blockIdx.z * kFpK, k1 = min(mz - 1, k0 + kFpK);
-  if (i > mx - 2 || j > my - 2 || k0 > mz - 2) return;
-  const long long sz = (long long)mx * my;
-  MarchFaces F;
-  F.gf.g = &g; F.gf.f1 = f1; F.gf.f2 = f2; F.gf.f3 = f3;
-  F.gf.i = i; F.gf.j = j;
-  const long long col = (long long)j * mx + i;  // (i, j) at k = 0
-  // k-face kk of this column; on a non-periodic k the faces below 0 do not exist (cells 1
-  // and 2 read faces 0 and above only, fp_offsets), so they are left at zero
-  auto kface = [&](int kk, int slot) {
-    const int f = face_image(kk, mz, g.kper);
-    if (f < 0) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) { F.wd[slot][c] = 0.0; F.wv[slot][c] = 0.0; }
-      return;
-    }
-    const long long q = col + (long long)f * sz;
-#pragma unroll
-    for (int c = 0; c < 3; c++) { F.wd[slot][c] = f3.div[c][q]; F.wv[slot][c] = f3.visc[c][q]; }
-  };
-  kface(k0 - 2, 0); kface(k0 - 1, 1); kface(k0, 2);
-  for (int k = k0; k < k1; k++) {
-    kface(k + 1, 3);
-    const long long p = col + (long long)k * sz;
-    F.gf.k = k;
-    F.gf.rowi = p - i; F.gf.rowj = p - (long long)j * mx; F.gf.rowk = col;
-    double fpv[3];
-    fp_cell(g, nv, p, i, j, k, F, fpv);
-    fpx[p] = fpv[0]; fpy[p] = fpv[1]; fpz[p] = fpv[2];
-#pragma unroll
-    for (int s = 0; s < 3; s++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) { F.wd[s][c] = F.wd[s + 1][c]; F.wv[s][c] = F.wv[s + 1][c]; }
-  }
-}
-
-static void launch_fp_march(Ctx *c, const FluxIn &f1, const FluxIn &f2, const FluxIn &f3) {
-  const Grid &g = c->g;
-  dim3 block(kFpTi, kFpTj), grid((g.mx - 2 + kFpTi - 1) / kFpTi, (g.my - 2 + kFpTj - 1) / kFpTj,
-                                 (g.mz - 2 + kFpK - 1) / kFpK);
-  k_fp_march<<<grid, block, 0, c->stream>>>(g, f1, f2, f3, c->nv, c->fp[0], c->fp[1], c->fp[2]);
+  int i, j, k;
+  dijk(g, p, i, j, k);
+  if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
+  GlobalFaces F;
+  F.g = &g; F.f1 = f1; F.f2 = f2; F.f3 = f3;
+  F.rowi = p - i; F.rowj = p - (long long)j * mx; F.rowk = p - (long long)k * mx * my;
+  F.i = i; F.j = j; F.k = k;
+  double fpv[3];
+  fp_cell(g, nv, p, i, j, k, F, fpv);
+  fpx[p] = fpv[0]; fpy[p] = fpv[1]; fpz[p] = fpv[2];
 }
 
 // Contravariant projection of Fp onto the faces, scale, masks and the boundary zeroing
@@ -1061,7 +1005,8 @@ int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
                                                         c->f[VFS_NU_T][0], flux_out(c, 0), flux_out(c, 1),
                                                         flux_out(c, 2));
   if ((rc = check_launch(c, "k_face_flux"))) return rc;
-  launch_fp_march(c, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2));
+  k_fp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2), c->nv,
+                                                   c->fp[0], c->fp[1], c->fp[2]);
   if ((rc = check_launch(c, "k_fp"))) return rc;
   V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
   k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], scale,
@@ -1106,7 +1051,8 @@ void launch_face_flux(Ctx *c) {
                                                            flux_out(c, 0), flux_out(c, 1), flux_out(c, 2));
 }
 void launch_fp(Ctx *c) {
-  launch_fp_march(c, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2));
+  k_fp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2), c->nv,
+                                                   c->fp[0], c->fp[1], c->fp[2]);
 }
 void launch_rhs(Ctx *c) {
   V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
@@ -1990,7 +1936,7 @@ int ff2_stage_tangent(Ctx *c, const double *const uc[3], const double *const uk[
   FluxIn f[3];
   for (int d = 0; d < 3; d++)
     for (int q = 0; q < 3; q++) { f[d].div[q] = tf[d][q]; f[d].visc[q] = tf[d][3 + q]; }
-  launch_fp_march(c, f[0], f[1], f[2]);
+  k_fp<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, f[0], f[1], f[2], c->nv, c->fp[0], c->fp[1], c->fp[2]);
   if ((rc = check_launch(c, "k_fp"))) return rc;
   k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], 1.0, field3(c, VFS_RHS),
                                                  1, a, cv(ddp), cv(dpu), dU);
