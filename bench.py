@@ -447,6 +447,24 @@ def main():
     its = float(np.mean([s.poisson.iterations for s in stats]))
     its64 = float(np.mean([s.poisson.iterations for s in stats64]))
 
+    # mixed against FP64 from one state: L2 and Linf of P and Ucat (both solves to rtol 1e-10)
+    keep = {f: ctx.get_field(f) for f in (vfs.UCONT, vfs.UCAT, vfs.P, vfs.UCAT_O, vfs.UCONT_O)}
+    ti = ctx.get_scalar(vfs.S_TI)
+    outs = {}
+    for prec in (0, 1):
+        for f, v in keep.items():
+            ctx.set_field(f, v)
+        ctx.set_scalar(vfs.S_TI, ti)
+        st = ctx.step(precision=prec, rtol=1e-10)
+        outs[prec] = (ctx.get_field(vfs.P), ctx.get_field(vfs.UCAT), st.max_div)
+
+    def rel(a, b):
+        return {"l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                "linf": float(np.abs(a - b).max() / np.abs(b).max())}
+    mixed_err = {"p": rel(outs[0][0], outs[1][0]), "u": rel(outs[0][1], outs[1][1]),
+                 "max_div": {"mixed": outs[0][2], "fp64": outs[1][2]},
+                 "note": "one step from the same state, mixed precision against the all-FP64 form"}
+
     # e2e: flow state from pinned host memory each step, result back to the host
     shp3 = ctx.shape + (3,)
     h_uc = torch.empty(shp3, dtype=torch.float64, pin_memory=True).numpy()
@@ -531,6 +549,7 @@ def main():
             "mixed_speedup_vs_fp64": round(ms_fp64 / ms_mixed, 3),
             "max_div": {"mixed": maxdiv, "fp64": maxdiv64},
             "poisson_iterations": {"mixed": its, "fp64": its64},
+            "mixed_vs_fp64": mixed_err,
             "adjoint_forward_ratio": adj.get("ratio") if adj else None,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms/step", "h2d_bytes_per_step": io_bytes,
                     "d2h_bytes_per_step": io_bytes},
