@@ -353,6 +353,15 @@ __global__ void __launch_bounds__(64) k_zline(ZL L, const Q4<T> *__restrict__ cp
 #ifndef VFS_ZTILE_W64
 #define VFS_ZTILE_W64 16   // columns per tile, FP64
 #endif
+#ifndef VFS_ZTILE_U32
+#define VFS_ZTILE_U32 2    // rows each thread loads before using them, FP32
+#endif
+#ifndef VFS_ZTILE_MINB
+#define VFS_ZTILE_MINB 5   // resident blocks per SM the register allocation must allow, FP32
+#endif
+#ifndef VFS_ZTILE_MINB64
+#define VFS_ZTILE_MINB64 1  // the same, FP64
+#endif
 constexpr int kTileThreads = VFS_ZTILE_THREADS;
 
 template <typename T>
@@ -375,7 +384,7 @@ __device__ __forceinline__ void scan_compose_down(T &A, T &B, int lane) {
 }
 
 template <typename T, int W>
-__global__ void __launch_bounds__(kTileThreads) k_zline_tile(ZL L, const Q4<T> *__restrict__ cpl,
+__global__ void __launch_bounds__(kTileThreads, sizeof(T) == 4 ? VFS_ZTILE_MINB : VFS_ZTILE_MINB64) k_zline_tile(ZL L, const Q4<T> *__restrict__ cpl,
                                                              const Q4<T> *__restrict__ tri, const T *__restrict__ b,
                                                              const T *__restrict__ xr, T *__restrict__ xw, int colour,
                                                              int x_zero) {
@@ -393,7 +402,7 @@ __global__ void __launch_bounds__(kTileThreads) k_zline_tile(ZL L, const Q4<T> *
   // A: the block size is a multiple of W, so each thread keeps one column and takes
   // every (blockDim/W)-th row; U rows are loaded before any of them is used.
   {
-    constexpr int U = sizeof(T) == 4 ? 6 : 3;
+    constexpr int U = sizeof(T) == 4 ? VFS_ZTILE_U32 : 3;
     const int w = threadIdx.x % W, jstep = blockDim.x / W;
     const int h = h0 + w;
     const int i = 2 * h + (colour ^ (k & 1));

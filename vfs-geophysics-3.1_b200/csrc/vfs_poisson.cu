@@ -265,7 +265,13 @@ int poisson_apply_dev(Ctx *c, const double *x, double *y) {
 // The FGMRES vectors are exactly zero off the unknowns, so every dot product runs over
 // the whole grid layout.  Reductions are deterministic: per-thread sums in a fixed order,
 // warp shuffles, a fixed-order sum over warps, then k_sum_rows over the block partials.
-static const int kKryBlocks = 148 * 4;
+#ifndef VFS_KRY_BLOCKS_PER_SM
+#define VFS_KRY_BLOCKS_PER_SM 4
+#endif
+#ifndef VFS_KRY_MINB
+#define VFS_KRY_MINB 1
+#endif
+static const int kKryBlocks = 148 * VFS_KRY_BLOCKS_PER_SM;
 static const int kKryThreads = 256;
 
 // Block sums of rows 0..nv-1 and of row NV (stored as row nv) of acc into
@@ -297,7 +303,7 @@ __device__ __forceinline__ void block_sums(const double (&acc)[NV + 1], int nv, 
 
 // <V_t, w> (t < nv) and <w, w>.
 template <int NV>
-__global__ void __launch_bounds__(kKryThreads) k_multidot(long long N, long long ldv, const double *__restrict__ V,
+__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_multidot(long long N, long long ldv, const double *__restrict__ V,
                                                           int nv, const double *__restrict__ w,
                                                           double *__restrict__ parts) {
   double acc[NV + 1];
@@ -330,7 +336,7 @@ __global__ void __launch_bounds__(kKryThreads) k_multidot(long long N, long long
 
 // w -= sum_t h_t V_t, with <V_t, w> (t < nv) and <w, w> of the result.
 template <int NV>
-__global__ void __launch_bounds__(kKryThreads) k_update_dots(long long N, long long ldv, const double *__restrict__ V,
+__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_dots(long long N, long long ldv, const double *__restrict__ V,
                                                              int nv, const double *__restrict__ h,
                                                              double *__restrict__ w, double *__restrict__ parts) {
   double hr[NV], acc[NV + 1];
@@ -371,7 +377,7 @@ __global__ void __launch_bounds__(kKryThreads) k_update_dots(long long N, long l
 
 // out = (w - sum_t h_t V_t) * scale.
 template <int NV>
-__global__ void __launch_bounds__(kKryThreads) k_update_scale(long long N, long long ldv, const double *__restrict__ V,
+__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_scale(long long N, long long ldv, const double *__restrict__ V,
                                                               int nv, const double *__restrict__ h,
                                                               const double *__restrict__ w, double scale,
                                                               double *__restrict__ out) {
@@ -405,7 +411,7 @@ __global__ void __launch_bounds__(kKryThreads) k_update_scale(long long N, long 
 
 // r = b - A x, with <r, r>.
 template <int NS>
-__global__ void __launch_bounds__(kKryThreads) k_residual(Grid g, const double *__restrict__ coef,
+__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_residual(Grid g, const double *__restrict__ coef,
                                                           const double *__restrict__ b, const double *__restrict__ x,
                                                           double *__restrict__ r, double *__restrict__ parts) {
   double acc[1] = {0};
