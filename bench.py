@@ -209,7 +209,7 @@ def timed(ctx, fn, reps, torch):
 # 128x96x128 cells, scaled by the cell ratio (x8) to 256x192x256 (profiles/
 # formfunction2_128x96x128.md): Formfunction_2 as the step runs it (k_face_flux, k_fp,
 # k_rhs) moved 1271.3 MB per launch there.
-KERNEL_TRAFFIC = {"formfunction2": 1271.3e6 * 8}
+KERNEL_TRAFFIC = {"formfunction2": 1268.8e6 * 8}
 
 KERNEL_BYTES = {
     # Formfunction_2 accumulating into Rhs (Formfunction_2(user, Rhs, scale) adds):
