@@ -352,7 +352,8 @@ typedef struct {
 
 /* Measures the step's fixed linear operators (Contra2Cart, FormBCS tail, Pressure_Gradient,
  * VolumeFlux, Poisson right-hand side, UpdatePressure, Projection, IB_BC, IB-node
- * interpolation) as sparse matrices from the forward kernels.  Needs metrics and nvert (and
+ * interpolation) as sparse matrices from the forward kernels (their transposes are the
+ * adjoint's operators; the tangent runs the kernels themselves).  Needs metrics and nvert (and
  * the IB-node list when immersed); a later change of nvert or of the grid needs a new
  * context.  The other adjoint entry points call it when needed. */
 int vfs_adjoint_setup(vfs_ctx *ctx);
@@ -365,10 +366,11 @@ int vfs_tangent(vfs_ctx *ctx, const vfs_adjoint_opts *opts, const double *dir, d
 int vfs_adjoint_gradient(vfs_ctx *ctx, const vfs_adjoint_opts *opts, double *grad, vfs_adjoint_stats *stats);
 /* Test hooks: the slots (field, component pairs) and entry count of measured operator op
  * (0 Contra2Cart, 1 FormBCS tail, 2 Pressure_Gradient, 3 VolumeFlux, 4 Poisson RHS, 5
- * UpdatePressure, 6 Projection, 7 IB_BC, 8 IB-node interpolation), and the operator
- * applied to in (slot-major, N per slot) by its kernels and by its matrix. */
+ * UpdatePressure, 6 Projection, 7 IB_BC, 8 IB-node interpolation); and, for vectors x and y
+ * (slot-major, N per slot), L x by the operator's kernels and L^T y by its measured matrix
+ * (the dot-product test <y, L x> = <L^T y, x>). */
 int vfs_adjoint_op_info(vfs_ctx *ctx, int op, int *nslot, int *fields, long long *nnz);
-int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *in, double *out_forward, double *out_matrix);
+int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *x, const double *y, double *Lx, double *LTy);
 
 #ifdef __cplusplus
 }

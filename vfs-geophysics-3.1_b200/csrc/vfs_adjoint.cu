@@ -35,11 +35,13 @@ struct Slot { int field, comp; };
 constexpr int kMaxSlots = 10;
 struct SlotPtrs { double *p[kMaxSlots]; };
 
+// A measured operator: its slots, the forward function (the tangent runs it on the
+// tangent fields), and its matrix by columns (the adjoint's rows).
 struct LinOp {
   int nslot = 0;
   Slot slot[kMaxSlots];
+  std::function<int(Ctx *)> fn;
   long long nnz = 0;
-  int *rp = nullptr, *ci = nullptr; double *rv = nullptr;   // CSR: rows are outputs
   int *cp = nullptr, *ri = nullptr; double *cvl = nullptr;  // CSC: rows of the transpose
 };
 
@@ -103,9 +105,8 @@ static int ensure_banks(Ctx *c) {
 }
 
 static void free_op(LinOp &o) {
-  cudaFree(o.rp); cudaFree(o.ci); cudaFree(o.rv);
   cudaFree(o.cp); cudaFree(o.ri); cudaFree(o.cvl);
-  o.rp = o.ci = o.cp = o.ri = nullptr; o.rv = o.cvl = nullptr; o.nnz = 0;
+  o.cp = o.ri = nullptr; o.cvl = nullptr; o.nnz = 0;
 }
 
 static void free_tapes(Adjoint &A) {
@@ -420,8 +421,8 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
     if (hn <= cap) {
       free_op(op);
       op.nnz = (long long)hn;
-      rc = compress(c, (long long)hn, n, rows, cols, vals, &op.rp, &op.ci, &op.rv);
-      if (!rc) rc = compress(c, (long long)hn, n, cols, rows, vals, &op.cp, &op.ri, &op.cvl);
+      rc = compress(c, (long long)hn, n, cols, rows, vals, &op.cp, &op.ri, &op.cvl);
+      if (!rc) op.fn = fn;
       cleanup();
       return rc;
     }
@@ -444,21 +445,31 @@ __global__ void k_spmv(long long n, long long N, const int *__restrict__ ptr, co
   y.p[r / N][r % N] = s;
 }
 
-// In place on bank b: slots <- L slots (transpose = 0) or L^T slots (transpose = 1).
+// In place on bank b: slots <- L slots (transpose = 0: the operator's own kernels run on
+// the bank's arrays, swapped in for the context's fields) or L^T slots (transpose = 1: the
+// measured matrix by columns).
 static int apply_op(Ctx *c, int o, int b, int transpose) {
   Adjoint &A = *c->adj;
   LinOp &op = A.op[o];
   const long long N = c->g.N, n = (long long)op.nslot * N;
+  int rc;
+  if (!transpose) {
+    double *keep[kMaxSlots];
+    for (int s = 0; s < op.nslot; s++) {
+      double *&f = c->f[op.slot[s].field][op.slot[s].comp];
+      keep[s] = f;
+      f = A.bank[b][op.slot[s].field][op.slot[s].comp];
+    }
+    rc = op.fn(c);
+    for (int s = 0; s < op.nslot; s++) c->f[op.slot[s].field][op.slot[s].comp] = keep[s];
+    return rc;
+  }
   SlotPtrs x, y;
   for (int s = 0; s < op.nslot; s++) {
     x.p[s] = A.bank[b][op.slot[s].field][op.slot[s].comp];
     y.p[s] = A.tmp[s];
   }
-  if (transpose)
-    k_spmv<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, op.cp, op.ri, op.cvl, x, y);
-  else
-    k_spmv<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, op.rp, op.ci, op.rv, x, y);
-  int rc;
+  k_spmv<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, op.cp, op.ri, op.cvl, x, y);
   if ((rc = check_launch(c, "k_spmv"))) return rc;
   for (int s = 0; s < op.nslot; s++)
     cudaMemcpyAsync(x.p[s], y.p[s], sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream);
@@ -1281,9 +1292,9 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
   return rc;
 }
 
-// One measured operator on host vectors (slot-major, N per slot): by its forward kernels
-// (out_fwd) and by its matrix (out_mat).
-static int op_check(Ctx *c, int o, const double *in, double *out_fwd, double *out_mat) {
+// One measured operator on host vectors (slot-major, N per slot): L x by its forward
+// kernels and L^T y by its measured matrix, for the dot-product test <y, L x> = <L^T y, x>.
+static int op_check(Ctx *c, int o, const double *x, const double *y, double *Lx, double *LTy) {
   int rc;
   if ((rc = adjoint_setup(c))) return rc;
   Adjoint &A = *c->adj;
@@ -1291,36 +1302,21 @@ static int op_check(Ctx *c, int o, const double *in, double *out_fwd, double *ou
   LinOp &op = A.op[o];
   const long long N = c->g.N;
   const size_t bytes = sizeof(double) * N;
-  std::vector<double *> keep(op.nslot, nullptr);
-  for (int s = 0; s < op.nslot; s++) {
-    if (cudaMalloc(&keep[s], bytes) != cudaSuccess) {
-      for (double *k : keep) cudaFree(k);
-      return set_err(c, VFS_ERR_CUDA, "adjoint: allocation failed");
-    }
-    double *f = c->f[op.slot[s].field][op.slot[s].comp];
-    cudaMemcpyAsync(keep[s], f, bytes, cudaMemcpyDeviceToDevice, c->stream);
-    cudaMemcpyAsync(f, in + s * N, bytes, cudaMemcpyHostToDevice, c->stream);
-    cudaMemcpyAsync(A.bank[TAN][op.slot[s].field][op.slot[s].comp], in + s * N, bytes, cudaMemcpyHostToDevice,
-                    c->stream);
-  }
-  const std::function<int(Ctx *)> fns[OP_N] = {
-      [](Ctx *x) { return contra2cart(x); },     [](Ctx *x) { return form_bcs_tail(x); },
-      [](Ctx *x) { return pressure_gradient_mode(x, 0, 0.0); },
-      [](Ctx *x) { return volume_flux(x); },     [](Ctx *x) { return poisson_rhs_local(x); },
-      [](Ctx *x) { return update_pressure(x); }, [](Ctx *x) { return projection(x); },
-      [](Ctx *x) { return ib_bc(x); },           [](Ctx *x) { return ibm_interpolation(x); }};
-  rc = fns[o](c);
-  if (!rc) rc = apply_op(c, o, TAN, 0);
-  for (int s = 0; s < op.nslot && !rc; s++) {
-    cudaMemcpyAsync(out_fwd + s * N, c->f[op.slot[s].field][op.slot[s].comp], bytes, cudaMemcpyDeviceToHost, c->stream);
-    cudaMemcpyAsync(out_mat + s * N, A.bank[TAN][op.slot[s].field][op.slot[s].comp], bytes, cudaMemcpyDeviceToHost,
-                    c->stream);
-  }
-  for (int s = 0; s < op.nslot; s++)
-    cudaMemcpyAsync(c->f[op.slot[s].field][op.slot[s].comp], keep[s], bytes, cudaMemcpyDeviceToDevice, c->stream);
-  cudaStreamSynchronize(c->stream);
-  for (double *k : keep) cudaFree(k);
   zero_bank(c, TAN);
+  zero_bank(c, ADJ);
+  for (int s = 0; s < op.nslot; s++) {
+    cudaMemcpyAsync(A.bank[TAN][op.slot[s].field][op.slot[s].comp], x + s * N, bytes, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(A.bank[ADJ][op.slot[s].field][op.slot[s].comp], y + s * N, bytes, cudaMemcpyHostToDevice, c->stream);
+  }
+  rc = apply_op(c, o, TAN, 0);
+  if (!rc) rc = apply_op(c, o, ADJ, 1);
+  for (int s = 0; s < op.nslot && !rc; s++) {
+    cudaMemcpyAsync(Lx + s * N, A.bank[TAN][op.slot[s].field][op.slot[s].comp], bytes, cudaMemcpyDeviceToHost, c->stream);
+    cudaMemcpyAsync(LTy + s * N, A.bank[ADJ][op.slot[s].field][op.slot[s].comp], bytes, cudaMemcpyDeviceToHost, c->stream);
+  }
+  cudaStreamSynchronize(c->stream);
+  zero_bank(c, TAN);
+  zero_bank(c, ADJ);
   cudaStreamSynchronize(c->stream);
   return rc;
 }
@@ -1387,11 +1383,11 @@ int vfs_adjoint_op_info(vfs_ctx *ctx, int op, int *nslot, int *fields, long long
   return op_info(c, op, nslot, fields, nnz);
 }
 
-int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *in, double *out_forward, double *out_matrix) {
+int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *x, const double *y, double *Lx, double *LTy) {
   Ctx *c = (Ctx *)ctx;
   VFS_ADJ_REQUIRE(c);
-  if (!in || !out_forward || !out_matrix) return set_err(c, VFS_ERR_INVALID, "vfs_adjoint_op_check: null argument");
-  return op_check(c, op, in, out_forward, out_matrix);
+  if (!x || !y || !Lx || !LTy) return set_err(c, VFS_ERR_INVALID, "vfs_adjoint_op_check: null argument");
+  return op_check(c, op, x, y, Lx, LTy);
 }
 
 }  // extern "C"

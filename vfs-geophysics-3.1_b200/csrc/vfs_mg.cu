@@ -602,7 +602,10 @@ __global__ void k_mg_active(long long n, const double *__restrict__ op, uint8_t 
 // single block), one thread block runs the rest of the V-cycle (smoothing, restriction, coarsest sweeps,
 // prolongation) with block barriers between the phases; the level data stay in L2.
 constexpr int kBottomMaxLevels = 12;
-constexpr int kBottomThreads = 512;
+#ifndef VFS_BOTTOM_THREADS
+#define VFS_BOTTOM_THREADS 512
+#endif
+constexpr int kBottomThreads = VFS_BOTTOM_THREADS;
 #ifndef VFS_BOTTOM_CELLS
 #define VFS_BOTTOM_CELLS 8192
 #endif

@@ -168,7 +168,7 @@ def load_library(path=None):
     lib.vfs_adjoint_gradient.argtypes = [vp, ctypes.POINTER(AdjointOpts), vp, ctypes.POINTER(AdjointStats)]
     lib.vfs_adjoint_op_info.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp,
                                         ctypes.POINTER(ctypes.c_longlong)]
-    lib.vfs_adjoint_op_check.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+    lib.vfs_adjoint_op_check.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp]
     if path is None:
         _lib = lib
     return lib
@@ -429,15 +429,17 @@ class Context:
         self._check(self.lib.vfs_adjoint_op_info(self.h, op, ctypes.byref(n), fields, ctypes.byref(nnz)))
         return [(fields[2 * s], fields[2 * s + 1]) for s in range(n.value)], nnz.value
 
-    def adjoint_op_check(self, op, x):
-        """The measured operator op applied to x (slots x N) by its kernels and by its matrix."""
+    def adjoint_op_check(self, op, x, y):
+        """(L x by the operator's kernels, L^T y by its measured matrix); x, y: slots x N."""
         slots, _ = self.adjoint_op_info(op)
         N = int(np.prod(self.shape))
         a = np.ascontiguousarray(x, dtype=np.float64).reshape(len(slots), N)
-        out_f = np.zeros_like(a)
-        out_m = np.zeros_like(a)
-        self._check(self.lib.vfs_adjoint_op_check(self.h, op, a.ctypes.data, out_f.ctypes.data, out_m.ctypes.data))
-        return out_f, out_m
+        b = np.ascontiguousarray(y, dtype=np.float64).reshape(len(slots), N)
+        lx = np.zeros_like(a)
+        lty = np.zeros_like(b)
+        self._check(self.lib.vfs_adjoint_op_check(self.h, op, a.ctypes.data, b.ctypes.data, lx.ctypes.data,
+                                                  lty.ctypes.data))
+        return lx, lty
 
 
 def _solve_opts(precision=0, rtol=1e-10, **kw):
