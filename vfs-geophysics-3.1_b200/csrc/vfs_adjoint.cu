@@ -916,7 +916,6 @@ static int tangent_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
     if ((rc = ff2_stage_tangent(c, t.uc[s], t.uk[s], a, dU, du, ddp, dpu, A.tface))) return rc;
     if ((rc = apply_op(c, OP_C2C, TAN, 0))) return rc;
   }
-  if ((rc = apply_op(c, OP_C2C, TAN, 0))) return rc;
   if (g.bc[5] == 4) {
     double fo = 0, area = 0;
     if ((rc = plane_sum(c, 1, 1, 0, dU.z, &fo))) return rc;
@@ -975,7 +974,6 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
     lfin = sa / area;
     if ((rc = plane_add(c, 1, 1, 0, -lfin, lU.z))) return rc;
   }
-  if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;
   for (int s = 3; s >= 0; s--) {
     const double a = kAlfa[s] * g.dt * g.st;
     if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;

@@ -1555,7 +1555,11 @@ int runge_kutta(Ctx *c) {
     if ((rc = formfunction2(c, 1.0, true, a))) return rc;
     if ((rc = contra2cart(c))) return rc;
   }
-  return form_bcs(c, true);
+  // FormBCS with the outlet rescaling (rhs.c:1670).  Its leading Contra2Cart would convert
+  // the Ucont the last stage has just converted, which reproduces the same Ucat, so it is
+  // skipped here as at the start of stages 2-4.
+  if (c->g.bc[5] == 4 && (rc = outlet_rescale(c))) return rc;
+  return form_bcs_tail(c);
 }
 
 
