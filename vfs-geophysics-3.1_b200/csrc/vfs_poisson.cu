@@ -272,7 +272,13 @@ int poisson_apply_dev(Ctx *c, const double *x, double *y) {
 #define VFS_KRY_MINB 1
 #endif
 static const int kKryBlocks = 148 * VFS_KRY_BLOCKS_PER_SM;
+// Blocks of the basis passes: a fixed multiple of the SM count, grid-stride (one point
+// pair per thread over the whole vector measured 7 % slower per step on the B200).
 static const int kKryThreads = 256;
+static int kry_grid(const Ctx *c) {
+  (void)c;
+  return kKryBlocks;
+}
 
 // Block sums of rows 0..nv-1 and of row NV (stored as row nv) of acc into
 // parts[row * gridDim.x + blockIdx.x].
@@ -409,19 +415,28 @@ __global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_scale(long
   }
 }
 
-// r = b - A x, with <r, r>.
+// r = b - A x, one point per thread, with the block sums of <r, r> in parts[blockIdx.x].
 template <int NS>
-__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_residual(Grid g, const double *__restrict__ coef,
-                                                          const double *__restrict__ b, const double *__restrict__ x,
-                                                          double *__restrict__ r, double *__restrict__ parts) {
-  double acc[1] = {0};
-  const long long N = g.N, stride = (long long)gridDim.x * blockDim.x;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += stride) {
+__global__ void __launch_bounds__(256) k_residual_pt(Grid g, const double *__restrict__ coef,
+                                                     const double *__restrict__ b, const double *__restrict__ x,
+                                                     double *__restrict__ r, double *__restrict__ parts) {
+  __shared__ double sh[8];
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double v2 = 0;
+  if (p < g.N) {
     const double v = b[p] - apply_row64<NS>(g, coef, x, p);
     r[p] = v;
-    acc[0] += v * v;
+    v2 = v * v;
   }
-  block_sums<0>(acc, 0, parts);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v2 += __shfl_down_sync(0xffffffffu, v2, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < 8; w++) s += sh[w];
+    parts[blockIdx.x] = s;
+  }
 }
 
 __global__ void k_sum_rows(const double *parts, int nrows, int ncols, double *out) {
@@ -457,9 +472,9 @@ static const int kRedBlocks = 148 * 2;
 
 // Sums the block partials of rows 0..nrows-1 (left by one of the kernels above in
 // c->red) and copies them to out on the host.
-static int finish_rows(Ctx *c, int nrows, double *out) {
-  double *res = c->red + (long long)nrows * kKryBlocks;
-  k_sum_rows<<<nrows, 256, 0, c->stream>>>(c->red, nrows, kKryBlocks, res);
+static int finish_rows(Ctx *c, int nrows, int ncols, double *out) {
+  double *res = c->red + (long long)nrows * ncols;
+  k_sum_rows<<<nrows, 256, 0, c->stream>>>(c->red, nrows, ncols, res);
   int rc;
   if ((rc = check_launch(c, "k_sum_rows"))) return rc;
   cudaMemcpyAsync(c->red_host, res, sizeof(double) * nrows, cudaMemcpyDeviceToHost, c->stream);
@@ -470,38 +485,41 @@ static int finish_rows(Ctx *c, int nrows, double *out) {
 
 // w = A z; h[0..nv-1] = <V_t, w>; h[nv] = <w, w>.
 static int apply_dots(Ctx *c, const double *z, double *w, const double *V, int nv, double *h) {
+  const int kg = kry_grid(c);
   int rc;
   if ((rc = poisson_apply_dev(c, z, w))) return rc;
   const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) k_multidot<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else if (nv <= 8) k_multidot<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else if (nv <= 16) k_multidot<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else k_multidot<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  if (nv <= 4) k_multidot<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else if (nv <= 8) k_multidot<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else if (nv <= 16) k_multidot<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else k_multidot<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
   if ((rc = check_launch(c, "k_multidot"))) return rc;
-  return finish_rows(c, nv + 1, h);
+  return finish_rows(c, nv + 1, kg, h);
 }
 
 // w -= V h (h on the device); out[0..nv-1] = <V_t, w>; out[nv] = <w, w>.
 static int update_dots(Ctx *c, const double *V, int nv, const double *hdev, double *w, double *out) {
+  const int kg = kry_grid(c);
   const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) k_update_dots<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else if (nv <= 8) k_update_dots<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else if (nv <= 16) k_update_dots<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else k_update_dots<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  if (nv <= 4) k_update_dots<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else if (nv <= 8) k_update_dots<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else if (nv <= 16) k_update_dots<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else k_update_dots<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
   int rc;
   if ((rc = check_launch(c, "k_update_dots"))) return rc;
-  return finish_rows(c, nv + 1, out);
+  return finish_rows(c, nv + 1, kg, out);
 }
 
 // out = (w - V h) * scale (h on the device).
 static int update_scale(Ctx *c, const double *V, int nv, const double *hdev, const double *w, double scale,
                         double *out) {
+  const int kg = kry_grid(c);
   const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) k_update_scale<4><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  else if (nv <= 8) k_update_scale<8><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  if (nv <= 4) k_update_scale<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  else if (nv <= 8) k_update_scale<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
   else if (nv <= 16)
-    k_update_scale<16><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  else k_update_scale<32><<<kKryBlocks, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+    k_update_scale<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  else k_update_scale<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
   return check_launch(c, "k_update_scale");
 }
 
@@ -531,18 +549,22 @@ static int residual(Ctx *c, const double *b, const double *x, double *r, double 
     k_sub_norm<<<kKryBlocks, 256, 0, c->stream>>>(c->g.N, b, r, c->red);
     if ((rc = check_launch(c, "k_sub_norm"))) return rc;
     double rr;
-    if ((rc = finish_rows(c, 1, &rr))) return rc;
+    if ((rc = finish_rows(c, 1, kKryBlocks, &rr))) return rc;
     *rnorm = sqrt(rr);
     return VFS_OK;
   }
-  if (c->ps.nslot == 7)
-    k_residual<7><<<kKryBlocks, kKryThreads, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
-  else
-    k_residual<NSLOT><<<kKryBlocks, kKryThreads, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
+  // one point per thread (the grid-stride form runs at a third of the bandwidth), then the
+  // block sums in a fixed order
+  const int nb = (int)nblocks(c->g.N, 256);
   int rc;
-  if ((rc = check_launch(c, "k_residual"))) return rc;
+  if ((rc = ensure_red(c, nb + 64))) return rc;
+  if (c->ps.nslot == 7)
+    k_residual_pt<7><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
+  else
+    k_residual_pt<NSLOT><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
+  if ((rc = check_launch(c, "k_residual_pt"))) return rc;
   double rr;
-  if ((rc = finish_rows(c, 1, &rr))) return rc;
+  if ((rc = reduce_sum(c, c->red, nb, &rr))) return rc;
   *rnorm = sqrt(rr);
   return VFS_OK;
 }
@@ -781,7 +803,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   }
   if (!P.hdev && cudaMalloc(&P.hdev, sizeof(double) * 64) != cudaSuccess)
     return set_err(c, VFS_ERR_CUDA, "poisson_solve: allocation failed");
-  if ((rc = ensure_red(c, 34 * kKryBlocks + 64))) return rc;
+  if ((rc = ensure_red(c, 34 * std::max(kKryBlocks, kry_grid(c)) + 64))) return rc;
   cudaEventRecord(c->ev0, c->stream);
   double *x = c->f[VFS_PHI][0];
   const double *b = c->f[VFS_B][0];
