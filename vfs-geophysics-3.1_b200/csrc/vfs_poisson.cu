@@ -688,26 +688,28 @@ __global__ void k_shift(long long n, const uint8_t *fluid, double val, double *x
 }
 
 __global__ void k_sum_fluid(long long n, const uint8_t *fluid, const double *a, double *parts) {
-  __shared__ double sh[256];
-  double s = 0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += stride)
-    if (fluid[p]) s += a[p];
-  sh[threadIdx.x] = s;
+  __shared__ double sh[8];
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double s = (p < n && fluid[p]) ? a[p] : 0.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < 8; w++) t += sh[w];
+    parts[blockIdx.x] = t;
   }
-  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
 }
 
+// Sum of a over the fluid cells: one point per thread, block sums in a fixed order.
 static int sum_fluid(Ctx *c, const double *a, double *out) {
   int rc;
-  if ((rc = ensure_red(c, kRedBlocks + 64))) return rc;
-  k_sum_fluid<<<kRedBlocks, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, a, c->red);
+  const int nb = (int)nblocks(c->g.N, 256);
+  if ((rc = ensure_red(c, nb + 64))) return rc;
+  k_sum_fluid<<<nb, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, a, c->red);
   if ((rc = check_launch(c, "k_sum_fluid"))) return rc;
-  return reduce_sum(c, c->red, kRedBlocks, out);
+  return reduce_sum(c, c->red, nb, out);
 }
 
 // VolumeFlux(user, Ucont, ...) (poisson.c:3306-3500) without sharp-interface IB nodes
@@ -1050,39 +1052,57 @@ int projection(Ctx *c) {
 // ------------------------------------------------------------------ Divergence
 // main.c:1083-1090: max |(dU + dV + dW) * aj| over interior cells with no solid in the
 // 7-point neighbourhood.
+// One point per thread; the block maxima go to parts[blockIdx.x].
 __global__ void k_divergence(Grid g, CV3 uc, const double *__restrict__ aj, const uint8_t *__restrict__ nv,
                              double *parts) {
-  __shared__ double sh[256];
-  double mval = 0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  __shared__ double sh[8];
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long sy = g.mx, sz = (long long)g.mx * g.my;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.N; p += stride) {
+  double mval = 0;
+  if (p < g.N) {
     int i, j, k;
     dijk(g, p, i, j, k);
-    if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2) continue;
-    double d = fabs((uc.x[p] - uc.x[p - 1] + uc.y[p] - uc.y[p - sy] + uc.z[p] - uc.z[p - sz]) * aj[p]);
-    if (nv[p] + nv[p + sz] + nv[p - sz] + nv[p + sy] + nv[p - sy] + nv[p + 1] + nv[p - 1] > 0) d = 0.;
-    mval = fmax(mval, d);
+    if (i >= 1 && i <= g.mx - 2 && j >= 1 && j <= g.my - 2 && k >= 1 && k <= g.mz - 2) {
+      double d = fabs((uc.x[p] - uc.x[p - 1] + uc.y[p] - uc.y[p - sy] + uc.z[p] - uc.z[p - sz]) * aj[p]);
+      if (nv[p] + nv[p + sz] + nv[p - sz] + nv[p + sy] + nv[p - sy] + nv[p + 1] + nv[p - 1] > 0) d = 0.;
+      mval = d;
+    }
   }
-  sh[threadIdx.x] = mval;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mval = fmax(mval, __shfl_down_sync(0xffffffffu, mval, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mval;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0;
+    for (int w = 0; w < 8; w++) m = fmax(m, sh[w]);
+    parts[blockIdx.x] = m;
+  }
+}
+
+// Maximum of n block maxima (one block).
+__global__ void k_max_parts(const double *parts, int n, double *out) {
+  __shared__ double sh[256];
+  double m = 0;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) m = fmax(m, parts[q]);
+  sh[threadIdx.x] = m;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
+  if (threadIdx.x == 0) out[0] = sh[0];
 }
 
 int divergence(Ctx *c, double *maxdiv) {
   int rc;
-  if ((rc = ensure_red(c, kRedBlocks + 64))) return rc;
-  k_divergence<<<kRedBlocks, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->f[VFS_AJ][0], c->nv, c->red);
+  const int nb = (int)nblocks(c->g.N, 256);
+  if ((rc = ensure_red(c, nb + 64))) return rc;
+  k_divergence<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->f[VFS_AJ][0], c->nv, c->red + 64);
+  k_max_parts<<<1, 256, 0, c->stream>>>(c->red + 64, nb, c->red);
   if ((rc = check_launch(c, "k_divergence"))) return rc;
-  cudaMemcpyAsync(c->red_host, c->red, sizeof(double) * kRedBlocks, cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(c->red_host, c->red, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "divergence sync failed");
-  double m = 0;
-  for (int q = 0; q < kRedBlocks; q++) m = std::max(m, c->red_host[q]);
-  *maxdiv = m;
+  *maxdiv = c->red_host[0];
   return VFS_OK;
 }
 
