@@ -102,7 +102,13 @@ typedef struct {
                         the grid coarsens to) */
   int pre_smooth, post_smooth; /* zebra line Gauss-Seidel sweeps per level (default 3, 3) */
   int coarse_iters;  /* sweeps on the coarsest level (default 4) */
-  int reserved[5];
+  int zero_guess;    /* 0 (default): start from the last solution, the VFS_PHI left by the
+                        previous solve, on the unknowns, as the reference's GMRES starts from
+                        the persistent Phi2 (poisson_hypre.c:571; Phi2 is created once,
+                        poisson.c:280-282); the first solve after the operator is built
+                        starts from 0, and one after VFS_PHI is set through vfs_set_field
+                        from the values set.  1: always start from 0. */
+  int reserved[4];
   double rtol;       /* relative residual target (default 1e-10) */
   double atol;       /* absolute residual target (default 0) */
   double reserved_d[4];
@@ -248,7 +254,8 @@ int vfs_poisson_lhs(vfs_ctx *ctx);
 int vfs_poisson_rhs(vfs_ctx *ctx);
 
 /* Poisson solve for VFS_PHI (replaces PoissonSolver_Hypre, poisson_hypre.c:498,
- * including Remove_Nullspace poisson_hypre.c:194 and Convert_Phi2_Phi poisson.c:92). */
+ * including Remove_Nullspace poisson_hypre.c:194 and Convert_Phi2_Phi poisson.c:92).
+ * Starts from the previous solution unless opts->zero_guess (see vfs_solve_opts). */
 int vfs_poisson_solve(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_solve_stats *stats);
 
 /* y = A x with the operator of vfs_poisson_lhs, on the grid layout (mx*my*mz doubles;

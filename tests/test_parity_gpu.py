@@ -209,6 +209,37 @@ def test_poisson_solve_matches_direct(name, precision):
 
 
 @pytest.mark.gpu
+def test_poisson_solve_starts_from_the_previous_solution():
+    """The solve's initial guess follows the reference's persistent Phi2 (zero when the
+    unknowns are numbered, poisson.c:280-282; the previous solution afterwards,
+    poisson_hypre.c:571): the first solve after PoissonLHSNew starts from 0 (initial
+    residual = |b|), a second solve of the same system starts at its solution and stops
+    at once, zero_guess = 1 reaches the same Phi from 0, and a Phi set through the ABI is
+    the next solve's starting point."""
+    case, (R, ctx) = _pair("cylinders")
+    ctx.poisson_lhs()
+    ctx.poisson_rhs()
+    first = ctx.poisson_solve(precision=1, rtol=1e-12)
+    assert first.converged == 1 and first.iterations > 0
+    b = ctx.get_field(vfs.B)
+    assert first.r0 == pytest.approx(np.linalg.norm(b), rel=1e-12)
+    phi = ctx.get_field(vfs.PHI)
+    again = ctx.poisson_solve(precision=1, rtol=1e-12)
+    # the first solve stops within twice the target on its true residual
+    assert again.converged == 1 and again.iterations <= 1
+    assert again.r0 <= 2.0001e-12 * first.r0
+    assert_close(ctx.get_field(vfs.PHI), phi, rtol=1e-10, atol_frac=1e-12, what="phi again")
+    cold = ctx.poisson_solve(precision=1, rtol=1e-12, zero_guess=1)
+    assert cold.r0 == pytest.approx(first.r0, rel=1e-12) and cold.iterations > 0
+    assert_close(ctx.get_field(vfs.PHI), phi, rtol=1e-8, atol_frac=1e-9, what="phi from 0")
+    ctx.set_field(vfs.PHI, 0.5 * phi)
+    half = ctx.poisson_solve(precision=1, rtol=1e-12)
+    assert half.r0 == pytest.approx(0.5 * first.r0, rel=1e-6)
+    assert_close(ctx.get_field(vfs.PHI), phi, rtol=1e-8, atol_frac=1e-9, what="phi from the set guess")
+    R.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", list(CASES))
 def test_form_metrics_bitwise(name):
     """FormMetrics on the device from the grid.dat nodes equals the reference's metrics,

@@ -807,31 +807,41 @@ static int vfi_lin(Ctx *c, const StepTape &t, int b, int adjoint) {
 // Tangent: the forward solver on the tangent right-hand side (Remove_Nullspace and the
 // periodic ghosts of Phi included).  Adjoint: the transpose of that map: the ghost copy
 // and the zero off the unknowns transposed, the fluid mean removed, then FGMRES with the
-// transposed operator; lambda_b is the solution on the unknowns.
+// transposed operator; lambda_b is the solution on the unknowns.  Both solve from 0 (a
+// linear map of the right-hand side) straight into the bank arrays, with the context's
+// B and Phi pointers swapped for the call, so the forward Phi, the next forward solve's
+// starting point, stays untouched.
+static int lin_solve_into(Ctx *c, double *rhs, double *sol, const vfs_solve_opts *o, bool transpose) {
+  vfs_solve_opts lo;
+  if (o) lo = *o;
+  else { memset(&lo, 0, sizeof(lo)); }
+  lo.zero_guess = 1;
+  double *fb = c->f[VFS_B][0], *fphi = c->f[VFS_PHI][0];
+  const bool guess = c->ps.guess;
+  c->f[VFS_B][0] = rhs;
+  c->f[VFS_PHI][0] = sol;
+  poisson_set_transpose(c, transpose);
+  vfs_solve_stats st;
+  int rc = poisson_solve(c, &lo, &st);
+  poisson_set_transpose(c, false);
+  c->f[VFS_B][0] = fb;
+  c->f[VFS_PHI][0] = fphi;
+  c->ps.guess = guess;
+  return rc == VFS_ERR_NOT_CONVERGED ? VFS_OK : rc;
+}
+
 static int solve_lin(Ctx *c, int b, const vfs_solve_opts *o) {
   const size_t bytes = sizeof(double) * c->g.N;
   const long long N = c->g.N;
   int rc;
   double *bb = bankp(c, b, VFS_B, 0), *ph = bankp(c, b, VFS_PHI, 0);
-  vfs_solve_stats st;
-  if (b == TAN) {
-    cudaMemcpyAsync(c->f[VFS_B][0], bb, bytes, cudaMemcpyDeviceToDevice, c->stream);
-    rc = poisson_solve(c, o, &st);
-    if (rc && rc != VFS_ERR_NOT_CONVERGED) return rc;
-    cudaMemcpyAsync(ph, c->f[VFS_PHI][0], bytes, cudaMemcpyDeviceToDevice, c->stream);
-    return VFS_OK;
-  }
+  if (b == TAN) return lin_solve_into(c, bb, ph, o, false);
   if ((rc = periodic_copy_adj3(c, V3{ph, nullptr, nullptr}))) return rc;
   k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, 0.0, 1, ph);
   double sum = 0;
   if ((rc = fluid_sum(c, ph, nullptr, &sum))) return rc;
   k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, -sum / (double)c->ps.nfluid, 1, ph);
-  cudaMemcpyAsync(c->f[VFS_B][0], ph, bytes, cudaMemcpyDeviceToDevice, c->stream);
-  poisson_set_transpose(c, true);
-  rc = poisson_solve(c, o, &st);
-  poisson_set_transpose(c, false);
-  if (rc && rc != VFS_ERR_NOT_CONVERGED) return rc;
-  cudaMemcpyAsync(bb, c->f[VFS_PHI][0], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  if ((rc = lin_solve_into(c, ph, bb, o, true))) return rc;
   k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, 0.0, 1, bb);
   cudaMemsetAsync(ph, 0, bytes, c->stream);
   return check_launch(c, "k_fluid_shift");
@@ -1017,10 +1027,11 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
 }
 
 // ---------------------------------------------------------------- state and objective
-static const int kCkptFields[5] = {VFS_UCONT, VFS_UCAT, VFS_P, VFS_UCAT_O, VFS_UCONT_O};
-static const int kCkptArrays = 13;
+// Phi is part of the state: the next Poisson solve starts from it.
+static const int kCkptFields[6] = {VFS_UCONT, VFS_UCAT, VFS_P, VFS_UCAT_O, VFS_UCONT_O, VFS_PHI};
+static const int kCkptArrays = 14;
 
-struct HostState { bool first_step = false; int ti = 0; double scal[VFS_NSCALARS] = {}; };
+struct HostState { bool first_step = false, guess = false; int ti = 0; double scal[VFS_NSCALARS] = {}; };
 
 static void save_state(Ctx *c, double *dst, HostState &h) {
   const size_t bytes = sizeof(double) * c->g.N;
@@ -1029,6 +1040,7 @@ static void save_state(Ctx *c, double *dst, HostState &h) {
     for (int q = 0; q < c->dof[f]; q++, a++)
       cudaMemcpyAsync(dst + (size_t)a * c->g.N, c->f[f][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
   h.first_step = c->first_step;
+  h.guess = c->ps.guess;
   h.ti = c->ti;
   memcpy(h.scal, c->scal, sizeof(h.scal));
 }
@@ -1039,6 +1051,7 @@ static void load_state(Ctx *c, const double *src, const HostState &h) {
     for (int q = 0; q < c->dof[f]; q++, a++)
       cudaMemcpyAsync(c->f[f][q], src + (size_t)a * c->g.N, bytes, cudaMemcpyDeviceToDevice, c->stream);
   c->first_step = h.first_step;
+  c->ps.guess = h.guess;
   c->ti = h.ti;
   memcpy(c->scal, h.scal, sizeof(h.scal));
 }

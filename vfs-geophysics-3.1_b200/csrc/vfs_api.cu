@@ -320,6 +320,7 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
                                                        c->f[field][1], c->f[field][2]);
   rc = check_launch(c, "k_unpack");
   if (field >= VFS_CSI && field <= VFS_KAJ) { c->metrics_set = true; c->ps.built = false; }
+  if (field == VFS_PHI) c->ps.guess = c->ps.built;  // the next solve starts from the values set
   if (cudaStreamSynchronize(c->stream) != cudaSuccess)
     return set_err(c, VFS_ERR_CUDA, "vfs_set_field: copy failed");
   return rc;

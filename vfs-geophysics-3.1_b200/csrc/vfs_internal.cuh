@@ -118,6 +118,7 @@ struct Poisson {
   double *w = nullptr, *r = nullptr, *t = nullptr;
   double *hdev = nullptr;   // Gram-Schmidt coefficients on the device (64 doubles)
   bool transpose = false;   // apply A^T (the adjoint solve)
+  bool guess = false;       // VFS_PHI holds the last solution for the current unknowns
 };
 
 // One immersed-boundary node of the IB-node list (IBMInfo, variables.h:95-172, as

@@ -643,6 +643,7 @@ int poisson_lhs(Ctx *c) {
   if ((rc = mg_setup(c))) return rc;
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "poisson_lhs failed");
   P.built = true;
+  P.guess = false;  // a fresh Phi2 with the unknown numbering (poisson.c:280-282)
   return VFS_OK;
 }
 
@@ -766,12 +767,40 @@ int poisson_rhs(Ctx *c) {
 }
 
 // ------------------------------------------------------------------ FGMRES
+// x = x on the unknowns, 0 elsewhere (the periodic ghost copies), with the block sums of
+// <b, b> in parts[blockIdx.x].
+__global__ void __launch_bounds__(256) k_guess(long long n, const uint8_t *__restrict__ fluid,
+                                               const double *__restrict__ b, double *__restrict__ x,
+                                               double *__restrict__ parts) {
+  __shared__ double sh[8];
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double v2 = 0;
+  if (p < n) {
+    if (!fluid[p]) x[p] = 0.0;
+    v2 = b[p] * b[p];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v2 += __shfl_down_sync(0xffffffffu, v2, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < 8; w++) s += sh[w];
+    parts[blockIdx.x] = s;
+  }
+}
+
 // Right-preconditioned flexible GMRES (Saad 1993) in FP64 with classical Gram-Schmidt,
-// re-orthogonalised where the first pass loses more than half the norm.  Solves A phi = b for the fluid unknowns, starting
-// from phi = 0 as HYPRE does with a zero initial vector (Petsc_to_Hypre_Vector of a fresh
-// Phi2), then removes the mean (Remove_Nullspace) and fills the grid Phi like
-// Convert_Phi2_Phi (poisson.c:92): non-fluid interior cells 0, periodic ghosts from
+// re-orthogonalised where the first pass loses more than half the norm.  Solves A phi = b
+// for the fluid unknowns, then removes the mean (Remove_Nullspace) and fills the grid Phi
+// like Convert_Phi2_Phi (poisson.c:92): non-fluid interior cells 0, periodic ghosts from
 // their images, other ghosts 0.
+// Initial guess: the reference hands HYPRE's GMRES the persistent Phi2, created zero once
+// with the unknown numbering (poisson.c:280-282) and holding the previous solution after
+// every solve (poisson_hypre.c:571, 604).  Here the previous solution is the grid Phi on
+// the unknowns (P.guess), so the first solve after the operator is built starts from 0
+// and later ones from the last Phi; zero_guess = 1 always starts from 0.  The target is
+// rtol * ||b|| either way, as in HYPRE's GMRES.
 int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   vfs_solve_opts o;
   memset(&o, 0, sizeof(o));
@@ -785,6 +814,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
     if (oin->pre_smooth > 0) o.pre_smooth = oin->pre_smooth;
     if (oin->post_smooth > 0) o.post_smooth = oin->post_smooth;
     if (oin->coarse_iters > 0) o.coarse_iters = oin->coarse_iters;
+    o.zero_guess = oin->zero_guess;
     if (oin->rtol > 0) o.rtol = oin->rtol;
     if (oin->atol > 0) o.atol = oin->atol;
   }
@@ -809,15 +839,27 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   cudaEventRecord(c->ev0, c->stream);
   double *x = c->f[VFS_PHI][0];
   const double *b = c->f[VFS_B][0];
-  cudaMemsetAsync(x, 0, sizeof(double) * N, c->stream);
+  const bool warm = P.guess && !o.zero_guess && !P.transpose;
+  double bnorm = 0;
+  if (warm) {
+    const int nb = (int)nblocks(N, 256);
+    if ((rc = ensure_red(c, nb + 64))) return rc;
+    k_guess<<<nb, 256, 0, c->stream>>>(N, P.fluid, b, x, c->red);
+    if ((rc = check_launch(c, "k_guess"))) return rc;
+    double bb = 0;
+    if ((rc = reduce_sum(c, c->red, nb, &bb))) return rc;
+    bnorm = sqrt(bb);
+  } else {
+    cudaMemsetAsync(x, 0, sizeof(double) * N, c->stream);
+  }
   const int m = o.restart;
   std::vector<double> H((m + 1) * m), cs(m), sn(m), gv(m + 1), y(m), h(m + 2), h2(m + 2);
   vfs_solve_stats s;
   memset(&s, 0, sizeof(s));
   double rnorm = 0;
-  if ((rc = residual(c, b, x, P.r, &rnorm))) return rc;  // x = 0: r = b
-  const double bnorm = rnorm;
-  s.r0 = bnorm;
+  if ((rc = residual(c, b, x, P.r, &rnorm))) return rc;  // from x = 0: r = b
+  if (!warm) bnorm = rnorm;
+  s.r0 = rnorm;
   const double tol = std::max(o.rtol * bnorm, o.atol);
   int it = 0;
   bool conv = bnorm <= tol;
@@ -923,6 +965,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   cudaEventSynchronize(c->ev1);
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  if (!P.transpose) P.guess = true;
   s.iterations = it;
   s.converged = conv ? 1 : 0;
   s.rfinal = rnorm;

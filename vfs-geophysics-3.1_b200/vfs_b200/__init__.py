@@ -62,7 +62,7 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [
         ("precision", ctypes.c_int), ("restart", ctypes.c_int), ("max_iter", ctypes.c_int),
         ("levels", ctypes.c_int), ("pre_smooth", ctypes.c_int), ("post_smooth", ctypes.c_int),
-        ("coarse_iters", ctypes.c_int), ("reserved", ctypes.c_int * 5),
+        ("coarse_iters", ctypes.c_int), ("zero_guess", ctypes.c_int), ("reserved", ctypes.c_int * 4),
         ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("reserved_d", ctypes.c_double * 4),
     ]
 
@@ -352,10 +352,10 @@ class Context:
         return y
 
     def poisson_solve(self, precision=0, rtol=1e-10, restart=30, max_iter=200, levels=0,
-                      pre_smooth=3, post_smooth=3, coarse_iters=4, allow_unconverged=False):
+                      pre_smooth=3, post_smooth=3, coarse_iters=4, allow_unconverged=False, zero_guess=0):
         o = SolveOpts(precision=precision, restart=restart, max_iter=max_iter, levels=levels,
                       pre_smooth=pre_smooth, post_smooth=post_smooth, coarse_iters=coarse_iters,
-                      rtol=rtol)
+                      rtol=rtol, zero_guess=zero_guess)
         st = SolveStats()
         allow = (ERR_NOT_CONVERGED,) if allow_unconverged else ()
         self._check(self.lib.vfs_poisson_solve(self.h, ctypes.byref(o), ctypes.byref(st)), allow)
@@ -373,10 +373,7 @@ class Context:
         return v.value
 
     def step(self, precision=0, rtol=1e-10, **kw):  # Flow_Solver, solvers.c:562 (implicit=0)
-        o = SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
-                      max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 0),
-                      pre_smooth=kw.get("pre_smooth", 3), post_smooth=kw.get("post_smooth", 3),
-                      coarse_iters=kw.get("coarse_iters", 4))
+        o = _solve_opts(precision, rtol, **kw)
         st = StepStats()
         self._check(self.lib.vfs_step(self.h, ctypes.byref(o), ctypes.byref(st)))
         return st
@@ -446,7 +443,7 @@ def _solve_opts(precision=0, rtol=1e-10, **kw):
     return SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
                      max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 0),
                      pre_smooth=kw.get("pre_smooth", 3), post_smooth=kw.get("post_smooth", 3),
-                     coarse_iters=kw.get("coarse_iters", 4))
+                     coarse_iters=kw.get("coarse_iters", 4), zero_guess=kw.get("zero_guess", 0))
 
 
 def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
