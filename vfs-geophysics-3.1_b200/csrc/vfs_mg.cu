@@ -522,31 +522,41 @@ __device__ __forceinline__ T zresid(const ZL &L, const Q4<T> *__restrict__ cpl, 
   return b[q] - ax;
 }
 
-// Coarse right-hand side: the sum of the residuals of the (active) children.
+// Coarse right-hand side: the sum of the residuals of the (active) children.  With
+// colour0_only the children of colour 1 ((i xor k) odd) are left out: after a zebra sweep
+// that ends with the colour-1 pass their line equations hold exactly (the j-line solve is
+// exact when j is not periodic), so their residuals are rounding only.
 template <typename T>
 __device__ __forceinline__ void zrestrict_cell(const ZL &F, const ZL &C, const Q4<T> *__restrict__ cpl,
                                               const Q4<T> *__restrict__ tri, const T *__restrict__ x,
-                                              const T *__restrict__ b, T *__restrict__ bc, long long t) {
+                                              const T *__restrict__ b, T *__restrict__ bc, long long t,
+                                              bool colour0_only = false) {
   const long long ncell = (long long)C.nx * C.ny * C.nz;
   if (t >= ncell) return;
   int I, J, K;
   zcell(C, t, I, J, K);
+  // every child's residual is formed (all its loads are in range) and an inactive child's
+  // left out by a select, so the loads of all children are in flight together
   T s = 0;
+#pragma unroll
   for (int c = 0; c < 2; c++)
+#pragma unroll
     for (int bb = 0; bb < 2; bb++)
+#pragma unroll
       for (int a = 0; a < 2; a++) {
+        if (colour0_only && a != c) continue;
         const int i = 2 * I + a, j = 2 * J + bb, k = 2 * K + c;
         const long long q = zidx(F, i, j, k);
-        if (tri[q].d == T(0)) continue;
-        s += zresid<T>(F, cpl, tri, x, b, i, j, k, q);
+        const T r = zresid<T>(F, cpl, tri, x, b, i, j, k, q);
+        if (tri[q].d != T(0)) s += r;
       }
   bc[zidx(C, I, J, K)] = s;
 }
 
-template <typename T>
+template <typename T, bool kColour0>
 __global__ void k_zrestrict(ZL F, ZL C, const Q4<T> *__restrict__ cpl, const Q4<T> *__restrict__ tri,
                             const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ bc) {
-  zrestrict_cell<T>(F, C, cpl, tri, x, b, bc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  zrestrict_cell<T>(F, C, cpl, tri, x, b, bc, blockIdx.x * (long long)blockDim.x + threadIdx.x, kColour0);
 }
 
 // x_fine += P x_coarse (cell-centred trilinear).
@@ -567,20 +577,35 @@ __device__ __forceinline__ void zprolong_cell(const ZL &F, const ZL &C, const ui
   if (Jn < 0 || Jn >= C.ny) Jn = C.jp ? (Jn + C.ny) % C.ny : -1;
   if (Kn < 0 || Kn >= C.nz) Kn = C.kp ? (Kn + C.nz) % C.nz : -1;
   const long long own = zidx(C, I, J, K);
+  // every load first (the flag and the value of each coarse neighbour are independent
+  // loads), then the sums in a fixed order: the loads do not wait on the flags
+  T v[8];
+  bool ok[8];
+#pragma unroll
+  for (int n = 1; n < 8; n++) {
+    const int a = n & 1, bb = (n >> 1) & 1, c = n >> 2;
+    const int ii = a ? In : I, jj = bb ? Jn : J, kk = c ? Kn : K;
+    const bool in = ii >= 0 && jj >= 0 && kk >= 0;
+    const long long qc = in ? zidx(C, ii, jj, kk) : own;
+    ok[n] = in && actC[qc];
+    v[n] = xc[qc];
+  }
+  const T xo = xc[own], xq = x[q];
   T wown = T(27) / T(64);
   T s = 0;
+#pragma unroll
   for (int c = 0; c < 2; c++)
+#pragma unroll
     for (int bb = 0; bb < 2; bb++)
+#pragma unroll
       for (int a = 0; a < 2; a++) {
         if (a + bb + c == 0) continue;
         const T w = (a ? T(1) : T(3)) * (bb ? T(1) : T(3)) * (c ? T(1) : T(3)) / T(64);
-        const int ii = a ? In : I, jj = bb ? Jn : J, kk = c ? Kn : K;
-        if (ii < 0 || jj < 0 || kk < 0) { wown += w; continue; }
-        const long long qc = zidx(C, ii, jj, kk);
-        if (!actC[qc]) { wown += w; continue; }
-        s += w * xc[qc];
+        const int n = a + 2 * bb + 4 * c;
+        if (!ok[n]) { wown += w; continue; }
+        s += w * v[n];
       }
-  x[q] += s + wown * xc[own];
+  x[q] = xq + (s + wown * xo);
 }
 
 template <typename T>
@@ -873,7 +898,12 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   const MGLevel &F = c->ps.lv[l], &C = c->ps.lv[l + 1];
   const long long nc = (long long)C.z.nx * C.z.ny * C.z.nz, nf = (long long)F.z.nx * F.z.ny * F.z.nz;
   const LvT<T> f = lvt<T>(F), cc = lvt<T>(C);
-  k_zrestrict<T><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
+  // the pre-smoothing ends with a colour-1 pass: on a zebra level without periodic j only
+  // the colour-0 residuals are left
+  if (F.zebra && !F.z.jp)
+    k_zrestrict<T, true><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
+  else
+    k_zrestrict<T, false><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
   if ((rc = check_launch(c, "k_zrestrict"))) return rc;
   if ((rc = mg_vcycle<T>(c, l + 1, nl, o))) return rc;
   k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, F.act, C.act, f.x, cc.x);

@@ -1123,17 +1123,28 @@ __global__ void k_divergence(Grid g, CV3 uc, const double *__restrict__ aj, cons
 }
 
 // Maximum of n block maxima (one block).
-__global__ void k_max_parts(const double *parts, int n, double *out) {
-  __shared__ double sh[256];
-  double m = 0;
-  for (int q = threadIdx.x; q < n; q += blockDim.x) m = fmax(m, parts[q]);
-  sh[threadIdx.x] = m;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
-    __syncthreads();
+// Maximum of n block partials (non-negative) in one block of 1024 threads, eight loads in
+// flight per thread.
+__global__ void __launch_bounds__(1024) k_max_parts(const double *parts, int n, double *out) {
+  __shared__ double sh[32];
+  double m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int q = threadIdx.x;
+  for (; q + 7 * 1024 < n; q += 8 * 1024) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) m[u] = fmax(m[u], parts[q + u * 1024]);
   }
-  if (threadIdx.x == 0) out[0] = sh[0];
+  for (; q < n; q += 1024) m[0] = fmax(m[0], parts[q]);
+  double t = fmax(fmax(fmax(m[0], m[1]), fmax(m[2], m[3])), fmax(fmax(m[4], m[5]), fmax(m[6], m[7])));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_down_sync(0xffffffffu, t, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    t = sh[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_down_sync(0xffffffffu, t, o));
+    if (threadIdx.x == 0) out[0] = t;
+  }
 }
 
 int divergence(Ctx *c, double *maxdiv) {
@@ -1141,7 +1152,7 @@ int divergence(Ctx *c, double *maxdiv) {
   const int nb = (int)nblocks(c->g.N, 256);
   if ((rc = ensure_red(c, nb + 64))) return rc;
   k_divergence<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->f[VFS_AJ][0], c->nv, c->red + 64);
-  k_max_parts<<<1, 256, 0, c->stream>>>(c->red + 64, nb, c->red);
+  k_max_parts<<<1, 1024, 0, c->stream>>>(c->red + 64, nb, c->red);
   if ((rc = check_launch(c, "k_divergence"))) return rc;
   cudaMemcpyAsync(c->red_host, c->red, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "divergence sync failed");
@@ -1174,6 +1185,16 @@ int run_kernel(Ctx *c, int which, int reps) {
       case 5: rc = mg_sweep_fine(c, 1); if (rc) return rc; break;
       case 7: rc = formfunction2_fused(c, 1.0, false, 0.0); if (rc) return rc; break;
       case 8: rc = formfunction2(c, 1.0, false, 0.0); if (rc) return rc; break;
+      case 9:
+      case 10: {  // one multigrid V-cycle (the preconditioner) on B, FP32 or FP64, into a work vector
+        vfs_solve_opts o;
+        memset(&o, 0, sizeof(o));
+        o.precision = which == 9 ? 0 : 1;
+        o.pre_smooth = 3; o.post_smooth = 3; o.coarse_iters = 4;
+        rc = mg_precondition(c, c->f[VFS_B][0], P.t, o);
+        if (rc) return rc;
+        break;
+      }
       case 6:
         k_projection<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->f[VFS_PHI][0], field3(c, VFS_UCONT));
         break;
