@@ -766,45 +766,67 @@ struct GlobalFaces {
   }
 };
 
-__global__ void k_fp(Grid g, FluxIn f1, FluxIn f2, FluxIn f3, const uint8_t *__restrict__ nv,
-                     double *fpx, double *fpy, double *fpz) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
+// Interior cell p away from walls, periodic images and solid cells: every wide difference
+// of Fp is the 4th-order one (faces c+1 and c-2 over 3) and every face is its own.
+__device__ __forceinline__ bool fp_regular(const Grid &g, const uint8_t *__restrict__ nv, long long p, int i, int j,
+                                           int k) {
+  const long long sy = g.mx, sz = (long long)g.mx * g.my;
+  return i >= 3 && i <= g.mx - 4 && j >= 3 && j <= g.my - 4 && k >= 3 && k <= g.mz - 4 &&
+         nv[p - 1] + nv[p] + nv[p + 1] + nv[p - sy] + nv[p + sy] + nv[p - sz] + nv[p + sz] == 0;
+}
+
+// fp_cell at a regular cell: constant offsets, the same arithmetic in the same order.
+__device__ __forceinline__ void fp_cell_regular(const Grid &g, const FluxIn &f1, const FluxIn &f2, const FluxIn &f3,
+                                                long long p, double fpv[3]) {
+  const long long st[3] = {1, g.mx, (long long)g.mx * g.my};
+  const FluxIn *fl[3] = {&f1, &f2, &f3};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    auto D = [&](int dir, int off) { return fl[dir]->div[c][p + off * st[dir]]; };
+    auto Vv = [&](int dir, int off) { return fl[dir]->visc[c][p + off * st[dir]]; };
+    const double div = (D(0, 0) - D(0, -1) + D(1, 0) - D(1, -1) + D(2, 0) - D(2, -1));
+    double acc = 0;
+    acc += (D(0, 1) - D(0, -2)) * (1. / 3.);
+    acc += (D(1, 1) - D(1, -2)) * (1. / 3.);
+    acc += (D(2, 1) - D(2, -2)) * (1. / 3.);
+    double v = 9. / 8. * div + -1. / 8. * acc;
+    v += (Vv(0, 0) - Vv(0, -1) + Vv(1, 0) - Vv(1, -1) + Vv(2, 0) - Vv(2, -1)) / 1.0;
+    fpv[c] = v;
+  }
+}
+
+// Fp at DA point p (nothing outside the interior cells).
+__device__ __forceinline__ void fp_point(const Grid &g, const FluxIn &f1, const FluxIn &f2, const FluxIn &f3,
+                                         const uint8_t *__restrict__ nv, long long p, double *fpx, double *fpy,
+                                         double *fpz) {
   const int mx = g.mx, my = g.my, mz = g.mz;
   int i, j, k;
   dijk(g, p, i, j, k);
   if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
   double fpv[3];
-  const long long sy = mx, sz = (long long)mx * my;
-  if (i >= 3 && i <= mx - 4 && j >= 3 && j <= my - 4 && k >= 3 && k <= mz - 4 &&
-      nv[p - 1] + nv[p] + nv[p + 1] + nv[p - sy] + nv[p + sy] + nv[p - sz] + nv[p + sz] == 0) {
-    // Away from walls, periodic images and solid cells every wide difference is the
-    // 4th-order one (faces c+1 and c-2 over 3) and every face is its own: fp_cell with
-    // constant offsets, the same arithmetic in the same order.
-    const long long st[3] = {1, sy, sz};
-    const FluxIn *fl[3] = {&f1, &f2, &f3};
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      auto D = [&](int dir, int off) { return fl[dir]->div[c][p + off * st[dir]]; };
-      auto Vv = [&](int dir, int off) { return fl[dir]->visc[c][p + off * st[dir]]; };
-      const double div = (D(0, 0) - D(0, -1) + D(1, 0) - D(1, -1) + D(2, 0) - D(2, -1));
-      double acc = 0;
-      acc += (D(0, 1) - D(0, -2)) * (1. / 3.);
-      acc += (D(1, 1) - D(1, -2)) * (1. / 3.);
-      acc += (D(2, 1) - D(2, -2)) * (1. / 3.);
-      double v = 9. / 8. * div + -1. / 8. * acc;
-      v += (Vv(0, 0) - Vv(0, -1) + Vv(1, 0) - Vv(1, -1) + Vv(2, 0) - Vv(2, -1)) / 1.0;
-      fpv[c] = v;
-    }
-    fpx[p] = fpv[0]; fpy[p] = fpv[1]; fpz[p] = fpv[2];
-    return;
+  if (fp_regular(g, nv, p, i, j, k)) {
+    fp_cell_regular(g, f1, f2, f3, p, fpv);
+  } else {
+    GlobalFaces F;
+    F.g = &g; F.f1 = f1; F.f2 = f2; F.f3 = f3;
+    F.rowi = p - i; F.rowj = p - (long long)j * mx; F.rowk = p - (long long)k * mx * my;
+    F.i = i; F.j = j; F.k = k;
+    fp_cell(g, nv, p, i, j, k, F, fpv);
   }
-  GlobalFaces F;
-  F.g = &g; F.f1 = f1; F.f2 = f2; F.f3 = f3;
-  F.rowi = p - i; F.rowj = p - (long long)j * mx; F.rowk = p - (long long)k * mx * my;
-  F.i = i; F.j = j; F.k = k;
-  fp_cell(g, nv, p, i, j, k, F, fpv);
   fpx[p] = fpv[0]; fpy[p] = fpv[1]; fpz[p] = fpv[2];
+}
+
+// Four resident blocks per SM (64 registers): 0.56 ms at 256 x 192 x 256 against 0.70 ms
+// uncapped (116 registers) and slower again at five or six (spills).
+#ifndef VFS_FP_MINB
+#define VFS_FP_MINB 4
+#endif
+__global__ void __launch_bounds__(256, VFS_FP_MINB) k_fp(Grid g, FluxIn f1, FluxIn f2, FluxIn f3,
+                                                         const uint8_t *__restrict__ nv, double *fpx, double *fpy,
+                                                         double *fpz) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  fp_point(g, f1, f2, f3, nv, p, fpx, fpy, fpz);
 }
 
 // Contravariant projection of Fp onto the faces, scale, masks and the boundary zeroing
@@ -1053,6 +1075,8 @@ static FluxIn flux_in(Ctx *c, int d) {
   return f;
 }
 
+void launch_fp(Ctx *c);
+
 // The 18 face-flux arrays of Formfunction_2 (one launch for the three face directions;
 // one launch per direction measured 30 % slower on the B200).
 static int face_fluxes(Ctx *c) {
@@ -1076,8 +1100,7 @@ int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   if ((rc = periodic_copy3(c, uc))) return rc;
   Metrics m = metrics(c);
   if ((rc = face_fluxes(c))) return rc;
-  k_fp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2), c->nv,
-                                                   c->fp[0], c->fp[1], c->fp[2]);
+  launch_fp(c);
   if ((rc = check_launch(c, "k_fp"))) return rc;
   V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
   k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], scale,
