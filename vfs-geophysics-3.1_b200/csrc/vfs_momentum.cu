@@ -653,10 +653,9 @@ __device__ __forceinline__ bool regular_faces(const uint8_t *__restrict__ nv, lo
 #ifndef VFS_FF_MINB
 #define VFS_FF_MINB 5
 #endif
-__global__ void __launch_bounds__(VFS_FF_THREADS, VFS_FF_MINB) k_face_flux(Grid g, Metrics m, CV3 uc, CV3 u, const uint8_t *__restrict__ nv,
-                            const double *__restrict__ nut, FluxOut f1, FluxOut f2, FluxOut f3) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
+__device__ __forceinline__ void face_flux_point(const Grid &g, const Metrics &m, CV3 uc, CV3 u,
+                                                const uint8_t *__restrict__ nv, const double *__restrict__ nut,
+                                                long long p, const FluxOut &f1, const FluxOut &f2, const FluxOut &f3) {
   const int mx = g.mx, my = g.my, mz = g.mz;
   int i, j, k;
   dijk(g, p, i, j, k);
@@ -693,6 +692,15 @@ __global__ void __launch_bounds__(VFS_FF_THREADS, VFS_FF_MINB) k_face_flux(Grid 
     f3.div[0][p] = d[0]; f3.div[1][p] = d[1]; f3.div[2][p] = d[2];
     f3.visc[0][p] = v[0]; f3.visc[1][p] = v[1]; f3.visc[2][p] = v[2];
   }
+}
+
+__global__ void __launch_bounds__(VFS_FF_THREADS, VFS_FF_MINB) k_face_flux(Grid g, Metrics m, CV3 uc, CV3 u,
+                                                                           const uint8_t *__restrict__ nv,
+                                                                           const double *__restrict__ nut, FluxOut f1,
+                                                                           FluxOut f2, FluxOut f3) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  face_flux_point(g, m, uc, u, nv, nut, p, f1, f2, f3);
 }
 
 // Fp at interior cells: 4th-order divergence correction 9/8*div - 1/8*wide/denom plus the
