@@ -366,7 +366,7 @@ def adjoint_window(nx, ny, nz, steps, every, torch):
     ctx.adjoint_setup()
     setup_s = time.perf_counter() - t0
     kw = dict(objective=vfs.OBJ_PRESSURE_DRAG, control=vfs.CTRL_INFLOW_PLANE, precision=1, rtol=1e-10)
-    ctx.adjoint_gradient(2, checkpoint_every=1, **kw)  # warm-up: tapes, Krylov space
+    ctx.adjoint_gradient(steps, checkpoint_every=every, **kw)  # warm-up: tapes, checkpoints, Krylov space
     torch.cuda.synchronize()
     # both sweeps wait on the host once per Krylov scalar (about a thousand round trips per
     # window), so a busy host stretches their event times: three windows, the median ratio
