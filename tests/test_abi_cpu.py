@@ -49,3 +49,34 @@ def test_bad_config_is_rejected_before_device_use():
     h = ctypes.c_void_p()
     rc = lib.vfs_create(ctypes.byref(cfg), 0, ctypes.byref(h))
     assert rc in (vfs.ERR_INVALID, vfs.ERR_NO_DEVICE)
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every public struct of include/vfs_b200.h has the size and field offsets the ctypes
+    mirror uses (compiled with the host C compiler: the structs hold no CUDA types)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    mirrors = {"vfs_config": vfs.VfsConfig, "vfs_solve_opts": vfs.SolveOpts, "vfs_solve_stats": vfs.SolveStats,
+               "vfs_step_stats": vfs.StepStats, "vfs_adjoint_opts": vfs.AdjointOpts,
+               "vfs_adjoint_stats": vfs.AdjointStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "vfs_b200.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append('  printf("%s sizeof %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in py._fields_:
+            lines.append('  printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, fname))
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, fname, val = line.split()
+        got[(cname, fname)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "sizeof")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
