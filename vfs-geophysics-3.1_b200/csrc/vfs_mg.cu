@@ -55,6 +55,40 @@ __device__ __forceinline__ void zcell(const ZL &L, long long t, int &i, int &j, 
   k = (int)kk;
 }
 
+// Programmatic dependent launch along the V-cycle's chain of short kernels: each kernel
+// lets its successor be scheduled as soon as all its own blocks have started, then waits
+// for its predecessor grid to complete (and its writes to be visible) before touching
+// memory, so the launch gap between kernels overlaps the tail of the previous one and
+// the results are those of plain stream order.  Outside such a launch both are no-ops.
+#ifndef VFS_PDL
+#define VFS_PDL 1
+#endif
+__device__ __forceinline__ void pdl_prologue() {
+#if VFS_PDL
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+template <typename... KArgs, typename... Args>
+static void launch_chain(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                         Args... args) {
+#if VFS_PDL
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+#else
+  kernel<<<grid, block, smem, stream>>>(static_cast<KArgs>(args)...);
+#endif
+}
+
 // ------------------------------------------------------------------ set-up (FP64)
 // Fine-level couplings from the reference operator (19 slots on the DA layout).
 __global__ void k_mg_fine_couplings(Grid g, ZL L, const double *__restrict__ coef, const uint8_t *__restrict__ fluid,
@@ -388,6 +422,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(T) == 4 ? VFS_ZTILE_MINB 
                                                              const Q4<T> *__restrict__ tri, const T *__restrict__ b,
                                                              const T *__restrict__ xr, T *__restrict__ xw, int colour,
                                                              int x_zero) {
+  pdl_prologue();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int hx = L.hx, ny = L.ny;
   const int P = ny | 1;
@@ -556,6 +591,7 @@ __device__ __forceinline__ void zrestrict_cell(const ZL &F, const ZL &C, const Q
 template <typename T, bool kColour0>
 __global__ void k_zrestrict(ZL F, ZL C, const Q4<T> *__restrict__ cpl, const Q4<T> *__restrict__ tri,
                             const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ bc) {
+  pdl_prologue();
   zrestrict_cell<T>(F, C, cpl, tri, x, b, bc, blockIdx.x * (long long)blockDim.x + threadIdx.x, kColour0);
 }
 
@@ -611,6 +647,7 @@ __device__ __forceinline__ void zprolong_cell(const ZL &F, const ZL &C, const ui
 template <typename T>
 __global__ void k_zprolong(ZL F, ZL C, const uint8_t *__restrict__ actF, const uint8_t *__restrict__ actC,
                            T *__restrict__ x, const T *__restrict__ xc) {
+  pdl_prologue();
   zprolong_cell<T>(F, C, actF, actC, x, xc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
@@ -678,6 +715,7 @@ __device__ void blk_smooth(const BLevel<T> &L, int sweeps, bool x_zero, T omega)
 
 template <typename T>
 __global__ void __launch_bounds__(kBottomThreads) k_mg_bottom(Bottom<T> B) {
+  pdl_prologue();
   for (int l = 0; l < B.nl - 1; l++) {
     const BLevel<T> &F = B.lv[l], &C = B.lv[l + 1];
     blk_smooth<T>(F, B.pre, true, B.omega);
@@ -699,6 +737,7 @@ __global__ void __launch_bounds__(kBottomThreads) k_mg_bottom(Bottom<T> B) {
 // DA-layout FP64 vector -> finest-level right-hand side.
 template <typename T>
 __global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, T *__restrict__ b) {
+  pdl_prologue();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long ncell = (long long)L.nx * L.ny * L.nz;
   if (t >= ncell) return;
@@ -711,6 +750,7 @@ __global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, T *__rest
 template <typename T>
 __global__ void k_from_zebra(Grid g, ZL L, const uint8_t *__restrict__ fluid, const T *__restrict__ x,
                              double *__restrict__ z) {
+  pdl_prologue();
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const unsigned up = (unsigned)p, umx = (unsigned)g.mx, umy = (unsigned)g.my;
@@ -831,8 +871,8 @@ static bool launch_tile_w(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour,
     attr_set = true;
   }
   const int tiles = (L.z.hx + W - 1) / W;
-  k_zline_tile<T, W><<<tiles * L.z.nz, kTileThreads, smem, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.x, v.x, colour,
-                                                                        x_zero);
+  launch_chain(k_zline_tile<T, W>, dim3(tiles * L.z.nz), dim3(kTileThreads), smem, c->stream, L.z, v.cpl, v.tri, v.b,
+               v.x, v.x, colour, x_zero);
   return true;
 }
 template <typename T>
@@ -882,7 +922,7 @@ static int mg_bottom(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
     d.x = v.x; d.b = v.b; d.xo = v.xo; d.ds = v.ds;
     d.zebra = L.zebra ? 1 : 0;
   }
-  k_mg_bottom<T><<<1, kBottomThreads, 0, c->stream>>>(B);
+  launch_chain(k_mg_bottom<T>, dim3(1), dim3(kBottomThreads), 0, c->stream, B);
   return check_launch(c, "k_mg_bottom");
 }
 
@@ -901,12 +941,14 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   // the pre-smoothing ends with a colour-1 pass: on a zebra level without periodic j only
   // the colour-0 residuals are left
   if (F.zebra && !F.z.jp)
-    k_zrestrict<T, true><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
+    launch_chain(k_zrestrict<T, true>, dim3(nblocks(nc, 128)), dim3(128), 0, c->stream, F.z, C.z, f.cpl, f.tri, f.x,
+                 f.b, cc.b);
   else
-    k_zrestrict<T, false><<<nblocks(nc, 128), 128, 0, c->stream>>>(F.z, C.z, f.cpl, f.tri, f.x, f.b, cc.b);
+    launch_chain(k_zrestrict<T, false>, dim3(nblocks(nc, 128)), dim3(128), 0, c->stream, F.z, C.z, f.cpl, f.tri,
+                 f.x, f.b, cc.b);
   if ((rc = check_launch(c, "k_zrestrict"))) return rc;
   if ((rc = mg_vcycle<T>(c, l + 1, nl, o))) return rc;
-  k_zprolong<T><<<nblocks(nf, 256), 256, 0, c->stream>>>(F.z, C.z, F.act, C.act, f.x, cc.x);
+  launch_chain(k_zprolong<T>, dim3(nblocks(nf, 256)), dim3(256), 0, c->stream, F.z, C.z, F.act, C.act, f.x, cc.x);
   if ((rc = check_launch(c, "k_zprolong"))) return rc;
   return mg_smooth<T>(c, l, o.post_smooth, false);
 }
@@ -918,11 +960,11 @@ static int mg_apply(Ctx *c, const double *v, double *z, const vfs_solve_opts &o)
   const long long ncell = (long long)L0.z.nx * L0.z.ny * L0.z.nz;
   const LvT<T> l0 = lvt<T>(L0);
   int rc;
-  k_to_zebra<T><<<nblocks(ncell, 256), 256, 0, c->stream>>>(c->g, L0.z, v, l0.b);
+  launch_chain(k_to_zebra<T>, dim3(nblocks(ncell, 256)), dim3(256), 0, c->stream, c->g, L0.z, v, l0.b);
   if ((rc = check_launch(c, "k_to_zebra"))) return rc;
   const int nl = o.levels > 0 ? std::min((int)P.lv.size(), o.levels) : (int)P.lv.size();
   if ((rc = mg_vcycle<T>(c, 0, nl, o))) return rc;
-  k_from_zebra<T><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, L0.z, P.fluid, l0.x, z);
+  launch_chain(k_from_zebra<T>, dim3(nblocks(c->g.N, 256)), dim3(256), 0, c->stream, c->g, L0.z, P.fluid, l0.x, z);
   return check_launch(c, "k_from_zebra");
 }
 
