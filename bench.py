@@ -16,7 +16,7 @@ field resident in HBM; the all-FP64 form is timed on the same state for the comp
 `e2e` runs the same step through the C ABI with the flow state (Ucont, Ucat, P) copied
 from pinned host memory before and back after every step.
 
-Multi-GPU: the reference's north star keeps this path on one GPU, so N GPUs run N
+Multi-GPU: the projection path runs on one GPU (no sharding), so N GPUs run N
 independent replicas (weak scaling); the step time is the maximum over ranks.
 
 `--impl reference` times the reference's own CPU code (oracle/_ref: its momentum.c,

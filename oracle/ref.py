@@ -2,7 +2,7 @@
 compiled against the single-rank PETSc shim (see oracle/build_ref.py).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
-CPU-baseline leg, as the checker.  Never part of the product path.
+CPU-baseline leg, to compare against.  Never part of the product path.
 
 The reference keeps its run options in C globals (main.c:1-393); they are plain symbols
 of the library and are set here by name before each set-up.  One Reference instance

@@ -2,7 +2,7 @@
 path (oracle/vfs_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and bench.py's CPU
-baseline as the checker, never by the product.  Arrays use the reference's DA layout
+baseline to compare against, never by the product.  Arrays use the reference's DA layout
 (numpy shape (mz, my, mx[, 3])).
 """
 import ctypes

@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This is the oracle: a plain-C restatement, written here, of
  * the reference functions the B200 library replaces.  Only tests/, __graft_entry__.smoke()
- * and bench.py's CPU-baseline leg call it, as the checker.  It is pinned bit for bit
+ * and bench.py's CPU-baseline leg call it, to compare against.  It is pinned bit for bit
  * against the reference's own code (oracle/_ref, the reference sources compiled under a
  * single-rank PETSc shim) by tests/test_oracle_cpu.py.
  *

@@ -1,7 +1,7 @@
 """The oracle library runs every reference call sequence the GPU parity tests use, in one
 process and in the same order (several reference set-ups in a row), on the CPU.  This
-keeps the checker itself sound before any GPU run: a fault in the shim-compiled reference
-shows up here, not on the GPU machine."""
+keeps the oracle itself sound before any GPU run: a fault in the shim-compiled reference
+shows up here, on the CPU."""
 import numpy as np
 import pytest
 
