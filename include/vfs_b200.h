@@ -290,8 +290,8 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
 /* Contra2Cart for callers that cannot allocate device memory, for instance a solver
  * embedded in a framework that owns every device allocation through its own pool, or a
  * process whose device memory is fixed before the solver starts.  No counterpart in the
- * reference: it is the same computation as vfs_contra2cart (rhs.c:57), on caller-owned
- * device buffers, without a context and without any allocation.
+ * reference: it is the same computation as vfs_contra2cart of this library, on
+ * caller-owned device buffers, without a context and without any allocation.
  *
  * All arrays are device pointers on the current device, in the reference's DA layout
  * with vector fields as three consecutive component blocks (x block, y block, z block,
@@ -302,10 +302,12 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
  *
  * Scratch lives in one static device array of VFS_NOALLOC_SCRATCH_BYTES (about 52 MB)
  * that every GPU loading the library holds until the process exits.  Grids above
- * VFS_NOALLOC_MAX_POINTS are rejected with VFS_ERR_INVALID.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Every call shares the array: calls that overlap on the GPU race.  The
- * call synchronises its stream before returning.  Nothing is allocated or freed. */
+ * VFS_NOALLOC_MAX_POINTS are rejected with VFS_ERR_INVALID.  Every call looks up the
+ * array's device address (cudaGetSymbolAddress) in the current device's context.  Every
+ * call shares the array: serialise calls on one stream; calls that overlap on the GPU
+ * (two streams, or two host threads) race.  The call reads back an error word and
+ * synchronises its stream before returning, so it cannot be captured into a CUDA graph.
+ * Nothing is allocated or freed. */
 int vfs_contra2cart_noalloc(const vfs_config *cfg, double *ucont, const double *csi, const double *eta,
                             const double *zet, const double *nvert, const double *ucat_old, double *ucat,
                             void *stream);

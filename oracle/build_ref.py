@@ -21,6 +21,8 @@ OUT = os.path.join(HERE, "_ref")
 OBJ = os.path.join(OUT, "obj")
 SHIM = os.path.join(HERE, "shim")
 LIB = os.path.join(OUT, "libvfsref.so")
+# The reference checkout: the REF_DIR environment variable, else the read-only mount.
+REF_DIR = os.environ.get("REF_DIR", "/root/reference")
 
 # Reference translation units compiled into the oracle (the hot path plus the set-up
 # code it needs: grid input, metrics, BCs, IB interpolation, LES, globals in main.c).
@@ -72,8 +74,9 @@ def _stub_asm(func_syms, data_syms):
     return "\n".join(lines) + "\n"
 
 
-def build(ref_dir="/root/reference", verbose=False):
+def build(ref_dir=None, verbose=False):
     """Compile the reference sources + shim + driver into oracle/_ref/libvfsref.so."""
+    ref_dir = ref_dir or REF_DIR
     if not os.path.isdir(ref_dir):
         raise FileNotFoundError("reference sources not found at %s" % ref_dir)
     os.makedirs(OBJ, exist_ok=True)
@@ -121,4 +124,4 @@ def build(ref_dir="/root/reference", verbose=False):
 
 
 if __name__ == "__main__":
-    build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", verbose=True)
+    build(sys.argv[1] if len(sys.argv) > 1 else REF_DIR, verbose=True)

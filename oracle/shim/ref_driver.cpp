@@ -213,6 +213,27 @@ int ref_set_inflow_plane(const double *plane) {
   return 0;
 }
 int ref_ib_bc(void) { IB_BC(g_user); return 0; }
+// The end of one physical time step in the reference's time loop (main.c:3571-3602):
+// the old-value copies that the next step reads (Ucont_o, Ucont_rm1, P_o, and lUcat_old,
+// the slip-wall ghost source of Contra2Cart), for the single block of the oracle.
+int ref_end_of_step(void) {
+  UserCtx *user = g_user;
+  if (immersed) {
+    VecCopy(user->Nvert, user->Nvert_o);
+    DAGlobalToLocalBegin(user->da, user->Nvert_o, INSERT_VALUES, user->lNvert_o);
+    DAGlobalToLocalEnd(user->da, user->Nvert_o, INSERT_VALUES, user->lNvert_o);
+  }
+  VecCopy(user->Ucont_o, user->Ucont_rm1);
+  VecCopy(user->Ucont, user->Ucont_o);
+  VecCopy(user->P, user->P_o);
+  DAGlobalToLocalBegin(user->fda, user->Ucont_o, INSERT_VALUES, user->lUcont_o);
+  DAGlobalToLocalEnd(user->fda, user->Ucont_o, INSERT_VALUES, user->lUcont_o);
+  DAGlobalToLocalBegin(user->fda, user->Ucont_rm1, INSERT_VALUES, user->lUcont_rm1);
+  DAGlobalToLocalEnd(user->fda, user->Ucont_rm1, INSERT_VALUES, user->lUcont_rm1);
+  DAGlobalToLocalBegin(user->fda, user->Ucat, INSERT_VALUES, user->lUcat_old);
+  DAGlobalToLocalEnd(user->fda, user->Ucat, INSERT_VALUES, user->lUcat_old);
+  return 0;
+}
 int ref_update_pressure(void) { return UpdatePressure(g_user); }
 int ref_projection(void) { return Projection(g_user); }
 int ref_divergence(void) { return Divergence(g_user); }

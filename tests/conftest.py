@@ -12,6 +12,18 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) GPU")
 
 
+def pytest_sessionfinish(session, exitstatus):
+    """With VFS_PARITY_REPORT set, write the achieved errors that the parity tests
+    recorded (helpers.report) to that file as JSON."""
+    path = os.environ.get("VFS_PARITY_REPORT")
+    if not path:
+        return
+    import json
+    from helpers import REPORT
+    with open(path, "w") as f:
+        json.dump(REPORT, f, indent=1, sort_keys=True)
+
+
 def _has_gpu():
     try:
         import torch

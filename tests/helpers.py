@@ -54,10 +54,25 @@ def build_pair(case, seed=0, les_nut=False, extra_globals=None):
     return R, ctx
 
 
+# Achieved errors of the parity tests, keyed "test id / quantity" (written out by
+# conftest.py when VFS_PARITY_REPORT names a file).
+REPORT = {}
+
+
+def report(what, value):
+    """Record an achieved error under the running test's id, and print it."""
+    import os
+    test = os.environ.get("PYTEST_CURRENT_TEST", "").split(" ")[0]
+    REPORT["%s / %s" % (test, what)] = float(value)
+    print("%s / %s: %.3e" % (test, what, value))
+
+
 def assert_close(a, b, rtol=1e-12, atol_frac=1e-13, what=""):
+    """max |a - b| <= (rtol + atol_frac) * max |b|; records the achieved max |a - b| / max |b|."""
     a = np.asarray(a)
     b = np.asarray(b)
     scale = max(np.abs(b).max(), 1e-300)
     err = np.abs(a - b).max()
+    report(what + " max|diff|/max|ref|", err / scale)
     assert err <= atol_frac * scale + rtol * scale, "%s: max |diff| %.3e (scale %.3e)" % (what, err, scale)
     return err / scale

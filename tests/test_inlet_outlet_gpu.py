@@ -117,9 +117,9 @@ def test_inflow_outflow_step(name):
     st = ctx.step(precision=0, rtol=1e-13)
     assert st.poisson.converged == 1
     assert abs(ctx.get_scalar(vfs.S_FLUX_IN) - R.flux_in()) <= 1e-12 * abs(R.flux_in())
-    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-8, atol_frac=1e-9, what="P")
-    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-9, atol_frac=1e-10, what="Ucont")
-    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-10, atol_frac=0, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-10, atol_frac=0, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-10, atol_frac=0, what="Ucat")
     assert st.max_div < 1e-8
     R.close()
     ctx.close()

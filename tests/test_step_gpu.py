@@ -2,7 +2,11 @@
 periodic channel, B200 library against the reference's own functions.  The reference's
 HYPRE solve is replaced by a dense least-squares solve of its own matrix and right-hand
 side (both mean-free, Remove_Nullspace), so the comparison is solver independent up to
-the Poisson tolerance; the GPU solve runs to rtol 1e-13."""
+the Poisson tolerance; the GPU solve runs to rtol 1e-13.
+
+Velocity and pressure must agree within 1e-10 relative to their largest magnitude (the
+FP64 contract), in both precisions of the solve's preconditioner; each test records the
+error it achieved (helpers.report)."""
 import numpy as np
 import pytest
 
@@ -74,9 +78,9 @@ def test_one_step_matches_reference(name, precision):
     flux, area = R.kflux()
     assert abs(st.mean_k_flux - flux) <= 1e-13 * abs(flux)
     assert abs(ctx.get_scalar(vfs.S_MEAN_K_AREA) - area) <= 1e-13 * area
-    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-8, atol_frac=1e-9, what="P")
-    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-9, atol_frac=1e-10, what="Ucont")
-    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-10, atol_frac=0, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-10, atol_frac=0, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-10, atol_frac=0, what="Ucat")
     assert st.max_div < 1e-8
     R.close()
 
@@ -146,9 +150,9 @@ def test_one_les_step_matches_reference(name):
     assert R.get("lCs").max() > 0.0
     assert_close(ctx.get_field(vfs.CS), R.get("lCs"), rtol=1e-12, atol_frac=1e-14, what="Cs")
     assert_close(ctx.get_field(vfs.NU_T), R.get("lNu_t"), rtol=1e-12, atol_frac=1e-14, what="nu_t")
-    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-8, atol_frac=1e-9, what="P")
-    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-9, atol_frac=1e-10, what="Ucont")
-    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-10, atol_frac=0, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-10, atol_frac=0, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-10, atol_frac=0, what="Ucat")
     assert st.max_div < 1e-8
     assert ctx.get_scalar(vfs.S_TI) == 3
     R.close()
@@ -191,8 +195,8 @@ def test_one_immersed_step_matches_reference(precision):
     reference_immersed_step(R)
     st = ctx.step(precision=precision, rtol=1e-13)
     assert st.poisson.converged == 1
-    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-8, atol_frac=1e-9, what="P")
-    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-9, atol_frac=1e-10, what="Ucont")
-    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-9, atol_frac=1e-10, what="Ucat")
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-10, atol_frac=0, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-10, atol_frac=0, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-10, atol_frac=0, what="Ucat")
     assert st.max_div < 1e-8
     R.close()

@@ -39,7 +39,7 @@ def test_noalloc_contra2cart_matches_context_path(which):
     d_csi = torch.from_numpy(_soa(m["csi"])).to(dev)
     d_eta = torch.from_numpy(_soa(m["eta"])).to(dev)
     d_zet = torch.from_numpy(_soa(m["zet"])).to(dev)
-    d_nv = torch.from_numpy(np.ascontiguousarray(case.nvert)).to(dev)
+    d_nv = torch.from_numpy(np.ascontiguousarray(case.nvert, dtype=np.float64)).to(dev)
     for seed in (0, 1):   # two calls in a row on different inputs
         u = cases.initial_ucat(case, seed=seed)
         uc = cases.ucont_from_ucat(case, u, m)
@@ -53,6 +53,8 @@ def test_noalloc_contra2cart_matches_context_path(which):
         d_uc = torch.from_numpy(_soa(uc)).to(dev)
         d_u = torch.from_numpy(_soa(u)).to(dev)
         d_uo = torch.from_numpy(_soa(uo)).to(dev)
+        for t in (d_uc, d_csi, d_eta, d_zet, d_nv, d_uo, d_u):
+            assert t.dtype == torch.float64 and t.is_contiguous()
         torch.cuda.synchronize()
         rc = lib.vfs_contra2cart_noalloc(ctypes.byref(cfg), d_uc.data_ptr(), d_csi.data_ptr(), d_eta.data_ptr(),
                                          d_zet.data_ptr(), d_nv.data_ptr(), d_uo.data_ptr(), d_u.data_ptr(), None)

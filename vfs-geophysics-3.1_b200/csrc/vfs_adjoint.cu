@@ -299,7 +299,7 @@ static int compress(Ctx *c, long long nnz, long long nrows, const int *a, const 
             cudaMalloc(&perm, sizeof(int) * (nnz + 1)) == cudaSuccess &&
             cudaMalloc(&perm_out, sizeof(int) * (nnz + 1)) == cudaSuccess;
   if (ok && nnz > 0) {
-    k_iota<<<nblocks(nnz, 256), 256, 0, c->stream>>>(nnz, perm);
+    c->launches++, k_iota<<<nblocks(nnz, 256), 256, 0, c->stream>>>(nnz, perm);
     cub::DeviceRadixSort::SortPairs(nullptr, tb, a, ka_out, perm, perm_out, (int)nnz, 0, 32, c->stream);
     ok = cudaMalloc(&tmp, tb) == cudaSuccess;
     if (ok) cub::DeviceRadixSort::SortPairs(tmp, tb, a, ka_out, perm, perm_out, (int)nnz, 0, 32, c->stream);
@@ -307,8 +307,8 @@ static int compress(Ctx *c, long long nnz, long long nrows, const int *a, const 
   ok = ok && cudaMalloc(ptr, sizeof(int) * (nrows + 1)) == cudaSuccess &&
        cudaMalloc(idx, sizeof(int) * (nnz + 1)) == cudaSuccess && cudaMalloc(val, sizeof(double) * (nnz + 1)) == cudaSuccess;
   if (ok) {
-    if (nnz > 0) k_gather_entries<<<nblocks(nnz, 256), 256, 0, c->stream>>>(nnz, perm_out, b, v, *idx, *val);
-    k_row_ptr<<<nblocks(nnz + 1, 256), 256, 0, c->stream>>>(nnz, nrows, ka_out, *ptr);
+    if (nnz > 0) c->launches++, k_gather_entries<<<nblocks(nnz, 256), 256, 0, c->stream>>>(nnz, perm_out, b, v, *idx, *val);
+    c->launches++, k_row_ptr<<<nblocks(nnz + 1, 256), 256, 0, c->stream>>>(nnz, nrows, ka_out, *ptr);
   }
   cudaStreamSynchronize(c->stream);
   cudaFree(tmp); cudaFree(perm); cudaFree(perm_out); cudaFree(ka_out);
@@ -373,7 +373,7 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
     // the operator must be linear: zero in, zero out
     for (int s = 0; s < op.nslot; s++) cudaMemsetAsync(live.p[s], 0, bytes, c->stream);
     if ((rc = fn(c))) { cleanup(); return rc; }
-    k_absmax<<<256, 256, 0, c->stream>>>(n, live, N, amax);
+    c->launches++, k_absmax<<<256, 256, 0, c->stream>>>(n, live, N, amax);
     if (host_max(c, amax) != 0) {
       cleanup();
       return set_err(c, VFS_ERR_INVALID, "adjoint: an operator of the step is not linear here");
@@ -383,7 +383,7 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
         double tiny = 0;
         for (int kind = 0; kind < 3; kind++) {
           for (int t = 0; t < op.nslot; t++) cudaMemsetAsync(live.p[t], 0, bytes, c->stream);
-          k_probe_seed<<<nblocks(N, 256), 256, 0, c->stream>>>(N, cm, cc, kind, live.p[s]);
+          c->launches++, k_probe_seed<<<nblocks(N, 256), 256, 0, c->stream>>>(N, cm, cc, kind, live.p[s]);
           if ((rc = fn(c))) { cleanup(); return rc; }
           if (kind < 2) {
             double *dst = kind == 0 ? y0 : y1;
@@ -391,13 +391,13 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
               cudaMemcpyAsync(dst + t * N, live.p[t], bytes, cudaMemcpyDeviceToDevice, c->stream);
           }
           if (kind == 0) {
-            k_absmax<<<256, 256, 0, c->stream>>>(n, live, N, amax);
+            c->launches++, k_absmax<<<256, 256, 0, c->stream>>>(n, live, N, amax);
             const double m = host_max(c, amax);
             gmax = std::max(gmax, m);
             tiny = 1e-12 * m;
           }
         }
-        k_probe_decode<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, cm, cc, s, y0, y1, live, tiny, rows, cols, vals,
+        c->launches++, k_probe_decode<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, cm, cc, s, y0, y1, live, tiny, rows, cols, vals,
                                                                cnt, cap, conf, worst);
         if ((rc = check_launch(c, "k_probe_decode"))) { cleanup(); return rc; }
       }
@@ -469,7 +469,7 @@ static int apply_op(Ctx *c, int o, int b, int transpose) {
     x.p[s] = A.bank[b][op.slot[s].field][op.slot[s].comp];
     y.p[s] = A.tmp[s];
   }
-  k_spmv<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, op.cp, op.ri, op.cvl, x, y);
+  c->launches++, k_spmv<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, op.cp, op.ri, op.cvl, x, y);
   if ((rc = check_launch(c, "k_spmv"))) return rc;
   for (int s = 0; s < op.nslot; s++)
     cudaMemcpyAsync(x.p[s], y.p[s], sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream);
@@ -580,7 +580,7 @@ __global__ void k_dot_mask(long long N, int mode, Grid g, const uint8_t *__restr
 static int dot(Ctx *c, int mode, const double *a, const double *b, double *out) {
   int rc;
   if ((rc = ensure_red(c, kAdjBlocks + 64))) return rc;
-  k_dot_mask<<<kAdjBlocks, 256, 0, c->stream>>>(c->g.N, mode, c->g, c->nv, a, b, c->red);
+  c->launches++, k_dot_mask<<<kAdjBlocks, 256, 0, c->stream>>>(c->g.N, mode, c->g, c->nv, a, b, c->red);
   if ((rc = check_launch(c, "k_dot_mask"))) return rc;
   return reduce_sum(c, c->red, kAdjBlocks, out);
 }
@@ -622,7 +622,7 @@ __global__ void k_fluid_sum(long long n, const uint8_t *fluid, const double *a, 
 static int fluid_sum(Ctx *c, const double *a, const double *w, double *out) {
   int rc;
   if ((rc = ensure_red(c, kAdjBlocks + 64))) return rc;
-  k_fluid_sum<<<kAdjBlocks, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, a, w, c->red);
+  c->launches++, k_fluid_sum<<<kAdjBlocks, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, a, w, c->red);
   if ((rc = check_launch(c, "k_fluid_sum"))) return rc;
   return reduce_sum(c, c->red, kAdjBlocks, out);
 }
@@ -660,7 +660,7 @@ __global__ void k_plane_sum(Grid g, Metrics m, const uint8_t *__restrict__ nv, i
 static int plane_sum(Ctx *c, int outlet, int fluid_only, int area_weight, const double *a, double *out) {
   int rc;
   if ((rc = ensure_red(c, kAdjBlocks + 64))) return rc;
-  k_plane_sum<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, metrics(c), c->nv, outlet, fluid_only, area_weight, a, c->red);
+  c->launches++, k_plane_sum<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, metrics(c), c->nv, outlet, fluid_only, area_weight, a, c->red);
   if ((rc = check_launch(c, "k_plane_sum"))) return rc;
   return reduce_sum(c, c->red, kAdjBlocks, out);
 }
@@ -678,7 +678,7 @@ __global__ void k_plane_add(Grid g, Metrics m, const uint8_t *__restrict__ nv, i
 }
 static int plane_add(Ctx *c, int outlet, int fluid_only, int area_weight, double s, double *y) {
   const long long npl = (long long)(c->g.mx - 2) * (c->g.my - 2);
-  k_plane_add<<<nblocks(npl, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, outlet, fluid_only, area_weight, s, y);
+  c->launches++, k_plane_add<<<nblocks(npl, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, outlet, fluid_only, area_weight, s, y);
   return check_launch(c, "k_plane_add");
 }
 
@@ -786,20 +786,20 @@ static int vfi_lin(Ctx *c, const StepTape &t, int b, int adjoint) {
   Metrics m = metrics(c);
   double sx = 0, area = 0, unused = 0;
   if (adjoint) {
-    k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, 2, 0.0, c->red);
+    c->launches++, k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, 2, 0.0, c->red);
     if ((rc = check_launch(c, "k_vfi_lin"))) return rc;
     if ((rc = reduce_sum(c, c->red, kAdjBlocks, &sx))) return rc;
-    k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, 0, 0.0, c->red);
+    c->launches++, k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, 0, 0.0, c->red);
     if ((rc = check_launch(c, "k_vfi_lin"))) return rc;
     if ((rc = reduce_sum(c, c->red, kAdjBlocks, &unused))) return rc;
   } else {
-    k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, 0, 0.0, c->red);
+    c->launches++, k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, 0, 0.0, c->red);
     if ((rc = check_launch(c, "k_vfi_lin"))) return rc;
     if ((rc = reduce_sum(c, c->red, kAdjBlocks, &sx))) return rc;
   }
   if ((rc = reduce_sum(c, c->red + kAdjBlocks, kAdjBlocks, &area))) return rc;
   const double s = area > 1.e-15 ? sx / area : 0.0;
-  k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, adjoint ? 3 : 1, adjoint ? -s : s, c->red);
+  c->launches++, k_vfi_lin<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, m, c->nv, base, x, adjoint ? 3 : 1, adjoint ? -s : s, c->red);
   return check_launch(c, "k_vfi_lin");
 }
 
@@ -837,12 +837,12 @@ static int solve_lin(Ctx *c, int b, const vfs_solve_opts *o) {
   double *bb = bankp(c, b, VFS_B, 0), *ph = bankp(c, b, VFS_PHI, 0);
   if (b == TAN) return lin_solve_into(c, bb, ph, o, false);
   if ((rc = periodic_copy_adj3(c, V3{ph, nullptr, nullptr}))) return rc;
-  k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, 0.0, 1, ph);
+  c->launches++, k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, 0.0, 1, ph);
   double sum = 0;
   if ((rc = fluid_sum(c, ph, nullptr, &sum))) return rc;
-  k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, -sum / (double)c->ps.nfluid, 1, ph);
+  c->launches++, k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, -sum / (double)c->ps.nfluid, 1, ph);
   if ((rc = lin_solve_into(c, ph, bb, o, true))) return rc;
-  k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, 0.0, 1, bb);
+  c->launches++, k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, 0.0, 1, bb);
   cudaMemsetAsync(ph, 0, bytes, c->stream);
   return check_launch(c, "k_fluid_shift");
 }
@@ -856,10 +856,10 @@ static int nullspace_scale_lin(Ctx *c, int b) {
   double sum = 0;
   if (b == TAN) {
     if ((rc = fluid_sum(c, x, nullptr, &sum))) return rc;
-    k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, aj, -sum / c->ps.sum_aj, 0, x);
+    c->launches++, k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, aj, -sum / c->ps.sum_aj, 0, x);
   } else {
     if ((rc = fluid_sum(c, x, aj, &sum))) return rc;
-    k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, -sum / c->ps.sum_aj, 0, x);
+    c->launches++, k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, -sum / c->ps.sum_aj, 0, x);
   }
   return check_launch(c, "k_fluid_shift");
 }
@@ -875,7 +875,7 @@ static void copy3(Ctx *c, double *const dst[3], double *const src[3]) {
 static int move_add3(Ctx *c, double *const dst[3], double *const src[3]) {
   const long long N = c->g.N;
   for (int q = 0; q < 3; q++) {
-    k_axpy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, 1.0, src[q], dst[q]);
+    c->launches++, k_axpy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, 1.0, src[q], dst[q]);
     cudaMemsetAsync(src[q], 0, sizeof(double) * N, c->stream);
   }
   return check_launch(c, "k_axpy");
@@ -899,14 +899,14 @@ static int tangent_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
   if (kforce(c) && (rc = dot(c, 1, dU.z, nullptr, &dF))) return rc;
   if ((rc = apply_op(c, OP_PG, TAN, 0))) return rc;
   if (kforce(c)) {
-    k_axpy<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, dF / (g.mz - 2), A.cz, ddp.z);
+    c->launches++, k_axpy<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, dF / (g.mz - 2), A.cz, ddp.z);
     if ((rc = check_launch(c, "k_axpy"))) return rc;
   }
   // RungeKutta
   double dfin = 0;
   if (inlet100(c)) {
     const long long npl = (long long)(g.mx - 2) * (g.my - 2);
-    k_inflow_tan<<<nblocks(npl, 256), 256, 0, c->stream>>>(g, metrics(c), c->nv, A.plane[TAN], dU, du);
+    c->launches++, k_inflow_tan<<<nblocks(npl, 256), 256, 0, c->stream>>>(g, metrics(c), c->nv, A.plane[TAN], dU, du);
     if ((rc = check_launch(c, "k_inflow_tan"))) return rc;
     double flux1 = 0;
     if ((rc = plane_sum(c, 0, 0, 0, dU.z, &flux1))) return rc;
@@ -1005,14 +1005,14 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
     } else if ((rc = plane_add(c, 0, 0, 0, lfin, lU.z))) {
       return rc;
     }
-    k_inflow_adj<<<nblocks(npl, 256), 256, 0, c->stream>>>(g, metrics(c), c->nv, A.plane[ADJ], lU, lu);
+    c->launches++, k_inflow_adj<<<nblocks(npl, 256), 256, 0, c->stream>>>(g, metrics(c), c->nv, A.plane[ADJ], lU, lu);
     if ((rc = check_launch(c, "k_inflow_adj"))) return rc;
   }
   // Pressure_Gradient and the k-flux forcing
   if (kforce(c)) {
     double lF = 0;
     if ((rc = dot(c, 0, A.cz, ldp.z, &lF))) return rc;
-    k_add_kflux<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, lF / (g.mz - 2), lU.z);
+    c->launches++, k_add_kflux<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, lF / (g.mz - 2), lU.z);
     if ((rc = check_launch(c, "k_add_kflux"))) return rc;
   }
   if ((rc = apply_op(c, OP_PG, ADJ, 1))) return rc;
@@ -1097,7 +1097,7 @@ static int objective(Ctx *c, int obj, bool seed, double *J) {
     lu = bank3(c, ADJ, VFS_UCAT);
     lp = bankp(c, ADJ, VFS_P, 0);
   }
-  k_objective<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, metrics(c), c->nv, obj, cv(field3(c, VFS_UCAT)), c->f[VFS_P][0],
+  c->launches++, k_objective<<<kAdjBlocks, 256, 0, c->stream>>>(c->g, metrics(c), c->nv, obj, cv(field3(c, VFS_UCAT)), c->f[VFS_P][0],
                                                  lu, lp, c->red);
   if ((rc = check_launch(c, "k_objective"))) return rc;
   return reduce_sum(c, c->red, kAdjBlocks, J);
@@ -1209,7 +1209,7 @@ static int tangent_run(Ctx *c, const vfs_adjoint_opts *o, const double *dir, dou
   cudaMemcpyAsync(dev, dir, sizeof(double) * nc, cudaMemcpyHostToDevice, c->stream);
   if (o->control == VFS_CTRL_INITIAL_UCONT) {
     V3 d = bank3(c, TAN, VFS_UCONT);
-    k_aos_to_soa<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, dev, d.x, d.y, d.z);
+    c->launches++, k_aos_to_soa<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, dev, d.x, d.y, d.z);
   } else {
     cudaMemcpyAsync(A.plane[TAN], dev, sizeof(double) * nc, cudaMemcpyDeviceToDevice, c->stream);
   }
@@ -1280,7 +1280,7 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
   if (!rc) {
     if (o->control == VFS_CTRL_INITIAL_UCONT) {
       V3 l = bank3(c, ADJ, VFS_UCONT);
-      k_soa_to_aos<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, dev, l.x, l.y, l.z);
+      c->launches++, k_soa_to_aos<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, dev, l.x, l.y, l.z);
     } else {
       cudaMemcpyAsync(dev, A.plane[ADJ], sizeof(double) * nc, cudaMemcpyDeviceToDevice, c->stream);
     }

@@ -20,7 +20,6 @@ int set_err(Ctx *c, int code, const std::string &msg) {
 }
 
 int check_launch(Ctx *c, const char *what) {
-  c->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(c, VFS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -98,7 +97,7 @@ static int ensure_stage(Ctx *c, size_t bytes) {
 int reduce_sum(Ctx *c, const double *parts, int nparts, double *out) {
   int rc = ensure_red(c, 64);
   if (rc) return rc;
-  k_sum_parts<<<1, kSumThreads, 0, c->stream>>>(parts, nparts, c->red + 63);
+  c->launches++, k_sum_parts<<<1, kSumThreads, 0, c->stream>>>(parts, nparts, c->red + 63);
   if ((rc = check_launch(c, "k_sum_parts"))) return rc;
   cudaMemcpyAsync(c->red_host + 63, c->red + 63, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess)
@@ -318,7 +317,7 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
   if (field == VFS_NVERT) {
     int *bad = (int *)c->red;  // first word of the reduction buffer as a flag
     cudaMemsetAsync(bad, 0, sizeof(int), c->stream);
-    k_nvert_to_u8<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, c->g.N, c->nv, bad);
+    c->launches++, k_nvert_to_u8<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, c->g.N, c->nv, bad);
     rc = check_launch(c, "k_nvert_to_u8");
     int hbad = 0;
     cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
@@ -330,7 +329,7 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
     c->ps.built = false;
     return rc;
   }
-  k_unpack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
+  c->launches++, k_unpack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
                                                        c->f[field][1], c->f[field][2]);
   rc = check_launch(c, "k_unpack");
   if (field >= VFS_CSI && field <= VFS_KAJ) { c->metrics_set = true; c->ps.built = false; }
@@ -349,7 +348,7 @@ int vfs_get_field(vfs_ctx *ctx, int field, double *host) {
   int rc = ensure_stage(c, sizeof(double) * (size_t)c->g.N * 3);
   if (rc) return rc;
   double *stage = c->stage;
-  k_pack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
+  c->launches++, k_pack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
                                                      c->f[field][1], c->f[field][2]);
   rc = check_launch(c, "k_pack");
   cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, c->stream);

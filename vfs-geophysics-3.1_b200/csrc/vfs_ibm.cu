@@ -527,9 +527,9 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
   S.xmin = xmin; S.xmax = xmax; S.ymin = ymin; S.ymax = ymax; S.zmin = zmin; S.zmax = zmax;
   S.dcx = dcx; S.dcy = dcy; S.dcz = dcz;
   int rc;
-  k_ibm_cast<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, S, cv(field3(c, VFS_CENT)), c->nv, ibi == 0 ? 1 : 0, err);
+  c->launches++, k_ibm_cast<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, S, cv(field3(c, VFS_CENT)), c->nv, ibi == 0 ? 1 : 0, err);
   if ((rc = check_launch(c, "k_ibm_cast"))) { cudaFree(buf); return rc; }
-  k_ibm_near<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, c->bcflag);
+  c->launches++, k_ibm_near<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, c->bcflag);
   if ((rc = check_launch(c, "k_ibm_near"))) { cudaFree(buf); return rc; }
   // the IB-node list of this body (ibm.c:347-505): cells marked 2, ascending
   {
@@ -541,7 +541,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
       cudaFree(buf);
       return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: allocation failed");
     }
-    k_ibm_collect<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->bcflag, cells, cnt, cap);
+    c->launches++, k_ibm_collect<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->bcflag, cells, cnt, cap);
     int hn = 0;
     cudaMemcpyAsync(&hn, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     cudaStreamSynchronize(c->stream);
@@ -569,7 +569,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
     G.cent = cv(field3(c, VFS_CENT));
     G.cells = cells;
     G.n = hn;
-    if (hn) k_ibm_nodes<<<nblocks(hn, 64), 64, 0, c->stream>>>(g, G, nodes + base, err);
+    if (hn) c->launches++, k_ibm_nodes<<<nblocks(hn, 64), 64, 0, c->stream>>>(g, G, nodes + base, err);
     if ((rc = check_launch(c, "k_ibm_nodes"))) { cudaFree(qd); cudaFree(nodes); cudaFree(buf); return rc; }
     cudaFreeAsync(cells, c->stream);
     cudaStreamSynchronize(c->stream);
@@ -588,7 +588,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
     if (ibi == 0) c->nib_unresolved = 0;
     for (const IbNode &nd : hnodes) c->nib_unresolved += nd.imode == -2;
   }
-  k_ibm_remap<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->bcflag, c->nv, c->f[VFS_NVERT][0]);
+  c->launches++, k_ibm_remap<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->bcflag, c->nv, c->f[VFS_NVERT][0]);
   if ((rc = check_launch(c, "k_ibm_remap"))) { cudaFree(buf); return rc; }
   cudaMemsetAsync(c->bcflag, 0, (size_t)g.N, c->stream);  // Contra2Cart's flag buffer, clear again
   int herr = 0;
@@ -679,7 +679,7 @@ __global__ void k_ib_faces(Grid g, Metrics m, CV3 u, const uint8_t *__restrict__
 }
 
 int ib_faces(Ctx *c) {
-  k_ib_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), cv(field3(c, VFS_UCAT)), c->nv,
+  c->launches++, k_ib_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), cv(field3(c, VFS_UCAT)), c->nv,
                                                          field3(c, VFS_UCONT));
   return check_launch(c, "k_ib_faces");
 }
@@ -688,10 +688,10 @@ int ibm_interpolation(Ctx *c) {
   int rc;
   if (c->nib > 0) {
     const Grid &g = c->g;
-    k_ibm_gather<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, cv(field3(c, VFS_UCAT)),
+    c->launches++, k_ibm_gather<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, cv(field3(c, VFS_UCAT)),
                                                              c->f[VFS_P][0], c->nv, c->ibbuf);
     if ((rc = check_launch(c, "k_ibm_gather"))) return rc;
-    k_ibm_scatter<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, c->ibbuf, field3(c, VFS_UCAT),
+    c->launches++, k_ibm_scatter<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, c->ibbuf, field3(c, VFS_UCAT),
                                                               c->f[VFS_P][0]);
     if ((rc = check_launch(c, "k_ibm_scatter"))) return rc;
   }
@@ -756,13 +756,13 @@ int volume_flux_ibm(Ctx *c, double *flux, double *area) {
   const int nb = 148 * 2;
   if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
   Metrics m = metrics(c);
-  k_vflux_ibm<0><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), 0.0, c->red);
+  c->launches++, k_vflux_ibm<0><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), 0.0, c->red);
   if ((rc = check_launch(c, "k_vflux_ibm"))) return rc;
   double f = 0, a = 0;
   if ((rc = reduce_sum(c, c->red, nb, &f))) return rc;
   if ((rc = reduce_sum(c, c->red + nb, nb, &a))) return rc;
   const double correction = (a > 1.e-15) ? f / a : 0;
-  k_vflux_ibm<1><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), correction, c->red);
+  c->launches++, k_vflux_ibm<1><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), correction, c->red);
   if ((rc = check_launch(c, "k_vflux_ibm"))) return rc;
   if (flux) *flux = f;
   if (area) *area = a;

@@ -508,16 +508,16 @@ int smagorinsky_constant(Ctx *c) {
     return VFS_OK;
   }
   if (g.les == 1) {  // les.c:74-77
-    k_fill<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, 0.01, cs);
+    c->launches++, k_fill<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, 0.01, cs);
     return check_launch(c, "k_fill");
   }
   Metrics m = metrics(c);
   double *LM, *MM, *cs_tmp;
   LesPrep o = les_scratch(c, &LM, &MM, &cs_tmp);
   CV3 u = cv(field3(c, VFS_UCAT));
-  k_les_prep<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, u, m.csi, m.eta, m.zet, m.aj, c->nv, o);
+  c->launches++, k_les_prep<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, u, m.csi, m.eta, m.zet, m.aj, c->nv, o);
   if ((rc = check_launch(c, "k_les_prep"))) return rc;
-  k_les_image<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, u, m.csi, m.eta, m.zet, m.aj, c->nv, o);
+  c->launches++, k_les_image<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, u, m.csi, m.eta, m.zet, m.aj, c->nv, o);
   if ((rc = check_launch(c, "k_les_image"))) return rc;
   cudaMemsetAsync(LM, 0, sizeof(double) * (size_t)g.N, c->stream);
   cudaMemsetAsync(MM, 0, sizeof(double) * (size_t)g.N, c->stream);
@@ -532,19 +532,19 @@ int smagorinsky_constant(Ctx *c) {
   for (int q = 0; q < 6; q++) in.ss[q] = o.ss[q];
   in.uf = CV3{o.uf[0], o.uf[1], o.uf[2]};
   dim3 grid((g.mx - 2 + LTX - 1) / LTX, (g.my - 2 + LTY - 1) / LTY, (g.mz - 2 + LTZ - 1) / LTZ);
-  k_les_lm<<<grid, kLesLmThreads, sizeof(LesLmSmem), c->stream>>>(g, in, m.csi, m.eta, m.zet, m.aj, c->nv, LM, MM);
+  c->launches++, k_les_lm<<<grid, kLesLmThreads, sizeof(LesLmSmem), c->stream>>>(g, in, m.csi, m.eta, m.zet, m.aj, c->nv, LM, MM);
   if ((rc = check_launch(c, "k_les_lm"))) return rc;
   if ((rc = periodic_copy3(c, V3{LM, MM, nullptr}))) return rc;
-  k_les_cs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, o.wgt, c->nv, LM, MM, c->max_cs, cs_tmp);
+  c->launches++, k_les_cs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, o.wgt, c->nv, LM, MM, c->max_cs, cs_tmp);
   if ((rc = check_launch(c, "k_les_cs"))) return rc;
-  k_les_refilter<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, o.wgt, c->nv, cs_tmp, cs);
+  c->launches++, k_les_refilter<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, o.wgt, c->nv, cs_tmp, cs);
   return check_launch(c, "k_les_refilter");
 }
 
 int eddy_viscosity(Ctx *c) {
   const Grid &g = c->g;
   Metrics m = metrics(c);
-  k_les_nut<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(field3(c, VFS_UCAT)), m.csi, m.eta, m.zet, m.aj, c->nv,
+  c->launches++, k_les_nut<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(field3(c, VFS_UCAT)), m.csi, m.eta, m.zet, m.aj, c->nv,
                                                      c->f[VFS_CS][0], c->f[VFS_NU_T][0]);
   return check_launch(c, "k_les_nut");
 }

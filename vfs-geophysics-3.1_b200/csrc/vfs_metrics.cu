@@ -158,10 +158,10 @@ int form_metrics(Ctx *c, const double *x, const double *y, const double *z) {
       cudaMemsetAsync(c->f[f][q], 0, sizeof(double) * (size_t)g.N, c->stream);
   V3 csi = field3(c, VFS_CSI), eta = field3(c, VFS_ETA), zet = field3(c, VFS_ZET);
   double *aj = c->f[VFS_AJ][0];
-  k_centre_metrics<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, n, field3(c, VFS_CENT), csi, eta, zet, aj);
+  c->launches++, k_centre_metrics<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, n, field3(c, VFS_CENT), csi, eta, zet, aj);
   if ((rc = check_launch(c, "k_centre_metrics"))) return rc;
   for (int dd = 0; dd < 3; dd++) {
-    k_ghost_plane<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, dd, csi, eta, zet, aj);
+    c->launches++, k_ghost_plane<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, dd, csi, eta, zet, aj);
     if ((rc = check_launch(c, "k_ghost_plane"))) return rc;
   }
   const int fields_c[4] = {VFS_CSI, VFS_ETA, VFS_ZET, VFS_AJ};
@@ -170,7 +170,7 @@ int form_metrics(Ctx *c, const double *x, const double *y, const double *z) {
     else rc = periodic_copy1(c, c->f[f][0]);
     if (rc) return rc;
   }
-  k_face_metrics<<<nblocks(g.N, 256), 256, 0, c->stream>>>(
+  c->launches++, k_face_metrics<<<nblocks(g.N, 256), 256, 0, c->stream>>>(
       g, cv(csi), cv(eta), cv(zet), aj, field3(c, VFS_ICSI), field3(c, VFS_IETA), field3(c, VFS_IZET),
       c->f[VFS_IAJ][0], field3(c, VFS_JCSI), field3(c, VFS_JETA), field3(c, VFS_JZET), c->f[VFS_JAJ][0],
       field3(c, VFS_KCSI), field3(c, VFS_KETA), field3(c, VFS_KZET), c->f[VFS_KAJ][0]);

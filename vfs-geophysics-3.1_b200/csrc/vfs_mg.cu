@@ -69,24 +69,32 @@ __device__ __forceinline__ void pdl_prologue() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 #endif
 }
+// Every launch is counted in the context's launch counter and its status is checked: the
+// return value of cudaLaunchKernelEx, then the sticky launch error.
 template <typename... KArgs, typename... Args>
-static void launch_chain(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
-                         Args... args) {
+static int launch_chain(Ctx *c, const char *what, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                        Args... args) {
+  c->launches++;
 #if VFS_PDL
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
-  cfg.stream = stream;
+  cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(c, VFS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
 #else
-  kernel<<<grid, block, smem, stream>>>(static_cast<KArgs>(args)...);
+  kernel<<<grid, block, smem, c->stream>>>(static_cast<KArgs>(args)...);
 #endif
+  return check_launch(c, what);
 }
 
 // ------------------------------------------------------------------ set-up (FP64)
@@ -811,18 +819,18 @@ int mg_setup(Ctx *c) {
     cudaMemsetAsync(L.v32, 0, sizeof(float) * 5 * n, c->stream);
     const long long ncell = (long long)nx * ny * nz;
     if (P.lv.empty()) {
-      k_mg_fine_couplings<<<nblocks(ncell, 128), 128, 0, c->stream>>>(g, L.z, P.coef, P.fluid, L.op64);
+      c->launches++, k_mg_fine_couplings<<<nblocks(ncell, 128), 128, 0, c->stream>>>(g, L.z, P.coef, P.fluid, L.op64);
     } else {
       const MGLevel &F = P.lv.back();
-      k_mg_coarse_couplings<<<nblocks(ncell, 128), 128, 0, c->stream>>>(F.z, L.z, F.op64, L.op64);
+      c->launches++, k_mg_coarse_couplings<<<nblocks(ncell, 128), 128, 0, c->stream>>>(F.z, L.z, F.op64, L.op64);
     }
     if ((rc = check_launch(c, "k_mg_couplings"))) { P.lv.push_back(L); return rc; }
-    k_mg_diag<<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64);
-    k_mg_thomas<<<nblocks((long long)nx * nz, 64), 64, 0, c->stream>>>(L.z, L.op64);
-    k_mg_active<<<nblocks(n, 256), 256, 0, c->stream>>>(n, L.op64, L.act);
-    k_mg_pack<double><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<double> *)L.pk64,
+    c->launches++, k_mg_diag<<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64);
+    c->launches++, k_mg_thomas<<<nblocks((long long)nx * nz, 64), 64, 0, c->stream>>>(L.z, L.op64);
+    c->launches++, k_mg_active<<<nblocks(n, 256), 256, 0, c->stream>>>(n, L.op64, L.act);
+    c->launches++, k_mg_pack<double><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<double> *)L.pk64,
                                                                  (Q4<double> *)L.pk64 + n);
-    k_mg_pack<float><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<float> *)L.pk32,
+    c->launches++, k_mg_pack<float><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<float> *)L.pk32,
                                                                 (Q4<float> *)L.pk32 + n);
     P.lv.push_back(L);
     if ((rc = check_launch(c, "k_mg_setup"))) return rc;
@@ -861,8 +869,9 @@ LvT<double> lvt<double>(const MGLevel &L) {
 static const double kJacobiOmega = 0.8;
 
 // Launches one tiled colour pass; false when the level's columns do not fit the tile.
+// rc receives the launch status.
 template <typename T, int W>
-static bool launch_tile_w(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour, int x_zero) {
+static bool launch_tile_w(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour, int x_zero, int &rc) {
   if (!tile_fits<T, W>(L.z.ny)) return false;
   const size_t smem = tile_smem<T, W>(L.z.ny);
   static bool attr_set = false;
@@ -871,15 +880,17 @@ static bool launch_tile_w(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour,
     attr_set = true;
   }
   const int tiles = (L.z.hx + W - 1) / W;
-  launch_chain(k_zline_tile<T, W>, dim3(tiles * L.z.nz), dim3(kTileThreads), smem, c->stream, L.z, v.cpl, v.tri, v.b,
-               v.x, v.x, colour, x_zero);
+  rc = launch_chain(c, "k_zline_tile", k_zline_tile<T, W>, dim3(tiles * L.z.nz), dim3(kTileThreads), smem, L.z,
+                    v.cpl, v.tri, v.b, v.x, v.x, colour, x_zero);
   return true;
 }
 template <typename T>
-static bool launch_zline_tile(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour, int x_zero) {
+static bool launch_zline_tile(Ctx *c, const MGLevel &L, const LvT<T> &v, int colour, int x_zero, int &rc) {
   if (sizeof(T) == 4)
-    return launch_tile_w<T, VFS_ZTILE_W32>(c, L, v, colour, x_zero) || launch_tile_w<T, 8>(c, L, v, colour, x_zero);
-  return launch_tile_w<T, VFS_ZTILE_W64>(c, L, v, colour, x_zero) || launch_tile_w<T, 8>(c, L, v, colour, x_zero);
+    return launch_tile_w<T, VFS_ZTILE_W32>(c, L, v, colour, x_zero, rc) ||
+           launch_tile_w<T, 8>(c, L, v, colour, x_zero, rc);
+  return launch_tile_w<T, VFS_ZTILE_W64>(c, L, v, colour, x_zero, rc) ||
+         launch_tile_w<T, 8>(c, L, v, colour, x_zero, rc);
 }
 
 // `sweeps` smoothing sweeps on level l; x_zero: x is taken as zero on entry.
@@ -888,21 +899,26 @@ static int mg_smooth(Ctx *c, int l, int sweeps, bool x_zero) {
   const MGLevel &L = c->ps.lv[l];
   const LvT<T> v = lvt<T>(L);
   const long long half = (long long)L.z.nz * L.z.hx;
+  int rc = VFS_OK;
   for (int s = 0; s < sweeps; s++) {
     const bool z = x_zero && s == 0;
     if (L.zebra) {
       for (int col = 0; col < 2; col++) {
         const int xz = (z && col == 0) ? 1 : 0;
-        if (!launch_zline_tile<T>(c, L, v, col, xz))
-          k_zline<T><<<nblocks(half, 64), 64, 0, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.x, v.ds, v.x, col, T(1), xz);
+        if (!launch_zline_tile<T>(c, L, v, col, xz, rc)) {
+          c->launches++, k_zline<T><<<nblocks(half, 64), 64, 0, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.x, v.ds, v.x, col, T(1), xz);
+          rc = check_launch(c, "k_zline");
+        }
+        if (rc) return rc;
       }
     } else {
       if (!z) cudaMemcpyAsync(v.xo, v.x, sizeof(T) * L.z.n, cudaMemcpyDeviceToDevice, c->stream);
-      k_zline<T><<<nblocks(2 * half, 64), 64, 0, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.xo, v.ds, v.x, -1,
+      c->launches++, k_zline<T><<<nblocks(2 * half, 64), 64, 0, c->stream>>>(L.z, v.cpl, v.tri, v.b, v.xo, v.ds, v.x, -1,
                                                                T(kJacobiOmega), z ? 1 : 0);
+      if ((rc = check_launch(c, "k_zline"))) return rc;
     }
   }
-  return check_launch(c, "k_zline");
+  return rc;
 }
 
 template <typename T>
@@ -922,8 +938,7 @@ static int mg_bottom(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
     d.x = v.x; d.b = v.b; d.xo = v.xo; d.ds = v.ds;
     d.zebra = L.zebra ? 1 : 0;
   }
-  launch_chain(k_mg_bottom<T>, dim3(1), dim3(kBottomThreads), 0, c->stream, B);
-  return check_launch(c, "k_mg_bottom");
+  return launch_chain(c, "k_mg_bottom", k_mg_bottom<T>, dim3(1), dim3(kBottomThreads), 0, B);
 }
 
 // V-cycle from level l (its right-hand side already in place); levels at or below
@@ -941,15 +956,16 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   // the pre-smoothing ends with a colour-1 pass: on a zebra level without periodic j only
   // the colour-0 residuals are left
   if (F.zebra && !F.z.jp)
-    launch_chain(k_zrestrict<T, true>, dim3(nblocks(nc, 128)), dim3(128), 0, c->stream, F.z, C.z, f.cpl, f.tri, f.x,
-                 f.b, cc.b);
+    rc = launch_chain(c, "k_zrestrict", k_zrestrict<T, true>, dim3(nblocks(nc, 128)), dim3(128), 0, F.z, C.z, f.cpl,
+                      f.tri, f.x, f.b, cc.b);
   else
-    launch_chain(k_zrestrict<T, false>, dim3(nblocks(nc, 128)), dim3(128), 0, c->stream, F.z, C.z, f.cpl, f.tri,
-                 f.x, f.b, cc.b);
-  if ((rc = check_launch(c, "k_zrestrict"))) return rc;
+    rc = launch_chain(c, "k_zrestrict", k_zrestrict<T, false>, dim3(nblocks(nc, 128)), dim3(128), 0, F.z, C.z, f.cpl,
+                      f.tri, f.x, f.b, cc.b);
+  if (rc) return rc;
   if ((rc = mg_vcycle<T>(c, l + 1, nl, o))) return rc;
-  launch_chain(k_zprolong<T>, dim3(nblocks(nf, 256)), dim3(256), 0, c->stream, F.z, C.z, F.act, C.act, f.x, cc.x);
-  if ((rc = check_launch(c, "k_zprolong"))) return rc;
+  if ((rc = launch_chain(c, "k_zprolong", k_zprolong<T>, dim3(nblocks(nf, 256)), dim3(256), 0, F.z, C.z, F.act,
+                         C.act, f.x, cc.x)))
+    return rc;
   return mg_smooth<T>(c, l, o.post_smooth, false);
 }
 
@@ -960,12 +976,13 @@ static int mg_apply(Ctx *c, const double *v, double *z, const vfs_solve_opts &o)
   const long long ncell = (long long)L0.z.nx * L0.z.ny * L0.z.nz;
   const LvT<T> l0 = lvt<T>(L0);
   int rc;
-  launch_chain(k_to_zebra<T>, dim3(nblocks(ncell, 256)), dim3(256), 0, c->stream, c->g, L0.z, v, l0.b);
-  if ((rc = check_launch(c, "k_to_zebra"))) return rc;
+  if ((rc = launch_chain(c, "k_to_zebra", k_to_zebra<T>, dim3(nblocks(ncell, 256)), dim3(256), 0, c->g, L0.z, v,
+                         l0.b)))
+    return rc;
   const int nl = o.levels > 0 ? std::min((int)P.lv.size(), o.levels) : (int)P.lv.size();
   if ((rc = mg_vcycle<T>(c, 0, nl, o))) return rc;
-  launch_chain(k_from_zebra<T>, dim3(nblocks(c->g.N, 256)), dim3(256), 0, c->stream, c->g, L0.z, P.fluid, l0.x, z);
-  return check_launch(c, "k_from_zebra");
+  return launch_chain(c, "k_from_zebra", k_from_zebra<T>, dim3(nblocks(c->g.N, 256)), dim3(256), 0, c->g, L0.z,
+                      P.fluid, l0.x, z);
 }
 
 // z = M^-1 v: one V-cycle in FP32 (precision 0) or FP64.

@@ -54,12 +54,12 @@ static long long ghost_points(const Grid &g) {
 
 int periodic_copy3(Ctx *c, V3 v) {
   if (!(c->g.iper || c->g.jper || c->g.kper)) return VFS_OK;
-  k_periodic_copy<<<nblocks(ghost_points(c->g), 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
+  c->launches++, k_periodic_copy<<<nblocks(ghost_points(c->g), 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
   return check_launch(c, "k_periodic_copy");
 }
 int periodic_copy1(Ctx *c, double *s) {
   if (!(c->g.iper || c->g.jper || c->g.kper)) return VFS_OK;
-  k_periodic_copy<<<nblocks(ghost_points(c->g), 256), 256, 0, c->stream>>>(c->g, s, nullptr, nullptr);
+  c->launches++, k_periodic_copy<<<nblocks(ghost_points(c->g), 256), 256, 0, c->stream>>>(c->g, s, nullptr, nullptr);
   return check_launch(c, "k_periodic_copy");
 }
 
@@ -322,7 +322,7 @@ int solid_list(Ctx *c) {
   if ((rc = ensure_red(c, 64))) return rc;
   unsigned long long *cnt = (unsigned long long *)(c->red + 62);
   cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), c->stream);
-  k_collect_solid<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->nv, nullptr, cnt);
+  c->launches++, k_collect_solid<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->nv, nullptr, cnt);
   unsigned long long n = 0;
   cudaMemcpyAsync(&n, cnt, sizeof(n), cudaMemcpyDeviceToHost, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "solid_list: count failed");
@@ -332,7 +332,7 @@ int solid_list(Ctx *c) {
     if (cudaMalloc(&c->solid, sizeof(long long) * n) != cudaSuccess)
       return set_err(c, VFS_ERR_CUDA, "solid_list: allocation failed");
     cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), c->stream);
-    k_collect_solid<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->nv, c->solid, cnt);
+    c->launches++, k_collect_solid<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->nv, c->solid, cnt);
     if ((rc = check_launch(c, "k_collect_solid"))) return rc;
   }
   c->nsolid = (long long)n;
@@ -345,21 +345,21 @@ int contra2cart(Ctx *c) {
   int rc;
   if ((rc = periodic_copy3(c, uc))) return rc;
   Metrics m = metrics(c);
-  k_contra2cart_interior<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(uc), m.csi, m.eta, m.zet, c->nv, ucat);
+  c->launches++, k_contra2cart_interior<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(uc), m.csi, m.eta, m.zet, c->nv, ucat);
   if ((rc = check_launch(c, "k_contra2cart_interior"))) return rc;
   if ((rc = periodic_copy3(c, ucat))) return rc;
   V3 out{c->bcbuf[0], c->bcbuf[1], c->bcbuf[2]};
   uint8_t *fl = c->bcflag;
   if ((rc = solid_list(c))) return rc;
   const long long ne = edge_points(g), ns = c->nsolid;
-  k_contra2cart_bc_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, m, c->nv, cv(ucat), cv(field3(c, VFS_UCAT_O)),
+  c->launches++, k_contra2cart_bc_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, m, c->nv, cv(ucat), cv(field3(c, VFS_UCAT_O)),
                                                                   out, fl);
-  if (ns > 0) k_solid_zero<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, out, fl);
+  if (ns > 0) c->launches++, k_solid_zero<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, out, fl);
   if ((rc = check_launch(c, "k_contra2cart_bc"))) return rc;
-  k_bc_commit_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, cv(out), fl, ucat);
-  if (ns > 0) k_bc_commit_list<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, cv(out), ucat);
-  k_bc_clear_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, fl);
-  if (ns > 0) k_bc_clear_list<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, fl);
+  c->launches++, k_bc_commit_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, cv(out), fl, ucat);
+  if (ns > 0) c->launches++, k_bc_commit_list<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, cv(out), ucat);
+  c->launches++, k_bc_clear_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, fl);
+  if (ns > 0) c->launches++, k_bc_clear_list<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, fl);
   if ((rc = check_launch(c, "k_bc_commit"))) return rc;
   return periodic_copy3(c, ucat);
 }
@@ -1092,7 +1092,7 @@ static int face_fluxes(Ctx *c) {
   Metrics m = metrics(c);
   CV3 uc = cv(field3(c, VFS_UCONT)), u = cv(field3(c, VFS_UCAT));
   const unsigned nb = nblocks(g.N, VFS_FF_THREADS);
-  k_face_flux<<<nb, VFS_FF_THREADS, 0, c->stream>>>(g, m, uc, u, c->nv, c->f[VFS_NU_T][0], flux_out(c, 0),
+  c->launches++, k_face_flux<<<nb, VFS_FF_THREADS, 0, c->stream>>>(g, m, uc, u, c->nv, c->f[VFS_NU_T][0], flux_out(c, 0),
                                                     flux_out(c, 1), flux_out(c, 2));
   return check_launch(c, "k_face_flux");
 }
@@ -1111,7 +1111,7 @@ int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   launch_fp(c);
   if ((rc = check_launch(c, "k_fp"))) return rc;
   V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
-  k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], scale,
+  c->launches++, k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], scale,
                                                  field3(c, VFS_RHS), rk_stage ? 1 : 0, rk_coeff,
                                                  cv(field3(c, VFS_DP)), cv(pu), uc);
   return check_launch(c, "k_rhs");
@@ -1130,17 +1130,17 @@ int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
     attr = true;
   }
   dim3 grid((g.mx - 2 + FTI - 1) / FTI, (g.my - 2 + FTJ - 1) / FTJ, (g.mz - 2 + FKC - 1) / FKC);
-  k_ff2_fused<<<grid, kFF2Threads, sizeof(FF2Smem), c->stream>>>(g, m, cv(uc), cv(field3(c, VFS_UCAT)), c->nv,
+  c->launches++, k_ff2_fused<<<grid, kFF2Threads, sizeof(FF2Smem), c->stream>>>(g, m, cv(uc), cv(field3(c, VFS_UCAT)), c->nv,
                                                                c->f[VFS_NU_T][0], scale, field3(c, VFS_RHS),
                                                                rk_stage ? 1 : 0, rk_coeff, cv(field3(c, VFS_DP)),
                                                                cv(pu));
   if ((rc = check_launch(c, "k_ff2_fused"))) return rc;
   const long long ng = 2LL * g.my * g.mz + 2LL * g.mx * g.mz + 2LL * g.mx * g.my;
-  k_rhs_ghosts<<<nblocks(ng, 256), 256, 0, c->stream>>>(g, m, c->nv, scale, field3(c, VFS_RHS), rk_stage ? 1 : 0,
+  c->launches++, k_rhs_ghosts<<<nblocks(ng, 256), 256, 0, c->stream>>>(g, m, c->nv, scale, field3(c, VFS_RHS), rk_stage ? 1 : 0,
                                                        rk_coeff, cv(field3(c, VFS_DP)), cv(pu));
   if ((rc = check_launch(c, "k_rhs_ghosts"))) return rc;
   if (rk_stage) {
-    k_rk_update<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, rk_coeff, cv(field3(c, VFS_RHS)), cv(pu), uc);
+    c->launches++, k_rk_update<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, rk_coeff, cv(field3(c, VFS_RHS)), cv(pu), uc);
     if ((rc = check_launch(c, "k_rk_update"))) return rc;
   }
   return VFS_OK;
@@ -1149,12 +1149,12 @@ int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
 // single-kernel launchers for the diagnostics entry point (vfs_run_kernel)
 void launch_face_flux(Ctx *c) { face_fluxes(c); }
 void launch_fp(Ctx *c) {
-  k_fp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2), c->nv,
+  c->launches++, k_fp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, flux_in(c, 0), flux_in(c, 1), flux_in(c, 2), c->nv,
                                                    c->fp[0], c->fp[1], c->fp[2]);
 }
 void launch_rhs(Ctx *c) {
   V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
-  k_rhs<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, c->fp[0], c->fp[1], c->fp[2], 1.0,
+  c->launches++, k_rhs<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, c->fp[0], c->fp[1], c->fp[2], 1.0,
                                                     field3(c, VFS_RHS), 0, 0.0, cv(field3(c, VFS_DP)), cv(pu),
                                                     field3(c, VFS_UCONT));
 }
@@ -1261,7 +1261,7 @@ int pressure_gradient_mode(Ctx *c, int mode, double kdiff) {
   int rc;
   // P's periodic ghosts are refreshed first (momentum.c:241-273)
   if ((rc = periodic_copy1(c, c->f[VFS_P][0]))) return rc;
-  k_pressure_gradient<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(
+  c->launches++, k_pressure_gradient<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(
       c->g, metrics(c), c->nv, c->f[VFS_P][0], kdiff, c->g.dt, c->scal[VFS_S_MEAN_K_AREA], mode,
       c->cfg.mean_pressure_gradient, field3(c, VFS_DP));
   return check_launch(c, "k_pressure_gradient");
@@ -1300,7 +1300,7 @@ int calc_k_flux(Ctx *c, double *flux) {
   int rc;
   const int nb = 148 * 4;
   if ((rc = ensure_red(c, nb + 64))) return rc;
-  k_kflux_parts<<<nb, 256, 0, c->stream>>>(c->g, c->f[VFS_UCONT][2], c->nv, c->red);
+  c->launches++, k_kflux_parts<<<nb, 256, 0, c->stream>>>(c->g, c->f[VFS_UCONT][2], c->nv, c->red);
   if ((rc = check_launch(c, "k_kflux_parts"))) return rc;
   double s = 0;
   if ((rc = reduce_sum(c, c->red, nb, &s))) return rc;
@@ -1339,7 +1339,7 @@ int calc_inlet_area(Ctx *c) {
   int rc;
   const int nb = 148 * 2;
   if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
-  k_area_parts<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_ZET)), c->nv, c->red);
+  c->launches++, k_area_parts<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_ZET)), c->nv, c->red);
   if ((rc = check_launch(c, "k_area_parts"))) return rc;
   double a = 0, b = 0;
   if ((rc = reduce_sum(c, c->red, nb, &a))) return rc;
@@ -1390,10 +1390,10 @@ int ib_bc(Ctx *c) {
     if ((rc = periodic_copy3(c, field3(c, VFS_UCAT)))) return rc;
     if ((rc = ib_faces(c))) return rc;
   }
-  k_ib_bc_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
+  c->launches++, k_ib_bc_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
   if ((rc = check_launch(c, "k_ib_bc_faces"))) return rc;
   if (c->g.iper || c->g.jper || c->g.kper) {
-    k_periodic_normal<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
+    c->launches++, k_periodic_normal<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
     if ((rc = check_launch(c, "k_periodic_normal"))) return rc;
   }
   return VFS_OK;
@@ -1507,7 +1507,7 @@ int inflow_flux(Ctx *c) {
   const long long npl = (long long)(g.mx - 2) * (g.my - 2);
   const int nb = (int)nblocks(npl, 256);
   if ((rc = ensure_red(c, nb + 64))) return rc;
-  k_inflow<<<nb, 256, 0, c->stream>>>(g, metrics(c), field3(c, VFS_UCONT), field3(c, VFS_UCAT), c->nv, prof, uin,
+  c->launches++, k_inflow<<<nb, 256, 0, c->stream>>>(g, metrics(c), field3(c, VFS_UCONT), field3(c, VFS_UCAT), c->nv, prof, uin,
                                      c->inflow_plane, c->inlet_nodes ? c->inlet_nodes + 1 * (size_t)(g.mx - 1) * (g.my - 1) : nullptr,
                                      c->red);
   if ((rc = check_launch(c, "k_inflow"))) return rc;
@@ -1515,7 +1515,7 @@ int inflow_flux(Ctx *c) {
   if ((rc = reduce_sum(c, c->red, nb, &flux1))) return rc;
   double flux_in = flux1;
   if (prof == 100 && inlet_flux > 0) {  // bcs.c:572-588 (sumFluxIn0 = inlet_flux)
-    k_inflow_rescale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), field3(c, VFS_UCONT), c->nv,
+    c->launches++, k_inflow_rescale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), field3(c, VFS_UCONT), c->nv,
                                                inlet_flux - flux1, area, c->red);
     if ((rc = check_launch(c, "k_inflow_rescale"))) return rc;
     if ((rc = reduce_sum(c, c->red, nb, &flux_in))) return rc;
@@ -1599,13 +1599,13 @@ int outlet_rescale(Ctx *c) {
     const long long npl = (long long)(g.mx - 2) * (g.my - 2);
     const int nb = (int)nblocks(npl, 256);
     if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
-    k_outlet_parts<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv, c->red);
+    c->launches++, k_outlet_parts<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv, c->red);
     if ((rc = check_launch(c, "k_outlet_parts"))) return rc;
     double flux_out = 0, area_sum = 0;
     if ((rc = reduce_sum(c, c->red, nb, &flux_out))) return rc;
     if ((rc = reduce_sum(c, c->red + nb, nb, &area_sum))) return rc;
     c->scal[VFS_S_FLUX_OUT] = flux_out;
-    k_outlet_scale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv,
+    c->launches++, k_outlet_scale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv,
                                              c->scal[VFS_S_FLUX_IN] - flux_out, area_sum);
     if ((rc = check_launch(c, "k_outlet_scale"))) return rc;
   }
@@ -1615,10 +1615,10 @@ int outlet_rescale(Ctx *c) {
 // FormBCS after the outlet rescaling: wall fluxes, Contra2Cart, box edges.
 int form_bcs_tail(Ctx *c) {
   int rc;
-  k_wall_flux<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
+  c->launches++, k_wall_flux<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
   if ((rc = check_launch(c, "k_wall_flux"))) return rc;
   if ((rc = contra2cart(c))) return rc;
-  k_zero_edges<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCAT));
+  c->launches++, k_zero_edges<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCAT));
   return check_launch(c, "k_zero_edges");
 }
 
@@ -2023,7 +2023,7 @@ __global__ void k_periodic_copy_adj(Grid g, double *a, double *b, double *c) {
 
 int periodic_copy_adj3(Ctx *c, V3 v) {
   if (!(c->g.iper || c->g.jper || c->g.kper)) return VFS_OK;
-  k_periodic_copy_adj<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
+  c->launches++, k_periodic_copy_adj<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
   return check_launch(c, "k_periodic_copy_adj");
 }
 
@@ -2038,14 +2038,14 @@ int ff2_stage_tangent(Ctx *c, const double *const uc[3], const double *const uk[
     for (int q = 0; q < 6; q++) fb.f[d][q] = tf[d][q];
   Metrics m = metrics(c);
   CV3 ucb{uc[0], uc[1], uc[2]}, ukb{uk[0], uk[1], uk[2]};
-  k_tan_face<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, c->nv, ucb, ukb, cv(dU), cv(du), fb);
+  c->launches++, k_tan_face<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, c->nv, ucb, ukb, cv(dU), cv(du), fb);
   if ((rc = check_launch(c, "k_tan_face"))) return rc;
   FluxIn f[3];
   for (int d = 0; d < 3; d++)
     for (int q = 0; q < 3; q++) { f[d].div[q] = tf[d][q]; f[d].visc[q] = tf[d][3 + q]; }
-  k_fp<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, f[0], f[1], f[2], c->nv, c->fp[0], c->fp[1], c->fp[2]);
+  c->launches++, k_fp<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, f[0], f[1], f[2], c->nv, c->fp[0], c->fp[1], c->fp[2]);
   if ((rc = check_launch(c, "k_fp"))) return rc;
-  k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], 1.0, field3(c, VFS_RHS),
+  c->launches++, k_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->fp[0], c->fp[1], c->fp[2], 1.0, field3(c, VFS_RHS),
                                                  1, a, cv(ddp), cv(dpu), dU);
   return check_launch(c, "k_rhs");
 }
@@ -2062,7 +2062,7 @@ int ff2_stage_adjoint(Ctx *c, const double *const uc[3], const double *const uk[
     for (int q = 0; q < 6; q++) cudaMemsetAsync(lf[d][q], 0, bytes, c->stream);
   }
   Metrics m = metrics(c);
-  k_adj_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, a, cv(lU), lpu, ldp, lfp[0], lfp[1], lfp[2]);
+  c->launches++, k_adj_rhs<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, a, cv(lU), lpu, ldp, lfp[0], lfp[1], lfp[2]);
   if ((rc = check_launch(c, "k_adj_rhs"))) return rc;
   cudaMemsetAsync(lU.x, 0, bytes, c->stream);
   cudaMemsetAsync(lU.y, 0, bytes, c->stream);
@@ -2070,10 +2070,10 @@ int ff2_stage_adjoint(Ctx *c, const double *const uc[3], const double *const uk[
   FaceBank fb;
   for (int d = 0; d < 3; d++)
     for (int q = 0; q < 6; q++) fb.f[d][q] = lf[d][q];
-  k_adj_fp<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, lfp[0], lfp[1], lfp[2], fb);
+  c->launches++, k_adj_fp<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, lfp[0], lfp[1], lfp[2], fb);
   if ((rc = check_launch(c, "k_adj_fp"))) return rc;
   CV3 ucb{uc[0], uc[1], uc[2]}, ukb{uk[0], uk[1], uk[2]};
-  k_adj_face<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, c->nv, ucb, ukb, fb, lU, lu);
+  c->launches++, k_adj_face<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, c->nv, ucb, ukb, fb, lU, lu);
   if ((rc = check_launch(c, "k_adj_face"))) return rc;
   return periodic_copy_adj3(c, lU);
 }

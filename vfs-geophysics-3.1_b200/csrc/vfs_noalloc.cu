@@ -41,23 +41,19 @@ static_assert(kScratchBytes == VFS_NOALLOC_SCRATCH_BYTES, "scratch size must mat
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-static unsigned char *g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_scratch on the current device.  In host code the symbol names a
-// host-side stand-in, not device memory, so it must never be passed to a kernel; the
-// address comes from cudaGetSymbolAddress, once per device, with that device current.
-int scratch_address(int dev, unsigned char **out) {
-  if (dev < 0 || dev >= kMaxDevices) return vfs::set_err(nullptr, VFS_ERR_INVALID, "vfs_contra2cart_noalloc: device id out of range");
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess || !p)
-      return vfs::set_err(nullptr, VFS_ERR_CUDA, std::string("vfs_contra2cart_noalloc: cudaGetSymbolAddress failed: ") +
-                                                     cudaGetErrorString(e));
-    g_scratch_addr[dev] = (unsigned char *)p;
-  }
-  *out = g_scratch_addr[dev];
+// Device address of g_scratch in the current device's context.  In host code the symbol
+// names a host-side stand-in, not device memory, so it must never be passed to a kernel;
+// the address comes from cudaGetSymbolAddress with the device current.  It is looked up
+// on every call (a cheap query next to the launches and the synchronisation that follow),
+// so a device reset or another context made current between calls never leaves a stale
+// address behind, and no cache is shared between host threads.
+int scratch_address(unsigned char **out) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess || !p)
+    return vfs::set_err(nullptr, VFS_ERR_CUDA, std::string("vfs_contra2cart_noalloc: cudaGetSymbolAddress failed: ") +
+                                                   cudaGetErrorString(e));
+  *out = (unsigned char *)p;
   return VFS_OK;
 }
 
@@ -88,7 +84,7 @@ extern "C" int vfs_contra2cart_noalloc(const vfs_config *cfg, double *ucont, con
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return set_err(nullptr, VFS_ERR_NO_DEVICE, "vfs_contra2cart_noalloc: no CUDA device");
   unsigned char *s = nullptr;
-  int rc = scratch_address(dev, &s);
+  int rc = scratch_address(&s);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   const long long N = g.N;

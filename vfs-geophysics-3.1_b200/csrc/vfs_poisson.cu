@@ -253,11 +253,11 @@ int poisson_set_transpose(Ctx *c, bool on) {
 int poisson_apply_dev(Ctx *c, const double *x, double *y) {
   if (c->ps.transpose) {
     cudaMemsetAsync(y, 0, sizeof(double) * c->g.N, c->stream);
-    k_apply_t<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.nslot, c->ps.coef, x, y);
+    c->launches++, k_apply_t<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.nslot, c->ps.coef, x, y);
     return check_launch(c, "k_apply_t");
   }
-  if (c->ps.nslot == 7) k_apply<7><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
-  else k_apply<NSLOT><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
+  if (c->ps.nslot == 7) c->launches++, k_apply<7><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
+  else c->launches++, k_apply<NSLOT><<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->ps.coef, x, y);
   return check_launch(c, "k_apply");
 }
 
@@ -474,7 +474,7 @@ static const int kRedBlocks = 148 * 2;
 // c->red) and copies them to out on the host.
 static int finish_rows(Ctx *c, int nrows, int ncols, double *out) {
   double *res = c->red + (long long)nrows * ncols;
-  k_sum_rows<<<nrows, 256, 0, c->stream>>>(c->red, nrows, ncols, res);
+  c->launches++, k_sum_rows<<<nrows, 256, 0, c->stream>>>(c->red, nrows, ncols, res);
   int rc;
   if ((rc = check_launch(c, "k_sum_rows"))) return rc;
   cudaMemcpyAsync(c->red_host, res, sizeof(double) * nrows, cudaMemcpyDeviceToHost, c->stream);
@@ -489,10 +489,10 @@ static int apply_dots(Ctx *c, const double *z, double *w, const double *V, int n
   int rc;
   if ((rc = poisson_apply_dev(c, z, w))) return rc;
   const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) k_multidot<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else if (nv <= 8) k_multidot<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else if (nv <= 16) k_multidot<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else k_multidot<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  if (nv <= 4) c->launches++, k_multidot<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else if (nv <= 8) c->launches++, k_multidot<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else if (nv <= 16) c->launches++, k_multidot<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
+  else c->launches++, k_multidot<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
   if ((rc = check_launch(c, "k_multidot"))) return rc;
   return finish_rows(c, nv + 1, kg, h);
 }
@@ -501,10 +501,10 @@ static int apply_dots(Ctx *c, const double *z, double *w, const double *V, int n
 static int update_dots(Ctx *c, const double *V, int nv, const double *hdev, double *w, double *out) {
   const int kg = kry_grid(c);
   const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) k_update_dots<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else if (nv <= 8) k_update_dots<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else if (nv <= 16) k_update_dots<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else k_update_dots<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  if (nv <= 4) c->launches++, k_update_dots<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else if (nv <= 8) c->launches++, k_update_dots<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else if (nv <= 16) c->launches++, k_update_dots<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
+  else c->launches++, k_update_dots<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
   int rc;
   if ((rc = check_launch(c, "k_update_dots"))) return rc;
   return finish_rows(c, nv + 1, kg, out);
@@ -515,11 +515,11 @@ static int update_scale(Ctx *c, const double *V, int nv, const double *hdev, con
                         double *out) {
   const int kg = kry_grid(c);
   const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) k_update_scale<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  else if (nv <= 8) k_update_scale<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  if (nv <= 4) c->launches++, k_update_scale<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  else if (nv <= 8) c->launches++, k_update_scale<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
   else if (nv <= 16)
-    k_update_scale<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  else k_update_scale<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+    c->launches++, k_update_scale<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
+  else c->launches++, k_update_scale<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
   return check_launch(c, "k_update_scale");
 }
 
@@ -546,7 +546,7 @@ static int residual(Ctx *c, const double *b, const double *x, double *r, double 
   if (c->ps.transpose) {
     int rc;
     if ((rc = poisson_apply_dev(c, x, r))) return rc;
-    k_sub_norm<<<kKryBlocks, 256, 0, c->stream>>>(c->g.N, b, r, c->red);
+    c->launches++, k_sub_norm<<<kKryBlocks, 256, 0, c->stream>>>(c->g.N, b, r, c->red);
     if ((rc = check_launch(c, "k_sub_norm"))) return rc;
     double rr;
     if ((rc = finish_rows(c, 1, kKryBlocks, &rr))) return rc;
@@ -559,9 +559,9 @@ static int residual(Ctx *c, const double *b, const double *x, double *r, double 
   int rc;
   if ((rc = ensure_red(c, nb + 64))) return rc;
   if (c->ps.nslot == 7)
-    k_residual_pt<7><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
+    c->launches++, k_residual_pt<7><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
   else
-    k_residual_pt<NSLOT><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
+    c->launches++, k_residual_pt<NSLOT><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
   if ((rc = check_launch(c, "k_residual_pt"))) return rc;
   double rr;
   if ((rc = reduce_sum(c, c->red, nb, &rr))) return rc;
@@ -623,11 +623,11 @@ int poisson_lhs(Ctx *c) {
     cudaMemsetAsync(P.r, 0, sizeof(double) * N, c->stream);
     cudaMemsetAsync(P.t, 0, sizeof(double) * N, c->stream);
   }
-  k_poisson_coef<<<nblocks(N, 128), 128, 0, c->stream>>>(g, metrics(c), c->nv, P.coef, P.fluid);
+  c->launches++, k_poisson_coef<<<nblocks(N, 128), 128, 0, c->stream>>>(g, metrics(c), c->nv, P.coef, P.fluid);
   if ((rc = check_launch(c, "k_poisson_coef"))) return rc;
   // fluid-cell count and sum of aj (Remove_Nullspace / Remove_Nullspace_Scale)
   if ((rc = ensure_red(c, 2 * kRedBlocks + 64))) return rc;
-  k_count_fluid<<<kRedBlocks, 256, 0, c->stream>>>(N, P.fluid, c->f[VFS_AJ][0], c->red);
+  c->launches++, k_count_fluid<<<kRedBlocks, 256, 0, c->stream>>>(N, P.fluid, c->f[VFS_AJ][0], c->red);
   if ((rc = check_launch(c, "k_count_fluid"))) return rc;
   double cnt = 0, saj = 0;
   if ((rc = reduce_sum(c, c->red, kRedBlocks, &cnt))) return rc;
@@ -635,7 +635,7 @@ int poisson_lhs(Ctx *c) {
   P.nfluid = (long long)llround(cnt);
   P.sum_aj = saj;
   // the apply reads only slots CP..BP when no row has a cross-derivative entry
-  k_count_cross<<<kRedBlocks, 256, 0, c->stream>>>(N, P.coef, c->red);
+  c->launches++, k_count_cross<<<kRedBlocks, 256, 0, c->stream>>>(N, P.coef, c->red);
   if ((rc = check_launch(c, "k_count_cross"))) return rc;
   double ncross = 0;
   if ((rc = reduce_sum(c, c->red, kRedBlocks, &ncross))) return rc;
@@ -708,7 +708,7 @@ static int sum_fluid(Ctx *c, const double *a, double *out) {
   int rc;
   const int nb = (int)nblocks(c->g.N, 256);
   if ((rc = ensure_red(c, nb + 64))) return rc;
-  k_sum_fluid<<<nb, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, a, c->red);
+  c->launches++, k_sum_fluid<<<nb, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, a, c->red);
   if ((rc = check_launch(c, "k_sum_fluid"))) return rc;
   return reduce_sum(c, c->red, nb, out);
 }
@@ -742,7 +742,7 @@ int volume_flux(Ctx *c) {
     if (c->tape && (rc = tape_vflux(c))) return rc;
     return volume_flux_ibm(c, nullptr, nullptr);
   }
-  k_volume_flux_blocked<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->nv, field3(c, VFS_UCONT));
+  c->launches++, k_volume_flux_blocked<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->nv, field3(c, VFS_UCONT));
   return check_launch(c, "k_volume_flux_blocked");
 }
 
@@ -750,7 +750,7 @@ int volume_flux(Ctx *c) {
 int poisson_rhs_local(Ctx *c) {
   int rc;
   if ((rc = periodic_copy3(c, field3(c, VFS_UCONT)))) return rc;
-  k_poisson_rhs<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->ps.fluid,
+  c->launches++, k_poisson_rhs<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->ps.fluid,
                                                              c->f[VFS_B][0]);
   return check_launch(c, "k_poisson_rhs");
 }
@@ -761,7 +761,7 @@ int poisson_rhs(Ctx *c) {
   if ((rc = poisson_rhs_local(c))) return rc;
   double sum = 0;
   if ((rc = sum_fluid(c, b, &sum))) return rc;
-  k_shift_scaled<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->ps.fluid, c->f[VFS_AJ][0], sum,
+  c->launches++, k_shift_scaled<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->ps.fluid, c->f[VFS_AJ][0], sum,
                                                              c->ps.sum_aj, b);
   return check_launch(c, "k_shift_scaled");
 }
@@ -844,7 +844,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   if (warm) {
     const int nb = (int)nblocks(N, 256);
     if ((rc = ensure_red(c, nb + 64))) return rc;
-    k_guess<<<nb, 256, 0, c->stream>>>(N, P.fluid, b, x, c->red);
+    c->launches++, k_guess<<<nb, 256, 0, c->stream>>>(N, P.fluid, b, x, c->red);
     if ((rc = check_launch(c, "k_guess"))) return rc;
     double bb = 0;
     if ((rc = reduce_sum(c, c->red, nb, &bb))) return rc;
@@ -869,7 +869,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
     fresh = false;
     const double beta = rnorm;
     if (beta <= tol) { conv = true; break; }
-    k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.r, 1.0 / beta, P.V);
+    c->launches++, k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.r, 1.0 / beta, P.V);
     if ((rc = check_launch(c, "k_scale_copy"))) return rc;
     std::fill(gv.begin(), gv.end(), 0.0);
     gv[0] = beta;
@@ -912,7 +912,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
           if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h3.data()))) return rc;
           hn = sqrt(std::max(h3[nv], 0.0));
           if (hn > 0) {
-            k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, 1.0 / hn, Vn);
+            c->launches++, k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, 1.0 / hn, Vn);
             if ((rc = check_launch(c, "k_scale_copy"))) return rc;
           }
         }
@@ -944,7 +944,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       y[t] = sum / H[t * m + t];
     }
     upload_h(c, y.data(), jdone, P.hdev);
-    k_lincomb_add<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z, jdone, P.hdev, x);
+    c->launches++, k_lincomb_add<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z, jdone, P.hdev, x);
     if ((rc = check_launch(c, "k_lincomb_add"))) return rc;
     if (rnorm <= tol) {
       // confirm with the true residual
@@ -957,7 +957,7 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   double sum = 0;
   if ((rc = sum_fluid(c, x, &sum))) return rc;
   const double val = -sum / (double)P.nfluid;
-  k_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.fluid, val, x);
+  c->launches++, k_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.fluid, val, x);
   if ((rc = check_launch(c, "k_shift"))) return rc;
   // Convert_Phi2_Phi: periodic ghosts take their images (x is 0 elsewhere off-fluid)
   if ((rc = periodic_copy1(c, x))) return rc;
@@ -989,7 +989,7 @@ __global__ void k_update_pressure(Grid g, const uint8_t *__restrict__ nv, const 
 
 int update_pressure(Ctx *c) {
   int rc;
-  k_update_pressure<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->nv, c->f[VFS_PHI][0], c->f[VFS_P][0]);
+  c->launches++, k_update_pressure<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, c->nv, c->f[VFS_PHI][0], c->f[VFS_P][0]);
   if ((rc = check_launch(c, "k_update_pressure"))) return rc;
   if ((rc = periodic_copy1(c, c->f[VFS_P][0]))) return rc;
   return periodic_copy1(c, c->f[VFS_PHI][0]);
@@ -1082,11 +1082,11 @@ __global__ void k_periodic_copy_comp(Grid g, V3 u) {
 
 int projection(Ctx *c) {
   int rc;
-  k_projection<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, c->f[VFS_PHI][0],
+  c->launches++, k_projection<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, c->f[VFS_PHI][0],
                                                            field3(c, VFS_UCONT));
   if ((rc = check_launch(c, "k_projection"))) return rc;
   if (c->g.iper || c->g.jper || c->g.kper) {
-    k_periodic_copy_comp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
+    c->launches++, k_periodic_copy_comp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
     if ((rc = check_launch(c, "k_periodic_copy_comp"))) return rc;
   }
   return contra2cart(c);
@@ -1151,8 +1151,8 @@ int divergence(Ctx *c, double *maxdiv) {
   int rc;
   const int nb = (int)nblocks(c->g.N, 256);
   if ((rc = ensure_red(c, nb + 64))) return rc;
-  k_divergence<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->f[VFS_AJ][0], c->nv, c->red + 64);
-  k_max_parts<<<1, 1024, 0, c->stream>>>(c->red + 64, nb, c->red);
+  c->launches++, k_divergence<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->f[VFS_AJ][0], c->nv, c->red + 64);
+  c->launches++, k_max_parts<<<1, 1024, 0, c->stream>>>(c->red + 64, nb, c->red);
   if ((rc = check_launch(c, "k_divergence"))) return rc;
   cudaMemcpyAsync(c->red_host, c->red, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "divergence sync failed");
@@ -1196,7 +1196,7 @@ int run_kernel(Ctx *c, int which, int reps) {
         break;
       }
       case 6:
-        k_projection<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->f[VFS_PHI][0], field3(c, VFS_UCONT));
+        c->launches++, k_projection<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->f[VFS_PHI][0], field3(c, VFS_UCONT));
         break;
       default: return set_err(c, VFS_ERR_INVALID, "run_kernel: unknown kernel id");
     }
