@@ -21,8 +21,10 @@ independent replicas (weak scaling); the step time is the maximum over ranks.
 
 `--impl reference` times the reference's own CPU code (oracle/_ref: its momentum.c,
 rhs.c, poisson.c ... under the single-rank shim; the Poisson solve, HYPRE in the
-reference, is scipy GMRES with an incomplete-LU preconditioner on the reference's own
-matrix) on a bounded sample of the workload and scales it to the full grid.
+reference, is FGMRES with a geometric multigrid preconditioner on the reference's own
+matrix, set up outside the step) on a 64x48x64 sample of the workload, and extrapolates
+each phase (momentum, Poisson, correction) to the full grid with an exponent fitted over
+three sample sizes; the line says "extrapolated" and carries the fit.
 """
 import argparse
 import ctypes
@@ -251,57 +253,80 @@ def roofline_probe(ctx, torch, reps=20):
 
 
 # ------------------------------------------------------------------ reference arm
-def reference_sample(nx=32, ny=24, nz=32, seed=0):
-    """One reference step (oracle/_ref) on a 32x24x32 sample of the workload, one host
-    thread; returns (ms for the sample, cells in the sample)."""
+# The reference's own CPU code (oracle/_ref) cannot run the 256x192x256 workload within a
+# bench run (a step there takes a few minutes on one core), so it runs on samples of the
+# workload, grids of the same domain and bodies with fewer cells, and the step time is
+# extrapolated phase by phase: each phase's cost is fitted as t = c * cells^a over three
+# sample sizes, and the sample's phase times are scaled by (cells ratio)^a.
+REF_SIZES = ((32, 24, 32), (64, 48, 64), (128, 96, 128))
+REF_STEP_SIZE = (64, 48, 64)
+PHASES = ("momentum", "poisson", "correction")
+
+
+class ReferenceSample:
+    """The reference's step (oracle/_ref via oracle.steps) on an nx x ny x nz sample of the
+    workload; the Poisson set-up (PoissonLHSNew and the solver's set-up) is done here,
+    outside the timed steps, as HYPRE's set-up runs at PoissonLHSNew time
+    (poisson_hypre.c:527)."""
+
+    def __init__(self, nx, ny, nz, seed=0):
+        from oracle import ref, steps
+        from vfs_b200 import cases
+        case = make_case(nx, ny, nz)
+        R = ref.Reference(case)
+        m = R.metrics()
+        u = turbulent_like(case, seed=seed)
+        uc = cases.ucont_from_ucat(case, u, m)
+        for n in ("Ucont", "lUcont", "Ucont_o", "lUcont_o"):
+            R.set(n, uc)
+        for n in ("Ucat", "lUcat", "lUcat_old"):
+            R.set(n, u)
+        R.set_inflow_plane(u[1])
+        ref.set_global("inlet_flux", R.inlet_area())
+        self.R = R
+        self.cells = nx * ny * nz
+        # the workload's Poisson tolerance
+        self.stepper = steps.ReferenceStepper(R, rtol=1e-10)
+
+    def step(self):
+        return self.stepper.step()
+
+    def close(self):
+        self.R.close()
+
+
+def reference_fit(steps_per_size=1):
+    """Phase times of one reference step at each of REF_SIZES (after one untimed step)
+    and the fitted exponent a of t = c * cells^a for every phase."""
     from threadpoolctl import threadpool_limits
+    rows = []
     with threadpool_limits(limits=1), quiet_stdout():
-        return _reference_sample(nx, ny, nz, seed)
+        for (nx, ny, nz) in REF_SIZES:
+            S = ReferenceSample(nx, ny, nz)
+            S.step()
+            t = [S.step() for _ in range(steps_per_size)]
+            rows.append((S.cells, {p: float(np.median([x[p] for x in t])) for p in PHASES}))
+            S.close()
+    cells = np.log([r[0] for r in rows])
+    expo = {}
+    for p in PHASES:
+        tp = np.log([max(r[1][p], 1e-9) for r in rows])
+        expo[p] = float(np.polyfit(cells, tp, 1)[0])
+    return rows, expo
 
 
-def _reference_sample(nx, ny, nz, seed):
-    import scipy.sparse as sp
-    import scipy.sparse.linalg as spla
-    from oracle import ref
-    from vfs_b200 import cases
-    case = make_case(nx, ny, nz)
-    case.dt = 5e-4
-    R = ref.Reference(case)
-    m = R.metrics()
-    u = turbulent_like(case, seed=seed)
-    uc = cases.ucont_from_ucat(case, u, m)
-    for n in ("Ucont", "lUcont", "Ucont_o", "lUcont_o"):
-        R.set(n, uc)
-    for n in ("Ucat", "lUcat", "lUcat_old"):
-        R.set(n, u)
-    R.set_inflow_plane(u[1])
-    ref.set_global("inlet_flux", R.inlet_area())
-    R.call("ref_poisson_lhs")   # first-step set-up, outside the timed sample
-    t0 = time.perf_counter()
-    R.call("ref_ib_bc")
-    R.set("Ucont", R.get("lUcont"))
-    R.call("ref_calc_k_flux")
-    R.call("ref_pressure_gradient")
-    R.call("ref_runge_kutta")
-    R.volume_flux()
-    b = R.poisson_rhs_hypre()
-    rp, col, val = R.poisson_csr()
-    n = len(rp) - 1
-    A = sp.csr_matrix((val, col, rp), shape=(n, n))
-    ilu = spla.spilu(A.tocsc(), drop_tol=1e-4, fill_factor=10)
-    M = spla.LinearOperator((n, n), ilu.solve)
-    x, info = spla.gmres(A, b, M=M, rtol=1e-10, restart=50, maxiter=200)
-    x = R.remove_nullspace(x)
-    R.set("Phi2", x)
-    R.call("ref_convert_phi2_phi")
-    R.call("ref_update_pressure")
-    R.call("ref_projection")
-    R.call("ref_ib_bc")
-    R.set("Ucont", R.get("lUcont"))
-    R.call("ref_contra2cart")
-    ms = (time.perf_counter() - t0) * 1e3
-    R.close()
-    return ms, nx * ny * nz
+def extrapolate(phase_s, cells, expo, full=NX * NY * NZ):
+    """ms of a full-size step from a sample's phase times and the fitted exponents."""
+    return 1e3 * sum(phase_s[p] * (full / cells) ** expo[p] for p in PHASES)
+
+
+def fit_note(rows, expo):
+    return ("extrapolated to 256x192x256 phase by phase: t = c * cells^a fitted over one reference step at "
+            "each of %s (a: %s); Poisson (HYPRE in the reference) by FGMRES with a geometric multigrid "
+            "preconditioner on the reference's own matrix, rtol 1e-10, its set-up outside the step; one host "
+            "thread (the oracle is single-rank)" % (
+                ", ".join("%dx%dx%d" % s for s in REF_SIZES),
+                ", ".join("%s %.2f" % (p, expo[p]) for p in PHASES)))
 
 
 def reference_arm(args, rank, world):
@@ -311,21 +336,28 @@ def reference_arm(args, rank, world):
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvfsref.so was not built"}))
         return
-    scale = (NX * NY * NZ)
+    from threadpoolctl import threadpool_limits
+    rows, expo = reference_fit()
     samples = []
-    for s in range(args.warmup + args.steps):
-        ms, cells = reference_sample(seed=s)
-        if s >= args.warmup:
-            samples.append(ms * scale / cells)
+    with threadpool_limits(limits=1), quiet_stdout():
+        S = ReferenceSample(*REF_STEP_SIZE)
+        for s in range(args.warmup + args.steps):
+            t = S.step()
+            if s >= args.warmup:
+                samples.append(extrapolate(t, S.cells, expo))
+        S.close()
     v = float(np.mean(samples))
+    sample = ("each step: one reference step (oracle/_ref, the reference's own momentum.c, rhs.c, poisson.c, "
+              "bcs.c ... under the single-rank shim) on a %dx%dx%d sample of the workload, %s"
+              % (REF_STEP_SIZE + (fit_note(rows, expo),)))
     out = {"metric": METRIC, "value": round(v, 3), "unit": "ms/step", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-           "config": {"workload": WORKLOAD, "precision": "reference FP64 CPU"},
+           "config": {"workload": WORKLOAD, "precision": "reference FP64 CPU", "extrapolated": True},
            "cpu_baseline": {"value": round(v, 3), "unit": "ms/step", "cores": 1, "kind": "reference",
-                            "sample": "one reference step on a 32x24x32-cell sample of the same workload, "
-                                      "scaled by the cell ratio (x512); Poisson solve by scipy GMRES+ILU "
-                                      "(HYPRE is not in the image); one host thread"},
+                            "sample": sample, "extrapolated": True,
+                            "fit": {"sizes": ["%dx%dx%d" % s for s in REF_SIZES],
+                                    "phase_seconds": [r[1] for r in rows], "exponent": expo}},
            "e2e": {"value": round(v, 3), "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -541,14 +573,14 @@ def main():
             try:
                 from oracle import ref
                 if ref.available():
-                    runs = [reference_sample(seed=s) for s in range(5)]
-                    ms_ref = float(np.median([r[0] for r in runs]))
-                    cells = runs[0][1]
-                    cpu = {"value": round(ms_ref * ncell / cells, 1), "unit": "ms/step", "cores": 1,
-                           "kind": "reference",
-                           "sample": "median of 5 reference steps (oracle/_ref) on a 32x24x32-cell sample "
-                                     "of this workload, scaled by the cell ratio (x512); Poisson by scipy "
-                                     "GMRES+ILU; one host thread"}
+                    rows, expo = reference_fit()
+                    cells, big = rows[-1]
+                    cpu = {"value": round(extrapolate(big, cells, expo), 1), "unit": "ms/step", "cores": 1,
+                           "kind": "reference", "extrapolated": True,
+                           "sample": "one reference step (oracle/_ref) on the 128x96x128 sample of this "
+                                     "workload, " + fit_note(rows, expo),
+                           "fit": {"sizes": ["%dx%dx%d" % s for s in REF_SIZES],
+                                   "phase_seconds": [r[1] for r in rows], "exponent": expo}}
             except Exception as e:  # the baseline is reported, never required
                 cpu = {"value": None, "unit": "ms/step", "cores": 1, "kind": "reference",
                        "sample": "failed: %s" % e}

@@ -321,10 +321,10 @@ int vfs_get_stream(vfs_ctx *ctx, void **stream);
  * synchronisation, on the context's current fields: 0 face fluxes of Formfunction_2
  * (three-kernel form), 1 its Fp, 2 its RHS projection, 3 FP64 Poisson operator apply,
  * 4 FP32 fine-level zebra line sweep (both colours), 5 the same in FP64, 6 Projection,
- * 7 Formfunction_2 as one fused kernel, 8 Formfunction_2 as a step runs it (kernels
- * 0-2), 9 one multigrid V-cycle of the preconditioner (FP32) applied to VFS_B, 10 the
- * same in FP64.  Kernels 7 and 8 add into RHS as vfs_formfunction2 does.  For timing
- * only. */
+ * 7 Formfunction_2 as three kernels (0-2), 8 Formfunction_2 as a step runs it, 9 one
+ * multigrid V-cycle of the preconditioner (FP32) applied to VFS_B, 10 the same in FP64,
+ * 11 Formfunction_2 as one k-marching kernel.  Kernels 7, 8 and 11 add into RHS as
+ * vfs_formfunction2 does.  For timing only. */
 int vfs_run_kernel(vfs_ctx *ctx, int which, int reps);
 
 /* ------------------------------------------------------------------ adjoint

@@ -292,16 +292,18 @@ def test_form_metrics_bitwise(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(CASES))
-def test_fused_formfunction2_matches_three_kernel_form(name):
-    """The single-kernel Formfunction_2 (diagnostic id 7) against the form a step runs
-    (id 8): same inputs, identical right-hand sides."""
+def test_formfunction2_forms_agree(name):
+    """The three forms of Formfunction_2 on the same inputs: the three-kernel form
+    (diagnostic id 7), the one-pass k-marching kernel (id 11) and the form a step runs
+    (id 8) give identical right-hand sides."""
     case, (R, ctx) = _pair(name)
     ctx.contra2cart()
     rhs0 = np.random.Generator(np.random.Philox(9)).standard_normal(R.shape + (3,))
     ctx.set_field(vfs.RHS, rhs0)
-    ctx.run_kernel(8, 1)
-    want = ctx.get_field(vfs.RHS)
-    ctx.set_field(vfs.RHS, rhs0)
     ctx.run_kernel(7, 1)
-    np.testing.assert_array_equal(ctx.get_field(vfs.RHS), want)
+    want = ctx.get_field(vfs.RHS)
+    for kid in (11, 8):
+        ctx.set_field(vfs.RHS, rhs0)
+        ctx.run_kernel(kid, 1)
+        np.testing.assert_array_equal(ctx.get_field(vfs.RHS), want, err_msg="kernel id %d" % kid)
     R.close()

@@ -204,7 +204,8 @@ int periodic_copy1(Ctx *c, double *s);
 int contra2cart(Ctx *c);
 int solid_list(Ctx *c);
 int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff);
-int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff);
+int formfunction2_split(Ctx *c, double scale, bool rk_stage, double rk_coeff);
+int formfunction2_onepass(Ctx *c, double scale, bool rk_stage, double rk_coeff);
 int pressure_gradient(Ctx *c);
 int calc_k_flux(Ctx *c, double *flux);
 int runge_kutta(Ctx *c);

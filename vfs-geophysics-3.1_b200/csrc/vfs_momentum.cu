@@ -418,10 +418,10 @@ __device__ __forceinline__ void flux_i(const Grid &g, const Metrics &m, CV3 uc, 
   const double nu = 1. / g.ren;
   const bool les = g.les != 0;
   (void)sx; (void)sy; (void)sz; (void)mx; (void)my; (void)mz;
-  const double ajc = m.iaj[p];
-  const double csi0 = m.icsi.x[p], csi1 = m.icsi.y[p], csi2 = m.icsi.z[p];
-  const double eta0 = m.ieta.x[p], eta1 = m.ieta.y[p], eta2 = m.ieta.z[p];
-  const double zet0 = m.izet.x[p], zet1 = m.izet.y[p], zet2 = m.izet.z[p];
+  const double ajc = __ldcs(m.iaj + p);
+  const double csi0 = __ldcs(m.icsi.x + p), csi1 = __ldcs(m.icsi.y + p), csi2 = __ldcs(m.icsi.z + p);
+  const double eta0 = __ldcs(m.ieta.x + p), eta1 = __ldcs(m.ieta.y + p), eta2 = __ldcs(m.ieta.z + p);
+  const double zet0 = __ldcs(m.izet.x + p), zet1 = __ldcs(m.izet.y + p), zet2 = __ldcs(m.izet.z + p);
   double dc[3], de[3], dz[3];
   dc[0] = u.x[p + sx] - u.x[p]; dc[1] = u.y[p + sx] - u.y[p]; dc[2] = u.z[p + sx] - u.z[p];
   cross_diff(u, p, p + sx, p + sy, p + sy + sx, p - sy, p - sy + sx,
@@ -491,10 +491,10 @@ __device__ __forceinline__ void flux_j(const Grid &g, const Metrics &m, CV3 uc, 
   const double nu = 1. / g.ren;
   const bool les = g.les != 0;
   (void)sx; (void)sy; (void)sz; (void)mx; (void)my; (void)mz;
-  const double ajc = m.jaj[p];
-  const double csi0 = m.jcsi.x[p], csi1 = m.jcsi.y[p], csi2 = m.jcsi.z[p];
-  const double eta0 = m.jeta.x[p], eta1 = m.jeta.y[p], eta2 = m.jeta.z[p];
-  const double zet0 = m.jzet.x[p], zet1 = m.jzet.y[p], zet2 = m.jzet.z[p];
+  const double ajc = __ldcs(m.jaj + p);
+  const double csi0 = __ldcs(m.jcsi.x + p), csi1 = __ldcs(m.jcsi.y + p), csi2 = __ldcs(m.jcsi.z + p);
+  const double eta0 = __ldcs(m.jeta.x + p), eta1 = __ldcs(m.jeta.y + p), eta2 = __ldcs(m.jeta.z + p);
+  const double zet0 = __ldcs(m.jzet.x + p), zet1 = __ldcs(m.jzet.y + p), zet2 = __ldcs(m.jzet.z + p);
   double dc[3], de[3], dz[3];
   cross_diff(u, p, p + sy, p + sx, p + sy + sx, p - sx, p + sy - sx,
              !kReg && (nv[p + sx] > 0 || nv[p + sy + sx] > 0),
@@ -564,10 +564,10 @@ __device__ __forceinline__ void flux_k(const Grid &g, const Metrics &m, CV3 uc, 
   const double nu = 1. / g.ren;
   const bool les = g.les != 0;
   (void)sx; (void)sy; (void)sz; (void)mx; (void)my; (void)mz;
-  const double ajc = m.kaj[p];
-  const double csi0 = m.kcsi.x[p], csi1 = m.kcsi.y[p], csi2 = m.kcsi.z[p];
-  const double eta0 = m.keta.x[p], eta1 = m.keta.y[p], eta2 = m.keta.z[p];
-  const double zet0 = m.kzet.x[p], zet1 = m.kzet.y[p], zet2 = m.kzet.z[p];
+  const double ajc = __ldcs(m.kaj + p);
+  const double csi0 = __ldcs(m.kcsi.x + p), csi1 = __ldcs(m.kcsi.y + p), csi2 = __ldcs(m.kcsi.z + p);
+  const double eta0 = __ldcs(m.keta.x + p), eta1 = __ldcs(m.keta.y + p), eta2 = __ldcs(m.keta.z + p);
+  const double zet0 = __ldcs(m.kzet.x + p), zet1 = __ldcs(m.kzet.y + p), zet2 = __ldcs(m.kzet.z + p);
   double dc[3], de[3], dz[3];
   cross_diff(u, p, p + sz, p + sx, p + sz + sx, p - sx, p + sz - sx,
              !kReg && (nv[p + sx] > 0 || nv[p + sz + sx] > 0),
@@ -923,31 +923,7 @@ __global__ void k_rhs(Grid g, Metrics m, const uint8_t *__restrict__ nv, const d
   rhs_point(g, m, nv, p, i, j, k, ghost, F, scale, rhs, rk, a, dP, pu, ucont);
 }
 
-// ------------------------------------------------------------------ fused Formfunction_2
-// One kernel for the face fluxes, Fp and the right-hand side (with the RK stage update):
-// a thread block owns an FTI x FTJ tile of cells in (i, j) and marches through FKC planes
-// of k.  For the current plane kc it computes, into shared memory, the i-face fluxes
-// (faces i0-2 .. i0+FTI+1) and j-face fluxes of the tile extended by one cell on the high
-// side, plus the k-face fluxes of plane kc+1 (a ring of four k-face planes kc-2 .. kc+1);
-// then Fp of the extended tile at plane kc (a ring of two Fp planes); then the right-hand
-// side of plane kc-1.  Only the inputs (velocities, metrics, nvert, nu_t) and the outputs
-// travel through HBM.  Neighbouring tiles read Ucont in their halos, so in RK mode the
-// kernel writes only the right-hand side and k_rk_update applies the stage update after.  Face indices are handled unwrapped within the tile: on a periodic
-// direction a face or cell outside 1..m-2 is computed at its periodic image, which is the
-// value the reference reads there.  Every expression is the one of the three-kernel path,
-// so the results are identical.
-constexpr int FTI = 32, FTJ = 8, FKC = 16;
-constexpr int FEI = FTI + 1, FEJ = FTJ + 1, FE = FEI * FEJ;
-constexpr int FAI = FTI + 4, FBJ = FTJ + 4;
-constexpr int FNI = FAI * FEJ, FNJ = FEI * FBJ;
-constexpr int kFF2Threads = 256;
-struct FF2Smem {
-  double ifl[6][FNI];      // i-faces of plane kc: div x,y,z then visc x,y,z
-  double jfl[6][FNJ];      // j-faces of plane kc
-  double kfl[4][6][FE];    // k-faces, ring over planes kc-2 .. kc+1
-  double fp[2][3][FE];     // Fp, ring over planes kc-1, kc
-};
-
+// ------------------------------------------------------------------ Formfunction_2, one pass
 // Image of a cell index (1..m-2 unchanged; m-1 -> 1 on a periodic direction), -1 if none.
 __device__ __forceinline__ int cell_image(int u, int m, int per) {
   if (u >= 1 && u <= m - 2) return u;
@@ -958,118 +934,6 @@ __device__ __forceinline__ int cell_image(int u, int m, int per) {
 __device__ __forceinline__ int face_image_or_none(int u, int m, int per) {
   const int f = face_image(u, m, per);
   return (f >= 0 && f <= m - 2) ? f : -1;
-}
-
-struct SmemFaces {
-  const FF2Smem *S;
-  int ei, ej, kc;
-  __device__ __forceinline__ double get(int dir, int q, int off) const {
-    if (dir == 0) return S->ifl[q][ej * FAI + ei + off + 2];
-    if (dir == 1) return S->jfl[q][(ej + off + 2) * FEI + ei];
-    return S->kfl[(kc + off + 4) & 3][q][ej * FEI + ei];
-  }
-  __device__ __forceinline__ double d(int dir, int c, int off) const { return get(dir, c, off); }
-  __device__ __forceinline__ double v(int dir, int c, int off) const { return get(dir, 3 + c, off); }
-};
-struct SmemFp {
-  const FF2Smem *S;
-  int t, s0, s1;
-  __device__ __forceinline__ double fp(int w, int c) const {
-    if (w == 0) return S->fp[s0][c][t];
-    if (w == 1) return S->fp[s0][c][t + 1];
-    if (w == 2) return S->fp[s0][c][t + FEI];
-    return S->fp[s1][c][t];
-  }
-};
-
-__device__ __forceinline__ void ff2_kfaces(const Grid &g, const Metrics &m, CV3 uc, CV3 u,
-                                           const uint8_t *__restrict__ nv, const double *__restrict__ nut,
-                                           FF2Smem &S, int i0, int j0, int kf) {
-  const int kimg = face_image_or_none(kf, g.mz, g.kper);
-  double (*dst)[FE] = S.kfl[(kf + 4) & 3];
-  for (int t = threadIdx.x; t < FE; t += blockDim.x) {
-    const int ei = t % FEI, ej = t / FEI;
-    const int ii = cell_image(i0 + ei, g.mx, g.iper), jj = cell_image(j0 + ej, g.my, g.jper);
-    double d[3] = {0, 0, 0}, v[3] = {0, 0, 0};
-    if (ii >= 0 && jj >= 0 && kimg >= 0) flux_k(g, m, uc, u, nv, nut, lidx(g, ii, jj, kimg), ii, jj, kimg, d, v);
-    dst[0][t] = d[0]; dst[1][t] = d[1]; dst[2][t] = d[2];
-    dst[3][t] = v[0]; dst[4][t] = v[1]; dst[5][t] = v[2];
-  }
-}
-
-__global__ void __launch_bounds__(kFF2Threads) k_ff2_fused(Grid g, Metrics m, CV3 uc, CV3 u,
-                                                           const uint8_t *__restrict__ nv,
-                                                           const double *__restrict__ nut, double scale, V3 rhs,
-                                                           int rk, double a, CV3 dP, CV3 pu) {
-  extern __shared__ __align__(16) unsigned char ff2_raw[];
-  FF2Smem &S = *reinterpret_cast<FF2Smem *>(ff2_raw);
-  const int i0 = 1 + blockIdx.x * FTI, j0 = 1 + blockIdx.y * FTJ, kb = 1 + blockIdx.z * FKC;
-  const int ke = min(kb + FKC, g.mz - 1);  // output planes kb .. ke-1
-  for (int kf = kb - 2; kf <= kb; kf++) ff2_kfaces(g, m, uc, u, nv, nut, S, i0, j0, kf);
-  for (int kc = kb; kc <= ke; kc++) {
-    const int kimg = cell_image(kc, g.mz, g.kper);
-    // i-faces and j-faces of plane kc, k-faces of plane kc+1
-    for (int t = threadIdx.x; t < FNI; t += blockDim.x) {
-      const int a_ = t % FAI, ej = t / FAI;
-      const int fi = face_image_or_none(i0 - 2 + a_, g.mx, g.iper), jj = cell_image(j0 + ej, g.my, g.jper);
-      double d[3] = {0, 0, 0}, v[3] = {0, 0, 0};
-      if (fi >= 0 && jj >= 0 && kimg >= 0) flux_i(g, m, uc, u, nv, nut, lidx(g, fi, jj, kimg), fi, jj, kimg, d, v);
-      S.ifl[0][t] = d[0]; S.ifl[1][t] = d[1]; S.ifl[2][t] = d[2];
-      S.ifl[3][t] = v[0]; S.ifl[4][t] = v[1]; S.ifl[5][t] = v[2];
-    }
-    for (int t = threadIdx.x; t < FNJ; t += blockDim.x) {
-      const int ei = t % FEI, b_ = t / FEI;
-      const int ii = cell_image(i0 + ei, g.mx, g.iper), fj = face_image_or_none(j0 - 2 + b_, g.my, g.jper);
-      double d[3] = {0, 0, 0}, v[3] = {0, 0, 0};
-      if (ii >= 0 && fj >= 0 && kimg >= 0) flux_j(g, m, uc, u, nv, nut, lidx(g, ii, fj, kimg), ii, fj, kimg, d, v);
-      S.jfl[0][t] = d[0]; S.jfl[1][t] = d[1]; S.jfl[2][t] = d[2];
-      S.jfl[3][t] = v[0]; S.jfl[4][t] = v[1]; S.jfl[5][t] = v[2];
-    }
-    ff2_kfaces(g, m, uc, u, nv, nut, S, i0, j0, kc + 1);
-    __syncthreads();
-    // Fp of the extended tile at plane kc
-    for (int t = threadIdx.x; t < FE; t += blockDim.x) {
-      const int ei = t % FEI, ej = t / FEI;
-      const int ii = cell_image(i0 + ei, g.mx, g.iper), jj = cell_image(j0 + ej, g.my, g.jper);
-      double fpv[3] = {0, 0, 0};
-      if (ii >= 0 && jj >= 0 && kimg >= 0) {
-        SmemFaces F;
-        F.S = &S; F.ei = ei; F.ej = ej; F.kc = kc;
-        fp_cell(g, nv, lidx(g, ii, jj, kimg), ii, jj, kimg, F, fpv);
-      }
-      S.fp[kc & 1][0][t] = fpv[0]; S.fp[kc & 1][1][t] = fpv[1]; S.fp[kc & 1][2][t] = fpv[2];
-    }
-    __syncthreads();
-    // right-hand side of plane kc-1
-    if (kc > kb) {
-      const int k = kc - 1;
-      for (int t = threadIdx.x; t < FTI * FTJ; t += blockDim.x) {
-        const int oi = t % FTI, oj = t / FTI;
-        const int i = i0 + oi, j = j0 + oj;
-        if (i > g.mx - 2 || j > g.my - 2) continue;
-        SmemFp F;
-        F.S = &S; F.t = oj * FEI + oi; F.s0 = k & 1; F.s1 = kc & 1;
-        rhs_point(g, m, nv, lidx(g, i, j, k), i, j, k, false, F, scale, rhs, rk, a, dP, pu, V3{nullptr, nullptr, nullptr});
-      }
-    }
-  }
-}
-
-// Ghost points of the right-hand side (zero, and the stage update in RK mode).
-__global__ void k_rhs_ghosts(Grid g, Metrics m, const uint8_t *__restrict__ nv, double scale, V3 rhs, int rk,
-                             double a, CV3 dP, CV3 pu) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long ni = 2LL * g.my * g.mz, nj = 2LL * g.mx * g.mz, nk = 2LL * g.mx * g.my;
-  if (t >= ni + nj + nk) return;
-  long long r = t;
-  int i, j, k;
-  if (r < ni) { i = (r & 1) ? g.mx - 1 : 0; r >>= 1; j = (int)(r % g.my); k = (int)(r / g.my); }
-  else if ((r -= ni) < nj) { j = (r & 1) ? g.my - 1 : 0; r >>= 1; i = (int)(r % g.mx); k = (int)(r / g.mx); }
-  else { r -= nj; k = (r & 1) ? g.mz - 1 : 0; r >>= 1; i = (int)(r % g.mx); j = (int)(r / g.mx); }
-  GlobalFp F;  // unused for ghost points
-  F.f[0] = F.f[1] = F.f[2] = nullptr;
-  F.q[0] = F.q[1] = F.q[2] = F.q[3] = 0;
-  rhs_point(g, m, nv, lidx(g, i, j, k), i, j, k, true, F, scale, rhs, rk, a, dP, pu, V3{nullptr, nullptr, nullptr});
 }
 
 static FluxOut flux_out(Ctx *c, int d) {
@@ -1097,11 +961,10 @@ static int face_fluxes(Ctx *c) {
   return check_launch(c, "k_face_flux");
 }
 
-// Formfunction_2 as three kernels: face fluxes, Fp, right-hand side (with the RK stage
-// update).  The single-kernel form (formfunction2_fused) gives the same results; on the
-// B200 it is slower at this tile size (its block barriers leave it latency-bound), so
-// the step uses this one.
-int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
+// Formfunction_2 as three kernels: face fluxes (written to 18 arrays), Fp, right-hand
+// side (with the RK stage update in place).  Same results as the one-pass form; kept as
+// the reference form for the kernel-level comparison and the diagnostics entry point.
+int formfunction2_split(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   const Grid &g = c->g;
   int rc;
   V3 uc = field3(c, VFS_UCONT);
@@ -1117,33 +980,295 @@ int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   return check_launch(c, "k_rhs");
 }
 
-int formfunction2_fused(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
+// One-pass Formfunction_2: face fluxes, Fp and the right-hand side (with the RK stage
+// update) of a tile of cells in one kernel, with no face-flux array in HBM.
+//
+// A thread block of NW warps owns a strip of planes kb .. ke-1 of an (i, j) tile: lane l
+// of warp w is the column (i0 - 2 + l, j0 + w), and the block marches through the planes
+// in k.  Per plane kc every thread computes the fluxes of three faces of its column: the
+// i-face and j-face of plane kc and the k-face of plane kc+1 (the reference's three face
+// loops, momentum.c:671-1415, through the same flux_i/j/k code as the split form).  Then
+//  * the four i-faces Fp needs (offsets -2..1) come from the neighbouring lanes (warp
+//    shuffles), so a warp produces Fp for its lanes 2..30 and the right-hand side for
+//    lanes 2..29 (28 columns; neighbouring tiles overlap by four lanes);
+//  * the j-faces go through shared memory: each warp writes its row's, warps 0-2 also
+//    compute rows j0-2, j0-1 and j0+NW, and after one block barrier every row reads the
+//    four faces around it; rows j0 .. j0+NW-2 produce the right-hand side, row j0+NW-1
+//    only its Fp (the +j neighbour of the row below);
+//  * the k-faces stay in registers as a ring over planes kc-2 .. kc+1 (each k-face is
+//    computed once per column).
+// The contravariant projection of the right-hand side at a cell (momentum.c:1686-1900)
+// reads csi.Fp, eta.Fp and zet.Fp of the cell and of its +i, +j and +k neighbours; each
+// thread forms the three products once for its own cell (at plane kc, with the metrics of
+// its own DA point: on a periodic ghost plane the reference pairs the ghost's metric
+// with the Fp of the periodic image) and the right-hand side of plane kc-1 takes them
+// from the lane to the right (shuffle), the row above (shared memory, previous plane)
+// and its own registers.  Every expression is the split form's, in the same order, so
+// the results are identical bit for bit.
+//
+// In RK mode the stage update Ucont' = pUcont + a (RHS - dP) is written to `out` (not in
+// place: neighbouring tiles still read Ucont in their halos); the caller swaps the two
+// arrays.  Ghost points of the DA are written by k_ff2_ghosts.
+constexpr int kMarchLanes = 32;
+constexpr int kMarchOut = 28;  // right-hand-side columns per warp
+
+template <int NW>
+struct MarchSmem {
+  double jf[2][NW + 3][6][kMarchLanes];      // j-face d(3), v(3) of rows j0-2 .. j0+NW, two planes
+  double fi[NW][6][kMarchLanes + 3];         // i-face d(3), v(3) of each row, lanes at +2
+  double ay[2][NW][kMarchLanes];             // eta.Fp of rows j0 .. j0+NW-1, two planes
+  double kd[4][3][NW * kMarchLanes];         // k-face d of faces f (slot f & 3), per thread
+  double kv[4][3][NW * kMarchLanes];         // k-face v of faces f (slot f & 3), per thread
+};
+
+// Fluxes of one face; zero where the face does not exist.  reg: the point's whole flux
+// stencil is regular fluid interior (regular_faces), so the branch-free form applies.
+// True when the three faces of point (i, j, k) take the interior form (face_flux_point's
+// test); false for a point that does not exist.
+__device__ __forceinline__ bool point_regular(const Grid &g, const uint8_t *__restrict__ nv, int i, int j, int k) {
+  if (i < 2 || i > g.mx - 3 || j < 2 || j > g.my - 3 || k < 2 || k > g.mz - 3) return false;
+  return regular_faces(nv, lidx(g, i, j, k), g.mx, (long long)g.mx * g.my);
+}
+
+template <int D>
+__device__ __forceinline__ void march_face(const Grid &g, const Metrics &m, CV3 uc, CV3 u,
+                                           const uint8_t *__restrict__ nv, const double *__restrict__ nut, int i,
+                                           int j, int k, bool reg, double d[3], double v[3]) {
+  d[0] = d[1] = d[2] = 0.0;
+  v[0] = v[1] = v[2] = 0.0;
+  if (i < 0 || j < 0 || k < 0) return;
+  const long long p = lidx(g, i, j, k);
+  if (D == 0) {
+    if (reg) flux_i<true>(g, m, uc, u, nv, nut, p, i, j, k, d, v);
+    else flux_i(g, m, uc, u, nv, nut, p, i, j, k, d, v);
+  } else if (D == 1) {
+    if (reg) flux_j<true>(g, m, uc, u, nv, nut, p, i, j, k, d, v);
+    else flux_j(g, m, uc, u, nv, nut, p, i, j, k, d, v);
+  } else {
+    if (reg) flux_k<true>(g, m, uc, u, nv, nut, p, i, j, k, d, v);
+    else flux_k(g, m, uc, u, nv, nut, p, i, j, k, d, v);
+  }
+}
+
+// Face values by offset from the cell, for fp_cell (d at offsets -2..1, v at -1..0), all
+// from shared memory: the i- and j-faces of the plane, and the thread's own ring of
+// k-faces (face f in slot f & 3).
+template <int NW>
+struct MarchFaces {
+  const MarchSmem<NW> *S;
+  int b, w, lane, t, kc;
+  __device__ __forceinline__ double d(int dir, int c, int off) const {
+    if (dir == 0) return S->fi[w][c][lane + 2 + off];
+    if (dir == 1) return S->jf[b][w + 2 + off][c][lane];
+    return S->kd[(kc + off) & 3][c][t];
+  }
+  __device__ __forceinline__ double v(int dir, int c, int off) const {
+    if (dir == 0) return S->fi[w][3 + c][lane + 2 + off];
+    if (dir == 1) return S->jf[b][w + 2 + off][3 + c][lane];
+    return S->kv[(kc + off) & 3][c][t];
+  }
+};
+
+#ifndef VFS_MARCH_NW
+#define VFS_MARCH_NW 16
+#endif
+#ifndef VFS_MARCH_MINB
+#define VFS_MARCH_MINB 1
+#endif
+#ifndef VFS_MARCH_KC
+#define VFS_MARCH_KC 32
+#endif
+
+template <int NW>
+__global__ void __launch_bounds__(kMarchLanes * NW, VFS_MARCH_MINB)
+    k_ff2_march(Grid g, Metrics m, CV3 uc, CV3 u, const uint8_t *__restrict__ nv, const double *__restrict__ nut,
+                double scale, V3 rhs, int rk, double a, CV3 dP, CV3 pu, V3 out, int kc_per_block) {
+  extern __shared__ __align__(16) unsigned char march_raw[];
+  MarchSmem<NW> &S = *reinterpret_cast<MarchSmem<NW> *>(march_raw);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  const long long sy = mx, sz = (long long)mx * my;
+  const int i0 = 1 + blockIdx.x * kMarchOut, j0 = 1 + blockIdx.y * (NW - 1);
+  const int kb = 1 + blockIdx.z * kc_per_block;
+  // the lanes' i-face slots 0, 1 and 34 (offsets beyond the warp) are read only by lanes
+  // whose Fp is not used; clear them once so that nothing uninitialised is read
+  if (lane < 3) {
+    const int slot = lane < 2 ? lane : kMarchLanes + 2;
+    for (int c = 0; c < 6; c++) S.fi[w][c][slot] = 0.0;
+  }
+  const int ke = min(kb + kc_per_block, mz - 1);  // right-hand side of planes kb .. ke-1
+  const int uI = i0 - 2 + lane, vJ = j0 + w;
+  const int ii = cell_image(uI, mx, g.iper), jj = cell_image(vJ, my, g.jper);
+  const int fi = face_image_or_none(uI, mx, g.iper), fj = face_image_or_none(vJ, my, g.jper);
+  // the extra j-face row of warps 0-2
+  const int hv = w == 0 ? j0 - 2 : (w == 1 ? j0 - 1 : j0 + NW);
+  const int hr = w == 0 ? 0 : (w == 1 ? 1 : NW + 2);
+  const int hfj = face_image_or_none(hv, my, g.jper);
+  // the DA point of this column (for the metrics of the projection products), if any
+  const bool col_da = uI >= 0 && uI <= mx - 1 && vJ <= my - 1;
+  const bool out_col = lane >= 2 && lane < 2 + kMarchOut && w <= NW - 2 && uI <= mx - 2 && vJ <= my - 2;
+
+  // k-face ring (shared memory, own slots): warmed up with the faces kb-2 .. kb
+  const int t = w * kMarchLanes + lane;
+  for (int f = kb - 2; f <= kb; f++) {
+    double d[3], v[3];
+    const int fk = face_image_or_none(f, mz, g.kper);
+    march_face<2>(g, m, uc, u, nv, nut, ii, jj, (ii >= 0 && jj >= 0) ? fk : -1, point_regular(g, nv, ii, jj, fk), d,
+                  v);
+#pragma unroll
+    for (int c = 0; c < 3; c++) { S.kd[f & 3][c][t] = d[c]; S.kv[f & 3][c][t] = v[c]; }
+  }
+  // regularity of the point (ii, jj, kc), the point of the i- and j-faces of plane kc
+  // away from periodic images; the k-face of plane kc computed it one plane earlier
+  bool reg_ij = point_regular(g, nv, ii, jj, kb), reg_next = false;
+  double ax_prev = 0, ay_prev = 0, az_prev = 0;
+  for (int kc = kb; kc <= ke; kc++) {
+    const int b = kc & 1;
+    const int kimg = cell_image(kc, mz, g.kper);
+    // k-face of plane kc+1 into the ring
+    {
+      double d[3], v[3];
+      const int fk = face_image_or_none(kc + 1, mz, g.kper);
+      reg_next = point_regular(g, nv, ii, jj, fk);
+      march_face<2>(g, m, uc, u, nv, nut, ii, jj, (ii >= 0 && jj >= 0) ? fk : -1, reg_next, d, v);
+#pragma unroll
+      for (int c = 0; c < 3; c++) { S.kd[(kc + 1) & 3][c][t] = d[c]; S.kv[(kc + 1) & 3][c][t] = v[c]; }
+    }
+    // i-face and j-face of plane kc
+    {
+      double d[3], v[3];
+      const bool same = fi == ii && fj == jj && kimg == kc;
+      march_face<0>(g, m, uc, u, nv, nut, fi, jj, (fi >= 0 && jj >= 0) ? kimg : -1,
+                    same ? reg_ij : point_regular(g, nv, fi, jj, kimg), d, v);
+      // a row's i-faces are read only by its own warp: the __syncwarp after the
+      // previous plane's Fp lets them be overwritten
+#pragma unroll
+      for (int c = 0; c < 3; c++) { S.fi[w][c][lane + 2] = d[c]; S.fi[w][3 + c][lane + 2] = v[c]; }
+      march_face<1>(g, m, uc, u, nv, nut, ii, fj, (ii >= 0 && fj >= 0) ? kimg : -1,
+                    same ? reg_ij : point_regular(g, nv, ii, fj, kimg), d, v);
+#pragma unroll
+      for (int c = 0; c < 3; c++) { S.jf[b][w + 2][c][lane] = d[c]; S.jf[b][w + 2][3 + c][lane] = v[c]; }
+      if (w < 3) {
+        march_face<1>(g, m, uc, u, nv, nut, ii, hfj, (ii >= 0 && hfj >= 0) ? kimg : -1,
+                      point_regular(g, nv, ii, hfj, kimg), d, v);
+#pragma unroll
+        for (int c = 0; c < 3; c++) { S.jf[b][hr][c][lane] = d[c]; S.jf[b][hr][3 + c][lane] = v[c]; }
+      }
+    }
+    __syncthreads();
+    // Fp of (uI, vJ, kc)
+    MarchFaces<NW> F;
+    F.S = &S; F.b = b; F.w = w; F.lane = lane; F.t = t; F.kc = kc;
+    double fpv[3] = {0, 0, 0};
+    if (ii >= 0 && jj >= 0 && kimg >= 0) fp_cell(g, nv, lidx(g, ii, jj, kimg), ii, jj, kimg, F, fpv);
+    __syncwarp();
+    // projection products of this cell at plane kc (metrics of its own DA point)
+    double ax = 0, ay = 0, az = 0;
+    if (col_da && kc <= mz - 1) {
+      const long long q = lidx(g, uI, vJ, kc);
+      ax = m.csi.x[q] * fpv[0] + m.csi.y[q] * fpv[1] + m.csi.z[q] * fpv[2];
+      ay = m.eta.x[q] * fpv[0] + m.eta.y[q] * fpv[1] + m.eta.z[q] * fpv[2];
+      az = m.zet.x[q] * fpv[0] + m.zet.y[q] * fpv[1] + m.zet.z[q] * fpv[2];
+    }
+    S.ay[b][w][lane] = ay;
+    // right-hand side of plane kc-1
+    const double ax_right = __shfl_down_sync(0xffffffffu, ax_prev, 1);
+    if (kc > kb && out_col && uI >= 1 && vJ >= 1) {
+      const int k = kc - 1;
+      const long long p = lidx(g, uI, vJ, k);
+      const double ay_up = S.ay[b ^ 1][w + 1][lane];
+      double r[3];
+      if (rk) { r[0] = 0; r[1] = 0; r[2] = 0; }
+      else { r[0] = rhs.x[p]; r[1] = rhs.y[p]; r[2] = rhs.z[p]; }
+      r[0] += scale * (0.5 * ax_prev + 0.5 * ax_right) * m.iaj[p];
+      r[1] += scale * (0.5 * ay_prev + 0.5 * ay_up) * m.jaj[p];
+      r[2] += scale * (0.5 * az_prev + 0.5 * az) * m.kaj[p];
+      if (nv[p] + nv[p + 1] > 0 || (!g.iper && uI == mx - 2)) r[0] = 0;
+      if (nv[p] + nv[p + sy] > 0 || (!g.jper && vJ == my - 2)) r[1] = 0;
+      if (nv[p] + nv[p + sz] > 0 || (!g.kper && k == mz - 2)) r[2] = 0;
+      if (!rk) {
+        rhs.x[p] = r[0]; rhs.y[p] = r[1]; rhs.z[p] = r[2];
+      } else {
+        r[0] = r[0] + -1 * dP.x[p];
+        r[1] = r[1] + -1 * dP.y[p];
+        r[2] = r[2] + -1 * dP.z[p];
+        out.x[p] = a * r[0] + pu.x[p];
+        out.y[p] = a * r[1] + pu.y[p];
+        out.z[p] = a * r[2] + pu.z[p];
+      }
+    }
+    ax_prev = ax; ay_prev = ay; az_prev = az;
+    reg_ij = reg_next && face_image_or_none(kc + 1, mz, g.kper) == kc + 1;
+  }
+}
+
+// Ghost points of the DA (an index 0 or m-1 in some direction): zero right-hand side, and
+// in RK mode the stage update  out = pUcont + a (0 - dP)  (k_rhs at a ghost point).
+__global__ void k_ff2_ghosts(Grid g, V3 rhs, int rk, double a, CV3 dP, CV3 pu, V3 out) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long ni = 2LL * g.my * g.mz, nj = 2LL * (g.mx - 2) * g.mz, nk = 2LL * (g.mx - 2) * (g.my - 2);
+  if (t >= ni + nj + nk) return;
+  long long r = t;
+  int i, j, k;
+  if (r < ni) { i = (r & 1) ? g.mx - 1 : 0; r >>= 1; j = (int)(r % g.my); k = (int)(r / g.my); }
+  else if ((r -= ni) < nj) { j = (r & 1) ? g.my - 1 : 0; r >>= 1; i = 1 + (int)(r % (g.mx - 2)); k = (int)(r / (g.mx - 2)); }
+  else { r -= nj; k = (r & 1) ? g.mz - 1 : 0; r >>= 1; i = 1 + (int)(r % (g.mx - 2)); j = 1 + (int)(r / (g.mx - 2)); }
+  const long long p = lidx(g, i, j, k);
+  double v[3] = {0, 0, 0};
+  if (!rk) {
+    rhs.x[p] = v[0]; rhs.y[p] = v[1]; rhs.z[p] = v[2];
+  } else {
+    v[0] = v[0] + -1 * dP.x[p];
+    v[1] = v[1] + -1 * dP.y[p];
+    v[2] = v[2] + -1 * dP.z[p];
+    out.x[p] = a * v[0] + pu.x[p];
+    out.y[p] = a * v[1] + pu.y[p];
+    out.z[p] = a * v[2] + pu.z[p];
+  }
+}
+
+// Formfunction_2 (momentum.c:456): adds scale * RHS into the context's RHS; in RK mode
+// (rk_stage) writes the stage update  pUcont + rk_coeff (RHS - dP)  into the RHS arrays
+// and swaps them with Ucont, so Ucont holds the updated fluxes (an RK step swaps four
+// times and ends with the original arrays).
+int formfunction2_onepass(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
   const Grid &g = c->g;
   int rc;
   V3 uc = field3(c, VFS_UCONT);
   if ((rc = periodic_copy3(c, uc))) return rc;
   Metrics m = metrics(c);
   V3 pu{c->pucont[0], c->pucont[1], c->pucont[2]};
+  V3 rhs = field3(c, VFS_RHS);
+  constexpr int NW = VFS_MARCH_NW;
+  const size_t smem = sizeof(MarchSmem<NW>);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_ff2_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FF2Smem));
+    cudaFuncSetAttribute(k_ff2_march<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  dim3 grid((g.mx - 2 + FTI - 1) / FTI, (g.my - 2 + FTJ - 1) / FTJ, (g.mz - 2 + FKC - 1) / FKC);
-  c->launches++, k_ff2_fused<<<grid, kFF2Threads, sizeof(FF2Smem), c->stream>>>(g, m, cv(uc), cv(field3(c, VFS_UCAT)), c->nv,
-                                                               c->f[VFS_NU_T][0], scale, field3(c, VFS_RHS),
-                                                               rk_stage ? 1 : 0, rk_coeff, cv(field3(c, VFS_DP)),
-                                                               cv(pu));
-  if ((rc = check_launch(c, "k_ff2_fused"))) return rc;
-  const long long ng = 2LL * g.my * g.mz + 2LL * g.mx * g.mz + 2LL * g.mx * g.my;
-  c->launches++, k_rhs_ghosts<<<nblocks(ng, 256), 256, 0, c->stream>>>(g, m, c->nv, scale, field3(c, VFS_RHS), rk_stage ? 1 : 0,
-                                                       rk_coeff, cv(field3(c, VFS_DP)), cv(pu));
-  if ((rc = check_launch(c, "k_rhs_ghosts"))) return rc;
+  const int kc = VFS_MARCH_KC;
+  dim3 grid((g.mx - 2 + kMarchOut - 1) / kMarchOut, (g.my - 2 + NW - 2) / (NW - 1), (g.mz - 2 + kc - 1) / kc);
+  c->launches++, k_ff2_march<NW><<<grid, dim3(kMarchLanes, NW), smem, c->stream>>>(
+      g, m, cv(uc), cv(field3(c, VFS_UCAT)), c->nv, c->f[VFS_NU_T][0], scale, rhs, rk_stage ? 1 : 0, rk_coeff,
+      cv(field3(c, VFS_DP)), cv(pu), rhs, kc);
+  if ((rc = check_launch(c, "k_ff2_march"))) return rc;
+  const long long ng = 2LL * g.my * g.mz + 2LL * (g.mx - 2) * g.mz + 2LL * (g.mx - 2) * (g.my - 2);
+  c->launches++, k_ff2_ghosts<<<nblocks(ng, 256), 256, 0, c->stream>>>(g, rhs, rk_stage ? 1 : 0, rk_coeff,
+                                                                      cv(field3(c, VFS_DP)), cv(pu), rhs);
+  if ((rc = check_launch(c, "k_ff2_ghosts"))) return rc;
   if (rk_stage) {
-    c->launches++, k_rk_update<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g.N, rk_coeff, cv(field3(c, VFS_RHS)), cv(pu), uc);
-    if ((rc = check_launch(c, "k_rk_update"))) return rc;
+    for (int q = 0; q < 3; q++) std::swap(c->f[VFS_UCONT][q], c->f[VFS_RHS][q]);
   }
   return VFS_OK;
+}
+
+// The form the step runs.
+#ifndef VFS_FF2_ONEPASS
+#define VFS_FF2_ONEPASS 0
+#endif
+int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff) {
+  return VFS_FF2_ONEPASS ? formfunction2_onepass(c, scale, rk_stage, rk_coeff)
+                         : formfunction2_split(c, scale, rk_stage, rk_coeff);
 }
 
 // single-kernel launchers for the diagnostics entry point (vfs_run_kernel)

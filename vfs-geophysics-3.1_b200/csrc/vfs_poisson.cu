@@ -1183,8 +1183,9 @@ int run_kernel(Ctx *c, int which, int reps) {
         break;
       case 4: rc = mg_sweep_fine(c, 0); if (rc) return rc; break;
       case 5: rc = mg_sweep_fine(c, 1); if (rc) return rc; break;
-      case 7: rc = formfunction2_fused(c, 1.0, false, 0.0); if (rc) return rc; break;
+      case 7: rc = formfunction2_split(c, 1.0, false, 0.0); if (rc) return rc; break;
       case 8: rc = formfunction2(c, 1.0, false, 0.0); if (rc) return rc; break;
+      case 11: rc = formfunction2_onepass(c, 1.0, false, 0.0); if (rc) return rc; break;
       case 9:
       case 10: {  // one multigrid V-cycle (the preconditioner) on B, FP32 or FP64, into a work vector
         vfs_solve_opts o;
