@@ -280,6 +280,29 @@ int vfs_divergence(vfs_ctx *ctx, double *max_div);
  * advances by one.  opts may be NULL for the defaults. */
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
 
+/* ---- restart files ---------------------------------------------------------------- */
+
+/* One vector in PETSc's binary Vec format, as the reference's restart files hold it
+ * (PetscViewerBinaryOpen + VecView / VecLoadIntoVector, main.c:777-780, 401-404): the
+ * class id 1211214 and the length as 32-bit big-endian integers, then n big-endian
+ * doubles.  values: host array of n doubles (a DA vector in its natural ordering, the
+ * layout of vfs_get_field).  Reading fails with VFS_ERR_INVALID when the file's length
+ * is not n.  Host-only: no context or GPU needed. */
+int vfs_petsc_vec_write(const char *path, const double *values, long long n);
+int vfs_petsc_vec_read(const char *path, double *values, long long n);
+
+/* Ucont_P_Binary_Output (main.c:765-1035): writes <dir>/vfield%06d_%1d.dat (Ucont),
+ * ufield (Ucat), pfield (P), nvfield (nvert) and, with les on, cs_ (the Smagorinsky
+ * coefficient), for time step ti and block `block` (0-9), in the reference's format. */
+int vfs_restart_write(vfs_ctx *ctx, const char *dir, int ti, int block);
+
+/* Ucont_P_Binary_Input (main.c:394-760): loads Ucont (and Ucont_o), P, Ucat (and the
+ * old Ucat of the slip walls), nvert when immersed = 1 (the reference's Nvert_o; classify
+ * the bodies again with vfs_ibm_search for the current flags) and, with les on, Cs (0
+ * when its file is absent); the run continues as a restart at time step ti (tistart = ti,
+ * the first step repeats the set-up of ti == tistart). */
+int vfs_restart_read(vfs_ctx *ctx, const char *dir, int ti, int block);
+
 /* ---- allocation-free variant ---------------------------------------------------- */
 
 /* Largest grid (DA points (IM+1)*(JM+1)*(KM+1)) vfs_contra2cart_noalloc accepts, and the

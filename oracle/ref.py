@@ -58,6 +58,8 @@ def lib():
         L.ref_ibm_classify.argtypes = [ctypes.c_int] * 2 + [vp] * 3 + [ctypes.c_int] + [vp] * 3 + [ctypes.c_int]
         L.ref_ibm_list.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int]
         L.ref_ibm_interpolation.argtypes = [ctypes.c_int]
+        L.ref_restart_output.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        L.ref_restart_input.argtypes = [ctypes.c_char_p, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -214,6 +216,14 @@ class Reference:
 
     def set_kflux(self, flux, area):
         lib().ref_set_kflux(flux, area)
+
+    def restart_output(self, directory, ti):
+        """Ucont_P_Binary_Output (main.c:765): the restart files of step ti in directory."""
+        self.call("ref_restart_output", os.fsencode(directory), ti)
+
+    def restart_input(self, directory, ti):
+        """Ucont_P_Binary_Input (main.c:394): loads the restart files of step ti."""
+        self.call("ref_restart_input", os.fsencode(directory), ti)
 
     def poisson_csr(self):
         L = lib()

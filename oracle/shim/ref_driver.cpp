@@ -33,6 +33,9 @@ extern void PoissonRHS2_hypre(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 extern void Remove_Nullspace(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 
 extern double inletArea;
+extern char path[256];                                  // main.c:210
+extern PetscErrorCode Ucont_P_Binary_Output(UserCtx *user);  // main.c:765
+extern PetscErrorCode Ucont_P_Binary_Input(UserCtx *user);   // main.c:394
 extern PetscInt point_cell_advanced(Cmpnts p, PetscInt ip, PetscInt jp, PetscInt kp, IBMNodes *ibm, PetscInt ncx,
                                     PetscInt ncy, PetscInt ncz, PetscReal dcx, PetscReal dcy, PetscReal xbp_min,
                                     PetscReal ybp_min, PetscReal zbp_max, LIST *cell_trg, PetscInt flg);
@@ -213,6 +216,24 @@ int ref_set_inflow_plane(const double *plane) {
   return 0;
 }
 int ref_ib_bc(void) { IB_BC(g_user); return 0; }
+// Restart files of time step `step` in directory dir: Ucont_P_Binary_Output /
+// Ucont_P_Binary_Input (main.c:765, main.c:394) with the run's `path` and `ti`.
+int ref_restart_output(const char *dir, int step) {
+  strncpy(path, dir, sizeof(path) - 1);
+  const int saved = ti;
+  ti = step;
+  const int rc = Ucont_P_Binary_Output(g_user);
+  ti = saved;
+  return rc;
+}
+int ref_restart_input(const char *dir, int step) {
+  strncpy(path, dir, sizeof(path) - 1);
+  const int saved = ti;
+  ti = step;
+  const int rc = Ucont_P_Binary_Input(g_user);
+  ti = saved;
+  return rc;
+}
 // The end of one physical time step in the reference's time loop (main.c:3571-3602):
 // the old-value copies that the next step reads (Ucont_o, Ucont_rm1, P_o, and lUcat_old,
 // the slip-wall ghost source of Contra2Cart), for the single block of the oracle.

@@ -3,6 +3,8 @@
 // compiled unmodified into oracle/_ref.  The product library never links it.
 #include "petsc_shim.h"
 
+#include <cstdio>
+#include <cstring>
 #include <map>
 #include <vector>
 #include <sys/time.h>
@@ -126,8 +128,52 @@ PetscErrorCode VecGetValues(Vec v, PetscInt n, const PetscInt *ix, PetscScalar *
 }
 PetscErrorCode VecAssemblyBegin(Vec) { return 0; }
 PetscErrorCode VecAssemblyEnd(Vec) { return 0; }
-PetscErrorCode VecView(Vec, PetscViewer) { return 0; }
-PetscErrorCode VecLoadIntoVector(PetscViewer, Vec) { return 0; }
+// PETSc binary viewer for Vec (the published PETSc binary format: the Vec class id
+// 1211214 and the global length as 32-bit big-endian integers, then the entries as
+// big-endian doubles, a DA vector in the natural (k, j, i, component) ordering, which is
+// this shim's storage order).
+struct ShimBinViewer {
+  FILE *f;
+  int write;
+};
+static void put_be32(FILE *f, int v) {
+  unsigned char b[4] = {(unsigned char)(v >> 24), (unsigned char)(v >> 16), (unsigned char)(v >> 8), (unsigned char)v};
+  fwrite(b, 1, 4, f);
+}
+static int get_be32(FILE *f, int *v) {
+  unsigned char b[4];
+  if (fread(b, 1, 4, f) != 4) return 1;
+  *v = (int)((unsigned)b[0] << 24 | (unsigned)b[1] << 16 | (unsigned)b[2] << 8 | (unsigned)b[3]);
+  return 0;
+}
+PetscErrorCode VecView(Vec x, PetscViewer v) {
+  ShimBinViewer *bv = (ShimBinViewer *)v;
+  if (!bv || !bv->write) return 0;
+  put_be32(bv->f, 1211214);
+  put_be32(bv->f, (int)x->n);
+  for (PetscInt q = 0; q < x->n; q++) {
+    unsigned long long u;
+    memcpy(&u, &x->data[q], 8);
+    unsigned char b[8];
+    for (int t = 0; t < 8; t++) b[t] = (unsigned char)(u >> (56 - 8 * t));
+    fwrite(b, 1, 8, bv->f);
+  }
+  return 0;
+}
+PetscErrorCode VecLoadIntoVector(PetscViewer v, Vec x) {
+  ShimBinViewer *bv = (ShimBinViewer *)v;
+  if (!bv || bv->write) return 1;
+  int cls = 0, n = 0;
+  if (get_be32(bv->f, &cls) || get_be32(bv->f, &n) || cls != 1211214 || n != (int)x->n) return 1;
+  for (PetscInt q = 0; q < x->n; q++) {
+    unsigned char b[8];
+    if (fread(b, 1, 8, bv->f) != 8) return 1;
+    unsigned long long u = 0;
+    for (int t = 0; t < 8; t++) u = (u << 8) | b[t];
+    memcpy(&x->data[q], &u, 8);
+  }
+  return 0;
+}
 PetscErrorCode VecScatterCreateToAll(Vec a, VecScatter *s, Vec *b) { *s = 0; VecDuplicate(a, b); return 0; }
 PetscErrorCode VecScatterCreateToZero(Vec a, VecScatter *s, Vec *b) { *s = 0; VecDuplicate(a, b); return 0; }
 PetscErrorCode VecScatterBegin(VecScatter, Vec a, Vec b, InsertMode, ScatterMode m) {
@@ -396,8 +442,20 @@ PetscErrorCode PetscOptionsInsertString(const char *) { return 0; }
 PetscErrorCode PetscOptionsInsertFile(MPI_Comm, const char *, PetscTruth) { return 0; }
 PetscErrorCode PetscOptionsClearValue(const char *) { return 0; }
 PetscErrorCode PetscOptionsSetValue(const char *, const char *) { return 0; }
-PetscErrorCode PetscViewerBinaryOpen(MPI_Comm, const char *, PetscFileMode, PetscViewer *v) { *v = 0; return 0; }
-PetscErrorCode PetscViewerDestroy(PetscViewer) { return 0; }
+PetscErrorCode PetscViewerBinaryOpen(MPI_Comm, const char *name, PetscFileMode mode, PetscViewer *v) {
+  FILE *f = fopen(name, mode == FILE_MODE_READ ? "rb" : "wb");
+  if (!f) { *v = 0; return 1; }
+  ShimBinViewer *bv = new ShimBinViewer;
+  bv->f = f;
+  bv->write = mode != FILE_MODE_READ;
+  *v = bv;
+  return 0;
+}
+PetscErrorCode PetscViewerDestroy(PetscViewer v) {
+  ShimBinViewer *bv = (ShimBinViewer *)v;
+  if (bv) { fclose(bv->f); delete bv; }
+  return 0;
+}
 
 // ------------------------------------------------------------------ HYPRE IJ vectors
 struct ShimIJ { int lo, hi; std::vector<double> v; };

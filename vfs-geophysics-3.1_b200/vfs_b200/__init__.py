@@ -114,9 +114,27 @@ EXPORTS = [
     "vfs_ibm_search", "vfs_ibm_list", "vfs_ibm_interpolation",
     "vfs_adjoint_setup", "vfs_objective", "vfs_tangent", "vfs_adjoint_gradient",
     "vfs_adjoint_op_info", "vfs_adjoint_op_check",
+    "vfs_petsc_vec_write", "vfs_petsc_vec_read", "vfs_restart_write", "vfs_restart_read",
 ]
 
 _lib = None
+
+
+def petsc_vec_write(path, values):
+    """One vector in PETSc's binary Vec format (the reference's restart files)."""
+    a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    lib = load_library()
+    if lib.vfs_petsc_vec_write(os.fsencode(path), a.ctypes.data, a.size):
+        raise VfsError(1, lib.vfs_last_error(None).decode())
+
+
+def petsc_vec_read(path, n):
+    """The n doubles of a PETSc binary Vec file."""
+    out = np.empty(n)
+    lib = load_library()
+    if lib.vfs_petsc_vec_read(os.fsencode(path), out.ctypes.data, n):
+        raise VfsError(1, lib.vfs_last_error(None).decode())
+    return out
 
 
 def load_library(path=None):
@@ -169,6 +187,10 @@ def load_library(path=None):
     lib.vfs_adjoint_op_info.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp,
                                         ctypes.POINTER(ctypes.c_longlong)]
     lib.vfs_adjoint_op_check.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp]
+    lib.vfs_petsc_vec_write.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong]
+    lib.vfs_petsc_vec_read.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong]
+    lib.vfs_restart_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    lib.vfs_restart_read.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
     if path is None:
         _lib = lib
     return lib
@@ -371,6 +393,12 @@ class Context:
         v = ctypes.c_double()
         self._check(self.lib.vfs_divergence(self.h, ctypes.byref(v)))
         return v.value
+
+    def restart_write(self, directory, ti, block=0):  # Ucont_P_Binary_Output, main.c:765
+        self._check(self.lib.vfs_restart_write(self.h, os.fsencode(directory), ti, block))
+
+    def restart_read(self, directory, ti, block=0):   # Ucont_P_Binary_Input, main.c:394
+        self._check(self.lib.vfs_restart_read(self.h, os.fsencode(directory), ti, block))
 
     def step(self, precision=0, rtol=1e-10, **kw):  # Flow_Solver, solvers.c:562 (implicit=0)
         o = _solve_opts(precision, rtol, **kw)
