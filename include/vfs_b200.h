@@ -44,7 +44,12 @@ typedef struct {
                             tistart (main.c:1747, solvers.c:652); values < 1 mean 1 */
   int tistart;           /* index of the first time step (main.c:5, -rstart) */
   int rstart;            /* non-zero for a restarted run (rstart_flg, main.c:1608) */
-  int reserved_i[5];
+  int wallfunction;      /* -wallfunction: the IB-node reconstruction uses the wall model
+                            wall_function_roughness_a (ks = 1e-4) from ti > 0 (ibm.c:3454-3474)
+                            instead of noslip */
+  int moving;            /* movefsi || rotatefsi: the bodies move (ibm.c:3444: IB nodes next
+                            to solid cells are reconstructed all the same) */
+  int reserved_i[3];
   double ren;            /* Reynolds number (user->ren) */
   double dt;             /* time step (user->dt) */
   double st;             /* Strouhal scaling (user->st) */
@@ -76,7 +81,8 @@ enum {
   VFS_JCSI = 20, VFS_JETA = 21, VFS_JZET = 22, VFS_JAJ = 23, /* j-face metrics */
   VFS_KCSI = 24, VFS_KETA = 25, VFS_KZET = 26, VFS_KAJ = 27, /* k-face metrics */
   VFS_CS = 28,      /* [1] dynamic Smagorinsky coefficient lCs */
-  VFS_NFIELDS = 29
+  VFS_USTAR = 29,   /* [1] friction velocity at IB nodes (lUstar, ibm_interpolation_advanced) */
+  VFS_NFIELDS = 30
 };
 
 /* Scalars for vfs_set_scalar / vfs_get_scalar. */
@@ -90,7 +96,10 @@ enum {
   VFS_S_FLUX_IN = 8,      /* FluxInSum: inlet flux of the last InflowFlux (bcs.c:785) */
   VFS_S_FLUX_OUT = 9,     /* FluxOutSum: outlet flux before the last rescaling (bcs.c:2369) */
   VFS_S_IB_UNRESOLVED = 10, /* IB nodes whose interception search failed ("IBM Searching Fail!") */
-  VFS_NSCALARS = 11
+  VFS_S_NBODIES = 11,     /* NumberOfBodies (main.c): the search of the last body (ibi =
+                           * NumberOfBodies-1) marks cells a moving body has uncovered
+                           * since the last step as IB nodes (ibm.c:346-357); default 1 */
+  VFS_NSCALARS = 12
 };
 
 /* Poisson solver options (replaces PoissonSolver_Hypre, poisson_hypre.c:498). */
@@ -168,6 +177,12 @@ int vfs_form_metrics(vfs_ctx *ctx, const double *x, const double *y, const doubl
  * cells interpolated across it; body 0 starts a new list, later bodies append. */
 int vfs_ibm_search(vfs_ctx *ctx, int ibi, int n_v, const double *x, const double *y, const double *z,
                    int n_elmt, const int *nv1, const int *nv2, const int *nv3);
+
+/* The surface velocity of body ibi's vertices (ibm->u, set by the reference's body-motion
+ * routines, e.g. Elmt_Move_FSI_TRANS), which the IB-node reconstruction interpolates to
+ * each node's nearest point (ibm.c:3430-3433).  Zero after every vfs_ibm_search of the
+ * body (a fixed body); n_v must be the body's vertex count. */
+int vfs_ibm_set_velocity(vfs_ctx *ctx, int ibi, int n_v, const double *u, const double *v, const double *w);
 
 /* The IB-node list: returns its length; with ints/dbls, copies up to cap nodes, 14 ints
  * each (i j k, nearest triangle, interception mode, stencil i1 j1 k1 i2 j2 k2 i3 j3 k3)

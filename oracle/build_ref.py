@@ -25,11 +25,13 @@ LIB = os.path.join(OUT, "libvfsref.so")
 REF_DIR = os.environ.get("REF_DIR", "/root/reference")
 
 # Reference translation units compiled into the oracle (the hot path plus the set-up
-# code it needs: grid input, metrics, BCs, IB interpolation, LES, globals in main.c).
+# code it needs: grid input, metrics, BCs, IB interpolation, LES, globals in main.c;
+# sediment_transport-Y.c for the wall model the IB interpolation calls,
+# wall_function_roughness_a).
 REF_SOURCES = [
     "main.c", "init.c", "metrics.c", "momentum.c", "rhs.c", "rhs2.c", "k-omega.c",
     "poisson.c", "poisson_hypre.c", "les.c", "bcs.c", "wallfunction.c", "ibm.c",
-    "compgeom.c", "level.c", "variables.c",
+    "compgeom.c", "level.c", "variables.c", "sediment_transport-Y.c",
 ]
 CXXFLAGS = ["-std=c++11", "-O2", "-fPIC", "-w", "-fpermissive", "-ffp-contract=off",
             "-DNDEBUG", "-I" + SHIM]

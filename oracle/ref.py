@@ -58,6 +58,7 @@ def lib():
         L.ref_ibm_classify.argtypes = [ctypes.c_int] * 2 + [vp] * 3 + [ctypes.c_int] + [vp] * 3 + [ctypes.c_int]
         L.ref_ibm_list.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int]
         L.ref_ibm_interpolation.argtypes = [ctypes.c_int]
+        L.ref_ibm_set_velocity.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.ref_restart_output.argtypes = [ctypes.c_char_p, ctypes.c_int]
         L.ref_restart_input.argtypes = [ctypes.c_char_p, ctypes.c_int]
         _lib = L
@@ -112,7 +113,10 @@ class Reference:
              "inletprofile": case.inletprofile, "poisson": 1, "implicit": 0, "ti": 0,
              "tistart": 0, "weno": 0, "second_order": 0, "central": 0, "inviscid": 0,
              "skew": 0, "clark": 0, "laplacian": 0, "dpdz_set": 0, "movefsi": 0,
-             "rotatefsi": 0, "inlet_flux": case.inlet_flux, "NumberOfBodies": 1}
+             "rotatefsi": 0, "inlet_flux": case.inlet_flux, "NumberOfBodies": 1,
+             "wallfunction": getattr(case, "wallfunction", 0)}
+        if getattr(case, "moving", 0):
+            g["movefsi"] = 1
         if extra_globals:
             g.update(extra_globals)
         for k, v in g.items():
@@ -195,6 +199,11 @@ class Reference:
         self.call("ref_ibm_classify", ibi, len(xs[0]), xs[0].ctypes.data, xs[1].ctypes.data, xs[2].ctypes.data,
                   len(t), cols[0].ctypes.data, cols[1].ctypes.data, cols[2].ctypes.data, int(build_list))
         return self.get("lNvert")
+
+    def ibm_set_velocity(self, u, v, w, ibi=0):
+        """ibm->u of body ibi (the surface velocity of its vertices)."""
+        a = [np.ascontiguousarray(t, dtype=np.float64) for t in (u, v, w)]
+        self.call("ref_ibm_set_velocity", ibi, len(a[0]), a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data)
 
     def ibm_list(self, ibi=0):
         """The IB-node list (ints (n, 14): i j k cell imode i1 j1 k1 i2 j2 k2 i3 j3 k3; doubles

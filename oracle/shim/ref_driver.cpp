@@ -398,6 +398,14 @@ int ref_ibm_classify(int ibi, int n_v, const double *x, const double *y, const d
             for (int ii = im; ii <= ip; ii++)
               if ((int)(nv[at(ii, jj, kk)] + 0.5) == 4) nv[p] = PetscMax(2, nv[p]);
       }
+  // cells a moving body has uncovered since the last step (Nvert_o > 2.5, now fluid)
+  // become IB nodes, at the search of the last body (ibm.c:346-357)
+  extern PetscInt NumberOfBodies;  // main.c
+  if (ibi == NumberOfBodies - 1) {
+    const double *nvo = g_user->lNvert_o->data;
+    for (long p = 0; p < (long)mx * my * mz; p++)
+      if (nvo[p] > 2.5 && nv[p] < 0.5) nv[p] = 2;
+  }
   if (build_list) {
     // the IB-node list of ibm.c:347-505 with the reference's own geometry (BoundingSphere,
     // nearestcell1, InterceptionPoint); the two fallbacks for a failed interception are
@@ -466,6 +474,14 @@ int ref_ibm_list(int ibi, int *ints, double *dbls, int cap) {
     d[0] = f.cr1; d[1] = f.cr2; d[2] = f.cr3; d[3] = f.cs1; d[4] = f.cs2; d[5] = f.cs3; d[6] = f.d_s; d[7] = f.d_i;
   }
   return n;
+}
+
+// The surface velocity of body ibi's vertices (ibm->u), as a body-motion routine leaves it.
+int ref_ibm_set_velocity(int ibi, int n_v, const double *u, const double *v, const double *w) {
+  IBMNodes &ibm = g_ibm[ibi];
+  if (n_v != ibm.n_v || !ibm.u) return 1;
+  for (int q = 0; q < n_v; q++) { ibm.u[q].x = u[q]; ibm.u[q].y = v[q]; ibm.u[q].z = w[q]; }
+  return 0;
 }
 
 // ibm_interpolation_advanced (ibm.c:3294) on the current fields.

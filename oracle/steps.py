@@ -31,18 +31,33 @@ class ReferenceStepper:
         self.ti = 0
         self.phi2 = None
         self.history = []
-        R.call("ref_poisson_lhs")                 # poisson_hypre.c:527 (set-up, once)
+        self._lhs()
+
+    def _lhs(self):
+        """PoissonLHSNew and the solver's set-up: once, or every step with moving bodies
+        (poisson_hypre.c:540-553)."""
+        R, c = self.R, self.case
+        R.call("ref_poisson_lhs")
         rp, col, val = R.poisson_csr()
-        c = self.case
         self.solver = poisson_mg.MGSolver(rp, col, val, R.gid(), (c.i_periodic, c.j_periodic, c.k_periodic))
+
+    def _ibm_interpolation(self):
+        """ibm_interpolation_advanced with the run's ti (its wall model applies from
+        ti > 0, ibm.c:3456)."""
+        ref.set_global("ti", self.ti)
+        self.R.call("ref_ibm_interpolation", 1)
+        ref.set_global("ti", 0)
 
     def step(self):
         R, case = self.R, self.case
         ref.set_global("ti", 0)
         t0 = time.perf_counter()
+        if self.ti > 0 and getattr(case, "moving", 0):
+            self._lhs()
+            self.phi2 = None          # the unknowns are numbered anew (setup_lidx2)
         if self.ti == 0:
             if case.immersed:
-                R.call("ref_ibm_interpolation", 1)    # solvers.c:607
+                self._ibm_interpolation()             # solvers.c:607
             R.call("ref_ib_bc")                       # solvers.c:609
             R.set("Ucont", R.get("lUcont"))
         R.call("ref_calc_k_flux")                     # solvers.c:644
@@ -68,7 +83,7 @@ class ReferenceStepper:
         R.call("ref_update_pressure")                 # solvers.c:1341
         R.call("ref_projection")                      # solvers.c:1342
         if case.immersed:
-            R.call("ref_ibm_interpolation", 1)        # solvers.c:1368
+            self._ibm_interpolation()                 # solvers.c:1368
         R.call("ref_ib_bc")                           # solvers.c:1381
         R.set("Ucont", R.get("lUcont"))
         R.call("ref_contra2cart")                     # solvers.c:1385

@@ -138,7 +138,7 @@ static const int kDof[VFS_NFIELDS] = {
     3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3,  // UCONT..CENT
     3, 3, 3, 1,                            // CSI ETA ZET AJ
     3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1,    // I J K face metrics
-    1};                                     // CS
+    1, 1};                                  // CS USTAR
 
 extern "C" {
 
@@ -195,9 +195,11 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
   g.iper = cfg->i_periodic; g.jper = cfg->j_periodic; g.kper = cfg->k_periodic;
   for (int q = 0; q < 6; q++) g.bc[q] = cfg->bctype[q];
   g.immersed = cfg->immersed; g.les = cfg->les;
+  g.wallfunction = cfg->wallfunction; g.moving = cfg->moving;
   g.ren = cfg->ren; g.dt = cfg->dt; g.st = cfg->st;
   c->scal[VFS_S_DT] = cfg->dt; c->scal[VFS_S_REN] = cfg->ren; c->scal[VFS_S_ST] = cfg->st;
   c->scal[VFS_S_INLET_FLUX] = cfg->inlet_flux;
+  c->scal[VFS_S_NBODIES] = 1;
   c->tistart = cfg->tistart;
   c->ti = cfg->tistart;
   c->rstart = cfg->rstart;
@@ -260,6 +262,8 @@ int vfs_destroy(vfs_ctx *ctx) {
   for (int f = 0; f < VFS_NFIELDS; f++)
     for (int q = 0; q < 3; q++) if (c->f[f][q]) cudaFree(c->f[f][q]);
   if (c->nv) cudaFree(c->nv);
+  if (c->nvo) cudaFree(c->nvo);
+  if (c->ibv) cudaFree(c->ibv);
   if (c->bcflag) cudaFree(c->bcflag);
   if (c->solid) cudaFree(c->solid);
   for (int d = 0; d < 3; d++)
@@ -529,8 +533,14 @@ int step_core(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
   if ((rc = divergence(c, &s.max_div))) return rc;
   if ((rc = ib_bc(c))) return rc;
   if ((rc = contra2cart(c))) return rc;
-  // end of the time step: keep Ucont and Ucat of this step (main.c:3584-3602)
+  // end of the time step: keep Ucont and Ucat of this step (main.c:3584-3602), and with
+  // immersed bodies the flags as Nvert_o (main.c:3571-3573)
   const size_t bytes = sizeof(double) * (size_t)c->g.N;
+  if (c->g.immersed) {
+    if (!c->nvo && cudaMalloc(&c->nvo, (size_t)c->g.N) != cudaSuccess)
+      return set_err(c, VFS_ERR_CUDA, "vfs_step: allocation failed");
+    cudaMemcpyAsync(c->nvo, c->nv, (size_t)c->g.N, cudaMemcpyDeviceToDevice, c->stream);
+  }
   for (int q = 0; q < 3; q++) {
     cudaMemcpyAsync(c->f[VFS_UCONT_O][q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
     cudaMemcpyAsync(c->f[VFS_UCAT_O][q], c->f[VFS_UCAT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);

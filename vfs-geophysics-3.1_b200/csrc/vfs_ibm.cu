@@ -144,6 +144,14 @@ __global__ void k_ibm_near(Grid g, const uint8_t *__restrict__ nv, uint8_t *out)
   out[p] = (uint8_t)v;
 }
 
+// Cells that were inside a body at the end of the last step (Nvert_o > 2.5) and are
+// now plain fluid become IB nodes (ibm.c:346-357, the search of the last body).
+__global__ void k_ibm_phase(Grid g, const uint8_t *__restrict__ nvo, uint8_t *fl) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  if (nvo[p] >= 3 && fl[p] == 0) fl[p] = 2;
+}
+
 // Back to 1 and 3 on the interior (ibm.c:507-514); the double field follows.
 __global__ void k_ibm_remap(Grid g, const uint8_t *__restrict__ in, uint8_t *nv, double *nvd) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -248,13 +256,25 @@ __device__ bool bary_by_normal(P3 q, P3 t1, P3 t2, P3 t3, double nx, double ny, 
   return true;
 }
 
+// Doubles per IB node in the reconstruction buffer: velocity (3), pressure, ustar.
+constexpr int kIbOut = 5;
+
 struct IbmGeom {
   IbmSurface S;
   const double *qx, *qy, *qz, *rad;  // bounding spheres (BoundingSphere)
   CV3 cent;
   const long long *cells;            // node cells (linear DA index), ascending
   int n;
+  int vbase;                         // first vertex of this body in the surface-velocity array
 };
+
+// The triangle data the reconstruction reads: its vertices (for the surface velocity,
+// ibm.c:3430-3433) and its unit normal (the wall models' n).
+__device__ __forceinline__ void node_triangle(const IbmGeom &G, IbNode &N) {
+  const int e = N.cell;
+  N.vtx[0] = G.vbase + G.S.n1[e]; N.vtx[1] = G.vbase + G.S.n2[e]; N.vtx[2] = G.vbase + G.S.n3[e];
+  N.nf[0] = G.S.nx[e]; N.nf[1] = G.S.ny[e]; N.nf[2] = G.S.nz[e];
+}
 
 __device__ __forceinline__ P3 vtx(const IbmSurface &S, int v) { return {S.x[v], S.y[v], S.z[v]}; }
 
@@ -325,6 +345,7 @@ __global__ void k_ibm_nodes(Grid g, IbmGeom G, IbNode *out, int *err) {
     atomicExch(err, 1);
     N.cell = 0; N.imode = -2; N.ds = N.di = 0;
     for (int v = 0; v < 3; v++) { N.st[3 * v] = i; N.st[3 * v + 1] = j; N.st[3 * v + 2] = k; N.cr[v] = N.cs[v] = 0; }
+    node_triangle(G, N);
     out[q] = N;
     return;
   }
@@ -380,6 +401,7 @@ __global__ void k_ibm_nodes(Grid g, IbmGeom G, IbNode *out, int *err) {
       N.imode = -2;
     }
   }
+  node_triangle(G, N);
   out[q] = N;
 }
 
@@ -531,6 +553,10 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
   if ((rc = check_launch(c, "k_ibm_cast"))) { cudaFree(buf); return rc; }
   c->launches++, k_ibm_near<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, c->bcflag);
   if ((rc = check_launch(c, "k_ibm_near"))) { cudaFree(buf); return rc; }
+  if (c->nvo && ibi == (int)c->scal[VFS_S_NBODIES] - 1) {
+    c->launches++, k_ibm_phase<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nvo, c->bcflag);
+    if ((rc = check_launch(c, "k_ibm_phase"))) { cudaFree(buf); return rc; }
+  }
   // the IB-node list of this body (ibm.c:347-505): cells marked 2, ascending
   {
     int *cnt = err + 1;
@@ -569,6 +595,29 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
     G.cent = cv(field3(c, VFS_CENT));
     G.cells = cells;
     G.n = hn;
+    // this body's vertices in the surface-velocity array (zero: a fixed body)
+    if ((int)c->vtx_base.size() <= ibi) c->vtx_base.resize(ibi + 1, -1);
+    if (ibi == 0) c->nvtx = 0;
+    for (size_t b = ibi + 1; b < c->vtx_base.size(); b++) c->vtx_base[b] = -1;
+    c->vtx_base[ibi] = c->nvtx;
+    G.vbase = c->nvtx;
+    {
+      double *nvb = nullptr;
+      const int ntot = c->nvtx + n_v;
+      if (cudaMalloc(&nvb, sizeof(double) * 3 * (size_t)ntot) != cudaSuccess) {
+        cudaFree(qd); cudaFree(nodes); cudaFreeAsync(cells, c->stream); cudaFree(buf);
+        return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: allocation failed");
+      }
+      cudaMemsetAsync(nvb, 0, sizeof(double) * 3 * (size_t)ntot, c->stream);
+      if (c->ibv && c->nvtx)
+        for (int d = 0; d < 3; d++)
+          cudaMemcpyAsync(nvb + (size_t)d * ntot, c->ibv + (size_t)d * c->nvtx, sizeof(double) * c->nvtx,
+                          cudaMemcpyDeviceToDevice, c->stream);
+      cudaStreamSynchronize(c->stream);
+      if (c->ibv) cudaFree(c->ibv);
+      c->ibv = nvb;
+      c->nvtx = ntot;
+    }
     if (hn) c->launches++, k_ibm_nodes<<<nblocks(hn, 64), 64, 0, c->stream>>>(g, G, nodes + base, err);
     if ((rc = check_launch(c, "k_ibm_nodes"))) { cudaFree(qd); cudaFree(nodes); cudaFree(buf); return rc; }
     cudaFreeAsync(cells, c->stream);
@@ -579,7 +628,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
     c->ibn = nodes;
     c->nib = base + hn;
     c->ibbuf = nullptr;
-    if (c->nib && cudaMalloc(&c->ibbuf, sizeof(double) * 4 * (size_t)c->nib) != cudaSuccess) {
+    if (c->nib && cudaMalloc(&c->ibbuf, sizeof(double) * kIbOut * (size_t)c->nib) != cudaSuccess) {
       cudaFree(buf);
       return set_err(c, VFS_ERR_CUDA, "vfs_ibm_search: allocation failed");
     }
@@ -614,8 +663,54 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
 // (sc = sb + d_i), zero when a stencil cell is not fluid or the node is solid, and the
 // pressure interpolated the same way.  All nodes read the fields as they were before the
 // pass (the reference reads the local copies lUcat and lP), then write.
+// The wall model of the reconstruction, wall_function_roughness_a (sediment_transport-Y.c:
+// 68-91) with its helpers E_coeff, u_hydset_roughness, f_hydset, df_hydset and
+// find_utau_hydset (sediment_transport-Y.c:16-66): a log law with a roughness shift for
+// the tangential velocity, solved for the friction velocity by Newton's method with a
+// central-difference derivative, in the reference's operation order.
+__device__ __forceinline__ double wf_e_coeff(double utau, double ks, double nu) {
+  const double kplus = utau * ks / nu;
+  const double kappa = 0.41, B = 5.5;
+  double dB = 0.0;
+  if (kplus <= 2.25) dB = 0.0;
+  else if (kplus > 2.25 && kplus < 90.) dB = (B - 8.5 + 1. / kappa * log(kplus)) * sin(0.4258 * (log(kplus) - 0.811));
+  else if (kplus >= 90.) dB = B - 8.5 + 1. / kappa * log(kplus);
+  return exp(kappa * (B - dB));
+}
+__device__ __forceinline__ double wf_u_hydset(double nu, double y, double utau, double ks) {
+  const double y0plus = 11.53, kappa = 0.41;
+  const double yplus = utau * y / nu;
+  if (yplus <= y0plus) return utau * yplus;
+  return utau / kappa * log(wf_e_coeff(utau, ks, nu) * yplus);
+}
+__device__ __forceinline__ double wf_f_hydset(double nu, double u, double y, double utau0, double ks) {
+  const double y0plus = 11.53, kappa = 0.41;
+  const double yplus = utau0 * y / nu;
+  if (yplus <= y0plus) return utau0 * yplus - u;
+  return utau0 * (1. / kappa * log(wf_e_coeff(utau0, ks, nu) * yplus)) - u;
+}
+__device__ __forceinline__ double wf_find_utau(double nu, double u, double y, double guess, double ks) {
+  double utau = guess, utau0 = guess;
+  const double eps = 1.e-7;
+  for (int ii = 0; ii < 30; ii++) {
+    const double df = (wf_f_hydset(nu, u, y, utau0 + eps, ks) - wf_f_hydset(nu, u, y, utau0 - eps, ks)) / (2. * eps);
+    utau = utau0 - wf_f_hydset(nu, u, y, utau0, ks) / df;
+    if (fabs(utau - utau0) < 1.e-7) break;
+    utau0 = utau;
+  }
+  return utau;
+}
+
+// One IB node of ibm_interpolation_advanced (ibm.c:3405-3530): the surface velocity Ua
+// from the triangle's vertex velocities (zero for a fixed body), Uc interpolated at the
+// node's three stencil cells; the node's velocity is 0 next to a solid stencil cell
+// (fixed bodies) or inside a body, the wall model's (wallfunction, from ti > 0), or
+// Ub = (sb/sc)(Uc - Ua) + Ua (noslip, wallfunction.c:134-150); the friction velocity of
+// either goes to ustar.  All nodes read the fields as they were before the pass (the
+// reference reads the local copies lUcat and lP), then write.
 __global__ void k_ibm_gather(Grid g, const IbNode *__restrict__ nodes, int n, CV3 ucat, const double *__restrict__ p,
-                             const uint8_t *__restrict__ nv, double *out) {
+                             const uint8_t *__restrict__ nv, const double *__restrict__ ibv, int nvtx, int ti,
+                             double *out) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const IbNode N = nodes[q];
@@ -624,33 +719,65 @@ __global__ void k_ibm_gather(Grid g, const IbNode *__restrict__ nodes, int n, CV
   const double sb = N.ds, sc = sb + N.di;
   const double sk1 = N.cr[0], sk2 = N.cr[1], sk3 = N.cr[2];
   const double cs1 = N.cs[0], cs2 = N.cs[1], cs3 = N.cs[2];
-  // surface velocity of a fixed body (ibm->u = 0) through the surface weights
-  const double z = 0.0;
-  const double uax = z * cs1 + z * cs2 + z * cs3, uay = uax, uaz = uax;
+  double uax = 0, uay = 0, uaz = 0;
+  if (N.cell >= 0) {
+    const int a = N.vtx[0], b = N.vtx[1], c = N.vtx[2];
+    uax = ibv[a] * cs1 + ibv[b] * cs2 + ibv[c] * cs3;
+    uay = ibv[nvtx + a] * cs1 + ibv[nvtx + b] * cs2 + ibv[nvtx + c] * cs3;
+    uaz = ibv[2 * nvtx + a] * cs1 + ibv[2 * nvtx + b] * cs2 + ibv[2 * nvtx + c] * cs3;
+  }
   const double ucx = (ucat.x[s1] * sk1 + ucat.x[s2] * sk2 + ucat.x[s3] * sk3);
   const double ucy = (ucat.y[s1] * sk1 + ucat.y[s2] * sk2 + ucat.y[s3] * sk3);
   const double ucz = (ucat.z[s1] * sk1 + ucat.z[s2] * sk2 + ucat.z[s3] * sk3);
   const long long pos = lidx(g, N.i, N.j, N.k);
-  double ub[3];
-  if ((double)nv[s1] + (double)nv[s2] + (double)nv[s3] > 0.1 || nv[pos] > 2) {
+  double ub[3], ustar;
+  if ((!g.moving && (double)nv[s1] + (double)nv[s2] + (double)nv[s3] > 0.1) || nv[pos] > 2) {
     ub[0] = ub[1] = ub[2] = 0;
-  } else {
+    ustar = 0;
+  } else if (g.wallfunction && ti > 0) {
+    const double nx = N.nf[0], ny = N.nf[1], nz = N.nf[2];
     const double u_c = ucx - uax, v_c = ucy - uay, w_c = ucz - uaz;
+    const double un = u_c * nx + v_c * ny + w_c * nz;
+    double ut = u_c - un * nx, vt = v_c - un * ny, wt = w_c - un * nz;
+    const double ut_mag = sqrt(ut * ut + vt * vt + wt * wt);
+    ustar = wf_find_utau(1. / g.ren, ut_mag, sc, 0.01, 0.0001);
+    const double ut_mag_modeled = wf_u_hydset(1. / g.ren, sb, ustar, 0.0001);
+    if (ut_mag > 1.e-10) {
+      ut *= ut_mag_modeled / ut_mag;
+      vt *= ut_mag_modeled / ut_mag;
+      wt *= ut_mag_modeled / ut_mag;
+    } else {
+      ut = vt = wt = 0;
+    }
+    ub[0] = ut + sb / sc * un * nx;
+    ub[1] = vt + sb / sc * un * ny;
+    ub[2] = wt + sb / sc * un * nz;
+    ub[0] += uax; ub[1] += uay; ub[2] += uaz;
+  } else {
+    const double nx = N.nf[0], ny = N.nf[1], nz = N.nf[2];
+    const double u_c = ucx - uax, v_c = ucy - uay, w_c = ucz - uaz;
+    const double un = u_c * nx + v_c * ny + w_c * nz;
+    const double ut = u_c - un * nx, vt = v_c - un * ny, wt = w_c - un * nz;
+    const double ut_mag = sqrt(ut * ut + vt * vt + wt * wt);
+    ustar = sqrt(ut_mag / sc / g.ren);
     ub[0] = sb / sc * u_c; ub[1] = sb / sc * v_c; ub[2] = sb / sc * w_c;
     ub[0] += uax; ub[1] += uay; ub[2] += uaz;
   }
   const double pn = (p[s1] * sk1 + p[s2] * sk2 + p[s3] * sk3);
-  out[4 * q] = ub[0]; out[4 * q + 1] = ub[1]; out[4 * q + 2] = ub[2]; out[4 * q + 3] = pn;
+  double *o = out + (size_t)kIbOut * q;
+  o[0] = ub[0]; o[1] = ub[1]; o[2] = ub[2]; o[3] = pn; o[4] = ustar;
 }
 
 __global__ void k_ibm_scatter(Grid g, const IbNode *__restrict__ nodes, int n, const double *__restrict__ in, V3 ucat,
-                              double *p) {
+                              double *p, double *ustar) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const IbNode N = nodes[q];
   const long long pos = lidx(g, N.i, N.j, N.k);
-  ucat.x[pos] = in[4 * q]; ucat.y[pos] = in[4 * q + 1]; ucat.z[pos] = in[4 * q + 2];
-  p[pos] = in[4 * q + 3];
+  const double *v = in + (size_t)kIbOut * q;
+  ucat.x[pos] = v[0]; ucat.y[pos] = v[1]; ucat.z[pos] = v[2];
+  p[pos] = v[3];
+  ustar[pos] = v[4];
 }
 
 // Face fluxes next to IB nodes from the averaged Cartesian velocity (ibm.c:3605-3650 and
@@ -689,10 +816,11 @@ int ibm_interpolation(Ctx *c) {
   if (c->nib > 0) {
     const Grid &g = c->g;
     c->launches++, k_ibm_gather<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, cv(field3(c, VFS_UCAT)),
-                                                             c->f[VFS_P][0], c->nv, c->ibbuf);
+                                                             c->f[VFS_P][0], c->nv, c->ibv, c->nvtx, c->ti,
+                                                             c->ibbuf);
     if ((rc = check_launch(c, "k_ibm_gather"))) return rc;
     c->launches++, k_ibm_scatter<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, c->ibbuf, field3(c, VFS_UCAT),
-                                                              c->f[VFS_P][0]);
+                                                              c->f[VFS_P][0], c->f[VFS_USTAR][0]);
     if ((rc = check_launch(c, "k_ibm_scatter"))) return rc;
   }
   if ((rc = ib_faces(c))) return rc;
@@ -770,6 +898,25 @@ int volume_flux_ibm(Ctx *c, double *flux, double *area) {
 }
 
 }  // namespace vfs
+
+extern "C" int vfs_ibm_set_velocity(vfs_ctx *ctx, int ibi, int n_v, const double *u, const double *v,
+                                    const double *w) {
+  vfs::Ctx *c = (vfs::Ctx *)ctx;
+  if (!c || !u || !v || !w || ibi < 0 || n_v < 1) return vfs::set_err(c, VFS_ERR_INVALID, "vfs_ibm_set_velocity: bad argument");
+  if (ibi >= (int)c->vtx_base.size() || c->vtx_base[ibi] < 0 || !c->ibv)
+    return vfs::set_err(c, VFS_ERR_STATE, "vfs_ibm_set_velocity: body not searched (vfs_ibm_search first)");
+  const int next = ibi + 1 < (int)c->vtx_base.size() && c->vtx_base[ibi + 1] >= 0 ? c->vtx_base[ibi + 1] : c->nvtx;
+  if (n_v != next - c->vtx_base[ibi])
+    return vfs::set_err(c, VFS_ERR_INVALID, "vfs_ibm_set_velocity: vertex count differs from the body's");
+  cudaSetDevice(c->device);
+  const double *src[3] = {u, v, w};
+  for (int d = 0; d < 3; d++)
+    cudaMemcpyAsync(c->ibv + (size_t)d * c->nvtx + c->vtx_base[ibi], src[d], sizeof(double) * n_v,
+                    cudaMemcpyHostToDevice, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return vfs::set_err(c, VFS_ERR_CUDA, "vfs_ibm_set_velocity: copy failed");
+  return VFS_OK;
+}
 
 extern "C" int vfs_ibm_search(vfs_ctx *ctx, int ibi, int n_v, const double *x, const double *y, const double *z,
                               int n_elmt, const int *nv1, const int *nv2, const int *nv3) {

@@ -28,6 +28,8 @@ struct Grid {
   int bc[6];            // bctype
   int immersed, les;
   double ren, dt, st;
+  int wallfunction;     // -wallfunction: wall model in the IB-node reconstruction
+  int moving;           // movefsi || rotatefsi: moving bodies
 };
 
 __host__ __device__ inline long long lidx(const Grid &g, int i, int j, int k) {
@@ -133,6 +135,8 @@ struct IbNode {
   double cr[3];       // stencil weights cr1..cr3
   double cs[3];       // surface weights cs1..cs3
   double ds, di;      // distance to the surface (d_s) and to the interception (d_i)
+  int vtx[3];         // vertices of the triangle `cell` in the surface-velocity array
+  double nf[3];       // its unit normal (the wall models' n)
 };
 
 // Forward quantities of one time step that its tangent and adjoint are linearised about:
@@ -157,6 +161,10 @@ struct Ctx {
   double *f[VFS_NFIELDS][3] = {};
   int dof[VFS_NFIELDS] = {};
   uint8_t *nv = nullptr;        // nvert as uint8
+  uint8_t *nvo = nullptr;       // Nvert_o: the flags at the end of the last step (immersed)
+  double *ibv = nullptr;        // surface velocity of every body's vertices (ibm->u), 3 x nvtx
+  int nvtx = 0;                 // vertices of all bodies searched so far
+  std::vector<int> vtx_base;    // first vertex of body ibi in ibv
   // scratch for Formfunction_2 (face fluxes and Fp) and Contra2Cart
   double *div[3][3] = {};       // div1..3 x comps
   double *visc[3][3] = {};

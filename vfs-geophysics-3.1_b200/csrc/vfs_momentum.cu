@@ -351,7 +351,8 @@ int contra2cart(Ctx *c) {
   V3 out{c->bcbuf[0], c->bcbuf[1], c->bcbuf[2]};
   uint8_t *fl = c->bcflag;
   if ((rc = solid_list(c))) return rc;
-  const long long ne = edge_points(g), ns = c->nsolid;
+  // solid points get Ucat = 0, except with moving bodies (rhs.c:298)
+  const long long ne = edge_points(g), ns = g.moving ? 0 : c->nsolid;
   c->launches++, k_contra2cart_bc_edges<<<nblocks(ne, 256), 256, 0, c->stream>>>(g, m, c->nv, cv(ucat), cv(field3(c, VFS_UCAT_O)),
                                                                   out, fl);
   if (ns > 0) c->launches++, k_solid_zero<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, out, fl);

@@ -26,8 +26,9 @@ ICSI, IETA, IZET, IAJ = 16, 17, 18, 19
 JCSI, JETA, JZET, JAJ = 20, 21, 22, 23
 KCSI, KETA, KZET, KAJ = 24, 25, 26, 27
 CS = 28
-NFIELDS = 29
-FIELD_DOF = [3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 1]
+USTAR = 29
+NFIELDS = 30
+FIELD_DOF = [3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 1, 1]
 METRIC_FIELDS = {
     "csi": CSI, "eta": ETA, "zet": ZET, "aj": AJ,
     "icsi": ICSI, "ieta": IETA, "izet": IZET, "iaj": IAJ,
@@ -50,7 +51,7 @@ class VfsConfig(ctypes.Structure):
         ("i_periodic", ctypes.c_int), ("j_periodic", ctypes.c_int), ("k_periodic", ctypes.c_int),
         ("immersed", ctypes.c_int), ("les", ctypes.c_int), ("inletprofile", ctypes.c_int),
         ("dynamic_freq", ctypes.c_int), ("tistart", ctypes.c_int), ("rstart", ctypes.c_int),
-        ("reserved_i", ctypes.c_int * 5),
+        ("wallfunction", ctypes.c_int), ("moving", ctypes.c_int), ("reserved_i", ctypes.c_int * 3),
         ("ren", ctypes.c_double), ("dt", ctypes.c_double), ("st", ctypes.c_double),
         ("inlet_flux", ctypes.c_double), ("mean_pressure_gradient", ctypes.c_double),
         ("dpdz_set", ctypes.c_int), ("reserved_j", ctypes.c_int * 7),
@@ -115,6 +116,7 @@ EXPORTS = [
     "vfs_adjoint_setup", "vfs_objective", "vfs_tangent", "vfs_adjoint_gradient",
     "vfs_adjoint_op_info", "vfs_adjoint_op_check",
     "vfs_petsc_vec_write", "vfs_petsc_vec_read", "vfs_restart_write", "vfs_restart_read",
+    "vfs_ibm_set_velocity",
 ]
 
 _lib = None
@@ -172,6 +174,7 @@ def load_library(path=None):
     lib.vfs_set_inflow_plane.argtypes = [vp, vp]
     lib.vfs_ibm_search.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, vp]
     lib.vfs_ibm_list.argtypes = [vp, vp, vp, ctypes.c_int]
+    lib.vfs_ibm_set_velocity.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp]
     lib.vfs_calc_k_flux.argtypes = [vp, dp]
     lib.vfs_divergence.argtypes = [vp, dp]
     lib.vfs_poisson_solve.argtypes = [vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats)]
@@ -299,6 +302,11 @@ class Context:
                                             xs[2].ctypes.data, len(t), cols[0].ctypes.data, cols[1].ctypes.data,
                                             cols[2].ctypes.data))
         return self.get_field(NVERT)
+
+    def ibm_set_velocity(self, u, v, w, ibi=0):  # ibm->u (surface velocity of the vertices)
+        a = [np.ascontiguousarray(t, dtype=np.float64) for t in (u, v, w)]
+        self._check(self.lib.vfs_ibm_set_velocity(self.h, ibi, len(a[0]), a[0].ctypes.data, a[1].ctypes.data,
+                                                  a[2].ctypes.data))
 
     def ibm_list(self):
         """The IB-node list: ints (n, 14) i j k cell imode i1 j1 k1 i2 j2 k2 i3 j3 k3 and
@@ -477,7 +485,7 @@ def _solve_opts(precision=0, rtol=1e-10, **kw):
 def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
                 inletprofile=13, ren=3000.0, dt=0.04, st=1.0, inlet_flux=-1.0,
                 mean_pressure_gradient=0.0, dpdz_set=0, dynamic_freq=1, tistart=0, rstart=0,
-                max_cs=0.5):
+                max_cs=0.5, wallfunction=0, moving=0):
     c = VfsConfig()
     c.IM, c.JM, c.KM = IM, JM, KM
     for q in range(6):
@@ -487,4 +495,5 @@ def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, im
     c.ren, c.dt, c.st = ren, dt, st
     c.inlet_flux, c.mean_pressure_gradient, c.dpdz_set = inlet_flux, mean_pressure_gradient, dpdz_set
     c.dynamic_freq, c.tistart, c.rstart, c.max_cs = dynamic_freq, tistart, rstart, max_cs
+    c.wallfunction, c.moving = wallfunction, moving
     return c

@@ -27,6 +27,7 @@ class Case:
         self.immersed, self.les = immersed, les
         self.ren, self.dt, self.st = ren, dt, st
         self.inletprofile, self.inlet_flux = inletprofile, inlet_flux
+        self.wallfunction, self.moving = 0, 0
         self.nvert = np.zeros(self.da_shape)
         self.ucat0 = None
 
@@ -49,7 +50,8 @@ class Case:
         from . import make_config
         return make_config(self.IM, self.JM, self.KM, self.bctype, self.i_periodic,
                            self.j_periodic, self.k_periodic, self.immersed, self.les,
-                           self.inletprofile, self.ren, self.dt, self.st, self.inlet_flux)
+                           self.inletprofile, self.ren, self.dt, self.st, self.inlet_flux,
+                           wallfunction=self.wallfunction, moving=self.moving)
 
 
 def tanh_stretch(n, beta, lo, hi):
