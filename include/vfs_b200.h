@@ -117,7 +117,14 @@ typedef struct {
                         poisson.c:280-282); the first solve after the operator is built
                         starts from 0, and one after VFS_PHI is set through vfs_set_field
                         from the values set.  1: always start from 0. */
-  int reserved[4];
+  int graph;         /* vfs_step only: 1 runs the step as one CUDA graph, captured on the
+                        first such step (and again after a set-up change) and replayed: the
+                        Poisson solve's loops are conditional nodes and no kernel waits for
+                        the host.  Same kernels, same results as 0 (launched one by one).
+                        Steps with set-up work (the first step, a new operator, moving
+                        bodies, the first two LES steps of a fresh run, a recorded tape)
+                        run launched one by one. */
+  int reserved[3];
   double rtol;       /* relative residual target (default 1e-10) */
   double atol;       /* absolute residual target (default 0) */
   double reserved_d[4];

@@ -43,6 +43,7 @@ Metrics metrics(Ctx *c) {
 
 int ensure_red(Ctx *c, int n) {
   if (n <= c->red_cap) return VFS_OK;
+  c->setup_epoch++;  // a captured step holds the old buffer
   if (c->red) cudaFree(c->red);
   if (c->red_host) cudaFreeHost(c->red_host);
   c->red = nullptr; c->red_host = nullptr;
@@ -91,6 +92,42 @@ static int ensure_stage(Ctx *c, size_t bytes) {
   if (cudaMalloc(&c->stage, bytes) != cudaSuccess)
     return set_err(c, VFS_ERR_CUDA, "staging buffer allocation failed");
   c->stage_bytes = bytes;
+  return VFS_OK;
+}
+
+// Sum of nparts partials into device memory dst (a device scalar), no host wait.
+int reduce_to(Ctx *c, const double *parts, int nparts, double *dst) {
+  c->launches++, k_sum_parts<<<1, kSumThreads, 0, c->stream>>>(parts, nparts, dst);
+  return check_launch(c, "k_sum_parts");
+}
+
+// Reads the device scalars into ds_out and refreshes the host mirror of the scalars a
+// step computes.  No-op while a step is being captured (the captured step reads them back
+// with its last node).
+int ds_fetch(Ctx *c) {
+  if (c->capturing) return VFS_OK;
+  cudaMemcpyAsync(c->ds_out, c->ds, sizeof(double) * DS_COUNT, cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "device scalar read failed");
+  c->scal[VFS_S_MEAN_K_FLUX] = c->ds_out[DS_MEAN_K_FLUX];
+  c->scal[VFS_S_FLUX_IN] = c->ds_out[DS_FLUX_IN];
+  c->scal[VFS_S_FLUX_OUT] = c->ds_out[DS_FLUX_OUT];
+  return VFS_OK;
+}
+
+// Host scalars with a device copy in ds (the step's kernels read ds).
+static const int kMirror[][2] = {{VFS_S_INLET_FLUX, DS_INLET_FLUX}, {VFS_S_INLET_AREA, DS_INLET_AREA},
+                                 {VFS_S_MEAN_K_AREA, DS_MEAN_K_AREA}, {VFS_S_MEAN_K_FLUX, DS_MEAN_K_FLUX},
+                                 {VFS_S_FLUX_IN, DS_FLUX_IN}, {VFS_S_FLUX_OUT, DS_FLUX_OUT}};
+
+// Writes the host scalars that have a device copy into ds (outside a step: vfs_create,
+// vfs_set_scalar, the set-up that computes them on the host), so that host and device
+// agree between steps.
+int ds_upload(Ctx *c) {
+  for (const auto &m : kMirror) {
+    c->ds_in[m[1]] = c->scal[m[0]];
+    cudaMemcpyAsync(c->ds + m[1], c->ds_in + m[1], sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "device scalar upload failed");
   return VFS_OK;
 }
 
@@ -242,11 +279,22 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
   okm &= cudaMalloc(&c->bcflag, (size_t)g.N) == cudaSuccess;
   if (okm) cudaMemsetAsync(c->bcflag, 0, (size_t)g.N, c->stream);
   okm &= ensure_red(c, 16384) == VFS_OK;
+  okm &= cudaMalloc(&c->ds, sizeof(double) * DS_COUNT) == cudaSuccess;
+  okm &= cudaMallocHost(&c->ds_in, sizeof(double) * DS_COUNT) == cudaSuccess;
+  okm &= cudaMallocHost(&c->ds_out, sizeof(double) * DS_COUNT) == cudaSuccess;
+  okm &= cudaMalloc(&c->kd, sizeof(KryDev)) == cudaSuccess;
+  okm &= cudaMallocHost(&c->kd_host, sizeof(KryDev)) == cudaSuccess;
+  if (okm) {
+    cudaMemsetAsync(c->ds, 0, sizeof(double) * DS_COUNT, c->stream);
+    cudaMemsetAsync(c->kd, 0, sizeof(KryDev), c->stream);
+    memset(c->ds_in, 0, sizeof(double) * DS_COUNT);
+    memset(c->ds_out, 0, sizeof(double) * DS_COUNT);
+  }
   if (!okm) {
     vfs_destroy((vfs_ctx *)c);
     return set_err(nullptr, VFS_ERR_CUDA, "vfs_create: device allocation failed");
   }
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess || ds_upload(c) != VFS_OK) {
     vfs_destroy((vfs_ctx *)c);
     return set_err(nullptr, VFS_ERR_CUDA, "vfs_create: initialisation failed");
   }
@@ -276,6 +324,14 @@ int vfs_destroy(vfs_ctx *ctx) {
   if (c->inlet_nodes) cudaFree(c->inlet_nodes);
   if (c->ibn) cudaFree(c->ibn);
   if (c->ibbuf) cudaFree(c->ibbuf);
+  step_graph_free(c);
+  if (c->ds) cudaFree(c->ds);
+  if (c->ds_in) cudaFreeHost(c->ds_in);
+  if (c->ds_out) cudaFreeHost(c->ds_out);
+  if (c->kd) cudaFree(c->kd);
+  if (c->kd_host) cudaFreeHost(c->kd_host);
+  for (int q = 0; q < 2; q++)
+    if (c->cap_streams[q]) cudaStreamDestroy(c->cap_streams[q]);
   adjoint_free(c);
   Poisson &P = c->ps;
   cudaFree(P.coef); cudaFree(P.fluid);
@@ -312,6 +368,7 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
   Ctx *c = (Ctx *)ctx;
   if (!c || !host || field < 0 || field >= VFS_NFIELDS) return set_err(c, VFS_ERR_INVALID, "vfs_set_field: bad argument");
   cudaSetDevice(c->device);
+  if (field == VFS_NVERT || (field >= VFS_CSI && field <= VFS_KAJ)) c->setup_epoch++;
   const int dof = c->dof[field];
   const size_t bytes = sizeof(double) * (size_t)c->g.N * dof;
   int rc = ensure_stage(c, sizeof(double) * (size_t)c->g.N * 3);
@@ -377,7 +434,9 @@ int vfs_set_scalar(vfs_ctx *ctx, int which, double value) {
   if (which == VFS_S_REN) c->g.ren = value;
   if (which == VFS_S_ST) c->g.st = value;
   if (which == VFS_S_TI) c->ti = (int)value;
-  return VFS_OK;
+  // kernel arguments of a captured step change: capture again
+  if (which == VFS_S_DT || which == VFS_S_REN || which == VFS_S_ST || which == VFS_S_TI) c->setup_epoch++;
+  return ds_upload(c);
 }
 
 int vfs_get_scalar(vfs_ctx *ctx, int which, double *value) {
@@ -488,6 +547,7 @@ int vfs_ibm_list(vfs_ctx *ctx, int *ints, double *dbls, int cap) {
 
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
   Ctx *c = (Ctx *)ctx; VFS_REQUIRE_SETUP(c);
+  if (opts && opts->graph) return step_graph(c, opts, st);
   return step_core(c, opts, st);
 }
 
@@ -496,6 +556,49 @@ int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *st) {
 namespace vfs {
 // One time step (vfs_step); with c->tape set it also records the stage states the
 // tangent and adjoint steps need.
+// The kernels of one time step after its set-up (Flow_Solver for implicit = 0,
+// solvers.c:644-1385, and the old-value copies of the time loop): launched one by one, or
+// captured into the step graph (c->capturing), where nothing waits for the host.
+static int step_body(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *s, int *solve_rc) {
+  int rc;
+  if ((rc = calc_k_flux(c, &s->mean_k_flux))) return rc;
+  if (c->g.les) {  // solvers.c:648-654
+    if ((rc = contra2cart(c))) return rc;
+    if ((c->ti % c->dynamic_freq == 0 || c->ti == c->tistart) && (rc = smagorinsky_constant(c))) return rc;
+    if ((rc = eddy_viscosity(c))) return rc;
+  }
+  if ((rc = pressure_gradient(c))) return rc;
+  if ((rc = runge_kutta(c))) return rc;
+  if ((rc = volume_flux(c))) return rc;  // poisson_hypre.c:566
+  if ((rc = poisson_rhs(c))) return rc;
+  rc = poisson_solve(c, opts, &s->poisson);
+  if (rc && rc != VFS_ERR_NOT_CONVERGED) return rc;
+  *solve_rc = rc;
+  if ((rc = update_pressure(c))) return rc;
+  if ((rc = projection(c))) return rc;
+  if (c->g.immersed && (rc = ibm_interpolation(c))) return rc;  // solvers.c:1366-1370
+  if ((rc = divergence(c, &s->max_div))) return rc;
+  if ((rc = ib_bc(c))) return rc;
+  if ((rc = contra2cart(c))) return rc;
+  // end of the time step: keep Ucont and Ucat of this step (main.c:3584-3602), and with
+  // immersed bodies the flags as Nvert_o (main.c:3571-3573)
+  const size_t bytes = sizeof(double) * (size_t)c->g.N;
+  if (c->g.immersed) {
+    if (!c->nvo) {
+      if (c->capturing) return set_err(c, VFS_ERR_STATE, "vfs_step: Nvert_o not allocated before capture");
+      if (cudaMalloc(&c->nvo, (size_t)c->g.N) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "vfs_step: allocation failed");
+    }
+    cudaMemcpyAsync(c->nvo, c->nv, (size_t)c->g.N, cudaMemcpyDeviceToDevice, c->stream);
+  }
+  for (int q = 0; q < 3; q++) {
+    cudaMemcpyAsync(c->f[VFS_UCONT_O][q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(c->f[VFS_UCAT_O][q], c->f[VFS_UCAT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  }
+  return VFS_OK;
+}
+
+// One time step (vfs_step), its kernels launched one by one; with c->tape set it also
+// records the stage states the tangent and adjoint steps need.
 int step_core(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
   int rc;
   vfs_step_stats s;
@@ -513,38 +616,8 @@ int step_core(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
   } else if (!c->ps.built && (rc = poisson_lhs(c))) {
     return rc;
   }
-  // Flow_Solver for implicit = 0 (solvers.c:644-1385)
-  if ((rc = calc_k_flux(c, &s.mean_k_flux))) return rc;
-  if (c->g.les) {  // solvers.c:648-654
-    if ((rc = contra2cart(c))) return rc;
-    if ((c->ti % c->dynamic_freq == 0 || c->ti == c->tistart) && (rc = smagorinsky_constant(c))) return rc;
-    if ((rc = eddy_viscosity(c))) return rc;
-  }
-  if ((rc = pressure_gradient(c))) return rc;
-  if ((rc = runge_kutta(c))) return rc;
-  if ((rc = volume_flux(c))) return rc;  // poisson_hypre.c:566
-  if ((rc = poisson_rhs(c))) return rc;
-  rc = poisson_solve(c, opts, &s.poisson);
-  if (rc && rc != VFS_ERR_NOT_CONVERGED) return rc;
-  const int solve_rc = rc;
-  if ((rc = update_pressure(c))) return rc;
-  if ((rc = projection(c))) return rc;
-  if (c->g.immersed && (rc = ibm_interpolation(c))) return rc;  // solvers.c:1366-1370
-  if ((rc = divergence(c, &s.max_div))) return rc;
-  if ((rc = ib_bc(c))) return rc;
-  if ((rc = contra2cart(c))) return rc;
-  // end of the time step: keep Ucont and Ucat of this step (main.c:3584-3602), and with
-  // immersed bodies the flags as Nvert_o (main.c:3571-3573)
-  const size_t bytes = sizeof(double) * (size_t)c->g.N;
-  if (c->g.immersed) {
-    if (!c->nvo && cudaMalloc(&c->nvo, (size_t)c->g.N) != cudaSuccess)
-      return set_err(c, VFS_ERR_CUDA, "vfs_step: allocation failed");
-    cudaMemcpyAsync(c->nvo, c->nv, (size_t)c->g.N, cudaMemcpyDeviceToDevice, c->stream);
-  }
-  for (int q = 0; q < 3; q++) {
-    cudaMemcpyAsync(c->f[VFS_UCONT_O][q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
-    cudaMemcpyAsync(c->f[VFS_UCAT_O][q], c->f[VFS_UCAT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
-  }
+  int solve_rc = VFS_OK;
+  if ((rc = step_body(c, opts, &s, &solve_rc))) return rc;
   c->ti++;
   cudaEventRecord(c->ev1, c->stream);
   cudaEventSynchronize(c->ev1);
@@ -553,5 +626,89 @@ int step_core(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
   s.ms = ms;
   if (st) *st = s;
   return solve_rc;
+}
+
+void step_graph_free(Ctx *c) {
+  if (c->sg.exec) cudaGraphExecDestroy(c->sg.exec);
+  if (c->sg.graph) cudaGraphDestroy(c->sg.graph);
+  c->sg.exec = nullptr;
+  c->sg.graph = nullptr;
+  c->sg.key = -1;
+}
+
+// Whether the next step is the same sequence of kernels as the last: no set-up work and no
+// decision that changes from step to step.
+static bool graph_eligible(const Ctx *c) {
+  if (c->first_step || c->tape || !c->ps.built || c->g.moving || c->nsolid < 0) return false;
+  if (c->g.les && (c->dynamic_freq != 1 || (c->ti < 2 && c->tistart == 0 && !c->rstart))) return false;
+  return true;
+}
+
+// The step as one CUDA graph: captured when it is missing or stale, then replayed.  The
+// host reads back the device scalars and the solve's state after the replay.
+int step_graph(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
+  if (!graph_eligible(c)) return step_core(c, opts, st);
+  int rc;
+  const bool fresh = c->sg.exec && c->sg.key == c->setup_epoch && !memcmp(&c->sg.opts, opts, sizeof(*opts));
+  if (!fresh) {
+    step_graph_free(c);
+    const long long l0 = c->launches;
+    vfs_step_stats s;
+    memset(&s, 0, sizeof(s));
+    int solve_rc = VFS_OK;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return set_err(c, VFS_ERR_CUDA, "vfs_step: stream capture failed to start");
+    c->capturing = true;
+    rc = step_body(c, opts, &s, &solve_rc);
+    c->capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      c->launches = l0;
+      return rc ? rc : set_err(c, VFS_ERR_CUDA, std::string("vfs_step: capture failed: ") + cudaGetErrorString(e));
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      cudaGetLastError();
+      c->launches = l0;
+      return set_err(c, VFS_ERR_CUDA, "vfs_step: graph instantiation failed");
+    }
+    c->sg.graph = graph;
+    c->sg.exec = exec;
+    c->sg.opts = *opts;
+    c->sg.key = c->setup_epoch;
+    c->sg.launches = c->launches - l0;   // kernels of a step with one Krylov cycle and iteration
+    c->launches = l0;
+  }
+  cudaEventRecord(c->ev0, c->stream);
+  if (cudaGraphLaunch(c->sg.exec, c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "vfs_step: graph launch failed");
+  cudaEventRecord(c->ev1, c->stream);
+  cudaMemcpyAsync(c->ds_out, c->ds, sizeof(double) * DS_COUNT, cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(c->kd_host, c->kd, sizeof(KryDev), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "vfs_step: graph replay failed");
+  const KryDev &k = *c->kd_host;
+  c->launches += c->sg.launches + (long long)(k.it > 0 ? k.it - 1 : 0) * c->sg.body_launches +
+                 (long long)(k.cycles > 0 ? k.cycles - 1 : 0) * c->sg.cycle_launches;
+  c->scal[VFS_S_MEAN_K_FLUX] = c->ds_out[DS_MEAN_K_FLUX];
+  c->scal[VFS_S_FLUX_IN] = c->ds_out[DS_FLUX_IN];
+  c->scal[VFS_S_FLUX_OUT] = c->ds_out[DS_FLUX_OUT];
+  vfs_step_stats s;
+  memset(&s, 0, sizeof(s));
+  s.mean_k_flux = c->ds_out[DS_MEAN_K_FLUX];
+  s.max_div = c->ds_out[DS_MAXDIV];
+  s.poisson.iterations = k.it;
+  s.poisson.converged = k.conv ? 1 : 0;
+  s.poisson.r0 = k.r0;
+  s.poisson.rfinal = k.rnorm;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  s.ms = ms;
+  s.poisson.ms = 0;  // not timed apart inside the graph
+  c->ti++;
+  if (st) *st = s;
+  return s.poisson.converged ? VFS_OK : set_err(c, VFS_ERR_NOT_CONVERGED, "poisson_solve: iteration cap reached");
 }
 }  // namespace vfs

@@ -653,6 +653,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
   c->nvert_set = true;
   c->nsolid = -1;
   c->ps.built = false;
+  c->setup_epoch++;
   return VFS_OK;
 }
 
@@ -835,8 +836,14 @@ __device__ __forceinline__ double face_area(CV3 m, long long p) {
 }
 
 template <int PASS>
-__global__ void k_vflux_ibm(Grid g, Metrics m, const uint8_t *__restrict__ nv, V3 uc, double correction,
+__global__ void k_vflux_ibm(Grid g, Metrics m, const uint8_t *__restrict__ nv, V3 uc, const double *__restrict__ ds,
                             double *parts) {
+  // pass 1: the net flux of pass 0 spread over the IB faces in proportion to their area
+  double correction = 0;
+  if (PASS == 1) {
+    const double f = ds[DS_VF_FLUX], a = ds[DS_VF_AREA];
+    correction = (a > 1.e-15) ? f / a : 0;
+  }
   __shared__ double s1[256], s2[256];
   double fsum = 0, asum = 0;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -884,16 +891,17 @@ int volume_flux_ibm(Ctx *c, double *flux, double *area) {
   const int nb = 148 * 2;
   if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
   Metrics m = metrics(c);
-  c->launches++, k_vflux_ibm<0><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), 0.0, c->red);
+  c->launches++, k_vflux_ibm<0><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), c->ds, c->red);
   if ((rc = check_launch(c, "k_vflux_ibm"))) return rc;
-  double f = 0, a = 0;
-  if ((rc = reduce_sum(c, c->red, nb, &f))) return rc;
-  if ((rc = reduce_sum(c, c->red + nb, nb, &a))) return rc;
-  const double correction = (a > 1.e-15) ? f / a : 0;
-  c->launches++, k_vflux_ibm<1><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), correction, c->red);
+  if ((rc = reduce_to(c, c->red, nb, c->ds + DS_VF_FLUX))) return rc;
+  if ((rc = reduce_to(c, c->red + nb, nb, c->ds + DS_VF_AREA))) return rc;
+  c->launches++, k_vflux_ibm<1><<<nb, 256, 0, c->stream>>>(c->g, m, c->nv, field3(c, VFS_UCONT), c->ds, c->red);
   if ((rc = check_launch(c, "k_vflux_ibm"))) return rc;
-  if (flux) *flux = f;
-  if (area) *area = a;
+  if ((flux || area) && !c->capturing) {
+    if ((rc = ds_fetch(c))) return rc;
+    if (flux) *flux = c->ds_out[DS_VF_FLUX];
+    if (area) *area = c->ds_out[DS_VF_AREA];
+  }
   return VFS_OK;
 }
 

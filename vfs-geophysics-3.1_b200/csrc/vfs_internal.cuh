@@ -149,6 +149,41 @@ struct StepTape {
 };
 struct Adjoint;
 
+// Scalars that a step's reductions produce and later kernels of the same step read; they
+// live on the device (Ctx::ds) so that no kernel waits for the host, and the host mirror
+// (Ctx::scal) is refreshed from them after the step.  The first three are inputs the
+// host sets.
+enum DScal {
+  DS_INLET_FLUX = 0, DS_INLET_AREA, DS_MEAN_K_AREA,
+  DS_KFLUX_SUM, DS_MEAN_K_FLUX, DS_FLUX1, DS_FLUX_IN, DS_FLUX_OUT, DS_AREA_OUT,
+  DS_BSUM, DS_PHISUM, DS_MAXDIV, DS_VF_FLUX, DS_VF_AREA,
+  DS_COUNT = 16
+};
+
+// Device-side state of the flexible GMRES solve (restart <= kKryMax): the Hessenberg
+// matrix, the Givens rotations and the loop control, so that the solve's kernels decide
+// on the device (and a captured graph can loop on conditional nodes).
+constexpr int kKryMax = 31;
+struct KryDev {
+  int j, it, jdone, reorth, degen, inner_go, outer_go, conv, fresh, check, maxit, m, cycles;
+  double tol, bnorm, bb, r0, rnorm, rr, hn, scale;
+  double hdev[kKryMax + 3];
+  double h[kKryMax + 3], h2[kKryMax + 3], h3[kKryMax + 3];
+  double H[(kKryMax + 1) * kKryMax], cs[kKryMax], sn[kKryMax], gv[kKryMax + 1], y[kKryMax];
+};
+
+// A step captured as one CUDA graph (vfs_solve_opts.graph), with the options it was
+// captured for.
+struct StepGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  vfs_solve_opts opts;
+  long long key = -1;            // invalidation counter value at capture
+  long long launches = 0;        // kernels of a replay with one Krylov cycle and iteration
+  long long body_launches = 0;   // kernels of one Krylov iteration
+  long long cycle_launches = 0;  // kernels of one Krylov restart cycle outside its iterations
+};
+
 struct Ctx {
   vfs_config cfg;
   Grid g;
@@ -195,6 +230,16 @@ struct Ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   StepTape *tape = nullptr;      // set while a step records its linearisation state
   Adjoint *adj = nullptr;        // tangent/adjoint workspace (vfs_adjoint.cu)
+  // device-resident step (CUDA graph)
+  double *ds = nullptr;          // DS_COUNT device scalars
+  double *ds_in = nullptr;       // pinned: host inputs copied to ds at the start of a step
+  double *ds_out = nullptr;      // pinned: ds read back after a step
+  KryDev *kd = nullptr;          // FGMRES state on the device
+  KryDev *kd_host = nullptr;     // pinned mirror of kd (solve statistics)
+  bool capturing = false;        // launches are being captured: no host synchronisation
+  StepGraph sg;
+  long long setup_epoch = 0;     // bumped whenever a captured step would be stale
+  cudaStream_t cap_streams[2] = {nullptr, nullptr};  // bodies of the solver's two loops
 };
 
 V3 field3(Ctx *c, int f);
@@ -203,6 +248,11 @@ Metrics metrics(Ctx *c);
 // launch bookkeeping / error checking
 int check_launch(Ctx *c, const char *what);
 int set_err(Ctx *c, int code, const std::string &msg);
+// device scalars: sum of parts into ds-slot memory without a host wait; read back
+int reduce_to(Ctx *c, const double *parts, int nparts, double *dst);
+int ds_fetch(Ctx *c);
+int ds_upload(Ctx *c);
+void step_graph_free(Ctx *c);
 
 inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
@@ -224,6 +274,7 @@ int ib_bc(Ctx *c);
 int pressure_forcing_mode(const Ctx *c);
 int pressure_gradient_mode(Ctx *c, int mode, double kdiff);
 int step_core(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st);
+int step_graph(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st);
 int form_bcs_tail(Ctx *c);
 int outlet_rescale(Ctx *c);
 
@@ -264,6 +315,7 @@ int divergence(Ctx *c, double *maxdiv);
 int mg_setup(Ctx *c);
 void mg_free(Poisson &P);
 int mg_precondition(Ctx *c, const double *v, double *z, const vfs_solve_opts &o);
+int mg_precondition_dyn(Ctx *c, const double *V, double *Z, long long ldv, const int *jslot, const vfs_solve_opts &o);
 int mg_sweep_fine(Ctx *c, int precision);
 
 // reductions (deterministic two-pass); result copied to host

@@ -76,6 +76,10 @@ static int launch_chain(Ctx *c, const char *what, void (*kernel)(KArgs...), dim3
                         Args... args) {
   c->launches++;
 #if VFS_PDL
+  if (c->capturing) {  // plain launches inside a captured step
+    kernel<<<grid, block, smem, c->stream>>>(static_cast<KArgs>(args)...);
+    return check_launch(c, what);
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
@@ -744,8 +748,10 @@ __global__ void __launch_bounds__(kBottomThreads) k_mg_bottom(Bottom<T> B) {
 
 // DA-layout FP64 vector -> finest-level right-hand side.
 template <typename T>
-__global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, T *__restrict__ b) {
+__global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, const int *__restrict__ jslot, long long ldv,
+                           T *__restrict__ b) {
   pdl_prologue();
+  if (jslot) v += (long long)(*jslot) * ldv;  // the j-th basis vector of a device-driven solve
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long ncell = (long long)L.nx * L.ny * L.nz;
   if (t >= ncell) return;
@@ -757,8 +763,9 @@ __global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, T *__rest
 // Finest-level solution -> DA-layout FP64 vector (zero off the unknowns).
 template <typename T>
 __global__ void k_from_zebra(Grid g, ZL L, const uint8_t *__restrict__ fluid, const T *__restrict__ x,
-                             double *__restrict__ z) {
+                             const int *__restrict__ jslot, long long ldv, double *__restrict__ z) {
   pdl_prologue();
+  if (jslot) z += (long long)(*jslot) * ldv;
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const unsigned up = (unsigned)p, umx = (unsigned)g.mx, umy = (unsigned)g.my;
@@ -970,24 +977,30 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
 }
 
 template <typename T>
-static int mg_apply(Ctx *c, const double *v, double *z, const vfs_solve_opts &o) {
+static int mg_apply(Ctx *c, const double *v, double *z, const vfs_solve_opts &o, const int *jslot = nullptr,
+                    long long ldv = 0) {
   Poisson &P = c->ps;
   const MGLevel &L0 = P.lv[0];
   const long long ncell = (long long)L0.z.nx * L0.z.ny * L0.z.nz;
   const LvT<T> l0 = lvt<T>(L0);
   int rc;
   if ((rc = launch_chain(c, "k_to_zebra", k_to_zebra<T>, dim3(nblocks(ncell, 256)), dim3(256), 0, c->g, L0.z, v,
-                         l0.b)))
+                         jslot, ldv, l0.b)))
     return rc;
   const int nl = o.levels > 0 ? std::min((int)P.lv.size(), o.levels) : (int)P.lv.size();
   if ((rc = mg_vcycle<T>(c, 0, nl, o))) return rc;
   return launch_chain(c, "k_from_zebra", k_from_zebra<T>, dim3(nblocks(c->g.N, 256)), dim3(256), 0, c->g, L0.z,
-                      P.fluid, l0.x, z);
+                      P.fluid, l0.x, jslot, ldv, z);
 }
 
 // z = M^-1 v: one V-cycle in FP32 (precision 0) or FP64.
 int mg_precondition(Ctx *c, const double *v, double *z, const vfs_solve_opts &o) {
   return o.precision == 0 ? mg_apply<float>(c, v, z, o) : mg_apply<double>(c, v, z, o);
+}
+
+// z_j = M^-1 v_j with v_j = V + j ldv, z_j = Z + j ldv and j read on the device (*jslot).
+int mg_precondition_dyn(Ctx *c, const double *V, double *Z, long long ldv, const int *jslot, const vfs_solve_opts &o) {
+  return o.precision == 0 ? mg_apply<float>(c, V, Z, o, jslot, ldv) : mg_apply<double>(c, V, Z, o, jslot, ldv);
 }
 
 // One smoothing sweep of the finest level (both colours), for timing.

@@ -336,6 +336,7 @@ int solid_list(Ctx *c) {
     if ((rc = check_launch(c, "k_collect_solid"))) return rc;
   }
   c->nsolid = (long long)n;
+  c->setup_epoch++;
   return VFS_OK;
 }
 
@@ -1296,7 +1297,8 @@ void launch_rhs(Ctx *c) {
 #endif
 __global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, Metrics m, const uint8_t *__restrict__ nv,
                                     const double *__restrict__ P, double kdiff, double kdt,
-                                    double karea, int kforce_mode, double mpg, V3 dp) {
+                                    double karea, int kforce_mode, double mpg, const double *__restrict__ ds,
+                                    V3 dp) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
@@ -1364,7 +1366,11 @@ __global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, 
     const double kz2 = m.kzet.x[p] * m.kzet.x[p] + m.kzet.y[p] * m.kzet.y[p] + m.kzet.z[p] * m.kzet.z[p];
     const double dz = 1. / m.kaj[p] / sqrt(kz2);
     if (kforce_mode == 1) dpdz += mpg * dz;
-    else if (kforce_mode == 2) dpdz += dz * kdiff / kdt / karea;
+    else if (kforce_mode == 2) {
+      // ds: the step's device scalars (mean_k_flux - inlet_flux, mean_k_area)
+      if (ds) { kdiff = ds[DS_MEAN_K_FLUX] - ds[DS_INLET_FLUX]; karea = ds[DS_MEAN_K_AREA]; }
+      dpdz += dz * kdiff / kdt / karea;
+    }
   }
   double oz = (dpdc * g31_k + dpde * g32_k + dpdz * g33_k) * m.kaj[p] / r3;
   if (i == 0 || nv[p] + nv[p + 1] > 0 || (!g.iper && i == mx - 2)) ox = 0;
@@ -1382,21 +1388,23 @@ int pressure_forcing_mode(const Ctx *c) {
   return 0;
 }
 
-// Pressure_Gradient with an explicit forcing mode and flux deficit kdiff.
-int pressure_gradient_mode(Ctx *c, int mode, double kdiff) {
+// Pressure_Gradient with an explicit forcing mode and flux deficit kdiff (ds null), or
+// with the flux deficit of the step's device scalars (ds = c->ds).
+static int pressure_gradient_launch(Ctx *c, int mode, double kdiff, const double *ds) {
   int rc;
   // P's periodic ghosts are refreshed first (momentum.c:241-273)
   if ((rc = periodic_copy1(c, c->f[VFS_P][0]))) return rc;
   c->launches++, k_pressure_gradient<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(
       c->g, metrics(c), c->nv, c->f[VFS_P][0], kdiff, c->g.dt, c->scal[VFS_S_MEAN_K_AREA], mode,
-      c->cfg.mean_pressure_gradient, field3(c, VFS_DP));
+      c->cfg.mean_pressure_gradient, ds, field3(c, VFS_DP));
   return check_launch(c, "k_pressure_gradient");
 }
 
-int pressure_gradient(Ctx *c) {
-  return pressure_gradient_mode(c, pressure_forcing_mode(c),
-                                c->scal[VFS_S_MEAN_K_FLUX] - c->scal[VFS_S_INLET_FLUX]);
-}
+int pressure_gradient_mode(Ctx *c, int mode, double kdiff) { return pressure_gradient_launch(c, mode, kdiff, nullptr); }
+
+// The step's Pressure_Gradient: Calc_k_Flux's result and the inlet flux from the device
+// scalars (which vfs_set_scalar keeps equal to the host's between steps).
+int pressure_gradient(Ctx *c) { return pressure_gradient_launch(c, pressure_forcing_mode(c), 0.0, c->ds); }
 
 // ------------------------------------------------------------------ Calc_k_Flux
 // rhs2.c:1562-1646: sum of Ucont.z over k-faces k = 1..mz-2, interior (i,j), whose two
@@ -1422,17 +1430,24 @@ __global__ void k_kflux_parts(Grid g, const double *__restrict__ uz, const uint8
   if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
 }
 
+// ds[dst] = ds[src] / den (one thread).
+__global__ void k_ds_div(double *ds, int dst, int src, double den) { ds[dst] = ds[src] / den; }
+// ds[dst] = ds[src] (one thread).
+__global__ void k_ds_copy(double *ds, int dst, int src) { ds[dst] = ds[src]; }
+
 int calc_k_flux(Ctx *c, double *flux) {
   int rc;
   const int nb = 148 * 4;
   if ((rc = ensure_red(c, nb + 64))) return rc;
   c->launches++, k_kflux_parts<<<nb, 256, 0, c->stream>>>(c->g, c->f[VFS_UCONT][2], c->nv, c->red);
   if ((rc = check_launch(c, "k_kflux_parts"))) return rc;
-  double s = 0;
-  if ((rc = reduce_sum(c, c->red, nb, &s))) return rc;
-  s /= (c->g.mz - 2);
-  c->scal[VFS_S_MEAN_K_FLUX] = s;
-  if (flux) *flux = s;
+  if ((rc = reduce_to(c, c->red, nb, c->ds + DS_KFLUX_SUM))) return rc;
+  c->launches++, k_ds_div<<<1, 1, 0, c->stream>>>(c->ds, DS_MEAN_K_FLUX, DS_KFLUX_SUM, (double)(c->g.mz - 2));
+  if ((rc = check_launch(c, "k_ds_div"))) return rc;
+  if (!c->capturing) {
+    if ((rc = ds_fetch(c))) return rc;
+    if (flux) *flux = c->scal[VFS_S_MEAN_K_FLUX];
+  }
   return VFS_OK;
 }
 
@@ -1472,7 +1487,7 @@ int calc_inlet_area(Ctx *c) {
   if ((rc = reduce_sum(c, c->red + nb, nb, &b))) return rc;
   c->scal[VFS_S_MEAN_K_AREA] = a / (double)(c->g.mz - 2);
   if (c->g.bc[4] == 5 || c->g.kper) c->scal[VFS_S_INLET_AREA] = b;
-  return VFS_OK;
+  return ds_upload(c);
 }
 
 // ------------------------------------------------------------------ IB_BC (no IB nodes)
@@ -1539,9 +1554,12 @@ int ib_bc(Ctx *c) {
 // velocity at k = 0 is -Ucat(k=1) + 2*u(face), u from the face flux by Cramer's rule
 // (Contra2Cart_single, rhs.c:34).
 __global__ void k_inflow(Grid g, Metrics m, V3 uc, V3 ucat, const uint8_t *__restrict__ nv, int profile,
-                         double uin_const, const double *__restrict__ plane, const double *__restrict__ ynode,
-                         double *parts) {
+                         const double *__restrict__ ds, const double *__restrict__ plane,
+                         const double *__restrict__ ynode, double *parts) {
   __shared__ double sh[256];
+  // uniform inflow of profile 2: the bulk velocity from the target flux (bcs.c:399-412)
+  const double inlet_flux = ds[DS_INLET_FLUX], inlet_area = ds[DS_INLET_AREA];
+  const double uin_const = (profile == 2) ? ((inlet_flux < 0) ? 1. : inlet_flux / inlet_area) : 0.0;
   const int nx = g.mx - 2, ny = g.my - 2;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double s = 0;
@@ -1595,8 +1613,13 @@ __global__ void k_inflow(Grid g, Metrics m, V3 uc, V3 ucat, const uint8_t *__res
 
 // Flux rescaling of the inlet plane (bcs.c:579-587): Ucont.z += dflux*|zet|/inletArea on
 // faces with a fluid downstream cell, and the partial sums of the new inlet flux.
-__global__ void k_inflow_rescale(Grid g, CV3 zet, V3 uc, const uint8_t *__restrict__ nv, double dflux,
-                                 double inlet_area, double *parts) {
+__global__ void k_inflow_rescale(Grid g, CV3 zet, V3 uc, const uint8_t *__restrict__ nv, const double *__restrict__ ds,
+                                 double *parts) {
+  // the target flux and the flux of the profile from the device scalars; with no target
+  // (inlet_flux <= 0) the plane is left as it is and only summed
+  const double inlet_flux = ds[DS_INLET_FLUX], inlet_area = ds[DS_INLET_AREA];
+  const bool rescale = inlet_flux > 0;
+  const double dflux = inlet_flux - ds[DS_FLUX1];
   __shared__ double sh[256];
   const int nx = g.mx - 2, ny = g.my - 2;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1605,8 +1628,10 @@ __global__ void k_inflow_rescale(Grid g, CV3 zet, V3 uc, const uint8_t *__restri
     const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
     const long long p = lidx(g, i, j, 0), p1 = p + (long long)g.mx * g.my;
     if (nv[p1] == 0) {
-      const double A = sqrt(zet.x[p] * zet.x[p] + zet.y[p] * zet.y[p] + zet.z[p] * zet.z[p]);
-      uc.z[p] += dflux * A / inlet_area;
+      if (rescale) {
+        const double A = sqrt(zet.x[p] * zet.x[p] + zet.y[p] * zet.y[p] + zet.z[p] * zet.z[p]);
+        uc.z[p] += dflux * A / inlet_area;
+      }
       s = uc.z[p];
     }
   }
@@ -1628,26 +1653,24 @@ int inflow_flux(Ctx *c) {
     return set_err(c, VFS_ERR_STATE, "InflowFlux: inletprofile 100 needs vfs_set_inflow_plane first");
   if (prof == 21 && !c->inlet_nodes)
     return set_err(c, VFS_ERR_STATE, "InflowFlux: inletprofile 21 needs the grid nodes (vfs_form_metrics)");
-  const double inlet_flux = c->scal[VFS_S_INLET_FLUX], area = c->scal[VFS_S_INLET_AREA];
-  const double uin = (prof == 2) ? ((inlet_flux < 0) ? 1. : inlet_flux / area) : 0.0;
   const long long npl = (long long)(g.mx - 2) * (g.my - 2);
   const int nb = (int)nblocks(npl, 256);
   if ((rc = ensure_red(c, nb + 64))) return rc;
-  c->launches++, k_inflow<<<nb, 256, 0, c->stream>>>(g, metrics(c), field3(c, VFS_UCONT), field3(c, VFS_UCAT), c->nv, prof, uin,
+  c->launches++, k_inflow<<<nb, 256, 0, c->stream>>>(g, metrics(c), field3(c, VFS_UCONT), field3(c, VFS_UCAT), c->nv, prof, c->ds,
                                      c->inflow_plane, c->inlet_nodes ? c->inlet_nodes + 1 * (size_t)(g.mx - 1) * (g.my - 1) : nullptr,
                                      c->red);
   if ((rc = check_launch(c, "k_inflow"))) return rc;
-  double flux1 = 0;
-  if ((rc = reduce_sum(c, c->red, nb, &flux1))) return rc;
-  double flux_in = flux1;
-  if (prof == 100 && inlet_flux > 0) {  // bcs.c:572-588 (sumFluxIn0 = inlet_flux)
+  if ((rc = reduce_to(c, c->red, nb, c->ds + DS_FLUX1))) return rc;
+  if (prof == 100) {  // bcs.c:572-588 (sumFluxIn0 = inlet_flux), when inlet_flux > 0
     c->launches++, k_inflow_rescale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), field3(c, VFS_UCONT), c->nv,
-                                               inlet_flux - flux1, area, c->red);
+                                               c->ds, c->red);
     if ((rc = check_launch(c, "k_inflow_rescale"))) return rc;
-    if ((rc = reduce_sum(c, c->red, nb, &flux_in))) return rc;
+    if ((rc = reduce_to(c, c->red, nb, c->ds + DS_FLUX_IN))) return rc;
+  } else {
+    c->launches++, k_ds_copy<<<1, 1, 0, c->stream>>>(c->ds, DS_FLUX_IN, DS_FLUX1);
+    if ((rc = check_launch(c, "k_ds_copy"))) return rc;
   }
-  c->scal[VFS_S_FLUX_IN] = flux_in;
-  return VFS_OK;
+  return ds_fetch(c);
 }
 
 // ------------------------------------------------------------------ FormBCS subset
@@ -1679,8 +1702,9 @@ __global__ void k_outlet_parts(Grid g, CV3 zet, const double *__restrict__ uz, c
   if (threadIdx.x == 0) { parts[blockIdx.x] = s1[0]; parts[gridDim.x + blockIdx.x] = s2[0]; }
 }
 
-__global__ void k_outlet_scale(Grid g, CV3 zet, double *uz, const uint8_t *__restrict__ nv, double dflux,
-                               double area_sum) {
+__global__ void k_outlet_scale(Grid g, CV3 zet, double *uz, const uint8_t *__restrict__ nv,
+                               const double *__restrict__ ds) {
+  const double dflux = ds[DS_FLUX_IN] - ds[DS_FLUX_OUT], area_sum = ds[DS_AREA_OUT];
   const int nx = g.mx - 2, ny = g.my - 2;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)nx * ny) return;
@@ -1727,15 +1751,12 @@ int outlet_rescale(Ctx *c) {
     if ((rc = ensure_red(c, 2 * nb + 64))) return rc;
     c->launches++, k_outlet_parts<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv, c->red);
     if ((rc = check_launch(c, "k_outlet_parts"))) return rc;
-    double flux_out = 0, area_sum = 0;
-    if ((rc = reduce_sum(c, c->red, nb, &flux_out))) return rc;
-    if ((rc = reduce_sum(c, c->red + nb, nb, &area_sum))) return rc;
-    c->scal[VFS_S_FLUX_OUT] = flux_out;
-    c->launches++, k_outlet_scale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv,
-                                             c->scal[VFS_S_FLUX_IN] - flux_out, area_sum);
+    if ((rc = reduce_to(c, c->red, nb, c->ds + DS_FLUX_OUT))) return rc;
+    if ((rc = reduce_to(c, c->red + nb, nb, c->ds + DS_AREA_OUT))) return rc;
+    c->launches++, k_outlet_scale<<<nb, 256, 0, c->stream>>>(g, cv(field3(c, VFS_ZET)), c->f[VFS_UCONT][2], c->nv, c->ds);
     if ((rc = check_launch(c, "k_outlet_scale"))) return rc;
   }
-  return VFS_OK;
+  return ds_fetch(c);
 }
 
 // FormBCS after the outlet rescaling: wall fluxes, Contra2Cart, box edges.

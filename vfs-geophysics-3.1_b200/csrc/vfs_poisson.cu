@@ -307,274 +307,7 @@ __device__ __forceinline__ void block_sums(const double (&acc)[NV + 1], int nv, 
 // basis vectors are stored ldv apart, ldv a multiple of 32, and every other vector is a
 // separate allocation, so pair loads are aligned; an odd last point is done alone.
 
-// <V_t, w> (t < nv) and <w, w>.
-template <int NV>
-__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_multidot(long long N, long long ldv, const double *__restrict__ V,
-                                                          int nv, const double *__restrict__ w,
-                                                          double *__restrict__ parts) {
-  double acc[NV + 1];
-#pragma unroll
-  for (int t = 0; t <= NV; t++) acc[t] = 0;
-  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
-  for (long long p2 = tid; p2 < N2; p2 += stride) {
-    const double2 wp = w2[p2];
-#pragma unroll
-    for (int t = 0; t < NV; t++) {
-      if (t < nv) {
-        const double2 v = reinterpret_cast<const double2 *>(V + t * ldv)[p2];
-        acc[t] += v.x * wp.x + v.y * wp.y;
-      }
-    }
-    acc[NV] += wp.x * wp.x + wp.y * wp.y;
-  }
-  if ((N & 1) && tid == 0) {
-    const long long p = N - 1;
-    const double wp = w[p];
-#pragma unroll
-    for (int t = 0; t < NV; t++)
-      if (t < nv) acc[t] += V[t * ldv + p] * wp;
-    acc[NV] += wp * wp;
-  }
-  block_sums<NV>(acc, nv, parts);
-}
-
-// w -= sum_t h_t V_t, with <V_t, w> (t < nv) and <w, w> of the result.
-template <int NV>
-__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_dots(long long N, long long ldv, const double *__restrict__ V,
-                                                             int nv, const double *__restrict__ h,
-                                                             double *__restrict__ w, double *__restrict__ parts) {
-  double hr[NV], acc[NV + 1];
-#pragma unroll
-  for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
-#pragma unroll
-  for (int t = 0; t <= NV; t++) acc[t] = 0;
-  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  double2 *__restrict__ w2 = reinterpret_cast<double2 *>(w);
-  for (long long p2 = tid; p2 < N2; p2 += stride) {
-    double2 v[NV];
-#pragma unroll
-    for (int t = 0; t < NV; t++)
-      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
-    double2 s = w2[p2];
-#pragma unroll
-    for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
-    w2[p2] = s;
-#pragma unroll
-    for (int t = 0; t < NV; t++) acc[t] += v[t].x * s.x + v[t].y * s.y;
-    acc[NV] += s.x * s.x + s.y * s.y;
-  }
-  if ((N & 1) && tid == 0) {
-    const long long p = N - 1;
-    double s = w[p];
-#pragma unroll
-    for (int t = 0; t < NV; t++)
-      if (t < nv) s -= hr[t] * V[t * ldv + p];
-    w[p] = s;
-#pragma unroll
-    for (int t = 0; t < NV; t++)
-      if (t < nv) acc[t] += V[t * ldv + p] * s;
-    acc[NV] += s * s;
-  }
-  block_sums<NV>(acc, nv, parts);
-}
-
-// out = (w - sum_t h_t V_t) * scale.
-template <int NV>
-__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_scale(long long N, long long ldv, const double *__restrict__ V,
-                                                              int nv, const double *__restrict__ h,
-                                                              const double *__restrict__ w, double scale,
-                                                              double *__restrict__ out) {
-  double hr[NV];
-#pragma unroll
-  for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
-  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
-  double2 *__restrict__ o2 = reinterpret_cast<double2 *>(out);
-  for (long long p2 = tid; p2 < N2; p2 += stride) {
-    double2 v[NV];
-#pragma unroll
-    for (int t = 0; t < NV; t++)
-      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
-    double2 s = w2[p2];
-#pragma unroll
-    for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
-    s.x *= scale; s.y *= scale;
-    o2[p2] = s;
-  }
-  if ((N & 1) && tid == 0) {
-    const long long p = N - 1;
-    double s = w[p];
-#pragma unroll
-    for (int t = 0; t < NV; t++)
-      if (t < nv) s -= hr[t] * V[t * ldv + p];
-    out[p] = s * scale;
-  }
-}
-
-// r = b - A x, one point per thread, with the block sums of <r, r> in parts[blockIdx.x].
-template <int NS>
-__global__ void __launch_bounds__(256) k_residual_pt(Grid g, const double *__restrict__ coef,
-                                                     const double *__restrict__ b, const double *__restrict__ x,
-                                                     double *__restrict__ r, double *__restrict__ parts) {
-  __shared__ double sh[8];
-  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  double v2 = 0;
-  if (p < g.N) {
-    const double v = b[p] - apply_row64<NS>(g, coef, x, p);
-    r[p] = v;
-    v2 = v * v;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v2 += __shfl_down_sync(0xffffffffu, v2, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v2;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0;
-    for (int w = 0; w < 8; w++) s += sh[w];
-    parts[blockIdx.x] = s;
-  }
-}
-
-__global__ void k_sum_rows(const double *parts, int nrows, int ncols, double *out) {
-  int r = blockIdx.x;
-  if (r >= nrows) return;
-  __shared__ double sh[256];
-  double s = 0;
-  for (int q = threadIdx.x; q < ncols; q += blockDim.x) s += parts[(long long)r * ncols + q];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) out[r] = sh[0];
-}
-
-__global__ void k_scale_copy(long long n, const double *a, double s, double *b) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p < n) b[p] = a[p] * s;
-}
-// x += sum_i y_i Z_i
-__global__ void k_lincomb_add(long long n, long long ldv, const double *__restrict__ Z, int m,
-                              const double *__restrict__ y, double *__restrict__ x) {
-  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  double s = x[p];
-  for (int t = 0; t < m; t++) s += y[t] * Z[(long long)t * ldv + p];
-  x[p] = s;
-}
-
 static const int kRedBlocks = 148 * 2;
-
-// Sums the block partials of rows 0..nrows-1 (left by one of the kernels above in
-// c->red) and copies them to out on the host.
-static int finish_rows(Ctx *c, int nrows, int ncols, double *out) {
-  double *res = c->red + (long long)nrows * ncols;
-  c->launches++, k_sum_rows<<<nrows, 256, 0, c->stream>>>(c->red, nrows, ncols, res);
-  int rc;
-  if ((rc = check_launch(c, "k_sum_rows"))) return rc;
-  cudaMemcpyAsync(c->red_host, res, sizeof(double) * nrows, cudaMemcpyDeviceToHost, c->stream);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "FGMRES reduction failed");
-  for (int t = 0; t < nrows; t++) out[t] = c->red_host[t];
-  return VFS_OK;
-}
-
-// w = A z; h[0..nv-1] = <V_t, w>; h[nv] = <w, w>.
-static int apply_dots(Ctx *c, const double *z, double *w, const double *V, int nv, double *h) {
-  const int kg = kry_grid(c);
-  int rc;
-  if ((rc = poisson_apply_dev(c, z, w))) return rc;
-  const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) c->launches++, k_multidot<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else if (nv <= 8) c->launches++, k_multidot<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else if (nv <= 16) c->launches++, k_multidot<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  else c->launches++, k_multidot<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, w, c->red);
-  if ((rc = check_launch(c, "k_multidot"))) return rc;
-  return finish_rows(c, nv + 1, kg, h);
-}
-
-// w -= V h (h on the device); out[0..nv-1] = <V_t, w>; out[nv] = <w, w>.
-static int update_dots(Ctx *c, const double *V, int nv, const double *hdev, double *w, double *out) {
-  const int kg = kry_grid(c);
-  const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) c->launches++, k_update_dots<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else if (nv <= 8) c->launches++, k_update_dots<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else if (nv <= 16) c->launches++, k_update_dots<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  else c->launches++, k_update_dots<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, c->red);
-  int rc;
-  if ((rc = check_launch(c, "k_update_dots"))) return rc;
-  return finish_rows(c, nv + 1, kg, out);
-}
-
-// out = (w - V h) * scale (h on the device).
-static int update_scale(Ctx *c, const double *V, int nv, const double *hdev, const double *w, double scale,
-                        double *out) {
-  const int kg = kry_grid(c);
-  const long long N = c->g.N, ldv = c->ps.ldv;
-  if (nv <= 4) c->launches++, k_update_scale<4><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  else if (nv <= 8) c->launches++, k_update_scale<8><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  else if (nv <= 16)
-    c->launches++, k_update_scale<16><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  else c->launches++, k_update_scale<32><<<kg, kKryThreads, 0, c->stream>>>(N, ldv, V, nv, hdev, w, scale, out);
-  return check_launch(c, "k_update_scale");
-}
-
-// r = b - r and the partial sums of r.r.
-__global__ void k_sub_norm(long long n, const double *__restrict__ b, double *r, double *parts) {
-  __shared__ double sh[256];
-  double s = 0;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const double v = b[p] - r[p];
-    r[p] = v;
-    s += v * v;
-  }
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
-}
-
-// r = b - A x; returns ||r||.
-static int residual(Ctx *c, const double *b, const double *x, double *r, double *rnorm) {
-  if (c->ps.transpose) {
-    int rc;
-    if ((rc = poisson_apply_dev(c, x, r))) return rc;
-    c->launches++, k_sub_norm<<<kKryBlocks, 256, 0, c->stream>>>(c->g.N, b, r, c->red);
-    if ((rc = check_launch(c, "k_sub_norm"))) return rc;
-    double rr;
-    if ((rc = finish_rows(c, 1, kKryBlocks, &rr))) return rc;
-    *rnorm = sqrt(rr);
-    return VFS_OK;
-  }
-  // one point per thread (the grid-stride form runs at a third of the bandwidth), then the
-  // block sums in a fixed order
-  const int nb = (int)nblocks(c->g.N, 256);
-  int rc;
-  if ((rc = ensure_red(c, nb + 64))) return rc;
-  if (c->ps.nslot == 7)
-    c->launches++, k_residual_pt<7><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
-  else
-    c->launches++, k_residual_pt<NSLOT><<<nb, 256, 0, c->stream>>>(c->g, c->ps.coef, b, x, r, c->red);
-  if ((rc = check_launch(c, "k_residual_pt"))) return rc;
-  double rr;
-  if ((rc = reduce_sum(c, c->red, nb, &rr))) return rc;
-  *rnorm = sqrt(rr);
-  return VFS_OK;
-}
-
-// Copies h[0..n-1] to the device vector hdev (through the pinned staging buffer).
-static void upload_h(Ctx *c, const double *h, int n, double *hdev) {
-  for (int t = 0; t < n; t++) c->red_host[t] = h[t];
-  cudaMemcpyAsync(hdev, c->red_host, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
-}
-
 // Number of non-zero cross-derivative slots (7..18) of the operator.
 __global__ void k_count_cross(long long N, const double *__restrict__ coef, double *parts) {
   __shared__ double sh[256];
@@ -644,6 +377,7 @@ int poisson_lhs(Ctx *c) {
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "poisson_lhs failed");
   P.built = true;
   P.guess = false;  // a fresh Phi2 with the unknown numbering (poisson.c:280-282)
+  c->setup_epoch++;
   return VFS_OK;
 }
 
@@ -673,11 +407,13 @@ __global__ void k_poisson_rhs(Grid g, CV3 uc, const uint8_t *__restrict__ fluid,
   b[p] = val;
 }
 
-// b += -sum(b) * aj / sum(aj) on fluid cells (Remove_Nullspace_Scale, poisson_hypre.c:110).
-__global__ void k_shift_scaled(long long n, const uint8_t *fluid, const double *aj, double sum, double sum_aj,
-                               double *b) {
+// b += -sum(b) * aj / sum(aj) on fluid cells (Remove_Nullspace_Scale, poisson_hypre.c:110),
+// sum(b) from the device scalars.
+__global__ void k_shift_scaled(long long n, const uint8_t *fluid, const double *aj, const double *__restrict__ ds,
+                               double sum_aj, double *b) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= n || !fluid[p]) return;
+  const double sum = ds[DS_BSUM];
   double val = -sum * aj[p] / sum_aj;
   b[p] += val;
 }
@@ -701,16 +437,6 @@ __global__ void k_sum_fluid(long long n, const uint8_t *fluid, const double *a, 
     for (int w = 0; w < 8; w++) t += sh[w];
     parts[blockIdx.x] = t;
   }
-}
-
-// Sum of a over the fluid cells: one point per thread, block sums in a fixed order.
-static int sum_fluid(Ctx *c, const double *a, double *out) {
-  int rc;
-  const int nb = (int)nblocks(c->g.N, 256);
-  if ((rc = ensure_red(c, nb + 64))) return rc;
-  c->launches++, k_sum_fluid<<<nb, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, a, c->red);
-  if ((rc = check_launch(c, "k_sum_fluid"))) return rc;
-  return reduce_sum(c, c->red, nb, out);
 }
 
 // VolumeFlux(user, Ucont, ...) (poisson.c:3306-3500) without sharp-interface IB nodes
@@ -759,9 +485,12 @@ int poisson_rhs(Ctx *c) {
   int rc;
   double *b = c->f[VFS_B][0];
   if ((rc = poisson_rhs_local(c))) return rc;
-  double sum = 0;
-  if ((rc = sum_fluid(c, b, &sum))) return rc;
-  c->launches++, k_shift_scaled<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->ps.fluid, c->f[VFS_AJ][0], sum,
+  const int nb = (int)nblocks(c->g.N, 256);
+  if ((rc = ensure_red(c, nb + 64))) return rc;
+  c->launches++, k_sum_fluid<<<nb, 256, 0, c->stream>>>(c->g.N, c->ps.fluid, b, c->red);
+  if ((rc = check_launch(c, "k_sum_fluid"))) return rc;
+  if ((rc = reduce_to(c, c->red, nb, c->ds + DS_BSUM))) return rc;
+  c->launches++, k_shift_scaled<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g.N, c->ps.fluid, c->f[VFS_AJ][0], c->ds,
                                                              c->ps.sum_aj, b);
   return check_launch(c, "k_shift_scaled");
 }
@@ -790,6 +519,603 @@ __global__ void __launch_bounds__(256) k_guess(long long n, const uint8_t *__res
   }
 }
 
+// ------------------------------------------------------------------ device-driven FGMRES
+// The same FGMRES as a sequence of kernels that read the iteration state from the device
+// (KryDev): the Gram-Schmidt decisions, the Hessenberg matrix, the Givens rotations and the
+// convergence tests run in one-thread kernels, and every kernel that depends on a
+// decision reads its flag (Guard) and returns at once when it does not apply.  Launched
+// from a host loop that reads the two loop flags, or captured into a graph whose two
+// loops are conditional WHILE nodes that the control kernels set, with the same kernels
+// and therefore the same results.
+
+// Run when (*flag != 0) == want; without a flag always.
+struct Guard {
+  const int *flag;
+  int want;
+};
+__device__ __forceinline__ bool guard_off(const Guard &q) { return q.flag && ((*q.flag != 0) != (q.want != 0)); }
+static Guard always() { return Guard{nullptr, 0}; }
+
+// base + (*j + off) * ldv (base when j is null).
+struct DynPtr {
+  double *base;
+  long long ldv;
+  const int *j;
+  int off;
+  __device__ __forceinline__ double *get() const { return j ? base + (long long)(*j + off) * ldv : base; }
+};
+
+// Sets a graph conditional from the device (only in a captured solve).
+__device__ __forceinline__ void set_cond(unsigned long long h, int use, int v) {
+  if (use) cudaGraphSetConditional((cudaGraphConditionalHandle)h, v ? 1u : 0u);
+}
+
+template <int NS>
+__global__ void k_apply_dyn(Grid g, const double *__restrict__ coef, DynPtr x, double *__restrict__ y) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  y[p] = apply_row64<NS>(g, coef, x.get(), p);
+}
+__global__ void k_apply_t_dyn(Grid g, int ns, const double *__restrict__ coef, DynPtr x, double *y, Guard q) {
+  if (guard_off(q)) return;
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const double xp = x.get()[p];
+  if (xp == 0.0) return;
+  int i, j, k;
+  dijk(g, p, i, j, k);
+  for (int t = 0; t < ns; t++) {
+    const double c = coef[t * g.N + p];
+    if (c != 0.0) atomicAdd(y + nb_index(g, i, j, k, t), c * xp);
+  }
+}
+__global__ void k_zero_g(long long n, double *y, Guard q) {
+  if (guard_off(q)) return;
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p < n) y[p] = 0.0;
+}
+
+// <V_t, w> (t < nv) and <w, w> with nv = j + 1 from the device state.
+template <int NV>
+__device__ __forceinline__ void multidot_body(long long N, long long ldv, const double *__restrict__ V, int nv,
+                                              const double *__restrict__ w, double *__restrict__ parts) {
+  double acc[NV + 1];
+#pragma unroll
+  for (int t = 0; t <= NV; t++) acc[t] = 0;
+  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
+  for (long long p2 = tid; p2 < N2; p2 += stride) {
+    const double2 wp = w2[p2];
+#pragma unroll
+    for (int t = 0; t < NV; t++) {
+      if (t < nv) {
+        const double2 v = reinterpret_cast<const double2 *>(V + t * ldv)[p2];
+        acc[t] += v.x * wp.x + v.y * wp.y;
+      }
+    }
+    acc[NV] += wp.x * wp.x + wp.y * wp.y;
+  }
+  if ((N & 1) && tid == 0) {
+    const long long p = N - 1;
+    const double wp = w[p];
+#pragma unroll
+    for (int t = 0; t < NV; t++)
+      if (t < nv) acc[t] += V[t * ldv + p] * wp;
+    acc[NV] += wp * wp;
+  }
+  block_sums<NV>(acc, nv, parts);
+}
+__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_multidot_dyn(long long N, long long ldv,
+                                                                             const double *__restrict__ V,
+                                                                             const KryDev *__restrict__ kd,
+                                                                             const double *__restrict__ w,
+                                                                             double *__restrict__ parts) {
+  const int nv = kd->j + 1;
+  if (nv <= 4) multidot_body<4>(N, ldv, V, nv, w, parts);
+  else if (nv <= 8) multidot_body<8>(N, ldv, V, nv, w, parts);
+  else if (nv <= 16) multidot_body<16>(N, ldv, V, nv, w, parts);
+  else multidot_body<32>(N, ldv, V, nv, w, parts);
+}
+
+// w -= sum_t h_t V_t (h = kd->hdev), with <V_t, w> and <w, w> of the result.
+template <int NV>
+__device__ __forceinline__ void update_dots_body(long long N, long long ldv, const double *__restrict__ V, int nv,
+                                                 const double *__restrict__ h, double *__restrict__ w,
+                                                 double *__restrict__ parts) {
+  double hr[NV], acc[NV + 1];
+#pragma unroll
+  for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
+#pragma unroll
+  for (int t = 0; t <= NV; t++) acc[t] = 0;
+  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double2 *__restrict__ w2 = reinterpret_cast<double2 *>(w);
+  for (long long p2 = tid; p2 < N2; p2 += stride) {
+    double2 v[NV];
+#pragma unroll
+    for (int t = 0; t < NV; t++)
+      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
+    double2 s = w2[p2];
+#pragma unroll
+    for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
+    w2[p2] = s;
+#pragma unroll
+    for (int t = 0; t < NV; t++) acc[t] += v[t].x * s.x + v[t].y * s.y;
+    acc[NV] += s.x * s.x + s.y * s.y;
+  }
+  if ((N & 1) && tid == 0) {
+    const long long p = N - 1;
+    double s = w[p];
+#pragma unroll
+    for (int t = 0; t < NV; t++)
+      if (t < nv) s -= hr[t] * V[t * ldv + p];
+    w[p] = s;
+#pragma unroll
+    for (int t = 0; t < NV; t++)
+      if (t < nv) acc[t] += V[t * ldv + p] * s;
+    acc[NV] += s * s;
+  }
+  block_sums<NV>(acc, nv, parts);
+}
+__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_dots_dyn(long long N, long long ldv,
+                                                                                const double *__restrict__ V,
+                                                                                const KryDev *__restrict__ kd,
+                                                                                double *__restrict__ w,
+                                                                                double *__restrict__ parts, Guard q) {
+  if (guard_off(q)) return;
+  const int nv = kd->j + 1;
+  if (nv <= 4) update_dots_body<4>(N, ldv, V, nv, kd->hdev, w, parts);
+  else if (nv <= 8) update_dots_body<8>(N, ldv, V, nv, kd->hdev, w, parts);
+  else if (nv <= 16) update_dots_body<16>(N, ldv, V, nv, kd->hdev, w, parts);
+  else update_dots_body<32>(N, ldv, V, nv, kd->hdev, w, parts);
+}
+
+// out = (w - sum_t h_t V_t) * scale (h = kd->hdev, scale = kd->scale).
+template <int NV>
+__device__ __forceinline__ void update_scale_body(long long N, long long ldv, const double *__restrict__ V, int nv,
+                                                  const double *__restrict__ h, const double *__restrict__ w,
+                                                  double scale, double *__restrict__ out) {
+  double hr[NV];
+#pragma unroll
+  for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
+  const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
+  double2 *__restrict__ o2 = reinterpret_cast<double2 *>(out);
+  for (long long p2 = tid; p2 < N2; p2 += stride) {
+    double2 v[NV];
+#pragma unroll
+    for (int t = 0; t < NV; t++)
+      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
+    double2 s = w2[p2];
+#pragma unroll
+    for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
+    s.x *= scale; s.y *= scale;
+    o2[p2] = s;
+  }
+  if ((N & 1) && tid == 0) {
+    const long long p = N - 1;
+    double s = w[p];
+#pragma unroll
+    for (int t = 0; t < NV; t++)
+      if (t < nv) s -= hr[t] * V[t * ldv + p];
+    out[p] = s * scale;
+  }
+}
+__global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_scale_dyn(long long N, long long ldv,
+                                                                                 const double *__restrict__ V,
+                                                                                 const KryDev *__restrict__ kd,
+                                                                                 const double *__restrict__ w,
+                                                                                 DynPtr out, Guard q) {
+  if (guard_off(q)) return;
+  const int nv = kd->j + 1;
+  double *o = out.get();
+  if (nv <= 4) update_scale_body<4>(N, ldv, V, nv, kd->hdev, w, kd->scale, o);
+  else if (nv <= 8) update_scale_body<8>(N, ldv, V, nv, kd->hdev, w, kd->scale, o);
+  else if (nv <= 16) update_scale_body<16>(N, ldv, V, nv, kd->hdev, w, kd->scale, o);
+  else update_scale_body<32>(N, ldv, V, nv, kd->hdev, w, kd->scale, o);
+}
+
+// Rows 0..nrows-1 of the block partials summed in a fixed order; nrows = j + 2 (the nv
+// dot products and the norm) from the device state.
+__global__ void k_sum_rows_dyn(const double *parts, const KryDev *kd, int ncols, double *out, Guard q) {
+  if (guard_off(q)) return;
+  const int r = blockIdx.x;
+  if (r >= kd->j + 2) return;
+  __shared__ double sh[256];
+  double s = 0;
+  for (int t = threadIdx.x; t < ncols; t += blockDim.x) s += parts[(long long)r * ncols + t];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[r] = sh[0];
+}
+
+// Sum of n partials (one block, fixed order, as k_sum_parts) into out, guarded.
+__global__ void __launch_bounds__(1024) k_sum_parts_g(const double *parts, int n, double *out, Guard q) {
+  if (guard_off(q)) return;
+  __shared__ double sh[32];
+  double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int t = threadIdx.x;
+  for (; t + 7 * 1024 < n; t += 8 * 1024) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) s[u] += parts[t + u * 1024];
+  }
+  for (; t < n; t += 1024) s[0] += parts[t];
+  double v = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = sh[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) out[0] = v;
+  }
+}
+
+// r = b - A x with the block sums of <r, r>, guarded.
+template <int NS>
+__global__ void __launch_bounds__(256) k_residual_g(Grid g, const double *__restrict__ coef,
+                                                    const double *__restrict__ b, const double *__restrict__ x,
+                                                    double *__restrict__ r, double *__restrict__ parts, Guard q) {
+  if (guard_off(q)) return;
+  __shared__ double sh[8];
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double v2 = 0;
+  if (p < g.N) {
+    const double v = b[p] - apply_row64<NS>(g, coef, x, p);
+    r[p] = v;
+    v2 = v * v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v2 += __shfl_down_sync(0xffffffffu, v2, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < 8; w++) s += sh[w];
+    parts[blockIdx.x] = s;
+  }
+}
+// r = b - r (r holding A x) and the partial sums of <r, r>, guarded (grid-stride).
+__global__ void k_sub_norm_g(long long n, const double *__restrict__ b, double *r, double *parts, Guard q) {
+  if (guard_off(q)) return;
+  __shared__ double sh[256];
+  double s = 0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const double v = b[p] - r[p];
+    r[p] = v;
+    s += v * v;
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
+}
+
+// dst = src * (*scale), guarded.
+__global__ void k_scale_copy_dyn(long long n, const double *__restrict__ src, const double *__restrict__ scale,
+                                 DynPtr dst, Guard q) {
+  if (guard_off(q)) return;
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p < n) dst.get()[p] = src[p] * (*scale);
+}
+// x += sum_t y_t Z_t for t < kd->jdone (y = kd->y).
+__global__ void k_lincomb_add_dyn(long long n, long long ldv, const double *__restrict__ Z,
+                                  const KryDev *__restrict__ kd, double *__restrict__ x) {
+  const int m = kd->jdone;
+  if (m <= 0) return;
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  double s = x[p];
+  for (int t = 0; t < m; t++) s += kd->y[t] * Z[(long long)t * ldv + p];
+  x[p] = s;
+}
+// x += -sum / nfluid on the fluid cells (sum = ds[DS_PHISUM]).
+__global__ void k_shift_mean(long long n, const uint8_t *fluid, const double *__restrict__ ds, double nfluid,
+                             double *x) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= n || !fluid[p]) return;
+  const double val = -ds[DS_PHISUM] / nfluid;
+  x[p] += val;
+}
+
+// ---- control kernels (one thread)
+// After the initial residual (kd->rr) and, with a starting guess, <b, b> (kd->bb).
+__global__ void k_kry_init(KryDev *kd, double rtol, double atol, int warm, int maxit, int m, unsigned long long h_outer,
+                           int use_graph) {
+  kd->rnorm = sqrt(kd->rr);
+  kd->bnorm = warm ? sqrt(kd->bb) : kd->rnorm;
+  kd->r0 = kd->rnorm;
+  kd->tol = fmax(rtol * kd->bnorm, atol);
+  kd->it = 0;
+  kd->cycles = 0;
+  kd->maxit = maxit;
+  kd->m = m;
+  kd->conv = kd->bnorm <= kd->tol;
+  kd->fresh = 1;
+  kd->jdone = 0;
+  kd->outer_go = !kd->conv && kd->it < maxit;
+  set_cond(h_outer, use_graph, kd->outer_go);
+}
+// Start of a restart cycle (kd->rr holds <r, r> of a new residual unless kd->fresh).
+__global__ void k_kry_cycle(KryDev *kd, unsigned long long h_inner, int use_graph) {
+  kd->cycles++;
+  if (!kd->fresh) kd->rnorm = sqrt(kd->rr);
+  kd->fresh = 0;
+  const double beta = kd->rnorm;
+  kd->j = 0;
+  kd->jdone = 0;
+  kd->check = 0;
+  if (beta <= kd->tol) {
+    kd->conv = 1;
+    kd->inner_go = 0;
+    kd->scale = 0;
+  } else {
+    kd->scale = 1.0 / beta;
+    for (int t = 0; t <= kd->m; t++) kd->gv[t] = 0.0;
+    kd->gv[0] = beta;
+    kd->inner_go = kd->it < kd->maxit;
+  }
+  set_cond(h_inner, use_graph, kd->inner_go);
+}
+// After h = V^T w and h[nv] = <w, w>: one Gram-Schmidt pass, or re-orthogonalise.
+__global__ void k_kry_ctl_a(KryDev *kd) {
+  const int j = kd->j, nv = j + 1, m = kd->m;
+  double proj0 = 0;
+  for (int t = 0; t < nv; t++) proj0 += kd->h[t] * kd->h[t];
+  const double hn2_0 = kd->h[nv] - proj0;  // |w - V h|^2 for orthonormal V
+  for (int t = 0; t < nv; t++) kd->hdev[t] = kd->h[t];
+  kd->degen = 0;
+  if (hn2_0 > 0.5 * kd->h[nv]) {
+    for (int t = 0; t < nv; t++) kd->H[t * m + j] = kd->h[t];
+    kd->hn = sqrt(hn2_0);
+    kd->scale = 1.0 / kd->hn;
+    kd->reorth = 0;
+  } else {
+    kd->reorth = 1;
+  }
+}
+// After w -= V h and h2 = V^T w: the second pass.
+__global__ void k_kry_ctl_b(KryDev *kd) {
+  if (!kd->reorth) return;
+  const int j = kd->j, nv = j + 1, m = kd->m;
+  const double ww = kd->h2[nv];
+  double proj = 0;
+  for (int t = 0; t < nv; t++) proj += kd->h2[t] * kd->h2[t];
+  const double hn2 = ww - proj;  // |w - V h2|^2 for orthonormal V
+  for (int t = 0; t < nv; t++) {
+    kd->hdev[t] = kd->h2[t];
+    kd->H[t * m + j] = kd->h[t] + kd->h2[t];
+  }
+  if (hn2 > 1e-4 * ww) {
+    kd->hn = sqrt(hn2);
+    kd->scale = 1.0 / kd->hn;
+    kd->degen = 0;
+  } else {
+    kd->degen = 1;  // w nearly in span(V): form w - V h2 and take its norm
+  }
+}
+// After the explicit w -= V h2 (degenerate case).
+__global__ void k_kry_ctl_c(KryDev *kd) {
+  if (!kd->degen) return;
+  const int nv = kd->j + 1;
+  kd->hn = sqrt(fmax(kd->h3[nv], 0.0));
+  kd->scale = kd->hn > 0 ? 1.0 / kd->hn : 0.0;
+}
+// Hessenberg column j: Givens rotations, residual estimate, loop control.
+__global__ void k_kry_givens(KryDev *kd, unsigned long long h_inner, int use_graph) {
+  const int j = kd->j, m = kd->m;
+  double *H = kd->H;
+  H[(j + 1) * m + j] = kd->hn;
+  for (int t = 0; t < j; t++) {
+    const double a = H[t * m + j], bb = H[(t + 1) * m + j];
+    H[t * m + j] = kd->cs[t] * a + kd->sn[t] * bb;
+    H[(t + 1) * m + j] = -kd->sn[t] * a + kd->cs[t] * bb;
+  }
+  const double a = H[j * m + j], bb = H[(j + 1) * m + j];
+  const double den = sqrt(a * a + bb * bb);
+  kd->cs[j] = den > 0 ? a / den : 1.0;
+  kd->sn[j] = den > 0 ? bb / den : 0.0;
+  H[j * m + j] = den;
+  H[(j + 1) * m + j] = 0;
+  kd->gv[j + 1] = -kd->sn[j] * kd->gv[j];
+  kd->gv[j] = kd->cs[j] * kd->gv[j];
+  kd->it++;
+  kd->jdone = j + 1;
+  kd->rnorm = fabs(kd->gv[j + 1]);
+  const bool stop = kd->rnorm <= kd->tol || kd->hn == 0;
+  kd->j = j + 1;
+  kd->inner_go = !stop && kd->j < m && kd->it < kd->maxit;
+  set_cond(h_inner, use_graph, kd->inner_go);
+}
+// Back substitution (y into hdev for the update) and the test for the true residual.
+__global__ void k_kry_backsub(KryDev *kd) {
+  const int jd = kd->jdone, m = kd->m;
+  for (int t = jd - 1; t >= 0; t--) {
+    double sum = kd->gv[t];
+    for (int u = t + 1; u < jd; u++) sum -= kd->H[t * m + u] * kd->y[u];
+    kd->y[t] = sum / kd->H[t * m + t];
+  }
+  kd->check = (jd > 0 && kd->rnorm <= kd->tol) ? 1 : 0;
+}
+// After the confirming residual (when kd->check): convergence and the outer loop.
+__global__ void k_kry_confirm(KryDev *kd, unsigned long long h_outer, int use_graph) {
+  if (kd->check) {
+    kd->rnorm = sqrt(kd->rr);
+    kd->fresh = 1;
+    kd->conv = kd->rnorm <= kd->tol * 1.0000001 || kd->rnorm <= 2 * kd->tol;
+  }
+  kd->outer_go = !kd->conv && kd->it < kd->maxit;
+  set_cond(h_outer, use_graph, kd->outer_go);
+}
+
+// ---- host side
+static DynPtr dyn(double *base, long long ldv, const int *j, int off) { return DynPtr{base, ldv, j, off}; }
+
+// r = b - A x and <r, r> into *rr, under guard q.
+static int residual_dev(Ctx *c, const double *b, double *x, double *r, double *rr, Guard q) {
+  Poisson &P = c->ps;
+  const long long N = c->g.N;
+  int rc;
+  if (P.transpose) {
+    c->launches++, k_zero_g<<<nblocks(N, 256), 256, 0, c->stream>>>(N, r, q);
+    c->launches++, k_apply_t_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, P.nslot, P.coef, dyn(x, 0, nullptr, 0), r, q);
+    c->launches++, k_sub_norm_g<<<kKryBlocks, 256, 0, c->stream>>>(N, b, r, c->red, q);
+    if ((rc = check_launch(c, "residual (transposed)"))) return rc;
+    c->launches++, k_sum_parts_g<<<1, 1024, 0, c->stream>>>(c->red, kKryBlocks, rr, q);
+    return check_launch(c, "k_sum_parts_g");
+  }
+  const int nb = (int)nblocks(N, 256);
+  if (P.nslot == 7)
+    c->launches++, k_residual_g<7><<<nb, 256, 0, c->stream>>>(c->g, P.coef, b, x, r, c->red, q);
+  else
+    c->launches++, k_residual_g<NSLOT><<<nb, 256, 0, c->stream>>>(c->g, P.coef, b, x, r, c->red, q);
+  if ((rc = check_launch(c, "k_residual_g"))) return rc;
+  c->launches++, k_sum_parts_g<<<1, 1024, 0, c->stream>>>(c->red, nb, rr, q);
+  return check_launch(c, "k_sum_parts_g");
+}
+
+// w = A z_j (z_j = Z + j ldv with j from the device state).
+static int apply_dyn(Ctx *c, double *Z, double *w) {
+  Poisson &P = c->ps;
+  const long long N = c->g.N;
+  KryDev *kd = c->kd;
+  if (P.transpose) {
+    c->launches++, k_zero_g<<<nblocks(N, 256), 256, 0, c->stream>>>(N, w, always());
+    c->launches++, k_apply_t_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, P.nslot, P.coef,
+                                                                          dyn(Z, P.ldv, &kd->j, 0), w, always());
+    return check_launch(c, "k_apply_t_dyn");
+  }
+  if (P.nslot == 7)
+    c->launches++, k_apply_dyn<7><<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, P.coef, dyn(Z, P.ldv, &kd->j, 0), w);
+  else
+    c->launches++, k_apply_dyn<NSLOT><<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, P.coef, dyn(Z, P.ldv, &kd->j, 0), w);
+  return check_launch(c, "k_apply_dyn");
+}
+
+// One Arnoldi step of the device-driven FGMRES (body of the inner loop).
+static int kry_body(Ctx *c, const vfs_solve_opts &o, unsigned long long h_inner, int use_graph) {
+  Poisson &P = c->ps;
+  KryDev *kd = c->kd;
+  const long long N = c->g.N;
+  const int kg = kry_grid(c);
+  int rc;
+  if ((rc = mg_precondition_dyn(c, P.V, P.Z, P.ldv, &kd->j, o))) return rc;          // z_j = M^-1 v_j
+  if ((rc = apply_dyn(c, P.Z, P.w))) return rc;                                          // w = A z_j
+  c->launches++, k_multidot_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w, c->red);
+  c->launches++, k_sum_rows_dyn<<<kKryMax + 2, 256, 0, c->stream>>>(c->red, kd, kg, kd->h, always());
+  c->launches++, k_kry_ctl_a<<<1, 1, 0, c->stream>>>(kd);
+  if ((rc = check_launch(c, "FGMRES Gram-Schmidt"))) return rc;
+  const Guard reorth{&kd->reorth, 1}, degen{&kd->degen, 1}, plain{&kd->degen, 0};
+  c->launches++, k_update_dots_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w, c->red, reorth);
+  c->launches++, k_sum_rows_dyn<<<kKryMax + 2, 256, 0, c->stream>>>(c->red, kd, kg, kd->h2, reorth);
+  c->launches++, k_kry_ctl_b<<<1, 1, 0, c->stream>>>(kd);
+  c->launches++, k_update_dots_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w, c->red, degen);
+  c->launches++, k_sum_rows_dyn<<<kKryMax + 2, 256, 0, c->stream>>>(c->red, kd, kg, kd->h3, degen);
+  c->launches++, k_kry_ctl_c<<<1, 1, 0, c->stream>>>(kd);
+  if ((rc = check_launch(c, "FGMRES re-orthogonalisation"))) return rc;
+  c->launches++, k_update_scale_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w,
+                                                                         dyn(P.V, P.ldv, &kd->j, 1), plain);
+  c->launches++, k_scale_copy_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, &kd->scale,
+                                                                           dyn(P.V, P.ldv, &kd->j, 1), degen);
+  c->launches++, k_kry_givens<<<1, 1, 0, c->stream>>>(kd, h_inner, use_graph);
+  return check_launch(c, "FGMRES Givens");
+}
+
+static int kry_cycle_start(Ctx *c, const double *b, double *x, unsigned long long h_inner, int use_graph) {
+  Poisson &P = c->ps;
+  KryDev *kd = c->kd;
+  const long long N = c->g.N;
+  int rc;
+  if ((rc = residual_dev(c, b, x, P.r, &kd->rr, Guard{&kd->fresh, 0}))) return rc;
+  c->launches++, k_kry_cycle<<<1, 1, 0, c->stream>>>(kd, h_inner, use_graph);
+  c->launches++, k_scale_copy_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.r, &kd->scale, dyn(P.V, P.ldv, nullptr, 0),
+                                                                           Guard{&kd->inner_go, 1});
+  return check_launch(c, "FGMRES cycle start");
+}
+
+static int kry_cycle_end(Ctx *c, const double *b, double *x, unsigned long long h_outer, int use_graph) {
+  Poisson &P = c->ps;
+  KryDev *kd = c->kd;
+  const long long N = c->g.N;
+  int rc;
+  c->launches++, k_kry_backsub<<<1, 1, 0, c->stream>>>(kd);
+  c->launches++, k_lincomb_add_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z, kd, x);
+  if ((rc = check_launch(c, "FGMRES update"))) return rc;
+  if ((rc = residual_dev(c, b, x, P.r, &kd->rr, Guard{&kd->check, 1}))) return rc;
+  c->launches++, k_kry_confirm<<<1, 1, 0, c->stream>>>(kd, h_outer, use_graph);
+  return check_launch(c, "FGMRES confirm");
+}
+
+// Reads one int of the device state (host loop of the stream form).
+static int read_flag(Ctx *c, const int *dev, int *out) {
+  cudaMemcpyAsync(&c->kd_host->inner_go, dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "FGMRES: flag read failed");
+  *out = c->kd_host->inner_go;
+  return VFS_OK;
+}
+
+// A WHILE conditional node on the graph being captured on c->stream, its body captured
+// on cap_streams[level] (c->stream switched to it until while_end).
+struct WhileLoop {
+  cudaGraphNode_t node;
+  cudaStream_t outer;
+};
+static int cond_handle(Ctx *c, cudaGraphConditionalHandle *h) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t graph;
+  if (cudaStreamGetCaptureInfo(c->stream, &st, nullptr, &graph, nullptr, nullptr) != cudaSuccess ||
+      st != cudaStreamCaptureStatusActive)
+    return set_err(c, VFS_ERR_CUDA, "step graph: stream not capturing");
+  if (cudaGraphConditionalHandleCreate(h, graph, 0, 0) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "step graph: conditional handle creation failed");
+  return VFS_OK;
+}
+static int while_begin(Ctx *c, int level, cudaGraphConditionalHandle h, WhileLoop &w) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t graph;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  if (cudaStreamGetCaptureInfo(c->stream, &st, nullptr, &graph, &deps, &ndeps) != cudaSuccess ||
+      st != cudaStreamCaptureStatusActive)
+    return set_err(c, VFS_ERR_CUDA, "step graph: stream not capturing");
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  if (cudaGraphAddNode(&w.node, graph, deps, ndeps, &p) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "step graph: conditional node creation failed");
+  if (cudaStreamUpdateCaptureDependencies(c->stream, &w.node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "step graph: capture dependencies");
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  if (!c->cap_streams[level] && cudaStreamCreateWithFlags(&c->cap_streams[level], cudaStreamNonBlocking) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "step graph: stream creation failed");
+  if (cudaStreamBeginCaptureToGraph(c->cap_streams[level], body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+      cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "step graph: body capture failed");
+  w.outer = c->stream;
+  c->stream = c->cap_streams[level];
+  return VFS_OK;
+}
+static int while_end(Ctx *c, WhileLoop &w) {
+  cudaGraph_t body = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &body);
+  c->stream = w.outer;
+  if (e != cudaSuccess) return set_err(c, VFS_ERR_CUDA, std::string("step graph: body capture: ") + cudaGetErrorString(e));
+  return VFS_OK;
+}
+
 // Right-preconditioned flexible GMRES (Saad 1993) in FP64 with classical Gram-Schmidt,
 // re-orthogonalised where the first pass loses more than half the norm.  Solves A phi = b
 // for the fluid unknowns, then removes the mean (Remove_Nullspace) and fills the grid Phi
@@ -801,6 +1127,8 @@ __global__ void __launch_bounds__(256) k_guess(long long n, const uint8_t *__res
 // the unknowns (P.guess), so the first solve after the operator is built starts from 0
 // and later ones from the last Phi; zero_guess = 1 always starts from 0.  The target is
 // rtol * ||b|| either way, as in HYPRE's GMRES.
+// The iteration runs on the device (KryDev); the host drives its two loops by reading
+// their flags, or, while a step is captured, the loops are conditional WHILE nodes.
 int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   vfs_solve_opts o;
   memset(&o, 0, sizeof(o));
@@ -818,13 +1146,14 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
     if (oin->rtol > 0) o.rtol = oin->rtol;
     if (oin->atol > 0) o.atol = oin->atol;
   }
-  if (o.restart > 31) o.restart = 31;
+  if (o.restart > kKryMax) o.restart = kKryMax;
   if (o.pre_smooth < 1) o.pre_smooth = 1;
   if (o.coarse_iters < 1) o.coarse_iters = 1;
   Poisson &P = c->ps;
   const long long N = c->g.N;
   int rc;
   if (P.restart < o.restart) {
+    if (c->capturing) return set_err(c, VFS_ERR_STATE, "poisson_solve: Krylov basis not allocated before capture");
     cudaFree(P.V); cudaFree(P.Z);
     P.V = P.Z = nullptr;
     P.ldv = (N + 31) / 32 * 32;
@@ -833,145 +1162,84 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       return set_err(c, VFS_ERR_CUDA, "poisson_solve: Krylov basis allocation failed");
     P.restart = o.restart;
   }
-  if (!P.hdev && cudaMalloc(&P.hdev, sizeof(double) * 64) != cudaSuccess)
-    return set_err(c, VFS_ERR_CUDA, "poisson_solve: allocation failed");
-  if ((rc = ensure_red(c, 34 * std::max(kKryBlocks, kry_grid(c)) + 64))) return rc;
-  cudaEventRecord(c->ev0, c->stream);
+  if ((rc = ensure_red(c, 34 * std::max(kKryBlocks, kry_grid(c)) + (int)nblocks(N, 256) + 64))) return rc;
+  if (!c->capturing) cudaEventRecord(c->ev0, c->stream);
+  KryDev *kd = c->kd;
   double *x = c->f[VFS_PHI][0];
   const double *b = c->f[VFS_B][0];
   const bool warm = P.guess && !o.zero_guess && !P.transpose;
-  double bnorm = 0;
   if (warm) {
     const int nb = (int)nblocks(N, 256);
-    if ((rc = ensure_red(c, nb + 64))) return rc;
     c->launches++, k_guess<<<nb, 256, 0, c->stream>>>(N, P.fluid, b, x, c->red);
+    c->launches++, k_sum_parts_g<<<1, 1024, 0, c->stream>>>(c->red, nb, &kd->bb, always());
     if ((rc = check_launch(c, "k_guess"))) return rc;
-    double bb = 0;
-    if ((rc = reduce_sum(c, c->red, nb, &bb))) return rc;
-    bnorm = sqrt(bb);
   } else {
     cudaMemsetAsync(x, 0, sizeof(double) * N, c->stream);
   }
+  if ((rc = residual_dev(c, b, x, P.r, &kd->rr, always()))) return rc;  // from x = 0: r = b
   const int m = o.restart;
-  std::vector<double> H((m + 1) * m), cs(m), sn(m), gv(m + 1), y(m), h(m + 2), h2(m + 2);
-  vfs_solve_stats s;
-  memset(&s, 0, sizeof(s));
-  double rnorm = 0;
-  if ((rc = residual(c, b, x, P.r, &rnorm))) return rc;  // from x = 0: r = b
-  if (!warm) bnorm = rnorm;
-  s.r0 = rnorm;
-  const double tol = std::max(o.rtol * bnorm, o.atol);
-  int it = 0;
-  bool conv = bnorm <= tol;
-  bool fresh = true;  // P.r holds b - A x for the current x
-  while (!conv && it < o.max_iter) {
-    if (!fresh && (rc = residual(c, b, x, P.r, &rnorm))) return rc;
-    fresh = false;
-    const double beta = rnorm;
-    if (beta <= tol) { conv = true; break; }
-    c->launches++, k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.r, 1.0 / beta, P.V);
-    if ((rc = check_launch(c, "k_scale_copy"))) return rc;
-    std::fill(gv.begin(), gv.end(), 0.0);
-    gv[0] = beta;
-    int jdone = 0;
-    for (int j = 0; j < m && it < o.max_iter; j++) {
-      const int nv = j + 1;
-      double *Vj = P.V + (long long)j * P.ldv, *Zj = P.Z + (long long)j * P.ldv;
-      if ((rc = mg_precondition(c, Vj, Zj, o))) return rc;
-      // classical Gram-Schmidt, re-orthogonalised when the first pass cancels more than half
-      // of w: (1) w = A z_j and h = V^T w; then either (2) v_{j+1} = (w - V h)/|.| or
-      // (2') w -= V h and h2 = V^T w, (3') v_{j+1} = (w - V h2)/|.|
-      if ((rc = apply_dots(c, Zj, P.w, P.V, nv, h.data()))) return rc;
-      upload_h(c, h.data(), nv, P.hdev);
-      double proj0 = 0;
-      for (int t = 0; t < nv; t++) proj0 += h[t] * h[t];
-      const double hn2_0 = h[nv] - proj0;  // |w - V h|^2 for orthonormal V
-      double *Vn = P.V + (long long)(j + 1) * P.ldv;
-      double hn;
-      if (hn2_0 > 0.5 * h[nv]) {
-        // w kept more than half its norm: one Gram-Schmidt pass is enough (the
-        // Daniel-Gragg-Kaufman-Stewart criterion), v_{j+1} = (w - V h)/|.|
-        for (int t = 0; t < nv; t++) H[t * m + j] = h[t];
-        hn = sqrt(hn2_0);
-        if ((rc = update_scale(c, P.V, nv, P.hdev, P.w, 1.0 / hn, Vn))) return rc;
-      } else {
-        // re-orthogonalise: w -= V h and h2 = V^T w, then v_{j+1} = (w - V h2)/|.|
-        if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h2.data()))) return rc;
-        const double ww = h2[nv];
-        double proj = 0;
-        for (int t = 0; t < nv; t++) proj += h2[t] * h2[t];
-        const double hn2 = ww - proj;  // |w - V h2|^2 for orthonormal V
-        upload_h(c, h2.data(), nv, P.hdev);
-        for (int t = 0; t < nv; t++) H[t * m + j] = h[t] + h2[t];
-        if (hn2 > 1e-4 * ww) {
-          hn = sqrt(hn2);
-          if ((rc = update_scale(c, P.V, nv, P.hdev, P.w, 1.0 / hn, Vn))) return rc;
-        } else {
-          // w is nearly in span(V): form w - V h2 explicitly and take its norm
-          std::vector<double> h3(nv + 1);
-          if ((rc = update_dots(c, P.V, nv, P.hdev, P.w, h3.data()))) return rc;
-          hn = sqrt(std::max(h3[nv], 0.0));
-          if (hn > 0) {
-            c->launches++, k_scale_copy<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, 1.0 / hn, Vn);
-            if ((rc = check_launch(c, "k_scale_copy"))) return rc;
-          }
-        }
+  const int use_graph = c->capturing ? 1 : 0;
+  cudaGraphConditionalHandle h_outer = 0, h_inner = 0;
+  if (use_graph && (rc = cond_handle(c, &h_outer))) return rc;
+  c->launches++, k_kry_init<<<1, 1, 0, c->stream>>>(kd, o.rtol, o.atol, warm ? 1 : 0, o.max_iter, m,
+                                                     (unsigned long long)h_outer, use_graph);
+  if ((rc = check_launch(c, "k_kry_init"))) return rc;
+  if (use_graph) {
+    WhileLoop w0, w1;
+    if ((rc = while_begin(c, 0, h_outer, w0))) return rc;
+    if ((rc = cond_handle(c, &h_inner))) return rc;
+    const long long l0 = c->launches;
+    if ((rc = kry_cycle_start(c, b, x, (unsigned long long)h_inner, 1))) return rc;
+    if ((rc = while_begin(c, 1, h_inner, w1))) return rc;
+    const long long l1 = c->launches;
+    if ((rc = kry_body(c, o, (unsigned long long)h_inner, 1))) return rc;
+    c->sg.body_launches = c->launches - l1;
+    if ((rc = while_end(c, w1))) return rc;
+    if ((rc = kry_cycle_end(c, b, x, (unsigned long long)h_outer, 1))) return rc;
+    c->sg.cycle_launches = c->launches - l0 - c->sg.body_launches;
+    if ((rc = while_end(c, w0))) return rc;
+  } else {
+    for (;;) {
+      int go = 0;
+      if ((rc = read_flag(c, &kd->outer_go, &go))) return rc;
+      if (!go) break;
+      if ((rc = kry_cycle_start(c, b, x, 0, 0))) return rc;
+      for (;;) {
+        if ((rc = read_flag(c, &kd->inner_go, &go))) return rc;
+        if (!go) break;
+        if ((rc = kry_body(c, o, 0, 0))) return rc;
       }
-      H[(j + 1) * m + j] = hn;
-      // Givens rotations
-      for (int t = 0; t < j; t++) {
-        const double a = H[t * m + j], bb = H[(t + 1) * m + j];
-        H[t * m + j] = cs[t] * a + sn[t] * bb;
-        H[(t + 1) * m + j] = -sn[t] * a + cs[t] * bb;
-      }
-      const double a = H[j * m + j], bb = H[(j + 1) * m + j];
-      const double den = sqrt(a * a + bb * bb);
-      cs[j] = den > 0 ? a / den : 1.0;
-      sn[j] = den > 0 ? bb / den : 0.0;
-      H[j * m + j] = den;
-      H[(j + 1) * m + j] = 0;
-      gv[j + 1] = -sn[j] * gv[j];
-      gv[j] = cs[j] * gv[j];
-      it++;
-      jdone = j + 1;
-      rnorm = fabs(gv[j + 1]);
-      if (rnorm <= tol || hn == 0) break;
-    }
-    // back substitution and update x += Z y
-    for (int t = jdone - 1; t >= 0; t--) {
-      double sum = gv[t];
-      for (int u = t + 1; u < jdone; u++) sum -= H[t * m + u] * y[u];
-      y[t] = sum / H[t * m + t];
-    }
-    upload_h(c, y.data(), jdone, P.hdev);
-    c->launches++, k_lincomb_add<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z, jdone, P.hdev, x);
-    if ((rc = check_launch(c, "k_lincomb_add"))) return rc;
-    if (rnorm <= tol) {
-      // confirm with the true residual
-      if ((rc = residual(c, b, x, P.r, &rnorm))) return rc;
-      fresh = true;
-      conv = rnorm <= tol * 1.0000001 || rnorm <= 2 * tol;
+      if ((rc = kry_cycle_end(c, b, x, 0, 0))) return rc;
     }
   }
   // Remove_Nullspace: phi += -mean(phi) over fluid cells
-  double sum = 0;
-  if ((rc = sum_fluid(c, x, &sum))) return rc;
-  const double val = -sum / (double)P.nfluid;
-  c->launches++, k_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.fluid, val, x);
-  if ((rc = check_launch(c, "k_shift"))) return rc;
+  {
+    const int nb = (int)nblocks(N, 256);
+    c->launches++, k_sum_fluid<<<nb, 256, 0, c->stream>>>(N, P.fluid, x, c->red);
+    if ((rc = check_launch(c, "k_sum_fluid"))) return rc;
+    if ((rc = reduce_to(c, c->red, nb, c->ds + DS_PHISUM))) return rc;
+    c->launches++, k_shift_mean<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.fluid, c->ds, (double)P.nfluid, x);
+    if ((rc = check_launch(c, "k_shift_mean"))) return rc;
+  }
   // Convert_Phi2_Phi: periodic ghosts take their images (x is 0 elsewhere off-fluid)
   if ((rc = periodic_copy1(c, x))) return rc;
+  if (!P.transpose) P.guess = true;
+  if (c->capturing) return VFS_OK;  // statistics after the replay
   cudaEventRecord(c->ev1, c->stream);
-  cudaEventSynchronize(c->ev1);
+  cudaMemcpyAsync(c->kd_host, kd, sizeof(KryDev), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaEventSynchronize(c->ev1) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "poisson_solve: failed");
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-  if (!P.transpose) P.guess = true;
-  s.iterations = it;
-  s.converged = conv ? 1 : 0;
-  s.rfinal = rnorm;
+  vfs_solve_stats s;
+  memset(&s, 0, sizeof(s));
+  s.iterations = c->kd_host->it;
+  s.converged = c->kd_host->conv ? 1 : 0;
+  s.rfinal = c->kd_host->rnorm;
+  s.r0 = c->kd_host->r0;
   s.ms = ms;
   if (st) *st = s;
-  return conv ? VFS_OK : set_err(c, VFS_ERR_NOT_CONVERGED, "poisson_solve: iteration cap reached");
+  return s.converged ? VFS_OK : set_err(c, VFS_ERR_NOT_CONVERGED, "poisson_solve: iteration cap reached");
 }
 
 // ------------------------------------------------------------------ UpdatePressure
@@ -1152,11 +1420,11 @@ int divergence(Ctx *c, double *maxdiv) {
   const int nb = (int)nblocks(c->g.N, 256);
   if ((rc = ensure_red(c, nb + 64))) return rc;
   c->launches++, k_divergence<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->f[VFS_AJ][0], c->nv, c->red + 64);
-  c->launches++, k_max_parts<<<1, 1024, 0, c->stream>>>(c->red + 64, nb, c->red);
+  c->launches++, k_max_parts<<<1, 1024, 0, c->stream>>>(c->red + 64, nb, c->ds + DS_MAXDIV);
   if ((rc = check_launch(c, "k_divergence"))) return rc;
-  cudaMemcpyAsync(c->red_host, c->red, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "divergence sync failed");
-  *maxdiv = c->red_host[0];
+  if (c->capturing || !maxdiv) return VFS_OK;
+  if ((rc = ds_fetch(c))) return rc;
+  *maxdiv = c->ds_out[DS_MAXDIV];
   return VFS_OK;
 }
 

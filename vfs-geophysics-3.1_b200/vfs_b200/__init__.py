@@ -63,7 +63,8 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [
         ("precision", ctypes.c_int), ("restart", ctypes.c_int), ("max_iter", ctypes.c_int),
         ("levels", ctypes.c_int), ("pre_smooth", ctypes.c_int), ("post_smooth", ctypes.c_int),
-        ("coarse_iters", ctypes.c_int), ("zero_guess", ctypes.c_int), ("reserved", ctypes.c_int * 4),
+        ("coarse_iters", ctypes.c_int), ("zero_guess", ctypes.c_int), ("graph", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
         ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("reserved_d", ctypes.c_double * 4),
     ]
 
@@ -479,7 +480,8 @@ def _solve_opts(precision=0, rtol=1e-10, **kw):
     return SolveOpts(precision=precision, rtol=rtol, restart=kw.get("restart", 30),
                      max_iter=kw.get("max_iter", 200), levels=kw.get("levels", 0),
                      pre_smooth=kw.get("pre_smooth", 3), post_smooth=kw.get("post_smooth", 3),
-                     coarse_iters=kw.get("coarse_iters", 4), zero_guess=kw.get("zero_guess", 0))
+                     coarse_iters=kw.get("coarse_iters", 4), zero_guess=kw.get("zero_guess", 0),
+                     graph=kw.get("graph", 0))
 
 
 def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
