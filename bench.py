@@ -416,6 +416,46 @@ def adjoint_window(nx, ny, nz, steps, every, torch):
                     "steps) / forward sweep of the same window; the window with the median of three ratios"}
 
 
+def immersed_variant(nx, ny, nz, torch, steps=10):
+    """The metric workload with the six cylinders as immersed bodies (immersed = 1): closed
+    triangulated cylinder surfaces, classified by the IB search, with the IB-node
+    reconstruction in every step (ibm_interpolation_advanced, noslip) and the immersed
+    VolumeFlux.  Mixed-precision step time in the graph form."""
+    import vfs_b200 as vfs
+    from vfs_b200 import cases
+    case = make_case(nx, ny, nz)
+    case.immersed = 1
+    case.nvert = np.zeros(case.da_shape)
+    ctx = vfs.Context(case.config())
+    ctx.form_metrics(case.X, case.Y, case.Z)
+    ctx.set_field(vfs.NVERT, case.nvert)
+    ctx.set_scalar(vfs.S_NBODIES, len(case.centers))
+    for ibi, (cx, cz) in enumerate(case.centers):
+        ctx.ibm_search(*cases.cylinder_surface((cx, cz), 0.5 * case.D, -0.1, case.Ly + 0.1, 96, 24), ibi=ibi)
+    nv = ctx.get_field(vfs.NVERT)
+    case.nvert = nv
+    m = {"icsi": ctx.get_field(vfs.ICSI), "jeta": ctx.get_field(vfs.JETA), "kzet": ctx.get_field(vfs.KZET)}
+    u = turbulent_like(case)
+    ctx.set_field(vfs.UCONT, cases.ucont_from_ucat(case, u, m))
+    ctx.set_field(vfs.UCAT, u)
+    ctx.set_field(vfs.UCAT_O, u)
+    ctx.set_inflow_plane(u[1])
+    _, inlet_area = ctx.calc_inlet_area()
+    ctx.set_scalar(vfs.S_INLET_FLUX, 1.0 * inlet_area)
+    ctx.contra2cart()
+    for _ in range(3):
+        ctx.step(precision=0, rtol=1e-10, graph=1)
+    ms, st = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10, graph=1), steps, torch)
+    nib = int(ctx.ibm_list()[0].shape[0])
+    ctx.close()
+    return {"workload": "the metric workload with the 6 cylinders as immersed bodies (immersed=1): closed "
+                        "triangulated surfaces (96 x 24 facets each), IB search, IB-node reconstruction "
+                        "(noslip) and immersed VolumeFlux every step",
+            "ib_nodes": nib, "ms_per_step": round(ms / steps, 3),
+            "poisson_iterations": float(np.mean([s.poisson.iterations for s in st])),
+            "max_div": max(s.max_div for s in st)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,6 +465,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", default=None, help="nx,ny,nz override (not for reported numbers)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
+    ap.add_argument("--no-immersed", action="store_true", help="skip the immersed-cylinder variant")
     ap.add_argument("--adjoint-size", default="128,128,128")
     ap.add_argument("--adjoint-steps", type=int, default=20)
     ap.add_argument("--profile-step", action="store_true",
@@ -480,20 +521,27 @@ def main():
             ctx.set_field(f, v)
         ctx.set_scalar(vfs.S_TI, ti)
 
-    for _ in range(2):  # FP64 multigrid set-up, outside the timed steps
-        ctx.step(precision=1, rtol=1e-10)
+    for _ in range(2):  # FP64 multigrid set-up and both step graphs, outside the timed steps
+        ctx.step(precision=1, rtol=1e-10, graph=1)
+    restore()
+    ctx.step(precision=0, rtol=1e-10, graph=1)
     restore()
     sampler = ClockSampler(local)
     with sampler:
         barrier()
-        ms_mixed, stats = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10), args.steps, torch)
+        ms_mixed, stats = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10, graph=1), args.steps, torch)
         barrier()
         restore()
         barrier()
-        ms_fp64, stats64 = timed(ctx, lambda: ctx.step(precision=1, rtol=1e-10), args.steps, torch)
+        ms_fp64, stats64 = timed(ctx, lambda: ctx.step(precision=1, rtol=1e-10, graph=1), args.steps, torch)
+        barrier()
+        restore()
+        barrier()
+        ms_launched, _ = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10), args.steps, torch)
         barrier()
     ms_mixed /= args.steps
     ms_fp64 /= args.steps
+    ms_launched /= args.steps
     maxdiv = max(s.max_div for s in stats)
     maxdiv64 = max(s.max_div for s in stats64)
     its = float(np.mean([s.poisson.iterations for s in stats]))
@@ -527,7 +575,7 @@ def main():
         ctx.set_field(vfs.UCONT, h_uc)
         ctx.set_field(vfs.UCAT, h_u)
         ctx.set_field(vfs.P, h_p)
-        st = ctx.step(precision=0, rtol=1e-10)
+        st = ctx.step(precision=0, rtol=1e-10, graph=1)
         ctx.get_field(vfs.UCONT, out=h_uc)
         ctx.get_field(vfs.UCAT, out=h_u)
         ctx.get_field(vfs.P, out=h_p)
@@ -554,9 +602,17 @@ def main():
         ms_mixed, ms_fp64, e2e_ms = [float(v) for v in t.tolist()]
 
     n0 = ctx.launch_count()
-    ctx.step(precision=0, rtol=1e-10)
+    ctx.step(precision=0, rtol=1e-10, graph=1)
     launches_per_step = ctx.launch_count() - n0
     ctx.close()
+    del keep
+
+    imm = None
+    if not args.no_immersed and not args.size:
+        try:
+            imm = immersed_variant(nx, ny, nz, torch)
+        except Exception as e:  # reported, never fatal for the forward numbers
+            imm = {"failed": str(e)}
 
     adj = None
     if not args.no_adjoint and not args.size:
@@ -595,6 +651,9 @@ def main():
                                     "sweeps, trilinear prolongation) in FP64 FGMRES(30)" % mg_levels(nx, ny, nz),
                        "l2": "inputs larger than L2 (every field is a %d MB array)" % (npts * 8 // 2 ** 20)},
             "fp64_ms_per_step": round(ms_fp64, 3),
+            "launched_ms_per_step": round(ms_launched, 3),
+            "step_form": "one CUDA graph per step (captured once, replayed; the Poisson solve's loops as "
+                         "conditional nodes); launched_ms_per_step: the same kernels launched one by one",
             "mixed_speedup_vs_fp64": round(ms_fp64 / ms_mixed, 3),
             "max_div": {"mixed": maxdiv, "fp64": maxdiv64},
             "poisson_iterations": {"mixed": its, "fp64": its64},
@@ -613,6 +672,8 @@ def main():
         }
         if adj is not None:
             out["adjoint"] = adj
+        if imm is not None:
+            out["immersed_variant"] = imm
         if cpu is not None:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))

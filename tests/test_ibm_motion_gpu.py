@@ -21,16 +21,22 @@ from helpers import assert_close, build_pair, small_channel
 pytestmark = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
 
 
+def _by_cell(ints, dbls):
+    """The list in (k, j, i) order (the reference builds it in its own order)."""
+    order = np.lexsort((ints[:, 0], ints[:, 1], ints[:, 2]))
+    return ints[order], dbls[order]
+
+
 def _sphere(dz=0.0):
     x, y, z, tri = cases.icosphere((np.pi / 2, 1.0, np.pi), 0.45, level=3)
     return x, y, z + dz, tri
 
 
 def _surface_velocity(x, y, z):
-    """A rigid translation plus a rotation about the sphere's axis (vertex velocities)."""
+    """Vertex velocities of a rigid motion: a translation (0.1, 0, 0.05) plus a rotation
+    about the sphere's centre."""
     cx, cy, cz = np.pi / 2, 1.0, np.pi
-    w = 0.3
-    return 0.1 - w * (z - cz) * 0.0 + 0.2 * (y - cy), -0.2 * (x - cx) + 0.0 * y, 0.05 + w * (x - cx)
+    return 0.1 + 0.2 * (y - cy), -0.2 * (x - cx) + 0.3 * (z - cz), 0.05 - 0.3 * (y - cy)
 
 
 @pytest.mark.gpu
@@ -51,7 +57,7 @@ def test_wall_model_reconstruction_matches_reference():
     ref.set_global("ti", 0)
     ctx.ibm_interpolation()
     nodes = ctx.get_field(vfs.NVERT) == 1
-    assert nodes.sum() > 100
+    assert nodes.sum() > 50
     want, got = R.get("Ucat"), ctx.get_field(vfs.UCAT)
     assert_close(got[nodes], want[nodes], rtol=1e-12, atol_frac=0, what="IB-node Ucat (wall model)")
     assert_close(got[~nodes], want[~nodes], rtol=0, atol_frac=0, what="Ucat elsewhere")
@@ -87,8 +93,8 @@ def test_moving_body_steps_match_reference(wallfunction):
         ctx.ibm_set_velocity(u, v, w)
         after = ctx.get_field(vfs.NVERT)
         np.testing.assert_array_equal(after, R.get("lNvert"), err_msg="nvert after the search of step %d" % s)
-        ints_r, dbl_r = R.ibm_list()
-        ints_g, dbl_g = ctx.ibm_list()
+        ints_r, dbl_r = _by_cell(*R.ibm_list())
+        ints_g, dbl_g = _by_cell(*ctx.ibm_list())
         np.testing.assert_array_equal(ints_g, ints_r)
         if s > 0:
             uncovered += int(((before > 2.5) & (after == 1)).sum())

@@ -39,7 +39,7 @@ METRIC_FIELDS = {
 
 # scalars
 (S_MEAN_K_FLUX, S_MEAN_K_AREA, S_INLET_FLUX, S_INLET_AREA, S_DT, S_REN, S_ST, S_TI, S_FLUX_IN, S_FLUX_OUT,
- S_IB_UNRESOLVED) = range(11)
+ S_IB_UNRESOLVED, S_NBODIES) = range(12)
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOT_CONVERGED, ERR_NO_DEVICE, ERR_STATE = range(6)
 

@@ -162,6 +162,38 @@ def icosphere(center=(0.0, 0.0, 0.0), radius=0.5, level=3):
     return v[:, 0].copy(), v[:, 1].copy(), v[:, 2].copy(), np.array(faces, dtype=np.int32)
 
 
+def cylinder_surface(center, radius, y0, y1, n_theta=64, n_y=16):
+    """Closed triangulated vertical cylinder (axis along y from y0 to y1, capped, outward
+    oriented) around center = (x, z): vertex coordinates x, y, z and the (n_elmt, 3) array
+    of 0-based vertex indices, like icosphere."""
+    cx, cz = center
+    th = 2 * np.pi * np.arange(n_theta) / n_theta
+    ys = np.linspace(y0, y1, n_y + 1)
+    xs, yy, zs = [], [], []
+    for yv in ys:
+        xs.extend(cx + radius * np.cos(th))
+        yy.extend(np.full(n_theta, yv))
+        zs.extend(cz + radius * np.sin(th))
+    xs += [cx, cx]
+    yy += [y0, y1]
+    zs += [cz, cz]
+    bot, top = len(xs) - 2, len(xs) - 1
+    faces = []
+    for r in range(n_y):
+        for q in range(n_theta):
+            a, b = r * n_theta + q, r * n_theta + (q + 1) % n_theta
+            c, d = a + n_theta, b + n_theta
+            # outward normal: (b - a) x (c - a) points away from the axis for this order
+            faces.append((a, c, b))
+            faces.append((b, c, d))
+    for q in range(n_theta):
+        a, b = q, (q + 1) % n_theta
+        faces.append((bot, a, b))                      # bottom cap, normal -y
+        c, d = n_y * n_theta + q, n_y * n_theta + (q + 1) % n_theta
+        faces.append((top, d, c))                      # top cap, normal +y
+    return (np.array(xs), np.array(yy), np.array(zs), np.array(faces, dtype=np.int32))
+
+
 def write_ucd(path, x, y, z, tri):
     """The surface in the reference's ibmdata UCD form (ibm_io.c:609-905): three header
     lines, 'n_v n_elmt 0 0 0', the vertices, then 1-based triangles."""
