@@ -35,22 +35,24 @@ class ReferenceStepper:
 
     def _lhs(self):
         """PoissonLHSNew and the solver's set-up: once, or every step with moving bodies
-        (poisson_hypre.c:540-553)."""
+        (poisson_hypre.c:540-553).  Run as at ti == tistart, when setup_lidx2 numbers the
+        unknowns into fresh vectors (poisson.c:207-282)."""
         R, c = self.R, self.case
+        ref.set_global("ti", 0)
         R.call("ref_poisson_lhs")
+        ref.set_global("ti", self.ti)
         rp, col, val = R.poisson_csr()
         self.solver = poisson_mg.MGSolver(rp, col, val, R.gid(), (c.i_periodic, c.j_periodic, c.k_periodic))
 
     def _ibm_interpolation(self):
-        """ibm_interpolation_advanced with the run's ti (its wall model applies from
-        ti > 0, ibm.c:3456)."""
-        ref.set_global("ti", self.ti)
+        """ibm_interpolation_advanced (its wall model applies from ti > 0, ibm.c:3456)."""
         self.R.call("ref_ibm_interpolation", 1)
-        ref.set_global("ti", 0)
 
     def step(self):
+        """One time step with the reference's ti set to the step index (les.c:69 and the
+        wall model of ibm.c:3456 read it)."""
         R, case = self.R, self.case
-        ref.set_global("ti", 0)
+        ref.set_global("ti", self.ti)
         t0 = time.perf_counter()
         if self.ti > 0 and getattr(case, "moving", 0):
             self._lhs()
@@ -63,9 +65,7 @@ class ReferenceStepper:
         R.call("ref_calc_k_flux")                     # solvers.c:644
         if case.les:                                  # solvers.c:648-654
             R.call("ref_contra2cart")
-            ref.set_global("ti", self.ti)
             R.call("ref_les", 1)                      # dynamic_freq = 1: every step
-            ref.set_global("ti", 0)
         R.call("ref_pressure_gradient")               # solvers.c:786
         R.call("ref_runge_kutta")                     # solvers.c:1294
         t1 = time.perf_counter()
@@ -91,6 +91,7 @@ class ReferenceStepper:
         t3 = time.perf_counter()
         self.history.append({"poisson_iterations": it, "poisson_relres": rr})
         self.ti += 1
+        ref.set_global("ti", 0)
         return {"momentum": t1 - t0, "poisson": t2 - t1, "correction": t3 - t2}
 
     def fields(self):
