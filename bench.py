@@ -225,6 +225,13 @@ KERNEL_BYTES = {
     "smoother_fp32": 32.0,
     # the same sweep in FP64
     "smoother_fp64": 64.0,
+    # Pressure_Gradient: P 8 + the nine face-metric products 72 + iaj, jaj, kaj 24 + nvert 1 + dP 24
+    "pressure_gradient": 129.0,
+    # UpdatePressure + Projection: Phi 8 + products 72 + face Jacobians 24 + nvert 1 + Ucont 24 + 24
+    # + P 8 + 8
+    "projection_update": 169.0,
+    # Contra2Cart interior + Divergence maxima: Ucont 24 + centre metrics 72 + aj 8 + nvert 1 + Ucat 24
+    "contra2cart_div": 129.0,
 }
 
 
@@ -240,7 +247,8 @@ def roofline_probe(ctx, torch, reps=20):
     """Time the profiled operators on the context's stream; returns per-launch ms."""
     res = {}
     for name, ids in (("formfunction2", (8,)), ("poisson_apply_fp64", (3,)), ("smoother_fp32", (4,)),
-                      ("smoother_fp64", (5,))):
+                      ("smoother_fp64", (5,)), ("pressure_gradient", (12,)), ("projection_update", (13,)),
+                      ("contra2cart_div", (14,)), ("vcycle_fp32", (9,)), ("vcycle_fp64", (10,))):
         for w in range(3):
             for i in ids:
                 ctx.run_kernel(i, 1)
@@ -594,6 +602,22 @@ def main():
     peak, peak_kind = hbm_peak()
     dom = "formfunction2"
     achieved = KERNEL_BYTES[dom] * ncell / (launch[dom] * 1e-3) / 1e9
+    kernel_frac = {k: round(KERNEL_BYTES[k] * ncell / (launch[k] * 1e-3) / 1e9 / peak, 3)
+                   for k in KERNEL_BYTES if k in launch}
+    # Amdahl: one V-cycle per FGMRES iteration; everything else in the step is the same FP64
+    # work in both forms
+    v32, v64 = launch["vcycle_fp32"], launch["vcycle_fp64"]
+    common = ms_mixed - its * v32
+    amdahl = {"vcycle_fp32_ms": round(v32, 4), "vcycle_fp64_ms": round(v64, 4),
+              "vcycle_speedup": round(v64 / v32, 3), "vcycles_per_step": {"mixed": its, "fp64": its64},
+              "rest_of_step_ms": round(common, 3),
+              "fp64_predicted_ms": round(common + its64 * v64, 3),
+              "formfunction2_ms_per_step": round(4 * launch["formfunction2"], 3),
+              "speedup_bound_vcycle_free": round(ms_fp64 / common, 3),
+              "speedup_bound_vcycle_2x": round(ms_fp64 / (common + its64 * v64 / 2), 3),
+              "note": "rest_of_step = mixed step - iterations x FP32 V-cycle (every other kernel is the "
+                      "same FP64 work in both forms); bounds: FP64 step / mixed step if the V-cycle cost "
+                      "nothing, or ran at twice the FP64 speed"}
     launches_per_step = None
 
     if dist is not None:
@@ -658,6 +682,7 @@ def main():
             "max_div": {"mixed": maxdiv, "fp64": maxdiv64},
             "poisson_iterations": {"mixed": its, "fp64": its64},
             "mixed_vs_fp64": mixed_err,
+            "amdahl": amdahl,
             "adjoint_forward_ratio": adj.get("ratio") if adj else None,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms/step", "h2d_bytes_per_step": io_bytes,
                     "d2h_bytes_per_step": io_bytes},
@@ -666,7 +691,8 @@ def main():
                          "traffic": KERNEL_TRAFFIC.get(dom), "traffic_unit": "bytes per launch", "kernel": dom,
                          "peak_source": peak_kind, "bytes_per_cell": KERNEL_BYTES[dom],
                          "ms_per_launch": round(launch[dom], 4),
-                         "other_ms_per_launch": {k: round(v, 4) for k, v in launch.items()}},
+                         "other_ms_per_launch": {k: round(v, 4) for k, v in launch.items()},
+                         "frac_of_peak": kernel_frac},
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": sampler.summary(),
         }

@@ -368,8 +368,10 @@ int vfs_get_stream(vfs_ctx *ctx, void **stream);
  * 4 FP32 fine-level zebra line sweep (both colours), 5 the same in FP64, 6 Projection,
  * 7 Formfunction_2 as three kernels (0-2), 8 Formfunction_2 as a step runs it, 9 one
  * multigrid V-cycle of the preconditioner (FP32) applied to VFS_B, 10 the same in FP64,
- * 11 Formfunction_2 as one k-marching kernel.  Kernels 7, 8 and 11 add into RHS as
- * vfs_formfunction2 does.  For timing only. */
+ * 11 Formfunction_2 as one k-marching kernel, 12 Pressure_Gradient, 13 UpdatePressure and
+ * Projection as one kernel, 14 the Contra2Cart interior kernel that also forms the block
+ * maxima of Divergence.  Kernels 7, 8 and 11 add into RHS as vfs_formfunction2 does.  For
+ * timing only. */
 int vfs_run_kernel(vfs_ctx *ctx, int which, int reps);
 
 /* ------------------------------------------------------------------ adjoint

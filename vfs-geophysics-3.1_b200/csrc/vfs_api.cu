@@ -311,6 +311,7 @@ int vfs_destroy(vfs_ctx *ctx) {
     for (int q = 0; q < 3; q++) if (c->f[f][q]) cudaFree(c->f[f][q]);
   if (c->nv) cudaFree(c->nv);
   if (c->nvo) cudaFree(c->nvo);
+  if (c->gab) cudaFree(c->gab);
   if (c->ibv) cudaFree(c->ibv);
   if (c->bcflag) cudaFree(c->bcflag);
   if (c->solid) cudaFree(c->solid);
@@ -393,7 +394,7 @@ int vfs_set_field(vfs_ctx *ctx, int field, const double *host) {
   c->launches++, k_unpack<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(stage, dof, c->g.N, c->f[field][0],
                                                        c->f[field][1], c->f[field][2]);
   rc = check_launch(c, "k_unpack");
-  if (field >= VFS_CSI && field <= VFS_KAJ) { c->metrics_set = true; c->ps.built = false; }
+  if (field >= VFS_CSI && field <= VFS_KAJ) { c->metrics_set = true; c->ps.built = false; c->gab_valid = false; }
   if (field == VFS_PHI) c->ps.guess = c->ps.built;  // the next solve starts from the values set
   if (cudaStreamSynchronize(c->stream) != cudaSuccess)
     return set_err(c, VFS_ERR_CUDA, "vfs_set_field: copy failed");
@@ -574,10 +575,12 @@ static int step_body(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *s, int 
   rc = poisson_solve(c, opts, &s->poisson);
   if (rc && rc != VFS_ERR_NOT_CONVERGED) return rc;
   *solve_rc = rc;
-  if ((rc = update_pressure(c))) return rc;
-  if ((rc = projection(c))) return rc;
+  // UpdatePressure + Projection (solvers.c:1341-1342), with Divergence (solvers.c:1378)
+  // formed in Projection's Contra2Cart when no IB-node reconstruction comes between
+  const bool fuse_div = !c->g.immersed;
+  if ((rc = correction(c, fuse_div))) return rc;
   if (c->g.immersed && (rc = ibm_interpolation(c))) return rc;  // solvers.c:1366-1370
-  if ((rc = divergence(c, &s->max_div))) return rc;
+  if ((rc = fuse_div ? divergence_finish(c, &s->max_div) : divergence(c, &s->max_div))) return rc;
   if ((rc = ib_bc(c))) return rc;
   if ((rc = contra2cart(c))) return rc;
   // end of the time step: keep Ucont and Ucat of this step (main.c:3584-3602), and with
@@ -649,6 +652,7 @@ static bool graph_eligible(const Ctx *c) {
 int step_graph(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
   if (!graph_eligible(c)) return step_core(c, opts, st);
   int rc;
+  if ((rc = ensure_gab(c))) return rc;   // set-up work stays outside the graph
   const bool fresh = c->sg.exec && c->sg.key == c->setup_epoch && !memcmp(&c->sg.opts, opts, sizeof(*opts));
   if (!fresh) {
     step_graph_free(c);

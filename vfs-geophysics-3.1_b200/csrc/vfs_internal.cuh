@@ -240,6 +240,8 @@ struct Ctx {
   StepGraph sg;
   long long setup_epoch = 0;     // bumped whenever a captured step would be stale
   cudaStream_t cap_streams[2] = {nullptr, nullptr};  // bodies of the solver's two loops
+  double *gab = nullptr;         // 9 x N face-metric products of Pressure_Gradient / Projection
+  bool gab_valid = false;        // false after any metric upload
 };
 
 V3 field3(Ctx *c, int f);
@@ -259,6 +261,7 @@ inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / 
 // momentum path
 int periodic_copy3(Ctx *c, V3 v);
 int periodic_copy1(Ctx *c, double *s);
+int ensure_gab(Ctx *c);
 int contra2cart(Ctx *c);
 int solid_list(Ctx *c);
 int formfunction2(Ctx *c, double scale, bool rk_stage, double rk_coeff);
@@ -310,6 +313,9 @@ int poisson_apply_dev(Ctx *c, const double *x, double *y);
 int update_pressure(Ctx *c);
 int projection(Ctx *c);
 int divergence(Ctx *c, double *maxdiv);
+int correction(Ctx *c, bool fuse_divergence);
+int divergence_finish(Ctx *c, double *maxdiv);
+int contra2cart_div(Ctx *c, bool with_divergence);
 
 // multigrid preconditioner (vfs_mg.cu)
 int mg_setup(Ctx *c);

@@ -190,6 +190,7 @@ int form_metrics(Ctx *c, const double *x, const double *y, const double *z) {
   cudaFreeAsync(d, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, VFS_ERR_CUDA, "form_metrics failed");
   c->metrics_set = true;
+  c->gab_valid = false;
   c->ps.built = false;
   return VFS_OK;
 }

@@ -93,6 +93,55 @@ __global__ void k_contra2cart_interior(Grid g, CV3 uc, CV3 csi, CV3 eta, CV3 zet
   ucat.z[p] = det2 / det;
 }
 
+// k_contra2cart_interior plus the block maxima of Divergence (main.c:1083-1090) on the
+// same Ucont: |(dU + dV + dW) aj| at interior cells with no solid in the 7-point
+// neighbourhood, 0 elsewhere; one partial per block of 256 threads in parts[blockIdx.x]
+// (the layout k_divergence writes).
+__global__ void __launch_bounds__(256) k_contra2cart_div(Grid g, CV3 uc, CV3 csi, CV3 eta, CV3 zet,
+                                                         const double *__restrict__ aj,
+                                                         const uint8_t *__restrict__ nv, V3 ucat, double *parts) {
+  __shared__ double sh[8];
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long sy = g.mx, sz = (long long)g.mx * g.my;
+  double dmax = 0;
+  if (p < g.N) {
+    int i, j, k;
+    dijk(g, p, i, j, k);
+    if (i >= 1 && i <= g.mx - 2 && j >= 1 && j <= g.my - 2 && k >= 1 && k <= g.mz - 2) {
+      const double ux0 = uc.x[p - 1], ux1 = uc.x[p], uy0 = uc.y[p - sy], uy1 = uc.y[p];
+      const double uz0 = uc.z[p - sz], uz1 = uc.z[p];
+      if (nv[p] + nv[p + sz] + nv[p - sz] + nv[p + sy] + nv[p - sy] + nv[p + 1] + nv[p - 1] == 0)
+        dmax = fabs((ux1 - ux0 + uy1 - uy0 + uz1 - uz0) * aj[p]);
+      if (nv[p] == 0) {
+        const double m00 = csi.x[p], m01 = csi.y[p], m02 = csi.z[p];
+        const double m10 = eta.x[p], m11 = eta.y[p], m12 = eta.z[p];
+        const double m20 = zet.x[p], m21 = zet.y[p], m22 = zet.z[p];
+        const double q0 = 0.5 * (ux0 + ux1), q1 = 0.5 * (uy0 + uy1), q2 = 0.5 * (uz0 + uz1);
+        const double det = m00 * (m11 * m22 - m12 * m21) - m01 * (m10 * m22 - m12 * m20) +
+                           m02 * (m10 * m21 - m11 * m20);
+        const double det0 = q0 * (m11 * m22 - m12 * m21) - q1 * (m01 * m22 - m02 * m21) +
+                            q2 * (m01 * m12 - m02 * m11);
+        const double det1 = -q0 * (m10 * m22 - m12 * m20) + q1 * (m00 * m22 - m02 * m20) -
+                            q2 * (m00 * m12 - m02 * m10);
+        const double det2 = q0 * (m10 * m21 - m11 * m20) - q1 * (m00 * m21 - m01 * m20) +
+                            q2 * (m00 * m11 - m01 * m10);
+        ucat.x[p] = det0 / det;
+        ucat.y[p] = det1 / det;
+        ucat.z[p] = det2 / det;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_down_sync(0xffffffffu, dmax, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = dmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mx = 0;
+    for (int w = 0; w < 8; w++) mx = fmax(mx, sh[w]);
+    parts[blockIdx.x] = mx;
+  }
+}
+
 // Covariant metric inverse (Calculate_Covariant_metrics, rhs2.c:538).
 __device__ void covariant(const double g[3][3], double G[3][3]) {
   const double a11 = g[0][0], a12 = g[0][1], a13 = g[0][2];
@@ -340,13 +389,33 @@ int solid_list(Ctx *c) {
   return VFS_OK;
 }
 
-int contra2cart(Ctx *c) {
+int contra2cart(Ctx *c) { return contra2cart_div(c, false); }
+
+// The interior kernel of contra2cart_div with the divergence maxima alone (diagnostics).
+int contra2cart_interior_div(Ctx *c) {
+  const Grid &g = c->g;
+  int rc;
+  if ((rc = ensure_red(c, (int)nblocks(g.N, 256) + 64))) return rc;
+  Metrics m = metrics(c);
+  c->launches++, k_contra2cart_div<<<nblocks(g.N, 256), 256, 0, c->stream>>>(
+      g, cv(field3(c, VFS_UCONT)), m.csi, m.eta, m.zet, m.aj, c->nv, field3(c, VFS_UCAT), c->red + 64);
+  return check_launch(c, "k_contra2cart_div");
+}
+
+// Contra2Cart; with_divergence: the interior kernel also writes the block maxima of
+// Divergence to c->red + 64 (sized by the caller).
+int contra2cart_div(Ctx *c, bool with_divergence) {
   const Grid &g = c->g;
   V3 uc = field3(c, VFS_UCONT), ucat = field3(c, VFS_UCAT);
   int rc;
   if ((rc = periodic_copy3(c, uc))) return rc;
   Metrics m = metrics(c);
-  c->launches++, k_contra2cart_interior<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(uc), m.csi, m.eta, m.zet, c->nv, ucat);
+  if (with_divergence)
+    c->launches++, k_contra2cart_div<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(uc), m.csi, m.eta, m.zet, m.aj,
+                                                                               c->nv, ucat, c->red + 64);
+  else
+    c->launches++, k_contra2cart_interior<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(uc), m.csi, m.eta, m.zet, c->nv,
+                                                                                    ucat);
   if ((rc = check_launch(c, "k_contra2cart_interior"))) return rc;
   if ((rc = periodic_copy3(c, ucat))) return rc;
   V3 out{c->bcbuf[0], c->bcbuf[1], c->bcbuf[2]};
@@ -1286,6 +1355,41 @@ void launch_rhs(Ctx *c) {
                                                     field3(c, VFS_UCONT));
 }
 
+// ------------------------------------------------------------------ face-metric products
+// The nine products of face metrics that Pressure_Gradient (momentum.c:311-319) and
+// Projection (poisson.c:2837-2960) form at every face: on the i-face icsi.icsi, ieta.icsi,
+// izet.icsi; on the j-face jcsi.jeta, jeta.jeta, jzet.jeta; on the k-face kcsi.kzet,
+// keta.kzet, kzet.kzet, each summed x + y + z in that order.  Stored once per metric upload
+// (9 x N doubles, slot q of point p at G[q*N + p]); both kernels read 12 doubles per point
+// (these and iaj, jaj, kaj) instead of the 30 face metrics, with the same bits as forming
+// them in place.
+__global__ void k_gab(Grid g, Metrics m, double *G) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const long long N = g.N;
+  G[p] = dot3(m.icsi.x[p], m.icsi.y[p], m.icsi.z[p], m.icsi.x[p], m.icsi.y[p], m.icsi.z[p]);
+  G[N + p] = dot3(m.ieta.x[p], m.ieta.y[p], m.ieta.z[p], m.icsi.x[p], m.icsi.y[p], m.icsi.z[p]);
+  G[2 * N + p] = dot3(m.izet.x[p], m.izet.y[p], m.izet.z[p], m.icsi.x[p], m.icsi.y[p], m.icsi.z[p]);
+  G[3 * N + p] = dot3(m.jcsi.x[p], m.jcsi.y[p], m.jcsi.z[p], m.jeta.x[p], m.jeta.y[p], m.jeta.z[p]);
+  G[4 * N + p] = dot3(m.jeta.x[p], m.jeta.y[p], m.jeta.z[p], m.jeta.x[p], m.jeta.y[p], m.jeta.z[p]);
+  G[5 * N + p] = dot3(m.jzet.x[p], m.jzet.y[p], m.jzet.z[p], m.jeta.x[p], m.jeta.y[p], m.jeta.z[p]);
+  G[6 * N + p] = dot3(m.kcsi.x[p], m.kcsi.y[p], m.kcsi.z[p], m.kzet.x[p], m.kzet.y[p], m.kzet.z[p]);
+  G[7 * N + p] = dot3(m.keta.x[p], m.keta.y[p], m.keta.z[p], m.kzet.x[p], m.kzet.y[p], m.kzet.z[p]);
+  G[8 * N + p] = dot3(m.kzet.x[p], m.kzet.y[p], m.kzet.z[p], m.kzet.x[p], m.kzet.y[p], m.kzet.z[p]);
+}
+
+int ensure_gab(Ctx *c) {
+  if (c->gab_valid) return VFS_OK;
+  if (c->capturing) return set_err(c, VFS_ERR_STATE, "face-metric products not formed before capture");
+  if (!c->gab && cudaMalloc(&c->gab, sizeof(double) * 9 * (size_t)c->g.N) != cudaSuccess)
+    return set_err(c, VFS_ERR_CUDA, "face-metric product allocation failed");
+  c->launches++, k_gab<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->gab);
+  int rc = check_launch(c, "k_gab");
+  if (rc == VFS_OK) c->gab_valid = true;
+  c->setup_epoch++;
+  return rc;
+}
+
 // ------------------------------------------------------------------ Pressure_Gradient
 // momentum.c:197-443 (levelset off): dP on the three faces of each interior cell, with
 // one-sided cross differences next to IB nodes (nvert == 1) and non-periodic walls, and
@@ -1295,7 +1399,9 @@ void launch_rhs(Ctx *c) {
 #ifndef VFS_PG_MINB
 #define VFS_PG_MINB 5
 #endif
-__global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, Metrics m, const uint8_t *__restrict__ nv,
+__global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, const double *__restrict__ G,
+                                    const double *__restrict__ iaj, const double *__restrict__ jaj,
+                                    const double *__restrict__ kaj, const uint8_t *__restrict__ nv,
                                     const double *__restrict__ P, double kdiff, double kdt,
                                     double karea, int kforce_mode, double mpg, const double *__restrict__ ds,
                                     V3 dp) {
@@ -1308,16 +1414,10 @@ __global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, 
     dp.x[p] = 0; dp.y[p] = 0; dp.z[p] = 0;  // VecSet(dP, 0) outside the loop
     return;
   }
-  const long long sy = mx, sz = (long long)mx * my;
-  const double g11_i = dot3(m.icsi.x[p], m.icsi.y[p], m.icsi.z[p], m.icsi.x[p], m.icsi.y[p], m.icsi.z[p]);
-  const double g12_i = dot3(m.ieta.x[p], m.ieta.y[p], m.ieta.z[p], m.icsi.x[p], m.icsi.y[p], m.icsi.z[p]);
-  const double g13_i = dot3(m.izet.x[p], m.izet.y[p], m.izet.z[p], m.icsi.x[p], m.icsi.y[p], m.icsi.z[p]);
-  const double g21_j = dot3(m.jcsi.x[p], m.jcsi.y[p], m.jcsi.z[p], m.jeta.x[p], m.jeta.y[p], m.jeta.z[p]);
-  const double g22_j = dot3(m.jeta.x[p], m.jeta.y[p], m.jeta.z[p], m.jeta.x[p], m.jeta.y[p], m.jeta.z[p]);
-  const double g23_j = dot3(m.jzet.x[p], m.jzet.y[p], m.jzet.z[p], m.jeta.x[p], m.jeta.y[p], m.jeta.z[p]);
-  const double g31_k = dot3(m.kcsi.x[p], m.kcsi.y[p], m.kcsi.z[p], m.kzet.x[p], m.kzet.y[p], m.kzet.z[p]);
-  const double g32_k = dot3(m.keta.x[p], m.keta.y[p], m.keta.z[p], m.kzet.x[p], m.kzet.y[p], m.kzet.z[p]);
-  const double g33_k = dot3(m.kzet.x[p], m.kzet.y[p], m.kzet.z[p], m.kzet.x[p], m.kzet.y[p], m.kzet.z[p]);
+  const long long sy = mx, sz = (long long)mx * my, N = g.N;
+  const double g11_i = __ldcs(G + p), g12_i = __ldcs(G + N + p), g13_i = __ldcs(G + 2 * N + p);
+  const double g21_j = __ldcs(G + 3 * N + p), g22_j = __ldcs(G + 4 * N + p), g23_j = __ldcs(G + 5 * N + p);
+  const double g31_k = __ldcs(G + 6 * N + p), g32_k = __ldcs(G + 7 * N + p), g33_k = __ldcs(G + 8 * N + p);
   const double r1 = 1.0, r2 = 1.0, r3 = 1.0;
   auto ib = [&](long long o) { return nv[o] == 1; };  // (int)(nvert+0.5)==1
   double dpdc, dpde, dpdz;
@@ -1334,7 +1434,7 @@ __global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, 
   else if (ib(p - sz) || ib(p - sz + 1) || (k == 1 && !g.kper))
     dpdz = (P[p + sz] - P[p] + P[p + sz + 1] - P[p + 1]) * 0.5;
   else dpdz = (P[p + sz] - P[p - sz] + P[p + sz + 1] - P[p - sz + 1]) * 0.25;
-  double ox = (dpdc * g11_i + dpde * g12_i + dpdz * g13_i) * m.iaj[p] / r1;
+  double ox = (dpdc * g11_i + dpde * g12_i + dpdz * g13_i) * iaj[p] / r1;
   // y face
   if (ib(p + 1) || ib(p + sy + 1) || (i == mx - 2 && !g.iper))
     dpdc = (P[p] - P[p - 1] + P[p + sy] - P[p + sy - 1]) * 0.5;
@@ -1348,7 +1448,7 @@ __global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, 
   else if (ib(p - sz) || ib(p - sz + sy) || (k == 1 && !g.kper))
     dpdz = (P[p + sz] - P[p] + P[p + sz + sy] - P[p + sy]) * 0.5;
   else dpdz = (P[p + sz] - P[p - sz] + P[p + sz + sy] - P[p - sz + sy]) * 0.25;
-  double oy = (dpdc * g21_j + dpde * g22_j + dpdz * g23_j) * m.jaj[p] / r2;
+  double oy = (dpdc * g21_j + dpde * g22_j + dpdz * g23_j) * jaj[p] / r2;
   // z face
   if (ib(p + 1) || ib(p + sz + 1) || (i == mx - 2 && !g.iper))
     dpdc = (P[p] - P[p - 1] + P[p + sz] - P[p + sz - 1]) * 0.5;
@@ -1363,8 +1463,7 @@ __global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, 
   if ((k == 0 || k == mz - 2) && g.kper) dpdz = P[p - (long long)k * sz + sz] - P[p];
   else dpdz = (P[p + sz] - P[p]);
   if (g.kper) {
-    const double kz2 = m.kzet.x[p] * m.kzet.x[p] + m.kzet.y[p] * m.kzet.y[p] + m.kzet.z[p] * m.kzet.z[p];
-    const double dz = 1. / m.kaj[p] / sqrt(kz2);
+    const double dz = 1. / kaj[p] / sqrt(g33_k);   // |kzet|^2 is g33
     if (kforce_mode == 1) dpdz += mpg * dz;
     else if (kforce_mode == 2) {
       // ds: the step's device scalars (mean_k_flux - inlet_flux, mean_k_area)
@@ -1372,7 +1471,7 @@ __global__ void __launch_bounds__(256, VFS_PG_MINB) k_pressure_gradient(Grid g, 
       dpdz += dz * kdiff / kdt / karea;
     }
   }
-  double oz = (dpdc * g31_k + dpde * g32_k + dpdz * g33_k) * m.kaj[p] / r3;
+  double oz = (dpdc * g31_k + dpde * g32_k + dpdz * g33_k) * kaj[p] / r3;
   if (i == 0 || nv[p] + nv[p + 1] > 0 || (!g.iper && i == mx - 2)) ox = 0;
   if (j == 0 || nv[p] + nv[p + sy] > 0 || (!g.jper && j == my - 2)) oy = 0;
   if (k == 0 || nv[p] + nv[p + sz] > 0 || (!g.kper && k == mz - 2)) oz = 0;
@@ -1392,11 +1491,12 @@ int pressure_forcing_mode(const Ctx *c) {
 // with the flux deficit of the step's device scalars (ds = c->ds).
 static int pressure_gradient_launch(Ctx *c, int mode, double kdiff, const double *ds) {
   int rc;
+  if ((rc = ensure_gab(c))) return rc;
   // P's periodic ghosts are refreshed first (momentum.c:241-273)
   if ((rc = periodic_copy1(c, c->f[VFS_P][0]))) return rc;
   c->launches++, k_pressure_gradient<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(
-      c->g, metrics(c), c->nv, c->f[VFS_P][0], kdiff, c->g.dt, c->scal[VFS_S_MEAN_K_AREA], mode,
-      c->cfg.mean_pressure_gradient, ds, field3(c, VFS_DP));
+      c->g, c->gab, c->f[VFS_IAJ][0], c->f[VFS_JAJ][0], c->f[VFS_KAJ][0], c->nv, c->f[VFS_P][0], kdiff, c->g.dt,
+      c->scal[VFS_S_MEAN_K_AREA], mode, c->cfg.mean_pressure_gradient, ds, field3(c, VFS_DP));
   return check_launch(c, "k_pressure_gradient");
 }
 

@@ -1279,26 +1279,35 @@ __device__ __forceinline__ double cross_phi(const double *phi, long long a0, lon
   return (phi[a0 + dp] + phi[a1 + dp] - phi[a0 - dp] - phi[a1 - dp]) * 0.25;
 }
 
-__global__ void k_projection(Grid g, Metrics m, const uint8_t *__restrict__ nv, const double *__restrict__ phi, V3 uc) {
+// Projection at interior point p with the face-metric products G (9 x N, k_gab) and
+// the face Jacobians; with kUpdate the same thread first applies UpdatePressure to P
+// (the two touch disjoint data: UpdatePressure reads Phi and writes P, Projection reads
+// Phi and writes Ucont), so one pass serves both.
+template <bool kUpdate>
+__global__ void __launch_bounds__(256) k_projection(Grid g, const double *__restrict__ G,
+                                                    const double *__restrict__ iaj, const double *__restrict__ jaj,
+                                                    const double *__restrict__ kaj, const uint8_t *__restrict__ nv,
+                                                    const double *__restrict__ phi, V3 uc, double *P) {
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const int mx = g.mx, my = g.my, mz = g.mz;
   int i, j, k;
   dijk(g, p, i, j, k);
   if (i < 1 || i > mx - 2 || j < 1 || j > my - 2 || k < 1 || k > mz - 2) return;
-  const long long sx = 1, sy = mx, sz = (long long)mx * my;
+  if (kUpdate) {  // poisson.c:3144-3305
+    if (nv[p] == 0) P[p] += phi[p];
+    if (nv[p] >= 2) P[p] = 0;
+  }
+  const long long sx = 1, sy = mx, sz = (long long)mx * my, N = g.N;
   const double coeff = 1.0, r1 = 1.0, r2 = 1.0, r3 = 1.0;
-  const double fac = g.dt * g.st;
   if (i < mx - 2 || (g.iper && i == mx - 2)) {
     double dpdc = phi[p + 1] - phi[p];
     if (i == mx - 2 && g.iper) dpdc = phi[p - i + 1] - phi[p];
     const double dpde = cross_phi(phi, p, p + sx, sy, j, my, g.jper, nv[p + sy] + nv[p + sy + sx], nv[p - sy] + nv[p - sy + sx]);
     const double dpdz = cross_phi(phi, p, p + sx, sz, k, mz, g.kper, nv[p + sz] + nv[p + sz + sx], nv[p - sz] + nv[p - sz + sx]);
     if (nv[p] + nv[p + 1] == 0) {
-      const double ix = m.icsi.x[p], iy = m.icsi.y[p], iz = m.icsi.z[p], a = m.iaj[p];
-      uc.x[p] -= (dpdc * (ix * ix + iy * iy + iz * iz) * a +
-                  dpde * (m.ieta.x[p] * ix + m.ieta.y[p] * iy + m.ieta.z[p] * iz) * a +
-                  dpdz * (m.izet.x[p] * ix + m.izet.y[p] * iy + m.izet.z[p] * iz) * a) *
+      const double a = iaj[p];
+      uc.x[p] -= (dpdc * __ldcs(G + p) * a + dpde * __ldcs(G + N + p) * a + dpdz * __ldcs(G + 2 * N + p) * a) *
                  g.dt * g.st / coeff / r1;
     }
   }
@@ -1309,10 +1318,9 @@ __global__ void k_projection(Grid g, Metrics m, const uint8_t *__restrict__ nv, 
     else dpde = phi[p + sy] - phi[p];
     const double dpdz = cross_phi(phi, p, p + sy, sz, k, mz, g.kper, nv[p + sz] + nv[p + sz + sy], nv[p - sz] + nv[p - sz + sy]);
     if (nv[p] + nv[p + sy] == 0 || nv[p] + nv[p + sy] == 5) {
-      const double jx = m.jeta.x[p], jy = m.jeta.y[p], jz = m.jeta.z[p], a = m.jaj[p];
-      uc.y[p] -= (dpdc * (m.jcsi.x[p] * jx + m.jcsi.y[p] * jy + m.jcsi.z[p] * jz) * a +
-                  dpde * (jx * jx + jy * jy + jz * jz) * a +
-                  dpdz * (m.jzet.x[p] * jx + m.jzet.y[p] * jy + m.jzet.z[p] * jz) * a) *
+      const double a = jaj[p];
+      uc.y[p] -= (dpdc * __ldcs(G + 3 * N + p) * a + dpde * __ldcs(G + 4 * N + p) * a +
+                  dpdz * __ldcs(G + 5 * N + p) * a) *
                  g.dt * g.st / coeff / r2;
     }
   }
@@ -1323,14 +1331,24 @@ __global__ void k_projection(Grid g, Metrics m, const uint8_t *__restrict__ nv, 
     if (k == mz - 2 && g.kper) dpdz = phi[p - (long long)k * sz + sz] - phi[p];
     else dpdz = phi[p + sz] - phi[p];
     if (nv[p] + nv[p + sz] == 0) {
-      const double kx = m.kzet.x[p], ky = m.kzet.y[p], kz = m.kzet.z[p], a = m.kaj[p];
-      uc.z[p] -= (dpdc * (m.kcsi.x[p] * kx + m.kcsi.y[p] * ky + m.kcsi.z[p] * kz) * a +
-                  dpde * (m.keta.x[p] * kx + m.keta.y[p] * ky + m.keta.z[p] * kz) * a +
-                  dpdz * (kx * kx + ky * ky + kz * kz) * a) *
+      const double a = kaj[p];
+      uc.z[p] -= (dpdc * __ldcs(G + 6 * N + p) * a + dpde * __ldcs(G + 7 * N + p) * a +
+                  dpdz * __ldcs(G + 8 * N + p) * a) *
                  g.dt * g.st / coeff / r3;
     }
   }
-  (void)fac;
+}
+
+static void launch_projection(Ctx *c, bool update_p) {
+  const Grid &g = c->g;
+  if (update_p)
+    c->launches++, k_projection<true><<<nblocks(g.N, 256), 256, 0, c->stream>>>(
+        g, c->gab, c->f[VFS_IAJ][0], c->f[VFS_JAJ][0], c->f[VFS_KAJ][0], c->nv, c->f[VFS_PHI][0],
+        field3(c, VFS_UCONT), c->f[VFS_P][0]);
+  else
+    c->launches++, k_projection<false><<<nblocks(g.N, 256), 256, 0, c->stream>>>(
+        g, c->gab, c->f[VFS_IAJ][0], c->f[VFS_JAJ][0], c->f[VFS_KAJ][0], c->nv, c->f[VFS_PHI][0],
+        field3(c, VFS_UCONT), nullptr);
 }
 
 // Component-wise periodic copy after Projection (poisson.c:3013-3046): a component is
@@ -1350,14 +1368,35 @@ __global__ void k_periodic_copy_comp(Grid g, V3 u) {
 
 int projection(Ctx *c) {
   int rc;
-  c->launches++, k_projection<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, metrics(c), c->nv, c->f[VFS_PHI][0],
-                                                           field3(c, VFS_UCONT));
+  if ((rc = ensure_gab(c))) return rc;
+  launch_projection(c, false);
   if ((rc = check_launch(c, "k_projection"))) return rc;
   if (c->g.iper || c->g.jper || c->g.kper) {
     c->launches++, k_periodic_copy_comp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
     if ((rc = check_launch(c, "k_periodic_copy_comp"))) return rc;
   }
   return contra2cart(c);
+}
+
+// UpdatePressure, Projection and its Contra2Cart as the step runs them (solvers.c:1341-1342):
+// UpdatePressure's P += Phi fused into the projection kernel, the periodic ghosts of P and
+// of the projected Ucont, then Contra2Cart; with fuse_divergence the Contra2Cart interior
+// kernel also forms the block maxima of Divergence (main.c:1083-1090) on the same Ucont
+// (valid when nothing changes Ucont between Contra2Cart and Divergence: no IB nodes), and
+// divergence_finish reduces them.  Phi's periodic ghosts, which UpdatePressure also
+// refreshes, already hold their images from the end of the Poisson solve.
+int correction(Ctx *c, bool fuse_divergence) {
+  int rc;
+  if ((rc = ensure_gab(c))) return rc;
+  launch_projection(c, true);
+  if ((rc = check_launch(c, "k_projection"))) return rc;
+  if ((rc = periodic_copy1(c, c->f[VFS_P][0]))) return rc;
+  if (c->g.iper || c->g.jper || c->g.kper) {
+    c->launches++, k_periodic_copy_comp<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCONT));
+    if ((rc = check_launch(c, "k_periodic_copy_comp"))) return rc;
+  }
+  if (fuse_divergence && (rc = ensure_red(c, (int)nblocks(c->g.N, 256) + 64))) return rc;
+  return contra2cart_div(c, fuse_divergence);
 }
 
 // ------------------------------------------------------------------ Divergence
@@ -1420,8 +1459,17 @@ int divergence(Ctx *c, double *maxdiv) {
   const int nb = (int)nblocks(c->g.N, 256);
   if ((rc = ensure_red(c, nb + 64))) return rc;
   c->launches++, k_divergence<<<nb, 256, 0, c->stream>>>(c->g, cv(field3(c, VFS_UCONT)), c->f[VFS_AJ][0], c->nv, c->red + 64);
-  c->launches++, k_max_parts<<<1, 1024, 0, c->stream>>>(c->red + 64, nb, c->ds + DS_MAXDIV);
   if ((rc = check_launch(c, "k_divergence"))) return rc;
+  return divergence_finish(c, maxdiv);
+}
+
+// Maximum of the block maxima of Divergence (in c->red + 64, one per block of 256 points)
+// into the device scalar; read back into *maxdiv unless capturing.
+int divergence_finish(Ctx *c, double *maxdiv) {
+  int rc;
+  const int nb = (int)nblocks(c->g.N, 256);
+  c->launches++, k_max_parts<<<1, 1024, 0, c->stream>>>(c->red + 64, nb, c->ds + DS_MAXDIV);
+  if ((rc = check_launch(c, "k_max_parts"))) return rc;
   if (c->capturing || !maxdiv) return VFS_OK;
   if ((rc = ds_fetch(c))) return rc;
   *maxdiv = c->ds_out[DS_MAXDIV];
@@ -1454,6 +1502,17 @@ int run_kernel(Ctx *c, int which, int reps) {
       case 7: rc = formfunction2_split(c, 1.0, false, 0.0); if (rc) return rc; break;
       case 8: rc = formfunction2(c, 1.0, false, 0.0); if (rc) return rc; break;
       case 11: rc = formfunction2_onepass(c, 1.0, false, 0.0); if (rc) return rc; break;
+      case 12: rc = pressure_gradient(c); if (rc) return rc; break;
+      case 13:
+        if ((rc = ensure_gab(c))) return rc;
+        launch_projection(c, true);
+        if ((rc = check_launch(c, "k_projection"))) return rc;
+        break;
+      case 14: {
+        extern int contra2cart_interior_div(Ctx *);
+        if ((rc = contra2cart_interior_div(c))) return rc;
+        break;
+      }
       case 9:
       case 10: {  // one multigrid V-cycle (the preconditioner) on B, FP32 or FP64, into a work vector
         vfs_solve_opts o;
@@ -1465,7 +1524,8 @@ int run_kernel(Ctx *c, int which, int reps) {
         break;
       }
       case 6:
-        c->launches++, k_projection<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, c->f[VFS_PHI][0], field3(c, VFS_UCONT));
+        if ((rc = ensure_gab(c))) return rc;
+        launch_projection(c, false);
         break;
       default: return set_err(c, VFS_ERR_INVALID, "run_kernel: unknown kernel id");
     }
