@@ -374,7 +374,7 @@ def reference_arm(args, rank, world):
 ADJ_WORKLOAD = ("wavy-wall channel %dx%dx%d cells (bottom y_w = 0.1 sin(2 pi x/Lx) cos(2 pi z/Lz)), "
                 "immersed sphere D=0.4 at the centre (icosphere, 20480 triangles, IB nodes), inlet k=0 "
                 "(inletprofile 100) and outlet k+, FP64 Poisson rtol 1e-10; objective: streamwise "
-                "pressure force on the body after %d steps; control: the inflow plane; checkpoint "
+                "drag on the body (pressure force plus viscous traction on its cell faces) after %d steps; control: the inflow plane; checkpoint "
                 "every %d steps")
 
 
@@ -405,23 +405,104 @@ def adjoint_window(nx, ny, nz, steps, every, torch):
     t0 = time.perf_counter()
     ctx.adjoint_setup()
     setup_s = time.perf_counter() - t0
-    kw = dict(objective=vfs.OBJ_PRESSURE_DRAG, control=vfs.CTRL_INFLOW_PLANE, precision=1, rtol=1e-10)
-    ctx.adjoint_gradient(steps, checkpoint_every=every, **kw)  # warm-up: tapes, checkpoints, Krylov space
+    kw = dict(objective=vfs.OBJ_DRAG, control=vfs.CTRL_INFLOW_PLANE, precision=1, rtol=1e-10)
+    for _ in range(2):  # warm-up: tapes, checkpoints, Krylov space, clocks
+        ctx.adjoint_gradient(steps, checkpoint_every=every, **kw)
     torch.cuda.synchronize()
-    # both sweeps wait on the host once per Krylov scalar (about a thousand round trips per
-    # window), so a busy host stretches their event times: three windows, the median ratio
+    # the launched steps of both sweeps read the solver's loop flags back once per Krylov
+    # iteration, so a busy host stretches their event times: three windows, the median ratio
     runs = [ctx.adjoint_gradient(steps, checkpoint_every=every, **kw) for _ in range(3)]
-    ctx.close()
     ratios = [r[1].ms_adjoint / r[1].ms_forward for r in runs]
     g, st = runs[int(np.argsort(ratios)[1])]
+    # central difference of J along one combined direction: 32 seeded interior inlet entries
+    # of the streamwise component, random signs, scaled by the plane's RMS streamwise velocity
+    plane = cases.inflow_plane(case)
+    rng = np.random.Generator(np.random.Philox(7))
+    d = np.zeros_like(plane)
+    jj = rng.integers(1, plane.shape[0] - 1, 32)
+    ii = rng.integers(1, plane.shape[1] - 1, 32)
+    d[jj, ii, 2] = rng.choice([-1.0, 1.0], 32) * float(np.sqrt((plane[..., 2] ** 2).mean()))
+    # J of the perturbed windows with the Poisson solves to rtol 1e-13: at rtol 1e-10 the
+    # solver's stopping point moves J by about 1e-12 of itself, which is 10 % of the change
+    # that a step of 1e-6 makes
+    kw_fd = dict(kw, rtol=1e-13)
+    ad = float((g * d).sum())
+    fd_check = {"direction": "32 seeded interior inlet entries of w, random signs, x RMS(w) of the plane",
+                "adjoint": ad, "poisson_rtol": 1e-13, "central_difference": {}, "rel_err": {}}
+    for eps in (1e-4, 1e-6):
+        jpm = []
+        for sgn in (1.0, -1.0):
+            ctx.set_inflow_plane(plane + sgn * eps * d)
+            jpm.append(ctx.objective(steps, **kw_fd))
+        fd = (jpm[0] - jpm[1]) / (2 * eps)
+        fd_check["central_difference"]["%g" % eps] = fd
+        fd_check["rel_err"]["%g" % eps] = abs(fd - ad) / max(abs(fd), abs(ad), 1e-300)
+    ctx.set_inflow_plane(plane)
+    ctx.close()
     return {"workload": ADJ_WORKLOAD % (nx, ny, nz, steps, every), "steps": steps, "checkpoint_every": every,
             "forward_ms": round(st.ms_forward, 2), "adjoint_ms": round(st.ms_adjoint, 2),
             "ratio": round(st.ms_adjoint / st.ms_forward, 3), "ratios_of_3_windows": [round(v, 3) for v in ratios],
             "recomputed_steps": st.recomputed_steps,
             "tape_bytes": st.tape_bytes, "operator_setup_s": round(setup_s, 1),
-            "J": st.J, "gradient_norm": float(np.sqrt((g * g).sum())),
+            "J": st.J, "gradient_norm": float(np.sqrt((g * g).sum())), "fd_check": fd_check,
             "note": "ratio = reverse sweep (recomputation of every checkpoint segment plus the adjoint "
                     "steps) / forward sweep of the same window; the window with the median of three ratios"}
+
+
+# Algorithmic bytes per cell of the step's parts (each input read once, each output written
+# once at its stored precision), for the large-window HBM figure.
+STEP_BYTES = {
+    "formfunction2": 4 * 417.0,           # four RK stages
+    "contra2cart": 10 * 121.0,            # two per RK stage, two in the correction
+    "pressure_gradient": 129.0,
+    "calc_k_flux_and_rhs": 25.0 + 33.0,   # Ucont.z + nvert; Ucont + nvert -> b
+    "projection_update": 169.0,
+    "divergence": 8.0,                    # aj, in Projection's Contra2Cart
+    "end_of_step_copies": 96.0,           # Ucont -> Ucont_o, Ucat -> Ucat_o
+    # per FGMRES iteration: the FP64 apply 73, one FP32 V-cycle (3+3 zebra sweeps at 32 B,
+    # restriction and prolongation about 40, the zebra layout conversions 24, coarser
+    # levels x 8/7: about 293), the basis passes (three over j+1 vectors, 8 B each, about
+    # 24 (j+1)) and the Z and V writes 16
+    "per_iteration_fixed": 73.0 + 293.0 + 16.0,
+}
+
+
+def step_bytes_per_cell(iterations):
+    it = int(round(iterations))
+    fixed = sum(v for k, v in STEP_BYTES.items() if k != "per_iteration_fixed")
+    krylov = sum(STEP_BYTES["per_iteration_fixed"] + 24.0 * (j + 1) for j in range(it))
+    return fixed + krylov
+
+
+def large_window(torch, nx=384, ny=256, nz=384, steps=50):
+    """A 50-step window on the 384 x 256 x 384 wavy-bottom open channel with the cylinder
+    array, mixed precision, the step as one CUDA graph: steps/s, algorithmic HBM GB/s
+    (STEP_BYTES), device memory held.  Forward only (see the note in the result)."""
+    import vfs_b200 as vfs
+    from vfs_b200 import cases
+    free0, total = torch.cuda.mem_get_info()
+    case = cases.inflow_outflow(cases.open_channel_cylinders(nx, ny, nz, wavy=0.05), 100)
+    case.immersed = 0
+    ctx, _ = setup_context(case)
+    for _ in range(3):
+        ctx.step(precision=0, rtol=1e-10, graph=1)
+    ms, stats = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10, graph=1), steps, torch)
+    free1, _ = torch.cuda.mem_get_info()
+    ctx.close()
+    its = float(np.mean([s.poisson.iterations for s in stats]))
+    ms_step = ms / steps
+    cells = nx * ny * nz
+    bpc = step_bytes_per_cell(its)
+    return {"workload": "wavy-bottom open channel %dx%dx%d cells (y_w = 0.05 sin(2 pi x/Lx) cos(2 pi z/Lz)), "
+                        "the 3x2 cylinder array as blocked cells, inlet k=0 (inletprofile 100), outlet k+, "
+                        "mixed precision, Poisson rtol 1e-10" % (nx, ny, nz),
+            "steps": steps, "ms_per_step": round(ms_step, 3), "steps_per_s": round(1000.0 / ms_step, 3),
+            "poisson_iterations": its, "max_div": max(s.max_div for s in stats),
+            "hbm_gbs": round(bpc * cells / (ms_step * 1e-3) / 1e9, 1), "bytes_per_cell_per_step": round(bpc, 1),
+            "device_memory_gb": round((free0 - free1) / 1e9, 2),
+            "note": "hbm_gbs = algorithmic bytes of the step (each input read once, each output written "
+                    "once; STEP_BYTES) / step time; the adjoint of this window is not run: its measured "
+                    "operators, tapes and checkpoints need more than the 180 GB of one B200 at this size"}
 
 
 def immersed_variant(nx, ny, nz, torch, steps=10):
@@ -474,6 +555,7 @@ def main():
     ap.add_argument("--size", default=None, help="nx,ny,nz override (not for reported numbers)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--no-immersed", action="store_true", help="skip the immersed-cylinder variant")
+    ap.add_argument("--no-large", action="store_true", help="skip the 384x256x384 50-step window")
     ap.add_argument("--adjoint-size", default="128,128,128")
     ap.add_argument("--adjoint-steps", type=int, default=20)
     ap.add_argument("--profile-step", action="store_true",
@@ -638,6 +720,13 @@ def main():
         except Exception as e:  # reported, never fatal for the forward numbers
             imm = {"failed": str(e)}
 
+    large = None
+    if not args.no_large and not args.size:
+        try:
+            large = large_window(torch)
+        except Exception as e:  # reported, never fatal for the forward numbers
+            large = {"failed": str(e)}
+
     adj = None
     if not args.no_adjoint and not args.size:
         ax, ay, az = (int(v) for v in args.adjoint_size.split(","))
@@ -700,6 +789,8 @@ def main():
             out["adjoint"] = adj
         if imm is not None:
             out["immersed_variant"] = imm
+        if large is not None:
+            out["large_window"] = large
         if cpu is not None:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))

@@ -382,8 +382,13 @@ int vfs_run_kernel(vfs_ctx *ctx, int which, int reps);
  * the state it had on entry. */
 enum {
   VFS_OBJ_KINETIC_ENERGY = 0, /* 0.5 * sum over interior fluid cells of |Ucat|^2 / aj */
-  VFS_OBJ_PRESSURE_DRAG = 1   /* sum over k-faces between a fluid cell and a body cell
+  VFS_OBJ_PRESSURE_DRAG = 1,  /* sum over k-faces between a fluid cell and a body cell
                                  (nvert > 0) of +-P(fluid)*|zet|: streamwise pressure force */
+  VFS_OBJ_DRAG = 2            /* VFS_OBJ_PRESSURE_DRAG plus the viscous traction on the i- and
+                                 j-faces between a fluid cell and a body cell (at rest):
+                                 2/ren * |csi|^2 (|eta|^2) * aj * w of the fluid cell per face,
+                                 the streamwise force of the pressure and shear stresses that
+                                 Calc_forces_SI (fsi.c:5151) sums over the body surface */
 };
 enum {
   VFS_CTRL_INITIAL_UCONT = 0, /* the Ucont the window starts from (DA layout, 3 per point) */

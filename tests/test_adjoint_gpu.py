@@ -6,8 +6,8 @@ seeded control entries, and checkpointing that does not change the gradient.
 
 Cases: the periodic channel with the k-flux forcing (initial-Ucont control, kinetic
 energy), the open channel with an inlet plane and blocked cylinders (inflow-plane control,
-pressure drag), and the wavy channel with an immersed sphere (initial-Ucont control,
-pressure drag on the IB nodes)."""
+drag: pressure force plus viscous traction), and the wavy channel with an immersed sphere
+(initial-Ucont control, drag on the body's cells)."""
 import numpy as np
 import pytest
 
@@ -26,12 +26,12 @@ def _case(name):
         c = cases.open_channel_cylinders(16, 12, 24, D=0.6, Lx=3.2, Lz=8.0, Ly=1.0)
         c.immersed = 0
         cases.inflow_outflow(c, 100)
-        return c, vfs.OBJ_PRESSURE_DRAG, vfs.CTRL_INFLOW_PLANE, None
+        return c, vfs.OBJ_DRAG, vfs.CTRL_INFLOW_PLANE, None
     c = cases.channel(16, 14, 20, wavy=0.1)
     c.immersed = 1
     c.inlet_flux = 5.0
     body = cases.icosphere((np.pi / 2, 1.0, np.pi), 0.45, level=3)
-    return c, vfs.OBJ_PRESSURE_DRAG, vfs.CTRL_INITIAL_UCONT, body
+    return c, vfs.OBJ_DRAG, vfs.CTRL_INITIAL_UCONT, body
 
 
 def _context(name, seed=0):
@@ -188,3 +188,33 @@ def test_checkpointing_does_not_change_the_gradient():
     assert s1.recomputed_steps == 3 and s3.recomputed_steps == 3
     np.testing.assert_allclose(g1, g3, rtol=1e-10, atol=1e-12 * np.abs(g3).max())
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_drag_objective_adds_the_viscous_traction():
+    """OBJ_DRAG - OBJ_PRESSURE_DRAG after one step equals the viscous traction summed on the
+    host from the state of the same step: 2/ren |csi|^2 aj w per i-face (|eta|^2 per j-face)
+    that a fluid cell shares with a body cell."""
+    ctx, case, obj, ctrl = _context("inlet")
+    jd = ctx.objective(1, objective=vfs.OBJ_DRAG, control=ctrl)
+    jp = ctx.objective(1, objective=vfs.OBJ_PRESSURE_DRAG, control=ctrl)
+    ctx.step(precision=1, rtol=1e-12)
+    u = ctx.get_field(vfs.UCAT)
+    nv = ctx.get_field(vfs.NVERT)
+    csi, eta, aj = ctx.get_field(vfs.CSI), ctx.get_field(vfs.ETA), ctx.get_field(vfs.AJ)
+    kz, jz, iz = nv.shape
+    jv = 0.0
+    for k in range(1, kz - 1):
+        for j in range(1, jz - 1):
+            for i in range(1, iz - 1):
+                if nv[k, j, i] != 0:
+                    continue
+                ni = int(i + 1 <= iz - 2 and nv[k, j, i + 1] > 0) + int(i - 1 >= 1 and nv[k, j, i - 1] > 0)
+                nj = int(j + 1 <= jz - 2 and nv[k, j + 1, i] > 0) + int(j - 1 >= 1 and nv[k, j - 1, i] > 0)
+                if ni or nj:
+                    ci = float(np.dot(csi[k, j, i], csi[k, j, i]))
+                    cj = float(np.dot(eta[k, j, i], eta[k, j, i]))
+                    jv += 2.0 / case.ren * (ni * ci + nj * cj) * aj[k, j, i] * u[k, j, i, 2]
+    ctx.close()
+    assert jv != 0.0
+    assert abs((jd - jp) - jv) <= 1e-9 * abs(jv), (jd - jp, jv)

@@ -1077,6 +1077,22 @@ __global__ void k_objective(Grid g, Metrics m, const uint8_t *__restrict__ nv, i
       if (k - 1 >= 1 && nv[p - sz] > 0) w -= centre_area(m.zet, p - sz);     // body upstream
       s += w * P[p];
       if (lp) lp[p] = w;
+      if (obj == VFS_OBJ_DRAG) {
+        // viscous traction on the cell's i- and j-faces shared with a body cell (at rest):
+        // nu * w / (dn/2) * area with the face area |csi| (|eta|) and the normal spacing
+        // dn = 1/(|csi| aj), i.e. 2 nu |csi|^2 aj w per face
+        const long long sy = g.mx;
+        const double ci = m.csi.x[p] * m.csi.x[p] + m.csi.y[p] * m.csi.y[p] + m.csi.z[p] * m.csi.z[p];
+        const double cj = m.eta.x[p] * m.eta.x[p] + m.eta.y[p] * m.eta.y[p] + m.eta.z[p] * m.eta.z[p];
+        int ni = 0, nj = 0;
+        if (i + 1 <= g.mx - 2 && nv[p + 1] > 0) ni++;
+        if (i - 1 >= 1 && nv[p - 1] > 0) ni++;
+        if (j + 1 <= g.my - 2 && nv[p + sy] > 0) nj++;
+        if (j - 1 >= 1 && nv[p - sy] > 0) nj++;
+        const double cv = 2.0 / g.ren * (ni * ci + nj * cj) * m.aj[p];
+        s += cv * u.z[p];
+        if (lu.z) lu.z[p] = cv;
+      }
     }
   }
   sh[threadIdx.x] = s;
@@ -1130,7 +1146,7 @@ static size_t control_size(const Ctx *c, int control) {
 
 static int check_opts(Ctx *c, const vfs_adjoint_opts *o) {
   if (!o || o->nsteps < 1) return set_err(c, VFS_ERR_INVALID, "adjoint: nsteps must be at least 1");
-  if (o->objective != VFS_OBJ_KINETIC_ENERGY && o->objective != VFS_OBJ_PRESSURE_DRAG)
+  if (o->objective != VFS_OBJ_KINETIC_ENERGY && o->objective != VFS_OBJ_PRESSURE_DRAG && o->objective != VFS_OBJ_DRAG)
     return set_err(c, VFS_ERR_INVALID, "adjoint: unknown objective");
   if (o->control != VFS_CTRL_INITIAL_UCONT && o->control != VFS_CTRL_INFLOW_PLANE)
     return set_err(c, VFS_ERR_INVALID, "adjoint: unknown control");
@@ -1219,14 +1235,14 @@ static int tangent_run(Ctx *c, const vfs_adjoint_opts *o, const double *dir, dou
   }
   if (!rc) rc = objective(c, o->objective, true, J);
   double d = 0, t = 0;
-  if (!rc) {
-    if (o->objective == VFS_OBJ_KINETIC_ENERGY) {
-      for (int q = 0; q < 3 && !rc; q++) {
-        rc = dot(c, 0, bankp(c, ADJ, VFS_UCAT, q), bankp(c, TAN, VFS_UCAT, q), &t);
-        d += t;
-      }
-    } else {
-      rc = dot(c, 0, bankp(c, ADJ, VFS_P, 0), bankp(c, TAN, VFS_P, 0), &d);
+  if (!rc) {  // dJ = <dJ/dUcat, dUcat> + <dJ/dP, dP> (the seeds not used by J are zero)
+    for (int q = 0; q < 3 && !rc; q++) {
+      rc = dot(c, 0, bankp(c, ADJ, VFS_UCAT, q), bankp(c, TAN, VFS_UCAT, q), &t);
+      d += t;
+    }
+    if (!rc && o->objective != VFS_OBJ_KINETIC_ENERGY) {
+      rc = dot(c, 0, bankp(c, ADJ, VFS_P, 0), bankp(c, TAN, VFS_P, 0), &t);
+      d += t;
     }
   }
   *dJ = d;

@@ -99,7 +99,7 @@ class AdjointStats(ctypes.Structure):
     ]
 
 
-OBJ_KINETIC_ENERGY, OBJ_PRESSURE_DRAG = 0, 1
+OBJ_KINETIC_ENERGY, OBJ_PRESSURE_DRAG, OBJ_DRAG = 0, 1, 2
 CTRL_INITIAL_UCONT, CTRL_INFLOW_PLANE = 0, 1
 OP_NAMES = ["contra2cart", "form_bcs_tail", "pressure_gradient", "volume_flux", "poisson_rhs",
             "update_pressure", "projection", "ib_bc", "ibm_interpolation"]

@@ -107,15 +107,20 @@ def cylinders_nvert(case, centers, radius):
 
 
 def open_channel_cylinders(nx=256, ny=192, nz=256, Lx=3.2, Ly=1.0, Lz=8.0, D=0.2, dt=5e-4,
-                           ren=1e4, beta=1.5):
+                           ren=1e4, beta=1.5, wavy=0.0):
     """Open channel with a staggered 3x2 array of vertical cylinders (D, spacing 4D):
     spanwise periodic (i), no-slip bottom (j-: 1), free-slip top (j+: 10), streamwise
-    periodic k with the bulk flux held by the k-periodic forcing (momentum.c:382-399)."""
+    periodic k with the bulk flux held by the k-periodic forcing (momentum.c:382-399).
+    With wavy > 0 the bottom is y_w = wavy*sin(2 pi x/Lx)*cos(2 pi z/Lz) and the nodes
+    follow y = y_w + eta*(Ly - y_w) (curvilinear)."""
     x = np.linspace(0.0, Lx, nx + 1)
     eta = np.linspace(0.0, 1.0, ny + 1)
     y = Ly * (1.0 - np.tanh(beta * (1.0 - eta)) / np.tanh(beta))
     z = np.linspace(0.0, Lz, nz + 1)
     Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    if wavy:
+        yw = wavy * np.sin(2 * np.pi * X / Lx) * np.cos(2 * np.pi * Z / Lz)
+        Y = yw + (Y / Ly) * (Ly - yw)
     c = Case("open_channel_cyl%dx%dx%d" % (nx, ny, nz), X, Y, Z, [7, 7, 1, 10, 7, 7],
              i_periodic=1, k_periodic=1, immersed=1, ren=ren, dt=dt, inletprofile=13)
     s = 4 * D
