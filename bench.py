@@ -337,6 +337,16 @@ def fit_note(rows, expo):
                 ", ".join("%s %.2f" % (p, expo[p]) for p in PHASES)))
 
 
+def arm_config(world, nx=NX, ny=NY, nz=NZ, size=None):
+    """The `config` object of the JSON line, the same for both arms."""
+    npts = (nx + 2) * (ny + 2) * (nz + 2)
+    return {"workload": WORKLOAD if not size else "size override %s" % size,
+            "cells": nx * ny * nz, "parallelism": "replicas" if world > 1 else "single-gpu",
+            "precision": "mixed: FP32 multigrid V-cycle (%d levels, zebra y-line Gauss-Seidel 3+3 "
+                         "sweeps, trilinear prolongation) in FP64 FGMRES(30)" % mg_levels(nx, ny, nz),
+            "l2": "inputs larger than L2 (every field is a %d MB array)" % (npts * 8 // 2 ** 20)}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -360,8 +370,8 @@ def reference_arm(args, rank, world):
               % (REF_STEP_SIZE + (fit_note(rows, expo),)))
     out = {"metric": METRIC, "value": round(v, 3), "unit": "ms/step", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-           "config": {"workload": WORKLOAD, "precision": "reference FP64 CPU", "extrapolated": True},
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference", "extrapolated": True,
+           "config": arm_config(world),
            "cpu_baseline": {"value": round(v, 3), "unit": "ms/step", "cores": 1, "kind": "reference",
                             "sample": sample, "extrapolated": True,
                             "fit": {"sizes": ["%dx%dx%d" % s for s in REF_SIZES],
@@ -758,11 +768,7 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD if not args.size else "size override %s" % args.size,
-                       "cells": ncell, "parallelism": "replicas" if world > 1 else "single-gpu",
-                       "precision": "mixed: FP32 multigrid V-cycle (%d levels, zebra y-line Gauss-Seidel 3+3 "
-                                    "sweeps, trilinear prolongation) in FP64 FGMRES(30)" % mg_levels(nx, ny, nz),
-                       "l2": "inputs larger than L2 (every field is a %d MB array)" % (npts * 8 // 2 ** 20)},
+            "config": arm_config(world, nx, ny, nz, args.size),
             "fp64_ms_per_step": round(ms_fp64, 3),
             "launched_ms_per_step": round(ms_launched, 3),
             "step_form": "one CUDA graph per step (captured once, replayed; the Poisson solve's loops as "

@@ -325,6 +325,23 @@ int vfs_restart_write(vfs_ctx *ctx, const char *dir, int ti, int block);
  * the first step repeats the set-up of ti == tistart). */
 int vfs_restart_read(vfs_ctx *ctx, const char *dir, int ti, int block);
 
+/* ---- grid.dat ---------------------------------------------------------------------- */
+
+/* The grid reader of MG_Initial (init.c:313-440).  format: 0 grid.dat in ASCII, 1 grid.dat
+ * in binary (the reference's -binary 1: native ints and doubles), 2 xyz.dat (-xyz 1: one
+ * block of a tensor-product grid).  vfs_grid_read returns the node counts of block `block`
+ * (0-based) in *IM, *JM, *KM and, when x is not NULL, its IM*JM*KM node coordinates
+ * ([k][j][i], i fastest; the layout of vfs_form_metrics) in x, y, z, each value v stored as
+ * v / cl * L_dim as the reference stores it (cl: -chact_leng, L_dim: both 1 for none); call
+ * it with x = NULL first to size the arrays.  vfs_grid_write writes one block in the same
+ * format (17 significant digits in the text forms); xyz.dat takes the tensor axes from the
+ * grid and fails with VFS_ERR_INVALID when the grid is not a tensor product.  Host-only:
+ * no context or GPU needed. */
+int vfs_grid_read(const char *path, int format, int block, double cl, double L_dim, int *IM, int *JM, int *KM,
+                  double *x, double *y, double *z);
+int vfs_grid_write(const char *path, int format, int IM, int JM, int KM, const double *x, const double *y,
+                   const double *z);
+
 /* ---- allocation-free variant ---------------------------------------------------- */
 
 /* Largest grid (DA points (IM+1)*(JM+1)*(KM+1)) vfs_contra2cart_noalloc accepts, and the

@@ -103,7 +103,7 @@ class Reference:
     """The reference solver state for one synthetic case (grid.dat / bcs.dat written to a
     scratch directory and read by MG_Initial)."""
 
-    def __init__(self, case, extra_globals=None):
+    def __init__(self, case, extra_globals=None, grid_writer=None):
         self.case = case
         L = lib()
         g = {"i_periodic": case.i_periodic, "j_periodic": case.j_periodic,
@@ -122,7 +122,10 @@ class Reference:
         for k, v in g.items():
             set_global(k, v)
         self.dir = tempfile.mkdtemp(prefix="vfsref_")
-        case.write_grid_dat(os.path.join(self.dir, "grid.dat"))
+        if grid_writer is None:
+            case.write_grid_dat(os.path.join(self.dir, "grid.dat"))
+        else:  # the caller writes grid.dat (or xyz.dat) into the directory
+            grid_writer(self.dir)
         case.write_bcs_dat(os.path.join(self.dir, "bcs.dat"))
         if L.ref_setup(self.dir.encode()):
             raise RuntimeError("reference MG_Initial failed")

@@ -153,3 +153,115 @@ extern "C" int vfs_restart_read(vfs_ctx *ctx, const char *dir, int ti, int block
   c->first_step = true;
   return VFS_OK;
 }
+
+// ------------------------------------------------------------------ grid.dat
+// The grid reader of MG_Initial (init.c:313-440): grid.dat in ASCII ("nblocks", then per
+// block "IM JM KM" and the IM*JM*KM node x coordinates, then y, then z, [k][j][i] with i
+// fastest, each scanned with %le), the same in binary (-binary 1: int nblocks, ints IM, JM,
+// KM, native doubles), or xyz.dat (-xyz 1: one block, "IM JM KM", then IM lines whose first
+// value is x(i), JM lines whose second is y(j), KM lines whose third is z(k): a tensor
+// grid).  Each value v is stored as v / cl * L_dim, as the reference stores it.
+namespace {
+
+bool skip_doubles(FILE *f, int format, long long n) {
+  double v;
+  for (long long q = 0; q < n; q++) {
+    if (format == 1 ? fread(&v, sizeof(double), 1, f) != 1 : fscanf(f, "%le", &v) != 1) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" int vfs_grid_read(const char *path, int format, int block, double cl, double L_dim, int *IM, int *JM,
+                             int *KM, double *x, double *y, double *z) {
+  if (!path || !IM || !JM || !KM || format < 0 || format > 2 || block < 0 || cl == 0.0)
+    return vfs::set_err(nullptr, VFS_ERR_INVALID, "vfs_grid_read: bad argument");
+  FILE *f = fopen(path, format == 1 ? "rb" : "r");
+  if (!f) return vfs::set_err(nullptr, VFS_ERR_INVALID, std::string("vfs_grid_read: cannot open ") + path);
+  auto fail = [&](const char *why) {
+    fclose(f);
+    return vfs::set_err(nullptr, VFS_ERR_INVALID, std::string("vfs_grid_read: ") + why + " in " + path);
+  };
+  int nblocks = 1;
+  if (format == 1 && fread(&nblocks, sizeof(int), 1, f) != 1) return fail("no block count");
+  if (format == 0 && fscanf(f, "%i\n", &nblocks) != 1) return fail("no block count");
+  if (block >= nblocks) return fail("no such block");
+  int d[3] = {0, 0, 0};
+  for (int bi = 0; bi <= block; bi++) {
+    if (format == 1) {
+      if (fread(d, sizeof(int), 3, f) != 3) return fail("truncated block header");
+    } else if (fscanf(f, "%i %i %i\n", &d[0], &d[1], &d[2]) != 3) {
+      return fail("truncated block header");
+    }
+    if (d[0] < 2 || d[1] < 2 || d[2] < 2) return fail("bad node counts");
+    const long long n = (long long)d[0] * d[1] * d[2];
+    if (bi < block && !skip_doubles(f, format, 3 * n)) return fail("truncated block");
+  }
+  *IM = d[0]; *JM = d[1]; *KM = d[2];
+  if (!x) { fclose(f); return VFS_OK; }
+  if (!y || !z) return fail("null coordinate array");
+  const long long nI = d[0], nJ = d[1], nK = d[2], n = nI * nJ * nK;
+  if (format == 2) {
+    std::vector<double> X(nI), Y(nJ), Z(nK);
+    double t0, t1;
+    for (long long i = 0; i < nI; i++) if (fscanf(f, "%le %le %le\n", &X[i], &t0, &t1) != 3) return fail("truncated x list");
+    for (long long j = 0; j < nJ; j++) if (fscanf(f, "%le %le %le\n", &t0, &Y[j], &t1) != 3) return fail("truncated y list");
+    for (long long k = 0; k < nK; k++) if (fscanf(f, "%le %le %le\n", &t0, &t1, &Z[k]) != 3) return fail("truncated z list");
+    for (long long k = 0; k < nK; k++)
+      for (long long j = 0; j < nJ; j++)
+        for (long long i = 0; i < nI; i++) {
+          const long long p = (k * nJ + j) * nI + i;
+          x[p] = X[i] / cl * L_dim;
+          y[p] = Y[j] / cl * L_dim;
+          z[p] = Z[k] / cl * L_dim;
+        }
+    fclose(f);
+    return VFS_OK;
+  }
+  double *dst[3] = {x, y, z};
+  for (int c = 0; c < 3; c++)
+    for (long long p = 0; p < n; p++) {
+      double v;
+      if (format == 1 ? fread(&v, sizeof(double), 1, f) != 1 : fscanf(f, "%le", &v) != 1) return fail("truncated coordinates");
+      dst[c][p] = v / cl * L_dim;
+    }
+  fclose(f);
+  return VFS_OK;
+}
+
+extern "C" int vfs_grid_write(const char *path, int format, int IM, int JM, int KM, const double *x, const double *y,
+                              const double *z) {
+  if (!path || !x || !y || !z || format < 0 || format > 2 || IM < 2 || JM < 2 || KM < 2)
+    return vfs::set_err(nullptr, VFS_ERR_INVALID, "vfs_grid_write: bad argument");
+  const long long nI = IM, nJ = JM, nK = KM, n = nI * nJ * nK;
+  if (format == 2) {  // a tensor grid only
+    for (long long k = 0; k < nK; k++)
+      for (long long j = 0; j < nJ; j++)
+        for (long long i = 0; i < nI; i++) {
+          const long long p = (k * nJ + j) * nI + i;
+          if (x[p] != x[i] || y[p] != y[j * nI] || z[p] != z[k * nJ * nI])
+            return vfs::set_err(nullptr, VFS_ERR_INVALID, "vfs_grid_write: xyz.dat holds tensor-product grids only");
+        }
+  }
+  FILE *f = fopen(path, format == 1 ? "wb" : "w");
+  if (!f) return vfs::set_err(nullptr, VFS_ERR_INVALID, std::string("vfs_grid_write: cannot create ") + path);
+  bool ok = true;
+  if (format == 1) {
+    const int hdr[4] = {1, IM, JM, KM};
+    ok = fwrite(hdr, sizeof(int), 4, f) == 4 && fwrite(x, sizeof(double), n, f) == (size_t)n &&
+         fwrite(y, sizeof(double), n, f) == (size_t)n && fwrite(z, sizeof(double), n, f) == (size_t)n;
+  } else if (format == 0) {
+    ok = fprintf(f, "1\n%d %d %d\n", IM, JM, KM) > 0;
+    const double *src[3] = {x, y, z};
+    for (int c = 0; c < 3 && ok; c++)
+      for (long long p = 0; p < n && ok; p++) ok = fprintf(f, "%.17e\n", src[c][p]) > 0;
+  } else {
+    ok = fprintf(f, "%d %d %d\n", IM, JM, KM) > 0;
+    for (long long i = 0; i < nI && ok; i++) ok = fprintf(f, "%.17e 0 0\n", x[i]) > 0;
+    for (long long j = 0; j < nJ && ok; j++) ok = fprintf(f, "0 %.17e 0\n", y[j * nI]) > 0;
+    for (long long k = 0; k < nK && ok; k++) ok = fprintf(f, "0 0 %.17e\n", z[k * nJ * nI]) > 0;
+  }
+  if (fclose(f) != 0) ok = false;
+  return ok ? VFS_OK : vfs::set_err(nullptr, VFS_ERR_INVALID, std::string("vfs_grid_write: write failed: ") + path);
+}

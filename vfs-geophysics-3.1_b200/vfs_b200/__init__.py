@@ -117,8 +117,10 @@ EXPORTS = [
     "vfs_adjoint_setup", "vfs_objective", "vfs_tangent", "vfs_adjoint_gradient",
     "vfs_adjoint_op_info", "vfs_adjoint_op_check",
     "vfs_petsc_vec_write", "vfs_petsc_vec_read", "vfs_restart_write", "vfs_restart_read",
-    "vfs_ibm_set_velocity",
+    "vfs_ibm_set_velocity", "vfs_grid_read", "vfs_grid_write",
 ]
+
+GRID_ASCII, GRID_BINARY, GRID_XYZ = 0, 1, 2
 
 _lib = None
 
@@ -138,6 +140,30 @@ def petsc_vec_read(path, n):
     if lib.vfs_petsc_vec_read(os.fsencode(path), out.ctypes.data, n):
         raise VfsError(1, lib.vfs_last_error(None).decode())
     return out
+
+
+def grid_read(path, fmt=GRID_ASCII, block=0, cl=1.0, L_dim=1.0):
+    """Node coordinates (x, y, z), each (KM, JM, IM), of one block of a grid.dat / xyz.dat
+    file, as the reference's MG_Initial reads them (init.c:313-440)."""
+    lib = load_library()
+    d = [ctypes.c_int() for _ in range(3)]
+    if lib.vfs_grid_read(os.fsencode(path), fmt, block, cl, L_dim, *[ctypes.byref(v) for v in d], None, None, None):
+        raise VfsError(1, lib.vfs_last_error(None).decode())
+    IM, JM, KM = (v.value for v in d)
+    x, y, z = (np.empty((KM, JM, IM)) for _ in range(3))
+    if lib.vfs_grid_read(os.fsencode(path), fmt, block, cl, L_dim, *[ctypes.byref(v) for v in d],
+                         x.ctypes.data, y.ctypes.data, z.ctypes.data):
+        raise VfsError(1, lib.vfs_last_error(None).decode())
+    return x, y, z
+
+
+def grid_write(path, x, y, z, fmt=GRID_ASCII):
+    """One block of node coordinates (each (KM, JM, IM)) as grid.dat / xyz.dat."""
+    lib = load_library()
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z)]
+    KM, JM, IM = a[0].shape
+    if lib.vfs_grid_write(os.fsencode(path), fmt, IM, JM, KM, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data):
+        raise VfsError(1, lib.vfs_last_error(None).decode())
 
 
 def load_library(path=None):
@@ -195,6 +221,10 @@ def load_library(path=None):
     lib.vfs_petsc_vec_read.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong]
     lib.vfs_restart_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
     lib.vfs_restart_read.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.vfs_grid_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ip, ip, ip, vp, vp, vp]
+    lib.vfs_grid_write.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
     if path is None:
         _lib = lib
     return lib
