@@ -303,6 +303,57 @@ class ReferenceSample:
         self.R.close()
 
 
+def host_max_div(uc, aj, nv):
+    """Divergence of main.c:1083-1090 on the host: max |(dU + dV + dW) aj| over interior
+    cells with no solid in the 7-point neighbourhood."""
+    d = ((uc[1:-1, 1:-1, 1:-1, 0] - uc[1:-1, 1:-1, :-2, 0]) + (uc[1:-1, 1:-1, 1:-1, 1] - uc[1:-1, :-2, 1:-1, 1]) +
+         (uc[1:-1, 1:-1, 1:-1, 2] - uc[:-2, 1:-1, 1:-1, 2])) * aj[1:-1, 1:-1, 1:-1]
+    s = (nv[1:-1, 1:-1, 1:-1] + nv[2:, 1:-1, 1:-1] + nv[:-2, 1:-1, 1:-1] + nv[1:-1, 2:, 1:-1] + nv[1:-1, :-2, 1:-1] +
+         nv[1:-1, 1:-1, 2:] + nv[1:-1, 1:-1, :-2])
+    return float(np.abs(np.where(s > 0, 0.0, d)).max())
+
+
+def vs_reference_step(nx=64, ny=48, nz=64, nsteps=3):
+    """The mixed and the FP64 forms against the reference's own FP64 steps (oracle/_ref,
+    its Poisson system solved to rtol 1e-10 like the library's) from the same state, on the
+    nx x ny x nz sample of the workload: L2 and Linf of P and Ucat after nsteps steps, and
+    each side's max |div u|."""
+    import vfs_b200 as vfs
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(limits=1), quiet_stdout():
+        S = ReferenceSample(nx, ny, nz)
+        R = S.R
+        m, u, uc, nv = R.metrics(), R.get("Ucat"), R.get("lUcont"), R.get("lNvert")
+        plane = u[1].copy()
+        for _ in range(nsteps):
+            S.step()
+        ref_p, ref_u, ref_uc = R.get("P"), R.get("Ucat"), R.get("lUcont")
+        S.close()
+    out = {"workload": "the metric workload on a %dx%dx%d grid, %d steps from the same state" % (nx, ny, nz, nsteps),
+           "reference_max_div": host_max_div(ref_uc, m["aj"], nv)}
+
+    def rel(a, b):
+        return {"l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                "linf": float(np.abs(a - b).max() / np.abs(b).max())}
+    for prec, name in ((0, "mixed"), (1, "fp64")):
+        case = make_case(nx, ny, nz)
+        ctx = vfs.Context(case.config())
+        ctx.set_metrics(m)
+        ctx.set_field(vfs.NVERT, nv)
+        ctx.set_field(vfs.UCONT, uc)
+        ctx.set_field(vfs.UCAT, u)
+        ctx.set_field(vfs.UCAT_O, u)
+        ctx.set_inflow_plane(plane)
+        ctx.set_scalar(vfs.S_INLET_FLUX, 0.0)
+        _, area = ctx.calc_inlet_area()
+        ctx.set_scalar(vfs.S_INLET_FLUX, area)
+        st = [ctx.step(precision=prec, rtol=1e-10) for _ in range(nsteps)]
+        out[name] = {"p": rel(ctx.get_field(vfs.P), ref_p), "u": rel(ctx.get_field(vfs.UCAT), ref_u),
+                     "max_div": st[-1].max_div}
+        ctx.close()
+    return out
+
+
 def reference_fit(steps_per_size=1):
     """Phase times of one reference step at each of REF_SIZES (after one untimed step)
     and the fitted exponent a of t = c * cells^a for every phase."""
@@ -452,6 +503,7 @@ def adjoint_window(nx, ny, nz, steps, every, torch):
     return {"workload": ADJ_WORKLOAD % (nx, ny, nz, steps, every), "steps": steps, "checkpoint_every": every,
             "forward_ms": round(st.ms_forward, 2), "adjoint_ms": round(st.ms_adjoint, 2),
             "ratio": round(st.ms_adjoint / st.ms_forward, 3), "ratios_of_3_windows": [round(v, 3) for v in ratios],
+            "windows_ms": [[round(r[1].ms_forward, 2), round(r[1].ms_adjoint, 2)] for r in runs],
             "recomputed_steps": st.recomputed_steps,
             "tape_bytes": st.tape_bytes, "operator_setup_s": round(setup_s, 1),
             "J": st.J, "gradient_norm": float(np.sqrt((g * g).sum())), "fd_check": fd_check,
@@ -748,6 +800,7 @@ def main():
     out = None
     if rank == 0:
         cpu = None
+        vsref = None
         if world == 1 and not args.no_cpu_baseline and not args.size:
             try:
                 from oracle import ref
@@ -763,6 +816,12 @@ def main():
             except Exception as e:  # the baseline is reported, never required
                 cpu = {"value": None, "unit": "ms/step", "cores": 1, "kind": "reference",
                        "sample": "failed: %s" % e}
+            try:
+                from oracle import ref
+                if ref.available():
+                    vsref = vs_reference_step()
+            except Exception as e:  # reported, never fatal
+                vsref = {"failed": str(e)}
         out = {
             "metric": METRIC, "value": round(ms_mixed * world / world, 3), "unit": "ms/step",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
@@ -777,6 +836,7 @@ def main():
             "max_div": {"mixed": maxdiv, "fp64": maxdiv64},
             "poisson_iterations": {"mixed": its, "fp64": its64},
             "mixed_vs_fp64": mixed_err,
+            "vs_reference_step": vsref,
             "amdahl": amdahl,
             "adjoint_forward_ratio": adj.get("ratio") if adj else None,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms/step", "h2d_bytes_per_step": io_bytes,
