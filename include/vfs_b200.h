@@ -49,7 +49,9 @@ typedef struct {
                             instead of noslip */
   int moving;            /* movefsi || rotatefsi: the bodies move (ibm.c:3444: IB nodes next
                             to solid cells are reconstructed all the same) */
-  int reserved_i[3];
+  int implicit;          /* -imp: 0 explicit 4-stage Runge-Kutta; 4 the matrix-free implicit
+                            momentum solve (Implicit_MatrixFree, implicitsolver.c:4196) */
+  int reserved_i[2];
   double ren;            /* Reynolds number (user->ren) */
   double dt;             /* time step (user->dt) */
   double st;             /* Strouhal scaling (user->st) */
@@ -59,7 +61,9 @@ typedef struct {
   int reserved_j[7];
   double max_cs;         /* -max_cs upper clip of Cs (main.c:216, default 0.5; values <= 0
                             select the default) */
-  double reserved_d[7];
+  double imp_tol;        /* -imp_tol: relative residual tolerance of the implicit momentum
+                            solve (imp_free_tol, main.c:212; values <= 0 select 1e-4) */
+  double reserved_d[6];
 } vfs_config;
 
 /* Field identifiers for vfs_set_field / vfs_get_field (dof in brackets). */
@@ -82,7 +86,9 @@ enum {
   VFS_KCSI = 24, VFS_KETA = 25, VFS_KZET = 26, VFS_KAJ = 27, /* k-face metrics */
   VFS_CS = 28,      /* [1] dynamic Smagorinsky coefficient lCs */
   VFS_USTAR = 29,   /* [1] friction velocity at IB nodes (lUstar, ibm_interpolation_advanced) */
-  VFS_NFIELDS = 30
+  VFS_RHS_O = 30,   /* [3] RHS_o: Formfunction_2 of the step's initial state (implicit = 4,
+                       solvers.c:1284-1286) */
+  VFS_NFIELDS = 31
 };
 
 /* Scalars for vfs_set_scalar / vfs_get_scalar. */
@@ -301,6 +307,37 @@ int vfs_divergence(vfs_ctx *ctx, double *max_div);
  * UpdatePressure, Projection, Divergence (solvers.c:562-1390 for implicit=0); then ti
  * advances by one.  opts may be NULL for the defaults. */
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
+
+/* ---- implicit momentum (implicit = 4) ----------------------------------------------- */
+
+typedef struct {
+  int newton_iterations;  /* nonlinear iterations taken */
+  int krylov_iterations;  /* GMRES iterations over all of them */
+  int converged;          /* 1 if |F| <= imp_tol |F0| */
+  int reserved_i;
+  double f0, ffinal;      /* 2-norms of the residual at the start and the end */
+  double reserved[4];
+} vfs_newton_stats;
+
+/* FormFunction_SNES (momentum.c:2197-2300) at the current VFS_UCONT: the wall faces of
+ * Ucont take zero normal flux, Ucat follows (Contra2Cart, IB_BC), and VFS_RHS receives
+ *   F = -Ucont/dt + Ucont_o/dt + 0.5 Formfunction_2(Ucont) + 0.5 RHS_o - dP
+ * (the Crank-Nicolson form: time_coeff() = 1 without level set or RANS, poisson.c:17).
+ * Reads VFS_UCONT_O, VFS_RHS_O, VFS_DP, VFS_NU_T; writes VFS_UCONT (its wall faces),
+ * VFS_UCAT and VFS_RHS. */
+int vfs_implicit_residual(vfs_ctx *ctx);
+
+/* Implicit_MatrixFree (implicitsolver.c:4196-4420): InflowFlux and FormBCS without the
+ * outlet rescaling, then Ucont solving F(Ucont) = 0 to |F| <= imp_tol |F0| by Newton's
+ * method with matrix-free Jacobian products (J v = (F(U + h v) - F(U)) / h, h by the
+ * Walker-Pernice rule), unpreconditioned GMRES(30) and a backtracking line search, all on
+ * the device; then the reference's boundary fix-ups of the solution, FormBCS with the
+ * outlet rescaling and, with immersed bodies after the first step, the IB-node
+ * reconstruction.  The reference hands F to PETSc's SNES (trust region, Eisenstat-Walker
+ * forcing); its iterates differ, the solution satisfies the same equations to the same
+ * tolerance.  vfs_step runs this in place of RungeKutta when implicit = 4, after forming
+ * VFS_RHS_O. */
+int vfs_implicit_momentum(vfs_ctx *ctx, vfs_newton_stats *stats);
 
 /* ---- restart files ---------------------------------------------------------------- */
 

@@ -33,6 +33,8 @@ extern void PoissonRHS2_hypre(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 extern void Remove_Nullspace(UserCtx *user, HYPRE_IJVector &B, int i_lower);
 
 extern double inletArea;
+extern PetscErrorCode FormFunction_SNES(SNES snes, Vec Ucont, Vec Rhs, void *ptr);  // momentum.c:2197
+static Vec g_Uin = 0;  // the Ucont handed to FormFunction_SNES
 extern char path[256];                                  // main.c:210
 extern PetscErrorCode Ucont_P_Binary_Output(UserCtx *user);  // main.c:765
 extern PetscErrorCode Ucont_P_Binary_Input(UserCtx *user);   // main.c:394
@@ -104,6 +106,11 @@ static Vec field_vec(const std::string &n) {
   if (n == "lKZet") return u->lKZet;
   if (n == "lKAj") return u->lKAj;
   if (n == "Phi2") return u->Phi2;
+  if (n == "RHS_o") return u->RHS_o;
+  if (n == "Uin") {
+    if (!g_Uin) VecDuplicate(u->Ucont, &g_Uin);
+    return g_Uin;
+  }
   if (n == "B") return g_B;
   if (n == "coor") { Vec c; DAGetGhostedCoordinates(u->da, &c); return c; }
   return 0;
@@ -114,6 +121,7 @@ extern "C" {
 // Reads <dir>/grid.dat and <dir>/bcs.dat with the reference's MG_Initial.  The caller
 // sets the reference globals that MG_Initial consults (les, immersed, rans ...) first.
 int ref_setup(const char *dir) {
+  g_Uin = 0;  // sized for the grid of the last set-up
   strncpy(path, dir, sizeof(path) - 1);
   strcpy(gridfile, "grid.dat");
   L_dim = 1.0;
@@ -216,6 +224,13 @@ int ref_set_inflow_plane(const double *plane) {
   return 0;
 }
 int ref_ib_bc(void) { IB_BC(g_user); return 0; }
+
+// FormFunction_SNES (momentum.c:2197): the implicit momentum residual of Uin into Rhs (it
+// also leaves the evaluated Ucont in Ucont/lUcont and its Ucat in Ucat/lUcat).
+int ref_formfunction_snes(void) {
+  if (!g_Uin) VecDuplicate(g_user->Ucont, &g_Uin);
+  return FormFunction_SNES(0, g_Uin, g_user->Rhs, g_user);
+}
 // Restart files of time step `step` in directory dir: Ucont_P_Binary_Output /
 // Ucont_P_Binary_Input (main.c:765, main.c:394) with the run's `path` and `ti`.
 int ref_restart_output(const char *dir, int step) {

@@ -1146,6 +1146,7 @@ static size_t control_size(const Ctx *c, int control) {
 
 static int check_opts(Ctx *c, const vfs_adjoint_opts *o) {
   if (!o || o->nsteps < 1) return set_err(c, VFS_ERR_INVALID, "adjoint: nsteps must be at least 1");
+  if (c->cfg.implicit) return set_err(c, VFS_ERR_INVALID, "adjoint: the implicit momentum solve is not differentiated");
   if (o->objective != VFS_OBJ_KINETIC_ENERGY && o->objective != VFS_OBJ_PRESSURE_DRAG && o->objective != VFS_OBJ_DRAG)
     return set_err(c, VFS_ERR_INVALID, "adjoint: unknown objective");
   if (o->control != VFS_CTRL_INITIAL_UCONT && o->control != VFS_CTRL_INFLOW_PLANE)

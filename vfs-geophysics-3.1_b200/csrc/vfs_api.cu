@@ -175,7 +175,8 @@ static const int kDof[VFS_NFIELDS] = {
     3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3,  // UCONT..CENT
     3, 3, 3, 1,                            // CSI ETA ZET AJ
     3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1,    // I J K face metrics
-    1, 1};                                  // CS USTAR
+    1, 1,                                   // CS USTAR
+    3};                                     // RHS_O
 
 extern "C" {
 
@@ -216,6 +217,8 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
     return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: immersed must be 0 or 1");
   if (cfg->les != 0 && cfg->les != 1 && cfg->les != 2)
     return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: les must be 0, 1 or 2");
+  if (cfg->implicit != 0 && cfg->implicit != 4)
+    return set_err(nullptr, VFS_ERR_INVALID, "vfs_create: implicit must be 0 (Runge-Kutta) or 4 (matrix-free)");
   if (cudaSetDevice(device) != cudaSuccess) return set_err(nullptr, VFS_ERR_CUDA, "cudaSetDevice failed");
   // The kernels are built for sm_100a only; refuse other GPUs up front.
   cudaDeviceProp prop;
@@ -312,6 +315,7 @@ int vfs_destroy(vfs_ctx *ctx) {
   if (c->nv) cudaFree(c->nv);
   if (c->nvo) cudaFree(c->nvo);
   if (c->gab) cudaFree(c->gab);
+  if (c->imp) cudaFree(c->imp);
   if (c->ibv) cudaFree(c->ibv);
   if (c->bcflag) cudaFree(c->bcflag);
   if (c->solid) cudaFree(c->solid);
@@ -569,7 +573,14 @@ static int step_body(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *s, int 
     if ((rc = eddy_viscosity(c))) return rc;
   }
   if ((rc = pressure_gradient(c))) return rc;
-  if ((rc = runge_kutta(c))) return rc;
+  if (c->cfg.implicit == 4) {  // solvers.c:1282-1289
+    if ((rc = implicit_rhs_o(c))) return rc;
+    // a Newton solve that stops at its iteration cap leaves the step going on, as the
+    // reference's SNESSolve does
+    if ((rc = implicit_momentum(c, nullptr)) && rc != VFS_ERR_NOT_CONVERGED) return rc;
+  } else if ((rc = runge_kutta(c))) {
+    return rc;
+  }
   if ((rc = volume_flux(c))) return rc;  // poisson_hypre.c:566
   if ((rc = poisson_rhs(c))) return rc;
   rc = poisson_solve(c, opts, &s->poisson);
@@ -642,7 +653,7 @@ void step_graph_free(Ctx *c) {
 // Whether the next step is the same sequence of kernels as the last: no set-up work and no
 // decision that changes from step to step.
 static bool graph_eligible(const Ctx *c) {
-  if (c->first_step || c->tape || !c->ps.built || c->g.moving || c->nsolid < 0) return false;
+  if (c->first_step || c->tape || !c->ps.built || c->g.moving || c->nsolid < 0 || c->cfg.implicit) return false;
   if (c->g.les && (c->dynamic_freq != 1 || (c->ti < 2 && c->tistart == 0 && !c->rstart))) return false;
   return true;
 }

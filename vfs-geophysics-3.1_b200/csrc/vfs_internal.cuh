@@ -240,6 +240,8 @@ struct Ctx {
   StepGraph sg;
   long long setup_epoch = 0;     // bumped whenever a captured step would be stale
   cudaStream_t cap_streams[2] = {nullptr, nullptr};  // bodies of the solver's two loops
+  double *imp = nullptr;         // implicit momentum workspace (vfs_implicit.cu)
+  int imp_m = 0;                 // its GMRES restart length
   double *gab = nullptr;         // 9 x N face-metric products of Pressure_Gradient / Projection
   bool gab_valid = false;        // false after any metric upload
 };
@@ -314,6 +316,10 @@ int update_pressure(Ctx *c);
 int projection(Ctx *c);
 int divergence(Ctx *c, double *maxdiv);
 int correction(Ctx *c, bool fuse_divergence);
+// implicit momentum (implicit = 4)
+int implicit_rhs_o(Ctx *c);
+int implicit_residual(Ctx *c);
+int implicit_momentum(Ctx *c, vfs_newton_stats *st);
 int divergence_finish(Ctx *c, double *maxdiv);
 int contra2cart_div(Ctx *c, bool with_divergence);
 

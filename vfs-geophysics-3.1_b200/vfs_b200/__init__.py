@@ -27,8 +27,9 @@ JCSI, JETA, JZET, JAJ = 20, 21, 22, 23
 KCSI, KETA, KZET, KAJ = 24, 25, 26, 27
 CS = 28
 USTAR = 29
-NFIELDS = 30
-FIELD_DOF = [3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 1, 1]
+RHS_O = 30
+NFIELDS = 31
+FIELD_DOF = [3, 3, 1, 1, 1, 1, 3, 3, 3, 3, 1, 3, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 3, 3, 3, 1, 1, 1, 3]
 METRIC_FIELDS = {
     "csi": CSI, "eta": ETA, "zet": ZET, "aj": AJ,
     "icsi": ICSI, "ieta": IETA, "izet": IZET, "iaj": IAJ,
@@ -51,11 +52,12 @@ class VfsConfig(ctypes.Structure):
         ("i_periodic", ctypes.c_int), ("j_periodic", ctypes.c_int), ("k_periodic", ctypes.c_int),
         ("immersed", ctypes.c_int), ("les", ctypes.c_int), ("inletprofile", ctypes.c_int),
         ("dynamic_freq", ctypes.c_int), ("tistart", ctypes.c_int), ("rstart", ctypes.c_int),
-        ("wallfunction", ctypes.c_int), ("moving", ctypes.c_int), ("reserved_i", ctypes.c_int * 3),
+        ("wallfunction", ctypes.c_int), ("moving", ctypes.c_int), ("implicit", ctypes.c_int),
+        ("reserved_i", ctypes.c_int * 2),
         ("ren", ctypes.c_double), ("dt", ctypes.c_double), ("st", ctypes.c_double),
         ("inlet_flux", ctypes.c_double), ("mean_pressure_gradient", ctypes.c_double),
         ("dpdz_set", ctypes.c_int), ("reserved_j", ctypes.c_int * 7),
-        ("max_cs", ctypes.c_double), ("reserved_d", ctypes.c_double * 7),
+        ("max_cs", ctypes.c_double), ("imp_tol", ctypes.c_double), ("reserved_d", ctypes.c_double * 6),
     ]
 
 
@@ -81,6 +83,14 @@ class StepStats(ctypes.Structure):
     _fields_ = [
         ("max_div", ctypes.c_double), ("mean_k_flux", ctypes.c_double),
         ("poisson", SolveStats), ("ms", ctypes.c_double), ("reserved", ctypes.c_double * 4),
+    ]
+
+
+class NewtonStats(ctypes.Structure):
+    _fields_ = [
+        ("newton_iterations", ctypes.c_int), ("krylov_iterations", ctypes.c_int), ("converged", ctypes.c_int),
+        ("reserved_i", ctypes.c_int), ("f0", ctypes.c_double), ("ffinal", ctypes.c_double),
+        ("reserved", ctypes.c_double * 4),
     ]
 
 
@@ -117,7 +127,8 @@ EXPORTS = [
     "vfs_adjoint_setup", "vfs_objective", "vfs_tangent", "vfs_adjoint_gradient",
     "vfs_adjoint_op_info", "vfs_adjoint_op_check",
     "vfs_petsc_vec_write", "vfs_petsc_vec_read", "vfs_restart_write", "vfs_restart_read",
-    "vfs_ibm_set_velocity", "vfs_grid_read", "vfs_grid_write",
+    "vfs_ibm_set_velocity", "vfs_grid_read", "vfs_grid_write", "vfs_implicit_residual",
+    "vfs_implicit_momentum",
 ]
 
 GRID_ASCII, GRID_BINARY, GRID_XYZ = 0, 1, 2
@@ -221,6 +232,8 @@ def load_library(path=None):
     lib.vfs_petsc_vec_read.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong]
     lib.vfs_restart_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
     lib.vfs_restart_read.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    lib.vfs_implicit_residual.argtypes = [vp]
+    lib.vfs_implicit_momentum.argtypes = [vp, ctypes.POINTER(NewtonStats)]
     ip = ctypes.POINTER(ctypes.c_int)
     lib.vfs_grid_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                   ip, ip, ip, vp, vp, vp]
@@ -445,6 +458,14 @@ class Context:
         self._check(self.lib.vfs_step(self.h, ctypes.byref(o), ctypes.byref(st)))
         return st
 
+    def implicit_residual(self):  # FormFunction_SNES, momentum.c:2197
+        self._check(self.lib.vfs_implicit_residual(self.h))
+
+    def implicit_momentum(self):  # Implicit_MatrixFree, implicitsolver.c:4196
+        st = NewtonStats()
+        self._check(self.lib.vfs_implicit_momentum(self.h, ctypes.byref(st)))
+        return st
+
     # ---- tangent-linear and adjoint of a window of steps (no reference counterpart)
     def _adj_opts(self, nsteps, objective, control, checkpoint_every, precision, rtol, kw):
         return AdjointOpts(nsteps=nsteps, checkpoint_every=checkpoint_every, objective=objective,
@@ -517,7 +538,7 @@ def _solve_opts(precision=0, rtol=1e-10, **kw):
 def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
                 inletprofile=13, ren=3000.0, dt=0.04, st=1.0, inlet_flux=-1.0,
                 mean_pressure_gradient=0.0, dpdz_set=0, dynamic_freq=1, tistart=0, rstart=0,
-                max_cs=0.5, wallfunction=0, moving=0):
+                max_cs=0.5, wallfunction=0, moving=0, implicit=0, imp_tol=1e-4):
     c = VfsConfig()
     c.IM, c.JM, c.KM = IM, JM, KM
     for q in range(6):
@@ -528,4 +549,5 @@ def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, im
     c.inlet_flux, c.mean_pressure_gradient, c.dpdz_set = inlet_flux, mean_pressure_gradient, dpdz_set
     c.dynamic_freq, c.tistart, c.rstart, c.max_cs = dynamic_freq, tistart, rstart, max_cs
     c.wallfunction, c.moving = wallfunction, moving
+    c.implicit, c.imp_tol = implicit, imp_tol
     return c

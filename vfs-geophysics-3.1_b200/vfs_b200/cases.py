@@ -28,6 +28,7 @@ class Case:
         self.ren, self.dt, self.st = ren, dt, st
         self.inletprofile, self.inlet_flux = inletprofile, inlet_flux
         self.wallfunction, self.moving = 0, 0
+        self.implicit, self.imp_tol = 0, 1e-4
         self.nvert = np.zeros(self.da_shape)
         self.ucat0 = None
 
@@ -51,7 +52,8 @@ class Case:
         return make_config(self.IM, self.JM, self.KM, self.bctype, self.i_periodic,
                            self.j_periodic, self.k_periodic, self.immersed, self.les,
                            self.inletprofile, self.ren, self.dt, self.st, self.inlet_flux,
-                           wallfunction=self.wallfunction, moving=self.moving)
+                           wallfunction=self.wallfunction, moving=self.moving,
+                           implicit=self.implicit, imp_tol=self.imp_tol)
 
 
 def tanh_stretch(n, beta, lo, hi):
