@@ -663,6 +663,69 @@ __global__ void k_zprolong(ZL F, ZL C, const uint8_t *__restrict__ actF, const u
   zprolong_cell<T>(F, C, actF, actC, x, xc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
+// The same prolongation from the coarse side: coarse cell t (natural index) loads its
+// 3 x 3 x 3 neighbourhood (values and activity) once and updates its eight children, each
+// child with zprolong_cell's neighbours, weights and order of summation, so the results are
+// the same bits.  Needs a fine level of exactly twice the coarse cells in every direction.
+template <typename T>
+__device__ __forceinline__ void zprolong8_cell(const ZL &F, const ZL &C, const uint8_t *__restrict__ actF,
+                                               const uint8_t *__restrict__ actC, T *__restrict__ x,
+                                               const T *__restrict__ xc, long long t) {
+  const long long nc = (long long)C.nx * C.ny * C.nz;
+  if (t >= nc) return;
+  int I, J, K;
+  zcell(C, t, I, J, K);
+  // neighbour index along one direction, wrapped on a periodic level, -1 beyond an edge
+  auto nb = [](int v, int n, int per) { return (v >= 0 && v < n) ? v : (per ? (v + n) % n : -1); };
+  const int Ii[3] = {nb(I - 1, C.nx, C.ip), I, nb(I + 1, C.nx, C.ip)};
+  const int Jj[3] = {nb(J - 1, C.ny, C.jp), J, nb(J + 1, C.ny, C.jp)};
+  const int Kk[3] = {nb(K - 1, C.nz, C.kp), K, nb(K + 1, C.nz, C.kp)};
+  const long long own = zidx(C, I, J, K);
+  T v[27];
+  unsigned ok = 0;
+#pragma unroll
+  for (int e = 0; e < 27; e++) {
+    const int a = e % 3, b = (e / 3) % 3, cc = e / 9;
+    const bool in = Ii[a] >= 0 && Jj[b] >= 0 && Kk[cc] >= 0;
+    const long long qc = in ? zidx(C, Ii[a], Jj[b], Kk[cc]) : own;
+    v[e] = xc[qc];
+    if (in && actC[qc]) ok |= 1u << e;
+  }
+  const T xo = v[13];
+#pragma unroll
+  for (int ch = 0; ch < 8; ch++) {
+    const int ai = ch & 1, aj = (ch >> 1) & 1, ak = ch >> 2;
+    const int i = 2 * I + ai, j = 2 * J + aj, k = 2 * K + ak;
+    const long long q = zidx(F, i, j, k);
+    if (!actF[q]) continue;
+    // offset of the other nearest coarse cell: +1 for an odd child index, -1 for an even one
+    const int di = ai ? 2 : 0, dj = aj ? 2 : 0, dk = ak ? 2 : 0;
+    const T xq = x[q];
+    T wown = T(27) / T(64);
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+          if (a + bb + c == 0) continue;
+          const T w = (a ? T(1) : T(3)) * (bb ? T(1) : T(3)) * (c ? T(1) : T(3)) / T(64);
+          const int e = (a ? di : 1) + 3 * (bb ? dj : 1) + 9 * (c ? dk : 1);
+          if (!((ok >> e) & 1u)) { wown += w; continue; }
+          s += w * v[e];
+        }
+    x[q] = xq + (s + wown * xo);
+  }
+}
+
+template <typename T>
+__global__ void k_zprolong8(ZL F, ZL C, const uint8_t *__restrict__ actF, const uint8_t *__restrict__ actC,
+                            T *__restrict__ x, const T *__restrict__ xc) {
+  pdl_prologue();
+  zprolong8_cell<T>(F, C, actF, actC, x, xc, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+
 // act[q] = 1 where the level's diagonal is non-zero (an active unknown).
 __global__ void k_mg_active(long long n, const double *__restrict__ op, uint8_t *__restrict__ act) {
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -950,6 +1013,9 @@ static int mg_bottom(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
 
 // V-cycle from level l (its right-hand side already in place); levels at or below
 // kBottomCells run inside one thread block.
+#ifndef VFS_PROLONG8
+#define VFS_PROLONG8 1
+#endif
 template <typename T>
 static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   int rc;
@@ -970,9 +1036,13 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
                       f.tri, f.x, f.b, cc.b);
   if (rc) return rc;
   if ((rc = mg_vcycle<T>(c, l + 1, nl, o))) return rc;
-  if ((rc = launch_chain(c, "k_zprolong", k_zprolong<T>, dim3(nblocks(nf, 256)), dim3(256), 0, F.z, C.z, F.act,
-                         C.act, f.x, cc.x)))
-    return rc;
+  if (VFS_PROLONG8 && F.z.nx == 2 * C.z.nx && F.z.ny == 2 * C.z.ny && F.z.nz == 2 * C.z.nz)
+    rc = launch_chain(c, "k_zprolong8", k_zprolong8<T>, dim3(nblocks(nc, 128)), dim3(128), 0, F.z, C.z, F.act,
+                      C.act, f.x, cc.x);
+  else
+    rc = launch_chain(c, "k_zprolong", k_zprolong<T>, dim3(nblocks(nf, 256)), dim3(256), 0, F.z, C.z, F.act,
+                      C.act, f.x, cc.x);
+  if (rc) return rc;
   return mg_smooth<T>(c, l, o.post_smooth, false);
 }
 
