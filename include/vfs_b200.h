@@ -129,7 +129,7 @@ typedef struct {
                         the host.  Same kernels, same results as 0 (launched one by one).
                         Steps with set-up work (the first step, a new operator, moving
                         bodies, the first two LES steps of a fresh run, a recorded tape)
-                        run launched one by one. */
+                        and implicit momentum steps run launched one by one. */
   int reserved[3];
   double rtol;       /* relative residual target (default 1e-10) */
   double atol;       /* absolute residual target (default 0) */
@@ -303,9 +303,10 @@ int vfs_divergence(vfs_ctx *ctx, double *max_div);
 
 /* One projection time step: Calc_k_Flux, the eddy viscosity when les != 0
  * (Contra2Cart, Compute_Smagorinsky_Constant_1 every dynamic_freq steps,
- * Compute_eddy_viscosity_LES), Pressure_Gradient, RungeKutta, Poisson (RHS, solve),
- * UpdatePressure, Projection, Divergence (solvers.c:562-1390 for implicit=0); then ti
- * advances by one.  opts may be NULL for the defaults. */
+ * Compute_eddy_viscosity_LES), Pressure_Gradient, RungeKutta (with implicit = 4: RHS_o and
+ * vfs_implicit_momentum instead, solvers.c:1282-1289), Poisson (RHS, solve),
+ * UpdatePressure, Projection, Divergence (solvers.c:562-1390); then ti advances by one.
+ * opts may be NULL for the defaults. */
 int vfs_step(vfs_ctx *ctx, const vfs_solve_opts *opts, vfs_step_stats *stats);
 
 /* ---- implicit momentum (implicit = 4) ----------------------------------------------- */
