@@ -63,7 +63,10 @@ typedef struct {
                             select the default) */
   double imp_tol;        /* -imp_tol: relative residual tolerance of the implicit momentum
                             solve (imp_free_tol, main.c:212; values <= 0 select 1e-4) */
-  double reserved_d[6];
+  double roughness;      /* -roughness (roughness_size, rough_set, main.c:2073): > 0 makes the
+                            wall model of body 0 the rough-wall log law
+                            wall_function_roughness_loglaw (wallfunction.c:71, ibm.c:3469) */
+  double reserved_d[5];
 } vfs_config;
 
 /* Field identifiers for vfs_set_field / vfs_get_field (dof in brackets). */

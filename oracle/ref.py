@@ -73,7 +73,7 @@ INT_GLOBALS = ("i_periodic", "j_periodic", "k_periodic", "ii_periodic", "jj_peri
                "wave_momentum_source", "wave_sponge_layer", "surface_tension",
                "air_flow_levelset_periodic", "dynamic_freq", "testfilter_ik", "testfilter_1d",
                "i_homo_filter", "j_homo_filter", "k_homo_filter", "NumberOfBodies")
-DBL_GLOBALS = ("inlet_flux", "mean_pressure_gradient", "max_cs")
+DBL_GLOBALS = ("inlet_flux", "mean_pressure_gradient", "max_cs", "roughness_size")
 
 
 def set_global(name, value):
@@ -114,7 +114,9 @@ class Reference:
              "tistart": 0, "weno": 0, "second_order": 0, "central": 0, "inviscid": 0,
              "skew": 0, "clark": 0, "laplacian": 0, "dpdz_set": 0, "movefsi": 0,
              "rotatefsi": 0, "inlet_flux": case.inlet_flux, "NumberOfBodies": 1,
-             "wallfunction": getattr(case, "wallfunction", 0)}
+             "wallfunction": getattr(case, "wallfunction", 0),
+             "rough_set": int(getattr(case, "roughness", 0.0) > 0),
+             "roughness_size": getattr(case, "roughness", 0.0)}
         if getattr(case, "moving", 0):
             g["movefsi"] = 1
         if extra_globals:

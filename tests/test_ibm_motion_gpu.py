@@ -3,7 +3,8 @@ rows 1 and 3), on the B200 against the reference's own functions.
 
 * ibm_interpolation_advanced (ibm.c:3405-3530) with -wallfunction from ti > 0: the node
   velocity from wall_function_roughness_a (sediment_transport-Y.c:68, compiled into the
-  oracle), the friction velocity ustar, a non-zero surface velocity of the body (ibm->u).
+  oracle) or, with -roughness, the rough-wall log law (wallfunction.c:71), the friction
+  velocity ustar, a non-zero surface velocity of the body (ibm->u).
   The wall model's logarithms, exponentials and sine are CUDA's and glibc's, which may
   differ in the last bit, so the comparison is to 1e-12 relative.
 * A body that moves between steps (movefsi): the IB search of every step with the cells
@@ -40,10 +41,14 @@ def _surface_velocity(x, y, z):
 
 
 @pytest.mark.gpu
-def test_wall_model_reconstruction_matches_reference():
+@pytest.mark.parametrize("roughness", [0.0, 1e-3])
+def test_wall_model_reconstruction_matches_reference(roughness):
+    """roughness 0: wall_function_roughness_a; > 0 (-roughness): body 0 takes the rough-wall
+    log law wall_function_roughness_loglaw (wallfunction.c:71)."""
     case = small_channel(16, 14, 20, wavy=0.1)
     case.immersed = 1
     case.wallfunction = 1
+    case.roughness = roughness
     R, ctx = build_pair(case)
     x, y, z, tri = _sphere()
     R.ibm_classify(x, y, z, tri, build_list=True)

@@ -236,6 +236,7 @@ int vfs_create(const vfs_config *cfg, int device, vfs_ctx **out) {
   for (int q = 0; q < 6; q++) g.bc[q] = cfg->bctype[q];
   g.immersed = cfg->immersed; g.les = cfg->les;
   g.wallfunction = cfg->wallfunction; g.moving = cfg->moving;
+  g.roughness = cfg->roughness > 0 ? cfg->roughness : 0.0;
   g.ren = cfg->ren; g.dt = cfg->dt; g.st = cfg->st;
   c->scal[VFS_S_DT] = cfg->dt; c->scal[VFS_S_REN] = cfg->ren; c->scal[VFS_S_ST] = cfg->st;
   c->scal[VFS_S_INLET_FLUX] = cfg->inlet_flux;

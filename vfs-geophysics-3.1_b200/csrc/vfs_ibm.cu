@@ -627,6 +627,7 @@ int ibm_search(Ctx *c, int ibi, int n_v, const double *x, const double *y, const
     if (c->ibbuf) cudaFree(c->ibbuf);
     c->ibn = nodes;
     c->nib = base + hn;
+    if (ibi == 0) c->nib_body0 = hn;
     c->ibbuf = nullptr;
     if (c->nib && cudaMalloc(&c->ibbuf, sizeof(double) * kIbOut * (size_t)c->nib) != cudaSuccess) {
       cudaFree(buf);
@@ -690,6 +691,25 @@ __device__ __forceinline__ double wf_f_hydset(double nu, double u, double y, dou
   if (yplus <= y0plus) return utau0 * yplus - u;
   return utau0 * (1. / kappa * log(wf_e_coeff(utau0, ks, nu) * yplus)) - u;
 }
+// The rough-wall log law of wall_function_roughness_loglaw (wallfunction.c:71-98,
+// 221-250, 423-437): u = utau (ln(y/ks)/kappa + 8.5), solved for utau by Newton's method
+// with a central-difference derivative (step 1e-7), at most 30 steps, stopping when a step
+// moves utau by less than 1e-10.
+__device__ __forceinline__ double wf_u_loglaw(double y, double utau, double ks) {
+  const double kappa = 0.41;
+  return utau * (1. / kappa * log(y / ks) + 8.5);
+}
+__device__ __forceinline__ double wf_find_utau_loglaw(double u, double y, double guess, double ks) {
+  double x = guess, x0 = guess;
+  const double eps = 1.e-7;
+  for (int i = 0; i < 30; i++) {
+    const double df = ((wf_u_loglaw(y, x0 + eps, ks) - u) - (wf_u_loglaw(y, x0 - eps, ks) - u)) / (2 * eps);
+    x = x0 - (wf_u_loglaw(y, x0, ks) - u) / df;
+    if (fabs(x0 - x) < 1.e-10) break;
+    x0 = x;
+  }
+  return x;
+}
 __device__ __forceinline__ double wf_find_utau(double nu, double u, double y, double guess, double ks) {
   double utau = guess, utau0 = guess;
   const double eps = 1.e-7;
@@ -711,7 +731,7 @@ __device__ __forceinline__ double wf_find_utau(double nu, double u, double y, do
 // reference reads the local copies lUcat and lP), then write.
 __global__ void k_ibm_gather(Grid g, const IbNode *__restrict__ nodes, int n, CV3 ucat, const double *__restrict__ p,
                              const uint8_t *__restrict__ nv, const double *__restrict__ ibv, int nvtx, int ti,
-                             double *out) {
+                             int nbody0, double *out) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const IbNode N = nodes[q];
@@ -735,6 +755,24 @@ __global__ void k_ibm_gather(Grid g, const IbNode *__restrict__ nodes, int n, CV
   if ((!g.moving && (double)nv[s1] + (double)nv[s2] + (double)nv[s3] > 0.1) || nv[pos] > 2) {
     ub[0] = ub[1] = ub[2] = 0;
     ustar = 0;
+  } else if (g.wallfunction && ti > 0 && g.roughness > 0 && q < nbody0) {
+    // rough_set && ibi == 0: the rough-wall log law, tangential velocity only (ibm.c:3468-3470)
+    const double nx = N.nf[0], ny = N.nf[1], nz = N.nf[2];
+    const double u_c = ucx - uax, v_c = ucy - uay, w_c = ucz - uaz;
+    const double un = u_c * nx + v_c * ny + w_c * nz;
+    double ut = u_c - un * nx, vt = v_c - un * ny, wt = w_c - un * nz;
+    const double ut_mag = sqrt(ut * ut + vt * vt + wt * wt);
+    ustar = wf_find_utau_loglaw(ut_mag, sc, 0.01, g.roughness);
+    const double ut_mag_modeled = wf_u_loglaw(sb, ustar, g.roughness);
+    if (ut_mag > 1.e-10) {
+      ut *= ut_mag_modeled / ut_mag;
+      vt *= ut_mag_modeled / ut_mag;
+      wt *= ut_mag_modeled / ut_mag;
+    } else {
+      ut = vt = wt = 0;
+    }
+    ub[0] = ut; ub[1] = vt; ub[2] = wt;
+    ub[0] += uax; ub[1] += uay; ub[2] += uaz;
   } else if (g.wallfunction && ti > 0) {
     const double nx = N.nf[0], ny = N.nf[1], nz = N.nf[2];
     const double u_c = ucx - uax, v_c = ucy - uay, w_c = ucz - uaz;
@@ -818,7 +856,7 @@ int ibm_interpolation(Ctx *c) {
     const Grid &g = c->g;
     c->launches++, k_ibm_gather<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, cv(field3(c, VFS_UCAT)),
                                                              c->f[VFS_P][0], c->nv, c->ibv, c->nvtx, c->ti,
-                                                             c->ibbuf);
+                                                             c->nib_body0, c->ibbuf);
     if ((rc = check_launch(c, "k_ibm_gather"))) return rc;
     c->launches++, k_ibm_scatter<<<nblocks(c->nib, 128), 128, 0, c->stream>>>(g, c->ibn, c->nib, c->ibbuf, field3(c, VFS_UCAT),
                                                               c->f[VFS_P][0], c->f[VFS_USTAR][0]);

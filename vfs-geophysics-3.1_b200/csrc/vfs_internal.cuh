@@ -30,6 +30,7 @@ struct Grid {
   double ren, dt, st;
   int wallfunction;     // -wallfunction: wall model in the IB-node reconstruction
   int moving;           // movefsi || rotatefsi: moving bodies
+  double roughness;     // -roughness: rough-wall log law for body 0 (0: unset)
 };
 
 __host__ __device__ inline long long lidx(const Grid &g, int i, int j, int k) {
@@ -216,6 +217,7 @@ struct Ctx {
   IbNode *ibn = nullptr;        // IB-node list of every searched body (device)
   int nib = 0;                  // its length
   int nib_unresolved = 0;       // nodes whose interception search failed (reference: garbage)
+  int nib_body0 = 0;            // the first nib_body0 nodes belong to body 0
   double *ibbuf = nullptr;      // per-node gather buffer (4 doubles per node)
   double *inflow_plane = nullptr;  // inlet velocity plane, my*mx Cartesian triples (inletprofile 100)
   double *inlet_nodes = nullptr;   // grid nodes of the k = 1 node plane: x, y, z blocks of JM*IM

@@ -57,7 +57,8 @@ class VfsConfig(ctypes.Structure):
         ("ren", ctypes.c_double), ("dt", ctypes.c_double), ("st", ctypes.c_double),
         ("inlet_flux", ctypes.c_double), ("mean_pressure_gradient", ctypes.c_double),
         ("dpdz_set", ctypes.c_int), ("reserved_j", ctypes.c_int * 7),
-        ("max_cs", ctypes.c_double), ("imp_tol", ctypes.c_double), ("reserved_d", ctypes.c_double * 6),
+        ("max_cs", ctypes.c_double), ("imp_tol", ctypes.c_double), ("roughness", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 5),
     ]
 
 
@@ -538,7 +539,7 @@ def _solve_opts(precision=0, rtol=1e-10, **kw):
 def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, immersed=0, les=0,
                 inletprofile=13, ren=3000.0, dt=0.04, st=1.0, inlet_flux=-1.0,
                 mean_pressure_gradient=0.0, dpdz_set=0, dynamic_freq=1, tistart=0, rstart=0,
-                max_cs=0.5, wallfunction=0, moving=0, implicit=0, imp_tol=1e-4):
+                max_cs=0.5, wallfunction=0, moving=0, implicit=0, imp_tol=1e-4, roughness=0.0):
     c = VfsConfig()
     c.IM, c.JM, c.KM = IM, JM, KM
     for q in range(6):
@@ -549,5 +550,5 @@ def make_config(IM, JM, KM, bctype, i_periodic=0, j_periodic=0, k_periodic=0, im
     c.inlet_flux, c.mean_pressure_gradient, c.dpdz_set = inlet_flux, mean_pressure_gradient, dpdz_set
     c.dynamic_freq, c.tistart, c.rstart, c.max_cs = dynamic_freq, tistart, rstart, max_cs
     c.wallfunction, c.moving = wallfunction, moving
-    c.implicit, c.imp_tol = implicit, imp_tol
+    c.implicit, c.imp_tol, c.roughness = implicit, imp_tol, roughness
     return c

@@ -29,6 +29,7 @@ class Case:
         self.inletprofile, self.inlet_flux = inletprofile, inlet_flux
         self.wallfunction, self.moving = 0, 0
         self.implicit, self.imp_tol = 0, 1e-4
+        self.roughness = 0.0
         self.nvert = np.zeros(self.da_shape)
         self.ucat0 = None
 
@@ -53,7 +54,7 @@ class Case:
                            self.j_periodic, self.k_periodic, self.immersed, self.les,
                            self.inletprofile, self.ren, self.dt, self.st, self.inlet_flux,
                            wallfunction=self.wallfunction, moving=self.moving,
-                           implicit=self.implicit, imp_tol=self.imp_tol)
+                           implicit=self.implicit, imp_tol=self.imp_tol, roughness=self.roughness)
 
 
 def tanh_stretch(n, beta, lo, hi):
