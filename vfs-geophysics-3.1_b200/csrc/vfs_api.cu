@@ -439,9 +439,15 @@ int vfs_set_scalar(vfs_ctx *ctx, int which, double value) {
   if (which == VFS_S_DT) c->g.dt = value;
   if (which == VFS_S_REN) c->g.ren = value;
   if (which == VFS_S_ST) c->g.st = value;
-  if (which == VFS_S_TI) c->ti = (int)value;
-  // kernel arguments of a captured step change: capture again
-  if (which == VFS_S_DT || which == VFS_S_REN || which == VFS_S_ST || which == VFS_S_TI) c->setup_epoch++;
+  // kernel arguments of a captured step change: capture again.  A captured step depends on
+  // ti only through the tests ti > 0 (the wall model of the IB-node reconstruction) and
+  // ti < 2 (the first LES steps, which are never captured)
+  if (which == VFS_S_DT || which == VFS_S_REN || which == VFS_S_ST) c->setup_epoch++;
+  if (which == VFS_S_TI) {
+    const int ti = (int)value;
+    if ((ti > 0) != (c->ti > 0) || (ti < 2) != (c->ti < 2)) c->setup_epoch++;
+    c->ti = ti;
+  }
   return ds_upload(c);
 }
 
