@@ -86,6 +86,27 @@ def test_one_step_matches_reference(name, precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("faces", [(1, 2), (1, 10), (1, -10), (1, 12), (12, 1), (1, 13), (1, 14), (1, 4)])
+def test_one_step_boundary_codes(faces):
+    """One step of the wavy channel with the j- and j+ faces set to the other wall codes
+    FormBCS and Contra2Cart handle (bcs.c:1841-2936, rhs.c:291-675): 2 moving lid (j+),
+    10 / -10 free slip, 12 moving wall, 13 and 14 slip lids, 4 outlet on j+."""
+    case = small_channel(wavy=0.15)
+    case.bctype[2], case.bctype[3] = faces
+    case.inlet_flux = 5.0
+    R, ctx = build_pair(case)
+    ref.set_global("inlet_flux", case.inlet_flux)
+    ctx.set_scalar(vfs.S_INLET_FLUX, case.inlet_flux)
+    reference_step(R)
+    st = ctx.step(precision=1, rtol=1e-13)
+    assert st.poisson.converged == 1
+    assert_close(ctx.get_field(vfs.P), R.get("P"), rtol=1e-10, atol_frac=0, what="P")
+    assert_close(ctx.get_field(vfs.UCONT), R.get("lUcont"), rtol=1e-10, atol_frac=0, what="Ucont")
+    assert_close(ctx.get_field(vfs.UCAT), R.get("Ucat"), rtol=1e-10, atol_frac=0, what="Ucat")
+    R.close()
+
+
+@pytest.mark.gpu
 def test_ten_steps_stay_divergence_free():
     """Ten steps on the 64^3 channel: every step ends with max|div| below 1e-8 in both
     precisions (the Divergence() gate of main.c:1083-1090)."""
