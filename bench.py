@@ -393,6 +393,14 @@ def fit_note(rows, expo):
                 ", ".join("%s %.2f" % (p, expo[p]) for p in PHASES)))
 
 
+def max_over_ranks(values, dist, torch, device):
+    """The largest of each value over the ranks of the process group (the replicas' step
+    times: the job is as slow as its slowest replica)."""
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def arm_config(world, nx=NX, ny=NY, nz=NZ, size=None):
     """The `config` object of the JSON line, the same for both arms."""
     npts = (nx + 2) * (ny + 2) * (nz + 2)
@@ -780,9 +788,7 @@ def main():
     launches_per_step = None
 
     if dist is not None:
-        t = torch.tensor([ms_mixed, ms_fp64, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_mixed, ms_fp64, e2e_ms = [float(v) for v in t.tolist()]
+        ms_mixed, ms_fp64, e2e_ms = max_over_ranks([ms_mixed, ms_fp64, e2e_ms], dist, torch, "cuda")
 
     n0 = ctx.launch_count()
     ctx.step(precision=0, rtol=1e-10, graph=1)
