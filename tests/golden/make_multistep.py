@@ -27,7 +27,7 @@ NPTS = 20000
 
 
 def main(out=os.path.join(HERE, "multistep_wavy_sphere_les_128x96x128.npz")):
-    case, body = multistep.config2_wavy_sphere()
+    case, body = multistep.wavy_sphere_les()
     t0 = time.time()
     run = multistep.ReferenceRun(case, body=body)
     nv = run.R.get("lNvert")

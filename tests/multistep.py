@@ -19,8 +19,8 @@ from vfs_b200 import cases
 import vfs_b200 as vfs
 
 
-def config1_channel():
-    """64^3 periodic channel (streamwise k), tanh stretch beta = 2 in y,
+def channel_64():
+    """The 64^3 periodic channel (streamwise k), tanh stretch beta = 2 in y,
     2pi x 2 x pi (x/z labels swapped so that k is streamwise), Re_b = 5600 (ren = 2800),
     laminar parabola + uniform noise 0.1 U_b (seed 0), dt = 1e-3, no immersed body, no LES."""
     c = cases.channel(64, 64, 64)
@@ -28,8 +28,8 @@ def config1_channel():
     return c
 
 
-def config2_wavy_sphere(nx=128, ny=96, nz=128, level=5):
-    """the channel mapping with the sinusoidal bottom wall
+def wavy_sphere_les(nx=128, ny=96, nz=128, level=5):
+    """The 128 x 96 x 128 channel mapping with the sinusoidal bottom wall
     y_w = 0.1 sin(2 pi x/Lx) cos(2 pi z/Lz), an immersed sphere of diameter 0.4 at the
     domain centre (icosphere of 20 * 4**level triangles; level 5 = 20480), dynamic
     Smagorinsky LES (les = 2), Re = 1e4, FP64, dt = 1e-3."""

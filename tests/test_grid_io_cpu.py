@@ -1,4 +1,4 @@
-"""grid.dat and xyz.dat (row (f) 2): the library's reader against the reference's own
+"""grid.dat and xyz.dat: the library's reader against the reference's own
 MG_Initial (init.c:313-440, compiled into oracle/_ref) on files in each of the three
 formats the reference reads, and round trips through the library's writer.  Host code
 only: no GPU."""

@@ -1,5 +1,5 @@
-"""Immersed-boundary reconstruction with a wall model and with moving bodies (section 8(f)
-rows 1 and 3), on the B200 against the reference's own functions.
+"""Immersed-boundary reconstruction with a wall model and with moving bodies, on the B200
+against the reference's own functions.
 
 * ibm_interpolation_advanced (ibm.c:3405-3530) with -wallfunction from ti > 0: the node
   velocity from wall_function_roughness_a (sediment_transport-Y.c:68, compiled into the

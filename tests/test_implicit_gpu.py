@@ -1,4 +1,4 @@
-"""Implicit momentum (implicit = 4, row (f) 4) on the B200 against the reference's own
+"""Implicit momentum (implicit = 4) on the B200 against the reference's own
 residual, FormFunction_SNES (momentum.c:2197-2300, compiled into oracle/_ref).
 
 * The residual F(Ucont) = -Ucont/dt + Ucont_o/dt + 0.5 Formfunction_2(Ucont) + 0.5 RHS_o

@@ -1,10 +1,10 @@
-"""Multi-step parity on the configurations' own grids: the B200 step repeated against the
+"""Multi-step parity on two workloads of their own size: the B200 step repeated against the
 reference's step (oracle/_ref) repeated from the same inputs (tests/multistep.py).
 
-* 64^3 periodic channel, 10 FP64 steps at dt = 1e-3 (config 1): the reference is run
+* 64^3 periodic channel, 10 FP64 steps at dt = 1e-3: the reference is run
   here, and P, Ucont and Ucat are compared over the whole DA grid.
 * 128x96x128 wavy-wall channel with the immersed 20480-triangle sphere and dynamic
-  Smagorinsky LES, 20 steps (config 2): the reference's 20 steps take minutes on one core,
+  Smagorinsky LES, 20 steps: the reference's 20 steps take minutes on one core,
   so its result is a committed fixture (tests/golden/make_multistep.py): the fields at
   20000 seeded points, plane sums and global norms, compared with the same quantities of
   the device run.
@@ -28,8 +28,8 @@ FIXTURE2 = os.path.join(HERE, "golden", "multistep_wavy_sphere_les_128x96x128.np
 
 
 @pytest.fixture(scope="module")
-def config1_reference():
-    run = multistep.ReferenceRun(multistep.config1_channel())
+def channel_64_reference():
+    run = multistep.ReferenceRun(multistep.channel_64())
     for _ in range(10):
         run.step()
     out = run.fields()
@@ -39,8 +39,8 @@ def config1_reference():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", [1, 0])
-def test_config1_ten_steps_match_reference(config1_reference, precision):
-    run, want = config1_reference
+def test_channel_64_ten_steps_match_reference(channel_64_reference, precision):
+    run, want = channel_64_reference
     ctx, stats = multistep.device_run(run.case, run.m, run.u0, run.uc0, 10, precision=precision)
     for s, st in enumerate(stats):
         assert st.poisson.converged == 1, s
@@ -54,12 +54,12 @@ def test_config1_ten_steps_match_reference(config1_reference, precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.skipif(not os.path.exists(FIXTURE2), reason="config-2 fixture not generated")
+@pytest.mark.skipif(not os.path.exists(FIXTURE2), reason="the 128x96x128 LES fixture is not generated")
 @pytest.mark.parametrize("precision", [1, 0])
-def test_config2_twenty_les_steps_match_reference_fixture(precision):
+def test_wavy_sphere_les_twenty_steps_match_reference_fixture(precision):
     import vfs_b200 as vfs
     fx = np.load(FIXTURE2)
-    case, body = multistep.config2_wavy_sphere()
+    case, body = multistep.wavy_sphere_les()
     nsteps = int(fx["nsteps"])
     # the reference's metrics are those FormMetrics gives bit for bit on the device
     ctx0 = vfs.Context(case.config())

@@ -1,4 +1,4 @@
-"""Restart files (section 8(f) row 2): the library's PETSc-binary Vec reader and writer
+"""Restart files: the library's PETSc-binary Vec reader and writer
 against the reference's own Ucont_P_Binary_Output / Ucont_P_Binary_Input (main.c:765,
 main.c:394), compiled into the oracle with the shim's binary viewer.  Host code only."""
 import os

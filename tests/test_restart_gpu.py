@@ -1,4 +1,4 @@
-"""Restart through the library (section 8(f) row 2): a run written to restart files with
+"""Restart through the library: a run written to restart files with
 vfs_restart_write and continued in a new context with vfs_restart_read gives the same
 steps as the run that never stopped, and the reference's own Ucont_P_Binary_Input
 (main.c:394) reads the files the library wrote."""
