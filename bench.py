@@ -214,12 +214,13 @@ def timed(ctx, fn, reps, torch):
 KERNEL_TRAFFIC = {"formfunction2": 1285.6e6 * 8}
 
 KERNEL_BYTES = {
-    # Formfunction_2 accumulating into Rhs (Formfunction_2(user, Rhs, scale) adds):
-    # Ucont 24 + Ucat 24 + nvert 1 + nu_t 8 + face metrics 240 + centre metrics 72 +
-    # Rhs read 24 + Rhs write 24
-    "formfunction2": 417.0,
-    # FP64 matrix-free Poisson apply: g_ab 72 + phi 8 + mask 1 + y 8
-    "poisson_apply_fp64": 89.0,
+    # Formfunction_2 accumulating into Rhs (Formfunction_2(user, Rhs, scale) adds), les = 0
+    # as in the workload (nu_t is not read): Ucont 24 + Ucat 24 + nvert 1 + face metrics 240
+    # + centre metrics 72 + Rhs read 24 + Rhs write 24
+    "formfunction2": 409.0,
+    # FP64 Poisson apply with the 7 stored stencil slots (no cross terms on this grid):
+    # coefficients 56 + phi 8 + mask 1 + y 8
+    "poisson_apply_fp64": 73.0,
     # one zebra line-Gauss-Seidel sweep (both colours) of the finest multigrid level, FP32:
     # couplings +i/+j/+k 12 + Thomas factors 8 + b 4 + x read 4 + x write 4
     "smoother_fp32": 32.0,
