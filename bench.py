@@ -538,7 +538,7 @@ def adjoint_window(nx, ny, nz, steps, every, torch):
 # Algorithmic bytes per cell of the step's parts (each input read once, each output written
 # once at its stored precision), for the large-window HBM figure.
 STEP_BYTES = {
-    "formfunction2": 4 * 417.0,           # four RK stages
+    "formfunction2": 4 * 433.0,           # four RK stages (pUcont and dP read, Ucont written)
     "contra2cart": 10 * 121.0,            # two per RK stage, two in the correction
     "pressure_gradient": 129.0,
     "calc_k_flux_and_rhs": 25.0 + 33.0,   # Ucont.z + nvert; Ucont + nvert -> b
