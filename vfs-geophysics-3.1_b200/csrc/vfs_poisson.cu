@@ -268,8 +268,11 @@ int poisson_apply_dev(Ctx *c, const double *x, double *y) {
 #ifndef VFS_KRY_BLOCKS_PER_SM
 #define VFS_KRY_BLOCKS_PER_SM 4
 #endif
+// Two resident blocks per SM cap the basis kernels at 128 registers (their 32-vector
+// branch spills; the common ones fit): the step went from 35.6 to 34.5 ms against one
+// block per SM at 250 registers (256 x 192 x 256, mixed, graph form).
 #ifndef VFS_KRY_MINB
-#define VFS_KRY_MINB 1
+#define VFS_KRY_MINB 2
 #endif
 static const int kKryBlocks = 148 * VFS_KRY_BLOCKS_PER_SM;
 // Blocks of the basis passes: a fixed multiple of the SM count, grid-stride (one point
