@@ -487,11 +487,16 @@ int vfs_tangent(vfs_ctx *ctx, const vfs_adjoint_opts *opts, const double *dir, d
 int vfs_adjoint_gradient(vfs_ctx *ctx, const vfs_adjoint_opts *opts, double *grad, vfs_adjoint_stats *stats);
 /* Test hooks: the slots (field, component pairs) and entry count of measured operator op
  * (0 Contra2Cart, 1 FormBCS tail, 2 Pressure_Gradient, 3 VolumeFlux, 4 Poisson RHS, 5
- * UpdatePressure, 6 Projection, 7 IB_BC, 8 IB-node interpolation); and, for vectors x and y
- * (slot-major, N per slot), L x by the operator's kernels and L^T y by its measured matrix
- * (the dot-product test <y, L x> = <L^T y, x>). */
+ * UpdatePressure, 6 Projection, 7 IB_BC, 8 IB-node interpolation); for vectors x and y
+ * (slot-major, N per slot), L x by the operator's kernels and L^T y by the transpose the
+ * adjoint sweep applies (the dot-product test <y, L x> = <L^T y, x>): hand-written kernels
+ * for Pressure_Gradient, VolumeFlux without IB nodes, the Poisson right-hand side,
+ * UpdatePressure and Projection, the measured matrix for the others; and L^T y by the
+ * measured matrix alone (vfs_adjoint_op_measured), against which the hand-written
+ * transposes are checked. */
 int vfs_adjoint_op_info(vfs_ctx *ctx, int op, int *nslot, int *fields, long long *nnz);
 int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *x, const double *y, double *Lx, double *LTy);
+int vfs_adjoint_op_measured(vfs_ctx *ctx, int op, const double *y, double *LTy);
 
 #ifdef __cplusplus
 }

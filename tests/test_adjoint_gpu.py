@@ -13,6 +13,7 @@ import pytest
 
 import vfs_b200 as vfs
 from vfs_b200 import cases
+from helpers import report
 
 NSTEPS = 2
 
@@ -97,8 +98,8 @@ NAMES = ["channel", "inlet", "sphere"]
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", NAMES)
 def test_measured_operators_match_kernels(name):
-    """Dot-product test of every measured operator: <y, L x> by its forward kernels equals
-    <L^T y, x> by its measured matrix."""
+    """Dot-product test of every operator: <y, L x> by its forward kernels equals <L^T y, x>
+    by the transpose the adjoint sweep applies (hand-written or measured)."""
     ctx, case, obj, ctrl = _context(name)
     rng = np.random.Generator(np.random.Philox(7))
     N = int(np.prod(ctx.shape))
@@ -115,6 +116,61 @@ def test_measured_operators_match_kernels(name):
         assert abs(a - b) <= 1e-12 * scale, (vfs.OP_NAMES[op], a, b, nnz)
         checked += 1
     assert checked >= 8
+    ctx.close()
+
+
+def _handwritten_check(ctx, seed):
+    """Each hand-written transpose against the measured matrix (element-wise, relative to
+    the largest entry) and in the dot-product test against the forward kernels."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    N = int(np.prod(ctx.shape))
+    worst = 0.0
+    for name in vfs.OP_HANDWRITTEN:
+        op = vfs.OP_NAMES.index(name)
+        slots, nnz = ctx.adjoint_op_info(op)
+        if not slots:
+            continue
+        x = rng.standard_normal((len(slots), N))
+        y = rng.standard_normal((len(slots), N))
+        lx, lty = ctx.adjoint_op_check(op, x, y)
+        lm = ctx.adjoint_op_measured(op, y)
+        err = float(np.abs(lty - lm).max() / np.abs(lm).max())
+        assert err <= 1e-13, (name, err)
+        a, b = float((y * lx).sum()), float((lty * x).sum())
+        assert abs(a - b) <= 1e-12 * float(np.abs(y * lx).sum()), (name, a, b)
+        worst = max(worst, err)
+    return worst
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_handwritten_transposes_match_measured(name):
+    ctx, case, obj, ctrl = _context(name)
+    _handwritten_check(ctx, 17)
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("periodic", ["ik", "ijk", "none"])
+def test_handwritten_transposes_random_nvert(periodic):
+    """Every branch of the stencils: nvert drawn from {0, 1, 2, 3} on a wavy grid (one-sided
+    cross differences next to IB nodes and solids, Projection's j-face nvert sum 5), with
+    periodic directions i and k, all three, or none (walls all round)."""
+    case = cases.channel(10, 9, 12, wavy=0.1)
+    case.i_periodic = int("i" in periodic)
+    case.j_periodic = int("j" in periodic)
+    case.k_periodic = int("k" in periodic)
+    case.bctype = [7 if case.i_periodic else 1] * 2 + [7 if case.j_periodic else 1] * 2 + \
+                  [7 if case.k_periodic else 1] * 2
+    rng = np.random.Generator(np.random.Philox(23))
+    nv = np.zeros(case.da_shape)
+    nv[1:-1, 1:-1, 1:-1] = rng.choice([0, 0, 0, 0, 1, 2, 3], size=nv[1:-1, 1:-1, 1:-1].shape)
+    case.nvert = nv
+    ctx = vfs.Context(case.config())
+    ctx.form_metrics(case.X, case.Y, case.Z)
+    ctx.set_field(vfs.NVERT, nv)
+    ctx.set_scalar(vfs.S_INLET_FLUX, 0.0)
+    report("hand-written vs measured transposes, random nvert " + periodic, _handwritten_check(ctx, 29))
     ctx.close()
 
 

@@ -41,7 +41,7 @@ def test_autograd_binding_matches_tangent_and_differences():
     d = rng.standard_normal(x0.shape)
     d[0], d[-1], d[:, 0], d[:, -1] = 0, 0, 0, 0
     Jt, dJ = ctx.tangent(d, NSTEPS, obj, ctrl)
-    assert float(J) == pytest.approx(Jt, rel=1e-12)
+    assert float(J.detach()) == pytest.approx(Jt, rel=1e-12)
     assert float((g * d).sum()) == pytest.approx(dJ, rel=1e-9)
     # central differences with a step of 1e-4 of the plane's largest value: at 1e-6 the
     # change of J (about 1e-6 relative) is within a few decades of the forward window's own

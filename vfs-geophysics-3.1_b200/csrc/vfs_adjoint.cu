@@ -5,18 +5,22 @@
 // Every operator of the step that is linear with coefficients fixed by the grid, nvert
 // and the boundary codes (Contra2Cart, the FormBCS wall/edge tail, Pressure_Gradient
 // without its flux forcing, the blocked-cell VolumeFlux, the local Poisson right-hand
-// side, UpdatePressure, Projection, IB_BC, the IB-node interpolation) is taken as a
+// side, UpdatePressure, Projection, IB_BC, the IB-node interpolation) is also taken as a
 // sparse matrix measured from the forward kernels themselves: the operator is applied to
 // coloured unit vectors (ColourMap below), each output is decoded to the one input of that
 // colour it depends on with two index-weighted probes, and a conflict (two inputs of one
 // colour reaching one output) is an error.  The matrix is therefore the forward code's,
-// branch for branch; its transpose gives the adjoint.
+// branch for branch.  The adjoint sweep applies the transposes of the boundary operators
+// (Contra2Cart, the FormBCS tail, IB_BC, the IB-node interpolation) by these matrices; the
+// stencils of the projection step (Pressure_Gradient, VolumeFlux, the Poisson right-hand
+// side, UpdatePressure, Projection) by hand-written gather kernels (vfs_adjoint_stencil.cu),
+// which the tests check against the measured matrices.
 //
-// Hand-written: Formfunction_2 with the RK stage update (vfs_momentum.cu), the global
-// couplings (k-flux forcing, inflow rescaling, outlet rescaling, the null-space shift of
-// the Poisson right-hand side, the immersed VolumeFlux correction), and the Poisson solve
-// (tangent: the forward solver on the tangent right-hand side; adjoint: FGMRES on the
-// transposed operator, right-hand side made mean-free on the unknowns).
+// Hand-written as well: Formfunction_2 with the RK stage update (vfs_momentum.cu), the
+// global couplings (k-flux forcing, inflow rescaling, outlet rescaling, the null-space
+// shift of the Poisson right-hand side, the immersed VolumeFlux correction), and the
+// Poisson solve (tangent: the forward solver on the tangent right-hand side; adjoint:
+// FGMRES on the transposed operator, right-hand side made mean-free on the unknowns).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -476,6 +480,35 @@ static int apply_op(Ctx *c, int o, int b, int transpose) {
   return VFS_OK;
 }
 
+// In place on the adjoint bank: slots <- L^T slots by the hand-written transpose where the
+// operator has one (vfs_adjoint_stencil.cu: Pressure_Gradient, the local Poisson right-hand
+// side, UpdatePressure, Projection; the blocked-cell VolumeFlux is a 0/1 diagonal, its own
+// transpose), else (or with measured) by the measured matrix.
+static bool handwritten(const Ctx *c, int o) {
+  switch (o) {
+    case OP_PG: case OP_PRL: case OP_UP: case OP_PJ: return true;
+    case OP_VF: return !c->g.immersed;
+    default: return false;
+  }
+}
+
+static int adjoint_apply(Ctx *c, int o, bool measured = false) {
+  if (measured || !handwritten(c, o)) return apply_op(c, o, ADJ, 1);
+  int rc;
+  V3 lU = bank3(c, ADJ, VFS_UCONT);
+  double *lP = bankp(c, ADJ, VFS_P, 0), *lphi = bankp(c, ADJ, VFS_PHI, 0);
+  switch (o) {
+    case OP_PG: return pressure_gradient_adjoint(c, lP, bank3(c, ADJ, VFS_DP));
+    case OP_PRL: return poisson_rhs_local_adjoint(c, lU, bankp(c, ADJ, VFS_B, 0));
+    case OP_UP: return update_pressure_adjoint(c, lP, lphi);
+    case OP_PJ:
+      if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;  // Projection closes with Contra2Cart
+      return projection_adjoint(c, lphi, lU);
+    case OP_VF: return apply_op(c, OP_VF, ADJ, 0);
+    default: return set_err(c, VFS_ERR_INVALID, "adjoint: no hand-written transpose");
+  }
+}
+
 // ---------------------------------------------------------------- set-up
 static void set_slots(LinOp &op, std::initializer_list<int> fields) {
   op.nslot = 0;
@@ -836,7 +869,7 @@ static int solve_lin(Ctx *c, int b, const vfs_solve_opts *o) {
   int rc;
   double *bb = bankp(c, b, VFS_B, 0), *ph = bankp(c, b, VFS_PHI, 0);
   if (b == TAN) return lin_solve_into(c, bb, ph, o, false);
-  if ((rc = periodic_copy_adj3(c, V3{ph, nullptr, nullptr}))) return rc;
+  if ((rc = periodic_copy1_adjoint(c, ph))) return rc;
   c->launches++, k_fluid_shift<<<nblocks(N, 256), 256, 0, c->stream>>>(N, c->ps.fluid, nullptr, 0.0, 1, ph);
   double sum = 0;
   if ((rc = fluid_sum(c, ph, nullptr, &sum))) return rc;
@@ -963,15 +996,15 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
   if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;
   if ((rc = apply_op(c, OP_IBBC, ADJ, 1))) return rc;
   if (imm && (rc = apply_op(c, OP_IBM, ADJ, 1))) return rc;
-  if ((rc = apply_op(c, OP_PJ, ADJ, 1))) return rc;
-  if ((rc = apply_op(c, OP_UP, ADJ, 1))) return rc;
+  if ((rc = adjoint_apply(c, OP_PJ))) return rc;
+  if ((rc = adjoint_apply(c, OP_UP))) return rc;
   if ((rc = solve_lin(c, ADJ, o))) return rc;
   if ((rc = nullspace_scale_lin(c, ADJ))) return rc;
-  if ((rc = apply_op(c, OP_PRL, ADJ, 1))) return rc;
+  if ((rc = adjoint_apply(c, OP_PRL))) return rc;
   cudaMemsetAsync(bankp(c, ADJ, VFS_B, 0), 0, bytes, c->stream);
   if (imm) {
     if ((rc = vfi_lin(c, t, ADJ, 1))) return rc;
-  } else if ((rc = apply_op(c, OP_VF, ADJ, 1))) {
+  } else if ((rc = adjoint_apply(c, OP_VF))) {
     return rc;
   }
   // RungeKutta, last to first
@@ -1015,10 +1048,7 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
     c->launches++, k_add_kflux<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, lF / (g.mz - 2), lU.z);
     if ((rc = check_launch(c, "k_add_kflux"))) return rc;
   }
-  if ((rc = apply_op(c, OP_PG, ADJ, 1))) return rc;
-  cudaMemsetAsync(ldp.x, 0, bytes, c->stream);
-  cudaMemsetAsync(ldp.y, 0, bytes, c->stream);
-  cudaMemsetAsync(ldp.z, 0, bytes, c->stream);
+  if ((rc = adjoint_apply(c, OP_PG))) return rc;  // clears ldP
   if (t.first_step) {
     if ((rc = apply_op(c, OP_IBBC, ADJ, 1))) return rc;
     if (imm && (rc = apply_op(c, OP_IBM, ADJ, 1))) return rc;
@@ -1320,9 +1350,11 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
   return rc;
 }
 
-// One measured operator on host vectors (slot-major, N per slot): L x by its forward
-// kernels and L^T y by its measured matrix, for the dot-product test <y, L x> = <L^T y, x>.
-static int op_check(Ctx *c, int o, const double *x, const double *y, double *Lx, double *LTy) {
+// One operator on host vectors (slot-major, N per slot): L x by its forward kernels and
+// L^T y by the transpose the adjoint sweep applies (hand-written where the operator has
+// one, else measured; measured: always the measured matrix), for the dot-product test
+// <y, L x> = <L^T y, x> and the comparison of the two transposes.
+static int op_check(Ctx *c, int o, const double *x, const double *y, double *Lx, double *LTy, bool measured) {
   int rc;
   if ((rc = adjoint_setup(c))) return rc;
   Adjoint &A = *c->adj;
@@ -1333,13 +1365,13 @@ static int op_check(Ctx *c, int o, const double *x, const double *y, double *Lx,
   zero_bank(c, TAN);
   zero_bank(c, ADJ);
   for (int s = 0; s < op.nslot; s++) {
-    cudaMemcpyAsync(A.bank[TAN][op.slot[s].field][op.slot[s].comp], x + s * N, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (x) cudaMemcpyAsync(A.bank[TAN][op.slot[s].field][op.slot[s].comp], x + s * N, bytes, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(A.bank[ADJ][op.slot[s].field][op.slot[s].comp], y + s * N, bytes, cudaMemcpyHostToDevice, c->stream);
   }
-  rc = apply_op(c, o, TAN, 0);
-  if (!rc) rc = apply_op(c, o, ADJ, 1);
+  rc = x ? apply_op(c, o, TAN, 0) : VFS_OK;
+  if (!rc) rc = adjoint_apply(c, o, measured);
   for (int s = 0; s < op.nslot && !rc; s++) {
-    cudaMemcpyAsync(Lx + s * N, A.bank[TAN][op.slot[s].field][op.slot[s].comp], bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (Lx) cudaMemcpyAsync(Lx + s * N, A.bank[TAN][op.slot[s].field][op.slot[s].comp], bytes, cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(LTy + s * N, A.bank[ADJ][op.slot[s].field][op.slot[s].comp], bytes, cudaMemcpyDeviceToHost, c->stream);
   }
   cudaStreamSynchronize(c->stream);
@@ -1415,7 +1447,14 @@ int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *x, const double *y,
   Ctx *c = (Ctx *)ctx;
   VFS_ADJ_REQUIRE(c);
   if (!x || !y || !Lx || !LTy) return set_err(c, VFS_ERR_INVALID, "vfs_adjoint_op_check: null argument");
-  return op_check(c, op, x, y, Lx, LTy);
+  return op_check(c, op, x, y, Lx, LTy, false);
+}
+
+int vfs_adjoint_op_measured(vfs_ctx *ctx, int op, const double *y, double *LTy) {
+  Ctx *c = (Ctx *)ctx;
+  VFS_ADJ_REQUIRE(c);
+  if (!y || !LTy) return set_err(c, VFS_ERR_INVALID, "vfs_adjoint_op_measured: null argument");
+  return op_check(c, op, nullptr, y, nullptr, LTy, true);
 }
 
 }  // extern "C"

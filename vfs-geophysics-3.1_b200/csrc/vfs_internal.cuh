@@ -290,7 +290,14 @@ int ff2_stage_tangent(Ctx *c, const double *const uc[3], const double *const uk[
                       V3 dpu, double *const tf[3][6]);
 int ff2_stage_adjoint(Ctx *c, const double *const uc[3], const double *const uk[3], double a, V3 lU, V3 lu, V3 ldp,
                       V3 lpu, double *const lf[3][6], double *const lfp[3]);
-int periodic_copy_adj3(Ctx *c, V3 v);
+
+// hand-written transposes of the projection step's stencils (vfs_adjoint_stencil.cu)
+int periodic_copy1_adjoint(Ctx *c, double *a);
+int periodic_copy3_adjoint(Ctx *c, V3 a);
+int pressure_gradient_adjoint(Ctx *c, double *lP, V3 ldp);
+int projection_adjoint(Ctx *c, double *lphi, V3 luc);
+int update_pressure_adjoint(Ctx *c, double *lP, double *lphi);
+int poisson_rhs_local_adjoint(Ctx *c, V3 luc, double *lb);
 
 // tangent / adjoint support (vfs_adjoint.cu)
 int tape_stage(Ctx *c, int stage);

@@ -2249,31 +2249,6 @@ __global__ void k_adj_rhs(Grid g, Metrics m, const uint8_t *__restrict__ nv, dou
   }
 }
 
-// Transpose of the periodic ghost copy: each ghost point hands its adjoint to its image.
-__global__ void k_periodic_copy_adj(Grid g, double *a, double *b, double *c) {
-  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p >= g.N) return;
-  int i, j, k;
-  dijk(g, p, i, j, k);
-  const bool gi = g.iper && (i == 0 || i == g.mx - 1), gj = g.jper && (j == 0 || j == g.my - 1);
-  const bool gk = g.kper && (k == 0 || k == g.mz - 1);
-  if (!(gi || gj || gk)) return;
-  const long long s = lidx(g, wrapi(g, i), wrapj(g, j), wrapk(g, k));
-  double *arr[3] = {a, b, c};
-  for (int t = 0; t < 3; t++) {
-    if (!arr[t]) continue;
-    const double v = arr[t][p];
-    arr[t][p] = 0;
-    if (v != 0) atomicAdd(arr[t] + s, v);
-  }
-}
-
-int periodic_copy_adj3(Ctx *c, V3 v) {
-  if (!(c->g.iper || c->g.jper || c->g.kper)) return VFS_OK;
-  c->launches++, k_periodic_copy_adj<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, v.x, v.y, v.z);
-  return check_launch(c, "k_periodic_copy_adj");
-}
-
 // Tangent of one stage: dU (in: tangent of the stage input; out: of the stage output).
 int ff2_stage_tangent(Ctx *c, const double *const uc[3], const double *const uk[3], double a, V3 dU, V3 du, V3 ddp,
                       V3 dpu, double *const tf[3][6]) {
@@ -2322,7 +2297,7 @@ int ff2_stage_adjoint(Ctx *c, const double *const uc[3], const double *const uk[
   CV3 ucb{uc[0], uc[1], uc[2]}, ukb{uk[0], uk[1], uk[2]};
   c->launches++, k_adj_face<<<nblocks(g.N, 128), 128, 0, c->stream>>>(g, m, c->nv, ucb, ukb, fb, lU, lu);
   if ((rc = check_launch(c, "k_adj_face"))) return rc;
-  return periodic_copy_adj3(c, lU);
+  return periodic_copy3_adjoint(c, lU);
 }
 
 }  // namespace vfs

@@ -114,6 +114,9 @@ OBJ_KINETIC_ENERGY, OBJ_PRESSURE_DRAG, OBJ_DRAG = 0, 1, 2
 CTRL_INITIAL_UCONT, CTRL_INFLOW_PLANE = 0, 1
 OP_NAMES = ["contra2cart", "form_bcs_tail", "pressure_gradient", "volume_flux", "poisson_rhs",
             "update_pressure", "projection", "ib_bc", "ibm_interpolation"]
+# operators whose adjoint is a hand-written kernel (VolumeFlux only without IB nodes, where
+# it is a 0/1 diagonal); the others are applied by their measured matrices
+OP_HANDWRITTEN = ["pressure_gradient", "volume_flux", "poisson_rhs", "update_pressure", "projection"]
 
 EXPORTS = [
     "vfs_create", "vfs_destroy", "vfs_last_error", "vfs_dims", "vfs_synchronize",
@@ -126,7 +129,7 @@ EXPORTS = [
     "vfs_smagorinsky_constant", "vfs_eddy_viscosity", "vfs_inflow_flux", "vfs_set_inflow_plane",
     "vfs_ibm_search", "vfs_ibm_list", "vfs_ibm_interpolation",
     "vfs_adjoint_setup", "vfs_objective", "vfs_tangent", "vfs_adjoint_gradient",
-    "vfs_adjoint_op_info", "vfs_adjoint_op_check",
+    "vfs_adjoint_op_info", "vfs_adjoint_op_check", "vfs_adjoint_op_measured",
     "vfs_petsc_vec_write", "vfs_petsc_vec_read", "vfs_restart_write", "vfs_restart_read",
     "vfs_ibm_set_velocity", "vfs_grid_read", "vfs_grid_write", "vfs_implicit_residual",
     "vfs_implicit_momentum",
@@ -229,6 +232,7 @@ def load_library(path=None):
     lib.vfs_adjoint_op_info.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp,
                                         ctypes.POINTER(ctypes.c_longlong)]
     lib.vfs_adjoint_op_check.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp]
+    lib.vfs_adjoint_op_measured.argtypes = [vp, ctypes.c_int, vp, vp]
     lib.vfs_petsc_vec_write.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong]
     lib.vfs_petsc_vec_read.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong]
     lib.vfs_restart_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
@@ -516,7 +520,8 @@ class Context:
         return [(fields[2 * s], fields[2 * s + 1]) for s in range(n.value)], nnz.value
 
     def adjoint_op_check(self, op, x, y):
-        """(L x by the operator's kernels, L^T y by its measured matrix); x, y: slots x N."""
+        """(L x by the operator's kernels, L^T y by the transpose the adjoint sweep applies:
+        hand-written for OP_HANDWRITTEN, else the measured matrix); x, y: slots x N."""
         slots, _ = self.adjoint_op_info(op)
         N = int(np.prod(self.shape))
         a = np.ascontiguousarray(x, dtype=np.float64).reshape(len(slots), N)
@@ -526,6 +531,15 @@ class Context:
         self._check(self.lib.vfs_adjoint_op_check(self.h, op, a.ctypes.data, b.ctypes.data, lx.ctypes.data,
                                                   lty.ctypes.data))
         return lx, lty
+
+    def adjoint_op_measured(self, op, y):
+        """L^T y by the operator's measured matrix (y: slots x N)."""
+        slots, _ = self.adjoint_op_info(op)
+        N = int(np.prod(self.shape))
+        b = np.ascontiguousarray(y, dtype=np.float64).reshape(len(slots), N)
+        lty = np.zeros_like(b)
+        self._check(self.lib.vfs_adjoint_op_measured(self.h, op, b.ctypes.data, lty.ctypes.data))
+        return lty
 
 
 def _solve_opts(precision=0, rtol=1e-10, **kw):
