@@ -468,13 +468,16 @@ typedef struct {
   int recomputed_steps;
   int checkpoints;
   long long tape_bytes;  /* per-segment linearisation state held on the device */
-  double reserved[4];
+  double poisson_iterations_forward;  /* mean FGMRES iterations of the forward steps' solves */
+  double poisson_iterations_adjoint;  /* mean FGMRES iterations of the transposed solves */
+  double reserved[2];
 } vfs_adjoint_stats;
 
 /* Measures the step's fixed linear operators (Contra2Cart, FormBCS tail, Pressure_Gradient,
  * VolumeFlux, Poisson right-hand side, UpdatePressure, Projection, IB_BC, IB-node
- * interpolation) as sparse matrices from the forward kernels (their transposes are the
- * adjoint's operators; the tangent runs the kernels themselves).  Needs metrics and nvert (and
+ * interpolation) as sparse matrices from the forward kernels: the adjoint applies the
+ * transposes of the boundary operators by them, and the tests check the hand-written
+ * transposes of the others against them; the tangent runs the kernels themselves.  Needs metrics and nvert (and
  * the IB-node list when immersed); a later change of nvert or of the grid needs a new
  * context.  The other adjoint entry points call it when needed. */
 int vfs_adjoint_setup(vfs_ctx *ctx);

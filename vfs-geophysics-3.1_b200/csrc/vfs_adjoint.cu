@@ -40,13 +40,17 @@ constexpr int kMaxSlots = 10;
 struct SlotPtrs { double *p[kMaxSlots]; };
 
 // A measured operator: its slots, the forward function (the tangent runs it on the
-// tangent fields), and its matrix by columns (the adjoint's rows).
+// tangent fields), and the transpose of its matrix.
 struct LinOp {
   int nslot = 0;
   Slot slot[kMaxSlots];
   std::function<int(Ctx *)> fn;
   long long nnz = 0;
-  int *cp = nullptr, *ri = nullptr; double *cvl = nullptr;  // CSC: rows of the transpose
+  // The transpose in sliced ELLPACK (slices of 32 rows; entry k of row 32 s + l at
+  // off[s] + 32 k + l): a warp reads its slice's columns and values coalesced.  Columns
+  // index the slots gathered end to end; padding points at a zero past them.
+  long long nslice = 0;
+  long long *off = nullptr; int *col = nullptr; double *val = nullptr;
 };
 
 enum { OP_C2C = 0, OP_FBT, OP_PG, OP_VF, OP_PRL, OP_UP, OP_PJ, OP_IBBC, OP_IBM, OP_N };
@@ -59,7 +63,7 @@ struct Adjoint {
   bool built = false;
   double *bank[2][VFS_NFIELDS][3] = {};
   double *pu[2][3] = {};            // tangent / adjoint of the RK base state pUcont
-  double *tmp[kMaxSlots] = {};      // SpMV results before they replace the slots
+  double *xcat = nullptr;           // SpMV input: the slots end to end, then zeros (padding)
   double *lface[3][6] = {};         // adjoint of the face fluxes: dir x (div xyz, visc xyz)
   double *lfp[3] = {};              // adjoint of Fp
   double *tface[3][6] = {};         // tangent face fluxes
@@ -69,6 +73,7 @@ struct Adjoint {
   double *ckpt = nullptr;           // checkpoints of the state
   int nckpt = 0;
   cudaEvent_t t0 = nullptr, t1 = nullptr;  // sweep timing (the step and the solver use the context's)
+  long long it_fwd = 0, n_fwd = 0, it_adj = 0, n_adj = 0;  // Poisson iterations and solves
 };
 
 static int grow(Ctx *c, double **p, size_t n) {
@@ -96,8 +101,7 @@ static int ensure_banks(Ctx *c) {
       if ((rc = grow(c, &A.pu[b][q], N))) return rc;
     if ((rc = grow(c, &A.plane[b], 3 * (size_t)c->g.mx * c->g.my))) return rc;
   }
-  for (int s = 0; s < kMaxSlots; s++)
-    if ((rc = grow(c, &A.tmp[s], N))) return rc;
+  if ((rc = grow(c, &A.xcat, kMaxSlots * N + 32))) return rc;
   for (int d = 0; d < 3; d++) {
     for (int q = 0; q < 6; q++) {
       if ((rc = grow(c, &A.lface[d][q], N))) return rc;
@@ -109,8 +113,8 @@ static int ensure_banks(Ctx *c) {
 }
 
 static void free_op(LinOp &o) {
-  cudaFree(o.cp); cudaFree(o.ri); cudaFree(o.cvl);
-  o.cp = o.ri = nullptr; o.cvl = nullptr; o.nnz = 0;
+  cudaFree(o.off); cudaFree(o.col); cudaFree(o.val);
+  o.off = nullptr; o.col = nullptr; o.val = nullptr; o.nnz = 0; o.nslice = 0;
 }
 
 static void free_tapes(Adjoint &A) {
@@ -132,7 +136,7 @@ void adjoint_free(Ctx *c) {
     for (int q = 0; q < 3; q++) cudaFree(A.pu[b][q]);
     cudaFree(A.plane[b]);
   }
-  for (int s = 0; s < kMaxSlots; s++) cudaFree(A.tmp[s]);
+  cudaFree(A.xcat);
   for (int d = 0; d < 3; d++) {
     for (int q = 0; q < 6; q++) { cudaFree(A.lface[d][q]); cudaFree(A.tface[d][q]); }
     cudaFree(A.lfp[d]);
@@ -320,6 +324,61 @@ static int compress(Ctx *c, long long nnz, long long nrows, const int *a, const 
   return check_launch(c, "k_row_ptr");
 }
 
+// Width of each 32-row slice: its longest row, as 32 x width entries (rows past n: none).
+__global__ void k_slice_width(long long n, long long nslice, const int *__restrict__ ptr, long long *w) {
+  const long long sl = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (sl >= nslice) return;
+  int m = 0;
+  for (long long r = 32 * sl; r < 32 * sl + 32 && r < n; r++) m = max(m, ptr[r + 1] - ptr[r]);
+  w[sl] = 32LL * m;
+}
+
+__global__ void k_sell_fill(long long n, long long nslice, const int *__restrict__ ptr, const int *__restrict__ idx,
+                            const double *__restrict__ v, const long long *__restrict__ off, int pad, int *col,
+                            double *val) {
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= 32 * nslice) return;
+  const long long sl = r >> 5, l = r & 31;
+  const int w = (int)((off[sl + 1] - off[sl]) >> 5);
+  const int b = r < n ? ptr[r] : 0, len = r < n ? ptr[r + 1] - ptr[r] : 0;
+  for (int k = 0; k < w; k++) {
+    const long long e = off[sl] + 32LL * k + l;
+    col[e] = k < len ? idx[b + k] : pad;
+    val[e] = k < len ? v[b + k] : 0.0;
+  }
+}
+
+// The row-compressed transpose (ptr, idx, val over n rows) in sliced ELLPACK; pad: the
+// column that padding entries read (a zero).
+static int to_sell(Ctx *c, long long n, const int *ptr, const int *idx, const double *v, int pad, LinOp &op) {
+  const long long ns = (n + 31) / 32;
+  long long *w = nullptr;
+  void *tmp = nullptr;
+  size_t tb = 0;
+  bool ok = cudaMalloc(&w, sizeof(long long) * (ns + 1)) == cudaSuccess &&
+            cudaMalloc(&op.off, sizeof(long long) * (ns + 1)) == cudaSuccess;
+  if (ok) {
+    cudaMemsetAsync(w + ns, 0, sizeof(long long), c->stream);
+    c->launches++, k_slice_width<<<nblocks(ns, 256), 256, 0, c->stream>>>(n, ns, ptr, w);
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, w, op.off, (int)(ns + 1), c->stream);
+    ok = cudaMalloc(&tmp, tb) == cudaSuccess;
+    if (ok) cub::DeviceScan::ExclusiveSum(tmp, tb, w, op.off, (int)(ns + 1), c->stream);
+  }
+  long long total = 0;
+  if (ok) {
+    cudaMemcpyAsync(&total, op.off + ns, sizeof(long long), cudaMemcpyDeviceToHost, c->stream);
+    ok = cudaStreamSynchronize(c->stream) == cudaSuccess;
+  }
+  ok = ok && cudaMalloc(&op.col, sizeof(int) * (total + 1)) == cudaSuccess &&
+       cudaMalloc(&op.val, sizeof(double) * (total + 1)) == cudaSuccess;
+  if (ok) c->launches++, k_sell_fill<<<nblocks(32 * ns, 256), 256, 0, c->stream>>>(n, ns, ptr, idx, v, op.off, pad, op.col, op.val);
+  cudaStreamSynchronize(c->stream);
+  cudaFree(w); cudaFree(tmp);
+  if (!ok) return set_err(c, VFS_ERR_CUDA, "adjoint: operator conversion failed");
+  op.nslice = ns;
+  return check_launch(c, "k_sell_fill");
+}
+
 static double host_max(Ctx *c, const double *dev) {
   double hm[256];
   cudaMemcpyAsync(hm, dev, sizeof(hm), cudaMemcpyDeviceToHost, c->stream);
@@ -336,7 +395,7 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
   const ColourMap cm = colour_map(g, q);
   const size_t bytes = sizeof(double) * N;
   int rc;
-  if (n >= (1LL << 31)) return set_err(c, VFS_ERR_INVALID, "adjoint: operator too large for 32-bit indices");
+  if (kMaxSlots * N + 32 >= (1LL << 31)) return set_err(c, VFS_ERR_INVALID, "adjoint: grid too large for 32-bit indices");
   double *backup = nullptr, *y0 = nullptr, *y1 = nullptr, *amax = nullptr;
   int *rows = nullptr, *cols = nullptr, *conf = nullptr;
   double *vals = nullptr;
@@ -425,7 +484,11 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
     if (hn <= cap) {
       free_op(op);
       op.nnz = (long long)hn;
-      rc = compress(c, (long long)hn, n, cols, rows, vals, &op.cp, &op.ri, &op.cvl);
+      int *ptr = nullptr, *idx = nullptr;
+      double *val = nullptr;
+      rc = compress(c, (long long)hn, n, cols, rows, vals, &ptr, &idx, &val);
+      if (!rc) rc = to_sell(c, n, ptr, idx, val, (int)(kMaxSlots * N), op);
+      cudaFree(ptr); cudaFree(idx); cudaFree(val);
       if (!rc) op.fn = fn;
       cleanup();
       return rc;
@@ -436,22 +499,27 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
   return set_err(c, VFS_ERR_INVALID, "adjoint: probe entry count changed between passes");
 }
 
-// out[r] = sum over the entries of row r of val * x[idx]; slot-major vectors.
-__global__ void k_spmv(long long n, long long N, const int *__restrict__ ptr, const int *__restrict__ idx,
-                       const double *__restrict__ val, SlotPtrs x, SlotPtrs y) {
+// y[r] = sum over the entries of row r of val * x[col], x the slots end to end; one
+// thread per row, a warp per slice.
+__global__ void __launch_bounds__(256) k_spmv_sell(long long n, long long N, const long long *__restrict__ off,
+                                                   const int *__restrict__ col, const double *__restrict__ val,
+                                                   const double *__restrict__ x, SlotPtrs y) {
   const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (r >= n) return;
+  const long long sl = r >> 5;
+  const long long b = off[sl] + (r & 31), e = off[sl + 1];
   double s = 0;
-  for (int e = ptr[r]; e < ptr[r + 1]; e++) {
-    const int col = idx[e];
-    s += val[e] * x.p[col / N][col % N];
-  }
-  y.p[r / N][r % N] = s;
+  for (long long k = b; k < e; k += 32) s += val[k] * x[col[k]];
+  const unsigned q = (unsigned)(r / N);
+  double *dst = y.p[0];
+#pragma unroll
+  for (int t = 1; t < kMaxSlots; t++) dst = q == (unsigned)t ? y.p[t] : dst;  // no local copy of y
+  dst[r - q * N] = s;
 }
 
 // In place on bank b: slots <- L slots (transpose = 0: the operator's own kernels run on
 // the bank's arrays, swapped in for the context's fields) or L^T slots (transpose = 1: the
-// measured matrix by columns).
+// measured matrix).
 static int apply_op(Ctx *c, int o, int b, int transpose) {
   Adjoint &A = *c->adj;
   LinOp &op = A.op[o];
@@ -468,16 +536,13 @@ static int apply_op(Ctx *c, int o, int b, int transpose) {
     for (int s = 0; s < op.nslot; s++) c->f[op.slot[s].field][op.slot[s].comp] = keep[s];
     return rc;
   }
-  SlotPtrs x, y;
+  SlotPtrs y;
   for (int s = 0; s < op.nslot; s++) {
-    x.p[s] = A.bank[b][op.slot[s].field][op.slot[s].comp];
-    y.p[s] = A.tmp[s];
+    y.p[s] = A.bank[b][op.slot[s].field][op.slot[s].comp];
+    cudaMemcpyAsync(A.xcat + s * N, y.p[s], sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream);
   }
-  c->launches++, k_spmv<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, op.cp, op.ri, op.cvl, x, y);
-  if ((rc = check_launch(c, "k_spmv"))) return rc;
-  for (int s = 0; s < op.nslot; s++)
-    cudaMemcpyAsync(x.p[s], y.p[s], sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream);
-  return VFS_OK;
+  c->launches++, k_spmv_sell<<<nblocks(n, 256), 256, 0, c->stream>>>(n, N, op.off, op.col, op.val, A.xcat, y);
+  return check_launch(c, "k_spmv_sell");
 }
 
 // In place on the adjoint bank: slots <- L^T slots by the hand-written transpose where the
@@ -855,8 +920,10 @@ static int lin_solve_into(Ctx *c, double *rhs, double *sol, const vfs_solve_opts
   c->f[VFS_PHI][0] = sol;
   poisson_set_transpose(c, transpose);
   vfs_solve_stats st;
+  memset(&st, 0, sizeof(st));
   int rc = poisson_solve(c, &lo, &st);
   poisson_set_transpose(c, false);
+  if (transpose) c->adj->it_adj += st.iterations, c->adj->n_adj++;
   c->f[VFS_B][0] = fb;
   c->f[VFS_PHI][0] = fphi;
   c->ps.guess = guess;
@@ -1224,8 +1291,10 @@ static double *ckpt(Ctx *c, int n) { return c->adj->ckpt + (size_t)n * kCkptArra
 static int step_forward(Ctx *c, const vfs_adjoint_opts *o, StepTape *t) {
   c->tape = t;
   vfs_step_stats st;
+  memset(&st, 0, sizeof(st));
   int rc = step_core(c, &o->solve, &st);
   c->tape = nullptr;
+  c->adj->it_fwd += st.poisson.iterations, c->adj->n_fwd++;
   return rc == VFS_ERR_NOT_CONVERGED ? VFS_OK : rc;
 }
 
@@ -1295,6 +1364,7 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
   std::vector<HostState> hs(nseg);
   if (!A.t0) cudaEventCreate(&A.t0);
   if (!A.t1) cudaEventCreate(&A.t1);
+  A.it_fwd = A.n_fwd = A.it_adj = A.n_adj = 0;
   cudaEventRecord(A.t0, c->stream);
   for (int sg = 0; sg < nseg && !rc; sg++) {
     save_state(c, ckpt(c, sg), hs[sg]);
@@ -1346,6 +1416,8 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
     stats->recomputed_steps = recomputed;
     stats->checkpoints = nseg;
     stats->tape_bytes = (long long)A.tapes.size() * (24 + (c->g.immersed ? 3 : 0)) * (long long)sizeof(double) * c->g.N;
+    stats->poisson_iterations_forward = A.n_fwd ? (double)A.it_fwd / A.n_fwd : 0.0;
+    stats->poisson_iterations_adjoint = A.n_adj ? (double)A.it_adj / A.n_adj : 0.0;
   }
   return rc;
 }

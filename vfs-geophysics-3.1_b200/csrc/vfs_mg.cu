@@ -864,29 +864,47 @@ void mg_free(Poisson &P) {
 }
 
 // Per level: raw FP64 couplings and Thomas factors (op64, used to build the next level),
-// the packed FP64 and FP32 operators, and the work vectors x | b | xo | ds (2n).
+// the packed FP64 and FP32 operators, and the work vectors x | b | xo | ds (2n).  A rebuild
+// on the same grid (every first time step runs PoissonLHSNew) keeps the levels' buffers.
 int mg_setup(Ctx *c) {
   Poisson &P = c->ps;
   const Grid &g = c->g;
   int rc;
-  mg_free(P);
+  std::vector<MGLevel> old;
+  old.swap(P.lv);
   int nx = g.mx - 2, ny = g.my - 2, nz = g.mz - 2;
   const int maxlev = 12;
+  auto fail = [&](int code, const char *msg) {
+    for (size_t l = P.lv.size(); l < old.size(); l++) P.lv.push_back(old[l]);  // freed by mg_free
+    return set_err(c, code, msg);
+  };
   while ((int)P.lv.size() < maxlev) {
     MGLevel L;
     L.z = make_zl(nx, ny, nz, g);
     L.zebra = !((L.z.ip && (nx & 1)) || (L.z.kp && (nz & 1)));
     const long long n = L.z.n;
-    if (n >= (1LL << 31)) return set_err(c, VFS_ERR_INVALID, "poisson_lhs: grid too large for the multigrid indexing");
-    bool ok = cudaMalloc(&L.op64, sizeof(double) * NOP * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.pk64, sizeof(double) * 8 * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.pk32, sizeof(float) * 8 * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.v64, sizeof(double) * 5 * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.v32, sizeof(float) * 5 * n) == cudaSuccess;
-    ok &= cudaMalloc(&L.act, n) == cudaSuccess;
-    if (!ok) {
-      P.lv.push_back(L);
-      return set_err(c, VFS_ERR_CUDA, "poisson_lhs: multigrid allocation failed");
+    if (n >= (1LL << 31)) return fail(VFS_ERR_INVALID, "poisson_lhs: grid too large for the multigrid indexing");
+    const size_t l = P.lv.size();
+    if (l < old.size() && old[l].z.n == n && old[l].op64) {
+      L.op64 = old[l].op64; L.pk64 = old[l].pk64; L.pk32 = old[l].pk32;
+      L.v64 = old[l].v64; L.v32 = old[l].v32; L.act = old[l].act;
+      old[l].op64 = nullptr;  // taken
+    } else {
+      if (l < old.size()) {
+        MGLevel &O = old[l];
+        cudaFree(O.op64); cudaFree(O.pk64); cudaFree(O.pk32); cudaFree(O.v64); cudaFree(O.v32); cudaFree(O.act);
+        O.op64 = nullptr;
+      }
+      bool ok = cudaMalloc(&L.op64, sizeof(double) * NOP * n) == cudaSuccess;
+      ok &= cudaMalloc(&L.pk64, sizeof(double) * 8 * n) == cudaSuccess;
+      ok &= cudaMalloc(&L.pk32, sizeof(float) * 8 * n) == cudaSuccess;
+      ok &= cudaMalloc(&L.v64, sizeof(double) * 5 * n) == cudaSuccess;
+      ok &= cudaMalloc(&L.v32, sizeof(float) * 5 * n) == cudaSuccess;
+      ok &= cudaMalloc(&L.act, n) == cudaSuccess;
+      if (!ok) {
+        P.lv.push_back(L);
+        return fail(VFS_ERR_CUDA, "poisson_lhs: multigrid allocation failed");
+      }
     }
     cudaMemsetAsync(L.op64, 0, sizeof(double) * NOP * n, c->stream);
     cudaMemsetAsync(L.pk64, 0, sizeof(double) * 8 * n, c->stream);
@@ -900,7 +918,7 @@ int mg_setup(Ctx *c) {
       const MGLevel &F = P.lv.back();
       c->launches++, k_mg_coarse_couplings<<<nblocks(ncell, 128), 128, 0, c->stream>>>(F.z, L.z, F.op64, L.op64);
     }
-    if ((rc = check_launch(c, "k_mg_couplings"))) { P.lv.push_back(L); return rc; }
+    if ((rc = check_launch(c, "k_mg_couplings"))) { P.lv.push_back(L); return fail(rc, "poisson_lhs: multigrid set-up failed"); }
     c->launches++, k_mg_diag<<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64);
     c->launches++, k_mg_thomas<<<nblocks((long long)nx * nz, 64), 64, 0, c->stream>>>(L.z, L.op64);
     c->launches++, k_mg_active<<<nblocks(n, 256), 256, 0, c->stream>>>(n, L.op64, L.act);
@@ -909,9 +927,13 @@ int mg_setup(Ctx *c) {
     c->launches++, k_mg_pack<float><<<nblocks(ncell, 128), 128, 0, c->stream>>>(L.z, L.op64, (Q4<float> *)L.pk32,
                                                                 (Q4<float> *)L.pk32 + n);
     P.lv.push_back(L);
-    if ((rc = check_launch(c, "k_mg_setup"))) return rc;
+    if ((rc = check_launch(c, "k_mg_setup"))) return fail(rc, "poisson_lhs: multigrid set-up failed");
     if ((nx & 1) || (ny & 1) || (nz & 1) || nx < 4 || ny < 4 || nz < 4) break;
     nx /= 2; ny /= 2; nz /= 2;
+  }
+  for (size_t l = P.lv.size(); l < old.size(); l++) {  // levels the new hierarchy does not reach
+    MGLevel &O = old[l];
+    cudaFree(O.op64); cudaFree(O.pk64); cudaFree(O.pk32); cudaFree(O.v64); cudaFree(O.v32); cudaFree(O.act);
   }
   return VFS_OK;
 }

@@ -106,7 +106,8 @@ class AdjointStats(ctypes.Structure):
     _fields_ = [
         ("J", ctypes.c_double), ("ms_forward", ctypes.c_double), ("ms_adjoint", ctypes.c_double),
         ("recomputed_steps", ctypes.c_int), ("checkpoints", ctypes.c_int), ("tape_bytes", ctypes.c_longlong),
-        ("reserved", ctypes.c_double * 4),
+        ("poisson_iterations_forward", ctypes.c_double), ("poisson_iterations_adjoint", ctypes.c_double),
+        ("reserved", ctypes.c_double * 2),
     ]
 
 
