@@ -473,13 +473,14 @@ typedef struct {
   double reserved[2];
 } vfs_adjoint_stats;
 
-/* Measures the step's fixed linear operators (Contra2Cart, FormBCS tail, Pressure_Gradient,
- * VolumeFlux, Poisson right-hand side, UpdatePressure, Projection, IB_BC, IB-node
- * interpolation) as sparse matrices from the forward kernels: the adjoint applies the
- * transposes of the boundary operators by them, and the tests check the hand-written
- * transposes of the others against them; the tangent runs the kernels themselves.  Needs metrics and nvert (and
- * the IB-node list when immersed); a later change of nvert or of the grid needs a new
- * context.  The other adjoint entry points call it when needed. */
+/* Sets up the adjoint.  The step's fixed linear operators (Contra2Cart, FormBCS tail,
+ * Pressure_Gradient, VolumeFlux, Poisson right-hand side, UpdatePressure, Projection, IB_BC,
+ * IB-node interpolation) are transposed by hand-written kernels, except IB_BC and the
+ * IB-node interpolation of a grid with IB nodes: those two are measured here as sparse
+ * matrices from the forward kernels (the others only when a test hook asks for their
+ * matrices).  The tangent runs the kernels themselves.  Needs metrics and nvert (and the
+ * IB-node list when immersed); a later change of nvert or of the grid needs a new context.
+ * The other adjoint entry points call it when needed. */
 int vfs_adjoint_setup(vfs_ctx *ctx);
 /* J after opts->nsteps steps from the current state. */
 int vfs_objective(vfs_ctx *ctx, const vfs_adjoint_opts *opts, double *J);
@@ -488,15 +489,13 @@ int vfs_objective(vfs_ctx *ctx, const vfs_adjoint_opts *opts, double *J);
 int vfs_tangent(vfs_ctx *ctx, const vfs_adjoint_opts *opts, const double *dir, double *J, double *dJ);
 /* dJ/dcontrol by the adjoint steps, recomputing each checkpoint segment forward. */
 int vfs_adjoint_gradient(vfs_ctx *ctx, const vfs_adjoint_opts *opts, double *grad, vfs_adjoint_stats *stats);
-/* Test hooks: the slots (field, component pairs) and entry count of measured operator op
- * (0 Contra2Cart, 1 FormBCS tail, 2 Pressure_Gradient, 3 VolumeFlux, 4 Poisson RHS, 5
- * UpdatePressure, 6 Projection, 7 IB_BC, 8 IB-node interpolation); for vectors x and y
- * (slot-major, N per slot), L x by the operator's kernels and L^T y by the transpose the
- * adjoint sweep applies (the dot-product test <y, L x> = <L^T y, x>): hand-written kernels
- * for Pressure_Gradient, VolumeFlux without IB nodes, the Poisson right-hand side,
- * UpdatePressure and Projection, the measured matrix for the others; and L^T y by the
- * measured matrix alone (vfs_adjoint_op_measured), against which the hand-written
- * transposes are checked. */
+/* Test hooks: the slots (field, component pairs) and entry count (0 until measured) of
+ * operator op (0 Contra2Cart, 1 FormBCS tail, 2 Pressure_Gradient, 3 VolumeFlux, 4 Poisson
+ * RHS, 5 UpdatePressure, 6 Projection, 7 IB_BC, 8 IB-node interpolation); for vectors x and
+ * y (slot-major, N per slot), L x by the operator's kernels and L^T y by the transpose the
+ * adjoint sweep applies (the dot-product test <y, L x> = <L^T y, x>); and L^T y by the
+ * operator's measured matrix (vfs_adjoint_op_measured, measured on first use), against
+ * which the hand-written transposes are checked. */
 int vfs_adjoint_op_info(vfs_ctx *ctx, int op, int *nslot, int *fields, long long *nnz);
 int vfs_adjoint_op_check(vfs_ctx *ctx, int op, const double *x, const double *y, double *Lx, double *LTy);
 int vfs_adjoint_op_measured(vfs_ctx *ctx, int op, const double *y, double *LTy);

@@ -105,7 +105,6 @@ static int ensure_banks(Ctx *c) {
   for (int d = 0; d < 3; d++) {
     for (int q = 0; q < 6; q++) {
       if ((rc = grow(c, &A.lface[d][q], N))) return rc;
-      if ((rc = grow(c, &A.tface[d][q], N))) return rc;
     }
     if ((rc = grow(c, &A.lfp[d], N))) return rc;
   }
@@ -421,12 +420,18 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
   }
   for (int s = 0; s < op.nslot; s++)
     cudaMemcpyAsync(backup + s * N, live.p[s], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  // room for 8 entries per output when that fits in 30 % of the free memory; else a
+  // counting pass first and then the exact count
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
   unsigned long long cap = (unsigned long long)(8 * n);
+  if ((double)cap * (2 * sizeof(int) + sizeof(double)) > 0.3 * (double)free_b) cap = 0;
   for (int pass = 0; pass < 2; pass++) {
     cudaFree(rows); cudaFree(cols); cudaFree(vals);
     rows = cols = nullptr; vals = nullptr;
-    if (cudaMalloc(&rows, sizeof(int) * cap) != cudaSuccess || cudaMalloc(&cols, sizeof(int) * cap) != cudaSuccess ||
-        cudaMalloc(&vals, sizeof(double) * cap) != cudaSuccess) {
+    const size_t ncap = cap > 0 ? cap : 1;
+    if (cudaMalloc(&rows, sizeof(int) * ncap) != cudaSuccess || cudaMalloc(&cols, sizeof(int) * ncap) != cudaSuccess ||
+        cudaMalloc(&vals, sizeof(double) * ncap) != cudaSuccess) {
       cleanup();
       return set_err(c, VFS_ERR_CUDA, "adjoint: probe entry allocation failed");
     }
@@ -487,6 +492,8 @@ static int probe(Ctx *c, const char *name, LinOp &op, int q, const std::function
       int *ptr = nullptr, *idx = nullptr;
       double *val = nullptr;
       rc = compress(c, (long long)hn, n, cols, rows, vals, &ptr, &idx, &val);
+      cudaFree(rows); cudaFree(cols); cudaFree(vals);  // before the sliced copy is allocated
+      rows = cols = nullptr; vals = nullptr;
       if (!rc) rc = to_sell(c, n, ptr, idx, val, (int)(kMaxSlots * N), op);
       cudaFree(ptr); cudaFree(idx); cudaFree(val);
       if (!rc) op.fn = fn;
@@ -551,23 +558,34 @@ static int apply_op(Ctx *c, int o, int b, int transpose) {
 // transpose), else (or with measured) by the measured matrix.
 static bool handwritten(const Ctx *c, int o) {
   switch (o) {
-    case OP_PG: case OP_PRL: case OP_UP: case OP_PJ: return true;
-    case OP_VF: return !c->g.immersed;
+    case OP_PG: case OP_PRL: case OP_UP: return true;
+    case OP_C2C: case OP_FBT: case OP_PJ: return contra2cart_linear(c->g);
+    case OP_VF: case OP_IBBC: return !c->g.immersed;
     default: return false;
   }
 }
 
+static int ensure_measured(Ctx *c, int o);
+
 static int adjoint_apply(Ctx *c, int o, bool measured = false) {
-  if (measured || !handwritten(c, o)) return apply_op(c, o, ADJ, 1);
   int rc;
-  V3 lU = bank3(c, ADJ, VFS_UCONT);
+  if (measured || !handwritten(c, o)) {
+    if ((rc = ensure_measured(c, o))) return rc;
+    return apply_op(c, o, ADJ, 1);
+  }
+  const long long N = c->g.N;
+  V3 lU = bank3(c, ADJ, VFS_UCONT), lu = bank3(c, ADJ, VFS_UCAT), luo = bank3(c, ADJ, VFS_UCAT_O);
+  V3 tmp{c->adj->xcat, c->adj->xcat + N, c->adj->xcat + 2 * N};
   double *lP = bankp(c, ADJ, VFS_P, 0), *lphi = bankp(c, ADJ, VFS_PHI, 0);
   switch (o) {
+    case OP_C2C: return contra2cart_adjoint(c, lU, lu, luo, tmp);
+    case OP_FBT: return form_bcs_tail_adjoint(c, lU, lu, luo, tmp);
+    case OP_IBBC: return ib_bc_adjoint(c, lU);
     case OP_PG: return pressure_gradient_adjoint(c, lP, bank3(c, ADJ, VFS_DP));
     case OP_PRL: return poisson_rhs_local_adjoint(c, lU, bankp(c, ADJ, VFS_B, 0));
     case OP_UP: return update_pressure_adjoint(c, lP, lphi);
     case OP_PJ:
-      if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;  // Projection closes with Contra2Cart
+      if ((rc = contra2cart_adjoint(c, lU, lu, luo, tmp))) return rc;  // Projection closes with Contra2Cart
       return projection_adjoint(c, lphi, lU);
     case OP_VF: return apply_op(c, OP_VF, ADJ, 0);
     default: return set_err(c, VFS_ERR_INVALID, "adjoint: no hand-written transpose");
@@ -591,6 +609,18 @@ static int check_supported(Ctx *c) {
   return VFS_OK;
 }
 
+static const char *const kOpName[OP_N] = {"Contra2Cart", "the FormBCS tail", "Pressure_Gradient", "VolumeFlux",
+                                          "the Poisson right-hand side", "UpdatePressure", "Projection", "IB_BC",
+                                          "the IB-node interpolation"};
+
+// The measured matrix of operator o (probed once).
+static int ensure_measured(Ctx *c, int o) {
+  LinOp &op = c->adj->op[o];
+  if (op.off) return VFS_OK;
+  if (!op.nslot) return set_err(c, VFS_ERR_INVALID, "adjoint: no such operator here");
+  return probe(c, kOpName[o], op, o == OP_IBM ? 7 : 5, op.fn);
+}
+
 // Measures the operators of the step (once per grid, nvert and boundary set).
 static int adjoint_setup(Ctx *c) {
   int rc;
@@ -602,28 +632,32 @@ static int adjoint_setup(Ctx *c) {
   if (!c->ps.built && (rc = poisson_lhs(c))) return rc;
   if ((rc = calc_inlet_area(c))) return rc;
   const bool imm = c->g.immersed != 0;
+  // every operator's slots and forward function (the tangent runs them); the matrices of
+  // those the sweep transposes by measured matrix now, the others on first request
   set_slots(A.op[OP_C2C], {VFS_UCONT, VFS_UCAT, VFS_UCAT_O});
-  if ((rc = probe(c, "Contra2Cart", A.op[OP_C2C], 5, [](Ctx *x) { return contra2cart(x); }))) return rc;
+  A.op[OP_C2C].fn = [](Ctx *x) { return contra2cart(x); };
   set_slots(A.op[OP_FBT], {VFS_UCONT, VFS_UCAT, VFS_UCAT_O});
-  if ((rc = probe(c, "the FormBCS tail", A.op[OP_FBT], 5, [](Ctx *x) { return form_bcs_tail(x); }))) return rc;
+  A.op[OP_FBT].fn = [](Ctx *x) { return form_bcs_tail(x); };
   set_slots(A.op[OP_PG], {VFS_P, VFS_DP});
-  if ((rc = probe(c, "Pressure_Gradient", A.op[OP_PG], 5, [](Ctx *x) { return pressure_gradient_mode(x, 0, 0.0); }))) return rc;
+  A.op[OP_PG].fn = [](Ctx *x) { return pressure_gradient_mode(x, 0, 0.0); };
   if (!imm) {
     set_slots(A.op[OP_VF], {VFS_UCONT});
-    if ((rc = probe(c, "VolumeFlux", A.op[OP_VF], 5, [](Ctx *x) { return volume_flux(x); }))) return rc;
+    A.op[OP_VF].fn = [](Ctx *x) { return volume_flux(x); };
   }
   set_slots(A.op[OP_PRL], {VFS_UCONT, VFS_B});
-  if ((rc = probe(c, "the Poisson right-hand side", A.op[OP_PRL], 5, [](Ctx *x) { return poisson_rhs_local(x); }))) return rc;
+  A.op[OP_PRL].fn = [](Ctx *x) { return poisson_rhs_local(x); };
   set_slots(A.op[OP_UP], {VFS_PHI, VFS_P});
-  if ((rc = probe(c, "UpdatePressure", A.op[OP_UP], 5, [](Ctx *x) { return update_pressure(x); }))) return rc;
+  A.op[OP_UP].fn = [](Ctx *x) { return update_pressure(x); };
   set_slots(A.op[OP_PJ], {VFS_PHI, VFS_UCONT, VFS_UCAT, VFS_UCAT_O});
-  if ((rc = probe(c, "Projection", A.op[OP_PJ], 5, [](Ctx *x) { return projection(x); }))) return rc;
+  A.op[OP_PJ].fn = [](Ctx *x) { return projection(x); };
   set_slots(A.op[OP_IBBC], {VFS_UCONT, VFS_UCAT});
-  if ((rc = probe(c, "IB_BC", A.op[OP_IBBC], 5, [](Ctx *x) { return ib_bc(x); }))) return rc;
+  A.op[OP_IBBC].fn = [](Ctx *x) { return ib_bc(x); };
   if (imm) {
     set_slots(A.op[OP_IBM], {VFS_UCAT, VFS_P, VFS_UCONT, VFS_UCAT_O});
-    if ((rc = probe(c, "the IB-node interpolation", A.op[OP_IBM], 7, [](Ctx *x) { return ibm_interpolation(x); }))) return rc;
+    A.op[OP_IBM].fn = [](Ctx *x) { return ibm_interpolation(x); };
   }
+  for (int o = 0; o < OP_N; o++)
+    if (A.op[o].nslot && !handwritten(c, o) && (rc = ensure_measured(c, o))) return rc;
   // dP.z per unit flux deficit of the k-periodic forcing: Pressure_Gradient with P = 0
   if (c->g.kper && pressure_forcing_mode(c) == 2) {
     const size_t bytes = sizeof(double) * c->g.N;
@@ -988,6 +1022,9 @@ static int tangent_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
   Adjoint &A = *c->adj;
   const Grid &g = c->g;
   int rc;
+  for (int d = 0; d < 3; d++)  // the tangent's face fluxes (only the tangent uses them)
+    for (int q = 0; q < 6; q++)
+      if ((rc = grow(c, &A.tface[d][q], g.N))) return rc;
   const bool imm = g.immersed != 0;
   V3 dU = bank3(c, TAN, VFS_UCONT), du = bank3(c, TAN, VFS_UCAT), ddp = bank3(c, TAN, VFS_DP);
   V3 dpu{A.pu[TAN][0], A.pu[TAN][1], A.pu[TAN][2]};
@@ -1060,9 +1097,9 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
   V3 lpu{A.pu[ADJ][0], A.pu[ADJ][1], A.pu[ADJ][2]};
   const size_t bytes = sizeof(double) * g.N;
   if ((rc = move_add3(c, A.bank[ADJ][VFS_UCAT], A.bank[ADJ][VFS_UCAT_O]))) return rc;  // Ucat_o = Ucat
-  if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;
-  if ((rc = apply_op(c, OP_IBBC, ADJ, 1))) return rc;
-  if (imm && (rc = apply_op(c, OP_IBM, ADJ, 1))) return rc;
+  if ((rc = adjoint_apply(c, OP_C2C))) return rc;
+  if ((rc = adjoint_apply(c, OP_IBBC))) return rc;
+  if (imm && (rc = adjoint_apply(c, OP_IBM))) return rc;
   if ((rc = adjoint_apply(c, OP_PJ))) return rc;
   if ((rc = adjoint_apply(c, OP_UP))) return rc;
   if ((rc = solve_lin(c, ADJ, o))) return rc;
@@ -1075,7 +1112,7 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
     return rc;
   }
   // RungeKutta, last to first
-  if ((rc = apply_op(c, OP_FBT, ADJ, 1))) return rc;
+  if ((rc = adjoint_apply(c, OP_FBT))) return rc;
   double lfin = 0;
   if (g.bc[5] == 4) {
     double sa = 0, area = 0;
@@ -1086,14 +1123,14 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
   }
   for (int s = 3; s >= 0; s--) {
     const double a = kAlfa[s] * g.dt * g.st;
-    if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;
+    if ((rc = adjoint_apply(c, OP_C2C))) return rc;
     if ((rc = ff2_stage_adjoint(c, t.uc[s], t.uk[s], a, lU, lu, ldp, lpu, A.lface, A.lfp))) return rc;
-    if (s == 0 && (rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;
+    if (s == 0 && (rc = adjoint_apply(c, OP_C2C))) return rc;
   }
   if ((rc = move_add3(c, A.bank[ADJ][VFS_UCONT], A.pu[ADJ]))) return rc;  // pUcont = Ucont
-  if (imm && (rc = apply_op(c, OP_IBM, ADJ, 1))) return rc;
-  if ((rc = apply_op(c, OP_FBT, ADJ, 1))) return rc;
-  if ((rc = apply_op(c, OP_C2C, ADJ, 1))) return rc;
+  if (imm && (rc = adjoint_apply(c, OP_IBM))) return rc;
+  if ((rc = adjoint_apply(c, OP_FBT))) return rc;
+  if ((rc = adjoint_apply(c, OP_C2C))) return rc;
   if (inlet100(c)) {
     const long long npl = (long long)(g.mx - 2) * (g.my - 2);
     if (c->scal[VFS_S_INLET_FLUX] > 0) {
@@ -1117,25 +1154,31 @@ static int adjoint_step(Ctx *c, const StepTape &t, const vfs_solve_opts *o) {
   }
   if ((rc = adjoint_apply(c, OP_PG))) return rc;  // clears ldP
   if (t.first_step) {
-    if ((rc = apply_op(c, OP_IBBC, ADJ, 1))) return rc;
-    if (imm && (rc = apply_op(c, OP_IBM, ADJ, 1))) return rc;
+    if ((rc = adjoint_apply(c, OP_IBBC))) return rc;
+    if (imm && (rc = adjoint_apply(c, OP_IBM))) return rc;
   }
   return VFS_OK;
 }
 
 // ---------------------------------------------------------------- state and objective
-// Phi is part of the state: the next Poisson solve starts from it.
-static const int kCkptFields[6] = {VFS_UCONT, VFS_UCAT, VFS_P, VFS_UCAT_O, VFS_UCONT_O, VFS_PHI};
-static const int kCkptArrays = 14;
+// Phi is part of the state: the next Poisson solve starts from it.  A checkpoint taken
+// between two steps holds Ucont, Ucat, P and Phi (8 arrays): each step ends by copying Ucont
+// and Ucat into Ucont_o and Ucat_o, which the load restores the same way.  The first
+// checkpoint, of a state set by the caller, also holds Ucat_o and Ucont_o (14 arrays).
+static const int kCkptFields[6] = {VFS_UCONT, VFS_UCAT, VFS_P, VFS_PHI, VFS_UCAT_O, VFS_UCONT_O};
+static const int kCkptArrays = 14, kCkptShort = 8;
 
-struct HostState { bool first_step = false, guess = false; int ti = 0; double scal[VFS_NSCALARS] = {}; };
+struct HostState { bool first_step = false, guess = false, full = true; int ti = 0; double scal[VFS_NSCALARS] = {}; };
 
-static void save_state(Ctx *c, double *dst, HostState &h) {
+static void save_state(Ctx *c, double *dst, HostState &h, bool full) {
   const size_t bytes = sizeof(double) * c->g.N;
   int a = 0;
-  for (int f : kCkptFields)
+  for (int f : kCkptFields) {
+    if (!full && (f == VFS_UCAT_O || f == VFS_UCONT_O)) continue;
     for (int q = 0; q < c->dof[f]; q++, a++)
       cudaMemcpyAsync(dst + (size_t)a * c->g.N, c->f[f][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  }
+  h.full = full;
   h.first_step = c->first_step;
   h.guess = c->ps.guess;
   h.ti = c->ti;
@@ -1144,9 +1187,16 @@ static void save_state(Ctx *c, double *dst, HostState &h) {
 static void load_state(Ctx *c, const double *src, const HostState &h) {
   const size_t bytes = sizeof(double) * c->g.N;
   int a = 0;
-  for (int f : kCkptFields)
+  for (int f : kCkptFields) {
+    if (!h.full && (f == VFS_UCAT_O || f == VFS_UCONT_O)) continue;
     for (int q = 0; q < c->dof[f]; q++, a++)
       cudaMemcpyAsync(c->f[f][q], src + (size_t)a * c->g.N, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  }
+  if (!h.full)
+    for (int q = 0; q < 3; q++) {
+      cudaMemcpyAsync(c->f[VFS_UCAT_O][q], c->f[VFS_UCAT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+      cudaMemcpyAsync(c->f[VFS_UCONT_O][q], c->f[VFS_UCONT][q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    }
   c->first_step = h.first_step;
   c->ps.guess = h.guess;
   c->ti = h.ti;
@@ -1279,14 +1329,16 @@ static int prepare(Ctx *c, const vfs_adjoint_opts *o) {
     cudaFree(A.ckpt);
     A.ckpt = nullptr;
     A.nckpt = 0;
-    if (cudaMalloc(&A.ckpt, sizeof(double) * kCkptArrays * (size_t)c->g.N * nck) != cudaSuccess)
+    if (cudaMalloc(&A.ckpt, sizeof(double) * (kCkptArrays + (size_t)kCkptShort * (nck - 1)) * c->g.N) != cudaSuccess)
       return set_err(c, VFS_ERR_CUDA, "adjoint: checkpoint allocation failed");
     A.nckpt = nck;
   }
   return VFS_OK;
 }
 
-static double *ckpt(Ctx *c, int n) { return c->adj->ckpt + (size_t)n * kCkptArrays * c->g.N; }
+static double *ckpt(Ctx *c, int n) {
+  return c->adj->ckpt + (n == 0 ? 0 : kCkptArrays + (size_t)kCkptShort * (n - 1)) * c->g.N;
+}
 
 static int step_forward(Ctx *c, const vfs_adjoint_opts *o, StepTape *t) {
   c->tape = t;
@@ -1302,7 +1354,7 @@ static int objective_run(Ctx *c, const vfs_adjoint_opts *o, double *J) {
   int rc;
   if ((rc = prepare(c, o))) return rc;
   HostState h0;
-  save_state(c, ckpt(c, 0), h0);
+  save_state(c, ckpt(c, 0), h0, true);
   for (int s = 0; s < o->nsteps && !rc; s++) rc = step_forward(c, o, nullptr);
   if (!rc) rc = objective(c, o->objective, false, J);
   load_state(c, ckpt(c, 0), h0);
@@ -1316,7 +1368,7 @@ static int tangent_run(Ctx *c, const vfs_adjoint_opts *o, const double *dir, dou
   if ((rc = ensure_tapes(c, 1))) return rc;
   Adjoint &A = *c->adj;
   HostState h0;
-  save_state(c, ckpt(c, 0), h0);
+  save_state(c, ckpt(c, 0), h0, true);
   zero_bank(c, TAN);
   zero_bank(c, ADJ);
   const size_t nc = control_size(c, o->control);
@@ -1367,7 +1419,7 @@ static int gradient_run(Ctx *c, const vfs_adjoint_opts *o, double *grad, vfs_adj
   A.it_fwd = A.n_fwd = A.it_adj = A.n_adj = 0;
   cudaEventRecord(A.t0, c->stream);
   for (int sg = 0; sg < nseg && !rc; sg++) {
-    save_state(c, ckpt(c, sg), hs[sg]);
+    save_state(c, ckpt(c, sg), hs[sg], sg == 0);
     for (int s = 0; s < std::min(every, n - sg * every) && !rc; s++) rc = step_forward(c, o, nullptr);
   }
   double J = 0;

@@ -151,10 +151,12 @@ __device__ __forceinline__ bool pghost(int v, int m, int per) { return per && (v
 // Transpose of the periodic copy (k_periodic_copy: every point with a periodic ghost
 // coordinate takes the value at its image wrapped in all three directions): each point
 // with no periodic ghost coordinate adds the adjoints of the ghosts that copy it.
-// comp < 0: the ghosts of any periodic direction (the scalar and 3-component copies);
-// comp = q: only ghosts along direction q (k_periodic_copy_comp, component q).  The
-// ghosts are cleared by k_pcopy_clear afterwards.
-__global__ void k_pcopy_gather(Grid g, int comp, double *a) {
+// comp < 0: the ghosts of any periodic direction (the scalar and 3-component copies, for
+// each of a[0..na-1]); comp = 3: component q of a 3-component field copies only across
+// direction q (k_periodic_copy_comp).  The ghosts are cleared by k_pcopy_clear afterwards.
+struct Arrays3 { double *a[3]; };
+
+__global__ void k_pcopy_gather(Grid g, int comp, int na, Arrays3 a) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   const Box b = box_of(g);
@@ -164,27 +166,32 @@ __global__ void k_pcopy_gather(Grid g, int comp, double *a) {
   int oi[3], oj[3], ok[3];
   const int ni = images(c[0], b.m[0], b.per[0], oi), nj = images(c[1], b.m[1], b.per[1], oj),
             nk = images(c[2], b.m[2], b.per[2], ok);
-  double acc = 0;
+  if (ni == 1 && nj == 1 && nk == 1) return;
+  double acc[3] = {0.0, 0.0, 0.0};
   for (int zk = 0; zk < nk; zk++)
     for (int yj = 0; yj < nj; yj++)
       for (int xi = 0; xi < ni; xi++) {
         if (xi == 0 && yj == 0 && zk == 0) continue;
-        if (comp == 0 && xi == 0) continue;  // component q copies only across its own direction
-        if (comp == 1 && yj == 0) continue;
-        if (comp == 2 && zk == 0) continue;
-        acc += a[lidx(g, oi[xi], oj[yj], ok[zk])];
+        const long long q = lidx(g, oi[xi], oj[yj], ok[zk]);
+        for (int t = 0; t < na; t++) {
+          // component t of a component-wise copy moves only across direction t
+          if (comp == 3 && (t == 0 ? xi : (t == 1 ? yj : zk)) == 0) continue;
+          acc[t] += a.a[t][q];
+        }
       }
-  if (acc != 0.0) a[p] += acc;
+  for (int t = 0; t < na; t++)
+    if (acc[t] != 0.0) a.a[t][p] += acc[t];
 }
 
-__global__ void k_pcopy_clear(Grid g, int comp, double *a) {
+__global__ void k_pcopy_clear(Grid g, int comp, int na, Arrays3 a) {
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   int c[3];
   dijk(g, p, c[0], c[1], c[2]);
-  const bool ti = pghost(c[0], g.mx, g.iper), tj = pghost(c[1], g.my, g.jper), tk = pghost(c[2], g.mz, g.kper);
-  const bool tgt = comp < 0 ? (ti || tj || tk) : (comp == 0 ? ti : (comp == 1 ? tj : tk));
-  if (tgt) a[p] = 0.0;
+  const bool t3[3] = {pghost(c[0], g.mx, g.iper), pghost(c[1], g.my, g.jper), pghost(c[2], g.mz, g.kper)};
+  const bool any = t3[0] || t3[1] || t3[2];
+  for (int t = 0; t < na; t++)
+    if (comp == 3 ? t3[t] : any) a.a[t][p] = 0.0;
 }
 
 // UpdatePressure's transpose: P += Phi on interior fluid cells, P = 0 on interior cells
@@ -229,28 +236,21 @@ __global__ void k_poisson_rhs_adjoint(Grid g, const uint8_t *__restrict__ fluid,
 
 static bool any_periodic(const Grid &g) { return g.iper || g.jper || g.kper; }
 
-// In place: a <- C^T a for the periodic copy C of a scalar (comp = -1) or of component q.
-static int pcopy_adjoint(Ctx *c, int comp, double *a) {
+// In place: the transpose of the periodic copy of na arrays (comp -1) or of the
+// component-wise copy of a 3-component field (comp 3).
+static int pcopy_adjoint(Ctx *c, int comp, int na, Arrays3 a) {
   int rc;
   const Grid &g = c->g;
-  c->launches++, k_pcopy_gather<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, comp, a);
+  if (!any_periodic(g)) return VFS_OK;
+  c->launches++, k_pcopy_gather<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, comp, na, a);
   if ((rc = check_launch(c, "k_pcopy_gather"))) return rc;
-  c->launches++, k_pcopy_clear<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, comp, a);
+  c->launches++, k_pcopy_clear<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, comp, na, a);
   return check_launch(c, "k_pcopy_clear");
 }
 
-int periodic_copy1_adjoint(Ctx *c, double *a) {
-  if (!any_periodic(c->g)) return VFS_OK;
-  return pcopy_adjoint(c, -1, a);
-}
+int periodic_copy1_adjoint(Ctx *c, double *a) { return pcopy_adjoint(c, -1, 1, Arrays3{{a, nullptr, nullptr}}); }
 
-int periodic_copy3_adjoint(Ctx *c, V3 a) {
-  int rc;
-  if (!any_periodic(c->g)) return VFS_OK;
-  if ((rc = pcopy_adjoint(c, -1, a.x))) return rc;
-  if ((rc = pcopy_adjoint(c, -1, a.y))) return rc;
-  return pcopy_adjoint(c, -1, a.z);
-}
+int periodic_copy3_adjoint(Ctx *c, V3 a) { return pcopy_adjoint(c, -1, 3, Arrays3{{a.x, a.y, a.z}}); }
 
 // Pressure_Gradient (no forcing term), slots (P, dP) -> (P', dP'), P' = C P, dP' = S P':
 // lP <- C^T (lP + S^T ldP), ldP <- 0.
@@ -275,11 +275,7 @@ int projection_adjoint(Ctx *c, double *lphi, V3 luc) {
   int rc;
   const Grid &g = c->g;
   if ((rc = ensure_gab(c))) return rc;
-  if (any_periodic(g)) {
-    if ((rc = pcopy_adjoint(c, 0, luc.x))) return rc;
-    if ((rc = pcopy_adjoint(c, 1, luc.y))) return rc;
-    if ((rc = pcopy_adjoint(c, 2, luc.z))) return rc;
-  }
+  if ((rc = pcopy_adjoint(c, 3, 3, Arrays3{{luc.x, luc.y, luc.z}}))) return rc;
   c->launches++, k_face_grad_adjoint<1><<<nblocks(g.N, 256), 256, 0, c->stream>>>(
       g, c->gab, c->f[VFS_IAJ][0], c->f[VFS_JAJ][0], c->f[VFS_KAJ][0], c->nv, cv(luc), -(g.dt * g.st), lphi);
   return check_launch(c, "k_face_grad_adjoint");

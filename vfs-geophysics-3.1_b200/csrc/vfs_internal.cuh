@@ -298,6 +298,11 @@ int pressure_gradient_adjoint(Ctx *c, double *lP, V3 ldp);
 int projection_adjoint(Ctx *c, double *lphi, V3 luc);
 int update_pressure_adjoint(Ctx *c, double *lP, double *lphi);
 int poisson_rhs_local_adjoint(Ctx *c, V3 luc, double *lb);
+// hand-written transposes of the boundary operators (vfs_momentum.cu)
+bool contra2cart_linear(const Grid &g);
+int contra2cart_adjoint(Ctx *c, V3 luc, V3 lucat, V3 luo, V3 tmp);
+int form_bcs_tail_adjoint(Ctx *c, V3 luc, V3 lucat, V3 luo, V3 tmp);
+int ib_bc_adjoint(Ctx *c, V3 luc);
 
 // tangent / adjoint support (vfs_adjoint.cu)
 int tape_stage(Ctx *c, int stage);

@@ -153,9 +153,17 @@ __device__ void covariant(const double g[3][3], double G[3][3]) {
   G[2][0] = (a32 * a21 - a31 * a22) / det, G[2][1] = -(a32 * a11 - a31 * a12) / det, G[2][2] = (a22 * a11 - a21 * a12) / det;
 }
 
+// Reader of a 3-component field for the boundary rules (the transposed kernel evaluates
+// them with unit-vector readers instead, ProbeAcc).
+struct FieldAcc {
+  CV3 a;
+  __device__ __forceinline__ double operator()(long long q, int c) const { return c == 0 ? a.x[q] : (c == 1 ? a.y[q] : a.z[q]); }
+};
+
 // Slip-wall ghost: mirror the neighbour's old velocity about the wall normal taken from
 // the covariant metric column `col` of the neighbour cell (rhs.c:384-478).
-__device__ void slip_ghost(long long nb, int col, double sgn, Metrics m, CV3 uo, double *o) {
+template <class UO>
+__device__ void slip_ghost(long long nb, int col, double sgn, const Metrics &m, const UO &uo, double *o) {
   double g[3][3], G[3][3];
   g[0][0] = m.csi.x[nb], g[0][1] = m.csi.y[nb], g[0][2] = m.csi.z[nb];
   g[1][0] = m.eta.x[nb], g[1][1] = m.eta.y[nb], g[1][2] = m.eta.z[nb];
@@ -165,39 +173,41 @@ __device__ void slip_ghost(long long nb, int col, double sgn, Metrics m, CV3 uo,
   if (sgn < 0) nx = -nx, ny = -ny, nz = -nz;
   double sum = sqrt(nx * nx + ny * ny + nz * nz);
   nx /= sum, ny /= sum, nz /= sum;
-  double un = uo.x[nb] * nx + uo.y[nb] * ny + uo.z[nb] * nz;
-  o[0] = uo.x[nb] - 2 * un * nx;
-  o[1] = uo.y[nb] - 2 * un * ny;
-  o[2] = uo.z[nb] - 2 * un * nz;
+  double un = uo(nb, 0) * nx + uo(nb, 1) * ny + uo(nb, 2) * nz;
+  o[0] = uo(nb, 0) - 2 * un * nx;
+  o[1] = uo(nb, 1) - 2 * un * ny;
+  o[2] = uo(nb, 2) - 2 * un * nz;
 }
 
 // Boundary part of Contra2Cart_2 (rhs.c:291-675), phase 1: every point the reference's
 // boundary loop assigns gets its new value in `out` (reads the pre-loop snapshot `ucat`),
 // `flag` marks it.  Phase 2 (k_bc_commit) copies the marked values, which reproduces the
 // reference's read-from-lUcat / write-to-Ucat semantics exactly.
-__device__ __forceinline__ void contra2cart_bc_point(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv,
-                                                     CV3 lu, CV3 uo, V3 out, uint8_t *flag, long long p, int i,
-                                                     int j, int k) {
+// The rule at point p as a function of the readers lu (the snapshot) and uo (Ucat_o):
+// whether it assigns p, and the value v.
+template <class LU, class UO>
+__device__ __forceinline__ bool contra2cart_bc_rule(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv,
+                                                    const LU &lu, const UO &uo, long long p, int i, int j, int k,
+                                                    double v[3]) {
   const int mx = g.mx, my = g.my, mz = g.mz;
   const long long sx = 1, sy = mx, sz = (long long)mx * my;
   const int *bc = g.bc;
   bool w = false;
   if (nv[p] == 3) {  // (int)(nvert+0.1)==3 and fixed bodies (rhs.c:296-299)
-    out.x[p] = 0; out.y[p] = 0; out.z[p] = 0;
-    flag[p] = 1;
-    return;
+    v[0] = 0; v[1] = 0; v[2] = 0;
+    return true;
   }
   // every rule below acts on a ghost point or on a cell (1 or mx-2, 1, k)
   if (!(i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == mz - 1 ||
         (j == 1 && (i == 1 || i == mx - 2))))
-    return;
-  double v[3] = {lu.x[p], lu.y[p], lu.z[p]};
+    return false;
+  v[0] = lu(p, 0); v[1] = lu(p, 1); v[2] = lu(p, 2);
   int solid_flag = 0;
   if (bc[3] == 13 && j == my - 1) {
-    v[0] = lu.x[p - sy]; v[2] = lu.z[p - sy]; v[1] = -lu.y[p - sy]; w = true;
+    v[0] = lu(p - sy, 0); v[2] = lu(p - sy, 2); v[1] = -lu(p - sy, 1); w = true;
   }
   if (bc[3] == 14 && j == my - 1) {
-    v[0] = lu.x[p - sy]; v[1] = lu.y[p - sy]; v[2] = -lu.z[p - sy]; w = true;
+    v[0] = lu(p - sy, 0); v[1] = lu(p - sy, 1); v[2] = -lu(p - sy, 2); w = true;
   }
   if (bc[0] == 10 && i == 0 && (j != 0 && k != 0)) {
     slip_ghost(p + sx, 0, -1.0, m, uo, v); w = true;
@@ -221,39 +231,39 @@ __device__ __forceinline__ void contra2cart_bc_point(const Grid &g, const Metric
   }
   // no-slip ghosts (rhs.c:511-534)
   if (i == 0 && bc[0] == 1 && (j != 0 && k != 0)) {
-    v[0] = -1 * lu.x[p + sx]; v[1] = -1 * lu.y[p + sx]; v[2] = -1 * lu.z[p + sx]; w = true; solid_flag = 1;
+    v[0] = -1 * lu(p + sx, 0); v[1] = -1 * lu(p + sx, 1); v[2] = -1 * lu(p + sx, 2); w = true; solid_flag = 1;
   }
   if (i == mx - 1 && bc[1] == 1 && (j != 0 && k != 0)) {
-    v[0] = -1 * lu.x[p - sx]; v[1] = -1 * lu.y[p - sx]; v[2] = -1 * lu.z[p - sx]; w = true; solid_flag = 1;
+    v[0] = -1 * lu(p - sx, 0); v[1] = -1 * lu(p - sx, 1); v[2] = -1 * lu(p - sx, 2); w = true; solid_flag = 1;
   }
   if (j == 0 && bc[2] == 1 && (i != 0 && k != 0)) {
-    v[0] = -1 * lu.x[p + sy]; v[1] = -1 * lu.y[p + sy]; v[2] = -1 * lu.z[p + sy]; w = true; solid_flag = 1;
+    v[0] = -1 * lu(p + sy, 0); v[1] = -1 * lu(p + sy, 1); v[2] = -1 * lu(p + sy, 2); w = true; solid_flag = 1;
   }
   if (j == my - 1 && bc[3] == 1 && (i != 0 && k != 0)) {
-    v[0] = -1 * lu.x[p - sy]; v[1] = -1 * lu.y[p - sy]; v[2] = -1 * lu.z[p - sy]; w = true; solid_flag = 1;
+    v[0] = -1 * lu(p - sy, 0); v[1] = -1 * lu(p - sy, 1); v[2] = -1 * lu(p - sy, 2); w = true; solid_flag = 1;
   }
   if (k == 0 && bc[4] == 1 && (i != 0 && j != 0)) {
-    v[0] = -1 * lu.x[p + sz]; v[1] = -1 * lu.y[p + sz]; v[2] = -1 * lu.z[p + sz]; w = true; solid_flag = 1;
+    v[0] = -1 * lu(p + sz, 0); v[1] = -1 * lu(p + sz, 1); v[2] = -1 * lu(p + sz, 2); w = true; solid_flag = 1;
   }
   if (k == mz - 1 && bc[5] == 1 && (i != 0 && j != 0)) {
-    v[0] = -1 * lu.x[p - sz]; v[1] = -1 * lu.y[p - sz]; v[2] = -1 * lu.z[p - sz]; w = true; solid_flag = 1;
+    v[0] = -1 * lu(p - sz, 0); v[1] = -1 * lu(p - sz, 1); v[2] = -1 * lu(p - sz, 2); w = true; solid_flag = 1;
   }
   if (j == my - 1 && bc[3] == 2) {
-    if (solid_flag) { v[0] = 2.0 - uo.x[p - sy]; v[1] = -uo.y[p - sy]; v[2] = -uo.z[p - sy]; }
-    else { v[0] = 2.0 - lu.x[p - sy]; v[1] = -lu.y[p - sy]; v[2] = -lu.z[p - sy]; }
+    if (solid_flag) { v[0] = 2.0 - uo(p - sy, 0); v[1] = -uo(p - sy, 1); v[2] = -uo(p - sy, 2); }
+    else { v[0] = 2.0 - lu(p - sy, 0); v[1] = -lu(p - sy, 1); v[2] = -lu(p - sy, 2); }
     w = true;
   }
   if (j == 0 && bc[2] == 12) {
-    v[0] = -lu.x[p + sy]; v[1] = -lu.y[p + sy]; v[2] = 2.0 - lu.z[p + sy]; w = true;
+    v[0] = -lu(p + sy, 0); v[1] = -lu(p + sy, 1); v[2] = 2.0 - lu(p + sy, 2); w = true;
     if (solid_flag) v[0] = v[1] = v[2] = 0;
   }
   if (j == my - 1 && bc[3] == 12) {
-    v[0] = -lu.x[p - sy]; v[1] = -lu.y[p - sy]; v[2] = 2.0 - lu.z[p - sy]; w = true;
+    v[0] = -lu(p - sy, 0); v[1] = -lu(p - sy, 1); v[2] = 2.0 - lu(p - sy, 2); w = true;
     if (solid_flag) v[0] = v[1] = v[2] = 0;
   }
   // outflow (rhs.c:573-597)
   if (bc[3] == 4 && j == my - 1 && (i != 0 && i != mx - 1 && k != 0 && k != mz - 1)) {
-    v[0] = lu.x[p - sy]; v[1] = lu.y[p - sy]; v[2] = lu.z[p - sy]; w = true;
+    v[0] = lu(p - sy, 0); v[1] = lu(p - sy, 1); v[2] = lu(p - sy, 2); w = true;
   }
   if (bc[5] == 4 && k == mz - 1 && (i != 0 && i != mx - 1 && j != 0 && j != my - 1)) {
     if (nv[p - sz] != 0) { v[0] = v[1] = v[2] = 0; w = true; }
@@ -264,7 +274,14 @@ __device__ __forceinline__ void contra2cart_bc_point(const Grid &g, const Metric
     if (bc[0] <= 1 && bc[2] <= 1 && (i == 1 && j == 1)) { v[0] = v[1] = v[2] = 0; w = true; }
     if (bc[1] <= 1 && bc[2] <= 1 && (i == mx - 2 && j == 1)) { v[0] = v[1] = v[2] = 0; w = true; }
   }
-  if (w) {
+  return w;
+}
+
+__device__ __forceinline__ void contra2cart_bc_point(const Grid &g, const Metrics &m, const uint8_t *__restrict__ nv,
+                                                     CV3 lu, CV3 uo, V3 out, uint8_t *flag, long long p, int i,
+                                                     int j, int k) {
+  double v[3];
+  if (contra2cart_bc_rule(g, m, nv, FieldAcc{lu}, FieldAcc{uo}, p, i, j, k, v)) {
     out.x[p] = v[0]; out.y[p] = v[1]; out.z[p] = v[2];
     flag[p] = 1;
   }
@@ -433,6 +450,158 @@ int contra2cart_div(Ctx *c, bool with_divergence) {
   if (ns > 0) c->launches++, k_bc_clear_list<<<nblocks(ns, 256), 256, 0, c->stream>>>(ns, c->solid, fl);
   if ((rc = check_launch(c, "k_bc_commit"))) return rc;
   return periodic_copy3(c, ucat);
+}
+
+// ------------------------------------------------------------------ Contra2Cart transpose
+// The adjoint of contra2cart (Ucont, Ucat, Ucat_o -> the same slots), as gathers:
+//   Ucont' = C Ucont; Ucat1 = I(Ucont') on the interior fluid cells; Ucat2 = C Ucat1;
+//   Ucat3 = B(Ucat2, Ucat_o) on the points the boundary phase assigns; Ucat' = C Ucat3
+// (C the periodic ghost copy, I the Cramer's-rule interior, B the boundary rules).  B's
+// coefficients come from the rules themselves, evaluated at unit vectors.
+
+// Points the boundary phase visits (edge_point): the ghost planes and (1 or mx-2, 1, k).
+__device__ __forceinline__ bool c2c_edge(const Grid &g, int i, int j, int k) {
+  return i == 0 || i == g.mx - 1 || j == 0 || j == g.my - 1 || k == 0 || k == g.mz - 1 ||
+         (j == 1 && (i == 1 || i == g.mx - 2));
+}
+
+// Reader for the coefficient evaluations: component c of point q is 1, all else 0 (q < 0:
+// the zero vector).
+struct ProbeAcc {
+  long long q;
+  int c;
+  __device__ __forceinline__ double operator()(long long r, int cc) const { return (r == q && cc == c) ? 1.0 : 0.0; }
+};
+
+// Points within one step of a point the boundary phase visits (the only ones B^T changes).
+__device__ __forceinline__ bool c2c_near(const Grid &g, int i, int j, int k) {
+  return i <= 2 || i >= g.mx - 3 || j <= 2 || j >= g.my - 2 || k <= 1 || k >= g.mz - 2;
+}
+
+// B^T, first half, at the points near the boundary: l2 = l3 off the assigned points (0 on
+// them) plus, over the assigned neighbours p (p = q or one step away: every rule reads
+// there), dB_p/dUcat2[q]^T l3[p]; lo (the Ucat_o adjoint) += dB_p/dUcat_o[q]^T l3[p].
+// The coefficients are the rule's value at unit vectors (evaluation e = 1..3: Ucat2
+// component e-1 of q; 4..6: Ucat_o component e-4; 0: whether p is assigned).  l2 is a
+// scratch copy (the next kernel moves it into l3), so that no thread reads an entry
+// another has already replaced.
+__global__ void k_c2c_bc_adjoint(Grid g, Metrics m, const uint8_t *__restrict__ nv, CV3 l3, V3 l2, V3 lo) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= g.N) return;
+  int i, j, k;
+  dijk(g, q, i, j, k);
+  const bool solid = nv[q] == 3 && !g.moving;  // k_solid_zero
+  if (!c2c_near(g, i, j, k) && !solid) return;
+  bool assigned = solid;
+  double a[3] = {0.0, 0.0, 0.0}, o[3] = {0.0, 0.0, 0.0};
+  if (c2c_near(g, i, j, k)) {
+#pragma unroll 1
+    for (int n = 0; n < 7; n++) {
+      int x[3] = {i, j, k};
+      if (n > 0) x[(n - 1) >> 1] += (n & 1) ? 1 : -1;
+      if (x[0] < 0 || x[0] >= g.mx || x[1] < 0 || x[1] >= g.my || x[2] < 0 || x[2] >= g.mz) continue;
+      if (!c2c_edge(g, x[0], x[1], x[2])) continue;
+      const long long p = lidx(g, x[0], x[1], x[2]);
+      if (nv[p] == 3) {  // assigned zero
+        if (n == 0) assigned = true;
+        continue;
+      }
+      const double l[3] = {l3.x[p], l3.y[p], l3.z[p]};
+#pragma unroll 1
+      for (int e = 0; e < 7; e++) {
+        const ProbeAcc A{(e >= 1 && e <= 3) ? q : -1, e - 1}, B{e >= 4 ? q : -1, e - 4};
+        double v[3];
+        const bool w = contra2cart_bc_rule(g, m, nv, A, B, p, x[0], x[1], x[2], v);
+        if (e == 0) {
+          if (!w) break;
+          if (n == 0) assigned = true;
+          if (l[0] == 0.0 && l[1] == 0.0 && l[2] == 0.0) break;
+          continue;
+        }
+        const double t = v[0] * l[0] + v[1] * l[1] + v[2] * l[2];
+        if (e <= 3) a[e - 1] += t;
+        else o[e - 4] += t;
+      }
+    }
+  }
+  if (!assigned) { a[0] += l3.x[q]; a[1] += l3.y[q]; a[2] += l3.z[q]; }
+  l2.x[q] = a[0]; l2.y[q] = a[1]; l2.z[q] = a[2];
+  if (o[0] != 0.0 || o[1] != 0.0 || o[2] != 0.0) { lo.x[q] += o[0]; lo.y[q] += o[1]; lo.z[q] += o[2]; }
+}
+
+// B^T, second half: the points the first half wrote take their new adjoints.
+__global__ void k_c2c_bc_adjoint_commit(Grid g, const uint8_t *__restrict__ nv, CV3 l2, V3 l3) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= g.N) return;
+  int i, j, k;
+  dijk(g, q, i, j, k);
+  if (!c2c_near(g, i, j, k) && !(nv[q] == 3 && !g.moving)) return;
+  l3.x[q] = l2.x[q]; l3.y[q] = l2.y[q]; l3.z[q] = l2.z[q];
+}
+
+// I^T, per cell: w_d = 0.5 * sum_c K[c][d] / det * lu_c on the cells the interior kernel
+// computes (K the cofactors of Cramer's rule: ucat_c = sum_d K[c][d] q_d / det, q_d the
+// average of the two d-faces), 0 elsewhere; those cells' lu are consumed (the forward
+// overwrites them).
+__global__ void k_c2c_interior_adjoint(Grid g, CV3 csi, CV3 eta, CV3 zet, const uint8_t *__restrict__ nv, V3 lu,
+                                       V3 w) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  int i, j, k;
+  dijk(g, p, i, j, k);
+  if (i < 1 || i > g.mx - 2 || j < 1 || j > g.my - 2 || k < 1 || k > g.mz - 2 || nv[p] != 0) {
+    w.x[p] = 0; w.y[p] = 0; w.z[p] = 0;
+    return;
+  }
+  const double m00 = csi.x[p], m01 = csi.y[p], m02 = csi.z[p];
+  const double m10 = eta.x[p], m11 = eta.y[p], m12 = eta.z[p];
+  const double m20 = zet.x[p], m21 = zet.y[p], m22 = zet.z[p];
+  const double det = m00 * (m11 * m22 - m12 * m21) - m01 * (m10 * m22 - m12 * m20) +
+                     m02 * (m10 * m21 - m11 * m20);
+  const double l0 = lu.x[p], l1 = lu.y[p], l2 = lu.z[p];
+  w.x[p] = 0.5 * ((m11 * m22 - m12 * m21) * l0 - (m10 * m22 - m12 * m20) * l1 + (m10 * m21 - m11 * m20) * l2) / det;
+  w.y[p] = 0.5 * (-(m01 * m22 - m02 * m21) * l0 + (m00 * m22 - m02 * m20) * l1 - (m00 * m21 - m01 * m20) * l2) / det;
+  w.z[p] = 0.5 * ((m01 * m12 - m02 * m11) * l0 - (m00 * m12 - m02 * m10) * l1 + (m00 * m11 - m01 * m10) * l2) / det;
+  lu.x[p] = 0; lu.y[p] = 0; lu.z[p] = 0;
+}
+
+// I^T, per face: the d-face f between cells f and f + d gathers both cells' w_d.
+__global__ void k_c2c_face_gather(Grid g, CV3 w, V3 luc) {
+  const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= g.N) return;
+  int i, j, k;
+  dijk(g, f, i, j, k);
+  const long long sy = g.mx, sz = (long long)g.mx * g.my;
+  const double ax = w.x[f] + (i + 1 < g.mx ? w.x[f + 1] : 0.0);
+  const double ay = w.y[f] + (j + 1 < g.my ? w.y[f + sy] : 0.0);
+  const double az = w.z[f] + (k + 1 < g.mz ? w.z[f + sz] : 0.0);
+  if (ax != 0.0) luc.x[f] += ax;
+  if (ay != 0.0) luc.y[f] += ay;
+  if (az != 0.0) luc.z[f] += az;
+}
+
+// Affine boundary rules (a constant 2.0 in the ghost value) have no transpose of this form.
+bool contra2cart_linear(const Grid &g) { return !(g.bc[3] == 2 || g.bc[2] == 12 || g.bc[3] == 12); }
+
+// In place: (luc, lucat, luo) <- the transpose of contra2cart applied to them; tmp: three
+// scratch arrays of N.
+int contra2cart_adjoint(Ctx *c, V3 luc, V3 lucat, V3 luo, V3 tmp) {
+  const Grid &g = c->g;
+  int rc;
+  if (!contra2cart_linear(g)) return set_err(c, VFS_ERR_INVALID, "contra2cart_adjoint: affine boundary rule");
+  Metrics m = metrics(c);
+  if ((rc = periodic_copy3_adjoint(c, lucat))) return rc;
+  c->launches++, k_c2c_bc_adjoint<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m, c->nv, cv(lucat), tmp, luo);
+  if ((rc = check_launch(c, "k_c2c_bc_adjoint"))) return rc;
+  c->launches++, k_c2c_bc_adjoint_commit<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, c->nv, cv(tmp), lucat);
+  if ((rc = check_launch(c, "k_c2c_bc_adjoint_commit"))) return rc;
+  if ((rc = periodic_copy3_adjoint(c, lucat))) return rc;
+  c->launches++, k_c2c_interior_adjoint<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, m.csi, m.eta, m.zet, c->nv,
+                                                                                  lucat, tmp);
+  if ((rc = check_launch(c, "k_c2c_interior_adjoint"))) return rc;
+  c->launches++, k_c2c_face_gather<<<nblocks(g.N, 256), 256, 0, c->stream>>>(g, cv(tmp), luc);
+  if ((rc = check_launch(c, "k_c2c_face_gather"))) return rc;
+  return periodic_copy3_adjoint(c, luc);
 }
 
 // ------------------------------------------------------------------ Formfunction_2
@@ -1640,6 +1809,53 @@ int ib_bc(Ctx *c) {
   return VFS_OK;
 }
 
+// Transpose of k_periodic_normal: each source face adds the adjoint of the ghost face
+// that copies it (i = 0 <- mx-2, mx-1 <- 1, per normal component); the ghosts are cleared.
+__global__ void k_periodic_normal_adjoint(Grid g, V3 uc) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const int mx = g.mx, my = g.my, mz = g.mz;
+  int i, j, k;
+  dijk(g, p, i, j, k);
+  const long long sy = mx, sz = (long long)mx * my;
+  if (g.iper) {
+    if (i == mx - 2) uc.x[p] += uc.x[p - (mx - 2)];
+    if (i == 1) uc.x[p] += uc.x[p + (mx - 2)];
+  }
+  if (g.jper) {
+    if (j == my - 2) uc.y[p] += uc.y[p - (long long)(my - 2) * sy];
+    if (j == 1) uc.y[p] += uc.y[p + (long long)(my - 2) * sy];
+  }
+  if (g.kper) {
+    if (k == mz - 2) uc.z[p] += uc.z[p - (long long)(mz - 2) * sz];
+    if (k == 1) uc.z[p] += uc.z[p + (long long)(mz - 2) * sz];
+  }
+}
+__global__ void k_periodic_normal_clear(Grid g, V3 uc) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  int i, j, k;
+  dijk(g, p, i, j, k);
+  if (g.iper && (i == 0 || i == g.mx - 1)) uc.x[p] = 0;
+  if (g.jper && (j == 0 || j == g.my - 1)) uc.y[p] = 0;
+  if (g.kper && (k == 0 || k == g.mz - 1)) uc.z[p] = 0;
+}
+
+// Transpose of ib_bc without IB nodes: k_periodic_normal, then the 0/1 diagonal
+// k_ib_bc_faces (its own transpose).
+int ib_bc_adjoint(Ctx *c, V3 luc) {
+  int rc;
+  if (c->g.immersed) return set_err(c, VFS_ERR_INVALID, "ib_bc_adjoint: IB nodes need the measured operator");
+  if (c->g.iper || c->g.jper || c->g.kper) {
+    c->launches++, k_periodic_normal_adjoint<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, luc);
+    if ((rc = check_launch(c, "k_periodic_normal_adjoint"))) return rc;
+    c->launches++, k_periodic_normal_clear<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, luc);
+    if ((rc = check_launch(c, "k_periodic_normal_clear"))) return rc;
+  }
+  c->launches++, k_ib_bc_faces<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, luc);
+  return check_launch(c, "k_ib_bc_faces");
+}
+
 // ------------------------------------------------------------------ InflowFlux
 // bcs.c:329-706 for an inlet on the k = 0 face (bctype[4] = 5), interior (i, j):
 //   inletprofile 2     uniform uin = inlet_flux/inletArea (1 when inlet_flux < 0);
@@ -1867,6 +2083,17 @@ int form_bcs_tail(Ctx *c) {
   if ((rc = contra2cart(c))) return rc;
   c->launches++, k_zero_edges<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, field3(c, VFS_UCAT));
   return check_launch(c, "k_zero_edges");
+}
+
+// Transpose of form_bcs_tail: k_wall_flux and k_zero_edges zero entries (0/1 diagonals,
+// their own transposes) around Contra2Cart.
+int form_bcs_tail_adjoint(Ctx *c, V3 luc, V3 lucat, V3 luo, V3 tmp) {
+  int rc;
+  c->launches++, k_zero_edges<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, lucat);
+  if ((rc = check_launch(c, "k_zero_edges"))) return rc;
+  if ((rc = contra2cart_adjoint(c, luc, lucat, luo, tmp))) return rc;
+  c->launches++, k_wall_flux<<<nblocks(c->g.N, 256), 256, 0, c->stream>>>(c->g, luc);
+  return check_launch(c, "k_wall_flux");
 }
 
 int form_bcs(Ctx *c, bool outflow_scale) {

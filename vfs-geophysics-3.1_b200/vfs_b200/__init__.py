@@ -115,9 +115,10 @@ OBJ_KINETIC_ENERGY, OBJ_PRESSURE_DRAG, OBJ_DRAG = 0, 1, 2
 CTRL_INITIAL_UCONT, CTRL_INFLOW_PLANE = 0, 1
 OP_NAMES = ["contra2cart", "form_bcs_tail", "pressure_gradient", "volume_flux", "poisson_rhs",
             "update_pressure", "projection", "ib_bc", "ibm_interpolation"]
-# operators whose adjoint is a hand-written kernel (VolumeFlux only without IB nodes, where
-# it is a 0/1 diagonal); the others are applied by their measured matrices
-OP_HANDWRITTEN = ["pressure_gradient", "volume_flux", "poisson_rhs", "update_pressure", "projection"]
+# operators whose adjoint is a hand-written kernel (VolumeFlux and IB_BC only without IB
+# nodes); IB_BC and the IB-node interpolation with IB nodes are applied by measured matrices
+OP_HANDWRITTEN = ["contra2cart", "form_bcs_tail", "pressure_gradient", "volume_flux", "poisson_rhs",
+                  "update_pressure", "projection", "ib_bc"]
 
 EXPORTS = [
     "vfs_create", "vfs_destroy", "vfs_last_error", "vfs_dims", "vfs_synchronize",
