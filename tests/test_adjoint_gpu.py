@@ -151,17 +151,21 @@ def test_handwritten_transposes_match_measured(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("periodic", ["ik", "ijk", "none"])
+@pytest.mark.parametrize("periodic", ["ik", "ijk", "none", "slip"])
 def test_handwritten_transposes_random_nvert(periodic):
-    """Every branch of the stencils: nvert drawn from {0, 1, 2, 3} on a wavy grid (one-sided
-    cross differences next to IB nodes and solids, Projection's j-face nvert sum 5), with
-    periodic directions i and k, all three, or none (walls all round)."""
+    """Every branch of the stencils and boundary rules: nvert drawn from {0, 1, 2, 3} on a
+    wavy grid (one-sided cross differences next to IB nodes and solids, Projection's j-face
+    nvert sum 5), with periodic directions i and k, all three, or none (walls all round), or
+    none with slip walls on both i faces and on top (their ghosts mirror Ucat_o), a no-slip
+    bottom and k- wall, and an outflow face at k+."""
     case = cases.channel(10, 9, 12, wavy=0.1)
     case.i_periodic = int("i" in periodic)
     case.j_periodic = int("j" in periodic)
     case.k_periodic = int("k" in periodic)
     case.bctype = [7 if case.i_periodic else 1] * 2 + [7 if case.j_periodic else 1] * 2 + \
                   [7 if case.k_periodic else 1] * 2
+    if periodic == "slip":
+        case.bctype = [10, 10, 1, 10, 1, 4]
     rng = np.random.Generator(np.random.Philox(23))
     nv = np.zeros(case.da_shape)
     nv[1:-1, 1:-1, 1:-1] = rng.choice([0, 0, 0, 0, 1, 2, 3], size=nv[1:-1, 1:-1, 1:-1].shape)
