@@ -629,6 +629,60 @@ def large_window(torch, nx=384, ny=256, nz=384, steps=50, every=7):
     return out
 
 
+# FP64 instructions per cell of one dynamic-Smagorinsky evaluation (Compute_Smagorinsky_
+# Constant_1 + Compute_eddy_viscosity_LES) on the 128 x 96 x 128 wavy channel, counted by
+# ncu (2 x DFMA + DMUL + DADD, executed thread instructions, every kernel of the call; the
+# division and square-root sequences count by their instructions):
+# profiles/les_dynamic_smagorinsky_128x96x128.md.
+LES_FLOPS_PER_CELL = 5373
+FP64_PEAK_TFLOPS = 37.0   # nominal B200 FP64 (vector), no measured figure in MEASURED_PEAKS.json
+
+
+def les_context(nx=128, ny=96, nz=128):
+    """Config 2's grid (128 x 96 x 128 channel, wavy bottom y_w = 0.1 sin cos) with the
+    dynamic Smagorinsky model (les = 2) and a seeded turbulent-like field."""
+    import vfs_b200 as vfs
+    from vfs_b200 import cases
+    case = cases.channel(nx, ny, nz, wavy=0.1)
+    case.les = 2
+    ctx = vfs.Context(case.config())
+    ctx.form_metrics(case.X, case.Y, case.Z)
+    ctx.set_field(vfs.NVERT, case.nvert)
+    m = {n: ctx.get_field(f) for n, f in vfs.METRIC_FIELDS.items()}
+    u = cases.initial_ucat(case, seed=0)
+    ctx.set_field(vfs.UCONT, cases.ucont_from_ucat(case, u, m))
+    ctx.set_field(vfs.UCAT, u)
+    ctx.set_field(vfs.UCAT_O, u)
+    ctx.contra2cart()
+    ctx.set_scalar(vfs.S_TI, 5)   # Cs is 0 in the first two steps of a fresh run (les.c:69-72)
+    return ctx, nx * ny * nz
+
+
+def les_probe(torch, reps=20):
+    """Time of one dynamic-Smagorinsky evaluation (the Cs field with its averaging and
+    clipping, then nu_t) on config 2's grid, and its FP64 rate against the nominal peak."""
+    ctx, cells = les_context()
+    for _ in range(3):
+        ctx.smagorinsky_constant()
+        ctx.eddy_viscosity()
+
+    def body():
+        ctx.smagorinsky_constant()
+        ctx.eddy_viscosity()
+    ms, _ = timed(ctx, body, reps, torch)
+    ctx.close()
+    ms /= reps
+    out = {"workload": "dynamic Smagorinsky (les = 2: Compute_Smagorinsky_Constant_1 + "
+                       "Compute_eddy_viscosity_LES) on the 128x96x128 wavy channel of config 2",
+           "ms_per_call": round(ms, 4), "cells": cells}
+    if LES_FLOPS_PER_CELL:
+        tf = LES_FLOPS_PER_CELL * cells / (ms * 1e-3) / 1e12
+        out.update({"fp64_flops_per_cell": LES_FLOPS_PER_CELL, "achieved_tflops": round(tf, 3),
+                    "peak_tflops": FP64_PEAK_TFLOPS, "peak_source": "nominal",
+                    "frac": round(tf / FP64_PEAK_TFLOPS, 4)})
+    return out
+
+
 def immersed_variant(nx, ny, nz, torch, steps=10):
     """The metric workload with the six cylinders as immersed bodies (immersed = 1): closed
     triangulated cylinder surfaces, classified by the IB search, with the IB-node
@@ -682,6 +736,9 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 384x256x384 50-step window")
     ap.add_argument("--adjoint-size", default="128,128,128")
     ap.add_argument("--adjoint-steps", type=int, default=20)
+    ap.add_argument("--profile-les", action="store_true",
+                    help="run one dynamic-Smagorinsky evaluation on config 2's grid inside "
+                         "cudaProfilerStart/Stop and exit (for ncu --profile-from-start off)")
     ap.add_argument("--profile-step", action="store_true",
                     help="after the warm-up, run one mixed step inside cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no JSON")
@@ -700,6 +757,20 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.profile_les:
+        lctx, _ = les_context()
+        for _ in range(3):
+            lctx.smagorinsky_constant()
+            lctx.eddy_viscosity()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        lctx.smagorinsky_constant()
+        lctx.eddy_viscosity()
+        lctx.synchronize()
+        torch.cuda.profiler.stop()
+        lctx.close()
+        return
 
     nx, ny, nz = (NX, NY, NZ) if not args.size else tuple(int(v) for v in args.size.split(","))
     case = make_case(nx, ny, nz)
@@ -842,6 +913,13 @@ def main():
         except Exception as e:  # reported, never fatal for the forward numbers
             imm = {"failed": str(e)}
 
+    les = None
+    if not args.size:
+        try:
+            les = les_probe(torch)
+        except Exception as e:  # reported, never fatal for the forward numbers
+            les = {"failed": str(e)}
+
     large = None
     if not args.no_large and not args.size:
         try:
@@ -917,6 +995,8 @@ def main():
             out["immersed_variant"] = imm
         if large is not None:
             out["large_window"] = large
+        if les is not None:
+            out["les"] = les
         if cpu is not None:
             out["cpu_baseline"] = cpu
         print(json.dumps(out))
