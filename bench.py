@@ -453,11 +453,9 @@ ADJ_WORKLOAD = ("wavy-wall channel %dx%dx%d cells (bottom y_w = 0.1 sin(2 pi x/L
                 "every %d steps")
 
 
-def adjoint_window(nx, ny, nz, steps, every, torch):
-    """The discrete adjoint of a window of FP64 steps on the curvilinear grid with the
-    sphere: gradient of the body's pressure force after `steps` steps with respect to the
-    inflow plane.  Returns the reverse sweep (segment recomputation + adjoint steps) and the
-    forward sweep timed on the device, and the one-off operator set-up time."""
+def adjoint_context(nx, ny, nz):
+    """The adjoint window's context: the curvilinear channel with the immersed sphere, an
+    inlet (inletprofile 100) and an outlet, a seeded initial field."""
     import vfs_b200 as vfs
     from vfs_b200 import cases
     case = cases.channel(nx, ny, nz, wavy=0.1)
@@ -477,6 +475,18 @@ def adjoint_window(nx, ny, nz, steps, every, torch):
     _, area = ctx.calc_inlet_area()
     ctx.set_scalar(vfs.S_INLET_FLUX, area)
     ctx.set_inflow_plane(cases.inflow_plane(case))
+    return ctx, case
+
+
+
+def adjoint_window(nx, ny, nz, steps, every, torch):
+    """The discrete adjoint of a window of FP64 steps on the curvilinear grid with the
+    sphere: gradient of the body's drag after `steps` steps with respect to the inflow
+    plane.  Returns the reverse sweep (segment recomputation + adjoint steps) and the
+    forward sweep timed on the device, and the one-off operator set-up time."""
+    import vfs_b200 as vfs
+    from vfs_b200 import cases
+    ctx, case = adjoint_context(nx, ny, nz)
     t0 = time.perf_counter()
     ctx.adjoint_setup()
     setup_s = time.perf_counter() - t0
@@ -736,6 +746,9 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 384x256x384 50-step window")
     ap.add_argument("--adjoint-size", default="128,128,128")
     ap.add_argument("--adjoint-steps", type=int, default=20)
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="run one 2-step adjoint gradient of the adjoint window (checkpoint every "
+                         "step) inside cudaProfilerStart/Stop and exit (for ncu --profile-from-start off)")
     ap.add_argument("--profile-les", action="store_true",
                     help="run one dynamic-Smagorinsky evaluation on config 2's grid inside "
                          "cudaProfilerStart/Stop and exit (for ncu --profile-from-start off)")
@@ -757,6 +770,19 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.profile_adjoint:
+        ax, ay, az = (int(v) for v in args.adjoint_size.split(","))
+        actx, _ = adjoint_context(ax, ay, az)
+        kw = dict(objective=vfs.OBJ_DRAG, control=vfs.CTRL_INFLOW_PLANE, precision=1, rtol=1e-10)
+        actx.adjoint_gradient(2, checkpoint_every=1, **kw)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        actx.adjoint_gradient(2, checkpoint_every=1, **kw)
+        actx.synchronize()
+        torch.cuda.profiler.stop()
+        actx.close()
+        return
 
     if args.profile_les:
         lctx, _ = les_context()
