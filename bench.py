@@ -11,8 +11,10 @@ inflow plane.  One step = Flow_Solver for implicit = 0: Calc_k_Flux, Pressure_Gr
 VolumeFlux, Poisson RHS, Poisson solve to rtol 1e-10, UpdatePressure, Projection,
 Divergence, IB_BC, Contra2Cart.
 
-`value` is the mixed-precision (FP32 V-cycle in FP64 FGMRES) step time in ms with every
-field resident in HBM; the all-FP64 form is timed on the same state for the comparison.
+`value` is the mixed-precision step time in ms with every field resident in HBM: FGMRES
+whose basis, preconditioned vectors and V-cycle are FP32, each restart cycle started from
+the FP64 residual (iterative refinement; `vfs_solve_opts.precision` 2).  The all-FP64 form
+and the form with only the V-cycle in FP32 (precision 0) are timed on the same state.
 `e2e` runs the same step through the C ABI with the flow state (Ucont, Ucat, P) copied
 from pinned host memory before and back after every step.
 
@@ -42,6 +44,10 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "vfs-geophysics-3.1_b200"))
 
 METRIC = "ms/step @256x192x256: mixed vs FP64 GPU at max|div u|<=1e-8; adjoint/forward ratio"
+# The mixed form of the metric: precision 2, the FP32 inner FGMRES (basis, preconditioned
+# vectors and V-cycle in FP32) in FP64 iterative refinement; precision 0 (only the V-cycle
+# in FP32) is timed beside it.
+MIXED = 2
 NX, NY, NZ = 256, 192, 256
 WORKLOAD = ("open channel 256x192x256 cells, 3x2 staggered cylinders D=0.2 spacing 4D as nvert "
             "blocked cells (immersed=0), no-slip bottom, free-slip top, periodic i, inlet k=0 "
@@ -340,7 +346,7 @@ def vs_reference_step(nx=64, ny=48, nz=64, nsteps=3):
             ref_p, ref_u, ref_uc = R.get("P"), R.get("Ucat"), R.get("lUcont")
             S.close()
         res = {"reference_max_div": host_max_div(ref_uc, m["aj"], nv)}
-        for prec, name in ((0, "mixed"), (1, "fp64")):
+        for prec, name in ((MIXED, "mixed"), (0, "mixed_fp32_vcycle"), (1, "fp64")):
             case = make_case(nx, ny, nz)
             ctx = vfs.Context(case.config())
             ctx.set_metrics(m)
@@ -407,8 +413,11 @@ def arm_config(world, nx=NX, ny=NY, nz=NZ, size=None):
     npts = (nx + 2) * (ny + 2) * (nz + 2)
     return {"workload": WORKLOAD if not size else "size override %s" % size,
             "cells": nx * ny * nz, "parallelism": "replicas" if world > 1 else "single-gpu",
-            "precision": "mixed: FP32 multigrid V-cycle (%d levels, zebra y-line Gauss-Seidel 3+3 "
-                         "sweeps, trilinear prolongation) in FP64 FGMRES(30)" % mg_levels(nx, ny, nz),
+            "precision": "mixed: FGMRES(30) with its basis, preconditioned vectors and operator products "
+                         "stored in FP32 (FP64 coefficients and sums), each restart cycle started from the FP64 "
+                         "residual and ended at a 1e-5 reduction (iterative refinement); FP32 multigrid "
+                         "V-cycle (%d levels, zebra y-line Gauss-Seidel 3+3 sweeps, trilinear prolongation)"
+                         % mg_levels(nx, ny, nz),
             "l2": "inputs larger than L2 (every field is a %d MB array)" % (npts * 8 // 2 ** 20)}
 
 
@@ -597,9 +606,10 @@ def large_window(torch, nx=384, ny=256, nz=384, steps=50, every=7):
     case = cases.inflow_outflow(cases.open_channel_cylinders(nx, ny, nz, wavy=0.05), 100)
     case.immersed = 0
     ctx, _ = setup_context(case)
+    ctx.step(precision=MIXED, rtol=1e-10)
     for _ in range(3):
-        ctx.step(precision=0, rtol=1e-10, graph=1)
-    ms, stats = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10, graph=1), steps, torch)
+        ctx.step(precision=MIXED, rtol=1e-10, graph=1)
+    ms, stats = timed(ctx, lambda: ctx.step(precision=MIXED, rtol=1e-10, graph=1), steps, torch)
     free1, _ = torch.cuda.mem_get_info()
     its = float(np.mean([s.poisson.iterations for s in stats]))
     ms_step = ms / steps
@@ -615,7 +625,7 @@ def large_window(torch, nx=384, ny=256, nz=384, steps=50, every=7):
            "note": "hbm_gbs = algorithmic bytes of the step (each input read once, each output written "
                    "once; STEP_BYTES) / step time"}
     # the adjoint of the window, from the state the forward window left
-    kw = dict(objective=vfs.OBJ_KINETIC_ENERGY, control=vfs.CTRL_INFLOW_PLANE, precision=0, rtol=1e-10)
+    kw = dict(objective=vfs.OBJ_KINETIC_ENERGY, control=vfs.CTRL_INFLOW_PLANE, precision=MIXED, rtol=1e-10)
     t0 = time.perf_counter()
     ctx.adjoint_setup()
     setup_s = time.perf_counter() - t0
@@ -720,9 +730,10 @@ def immersed_variant(nx, ny, nz, torch, steps=10):
     _, inlet_area = ctx.calc_inlet_area()
     ctx.set_scalar(vfs.S_INLET_FLUX, 1.0 * inlet_area)
     ctx.contra2cart()
+    ctx.step(precision=MIXED, rtol=1e-10)
     for _ in range(3):
-        ctx.step(precision=0, rtol=1e-10, graph=1)
-    ms, st = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10, graph=1), steps, torch)
+        ctx.step(precision=MIXED, rtol=1e-10, graph=1)
+    ms, st = timed(ctx, lambda: ctx.step(precision=MIXED, rtol=1e-10, graph=1), steps, torch)
     nib = int(ctx.ibm_list()[0].shape[0])
     ctx.close()
     return {"workload": "the metric workload with the 6 cylinders as immersed bodies (immersed=1): closed "
@@ -832,15 +843,18 @@ def main():
             ctx.set_field(f, v)
         ctx.set_scalar(vfs.S_TI, ti)
 
-    for _ in range(2):  # FP64 multigrid set-up and both step graphs, outside the timed steps
+    for _ in range(2):  # FP64 multigrid set-up and the step graphs, outside the timed steps
         ctx.step(precision=1, rtol=1e-10, graph=1)
-    restore()
-    ctx.step(precision=0, rtol=1e-10, graph=1)
+    for prec in (MIXED, 0):
+        restore()
+        ctx.step(precision=prec, rtol=1e-10)            # the form's workspace
+        restore()
+        ctx.step(precision=prec, rtol=1e-10, graph=1)   # its graph
     restore()
     sampler = ClockSampler(local)
     with sampler:
         barrier()
-        ms_mixed, stats = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10, graph=1), args.steps, torch)
+        ms_mixed, stats = timed(ctx, lambda: ctx.step(precision=MIXED, rtol=1e-10, graph=1), args.steps, torch)
         barrier()
         restore()
         barrier()
@@ -848,20 +862,27 @@ def main():
         barrier()
         restore()
         barrier()
-        ms_launched, _ = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10), args.steps, torch)
+        ms_vc, stats0 = timed(ctx, lambda: ctx.step(precision=0, rtol=1e-10, graph=1), args.steps, torch)
+        barrier()
+        restore()
+        barrier()
+        ms_launched, _ = timed(ctx, lambda: ctx.step(precision=MIXED, rtol=1e-10), args.steps, torch)
         barrier()
     ms_mixed /= args.steps
     ms_fp64 /= args.steps
+    ms_vc /= args.steps
     ms_launched /= args.steps
     maxdiv = max(s.max_div for s in stats)
     maxdiv64 = max(s.max_div for s in stats64)
+    maxdiv0 = max(s.max_div for s in stats0)
     its = float(np.mean([s.poisson.iterations for s in stats]))
     its64 = float(np.mean([s.poisson.iterations for s in stats64]))
+    its0 = float(np.mean([s.poisson.iterations for s in stats0]))
 
     # mixed against FP64 from one state: L2 and Linf of P and Ucat (both solves to rtol 1e-10,
     # both from the same Phi)
     outs = {}
-    for prec in (0, 1):
+    for prec in (MIXED, 0, 1):
         restore()
         st = ctx.step(precision=prec, rtol=1e-10)
         outs[prec] = (ctx.get_field(vfs.P), ctx.get_field(vfs.UCAT), st.max_div)
@@ -869,9 +890,11 @@ def main():
     def rel(a, b):
         return {"l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
                 "linf": float(np.abs(a - b).max() / np.abs(b).max())}
-    mixed_err = {"p": rel(outs[0][0], outs[1][0]), "u": rel(outs[0][1], outs[1][1]),
-                 "max_div": {"mixed": outs[0][2], "fp64": outs[1][2]},
-                 "note": "one step from the same state, mixed precision against the all-FP64 form"}
+    mixed_err = {"p": rel(outs[MIXED][0], outs[1][0]), "u": rel(outs[MIXED][1], outs[1][1]),
+                 "max_div": {"mixed": outs[MIXED][2], "fp64": outs[1][2]},
+                 "fp32_vcycle_form": {"p": rel(outs[0][0], outs[1][0]), "u": rel(outs[0][1], outs[1][1]),
+                                      "max_div": outs[0][2]},
+                 "note": "one step from the same state, the mixed forms against the all-FP64 form"}
 
     # e2e: flow state from pinned host memory each step, result back to the host
     shp3 = ctx.shape + (3,)
@@ -886,7 +909,7 @@ def main():
         ctx.set_field(vfs.UCONT, h_uc)
         ctx.set_field(vfs.UCAT, h_u)
         ctx.set_field(vfs.P, h_p)
-        st = ctx.step(precision=0, rtol=1e-10, graph=1)
+        st = ctx.step(precision=MIXED, rtol=1e-10, graph=1)
         ctx.get_field(vfs.UCONT, out=h_uc)
         ctx.get_field(vfs.UCAT, out=h_u)
         ctx.get_field(vfs.P, out=h_p)
@@ -907,27 +930,27 @@ def main():
     achieved = KERNEL_BYTES[dom] * ncell / (launch[dom] * 1e-3) / 1e9
     kernel_frac = {k: round(KERNEL_BYTES[k] * ncell / (launch[k] * 1e-3) / 1e9 / peak, 3)
                    for k in KERNEL_BYTES if k in launch}
-    # Amdahl: one V-cycle per FGMRES iteration; everything else in the step is the same FP64
-    # work in both forms
+    # Amdahl of the FP32 V-cycle form (precision 0): one V-cycle per FGMRES iteration;
+    # everything else in its step is the same FP64 work as in the FP64 form
     v32, v64 = launch["vcycle_fp32"], launch["vcycle_fp64"]
-    common = ms_mixed - its * v32
+    common = ms_vc - its0 * v32
     amdahl = {"vcycle_fp32_ms": round(v32, 4), "vcycle_fp64_ms": round(v64, 4),
               "vcycle_speedup": round(v64 / v32, 3), "vcycles_per_step": {"mixed": its, "fp64": its64},
-              "rest_of_step_ms": round(common, 3),
+              "vcycles_per_step_fp32_vcycle_form": its0, "rest_of_step_ms": round(common, 3),
               "fp64_predicted_ms": round(common + its64 * v64, 3),
               "formfunction2_ms_per_step": round(4 * launch["formfunction2"], 3),
               "speedup_bound_vcycle_free": round(ms_fp64 / common, 3),
               "speedup_bound_vcycle_2x": round(ms_fp64 / (common + its64 * v64 / 2), 3),
-              "note": "rest_of_step = mixed step - iterations x FP32 V-cycle (every other kernel is the "
-                      "same FP64 work in both forms); bounds: FP64 step / mixed step if the V-cycle cost "
-                      "nothing, or ran at twice the FP64 speed"}
+              "note": "for the FP32 V-cycle form (precision 0): rest_of_step = its step - iterations x FP32 "
+                      "V-cycle (every other kernel is the same FP64 work as in the FP64 form); bounds: FP64 "
+                      "step / that step if the V-cycle cost nothing, or ran at twice the FP64 speed"}
     launches_per_step = None
 
     if dist is not None:
         ms_mixed, ms_fp64, e2e_ms = max_over_ranks([ms_mixed, ms_fp64, e2e_ms], dist, torch, "cuda")
 
     n0 = ctx.launch_count()
-    ctx.step(precision=0, rtol=1e-10, graph=1)
+    ctx.step(precision=MIXED, rtol=1e-10, graph=1)
     launches_per_step = ctx.launch_count() - n0
     ctx.close()
     del keep
@@ -997,6 +1020,9 @@ def main():
             "step_form": "one CUDA graph per step (captured once, replayed; the Poisson solve's loops as "
                          "conditional nodes); launched_ms_per_step: the same kernels launched one by one",
             "mixed_speedup_vs_fp64": round(ms_fp64 / ms_mixed, 3),
+            "fp32_vcycle_form": {"ms_per_step": round(ms_vc, 3), "speedup_vs_fp64": round(ms_fp64 / ms_vc, 3),
+                                 "poisson_iterations": its0, "max_div": maxdiv0,
+                                 "note": "precision 0: only the V-cycle in FP32, the Krylov vectors FP64"},
             "max_div": {"mixed": maxdiv, "fp64": maxdiv64},
             "poisson_iterations": {"mixed": its, "fp64": its64},
             "mixed_vs_fp64": mixed_err,

@@ -113,7 +113,12 @@ enum {
 
 /* Poisson solver options (replaces PoissonSolver_Hypre, poisson_hypre.c:498). */
 typedef struct {
-  int precision;     /* 0: mixed (FP32 V-cycle inside FP64 FGMRES), 1: all-FP64 */
+  int precision;     /* 0: mixed (FP32 V-cycle inside FP64 FGMRES), 1: all-FP64, 2: FP32 inner
+                        FGMRES (basis, preconditioned vectors, operator apply and V-cycle in
+                        FP32) as iterative refinement: every restart cycle starts from the FP64
+                        residual b - A x and ends when its estimate has fallen by 1e-5 (or at
+                        `restart`), x and the stopping test stay FP64; the transposed (adjoint)
+                        solve runs as 0 */
   int restart;       /* FGMRES restart length (default 30) */
   int max_iter;      /* outer iteration cap (default 200) */
   int levels;        /* multigrid levels including the finest (default 0: every level

@@ -51,7 +51,7 @@ def _context(case):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["inflow_outflow", "les", "sphere"])
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_graph_step_matches_launched_step(name, precision):
     case = _cases()[name]()
     a, b = _context(case), _context(case)

@@ -38,7 +38,7 @@ def channel_64_reference():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [1, 0])
+@pytest.mark.parametrize("precision", [1, 0, 2])
 def test_channel_64_ten_steps_match_reference(channel_64_reference, precision):
     run, want = channel_64_reference
     ctx, stats = multistep.device_run(run.case, run.m, run.u0, run.uc0, 10, precision=precision)

@@ -217,9 +217,9 @@ def test_update_pressure_projection_divergence(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_poisson_solve_matches_direct(name, precision):
-    """Solve to rtol 1e-13 (mixed and FP64) and compare Phi with a dense least-squares
+    """Solve to rtol 1e-13 (mixed, FP64, and FP32 inner FGMRES in FP64 refinement) and compare Phi with a dense least-squares
     solve of the reference's own matrix and right-hand side, both mean-free, to 1e-10
     relative to max |Phi|."""
     case, (R, ctx) = _pair(name)

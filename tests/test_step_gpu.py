@@ -65,7 +65,7 @@ STEP_CASES = {"channel": lambda: small_channel(), "wavy": lambda: small_channel(
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(STEP_CASES))
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_one_step_matches_reference(name, precision):
     case = STEP_CASES[name]()
     case.inlet_flux = 5.0

@@ -342,6 +342,7 @@ int vfs_destroy(vfs_ctx *ctx) {
   Poisson &P = c->ps;
   cudaFree(P.coef); cudaFree(P.fluid);
   cudaFree(P.V); cudaFree(P.Z); cudaFree(P.w); cudaFree(P.r); cudaFree(P.t); cudaFree(P.hdev);
+  cudaFree(P.V32); cudaFree(P.Z32); cudaFree(P.w32);
   mg_free(P);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -671,6 +672,7 @@ int step_graph(Ctx *c, const vfs_solve_opts *opts, vfs_step_stats *st) {
   if (!graph_eligible(c)) return step_core(c, opts, st);
   int rc;
   if ((rc = ensure_gab(c))) return rc;   // set-up work stays outside the graph
+  if ((rc = poisson_prepare(c, opts))) return rc;
   const bool fresh = c->sg.exec && c->sg.key == c->setup_epoch && !memcmp(&c->sg.opts, opts, sizeof(*opts));
   if (!fresh) {
     step_graph_free(c);

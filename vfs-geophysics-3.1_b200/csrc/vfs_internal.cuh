@@ -119,6 +119,9 @@ struct Poisson {
   double *V = nullptr;      // (restart+1) * ldv
   double *Z = nullptr;      // restart * ldv
   double *w = nullptr, *r = nullptr, *t = nullptr;
+  // precision 2 (FP32 inner FGMRES): the basis, the preconditioned vectors and w in FP32
+  int restart32 = 0;
+  float *V32 = nullptr, *Z32 = nullptr, *w32 = nullptr;
   double *hdev = nullptr;   // Gram-Schmidt coefficients on the device (64 doubles)
   bool transpose = false;   // apply A^T (the adjoint solve)
   bool guess = false;       // VFS_PHI holds the last solution for the current unknowns
@@ -168,6 +171,7 @@ constexpr int kKryMax = 31;
 struct KryDev {
   int j, it, jdone, reorth, degen, inner_go, outer_go, conv, fresh, check, maxit, m, cycles;
   double tol, bnorm, bb, r0, rnorm, rr, hn, scale;
+  double inner_rtol, beta;  // precision 2: a cycle ends once its estimate is below inner_rtol * beta
   double hdev[kKryMax + 3];
   double h[kKryMax + 3], h2[kKryMax + 3], h3[kKryMax + 3];
   double H[(kKryMax + 1) * kKryMax], cs[kKryMax], sn[kKryMax], gv[kKryMax + 1], y[kKryMax];
@@ -325,6 +329,7 @@ int poisson_rhs_local(Ctx *c);
 int poisson_set_transpose(Ctx *c, bool on);
 int volume_flux(Ctx *c);
 int poisson_solve(Ctx *c, const vfs_solve_opts *o, vfs_solve_stats *st);
+int poisson_prepare(Ctx *c, const vfs_solve_opts *o);
 int poisson_apply_dev(Ctx *c, const double *x, double *y);
 int update_pressure(Ctx *c);
 int projection(Ctx *c);
@@ -342,6 +347,7 @@ int mg_setup(Ctx *c);
 void mg_free(Poisson &P);
 int mg_precondition(Ctx *c, const double *v, double *z, const vfs_solve_opts &o);
 int mg_precondition_dyn(Ctx *c, const double *V, double *Z, long long ldv, const int *jslot, const vfs_solve_opts &o);
+int mg_precondition_dyn32(Ctx *c, const float *V, float *Z, long long ldv, const int *jslot, const vfs_solve_opts &o);
 int mg_sweep_fine(Ctx *c, int precision);
 
 // reductions (deterministic two-pass); result copied to host

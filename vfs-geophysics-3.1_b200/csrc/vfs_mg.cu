@@ -740,17 +740,18 @@ __global__ void k_mg_active(long long n, const double *__restrict__ op, uint8_t 
 
 // ------------------------------------------------------------------ bottom of the V-cycle
 // The coarse levels are too small to fill the GPU, and a launch per colour pass costs
-// more than the work.  From the first level of at most kBottomCells cells down (8192: on
-// the B200 a 32 x 24 x 32 level is faster as ordinary launches, a 16 x 12 x 16 one in a
-// single block), one thread block runs the rest of the V-cycle (smoothing, restriction, coarsest sweeps,
-// prolongation) with block barriers between the phases; the level data stay in L2.
+// more than the work.  From the first level of at most kBottomCells cells down, one thread
+// block runs the rest of the V-cycle (smoothing, restriction, coarsest sweeps,
+// prolongation) with block barriers between the phases; the level data stay in L2.  On the
+// B200 at 256 x 192 x 256 (V-cycle ms, FP32 / FP64): 512 cells (the 8 x 6 x 8 level down)
+// 1.450 / 2.268, 4096 or 8192 1.470 / 2.313, 32768 1.772 / 2.738.
 constexpr int kBottomMaxLevels = 12;
 #ifndef VFS_BOTTOM_THREADS
 #define VFS_BOTTOM_THREADS 512
 #endif
 constexpr int kBottomThreads = VFS_BOTTOM_THREADS;
 #ifndef VFS_BOTTOM_CELLS
-#define VFS_BOTTOM_CELLS 8192
+#define VFS_BOTTOM_CELLS 512
 #endif
 constexpr long long kBottomCells = VFS_BOTTOM_CELLS;
 
@@ -815,9 +816,9 @@ __global__ void __launch_bounds__(kBottomThreads) k_mg_bottom(Bottom<T> B) {
   }
 }
 
-// DA-layout FP64 vector -> finest-level right-hand side.
-template <typename T>
-__global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, const int *__restrict__ jslot, long long ldv,
+// DA-layout vector (FP64, or FP32 in the FP32 inner Krylov) -> finest-level right-hand side.
+template <typename T, typename VT>
+__global__ void k_to_zebra(Grid g, ZL L, const VT *__restrict__ v, const int *__restrict__ jslot, long long ldv,
                            T *__restrict__ b) {
   pdl_prologue();
   if (jslot) v += (long long)(*jslot) * ldv;  // the j-th basis vector of a device-driven solve
@@ -829,10 +830,10 @@ __global__ void k_to_zebra(Grid g, ZL L, const double *__restrict__ v, const int
   b[zidx(L, i, j, k)] = (T)v[lidx(g, i + 1, j + 1, k + 1)];
 }
 
-// Finest-level solution -> DA-layout FP64 vector (zero off the unknowns).
-template <typename T>
+// Finest-level solution -> DA-layout vector (zero off the unknowns).
+template <typename T, typename VT>
 __global__ void k_from_zebra(Grid g, ZL L, const uint8_t *__restrict__ fluid, const T *__restrict__ x,
-                             const int *__restrict__ jslot, long long ldv, double *__restrict__ z) {
+                             const int *__restrict__ jslot, long long ldv, VT *__restrict__ z) {
   pdl_prologue();
   if (jslot) z += (long long)(*jslot) * ldv;
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -843,7 +844,7 @@ __global__ void k_from_zebra(Grid g, ZL L, const uint8_t *__restrict__ fluid, co
   double v = 0;
   if (fluid[p] && i >= 1 && i <= g.mx - 2 && j >= 1 && j <= g.my - 2 && k >= 1 && k <= g.mz - 2)
     v = (double)x[zidx(L, i - 1, j - 1, k - 1)];
-  z[p] = v;
+  z[p] = (VT)v;
 }
 
 // ------------------------------------------------------------------ host side
@@ -1074,31 +1075,36 @@ static int mg_vcycle(Ctx *c, int l, int nl, const vfs_solve_opts &o) {
   return mg_smooth<T>(c, l, o.post_smooth, false);
 }
 
-template <typename T>
-static int mg_apply(Ctx *c, const double *v, double *z, const vfs_solve_opts &o, const int *jslot = nullptr,
+template <typename T, typename VT = double>
+static int mg_apply(Ctx *c, const VT *v, VT *z, const vfs_solve_opts &o, const int *jslot = nullptr,
                     long long ldv = 0) {
   Poisson &P = c->ps;
   const MGLevel &L0 = P.lv[0];
   const long long ncell = (long long)L0.z.nx * L0.z.ny * L0.z.nz;
   const LvT<T> l0 = lvt<T>(L0);
   int rc;
-  if ((rc = launch_chain(c, "k_to_zebra", k_to_zebra<T>, dim3(nblocks(ncell, 256)), dim3(256), 0, c->g, L0.z, v,
+  if ((rc = launch_chain(c, "k_to_zebra", k_to_zebra<T, VT>, dim3(nblocks(ncell, 256)), dim3(256), 0, c->g, L0.z, v,
                          jslot, ldv, l0.b)))
     return rc;
   const int nl = o.levels > 0 ? std::min((int)P.lv.size(), o.levels) : (int)P.lv.size();
   if ((rc = mg_vcycle<T>(c, 0, nl, o))) return rc;
-  return launch_chain(c, "k_from_zebra", k_from_zebra<T>, dim3(nblocks(c->g.N, 256)), dim3(256), 0, c->g, L0.z,
+  return launch_chain(c, "k_from_zebra", k_from_zebra<T, VT>, dim3(nblocks(c->g.N, 256)), dim3(256), 0, c->g, L0.z,
                       P.fluid, l0.x, jslot, ldv, z);
 }
 
 // z = M^-1 v: one V-cycle in FP32 (precision 0) or FP64.
 int mg_precondition(Ctx *c, const double *v, double *z, const vfs_solve_opts &o) {
-  return o.precision == 0 ? mg_apply<float>(c, v, z, o) : mg_apply<double>(c, v, z, o);
+  return o.precision != 1 ? mg_apply<float>(c, v, z, o) : mg_apply<double>(c, v, z, o);
 }
 
 // z_j = M^-1 v_j with v_j = V + j ldv, z_j = Z + j ldv and j read on the device (*jslot).
 int mg_precondition_dyn(Ctx *c, const double *V, double *Z, long long ldv, const int *jslot, const vfs_solve_opts &o) {
-  return o.precision == 0 ? mg_apply<float>(c, V, Z, o, jslot, ldv) : mg_apply<double>(c, V, Z, o, jslot, ldv);
+  return o.precision != 1 ? mg_apply<float>(c, V, Z, o, jslot, ldv) : mg_apply<double>(c, V, Z, o, jslot, ldv);
+}
+
+// The same with FP32 vectors (the FP32 inner Krylov of precision 2): an FP32 V-cycle.
+int mg_precondition_dyn32(Ctx *c, const float *V, float *Z, long long ldv, const int *jslot, const vfs_solve_opts &o) {
+  return mg_apply<float, float>(c, V, Z, o, jslot, ldv);
 }
 
 // One smoothing sweep of the finest level (both colours), for timing.

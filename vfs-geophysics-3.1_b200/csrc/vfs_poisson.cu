@@ -540,13 +540,31 @@ __device__ __forceinline__ bool guard_off(const Guard &q) { return q.flag && ((*
 static Guard always() { return Guard{nullptr, 0}; }
 
 // base + (*j + off) * ldv (base when j is null).
-struct DynPtr {
-  double *base;
+template <typename B>
+struct DynPtrT {
+  B *base;
   long long ldv;
   const int *j;
   int off;
-  __device__ __forceinline__ double *get() const { return j ? base + (long long)(*j + off) * ldv : base; }
+  __device__ __forceinline__ B *get() const { return j ? base + (long long)(*j + off) * ldv : base; }
 };
+using DynPtr = DynPtrT<double>;
+
+// Two consecutive basis entries as FP64 (the FP32 basis of precision 2 is widened on load
+// and rounded on store; every sum and product is FP64).
+__device__ __forceinline__ double2 ld2(const double *__restrict__ p, long long i) {
+  return reinterpret_cast<const double2 *>(p)[i];
+}
+__device__ __forceinline__ double2 ld2(const float *__restrict__ p, long long i) {
+  const float2 f = reinterpret_cast<const float2 *>(p)[i];
+  return make_double2((double)f.x, (double)f.y);
+}
+__device__ __forceinline__ void st2(double *__restrict__ p, long long i, double2 v) {
+  reinterpret_cast<double2 *>(p)[i] = v;
+}
+__device__ __forceinline__ void st2(float *__restrict__ p, long long i, double2 v) {
+  reinterpret_cast<float2 *>(p)[i] = make_float2((float)v.x, (float)v.y);
+}
 
 // Sets a graph conditional from the device (only in a captured solve).
 __device__ __forceinline__ void set_cond(unsigned long long h, int use, int v) {
@@ -558,6 +576,27 @@ __global__ void k_apply_dyn(Grid g, const double *__restrict__ coef, DynPtr x, d
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= g.N) return;
   y[p] = apply_row64<NS>(g, coef, x.get(), p);
+}
+// The inner operator of precision 2: FP32 vectors, the FP64 coefficients, FP64 products and
+// sum, the result rounded to FP32 (FP32 coefficients measured 20-40 % more iterations:
+// iterative refinement converges at the rate of the inner operator's error).
+template <int NS>
+__global__ void k_apply32_dyn(Grid g, const double *__restrict__ coef, DynPtrT<float> xp, float *__restrict__ y) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= g.N) return;
+  const float *__restrict__ x = xp.get();
+  const unsigned up = (unsigned)p, umx = (unsigned)g.mx, umy = (unsigned)g.my;
+  const unsigned q = up / umx;
+  const int i = (int)(up - q * umx);
+  const unsigned kk = q / umy;
+  const int j = (int)(q - kk * umy), k = (int)kk;
+  double s = 0.0;
+#pragma unroll
+  for (int t = 0; t < NS; t++) {
+    const double c = coef[t * g.N + p];
+    if (c != 0.0) s += c * (double)x[nb_index(g, i, j, k, t)];
+  }
+  y[p] = (float)s;
 }
 __global__ void k_apply_t_dyn(Grid g, int ns, const double *__restrict__ coef, DynPtr x, double *y, Guard q) {
   if (guard_off(q)) return;
@@ -578,22 +617,22 @@ __global__ void k_zero_g(long long n, double *y, Guard q) {
   if (p < n) y[p] = 0.0;
 }
 
-// <V_t, w> (t < nv) and <w, w> with nv = j + 1 from the device state.
-template <int NV>
-__device__ __forceinline__ void multidot_body(long long N, long long ldv, const double *__restrict__ V, int nv,
-                                              const double *__restrict__ w, double *__restrict__ parts) {
+// <V_t, w> (t < nv) and <w, w> with nv = j + 1 from the device state (B: the basis type,
+// FP64, or FP32 for precision 2; the sums are FP64).
+template <int NV, typename B>
+__device__ __forceinline__ void multidot_body(long long N, long long ldv, const B *__restrict__ V, int nv,
+                                              const B *__restrict__ w, double *__restrict__ parts) {
   double acc[NV + 1];
 #pragma unroll
   for (int t = 0; t <= NV; t++) acc[t] = 0;
   const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
   for (long long p2 = tid; p2 < N2; p2 += stride) {
-    const double2 wp = w2[p2];
+    const double2 wp = ld2(w, p2);
 #pragma unroll
     for (int t = 0; t < NV; t++) {
       if (t < nv) {
-        const double2 v = reinterpret_cast<const double2 *>(V + t * ldv)[p2];
+        const double2 v = ld2(V + t * ldv, p2);
         acc[t] += v.x * wp.x + v.y * wp.y;
       }
     }
@@ -601,18 +640,19 @@ __device__ __forceinline__ void multidot_body(long long N, long long ldv, const 
   }
   if ((N & 1) && tid == 0) {
     const long long p = N - 1;
-    const double wp = w[p];
+    const double wp = (double)w[p];
 #pragma unroll
     for (int t = 0; t < NV; t++)
-      if (t < nv) acc[t] += V[t * ldv + p] * wp;
+      if (t < nv) acc[t] += (double)V[t * ldv + p] * wp;
     acc[NV] += wp * wp;
   }
   block_sums<NV>(acc, nv, parts);
 }
+template <typename B>
 __global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_multidot_dyn(long long N, long long ldv,
-                                                                             const double *__restrict__ V,
+                                                                             const B *__restrict__ V,
                                                                              const KryDev *__restrict__ kd,
-                                                                             const double *__restrict__ w,
+                                                                             const B *__restrict__ w,
                                                                              double *__restrict__ parts) {
   const int nv = kd->j + 1;
   if (nv <= 4) multidot_body<4>(N, ldv, V, nv, w, parts);
@@ -622,9 +662,9 @@ __global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_multidot_dyn(long
 }
 
 // w -= sum_t h_t V_t (h = kd->hdev), with <V_t, w> and <w, w> of the result.
-template <int NV>
-__device__ __forceinline__ void update_dots_body(long long N, long long ldv, const double *__restrict__ V, int nv,
-                                                 const double *__restrict__ h, double *__restrict__ w,
+template <int NV, typename B>
+__device__ __forceinline__ void update_dots_body(long long N, long long ldv, const B *__restrict__ V, int nv,
+                                                 const double *__restrict__ h, B *__restrict__ w,
                                                  double *__restrict__ parts) {
   double hr[NV], acc[NV + 1];
 #pragma unroll
@@ -633,38 +673,39 @@ __device__ __forceinline__ void update_dots_body(long long N, long long ldv, con
   for (int t = 0; t <= NV; t++) acc[t] = 0;
   const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  double2 *__restrict__ w2 = reinterpret_cast<double2 *>(w);
   for (long long p2 = tid; p2 < N2; p2 += stride) {
     double2 v[NV];
 #pragma unroll
-    for (int t = 0; t < NV; t++)
-      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
-    double2 s = w2[p2];
+    for (int t = 0; t < NV; t++) v[t] = t < nv ? ld2(V + t * ldv, p2) : make_double2(0.0, 0.0);
+    double2 s = ld2(w, p2);
 #pragma unroll
     for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
-    w2[p2] = s;
+    st2(w, p2, s);
+    if (sizeof(B) == 4) s = ld2(w, p2);  // the stored (rounded) values enter the dots
 #pragma unroll
     for (int t = 0; t < NV; t++) acc[t] += v[t].x * s.x + v[t].y * s.y;
     acc[NV] += s.x * s.x + s.y * s.y;
   }
   if ((N & 1) && tid == 0) {
     const long long p = N - 1;
-    double s = w[p];
+    double s = (double)w[p];
 #pragma unroll
     for (int t = 0; t < NV; t++)
-      if (t < nv) s -= hr[t] * V[t * ldv + p];
-    w[p] = s;
+      if (t < nv) s -= hr[t] * (double)V[t * ldv + p];
+    w[p] = (B)s;
+    s = (double)w[p];
 #pragma unroll
     for (int t = 0; t < NV; t++)
-      if (t < nv) acc[t] += V[t * ldv + p] * s;
+      if (t < nv) acc[t] += (double)V[t * ldv + p] * s;
     acc[NV] += s * s;
   }
   block_sums<NV>(acc, nv, parts);
 }
+template <typename B>
 __global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_dots_dyn(long long N, long long ldv,
-                                                                                const double *__restrict__ V,
+                                                                                const B *__restrict__ V,
                                                                                 const KryDev *__restrict__ kd,
-                                                                                double *__restrict__ w,
+                                                                                B *__restrict__ w,
                                                                                 double *__restrict__ parts, Guard q) {
   if (guard_off(q)) return;
   const int nv = kd->j + 1;
@@ -675,45 +716,43 @@ __global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_dots_dyn(l
 }
 
 // out = (w - sum_t h_t V_t) * scale (h = kd->hdev, scale = kd->scale).
-template <int NV>
-__device__ __forceinline__ void update_scale_body(long long N, long long ldv, const double *__restrict__ V, int nv,
-                                                  const double *__restrict__ h, const double *__restrict__ w,
-                                                  double scale, double *__restrict__ out) {
+template <int NV, typename B>
+__device__ __forceinline__ void update_scale_body(long long N, long long ldv, const B *__restrict__ V, int nv,
+                                                  const double *__restrict__ h, const B *__restrict__ w,
+                                                  double scale, B *__restrict__ out) {
   double hr[NV];
 #pragma unroll
   for (int t = 0; t < NV; t++) hr[t] = t < nv ? h[t] : 0.0;
   const long long N2 = N >> 1, stride = (long long)gridDim.x * blockDim.x;
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(w);
-  double2 *__restrict__ o2 = reinterpret_cast<double2 *>(out);
   for (long long p2 = tid; p2 < N2; p2 += stride) {
     double2 v[NV];
 #pragma unroll
-    for (int t = 0; t < NV; t++)
-      v[t] = t < nv ? reinterpret_cast<const double2 *>(V + t * ldv)[p2] : make_double2(0.0, 0.0);
-    double2 s = w2[p2];
+    for (int t = 0; t < NV; t++) v[t] = t < nv ? ld2(V + t * ldv, p2) : make_double2(0.0, 0.0);
+    double2 s = ld2(w, p2);
 #pragma unroll
     for (int t = 0; t < NV; t++) { s.x -= hr[t] * v[t].x; s.y -= hr[t] * v[t].y; }
     s.x *= scale; s.y *= scale;
-    o2[p2] = s;
+    st2(out, p2, s);
   }
   if ((N & 1) && tid == 0) {
     const long long p = N - 1;
-    double s = w[p];
+    double s = (double)w[p];
 #pragma unroll
     for (int t = 0; t < NV; t++)
-      if (t < nv) s -= hr[t] * V[t * ldv + p];
-    out[p] = s * scale;
+      if (t < nv) s -= hr[t] * (double)V[t * ldv + p];
+    out[p] = (B)(s * scale);
   }
 }
+template <typename B>
 __global__ void __launch_bounds__(kKryThreads, VFS_KRY_MINB) k_update_scale_dyn(long long N, long long ldv,
-                                                                                 const double *__restrict__ V,
+                                                                                 const B *__restrict__ V,
                                                                                  const KryDev *__restrict__ kd,
-                                                                                 const double *__restrict__ w,
-                                                                                 DynPtr out, Guard q) {
+                                                                                 const B *__restrict__ w,
+                                                                                 DynPtrT<B> out, Guard q) {
   if (guard_off(q)) return;
   const int nv = kd->j + 1;
-  double *o = out.get();
+  B *o = out.get();
   if (nv <= 4) update_scale_body<4>(N, ldv, V, nv, kd->hdev, w, kd->scale, o);
   else if (nv <= 8) update_scale_body<8>(N, ldv, V, nv, kd->hdev, w, kd->scale, o);
   else if (nv <= 16) update_scale_body<16>(N, ldv, V, nv, kd->hdev, w, kd->scale, o);
@@ -805,22 +844,24 @@ __global__ void k_sub_norm_g(long long n, const double *__restrict__ b, double *
   if (threadIdx.x == 0) parts[blockIdx.x] = sh[0];
 }
 
-// dst = src * (*scale), guarded.
-__global__ void k_scale_copy_dyn(long long n, const double *__restrict__ src, const double *__restrict__ scale,
-                                 DynPtr dst, Guard q) {
+// dst = src * (*scale), guarded (FP64 arithmetic, stored in dst's type).
+template <typename S, typename D>
+__global__ void k_scale_copy_dyn(long long n, const S *__restrict__ src, const double *__restrict__ scale,
+                                 DynPtrT<D> dst, Guard q) {
   if (guard_off(q)) return;
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (p < n) dst.get()[p] = src[p] * (*scale);
+  if (p < n) dst.get()[p] = (D)((double)src[p] * (*scale));
 }
-// x += sum_t y_t Z_t for t < kd->jdone (y = kd->y).
-__global__ void k_lincomb_add_dyn(long long n, long long ldv, const double *__restrict__ Z,
+// x += sum_t y_t Z_t for t < kd->jdone (y = kd->y); x is FP64 whatever Z's type.
+template <typename B>
+__global__ void k_lincomb_add_dyn(long long n, long long ldv, const B *__restrict__ Z,
                                   const KryDev *__restrict__ kd, double *__restrict__ x) {
   const int m = kd->jdone;
   if (m <= 0) return;
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= n) return;
   double s = x[p];
-  for (int t = 0; t < m; t++) s += kd->y[t] * Z[(long long)t * ldv + p];
+  for (int t = 0; t < m; t++) s += kd->y[t] * (double)Z[(long long)t * ldv + p];
   x[p] = s;
 }
 // x += -sum / nfluid on the fluid cells (sum = ds[DS_PHISUM]).
@@ -835,7 +876,8 @@ __global__ void k_shift_mean(long long n, const uint8_t *fluid, const double *__
 // ---- control kernels (one thread)
 // After the initial residual (kd->rr) and, with a starting guess, <b, b> (kd->bb).
 __global__ void k_kry_init(KryDev *kd, double rtol, double atol, int warm, int maxit, int m, unsigned long long h_outer,
-                           int use_graph) {
+                           int use_graph, double inner_rtol) {
+  kd->inner_rtol = inner_rtol;
   kd->rnorm = sqrt(kd->rr);
   kd->bnorm = warm ? sqrt(kd->bb) : kd->rnorm;
   kd->r0 = kd->rnorm;
@@ -856,6 +898,7 @@ __global__ void k_kry_cycle(KryDev *kd, unsigned long long h_inner, int use_grap
   if (!kd->fresh) kd->rnorm = sqrt(kd->rr);
   kd->fresh = 0;
   const double beta = kd->rnorm;
+  kd->beta = beta;
   kd->j = 0;
   kd->jdone = 0;
   kd->check = 0;
@@ -936,7 +979,9 @@ __global__ void k_kry_givens(KryDev *kd, unsigned long long h_inner, int use_gra
   kd->it++;
   kd->jdone = j + 1;
   kd->rnorm = fabs(kd->gv[j + 1]);
-  const bool stop = kd->rnorm <= kd->tol || kd->hn == 0;
+  // precision 2 also ends the cycle (an iterative-refinement sweep) once the FP32 Arnoldi
+  // estimate has fallen by inner_rtol; the next cycle restarts from the FP64 residual
+  const bool stop = kd->rnorm <= kd->tol || kd->hn == 0 || kd->rnorm <= kd->inner_rtol * kd->beta;
   kd->j = j + 1;
   kd->inner_go = !stop && kd->j < m && kd->it < kd->maxit;
   set_cond(h_inner, use_graph, kd->inner_go);
@@ -1005,55 +1050,88 @@ static int apply_dyn(Ctx *c, double *Z, double *w) {
     c->launches++, k_apply_dyn<NSLOT><<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, P.coef, dyn(Z, P.ldv, &kd->j, 0), w);
   return check_launch(c, "k_apply_dyn");
 }
+static int apply32_dyn(Ctx *c, float *Z, float *w) {
+  Poisson &P = c->ps;
+  const long long N = c->g.N;
+  const DynPtrT<float> z{Z, P.ldv, &c->kd->j, 0};
+  if (P.nslot == 7)
+    c->launches++, k_apply32_dyn<7><<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, P.coef, z, w);
+  else
+    c->launches++, k_apply32_dyn<NSLOT><<<nblocks(N, 256), 256, 0, c->stream>>>(c->g, P.coef, z, w);
+  return check_launch(c, "k_apply32_dyn");
+}
 
-// One Arnoldi step of the device-driven FGMRES (body of the inner loop).
-static int kry_body(Ctx *c, const vfs_solve_opts &o, unsigned long long h_inner, int use_graph) {
+// One Arnoldi step of the device-driven FGMRES (body of the inner loop), on the basis of
+// type B (FP64; FP32 for precision 2, whose preconditioner and operator apply are FP32).
+template <typename B>
+static int kry_body_t(Ctx *c, const vfs_solve_opts &o, unsigned long long h_inner, int use_graph, B *V, B *Z, B *w) {
   Poisson &P = c->ps;
   KryDev *kd = c->kd;
   const long long N = c->g.N;
   const int kg = kry_grid(c);
   int rc;
-  if ((rc = mg_precondition_dyn(c, P.V, P.Z, P.ldv, &kd->j, o))) return rc;          // z_j = M^-1 v_j
-  if ((rc = apply_dyn(c, P.Z, P.w))) return rc;                                          // w = A z_j
-  c->launches++, k_multidot_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w, c->red);
+  if (sizeof(B) == 4) {
+    if ((rc = mg_precondition_dyn32(c, (const float *)V, (float *)Z, P.ldv, &kd->j, o))) return rc;  // z_j = M^-1 v_j
+    if ((rc = apply32_dyn(c, (float *)Z, (float *)w))) return rc;                                     // w = A z_j
+  } else {
+    if ((rc = mg_precondition_dyn(c, (const double *)V, (double *)Z, P.ldv, &kd->j, o))) return rc;
+    if ((rc = apply_dyn(c, (double *)Z, (double *)w))) return rc;
+  }
+  c->launches++, k_multidot_dyn<B><<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, V, kd, w, c->red);
   c->launches++, k_sum_rows_dyn<<<kKryMax + 2, 256, 0, c->stream>>>(c->red, kd, kg, kd->h, always());
   c->launches++, k_kry_ctl_a<<<1, 1, 0, c->stream>>>(kd);
   if ((rc = check_launch(c, "FGMRES Gram-Schmidt"))) return rc;
   const Guard reorth{&kd->reorth, 1}, degen{&kd->degen, 1}, plain{&kd->degen, 0};
-  c->launches++, k_update_dots_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w, c->red, reorth);
+  c->launches++, k_update_dots_dyn<B><<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, V, kd, w, c->red, reorth);
   c->launches++, k_sum_rows_dyn<<<kKryMax + 2, 256, 0, c->stream>>>(c->red, kd, kg, kd->h2, reorth);
   c->launches++, k_kry_ctl_b<<<1, 1, 0, c->stream>>>(kd);
-  c->launches++, k_update_dots_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w, c->red, degen);
+  c->launches++, k_update_dots_dyn<B><<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, V, kd, w, c->red, degen);
   c->launches++, k_sum_rows_dyn<<<kKryMax + 2, 256, 0, c->stream>>>(c->red, kd, kg, kd->h3, degen);
   c->launches++, k_kry_ctl_c<<<1, 1, 0, c->stream>>>(kd);
   if ((rc = check_launch(c, "FGMRES re-orthogonalisation"))) return rc;
-  c->launches++, k_update_scale_dyn<<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, P.V, kd, P.w,
-                                                                         dyn(P.V, P.ldv, &kd->j, 1), plain);
-  c->launches++, k_scale_copy_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.w, &kd->scale,
-                                                                           dyn(P.V, P.ldv, &kd->j, 1), degen);
+  const DynPtrT<B> next{V, P.ldv, &kd->j, 1};
+  c->launches++, k_update_scale_dyn<B><<<kg, kKryThreads, 0, c->stream>>>(N, P.ldv, V, kd, w, next, plain);
+  c->launches++, k_scale_copy_dyn<B, B><<<nblocks(N, 256), 256, 0, c->stream>>>(N, w, &kd->scale, next, degen);
   c->launches++, k_kry_givens<<<1, 1, 0, c->stream>>>(kd, h_inner, use_graph);
   return check_launch(c, "FGMRES Givens");
 }
 
-static int kry_cycle_start(Ctx *c, const double *b, double *x, unsigned long long h_inner, int use_graph) {
+static bool fp32_inner(const vfs_solve_opts &o) { return o.precision == 2; }
+
+static int kry_body(Ctx *c, const vfs_solve_opts &o, unsigned long long h_inner, int use_graph) {
+  Poisson &P = c->ps;
+  return fp32_inner(o) ? kry_body_t<float>(c, o, h_inner, use_graph, P.V32, P.Z32, P.w32)
+                       : kry_body_t<double>(c, o, h_inner, use_graph, P.V, P.Z, P.w);
+}
+
+static int kry_cycle_start(Ctx *c, const vfs_solve_opts &o, const double *b, double *x, unsigned long long h_inner,
+                           int use_graph) {
   Poisson &P = c->ps;
   KryDev *kd = c->kd;
   const long long N = c->g.N;
   int rc;
   if ((rc = residual_dev(c, b, x, P.r, &kd->rr, Guard{&kd->fresh, 0}))) return rc;
   c->launches++, k_kry_cycle<<<1, 1, 0, c->stream>>>(kd, h_inner, use_graph);
-  c->launches++, k_scale_copy_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.r, &kd->scale, dyn(P.V, P.ldv, nullptr, 0),
-                                                                           Guard{&kd->inner_go, 1});
+  if (fp32_inner(o))
+    c->launches++, k_scale_copy_dyn<double, float><<<nblocks(N, 256), 256, 0, c->stream>>>(
+        N, P.r, &kd->scale, DynPtrT<float>{P.V32, P.ldv, nullptr, 0}, Guard{&kd->inner_go, 1});
+  else
+    c->launches++, k_scale_copy_dyn<double, double><<<nblocks(N, 256), 256, 0, c->stream>>>(
+        N, P.r, &kd->scale, dyn(P.V, P.ldv, nullptr, 0), Guard{&kd->inner_go, 1});
   return check_launch(c, "FGMRES cycle start");
 }
 
-static int kry_cycle_end(Ctx *c, const double *b, double *x, unsigned long long h_outer, int use_graph) {
+static int kry_cycle_end(Ctx *c, const vfs_solve_opts &o, const double *b, double *x, unsigned long long h_outer,
+                         int use_graph) {
   Poisson &P = c->ps;
   KryDev *kd = c->kd;
   const long long N = c->g.N;
   int rc;
   c->launches++, k_kry_backsub<<<1, 1, 0, c->stream>>>(kd);
-  c->launches++, k_lincomb_add_dyn<<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z, kd, x);
+  if (fp32_inner(o))
+    c->launches++, k_lincomb_add_dyn<float><<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z32, kd, x);
+  else
+    c->launches++, k_lincomb_add_dyn<double><<<nblocks(N, 256), 256, 0, c->stream>>>(N, P.ldv, P.Z, kd, x);
   if ((rc = check_launch(c, "FGMRES update"))) return rc;
   if ((rc = residual_dev(c, b, x, P.r, &kd->rr, Guard{&kd->check, 1}))) return rc;
   c->launches++, k_kry_confirm<<<1, 1, 0, c->stream>>>(kd, h_outer, use_graph);
@@ -1132,7 +1210,9 @@ static int while_end(Ctx *c, WhileLoop &w) {
 // rtol * ||b|| either way, as in HYPRE's GMRES.
 // The iteration runs on the device (KryDev); the host drives its two loops by reading
 // their flags, or, while a step is captured, the loops are conditional WHILE nodes.
-int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
+// The solver options with defaults filled in (precision 2 falls back to 0 for the
+// transposed operator, which has no FP32 form).
+static vfs_solve_opts solve_opts(const Ctx *c, const vfs_solve_opts *oin) {
   vfs_solve_opts o;
   memset(&o, 0, sizeof(o));
   o.precision = 0; o.restart = 30; o.max_iter = 200; o.levels = 0; o.pre_smooth = 3; o.post_smooth = 3;
@@ -1152,19 +1232,54 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   if (o.restart > kKryMax) o.restart = kKryMax;
   if (o.pre_smooth < 1) o.pre_smooth = 1;
   if (o.coarse_iters < 1) o.coarse_iters = 1;
+  if (o.precision == 2 && c->ps.transpose) o.precision = 0;
+  return o;
+}
+
+// The inner tolerance of precision 2: an FP32 cycle reduces its residual estimate by at
+// most this factor before the FP64 residual is formed again (FP32 keeps about 7 digits).
+static const double kInnerRtol = 1e-5;
+
+// Allocates the solver's workspace for options o (the Krylov basis, and for precision 2
+// its FP32 form); outside a stream capture.
+int poisson_prepare(Ctx *c, const vfs_solve_opts *oin) {
+  const vfs_solve_opts o = solve_opts(c, oin);
   Poisson &P = c->ps;
   const long long N = c->g.N;
-  int rc;
+  const bool f32 = o.precision == 2;
+  if (P.restart >= o.restart && (!f32 || P.restart32 >= o.restart)) return VFS_OK;
+  if (c->capturing) return set_err(c, VFS_ERR_STATE, "poisson_solve: Krylov basis not allocated before capture");
+  c->setup_epoch++;  // a captured step graph holds the old buffers
+  P.ldv = (N + 31) / 32 * 32;
   if (P.restart < o.restart) {
-    if (c->capturing) return set_err(c, VFS_ERR_STATE, "poisson_solve: Krylov basis not allocated before capture");
     cudaFree(P.V); cudaFree(P.Z);
     P.V = P.Z = nullptr;
-    P.ldv = (N + 31) / 32 * 32;
+    P.restart = 0;
     if (cudaMalloc(&P.V, sizeof(double) * P.ldv * (o.restart + 1)) != cudaSuccess ||
         cudaMalloc(&P.Z, sizeof(double) * P.ldv * o.restart) != cudaSuccess)
       return set_err(c, VFS_ERR_CUDA, "poisson_solve: Krylov basis allocation failed");
     P.restart = o.restart;
   }
+  if (!f32) return VFS_OK;
+  if (P.restart32 < o.restart) {
+    cudaFree(P.V32); cudaFree(P.Z32); cudaFree(P.w32);
+    P.V32 = P.Z32 = P.w32 = nullptr;
+    P.restart32 = 0;
+    if (cudaMalloc(&P.V32, sizeof(float) * P.ldv * (o.restart + 1)) != cudaSuccess ||
+        cudaMalloc(&P.Z32, sizeof(float) * P.ldv * o.restart) != cudaSuccess ||
+        cudaMalloc(&P.w32, sizeof(float) * P.ldv) != cudaSuccess)
+      return set_err(c, VFS_ERR_CUDA, "poisson_solve: FP32 Krylov basis allocation failed");
+    P.restart32 = o.restart;
+  }
+  return VFS_OK;
+}
+
+int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
+  const vfs_solve_opts o = solve_opts(c, oin);
+  Poisson &P = c->ps;
+  const long long N = c->g.N;
+  int rc;
+  if ((rc = poisson_prepare(c, &o))) return rc;
   if ((rc = ensure_red(c, 34 * std::max(kKryBlocks, kry_grid(c)) + (int)nblocks(N, 256) + 64))) return rc;
   if (!c->capturing) cudaEventRecord(c->ev0, c->stream);
   KryDev *kd = c->kd;
@@ -1185,20 +1300,21 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
   cudaGraphConditionalHandle h_outer = 0, h_inner = 0;
   if (use_graph && (rc = cond_handle(c, &h_outer))) return rc;
   c->launches++, k_kry_init<<<1, 1, 0, c->stream>>>(kd, o.rtol, o.atol, warm ? 1 : 0, o.max_iter, m,
-                                                     (unsigned long long)h_outer, use_graph);
+                                                     (unsigned long long)h_outer, use_graph,
+                                                     o.precision == 2 ? kInnerRtol : 0.0);
   if ((rc = check_launch(c, "k_kry_init"))) return rc;
   if (use_graph) {
     WhileLoop w0, w1;
     if ((rc = while_begin(c, 0, h_outer, w0))) return rc;
     if ((rc = cond_handle(c, &h_inner))) return rc;
     const long long l0 = c->launches;
-    if ((rc = kry_cycle_start(c, b, x, (unsigned long long)h_inner, 1))) return rc;
+    if ((rc = kry_cycle_start(c, o, b, x, (unsigned long long)h_inner, 1))) return rc;
     if ((rc = while_begin(c, 1, h_inner, w1))) return rc;
     const long long l1 = c->launches;
     if ((rc = kry_body(c, o, (unsigned long long)h_inner, 1))) return rc;
     c->sg.body_launches = c->launches - l1;
     if ((rc = while_end(c, w1))) return rc;
-    if ((rc = kry_cycle_end(c, b, x, (unsigned long long)h_outer, 1))) return rc;
+    if ((rc = kry_cycle_end(c, o, b, x, (unsigned long long)h_outer, 1))) return rc;
     c->sg.cycle_launches = c->launches - l0 - c->sg.body_launches;
     if ((rc = while_end(c, w0))) return rc;
   } else {
@@ -1206,13 +1322,13 @@ int poisson_solve(Ctx *c, const vfs_solve_opts *oin, vfs_solve_stats *st) {
       int go = 0;
       if ((rc = read_flag(c, &kd->outer_go, &go))) return rc;
       if (!go) break;
-      if ((rc = kry_cycle_start(c, b, x, 0, 0))) return rc;
+      if ((rc = kry_cycle_start(c, o, b, x, 0, 0))) return rc;
       for (;;) {
         if ((rc = read_flag(c, &kd->inner_go, &go))) return rc;
         if (!go) break;
         if ((rc = kry_body(c, o, 0, 0))) return rc;
       }
-      if ((rc = kry_cycle_end(c, b, x, 0, 0))) return rc;
+      if ((rc = kry_cycle_end(c, o, b, x, 0, 0))) return rc;
     }
   }
   // Remove_Nullspace: phi += -mean(phi) over fluid cells
@@ -1486,7 +1602,6 @@ namespace vfs {
 // Launches one kernel of the path `reps` times on the context's stream (no host sync),
 // so a caller can bracket it with events recorded on that stream.
 int run_kernel(Ctx *c, int which, int reps) {
-  const Grid &g = c->g;
   Poisson &P = c->ps;
   int rc = VFS_OK;
   if ((which >= 3) && !P.built && (rc = poisson_lhs(c))) return rc;

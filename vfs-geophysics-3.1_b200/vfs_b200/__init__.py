@@ -184,7 +184,8 @@ def grid_write(path, x, y, z, fmt=GRID_ASCII):
 
 
 def load_library(path=None):
-    """Load libvfs_b200.so (built in-tree by build.py).  Raises if it is absent."""
+    """Load libvfs_b200.so (built in-tree by build.py), or the library at `path`, which the
+    contexts created afterwards then use.  Raises if it is absent."""
     global _lib
     if _lib is not None and path is None:
         return _lib
@@ -245,8 +246,7 @@ def load_library(path=None):
     lib.vfs_grid_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                   ip, ip, ip, vp, vp, vp]
     lib.vfs_grid_write.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
-    if path is None:
-        _lib = lib
+    _lib = lib
     return lib
 
 
